@@ -1,0 +1,87 @@
+"""ctypes binding of libcmmdft_b200.so (the C ABI declared in include/cmmdft_b200.h).
+
+The product path has no CPU fallback: importing this module on a machine
+without the built library, or calling a kernel without a CUDA device, raises.
+"""
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libcmmdft_b200.so")
+
+# cmm_stat_* slots (include/cmmdft_b200.h)
+STAT_N, STAT_IUE, STAT_NONFIN, STAT_FID, STAT_FEXT, STAT_RES2, STAT_PHI, STAT_MFA, \
+    STAT_N3MAX, STAT_GNONFIN, STAT_GRAM0 = range(11)
+NSTAT = 18
+MAX_HIST = 8
+MAX_FIELDS = 12
+FMT, MFMT, WBII, ANTISYM = 0, 1, 2, 8
+CLIP_NONE, CLIP_PICARD, CLIP_DENSITY = 0, 1, 2
+
+
+class CmmError(RuntimeError):
+    """A cmm_* entry point returned a non-zero status."""
+
+
+_lib = None
+
+c_int, c_double, c_void_p, c_ll = ctypes.c_int, ctypes.c_double, ctypes.c_void_p, ctypes.c_longlong
+P = ctypes.POINTER
+
+_SIGS = {
+    "cmm_version": ([], c_int),
+    "cmm_status_string": ([c_int], ctypes.c_char_p),
+    "cmm_grid_create": ([c_int, c_int, c_int, P(c_double), P(c_void_p)], c_int),
+    "cmm_grid_destroy": ([c_void_p], c_int),
+    "cmm_grid_spectrum_size": ([c_void_p, P(c_ll), P(c_int)], c_int),
+    "cmm_spectrum_index": ([c_void_p, P(c_int), P(c_int), P(c_int)], c_int),
+    "cmm_plane_smem_bytes": ([c_void_p, c_int, P(ctypes.c_size_t)], c_int),
+    "cmm_extpot_lj": ([c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_double, c_double,
+                       c_double, c_double, c_void_p, c_void_p], c_int),
+    "cmm_rfft3d": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
+    "cmm_irfft3d": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
+    "cmm_mfa_kernel": ([c_void_p, c_double, c_double, c_double, c_double, c_double, c_int, c_void_p,
+                        c_void_p, P(ctypes.c_size_t), P(c_double), c_void_p], c_int),
+    "cmm_fmt_c1": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p,
+                    c_void_p, c_void_p, c_int, c_int, c_void_p], c_int),
+    "cmm_picard_static_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_void_p,
+                                c_void_p, c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int, c_void_p], c_int),
+    "cmm_residual_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_ll,
+                           c_void_p, P(c_void_p), c_int, c_ll, c_void_p, c_int, c_void_p], c_int),
+    "cmm_mix_step": ([c_void_p, c_int, c_void_p, c_void_p, P(c_void_p), P(c_ll), c_int, c_int, c_double,
+                      c_double, c_void_p, c_ll, c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int,
+                      c_void_p], c_int),
+    "cmm_stats_finalize": ([c_int, c_void_p, c_void_p, c_int, ctypes.c_uint, c_void_p, c_void_p], c_int),
+}
+
+
+def lib():
+    """Load the library (once) and declare every exported signature."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise CmmError("%s is missing: build it with `python -m cmmdft_b200.build` "
+                       "(there is no CPU fallback)" % LIB_PATH)
+    L = ctypes.CDLL(LIB_PATH)
+    for name, (args, res) in _SIGS.items():
+        fn = getattr(L, name)
+        fn.argtypes = args
+        fn.restype = res
+    _lib = L
+    return L
+
+
+def exported_symbols():
+    return list(_SIGS)
+
+
+def check(rc, what=""):
+    if rc != 0:
+        msg = lib().cmm_status_string(rc).decode()
+        raise CmmError("%s failed: %s (status %d)" % (what or "cmm call", msg, rc))
+
+
+def ptr(t):
+    """Device pointer of a torch tensor (None -> NULL)."""
+    return None if t is None else ctypes.c_void_p(t.data_ptr())

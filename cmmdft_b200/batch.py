@@ -1,0 +1,501 @@
+"""Batched fixed-point solves on one grid shape (one "shape group").
+
+``BatchSolve`` runs B independent solves (e.g. the pressures of an isotherm
+on one host) together: every field operation is one kernel launch over all
+active instances, and the per-instance control flow of the reference's
+solvers is evaluated on the host from per-instance scalars (one small
+device-to-host read per decision point).  A batch of one is the plain
+per-point solve.
+
+Control flow restated from cmmdft/solver.py:
+  Solver._solve / solve            :236-345 (loop, non-finite retry)
+  _check_convergence               :167-234 (RES / RIUE)
+  _get_Omega                       :103-119
+  Picard.update_rho_static         :392-401
+  Picard.update_rho_hybrid         :403-457 (+ _get_alpha_max :150-165)
+  Anderson.update_rho              :546-579
+  Anderson.update_rho_Anderson     :581-604 (+ damping :537-544)
+The Anderson mixing coefficients minimise ||sum a_i r_i|| subject to
+a_i >= 0, sum a_i = 1 exactly (active-set enumeration on the Gram matrix)
+instead of through SLSQP; both target the same minimiser.
+"""
+import itertools
+
+import numpy as np
+import scipy.optimize as opt
+import torch
+
+from . import _lib as L
+from . import engine as E
+from .units import angstrom, kjmol
+
+
+class NoSolutionError(Exception):
+    """All retries of a solve hit non-finite densities (solver.py:343-345)."""
+
+
+def simplex_qp(M, idx):
+    """argmin_a a^T M a  s.t. a >= 0, sum a = 1, over the entries ``idx``.
+
+    Exact minimiser by enumerating supports: on each support S the
+    equality-constrained minimum is a_S = M_SS^+ 1 / (1^T M_SS^+ 1); the
+    feasible candidate with the lowest objective is the global minimum of
+    this convex problem.
+    """
+    n = len(idx)
+    Ms = M[np.ix_(idx, idx)]
+    best, best_val = None, np.inf
+    scale = max(np.max(np.abs(np.diag(Ms))), 1e-300)
+    for k in range(1, n + 1):
+        for S in itertools.combinations(range(n), k):
+            A = Ms[np.ix_(S, S)] / scale
+            one = np.ones(k)
+            try:
+                x = np.linalg.solve(A, one)
+            except np.linalg.LinAlgError:
+                x = np.linalg.lstsq(A, one, rcond=None)[0]
+            s = x.sum()
+            if not np.isfinite(s) or abs(s) < 1e-300:
+                continue
+            a = x / s
+            if np.any(a < -1e-14):
+                continue
+            a = np.clip(a, 0.0, None)
+            a /= a.sum()
+            full = np.zeros(n)
+            full[list(S)] = a
+            val = full @ Ms @ full
+            if val < best_val * (1 - 1e-13) or best is None:
+                best, best_val = full, val
+    if best is None:
+        best = np.full(n, 1.0 / n)
+    return best
+
+
+class BatchSolve(object):
+    """Solve B fixed points that share a Functional (grid, host, guest, T).
+
+    method: 'static' (Picard), 'hybrid' (Picard line search), 'anderson'
+    or 'hybridanderson' (the reference's Anderson default).
+    """
+
+    def __init__(self, fn, chempots, method='hybridanderson', nsteps=500, threshold=1e-6,
+                 criterion='res', alpha_mix=0.1, m=5, damping=0.3, delta=0.2, damping_max=0.8,
+                 damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5)):
+        self.fn = fn
+        self.plan = fn.plan
+        self.mu = np.asarray(chempots, dtype=np.float64).ravel()
+        self.B = B = len(self.mu)
+        self.method = method.lower()
+        assert self.method in ('static', 'hybrid', 'anderson', 'hybridanderson'), method
+        self.nsteps = int(nsteps)
+        crit = criterion if isinstance(criterion, (list, tuple)) else [criterion]
+        thr = threshold if isinstance(threshold, (list, tuple)) else [threshold] * len(crit)
+        self.criteria = [c.lower() for c in crit]
+        for c in self.criteria:
+            if c not in ('res', 'riue'):
+                raise NotImplementedError("criterion %r" % c)
+        self.thresholds = [float(t) for t in thr]
+        self.alpha_mix = float(alpha_mix)
+        self.thresh = 1 * kjmol
+        self.m = int(m)
+        self.damping0 = float(damping)
+        self.damping_max, self.damping_min = damping_max, damping_min
+        self.adaptive = adaptive_damping
+        self.dfac = damping_factors
+        self.delta = delta
+        beta = fn.beta
+        # fugacity = exp(beta mu) / beta / Lambda^3 (solver.py:92)
+        self.fug = np.exp(beta * self.mu) / beta / fn.wavelength ** 3
+        n1, n2, n3 = self.plan.npoints
+        self.npts = n1 * n2 * n3
+        self.dr = self.plan.dr
+        dev = 'cuda'
+        f64 = torch.float64
+        self.nring = max(self.m, 2) if 'anderson' in self.method else 2
+        self.ring = torch.zeros((self.nring, B, n1, n2, n3), dtype=f64, device=dev)
+        self.rres = torch.zeros((self.nring, B, n1, n2, n3), dtype=f64, device=dev)
+        self.trial = torch.empty((B, n1, n2, n3), dtype=f64, device=dev)
+        self.rho0 = torch.empty((B, n1, n2, n3), dtype=f64, device=dev)
+        self.rhohat = self.plan.new_spec(B)
+        self.that = self.plan.new_spec(B)
+        self.chat = self.plan.new_spec(B)
+        self.chat2 = self.plan.new_spec(B)
+        self.buf = E.Buffers(self.plan, B)
+        self.buf.part[:, L.STAT_N3MAX, :] = -np.inf
+        self.params = torch.zeros((B, 4), dtype=f64, device=dev)
+        self.coef = torch.zeros((B, L.MAX_FIELDS), dtype=f64, device=dev)
+        self.active = torch.zeros(B, dtype=torch.int32, device=dev)
+        self.mask_host = np.zeros(B, dtype=bool)
+        self.kernel_launches = 0
+        self.omega_evals = 0
+
+    # ------------------------------------------------------------ helpers --
+    def _set_active(self, mask):
+        self.mask_host = np.asarray(mask, dtype=bool).copy()
+        self.active.copy_(torch.as_tensor(self.mask_host.astype(np.int32)), non_blocking=False)
+
+    def _stats(self, mask_bits=(1 << L.NSTAT) - 1):
+        E.finalize(self.buf, mask_bits, self.active)
+        self.kernel_launches += 1
+        return self.buf.stats.cpu().numpy()
+
+    def _mix(self, coefs, fields, clip, ref, out, thr=0.0):
+        """out = sum_j coefs[:, j] * fields[j] (fields: [B, ...] tensors); spectrum into self.that."""
+        c = np.zeros((self.B, L.MAX_FIELDS))
+        c[:, :len(fields)] = coefs
+        self.coef.copy_(torch.as_tensor(c))
+        E.mix_step(self.fn, self.buf, self.coef, fields, [self.npts] * len(fields), clip, ref, out, self.that,
+                   thr=thr, active=self.active)
+        self.kernel_launches += 1
+
+    def _c1(self, spec, chat, want):
+        self.fn.c1(self.buf, spec, chat, want=want, active=self.active)
+        self.kernel_launches += 3 if (want & 1) else 2
+
+    def _residual(self, chat, rho, r_out, hist):
+        self.params[:, 0] = torch.as_tensor(self.fug)
+        E.residual_step(self.fn, self.buf, self.params, chat, rho, r_out, hist=hist, hstride=self.npts,
+                        active=self.active)
+        self.kernel_launches += 1
+
+    def _omega(self, st, b):
+        """Grand potential from the per-instance sums (solver.py:103-119)."""
+        beta, dr = self.fn.beta, self.dr
+        N = st[L.STAT_N] * dr
+        Fid = (st[L.STAT_FID] * dr) / beta
+        G = Fid - self.mu[b] * N
+        G += (st[L.STAT_PHI] * dr) / beta
+        G += 0.5 * (st[L.STAT_MFA] * dr)
+        G += st[L.STAT_FEXT] * dr
+        return G
+
+    def _omega_parts(self, st):
+        beta, dr = self.fn.beta, self.dr
+        return dict(N=st[L.STAT_N] * dr, Fid=(st[L.STAT_FID] * dr) / beta,
+                    HardSphere=(st[L.STAT_PHI] * dr) / beta, MFA=0.5 * (st[L.STAT_MFA] * dr),
+                    ExtPot=st[L.STAT_FEXT] * dr)
+
+    def _eval_density(self, mask, coefs, fields, clip, out, want, ref):
+        """Mix a density into `out`, forward it, run the functional pipeline
+        (want bits: 1 C1 spectrum into chat2, 2 free-energy sums, 4 max n3)."""
+        self._set_active(mask)
+        self._mix(coefs, fields, clip, ref, out)
+        self._c1(self.that, self.chat2 if (want & 1) else None, want)
+        return self._stats()
+
+    # ------------------------------------------------------------- solve ---
+    def initial_density(self, rho0):
+        self.rho0.copy_(rho0)
+
+    def solve(self, rho0, cf=None):
+        """Run all instances from rho0 [B, N1, N2, N3]; returns (N, rho, converged)."""
+        self.initial_density(rho0)
+        B = self.B
+        self.cf = np.ones(B) if cf is None else np.asarray(cf, dtype=float).copy()
+        self.result = torch.empty_like(self.rho0)
+        self.N_out = np.full(B, np.nan)
+        self.conv = np.zeros(B, dtype=bool)
+        self.steps = np.zeros(B, dtype=int)
+        self.failed = np.zeros(B, dtype=bool)
+        self.history = [[] for _ in range(B)]
+        todo = np.ones(B, dtype=bool)
+        while todo.any():
+            retry = self._solve_once(todo)
+            # non-finite -> halve the correction factor and restart (solver.py:335-345)
+            for b in np.where(retry)[0]:
+                self.cf[b] /= 2
+                if self.cf[b] < 0.25:
+                    self.failed[b] = True
+                    retry[b] = False
+            todo = retry
+        if self.failed.any():
+            raise NoSolutionError("instances %s hit non-finite densities on every retry"
+                                  % list(np.where(self.failed)[0]))
+        return self.N_out, self.result, self.conv
+
+    def _init_state(self, todo):
+        """rho0 -> ring slot 0, its spectrum, C1, Omega and (for Anderson) r_0."""
+        st = self._eval_density(todo, np.ones((self.B, 1)), [self.rho0], L.CLIP_NONE, self.ring[0],
+                                1 | 2 | 4, self.rho0)
+        self.rhohat.copy_(self.that)
+        self.chat.copy_(self.chat2)
+        self.omega0 = np.array([self._omega(st[b], b) for b in range(self.B)])
+        self.n3max = st[:, L.STAT_N3MAX].copy()
+        self.Ncur = st[:, L.STAT_N] * self.dr
+        return st
+
+    def _solve_once(self, todo):
+        method = self.method
+        self._init_state(todo)
+        live = todo.copy()
+        retry = np.zeros(self.B, dtype=bool)
+        if method == 'static':
+            return self._loop_static(live, retry)
+        return self._loop_general(live, retry)
+
+    # ---------------------------------------------------- static Picard ---
+    def _loop_static(self, live, retry):
+        B = self.B
+        cur = np.zeros(B, dtype=int)  # ring slot of the current density
+        thr = 1e-10 / angstrom ** 3
+        prev = None  # stats of the previous launch
+        step = 0
+        self._set_active(live)
+        pending = np.zeros(B, dtype=bool)  # instances whose step `step` awaits its RES check
+        while live.any():
+            step += 1
+            a = self.alpha_mix * self.cf
+            self.params[:, 0] = torch.as_tensor(self.fug)
+            self.params[:, 1] = torch.as_tensor(a)
+            # slot choice: ring slot (cur+1)%2 per instance -> launch per parity group
+            for par in (0, 1):
+                grp = live & (cur == par)
+                if not grp.any():
+                    continue
+                self._set_active(grp)
+                E.picard_static_step(self.fn, self.buf, self.params, thr, self.chat, self.ring[par],
+                                     self.ring[1 - par], self.rhohat, active=self.active)
+                self.kernel_launches += 1
+            self._set_active(live)
+            st = self._stats()
+            # RES of the density produced by the previous step
+            for b in np.where(live)[0]:
+                if step > 1:
+                    N = prev[b, L.STAT_N] * self.dr
+                    res = np.sqrt(st[b, L.STAT_RES2]) / np.sqrt(N) / np.sqrt(self.npts)
+                    iue = prev[b, L.STAT_IUE] * self.dr
+                    if self._converged(b, N, res, iue):
+                        self._finish(b, self.ring[cur[b], b], N, step - 1, True)
+                        live[b] = False
+                        continue
+                    if step - 1 >= self.nsteps:
+                        self._finish(b, self.ring[cur[b], b], N, step - 1, False)
+                        live[b] = False
+                        continue
+                if st[b, L.STAT_NONFIN] > 0:
+                    retry[b] = True
+                    live[b] = False
+                    continue
+                cur[b] = 1 - cur[b]
+            if not live.any():
+                break
+            self._set_active(live)
+            self._c1(self.rhohat, self.chat, 1)
+            prev = st
+        return retry
+
+    def _converged(self, b, N, res, iue):
+        ok = True
+        riue = iue / N if N > 0 else np.nan
+        for c, t in zip(self.criteria, self.thresholds):
+            v = res if c == 'res' else riue
+            ok = ok and (v < t)
+        self.history[b].append((N, res, riue))
+        if iue == 0 and np.isnan(riue):
+            ok = True
+        return bool(ok)
+
+    def _finish(self, b, rho_b, N, steps, conv):
+        self.result[b].copy_(rho_b)
+        self.N_out[b] = N
+        self.conv[b] = conv
+        self.steps[b] = steps
+
+    # -------------------------------------------- hybrid / Anderson loop ---
+    def _loop_general(self, live, retry):
+        B, m = self.B, self.nring
+        anderson = 'anderson' in self.method
+        pure = self.method == 'anderson'
+        # ring bookkeeping: density j and residual j live in slot j % m
+        self.gram = np.zeros((B, m, m))
+        self.rnorm2 = np.zeros((B, m))
+        self.And_true = np.zeros(B, dtype=bool)
+        self.it_eps0 = np.full(B, np.nan)
+        self.damping = np.full(B, self.damping0)
+        self.last_stats = np.zeros((B, L.NSTAT))
+        # r_0 for the initial density
+        self._set_active(live)
+        self._residual(self.chat, self.ring[0], self.rres[0], [])
+        st = self._stats()
+        self.rnorm2[:, 0] = st[:, L.STAT_RES2]
+        self.gnonfin = st[:, L.STAT_GNONFIN].copy()
+        k = 0
+        while live.any():
+            k += 1  # curr_step
+            s_prev = (k - 1) % m
+            s_new = k % m
+            # --- Anderson.update_rho bookkeeping (solver.py:546-561)
+            res_norm = np.sqrt(self.rnorm2[:, s_prev])
+            it_eps = res_norm / self.Ncur
+            if k < 3:
+                self.it_eps0 = np.where(live, it_eps, self.it_eps0)
+            if anderson:
+                cond = pure | ((it_eps <= self.it_eps0 * self.delta) & (k > 4)) | self.And_true
+            else:
+                cond = np.zeros(B, dtype=bool)
+            cond &= live
+            hyb = live & ~cond
+            prev_omega = self.omega0.copy()
+            if cond.any():
+                ok = self._anderson_candidate(cond, k, s_prev, s_new)
+                self.And_true |= cond
+                hyb |= cond & ~ok
+            if hyb.any():
+                self._hybrid_step(hyb, k, s_prev, s_new)
+            # --- after the update: non-finite check, N, convergence (solver.py:286-305)
+            for b in np.where(live)[0]:
+                self.steps[b] = k
+                st_b = self.last_stats[b]
+                if st_b[L.STAT_NONFIN] > 0:
+                    retry[b] = True
+                    live[b] = False
+                    continue
+                N = st_b[L.STAT_N] * self.dr
+                res = np.sqrt(self.rnorm2[b, s_new]) / np.sqrt(N) / np.sqrt(self.npts)
+                iue = st_b[L.STAT_IUE] * self.dr
+                self.Ncur[b] = N
+                if self._converged(b, N, res, iue):
+                    self._finish(b, self.ring[s_new, b], N, k, True)
+                    live[b] = False
+                elif k >= self.nsteps:
+                    self._finish(b, self.ring[s_new, b], N, k, False)
+                    live[b] = False
+        return retry
+
+    def _valid_hist(self, k_new, s_new):
+        """Slots of residuals r_{k_new-m+1} .. r_{k_new-1} (excluding s_new)."""
+        m = self.nring
+        return [j % m for j in range(max(0, k_new - m + 1), k_new)]
+
+    def _post_update(self, mask, k, s_new, st_mix):
+        """C1, Omega and residual of the density just written to ring slot s_new."""
+        self._c1(self.that, self.chat2, 1 | 2 | 4)
+        hist_slots = self._valid_hist(k, s_new)
+        self._residual(self.chat2, self.ring[s_new], self.rres[s_new], [self.rres[j] for j in hist_slots])
+        st = self._stats()
+        for b in np.where(mask)[0]:
+            self.rhohat[b].copy_(self.that[b])
+            self.chat[b].copy_(self.chat2[b])
+        return st, hist_slots
+
+    def _commit_residual(self, mask, st, k, s_new, hist_slots):
+        for b in np.where(mask)[0]:
+            self.rnorm2[b, s_new] = st[b, L.STAT_RES2]
+            self.gram[b, s_new, s_new] = st[b, L.STAT_RES2]
+            for h, j in enumerate(hist_slots):
+                g = st[b, L.STAT_GRAM0 + h]
+                self.gram[b, s_new, j] = g
+                self.gram[b, j, s_new] = g
+            self.n3max[b] = st[b, L.STAT_N3MAX]
+            self.last_stats[b] = st[b]
+
+    def _anderson_candidate(self, mask, k, s_prev, s_new):
+        """Anderson.update_rho_Anderson + the acceptance tests; returns accepted mask."""
+        B, m = self.B, self.nring
+        mk = min(k, self.m)
+        slots = [j % m for j in range(k - mk, k)]  # oldest .. newest
+        coefs = np.zeros((B, 2 * mk))
+        for b in np.where(mask)[0]:
+            al = simplex_qp(self.gram[b], slots)
+            if self.adaptive:  # _get_damping_coefficient (solver.py:537-544)
+                r = np.sqrt(self.rnorm2[b, s_prev])
+                p = np.sqrt(self.rnorm2[b, (k - 2) % m]) if k >= 2 else 0.0
+                if r < p:
+                    self.damping[b] = min(self.damping[b] * self.dfac[0], self.damping_max)
+                else:
+                    self.damping[b] = max(self.damping[b] * self.dfac[1], self.damping_min)
+            d = self.cf[b] * self.damping[b]
+            coefs[b, :mk] = al
+            coefs[b, mk:] = d * al
+        fields = [self.ring[j] for j in slots] + [self.rres[j] for j in slots]
+        self._set_active(mask)
+        self._mix(coefs, fields, L.CLIP_DENSITY, self.ring[s_prev], self.ring[s_new])
+        st, hist_slots = self._post_update(mask, k, s_new, None)
+        ok = np.zeros(B, dtype=bool)
+        for b in np.where(mask)[0]:
+            if st[b, L.STAT_GNONFIN] > 0:
+                continue
+            om = self._omega(st[b], b)
+            prev = self.omega0[b]
+            self.omega0[b] = om  # _get_Omega stores omega0 even when rejected
+            self.omega_evals += 1
+            if om > prev * 0.8:
+                continue
+            ok[b] = True
+        self._commit_residual(ok, st, k, s_new, hist_slots)
+        return ok
+
+    def _trial_omega(self, mask, alpha, s_prev):
+        """Omega((1-a) rho + a G) = Omega(rho + a r) for every instance in mask."""
+        coefs = np.zeros((self.B, 2))
+        coefs[:, 0] = 1.0
+        coefs[:, 1] = alpha
+        st = self._eval_density(mask, coefs, [self.ring[s_prev], self.rres[s_prev]], L.CLIP_NONE,
+                                self.trial, 2, self.ring[s_prev])
+        self.omega_evals += int(mask.sum())
+        return np.array([self._omega(st[b], b) if mask[b] else np.nan for b in range(self.B)])
+
+    def _hybrid_step(self, mask, k, s_prev, s_new):
+        """Picard.update_rho_hybrid for the instances in mask (solver.py:403-457)."""
+        B = self.B
+        prev = self.omega0.copy()
+        # alpha_max from max n3 of rho and of G = rho + r (solver.py:150-165)
+        coefs = np.ones((B, 2))
+        stn = self._eval_density(mask, coefs, [self.ring[s_prev], self.rres[s_prev]], L.CLIP_NONE,
+                                 self.trial, 4, self.ring[s_prev])
+        amax = np.zeros(B)
+        for b in np.where(mask)[0]:
+            a, g = self.n3max_of_current(b), stn[b, L.STAT_N3MAX]
+            amax[b] = np.min([abs((1 - a) / ((g - a) + 1e-16)), 1])
+        aopt = np.zeros(B)
+        mn = np.zeros(B)
+        mx = np.zeros(B)
+        need = mask & ~np.isclose(amax, 0)
+        if need.any():
+            a1 = 0.45 * amax
+            o1 = self._trial_omega(need, a1, s_prev)
+            a2 = np.where(o1 <= prev, 0.9 * amax, 0.225 * amax)
+            o2 = self._trial_omega(need, a2, s_prev)
+            for b in np.where(need)[0]:
+                c, bb, a = np.polyfit([0, a1[b], a2[b]], [prev[b], o1[b], o2[b]], 2)
+                hi = max(a1[b], a2[b])
+                al = np.linspace(-hi / 4, hi, 10000)
+                om = a + bb * al + c * al ** 2
+                aopt[b] = al[np.where(om == np.min(om))[0][0]]
+                mn[b] = np.min(om) / kjmol
+                mx[b] = np.max(om) / kjmol
+            self.omega0 = np.where(need, o2, self.omega0)
+        for b in np.where(mask)[0]:
+            if aopt[b] <= 0:
+                if mx[b] - mn[b] > self.thresh:
+                    one = np.zeros(B, dtype=bool)
+                    one[b] = True
+
+                    def fun(alpha, b=b, one=one):
+                        al = np.zeros(B)
+                        al[b] = float(np.asarray(alpha).ravel()[0])
+                        o = self._trial_omega(one, al, s_prev)[b]
+                        self.omega0[b] = o
+                        return o
+                    bnd = opt.Bounds(0.01 * amax[b], 0.9 * amax[b])
+                    aopt[b] = float(opt.minimize(fun, [self.alpha_mix * amax[b]], bounds=bnd, method='SLSQP',
+                                                 options={'ftol': 1e-8}).x[0])
+                else:
+                    aopt[b] = self.alpha_mix * amax[b]
+            if aopt[b] <= 0 or np.isclose(aopt[b], 0):
+                aopt[b] = self.alpha_mix * amax[b]
+        coefs = np.zeros((B, 2))
+        coefs[:, 0] = 1.0
+        coefs[:, 1] = aopt * self.cf
+        self._set_active(mask)
+        self._mix(coefs, [self.ring[s_prev], self.rres[s_prev]], L.CLIP_DENSITY, self.ring[s_prev],
+                  self.ring[s_new])
+        st, hist_slots = self._post_update(mask, k, s_new, None)
+        for b in np.where(mask)[0]:
+            self.omega0[b] = self._omega(st[b], b)
+            self.omega_evals += 1
+        self._commit_residual(mask, st, k, s_new, hist_slots)
+
+    def n3max_of_current(self, b):
+        return self.n3max[b]

@@ -1,0 +1,58 @@
+// Shared definitions for the cmmdft_b200 CUDA sources.
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stddef.h>
+
+#include "fft_core.cuh"
+#include "../../include/cmmdft_b200.h"
+
+#define CMM_MAX_N 1024        // longest axis a grid plan accepts
+#define CMM_MAX_FIELDS 12     // fields a mix launch combines
+#define CMM_PLANE_THREADS 512
+#define CMM_COL_THREADS 256
+
+// Per-instance reduction slots (see cmm_stat_* in the public header).
+#define NQ CMM_NSTAT
+
+// Device-side description of one grid plan.  Every table is indexed by the
+// POSITION at which a frequency is stored (digit-reversed layout), so the
+// k-space stages never permute data.
+struct GridDev {
+  int n1, n2, n3, h3, m3;      // h3 = n3/2+1 stored z frequencies, m3 = n3/2
+  FftAxis ax1, ax2, ax3;       // ax3 is the half-length complex z transform (length m3)
+  const double2* tw1;          // w_{n1}^t, t < n1
+  const double2* tw2;          // w_{n2}^t
+  const double2* tw3;          // w_{n3}^t (the z transform and the R2C twist)
+  const int* zpos;             // z position of frequency k < m3
+  const int* k1pos;            // x frequency at DIF position p (column passes)
+  const double* kp1;           // signed k component (bohr^-1) at x position
+  const double* kp2;
+  const double* kp3;           // at z position p3 <= m3
+  const double* sl1;           // Lanczos sinc factor at x position
+  const double* sl2;
+  const double* sl3;
+  const int* nq1;              // 1 where the x position holds the Nyquist frequency of an even axis
+  const int* nq2;
+  const int* nq3;
+  const double* wt3;           // Parseval weight at z position (1 for k3 = 0 and k3 = n3/2, else 2)
+};
+
+struct cmm_grid {
+  int n1, n2, n3, h3, m3;
+  double rvecs[9];
+  double spacing[3];
+  double volume;
+  FftAxis ax1, ax2, ax3;
+  // host copies of the position tables
+  int* hpos_k1;                // k index at x position (DIF output order)
+  int* hpos_k2;
+  int* hpos_k3;                // k index at z position (p < m3 -> DIF; p == m3 -> m3)
+  // one device allocation holding every table
+  void* dmem;
+  GridDev dev;
+};
+
+static inline int cmm_div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
+
+__device__ __forceinline__ bool cmm_isfinite(double x) { return isfinite(x); }

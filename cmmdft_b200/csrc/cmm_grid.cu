@@ -1,0 +1,227 @@
+// Grid plans: radix factorisation, twiddle tables, digit-reversal position
+// tables and per-position k-space tables.
+//
+// Reference: the k-grid, scalprod and Lanczos tables of Grid.__init__
+// (cmmdft/system.py:232-295).  The k component of axis a at signed
+// frequency m is computed the way numpy does it there:
+//   k = (2 pi) * (m * (1 / (N * d)))   with d = |rvecs[:, a]| / N  (column norm)
+// and the Lanczos factor per axis is np.sinc(k / kcut), kcut = 2 pi / d.
+#include <cmath>
+#include <cstdlib>
+#include <cstring>
+#include <vector>
+
+#include "cmm_common.cuh"
+
+static const char* kStatusText[] = {
+    "ok", "bad argument", "unsupported grid shape", "CUDA runtime error",
+    "plane or tile does not fit in shared memory", "out of memory",
+    "workspace too small", "unsupported option"};
+
+extern "C" int cmm_version(void) { return 100; }
+
+extern "C" const char* cmm_status_string(int s) {
+  if (s < 0 || s > 7) return "unknown status";
+  return kStatusText[s];
+}
+
+// Radices for length n: 8s first, then 4, 2, then odd primes (<= 16).
+static bool factorise(int n, FftAxis* ax) {
+  ax->n = n;
+  ax->nstage = 0;
+  int m = n;
+  std::vector<int> r;
+  while (m % 8 == 0) { r.push_back(8); m /= 8; }
+  while (m % 4 == 0) { r.push_back(4); m /= 4; }
+  while (m % 2 == 0) { r.push_back(2); m /= 2; }
+  for (int p = 3; p <= 13 && m > 1; p += 2)
+    while (m % p == 0) { r.push_back(p); m /= p; }
+  if (m != 1) return false;  // prime factor > 13 (needs Bluestein; not in this build)
+  if ((int)r.size() > CMM_MAX_STAGES) return false;
+  if (r.empty()) r.push_back(1);
+  int L = n;
+  for (size_t s = 0; s < r.size(); ++s) {
+    ax->radix[s] = r[s];
+    ax->span[s] = L;
+    L /= r[s];
+  }
+  ax->nstage = (int)r.size();
+  if (n == 1) ax->nstage = 0;
+  return true;
+}
+
+// Frequency index stored at each DIF output position: position
+// p = q0*s0 + q1*s1 + ... holds k = q0 + R0*(q1 + R1*(q2 + ...)).
+static void dif_positions(const FftAxis& ax, int* k_of_pos) {
+  const int n = ax.n;
+  for (int p = 0; p < n; ++p) {
+    int rem = p, k = 0, mul = 1;
+    for (int s = 0; s < ax.nstage; ++s) {
+      int stride = ax.span[s] / ax.radix[s];
+      int q = rem / stride;
+      rem -= q * stride;
+      k += q * mul;
+      mul *= ax.radix[s];
+    }
+    k_of_pos[p] = (ax.nstage == 0) ? 0 : k;
+  }
+}
+
+static void twiddles(int n, std::vector<double>& out) {
+  out.resize(2 * (size_t)n);
+  for (int t = 0; t < n; ++t) {
+    long double a = -2.0L * 3.141592653589793238462643383279502884L * (long double)t / (long double)n;
+    out[2 * t] = (double)cosl(a);
+    out[2 * t + 1] = (double)sinl(a);
+  }
+}
+
+static int signed_freq(int k, int n) {
+  // numpy.fft.fftfreq ordering: [0, 1, ..., (n-1)/2, -(n/2), ..., -1]
+  int half = (n - 1) / 2 + 1;  // number of non-negative entries
+  return (k < half) ? k : k - n;
+}
+
+static double np_sinc(double x) {
+  // numpy.sinc: y = pi * (x == 0 ? 1e-20 : x); sin(y) / y
+  volatile double y = M_PI * (x == 0.0 ? 1.0e-20 : x);
+  return sin(y) / y;
+}
+
+extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_grid** out) {
+  if (!out || !rvecs || n1 < 1 || n2 < 1 || n3 < 2) return CMM_ERR_ARG;
+  if (n1 > CMM_MAX_N || n2 > CMM_MAX_N || n3 > CMM_MAX_N) return CMM_ERR_SHAPE;
+  if (n3 % 2) return CMM_ERR_SHAPE;  // the z axis is transformed as a half-length complex FFT
+  cmm_grid* g = (cmm_grid*)calloc(1, sizeof(cmm_grid));
+  if (!g) return CMM_ERR_NOMEM;
+  g->n1 = n1; g->n2 = n2; g->n3 = n3; g->m3 = n3 / 2; g->h3 = n3 / 2 + 1;
+  memcpy(g->rvecs, rvecs, 9 * sizeof(double));
+  int N[3] = {n1, n2, n3};
+  for (int a = 0; a < 3; ++a) {
+    double c0 = rvecs[0 * 3 + a], c1 = rvecs[1 * 3 + a], c2 = rvecs[2 * 3 + a];
+    g->spacing[a] = sqrt(c0 * c0 + c1 * c1 + c2 * c2) / N[a];  // column norms (system.py:262-266)
+  }
+  {
+    const double* r = rvecs;
+    double det = r[0] * (r[4] * r[8] - r[5] * r[7]) - r[1] * (r[3] * r[8] - r[5] * r[6]) +
+                 r[2] * (r[3] * r[7] - r[4] * r[6]);
+    g->volume = fabs(det);
+  }
+  if (!factorise(n1, &g->ax1) || !factorise(n2, &g->ax2) || !factorise(g->m3, &g->ax3)) {
+    free(g);
+    return CMM_ERR_SHAPE;
+  }
+  const int m3 = g->m3, h3 = g->h3;
+  g->hpos_k1 = (int*)malloc(sizeof(int) * n1);
+  g->hpos_k2 = (int*)malloc(sizeof(int) * n2);
+  g->hpos_k3 = (int*)malloc(sizeof(int) * h3);
+  std::vector<int> zdif(m3), zpos(m3);
+  dif_positions(g->ax1, g->hpos_k1);
+  dif_positions(g->ax2, g->hpos_k2);
+  dif_positions(g->ax3, zdif.data());
+  for (int p = 0; p < m3; ++p) { g->hpos_k3[p] = zdif[p]; zpos[zdif[p]] = p; }
+  g->hpos_k3[m3] = m3;
+
+  std::vector<double> tw1, tw2, tw3;
+  twiddles(n1, tw1); twiddles(n2, tw2); twiddles(n3, tw3);
+
+  // per-position k tables
+  std::vector<double> kp[3], sl[3], wt3(h3);
+  std::vector<int> nq[3];
+  const int* kof[3] = {g->hpos_k1, g->hpos_k2, g->hpos_k3};
+  int npos[3] = {n1, n2, h3};
+  for (int a = 0; a < 3; ++a) {
+    kp[a].resize(npos[a]); sl[a].resize(npos[a]); nq[a].resize(npos[a]);
+    const double d = g->spacing[a];
+    const double val = 1.0 / (N[a] * d);
+    const double twopi = 2.0 * M_PI;
+    const double kcut = 2.0 * M_PI / d;
+    for (int p = 0; p < npos[a]; ++p) {
+      int k = kof[a][p];
+      int m = signed_freq(k, N[a]);
+      volatile double f = (double)m * val;
+      volatile double kk = twopi * f;
+      kp[a][p] = kk;
+      sl[a][p] = np_sinc(kk / kcut);
+      nq[a][p] = (N[a] % 2 == 0 && k == N[a] / 2) ? 1 : 0;
+    }
+  }
+  for (int p = 0; p < h3; ++p) {
+    int k = g->hpos_k3[p];
+    wt3[p] = (k == 0 || k == m3) ? 1.0 : 2.0;
+  }
+
+  // one device block for everything
+  size_t off = 0;
+  auto bump = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~(size_t)255; return o; };
+  size_t o_tw1 = bump(sizeof(double) * tw1.size()), o_tw2 = bump(sizeof(double) * tw2.size()),
+         o_tw3 = bump(sizeof(double) * tw3.size()), o_zpos = bump(sizeof(int) * m3),
+         o_k1 = bump(sizeof(int) * n1);
+  size_t o_kp[3], o_sl[3], o_nq[3];
+  for (int a = 0; a < 3; ++a) {
+    o_kp[a] = bump(sizeof(double) * npos[a]);
+    o_sl[a] = bump(sizeof(double) * npos[a]);
+    o_nq[a] = bump(sizeof(int) * npos[a]);
+  }
+  size_t o_wt3 = bump(sizeof(double) * h3);
+  std::vector<char> host(off);
+  memcpy(&host[o_tw1], tw1.data(), sizeof(double) * tw1.size());
+  memcpy(&host[o_tw2], tw2.data(), sizeof(double) * tw2.size());
+  memcpy(&host[o_tw3], tw3.data(), sizeof(double) * tw3.size());
+  memcpy(&host[o_zpos], zpos.data(), sizeof(int) * m3);
+  memcpy(&host[o_k1], g->hpos_k1, sizeof(int) * n1);
+  for (int a = 0; a < 3; ++a) {
+    memcpy(&host[o_kp[a]], kp[a].data(), sizeof(double) * npos[a]);
+    memcpy(&host[o_sl[a]], sl[a].data(), sizeof(double) * npos[a]);
+    memcpy(&host[o_nq[a]], nq[a].data(), sizeof(int) * npos[a]);
+  }
+  memcpy(&host[o_wt3], wt3.data(), sizeof(double) * h3);
+  if (cudaMalloc(&g->dmem, off) != cudaSuccess) {
+    free(g->hpos_k1); free(g->hpos_k2); free(g->hpos_k3); free(g);
+    return CMM_ERR_NOMEM;
+  }
+  if (cudaMemcpy(g->dmem, host.data(), off, cudaMemcpyHostToDevice) != cudaSuccess) {
+    cudaFree(g->dmem);
+    free(g->hpos_k1); free(g->hpos_k2); free(g->hpos_k3); free(g);
+    return CMM_ERR_CUDA;
+  }
+  char* b = (char*)g->dmem;
+  GridDev& d = g->dev;
+  d.n1 = n1; d.n2 = n2; d.n3 = n3; d.h3 = h3; d.m3 = m3;
+  d.ax1 = g->ax1; d.ax2 = g->ax2; d.ax3 = g->ax3;
+  d.tw1 = (const double2*)(b + o_tw1);
+  d.tw2 = (const double2*)(b + o_tw2);
+  d.tw3 = (const double2*)(b + o_tw3);
+  d.zpos = (const int*)(b + o_zpos);
+  d.k1pos = (const int*)(b + o_k1);
+  d.kp1 = (const double*)(b + o_kp[0]); d.kp2 = (const double*)(b + o_kp[1]); d.kp3 = (const double*)(b + o_kp[2]);
+  d.sl1 = (const double*)(b + o_sl[0]); d.sl2 = (const double*)(b + o_sl[1]); d.sl3 = (const double*)(b + o_sl[2]);
+  d.nq1 = (const int*)(b + o_nq[0]); d.nq2 = (const int*)(b + o_nq[1]); d.nq3 = (const int*)(b + o_nq[2]);
+  d.wt3 = (const double*)(b + o_wt3);
+  *out = g;
+  return CMM_OK;
+}
+
+extern "C" int cmm_grid_destroy(cmm_grid* g) {
+  if (!g) return CMM_OK;
+  if (g->dmem) cudaFree(g->dmem);
+  free(g->hpos_k1); free(g->hpos_k2); free(g->hpos_k3);
+  free(g);
+  return CMM_OK;
+}
+
+extern "C" int cmm_grid_spectrum_size(const cmm_grid* g, long long* nspec, int* h3) {
+  if (!g) return CMM_ERR_ARG;
+  if (nspec) *nspec = (long long)g->n1 * g->n2 * g->h3;
+  if (h3) *h3 = g->h3;
+  return CMM_OK;
+}
+
+extern "C" int cmm_spectrum_index(const cmm_grid* g, int* k1, int* k2, int* k3) {
+  if (!g || !k1 || !k2 || !k3) return CMM_ERR_ARG;
+  // spectra in HBM keep x natural (the column passes undo their own x order)
+  for (int i = 0; i < g->n1; ++i) k1[i] = i;
+  memcpy(k2, g->hpos_k2, sizeof(int) * g->n2);
+  memcpy(k3, g->hpos_k3, sizeof(int) * g->h3);
+  return CMM_OK;
+}

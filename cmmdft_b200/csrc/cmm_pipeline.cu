@@ -1,0 +1,852 @@
+// Fused FP64 grid-solve kernels for sm_100a.
+//
+// Per fixed-point iteration the solve runs four passes over HBM:
+//   plane  (one CTA per x-plane): inverse y/z of the C1 spectrum, the update
+//          (Picard / residual / mix), forward z (R2C) + y of the new density
+//   column (one CTA per tile of (y,z) columns): forward x, the analytic FMT
+//          weights, inverse x of the 5 weighted-density spectra
+//   plane  : inverse y/z of 5 fields, White-Bear dPhi/dn, forward z/y of 5
+//   column : forward x of 5 dPhi spectra and rho_hat, back-convolution with the
+//          weights plus the MFA kernel, inverse x of the C1 spectrum
+// All transforms are in place in shared memory (fft_core.cuh).
+#include <cmath>
+#include <cstdio>
+
+#include "cmm_common.cuh"
+
+// --------------------------------------------------------- shared tables --
+struct PlaneSmem {
+  double2* slots;   // nslot * n2 * h3
+  double2* tw2;     // n2
+  double2* tw3;     // n3
+  int* zpos;        // m3
+};
+
+__host__ __device__ inline size_t plane_smem_bytes(int n2, int n3, int nslot) {
+  int h3 = n3 / 2 + 1, m3 = n3 / 2;
+  size_t b = sizeof(double2) * ((size_t)nslot * n2 * h3 + n2 + n3);
+  b += sizeof(int) * m3;
+  return (b + 15) & ~(size_t)15;
+}
+
+__device__ inline PlaneSmem plane_smem_setup(const GridDev& g, int nslot) {
+  extern __shared__ double2 smem_d2[];
+  PlaneSmem s;
+  s.slots = smem_d2;
+  s.tw2 = s.slots + (size_t)nslot * g.n2 * g.h3;
+  s.tw3 = s.tw2 + g.n2;
+  s.zpos = (int*)(s.tw3 + g.n3);
+  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) s.tw2[i] = g.tw2[i];
+  for (int i = threadIdx.x; i < g.n3; i += blockDim.x) s.tw3[i] = g.tw3[i];
+  for (int i = threadIdx.x; i < g.m3; i += blockDim.x) s.zpos[i] = g.zpos[i];
+  return s;
+}
+
+// ------------------------------------------------ plane transforms ------
+// Forward: real rows (natural z) in each slot -> DIF z, R2C twist, DIF y.
+__device__ void plane_forward(const GridDev& g, const PlaneSmem& s, int nslot) {
+  const int n2 = g.n2, h3 = g.h3, m3 = g.m3;
+  PencilSet rows = {nslot * n2, nslot * n2, 0, h3, 1, false};
+  fft_pencils<false>(s.slots, g.ax3, s.tw3, 2, rows);
+  // R2C twist on every row: pairs (k, m3-k), k = 0..m3/2
+  const int np = m3 / 2 + 1;
+  const int total = nslot * n2 * np;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int row = t / np, k = t - row * np;
+    double2* rp = s.slots + (size_t)row * h3;
+    if (k == 0) {
+      double2 z0 = rp[0];
+      rp[0] = make_double2(z0.x + z0.y, 0.0);
+      rp[m3] = make_double2(z0.x - z0.y, 0.0);
+    } else {
+      const int pk = s.zpos[k], pm = s.zpos[m3 - k];
+      double2 zk = rp[pk], zm = rp[pm];
+      // E = (zk + conj zm)/2 ; O = -i (zk - conj zm)/2
+      double2 E = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
+      double2 O = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
+      double2 WO = cmul(s.tw3[k], O);
+      double2 xk = cadd(E, WO);
+      double2 xm = cconj(csub(E, WO));
+      rp[pk] = xk;
+      if (pm != pk) rp[pm] = xm;
+    }
+  }
+  __syncthreads();
+  PencilSet cols = {nslot * h3, h3, n2 * h3, 1, h3, true};
+  fft_pencils<false>(s.slots, g.ax2, s.tw2, 1, cols);
+}
+
+// Inverse: spectrum slots -> DIT y, C2R twist, DIT z -> real rows (unnormalised).
+__device__ void plane_inverse(const GridDev& g, const PlaneSmem& s, int nslot) {
+  const int n2 = g.n2, h3 = g.h3, m3 = g.m3;
+  PencilSet cols = {nslot * h3, h3, n2 * h3, 1, h3, true};
+  fft_pencils<true>(s.slots, g.ax2, s.tw2, 1, cols);
+  const int np = m3 / 2 + 1;
+  const int total = nslot * n2 * np;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int row = t / np, k = t - row * np;
+    double2* rp = s.slots + (size_t)row * h3;
+    if (k == 0) {
+      // real parts of the DC and Nyquist bins (Grid.ifft keeps .real)
+      double x0 = rp[0].x, xm = rp[m3].x;
+      rp[0] = make_double2(x0 + xm, x0 - xm);
+    } else {
+      const int pk = s.zpos[k], pm = s.zpos[m3 - k];
+      double2 xk = rp[pk], xm = rp[pm];
+      double2 e = make_double2(xk.x + xm.x, xk.y - xm.y);           // xk + conj(xm)
+      double2 o = cmulc(make_double2(xk.x - xm.x, xk.y + xm.y), s.tw3[k]);  // (xk - conj xm) conj(W^k)
+      // Zin[k] = e + i o ; Zin[m3-k] = conj(e) + i conj(o)
+      rp[pk] = make_double2(e.x - o.y, e.y + o.x);
+      if (pm != pk) rp[pm] = make_double2(e.x + o.y, -e.y + o.x);
+    }
+  }
+  __syncthreads();
+  PencilSet rows = {nslot * n2, nslot * n2, 0, h3, 1, false};
+  fft_pencils<true>(s.slots, g.ax3, s.tw3, 2, rows);
+}
+
+// Real element (y=r, z=j) of slot f, in the row layout of a transformed plane.
+__device__ __forceinline__ double& rel(const PlaneSmem& s, const GridDev& g, int f, int r, int j) {
+  return ((double*)(s.slots + ((size_t)f * g.n2 + r) * g.h3))[j];
+}
+
+// Copy nslot spectrum planes from global (field stride fs, in double2) into smem.
+__device__ inline void load_spec_planes(const GridDev& g, const PlaneSmem& s, int nslot,
+                                        const double2* src, size_t plane_off, size_t fs) {
+  const int cnt = g.n2 * g.h3;
+  for (int f = 0; f < nslot; ++f) {
+    const double2* p = src + f * fs + plane_off;
+    double2* d = s.slots + (size_t)f * cnt;
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) d[i] = __ldg(p + i);
+  }
+}
+
+__device__ inline void store_spec_planes(const GridDev& g, const PlaneSmem& s, int nslot,
+                                         double2* dst, size_t plane_off, size_t fs) {
+  const int cnt = g.n2 * g.h3;
+  for (int f = 0; f < nslot; ++f) {
+    double2* p = dst + f * fs + plane_off;
+    const double2* d = s.slots + (size_t)f * cnt;
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) p[i] = d[i];
+  }
+}
+
+// ---------------------------------------------------- block reductions --
+__device__ inline double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = 0.0;
+  if (threadIdx.x < 32) {
+    r = (l < nw) ? red[l] : 0.0;
+    for (int o = 16; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  }
+  return r;  // valid in thread 0
+}
+
+__device__ inline double block_max(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_xor_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double r = -INFINITY;
+  if (threadIdx.x < 32) {
+    r = (l < nw) ? red[l] : -INFINITY;
+    for (int o = 16; o > 0; o >>= 1) r = fmax(r, __shfl_xor_sync(0xffffffffu, r, o));
+  }
+  return r;
+}
+
+__device__ inline void put_part(double* part, int b, int q, int nslot, int slot, double v) {
+  if (threadIdx.x == 0) part[((size_t)b * NQ + q) * nslot + slot] = v;
+}
+
+// ================================================ 3D FFT (setup / tests) ==
+__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+k_plane_r2c(GridDev g, const double* __restrict__ in, double2* __restrict__ out) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  PlaneSmem s = plane_smem_setup(g, 1);
+  const size_t roff = ((size_t)b * g.n1 + i1) * g.n2 * g.n3;
+  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
+    int r = i / g.n3, j = i - r * g.n3;
+    rel(s, g, 0, r, j) = __ldg(in + roff + i);
+  }
+  __syncthreads();
+  plane_forward(g, s, 1);
+  store_spec_planes(g, s, 1, out, ((size_t)b * g.n1 + i1) * g.n2 * g.h3, 0);
+}
+
+__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+k_plane_c2r(GridDev g, const double2* __restrict__ in, double* __restrict__ out) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  PlaneSmem s = plane_smem_setup(g, 1);
+  load_spec_planes(g, s, 1, in, ((size_t)b * g.n1 + i1) * g.n2 * g.h3, 0);
+  __syncthreads();
+  plane_inverse(g, s, 1);
+  const size_t roff = ((size_t)b * g.n1 + i1) * g.n2 * g.n3;
+  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
+    int r = i / g.n3, j = i - r * g.n3;
+    out[roff + i] = rel(s, g, 0, r, j);
+  }
+}
+
+// Column tile geometry: TC consecutive (y,z) columns of one instance.
+struct ColSmem {
+  double2* slots;   // nslot * n1 * tc
+  double2* tw1;     // n1
+};
+
+__host__ __device__ inline size_t col_smem_bytes(int n1, int tc, int nslot) {
+  return sizeof(double2) * ((size_t)nslot * n1 * tc + n1);
+}
+
+__device__ inline ColSmem col_smem_setup(const GridDev& g, int nslot, int tc) {
+  extern __shared__ double2 smem_d2[];
+  ColSmem s;
+  s.slots = smem_d2;
+  s.tw1 = s.slots + (size_t)nslot * g.n1 * tc;
+  for (int i = threadIdx.x; i < g.n1; i += blockDim.x) s.tw1[i] = g.tw1[i];
+  return s;
+}
+
+// Load a tile [n1][tc] of field f (instance b) into slot f; zero-fill past the end.
+__device__ inline void load_col_tile(const GridDev& g, const ColSmem& s, int slot, const double2* src,
+                                     int b, int c0, int tc) {
+  const int nc = g.n2 * g.h3;
+  const size_t base = (size_t)b * g.n1 * nc;
+  double2* d = s.slots + (size_t)slot * g.n1 * tc;
+  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
+    const int r = i / tc, c = i - r * tc;
+    const int col = c0 + c;
+    d[i] = (col < nc) ? __ldg(src + base + (size_t)r * nc + col) : make_double2(0.0, 0.0);
+  }
+}
+
+__device__ inline void store_col_tile(const GridDev& g, const ColSmem& s, int slot, double2* dst,
+                                      int b, int c0, int tc) {
+  const int nc = g.n2 * g.h3;
+  const size_t base = (size_t)b * g.n1 * nc;
+  const double2* d = s.slots + (size_t)slot * g.n1 * tc;
+  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
+    const int r = i / tc, c = i - r * tc;
+    const int col = c0 + c;
+    if (col < nc) dst[base + (size_t)r * nc + col] = d[i];
+  }
+}
+
+__device__ inline void col_fft(const GridDev& g, const ColSmem& s, int nslot, int tc, bool inv) {
+  PencilSet ps = {nslot * tc, nslot * tc, 0, 1, tc, true};
+  if (inv) fft_pencils<true>(s.slots, g.ax1, s.tw1, 1, ps);
+  else fft_pencils<false>(s.slots, g.ax1, s.tw1, 1, ps);
+}
+
+// Plain x transform of a tile (setup / tests).  Forward leaves x in DIF
+// order when `keep_dif`; the HBM layout keeps x natural, so the 3D FFT
+// entry points run forward then un-permute in the same kernel.
+__global__ void __launch_bounds__(CMM_COL_THREADS)
+k_col_fft(GridDev g, const double2* in, double2* out, int tc, int inv,
+          const int* __restrict__ k1_of_pos) {
+  const int b = blockIdx.y, c0 = blockIdx.x * tc;
+  ColSmem s = col_smem_setup(g, 1, tc);
+  // forward: load natural x, DIF, write natural (permute via k1_of_pos)
+  // inverse: load natural x, permute into DIF order, DIT, write natural
+  const int nc = g.n2 * g.h3;
+  const size_t base = (size_t)b * g.n1 * nc;
+  double2* d = s.slots;
+  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
+    const int p = i / tc, c = i - p * tc;
+    const int col = c0 + c;
+    const int r = inv ? k1_of_pos[p] : p;
+    d[i] = (col < nc) ? in[base + (size_t)r * nc + col] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  col_fft(g, s, 1, tc, inv != 0);
+  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
+    const int p = i / tc, c = i - p * tc;
+    const int col = c0 + c;
+    const int r = inv ? p : k1_of_pos[p];
+    if (col < nc) out[base + (size_t)r * nc + col] = d[i];
+  }
+}
+
+// ================================================ FMT weights ===========
+// Weights of HardSphereFunctional._init_weight_functions
+// (cmmdft/functionals.py:421-455) at one stored frequency.  Vector weights
+// are replaced by their Hermitian part: zero on their own axis' Nyquist plane
+// (what Grid.ifft's .real keeps of a purely imaginary self-conjugate bin).
+struct Weights {
+  double w0;      // kw0 = j0(kR) sigma_L
+  double w3;      // kw3 = (4 pi R^3 / 3) * 3 (sin x - x cos x) / x^3 * sigma_L
+  double v[3];    // kwv2 = -i * kw3 * k  -> stored as the real factor of -i
+};
+
+__device__ __forceinline__ Weights fmt_weights(double kx, double ky, double kz, double sl, double R,
+                                               int nqx, int nqy, int nqz) {
+  Weights w;
+  double kk = sqrt(kx * kx + ky * ky + kz * kz);
+  double om = kk * R;
+  if (fabs(om) <= 1e-8) {  // np.isclose(omega, 0)
+    w.w0 = sl;
+    w.w3 = (4.0 * M_PI * R * R * R / 3.0) * sl;
+    w.v[0] = w.v[1] = w.v[2] = 0.0;
+    return w;
+  }
+  double sn, cs;
+  sincos(om, &sn, &cs);
+  double y = M_PI * (om / M_PI);
+  double j0 = sin(y) / y;  // np.sinc(omega / pi)
+  double j2 = 3.0 * (sn - om * cs) / (om * om * om);
+  w.w0 = j0 * sl;
+  w.w3 = (4.0 * M_PI * R * R * R / 3.0) * (j2 * sl);
+  w.v[0] = nqx ? 0.0 : w.w3 * kx;
+  w.v[1] = nqy ? 0.0 : w.w3 * ky;
+  w.v[2] = nqz ? 0.0 : w.w3 * kz;
+  return w;
+}
+
+// ================================== column pass 1: rho_hat -> 5 fields ==
+// Outputs (field stride fsw): 0 = n0 (w0), 1 = n3 (w3), 2..4 = nv2 (x, y, z).
+__global__ void __launch_bounds__(CMM_COL_THREADS)
+k_col_weights(GridDev g, const int* __restrict__ active, double R, double inv_npts,
+              const double2* __restrict__ rhohat, double2* __restrict__ wout, size_t fsw,
+              const double2* __restrict__ kst, double* __restrict__ part, int nslot_part,
+              int want_value, int tc) {
+  const int b = blockIdx.y, tile = blockIdx.x, c0 = tile * tc;
+  if (active && !active[b]) return;
+  ColSmem s = col_smem_setup(g, 5, tc);
+  load_col_tile(g, s, 0, rhohat, b, c0, tc);
+  __syncthreads();
+  col_fft(g, s, 1, tc, false);
+  const int nc = g.n2 * g.h3;
+  double mfa = 0.0;
+  const size_t per = (size_t)g.n1 * tc;
+  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
+    const int p1 = i / tc, c = i - p1 * tc;
+    const int col = c0 + c;
+    if (col >= nc) continue;
+    const int p2 = col / g.h3, p3 = col - p2 * g.h3;
+    double2 F = s.slots[i];
+    const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];
+    Weights w = fmt_weights(g.kp1[p1], g.kp2[p2], g.kp3[p3], sl, R, g.nq1[p1], g.nq2[p2], g.nq3[p3]);
+    if (want_value) {
+      double2 K = __ldg(kst + (size_t)p1 * nc + col);
+      mfa += g.wt3[p3] * (F.x * F.x + F.y * F.y) * K.x;
+    }
+    F = cscale(F, inv_npts);
+    s.slots[1 * per + i] = cscale(F, w.w3);
+    // -i * v * F
+    s.slots[2 * per + i] = make_double2(F.y * w.v[0], -F.x * w.v[0]);
+    s.slots[3 * per + i] = make_double2(F.y * w.v[1], -F.x * w.v[1]);
+    s.slots[4 * per + i] = make_double2(F.y * w.v[2], -F.x * w.v[2]);
+    s.slots[i] = cscale(F, w.w0);
+  }
+  __syncthreads();
+  col_fft(g, s, 5, tc, true);
+  for (int f = 0; f < 5; ++f) store_col_tile(g, s, f, wout + f * fsw, b, c0, tc);
+  if (want_value) {
+    __shared__ double red[32];
+    double t = block_sum(mfa, red);
+    put_part(part, b, CMM_STAT_MFA, nslot_part, tile, t);
+  }
+}
+
+// ======================== column pass 2: dPhi spectra -> C1 spectrum ====
+// Inputs: 5 dPhi spectra (field stride fsg): g_s (pairs with w0), g3 (w3),
+// gv (x,y,z, pairs with kwv2); rho_hat for the MFA term.
+__global__ void __launch_bounds__(CMM_COL_THREADS)
+k_col_backconv(GridDev g, const int* __restrict__ active, double R, double scale,
+               const double2* __restrict__ gin, size_t fsg, const double2* __restrict__ rhohat,
+               const double2* __restrict__ kst, double2* __restrict__ chat, int tc) {
+  const int b = blockIdx.y, c0 = blockIdx.x * tc;
+  if (active && !active[b]) return;
+  ColSmem s = col_smem_setup(g, 6, tc);
+  for (int f = 0; f < 5; ++f) load_col_tile(g, s, f, gin + f * fsg, b, c0, tc);
+  load_col_tile(g, s, 5, rhohat, b, c0, tc);
+  __syncthreads();
+  col_fft(g, s, 6, tc, false);
+  const int nc = g.n2 * g.h3;
+  const size_t per = (size_t)g.n1 * tc;
+  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
+    const int p1 = i / tc, c = i - p1 * tc;
+    const int col = c0 + c;
+    if (col >= nc) continue;
+    const int p2 = col / g.h3, p3 = col - p2 * g.h3;
+    const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];
+    Weights w = fmt_weights(g.kp1[p1], g.kp2[p2], g.kp3[p3], sl, R, g.nq1[p1], g.nq2[p2], g.nq3[p3]);
+    double2 acc = cadd(cscale(s.slots[i], w.w0), cscale(s.slots[per + i], w.w3));
+    // - sum_j G_j * (-i v_j) = + i * sum_j v_j G_j
+    double2 gv = make_double2(0.0, 0.0);
+    for (int a = 0; a < 3; ++a) gv = cadd(gv, cscale(s.slots[(2 + a) * per + i], w.v[a]));
+    acc = cadd(acc, make_double2(-gv.y, gv.x));
+    acc = cscale(acc, scale);
+    double2 K = __ldg(kst + (size_t)p1 * nc + col);
+    acc = cadd(acc, cmul(s.slots[5 * per + i], K));
+    s.slots[i] = acc;
+  }
+  __syncthreads();
+  col_fft(g, s, 1, tc, true);
+  store_col_tile(g, s, 0, chat, b, c0, tc);
+}
+
+// ===================================== plane pass: dPhi/dn (White-Bear) ==
+// Arithmetic of _phi*, _dphi*, get_phi and _get_dphi_* (cmmdft/functionals.py:620-767).
+struct PhiOut { double gs, g3, gv[3], phi; };
+
+__device__ __forceinline__ void phi_funcs(double n3, double ln, double n32, double n33, int base,
+                                          double& p2, double& dp2, double& p3, double& dp3) {
+  const double q = (1 - 2 * n3 + n32);
+  const double c = (1 - 3 * n3 + 3 * n32 - n33);
+  if (base == CMM_FMT) {
+    p2 = 1 / (1.0 - n3);
+    dp2 = 1 / q;
+    p3 = 1 / (24 * M_PI * q);
+    dp3 = 1 / (12 * M_PI * c);
+  } else if (base == CMM_MFMT) {
+    p2 = 1 / (1.0 - n3);
+    dp2 = 1 / q;
+    if (n3 <= 1e-8) {
+      p3 = (1.0 - 2 * n3 / 9 - n32 / 18) / (24 * M_PI * q);
+      dp3 = (8.0 / 3 - 0.5 * n3 - 0.1 * n32) / (36 * M_PI * c);
+    } else {
+      p3 = (n3 + q * ln) / (36 * M_PI * n32 * q);
+      dp3 = -(2 * n3 - 5 * n32 + n33 + 2 * c * ln) / (36 * M_PI * n33 * c);
+    }
+  } else {  // WBII
+    if (n3 <= 1e-8) {
+      p2 = (1 + n32 / 9) / (1 - n3);
+      dp2 = (1 + 2 * n3 / 9 + n32 / 18) / q;
+      p3 = (1 - 4 * n3 / 9 + n32 / 18) / (24 * M_PI * q);
+      dp3 = (7.0 / 3 - n3 / 2 + n32 / 10) / (36 * M_PI * c);
+    } else {
+      p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) / (3 * (n3 - n32));
+      dp2 = -2 * (n3 - 3 * n32 + q * ln) / (3 * n32 * q);
+      p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) / ((3 * n32) * 24 * M_PI * q);
+      dp3 = (2 * n3 - 5 * n32 + 6 * n33 - n32 * n32 + 2 * c * ln) / (36 * M_PI * n33 * c);
+    }
+  }
+}
+
+__device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, double vy, double vz,
+                                            double R, int version) {
+  const double n1 = R * n0;
+  const double n2 = (4.0 * M_PI * R * R) * n0;
+  const double i4r = 1.0 / (4 * M_PI * R);
+  const double ux = vx * i4r, uy = vy * i4r, uz = vz * i4r;  // nv1
+  const double n3 = fmin(fmax(n3raw, 1e-30), 0.99);
+  const double ln = log(1 - n3);
+  const double n32 = n3 * n3, n33 = n32 * n3;
+  const int base = version & 3;
+  const bool anti = (version & CMM_ANTISYM) != 0;
+  double p2, dp2, p3, dp3;
+  phi_funcs(n3, ln, n32, n33, base, p2, dp2, p3, dp3);
+  const double p1 = -ln, dp1 = 1.0 / (1.0 - n3);
+  const double vv = vx * vx + vy * vy + vz * vz;
+  const double uv = ux * vx + uy * vy + uz * vz;
+  double xi = 0.0, pref3;
+  if (anti) {
+    xi = vv / (n2 * n2 + 1e-16);
+    xi = fmin(fmax(xi, 0.0), 1.0);
+    const double om = 1 - xi;
+    pref3 = (n2 * n2 * n2) * (om * om * om);
+  } else {
+    pref3 = n2 * n2 * n2 - 3.0 * n2 * vv;
+  }
+  const double s12 = n1 * n2 - uv;
+  PhiOut o;
+  o.phi = n0 * p1 + s12 * p2 + pref3 * p3;
+  const double d0 = p1;
+  const double d1 = n2 * p2;
+  double d2 = n1 * p2;
+  if (anti) d2 += (3 * (n2 * n2) * (1 + xi) * ((1 - xi) * (1 - xi))) * p3;
+  else d2 += 3 * (n2 * n2 - vv) * p3;
+  const double d3 = n0 * dp1 + s12 * dp2 + pref3 * dp3;
+  const double f3 = anti ? (-6 * n2 * ((1 - xi) * (1 - xi)) * p3) : (-6 * n2 * p3);
+  // dPhi/dnv1 = -nv2 p2 ; dPhi/dnv2 = -nv1 p2 + nv2 f3
+  o.gs = d0 + R * d1 + (4.0 * M_PI * R * R) * d2;
+  o.g3 = d3;
+  const double v[3] = {vx, vy, vz}, u[3] = {ux, uy, uz};
+  for (int a = 0; a < 3; ++a) {
+    const double dv1 = -v[a] * p2;
+    const double dv2 = -u[a] * p2 + v[a] * f3;
+    o.gv[a] = dv1 * i4r + dv2;
+  }
+  return o;
+}
+
+__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version,
+            const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
+            double* __restrict__ part, int nslot_part, int want) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
+  PlaneSmem s = plane_smem_setup(g, 5);
+  const size_t poff = ((size_t)b * g.n1 + i1) * g.n2 * g.h3;
+  load_spec_planes(g, s, 5, win, poff, fsw);
+  __syncthreads();
+  plane_inverse(g, s, 5);
+  double phi = 0.0, n3max = -INFINITY;
+  const bool do_c1 = (want & 1) != 0;
+  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
+    const int r = i / g.n3, j = i - r * g.n3;
+    double& a0 = rel(s, g, 0, r, j);
+    double& a3 = rel(s, g, 1, r, j);
+    double& ax = rel(s, g, 2, r, j);
+    double& ay = rel(s, g, 3, r, j);
+    double& az = rel(s, g, 4, r, j);
+    n3max = fmax(n3max, a3);
+    PhiOut o = fmt_point(a0, a3, ax, ay, az, R, version);
+    phi += o.phi;
+    if (do_c1) {
+      a0 = o.gs; a3 = o.g3; ax = o.gv[0]; ay = o.gv[1]; az = o.gv[2];
+    }
+  }
+  __syncthreads();
+  __shared__ double red[32];
+  if (want & 2) {
+    double t = block_sum(phi, red);
+    put_part(part, b, CMM_STAT_PHI, nslot_part, i1, t);
+  }
+  if (want & 4) {
+    double t = block_max(n3max, red);
+    put_part(part, b, CMM_STAT_N3MAX, nslot_part, i1, t);
+  }
+  if (!do_c1) return;
+  __syncthreads();
+  plane_forward(g, s, 5);
+  store_spec_planes(g, s, 5, gout, poff, fsg);
+}
+
+// ========================================== plane pass: solver updates ==
+struct PlaneStats {
+  double n, iue, nonfin, fid, fext;
+};
+
+__device__ __forceinline__ void stats_point(PlaneStats& st, double rho, double ref, double V,
+                                            double lambda3) {
+  st.n += rho;
+  st.iue += fabs(rho - ref);
+  st.nonfin += cmm_isfinite(rho) ? 0.0 : 1.0;
+  const double rr = (rho < 1e-12) ? 1e-30 : rho;  // Solver._clip_density
+  st.fid += rr * (log(lambda3 * rr) - 1.0);
+  st.fext += rho * V;
+}
+
+__device__ inline void stats_store(const PlaneStats& st, double* part, int b, int nslot, int slot) {
+  __shared__ double red[32];
+  double t;
+  t = block_sum(st.n, red);      put_part(part, b, CMM_STAT_N, nslot, slot, t);
+  t = block_sum(st.iue, red);    put_part(part, b, CMM_STAT_IUE, nslot, slot, t);
+  t = block_sum(st.nonfin, red); put_part(part, b, CMM_STAT_NONFIN, nslot, slot, t);
+  t = block_sum(st.fid, red);    put_part(part, b, CMM_STAT_FID, nslot, slot, t);
+  t = block_sum(st.fext, red);   put_part(part, b, CMM_STAT_FEXT, nslot, slot, t);
+}
+
+// Static Picard step fused with the C1 inverse and the forward of rho'.
+__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
+               double beta, double lambda3, double thr, const double2* __restrict__ chat,
+               const double* __restrict__ rho, const double* __restrict__ V, long long vstride,
+               double* __restrict__ rho_out, double2* __restrict__ rhohat_out,
+               double* __restrict__ part, int nslot_part) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
+  PlaneSmem s = plane_smem_setup(g, 1);
+  const size_t poff = ((size_t)b * g.n1 + i1) * g.n2 * g.h3;
+  load_spec_planes(g, s, 1, chat, poff, 0);
+  __syncthreads();
+  plane_inverse(g, s, 1);
+  const double fug = params[b * 4 + 0], a = params[b * 4 + 1];
+  const size_t roff = ((size_t)b * g.n1 + i1) * g.n2 * g.n3;
+  const double* Vp = V + b * vstride + (size_t)i1 * g.n2 * g.n3;
+  PlaneStats st = {0, 0, 0, 0, 0};
+  double res2 = 0.0, gnf = 0.0;
+  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
+    const int r = i / g.n3, j = i - r * g.n3;
+    double& cell = rel(s, g, 0, r, j);
+    const double v = __ldg(Vp + i);
+    const double C1 = cell + v;
+    const double G = beta * exp(-beta * C1) * fug;
+    const double x = __ldg(rho + roff + i);
+    res2 += (G - x) * (G - x);
+    gnf += cmm_isfinite(G) ? 0.0 : 1.0;
+    double xn = (1.0 - a) * x + a * G;
+    if (xn < thr) xn = 0.0;
+    rho_out[roff + i] = xn;
+    stats_point(st, xn, x, v, lambda3);
+    cell = xn;
+  }
+  {
+    __shared__ double red2[32];
+    double t = block_sum(res2, red2);
+    put_part(part, b, CMM_STAT_RES2, nslot_part, i1, t);
+    t = block_sum(gnf, red2);
+    put_part(part, b, CMM_STAT_GNONFIN, nslot_part, i1, t);
+  }
+  stats_store(st, part, b, nslot_part, i1);
+  __syncthreads();
+  plane_forward(g, s, 1);
+  store_spec_planes(g, s, 1, rhohat_out, poff, 0);
+}
+
+struct HistPtrs { const double* p[CMM_MAX_HIST]; };
+
+// Residual r = G(C1) - rho with the Gram row against stored residuals.
+__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+k_plane_residual(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
+                 double beta, const double2* __restrict__ chat, const double* __restrict__ rho,
+                 const double* __restrict__ V, long long vstride, double* __restrict__ r_out,
+                 HistPtrs hist, int nhist, long long hstride, double* __restrict__ part,
+                 int nslot_part) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
+  PlaneSmem s = plane_smem_setup(g, 1);
+  const size_t poff = ((size_t)b * g.n1 + i1) * g.n2 * g.h3;
+  load_spec_planes(g, s, 1, chat, poff, 0);
+  __syncthreads();
+  plane_inverse(g, s, 1);
+  const double fug = params[b * 4 + 0];
+  const size_t roff = ((size_t)b * g.n1 + i1) * g.n2 * g.n3;
+  const size_t hoff = (size_t)b * hstride + (size_t)i1 * g.n2 * g.n3;
+  const double* Vp = V + b * vstride + (size_t)i1 * g.n2 * g.n3;
+  double res2 = 0.0, gnf = 0.0;
+  double gram[CMM_MAX_HIST];
+#pragma unroll
+  for (int j = 0; j < CMM_MAX_HIST; ++j) gram[j] = 0.0;
+  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
+    const int r = i / g.n3, j = i - r * g.n3;
+    const double C1 = rel(s, g, 0, r, j) + __ldg(Vp + i);
+    const double G = beta * exp(-beta * C1) * fug;
+    const double x = __ldg(rho + roff + i);
+    const double rr = G - x;
+    res2 += rr * rr;
+    gnf += cmm_isfinite(G) ? 0.0 : 1.0;
+    r_out[roff + i] = rr;
+#pragma unroll
+    for (int h = 0; h < CMM_MAX_HIST; ++h)
+      if (h < nhist) gram[h] += rr * __ldg(hist.p[h] + hoff + i);
+  }
+  __shared__ double red[32];
+  double t = block_sum(res2, red);
+  put_part(part, b, CMM_STAT_RES2, nslot_part, i1, t);
+  t = block_sum(gnf, red);
+  put_part(part, b, CMM_STAT_GNONFIN, nslot_part, i1, t);
+  for (int h = 0; h < nhist; ++h) {
+    t = block_sum(gram[h], red);
+    put_part(part, b, CMM_STAT_GRAM0 + h, nslot_part, i1, t);
+  }
+}
+
+struct FieldPtrs { const double* p[CMM_MAX_FIELDS]; long long stride[CMM_MAX_FIELDS]; };
+
+// rho' = sum_j c_j field_j, clipped, with stats and the forward transform.
+__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+k_plane_mix(GridDev g, const int* __restrict__ active, const double* __restrict__ coef,
+            FieldPtrs fields, int nfield, int clip, double thr, double lambda3, const double* __restrict__ ref,
+            long long refstride, const double* __restrict__ V, long long vstride,
+            double* __restrict__ rho_out, double2* __restrict__ rhohat_out,
+            double* __restrict__ part, int nslot_part) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
+  PlaneSmem s = plane_smem_setup(g, 1);
+  const size_t plane = (size_t)i1 * g.n2 * g.n3;
+  const size_t roff = (size_t)b * g.n1 * g.n2 * g.n3 + plane;
+  const double* Vp = V + b * vstride + plane;
+  const double* Rp = ref + b * refstride + plane;
+  double c[CMM_MAX_FIELDS];
+#pragma unroll
+  for (int j = 0; j < CMM_MAX_FIELDS; ++j) c[j] = (j < nfield) ? coef[b * CMM_MAX_FIELDS + j] : 0.0;
+  PlaneStats st = {0, 0, 0, 0, 0};
+  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
+    const int r = i / g.n3, j = i - r * g.n3;
+    double x = 0.0;
+#pragma unroll
+    for (int f = 0; f < CMM_MAX_FIELDS; ++f)
+      if (f < nfield && c[f] != 0.0) x += c[f] * __ldg(fields.p[f] + b * fields.stride[f] + plane + i);
+    if (clip == CMM_CLIP_DENSITY) x = (x < 1e-12) ? 1e-30 : x;
+    else if (clip == CMM_CLIP_PICARD && x < thr) x = 0.0;
+    rho_out[roff + i] = x;
+    stats_point(st, x, __ldg(Rp + i), __ldg(Vp + i), lambda3);
+    rel(s, g, 0, r, j) = x;
+  }
+  stats_store(st, part, b, nslot_part, i1);
+  __syncthreads();
+  plane_forward(g, s, 1);
+  store_spec_planes(g, s, 1, rhohat_out, ((size_t)b * g.n1 + i1) * g.n2 * g.h3, 0);
+}
+
+// ============================================================ finalize ==
+__global__ void k_stats_finalize(const int* __restrict__ active, const double* __restrict__ part,
+                                 int nslot, unsigned mask, double* __restrict__ stats) {
+  const int b = blockIdx.x, q = threadIdx.y;
+  if (q >= NQ || !((mask >> q) & 1u)) return;
+  if (active && !active[b]) return;
+  const double* p = part + ((size_t)b * NQ + q) * nslot;
+  const bool mx = (q == CMM_STAT_N3MAX);
+  double acc = mx ? -INFINITY : 0.0;
+  for (int i = threadIdx.x; i < nslot; i += 32) acc = mx ? fmax(acc, p[i]) : acc + p[i];
+  for (int o = 16; o > 0; o >>= 1) {
+    double v = __shfl_xor_sync(0xffffffffu, acc, o);
+    acc = mx ? fmax(acc, v) : acc + v;
+  }
+  if (threadIdx.x == 0) stats[(size_t)b * NQ + q] = acc;
+}
+
+// ============================================================ host side ==
+static int last_err() { return (cudaPeekAtLastError() == cudaSuccess) ? CMM_OK : CMM_ERR_CUDA; }
+
+static int set_smem(const void* fn, size_t bytes) {
+  if (bytes > 232448) return CMM_ERR_SMEM;
+  if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
+    return CMM_ERR_CUDA;
+  return CMM_OK;
+}
+
+// Column tile width: >= 8 columns (128 B rows) when it fits, scaled down for long x.
+static int col_tile(const cmm_grid* g, int nslot) {
+  int tc = 16;
+  while (tc > 1 && col_smem_bytes(g->n1, tc, nslot) > 200 * 1024) tc /= 2;
+  return tc;
+}
+
+extern "C" int cmm_plane_smem_bytes(const cmm_grid* g, int nslot, size_t* bytes) {
+  if (!g || !bytes) return CMM_ERR_ARG;
+  *bytes = plane_smem_bytes(g->n2, g->n3, nslot);
+  return CMM_OK;
+}
+
+extern "C" int cmm_rfft3d(const cmm_grid* g, int batch, const double* d_in, double* d_spec, void* stream) {
+  if (!g || !d_in || !d_spec || batch < 1) return CMM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  int rc = set_smem((const void*)k_plane_r2c, ps);
+  if (rc) return rc;
+  k_plane_r2c<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, st>>>(g->dev, d_in, (double2*)d_spec);
+  int tc = col_tile(g, 1);
+  size_t cs = col_smem_bytes(g->n1, tc, 1);
+  rc = set_smem((const void*)k_col_fft, cs);
+  if (rc) return rc;
+  const int* k1 = g->dev.k1pos;
+  int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
+  k_col_fft<<<dim3(ntile, batch), CMM_COL_THREADS, cs, st>>>(g->dev, (const double2*)d_spec, (double2*)d_spec, tc, 0, k1);
+  return last_err();
+}
+
+extern "C" int cmm_irfft3d(const cmm_grid* g, int batch, double* d_spec, double* d_out, void* stream) {
+  if (!g || !d_spec || !d_out || batch < 1) return CMM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  int tc = col_tile(g, 1);
+  size_t cs = col_smem_bytes(g->n1, tc, 1);
+  int rc = set_smem((const void*)k_col_fft, cs);
+  if (rc) return rc;
+  const int* k1 = g->dev.k1pos;
+  int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
+  // in place on the caller's spectrum (it is consumed)
+  k_col_fft<<<dim3(ntile, batch), CMM_COL_THREADS, cs, st>>>(g->dev, (const double2*)d_spec, (double2*)d_spec, tc, 1, k1);
+  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  rc = set_smem((const void*)k_plane_c2r, ps);
+  if (rc) return rc;
+  k_plane_c2r<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, st>>>(g->dev, (const double2*)d_spec, d_out);
+  return last_err();
+}
+
+extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, double R, double beta,
+                          int version, const double* d_kst, const double* d_rhohat, double* d_chat,
+                          double* d_work, double* d_part, int nslot, int want, void* stream) {
+  if (!g || batch < 1 || !d_kst || !d_rhohat || !d_work || !d_part) return CMM_ERR_ARG;
+  if ((want & 1) && !d_chat) return CMM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t fs = (size_t)batch * g->n1 * g->n2 * g->h3;  // field stride (double2)
+  double2* wbuf = (double2*)d_work;          // 5 weighted-density spectra
+  double2* gbuf = wbuf + 5 * fs;             // 5 dPhi spectra
+  const double npts = (double)g->n1 * g->n2 * g->n3;
+  int tc = col_tile(g, 6);
+  int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
+  if (nslot < g->n1 || nslot < ntile) return CMM_ERR_WORKSPACE;
+  size_t cs5 = col_smem_bytes(g->n1, tc, 5), cs6 = col_smem_bytes(g->n1, tc, 6);
+  int rc = set_smem((const void*)k_col_weights, cs5);
+  if (rc) return rc;
+  k_col_weights<<<dim3(ntile, batch), CMM_COL_THREADS, cs5, st>>>(
+      g->dev, d_active, R, 1.0 / npts, (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst,
+      d_part, nslot, (want & 2) ? 1 : 0, tc);
+  size_t ps = plane_smem_bytes(g->n2, g->n3, 5);
+  rc = set_smem((const void*)k_plane_fmt, ps);
+  if (rc) return rc;
+  k_plane_fmt<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, st>>>(g->dev, d_active, R, version, wbuf, fs,
+                                                                gbuf, fs, d_part, nslot, want);
+  if (want & 1) {
+    rc = set_smem((const void*)k_col_backconv, cs6);
+    if (rc) return rc;
+    k_col_backconv<<<dim3(ntile, batch), CMM_COL_THREADS, cs6, st>>>(
+        g->dev, d_active, R, 1.0 / (beta * npts), gbuf, fs, (const double2*)d_rhohat,
+        (const double2*)d_kst, (double2*)d_chat, tc);
+  }
+  return last_err();
+}
+
+extern "C" int cmm_picard_static_step(const cmm_grid* g, int batch, const int* d_active,
+                                      const double* d_params, double beta, double lambda3, double thr,
+                                      const double* d_chat, const double* d_rho, const double* d_V,
+                                      long long vstride, double* d_rho_out, double* d_rhohat_out,
+                                      double* d_part, int nslot, void* stream) {
+  if (!g || batch < 1 || !d_params || !d_chat || !d_rho || !d_V || !d_rho_out || !d_rhohat_out || !d_part)
+    return CMM_ERR_ARG;
+  if (nslot < g->n1) return CMM_ERR_WORKSPACE;
+  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  int rc = set_smem((const void*)k_plane_picard, ps);
+  if (rc) return rc;
+  k_plane_picard<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(
+      g->dev, d_active, d_params, beta, lambda3, thr, (const double2*)d_chat, d_rho, d_V, vstride,
+      d_rho_out, (double2*)d_rhohat_out, d_part, nslot);
+  return last_err();
+}
+
+extern "C" int cmm_residual_step(const cmm_grid* g, int batch, const int* d_active, const double* d_params,
+                                 double beta, const double* d_chat, const double* d_rho, const double* d_V,
+                                 long long vstride, double* d_r_out, const double* const* d_hist, int nhist,
+                                 long long hstride, double* d_part, int nslot, void* stream) {
+  if (!g || batch < 1 || !d_params || !d_chat || !d_rho || !d_V || !d_r_out || !d_part) return CMM_ERR_ARG;
+  if (nhist < 0 || nhist > CMM_MAX_HIST || (nhist && !d_hist)) return CMM_ERR_ARG;
+  if (nslot < g->n1) return CMM_ERR_WORKSPACE;
+  HistPtrs hp;
+  for (int j = 0; j < CMM_MAX_HIST; ++j) hp.p[j] = (j < nhist) ? d_hist[j] : nullptr;
+  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  int rc = set_smem((const void*)k_plane_residual, ps);
+  if (rc) return rc;
+  k_plane_residual<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(
+      g->dev, d_active, d_params, beta, (const double2*)d_chat, d_rho, d_V, vstride, d_r_out, hp, nhist,
+      hstride, d_part, nslot);
+  return last_err();
+}
+
+extern "C" int cmm_mix_step(const cmm_grid* g, int batch, const int* d_active, const double* d_coef,
+                            const double* const* d_fields, const long long* fstride, int nfield, int clip,
+                            double thr, double lambda3, const double* d_ref, long long refstride, const double* d_V,
+                            long long vstride, double* d_rho_out, double* d_rhohat_out, double* d_part,
+                            int nslot, void* stream) {
+  if (!g || batch < 1 || !d_coef || !d_fields || !fstride || !d_ref || !d_V || !d_rho_out || !d_rhohat_out)
+    return CMM_ERR_ARG;
+  if (nfield < 1 || nfield > CMM_MAX_FIELDS) return CMM_ERR_ARG;
+  if (nslot < g->n1) return CMM_ERR_WORKSPACE;
+  FieldPtrs fp;
+  for (int j = 0; j < CMM_MAX_FIELDS; ++j) {
+    fp.p[j] = (j < nfield) ? d_fields[j] : nullptr;
+    fp.stride[j] = (j < nfield) ? fstride[j] : 0;
+  }
+  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  int rc = set_smem((const void*)k_plane_mix, ps);
+  if (rc) return rc;
+  k_plane_mix<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(
+      g->dev, d_active, d_coef, fp, nfield, clip, thr, lambda3, d_ref, refstride, d_V, vstride, d_rho_out,
+      (double2*)d_rhohat_out, d_part, nslot);
+  return last_err();
+}
+
+extern "C" int cmm_stats_finalize(int batch, const int* d_active, const double* d_part, int nslot,
+                                  unsigned mask, double* d_stats, void* stream) {
+  if (batch < 1 || !d_part || !d_stats || nslot < 1) return CMM_ERR_ARG;
+  k_stats_finalize<<<batch, dim3(32, NQ), 0, (cudaStream_t)stream>>>(d_active, d_part, nslot, mask, d_stats);
+  return last_err();
+}

@@ -1,0 +1,213 @@
+"""Device-side objects: grid plans, the functional pipeline and its buffers.
+
+Everything here drives the CUDA library through its C ABI (``_lib``) with
+torch tensors as device memory and the current torch stream.  There is no CPU
+path: every method requires a CUDA device.
+"""
+import ctypes
+
+import numpy as np
+import torch
+
+from . import _lib as L
+from ._lib import check, ptr
+
+
+def _stream():
+    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+def require_cuda():
+    if not torch.cuda.is_available():
+        raise L.CmmError("cmmdft_b200 needs a CUDA device (sm_100a); there is no CPU fallback")
+
+
+class GridPlan(object):
+    """A grid plan for an N1 x N2 x N3 grid of the cell ``rvecs`` (rows, bohr).
+
+    Wraps ``cmm_grid_create``; owns the plan's device tables.
+    """
+
+    def __init__(self, npoints, rvecs):
+        require_cuda()
+        self.lib = L.lib()
+        n1, n2, n3 = [int(n) for n in npoints]
+        self.npoints = (n1, n2, n3)
+        self.rvecs = np.ascontiguousarray(rvecs, dtype=np.float64).reshape(3, 3)
+        h = ctypes.c_void_p()
+        rv = (ctypes.c_double * 9)(*self.rvecs.ravel().tolist())
+        check(self.lib.cmm_grid_create(n1, n2, n3, rv, ctypes.byref(h)), "cmm_grid_create")
+        self.handle = h
+        ns = ctypes.c_longlong()
+        h3 = ctypes.c_int()
+        check(self.lib.cmm_grid_spectrum_size(h, ctypes.byref(ns), ctypes.byref(h3)))
+        self.nspec = int(ns.value)
+        self.h3 = int(h3.value)
+        self.npts = n1 * n2 * n3
+        k1 = (ctypes.c_int * n1)()
+        k2 = (ctypes.c_int * n2)()
+        k3 = (ctypes.c_int * self.h3)()
+        check(self.lib.cmm_spectrum_index(h, k1, k2, k3))
+        self.k1 = np.array(k1[:], dtype=np.int64)
+        self.k2 = np.array(k2[:], dtype=np.int64)
+        self.k3 = np.array(k3[:], dtype=np.int64)
+        self.volume = float(abs(np.linalg.det(self.rvecs)))
+        self.dr = self.volume / self.npts
+
+    def __del__(self):
+        try:
+            if getattr(self, "handle", None) is not None:
+                self.lib.cmm_grid_destroy(self.handle)
+                self.handle = None
+        except Exception:
+            pass
+
+    # ---- spectra -------------------------------------------------------
+    def new_spec(self, batch=1):
+        return torch.empty((batch, self.nspec * 2), dtype=torch.float64, device="cuda")
+
+    def rfft(self, x):
+        """Half spectrum (plan layout, unnormalised) of real fields [B, N1, N2, N3]."""
+        x = x.contiguous()
+        B = x.shape[0]
+        out = self.new_spec(B)
+        check(self.lib.cmm_rfft3d(self.handle, B, ptr(x), ptr(out), _stream()), "cmm_rfft3d")
+        return out
+
+    def irfft(self, spec):
+        """Inverse of :meth:`rfft` times N (unnormalised), as real fields."""
+        s = spec.clone()
+        B = s.shape[0]
+        out = torch.empty((B,) + self.npoints, dtype=torch.float64, device="cuda")
+        check(self.lib.cmm_irfft3d(self.handle, B, ptr(s), ptr(out), _stream()), "cmm_irfft3d")
+        return out
+
+    def spec_to_full(self, spec):
+        """Full numpy spectrum [B, N1, N2, N3] (scipy fftn order) from a plan-layout spectrum."""
+        n1, n2, n3 = self.npoints
+        s = spec.detach().cpu().numpy().view(np.complex128).reshape(-1, n1, n2, self.h3)
+        B = s.shape[0]
+        full = np.zeros((B, n1, n2, n3), dtype=np.complex128)
+        k2 = self.k2[None, :, None]
+        k3 = self.k3[None, None, :]
+        k1 = self.k1[:, None, None]
+        for b in range(B):
+            full[b][k1, k2, k3] = s[b]
+            # Hermitian completion
+            kk1 = (-k1) % n1
+            kk2 = (-k2) % n2
+            kk3 = (-k3) % n3
+            full[b][kk1, kk2, kk3] = np.conj(s[b])
+            full[b][k1, k2, k3] = s[b]
+        return full
+
+
+class Buffers(object):
+    """Workspace of one shape group of ``batch`` instances."""
+
+    def __init__(self, plan, batch, nhist=0):
+        self.plan = plan
+        self.batch = batch
+        n1, n2, n3 = plan.npoints
+        dev = "cuda"
+        f64 = torch.float64
+        fs = plan.nspec * 2
+        self.work = torch.empty((10, batch, fs), dtype=f64, device=dev)
+        self.nslot = max(n1, -(-(n2 * plan.h3) // 1))  # >= ntiles for any column tile >= 1
+        self.part = torch.zeros((batch, L.NSTAT, self.nslot), dtype=f64, device=dev)
+        self.stats = torch.zeros((batch, L.NSTAT), dtype=f64, device=dev)
+        self.active = torch.ones(batch, dtype=torch.int32, device=dev)
+
+
+class Functional(object):
+    """Device data of the WBII/FMT + MFA + external-potential functional of one
+    host, guest, grid and temperature.
+
+    Mirrors the part list FreeEnergy builds with add_hard_sphere,
+    add_mean_field and add_external_potential (cmmdft/functionals.py:176-337).
+    """
+
+    def __init__(self, plan, R, beta, wavelength, V, version=L.WBII, kst=None, vdw_a=None):
+        self.plan = plan
+        self.R = float(R)
+        self.beta = float(beta)
+        self.wavelength = float(wavelength)
+        self.lambda3 = float(wavelength) ** 3
+        self.V = V.contiguous()                       # [N1, N2, N3] device
+        self.version = int(version)
+        self.kst = kst                                # MFA kernel spectrum (or zeros)
+        if self.kst is None:
+            self.kst = torch.zeros(plan.nspec * 2, dtype=torch.float64, device="cuda")
+        self.vdw_a = vdw_a
+
+    def c1(self, buf, rhohat, chat, want=1, active=None, batch=None):
+        """Spectrum of C1 - V (HardSphere.derive + MFA.derive) for every instance."""
+        B = buf.batch if batch is None else batch
+        check(L.lib().cmm_fmt_c1(self.plan.handle, B, ptr(active), self.R, self.beta, self.version,
+                                 ptr(self.kst), ptr(rhohat), ptr(chat), ptr(buf.work), ptr(buf.part),
+                                 buf.nslot, int(want), _stream()), "cmm_fmt_c1")
+
+
+def mfa_kernel_spectrum(plan, sigma, epsilon, cutoff, rmin=None, limit=0.0, rep=1):
+    """MFA kernel spectrum for MFAFunctional.generate_potential_lj and its vdW ``a``."""
+    lib = L.lib()
+    if rmin is None:
+        rmin = sigma
+    cut = -1.0 if cutoff is None else float(cutoff)
+    need = ctypes.c_size_t(0)
+    check(lib.cmm_mfa_kernel(plan.handle, sigma, epsilon, cut, rmin, limit, rep, None, None,
+                             ctypes.byref(need), None, _stream()), "cmm_mfa_kernel(size)")
+    work = torch.empty(int(need.value) // 8 + 1, dtype=torch.float64, device="cuda")
+    kst = torch.empty(plan.nspec * 2, dtype=torch.float64, device="cuda")
+    a = ctypes.c_double(0.0)
+    check(lib.cmm_mfa_kernel(plan.handle, sigma, epsilon, cut, rmin, limit, rep, ptr(kst), ptr(work),
+                             ctypes.byref(need), ctypes.byref(a), _stream()), "cmm_mfa_kernel")
+    return kst, float(a.value)
+
+
+def external_potential(plan, pos, type_ids, type_sigma, type_epsilon, guest_sigma, guest_epsilon,
+                       cutoff, v_cap):
+    """LJ external potential of a host on the plan's grid (device tensor [N1,N2,N3])."""
+    dev = "cuda"
+    pos_t = torch.as_tensor(np.ascontiguousarray(pos, dtype=np.float64), device=dev)
+    typ_t = torch.as_tensor(np.ascontiguousarray(type_ids, dtype=np.int32), device=dev)
+    sig_t = torch.as_tensor(np.ascontiguousarray(type_sigma, dtype=np.float64), device=dev)
+    eps_t = torch.as_tensor(np.ascontiguousarray(type_epsilon, dtype=np.float64), device=dev)
+    V = torch.empty(plan.npoints, dtype=torch.float64, device=dev)
+    check(L.lib().cmm_extpot_lj(plan.handle, ptr(pos_t), ptr(typ_t), int(len(pos_t)), ptr(sig_t), ptr(eps_t),
+                                int(len(sig_t)), float(guest_sigma), float(guest_epsilon), float(cutoff),
+                                float(v_cap), ptr(V), _stream()), "cmm_extpot_lj")
+    return V
+
+
+def finalize(buf, mask, active=None):
+    check(L.lib().cmm_stats_finalize(buf.batch, ptr(active), ptr(buf.part), buf.nslot, ctypes.c_uint(mask),
+                                     ptr(buf.stats), _stream()), "cmm_stats_finalize")
+
+
+def picard_static_step(fn, buf, params, thr, chat, rho, rho_out, rhohat_out, active=None, vstride=0):
+    check(L.lib().cmm_picard_static_step(fn.plan.handle, buf.batch, ptr(active), ptr(params), fn.beta,
+                                         fn.lambda3, float(thr), ptr(chat), ptr(rho), ptr(fn.V), int(vstride),
+                                         ptr(rho_out), ptr(rhohat_out), ptr(buf.part), buf.nslot, _stream()),
+          "cmm_picard_static_step")
+
+
+def residual_step(fn, buf, params, chat, rho, r_out, hist=(), hstride=0, active=None, vstride=0):
+    n = len(hist)
+    arr = (ctypes.c_void_p * max(n, 1))(*[h.data_ptr() for h in hist]) if n else None
+    check(L.lib().cmm_residual_step(fn.plan.handle, buf.batch, ptr(active), ptr(params), fn.beta, ptr(chat),
+                                    ptr(rho), ptr(fn.V), int(vstride), ptr(r_out), arr, n, int(hstride),
+                                    ptr(buf.part), buf.nslot, _stream()), "cmm_residual_step")
+
+
+def mix_step(fn, buf, coef, fields, strides, clip, ref, rho_out, rhohat_out, thr=0.0, active=None,
+             refstride=None, vstride=0):
+    n = len(fields)
+    arr = (ctypes.c_void_p * n)(*[f.data_ptr() for f in fields])
+    st = (ctypes.c_longlong * n)(*[int(s) for s in strides])
+    if refstride is None:
+        refstride = fn.plan.npts
+    check(L.lib().cmm_mix_step(fn.plan.handle, buf.batch, ptr(active), ptr(coef), arr, st, n, int(clip),
+                               float(thr), fn.lambda3, ptr(ref), int(refstride), ptr(fn.V), int(vstride),
+                               ptr(rho_out), ptr(rhohat_out), ptr(buf.part), buf.nslot, _stream()),
+          "cmm_mix_step")

@@ -1,0 +1,232 @@
+"""Bulk equations of state (host-side scalars).
+
+Restates cmmdft/eos.py: the EquationOfState interface (:22-223), SumOfEOS
+(:226-265), the modified Benedict-Webb-Rubin LJ equation of Johnson, Zollweg
+and Gubbins (Mol. Phys. 78, 591 (1993), regression parameters of their
+Table 10; cmmdft/eos.py:295-469), Carnahan-Starling (:471-520) and the
+mean-field EOS (:523-546).  These are scalar/1-D numpy evaluations that set
+up mu(P) and bulk densities; the grid solve never calls them per point.
+"""
+import numpy as np
+from scipy.optimize import brentq
+
+from .units import angstrom, boltzmann, planck
+
+__all__ = ['EquationOfState', 'SumOfEOS', 'ModifiedBenedictWebbRubinEOS', 'CarnahanStarlingEOS', 'MFAEOS']
+
+
+class EquationOfState(object):
+    def __init__(self, mass):
+        self.mass = mass
+        self.temperature = None
+
+    def set_temperature(self, temperature):
+        self.temperature = temperature
+        self.wvl = planck / np.sqrt(2 * np.pi * self.mass * boltzmann * temperature)
+
+    def excess_free_energy_particle(self, rho):
+        raise NotImplementedError
+
+    def derivative_excess_free_energy_particle(self, rho):
+        raise NotImplementedError
+
+    def excess_free_energy_volume(self, rho):
+        return rho * self.excess_free_energy_particle(rho)
+
+    def derivative_excess_free_energy_volume(self, rho):
+        v = rho * self.derivative_excess_free_energy_particle(rho)
+        v += self.excess_free_energy_particle(rho)
+        return v
+
+    def compute_chempot(self, rho):
+        kT = boltzmann * self.temperature
+        return kT * np.log(self.wvl ** 3 * rho) + self.derivative_excess_free_energy_volume(rho)
+
+    def compute_pressure(self, rho):
+        kT = boltzmann * self.temperature
+        return kT * rho + rho ** 2 * self.derivative_excess_free_energy_particle(rho)
+
+    def get_rough_density_grid(self, npoints):
+        return np.logspace(-10, 0, npoints) / angstrom ** 3
+
+    def _brackets(self, values, grid_values, grid):
+        out = []
+        for v in values:
+            iv = []
+            for j in range(1, len(grid)):
+                if grid_values[j - 1] <= v <= grid_values[j]:
+                    iv.append((grid[j - 1], grid[j]))
+            out.append(iv)
+        return out
+
+    def solve_densities_from_chempots(self, chempots, n_rough_gridpoints=1000):
+        """All roots rho of mu(rho) = mu per chempot (<= 2 branches kept), eos.py:85-119."""
+        grid = self.get_rough_density_grid(n_rough_gridpoints)
+        kT = boltzmann * self.temperature
+        mg = kT * np.log(self.wvl ** 3 * grid) + self.excess_free_energy_particle(grid) + \
+            grid * self.derivative_excess_free_energy_particle(grid)
+        out = np.zeros([len(chempots), 2]) * np.nan
+        for i, (mu, iv) in enumerate(zip(chempots, self._brackets(chempots, mg, grid))):
+            f = lambda r: kT * np.log(self.wvl ** 3 * r) + self.excess_free_energy_particle(r) + \
+                r * self.derivative_excess_free_energy_particle(r) - mu
+            sols = sorted(brentq(f, a, b) for a, b in iv)
+            if len(sols) > 3:
+                raise ValueError('more than 3 density branches')
+            out[i, :len(sols)] = sols
+        return out
+
+    def solve_densities_from_pressures(self, pressures, n_rough_gridpoints=10000):
+        """All roots rho of p(rho) = p, eos.py:121-157."""
+        grid = self.get_rough_density_grid(n_rough_gridpoints)
+        kT = boltzmann * self.temperature
+        pg = kT * grid + grid ** 2 * self.derivative_excess_free_energy_particle(grid)
+        out = np.zeros([len(pressures), 3]) * np.nan
+        for i, (p, iv) in enumerate(zip(pressures, self._brackets(pressures, pg, grid))):
+            f = lambda r: kT * r + r ** 2 * self.derivative_excess_free_energy_particle(r) - p
+            sols = sorted(brentq(f, a, b) for a, b in iv)
+            if len(sols) > 3:
+                raise ValueError('more than 3 density branches')
+            out[i, :len(sols)] = sols
+        return out
+
+    def calculate_mu(self, temp, pressure):
+        """Chemical potential of the lowest-density branch at (T, P), eos.py:209-215."""
+        self.set_temperature(temp)
+        rho = self.solve_densities_from_pressures([pressure])[0][0]
+        return self.compute_chempot(rho)
+
+    def bulk_density(self, temp, chempot):
+        """Lowest density branch at (T, mu) (Calculator.return_loading, calculator.py:129-131)."""
+        self.set_temperature(temp)
+        return float(np.nanmin(self.solve_densities_from_chempots([chempot]), axis=1)[0])
+
+
+class SumOfEOS(EquationOfState):
+    def __init__(self, mass, list_eos, factors=None):
+        EquationOfState.__init__(self, mass)
+        self.list_eos = list(list_eos)
+        self.factors = [1.0] * len(self.list_eos) if factors is None else list(factors)
+
+    def set_temperature(self, temperature):
+        for e in self.list_eos:
+            e.set_temperature(temperature)
+        EquationOfState.set_temperature(self, temperature)
+
+    def _sum(self, name, rho):
+        r = rho * 0.0
+        for e, f in zip(self.list_eos, self.factors):
+            r += f * getattr(e, name)(rho)
+        return r
+
+    def excess_free_energy_particle(self, rho):
+        return self._sum('excess_free_energy_particle', rho)
+
+    def excess_free_energy_volume(self, rho):
+        return self._sum('excess_free_energy_volume', rho)
+
+    def derivative_excess_free_energy_particle(self, rho):
+        return self._sum('derivative_excess_free_energy_particle', rho)
+
+    def derivative_excess_free_energy_volume(self, rho):
+        return self._sum('derivative_excess_free_energy_volume', rho)
+
+
+# Johnson-Zollweg-Gubbins (1993) Table 10 regression parameters x1..x32.
+_MBWR_X = (0.8623085097507421, 2.976218765822098, -8.402230115796038, 0.1054136629203555,
+           -0.8564583828174598, 1.582759470107601, 0.7639421948305453, 1.753173414312048,
+           2.798291772190376e+3, -4.8394220260857657e-2, 0.9963265197721935, -3.698000291272493e+1,
+           2.084012299434647e+1, 8.305402124717285e+1, -9.574799715203068e+2, -1.477746229234994e+2,
+           6.398607852471505e+1, 1.603993673294834e+1, 6.805916615864377e+1, -2.791293578795945e+3,
+           -6.245128304568454, -8.116836104958410e+3, 1.488735559561229e+1, -1.059346754655084e+4,
+           -1.131607632802822e+2, -8.867771540418822e+3, -3.986982844450543e+1, -4.689270299917261e+3,
+           2.593535277438717e+2, -2.694523589434903e+3, -7.218487631550215e+2, 1.721802063863269e+2)
+
+
+class ModifiedBenedictWebbRubinEOS(EquationOfState):
+    name = 'MBWR'
+    gamma = 3.0
+
+    def __init__(self, mass, sigma, epsilon):
+        EquationOfState.__init__(self, mass)
+        self.sigma, self.epsilon = sigma, epsilon
+
+    def set_temperature(self, temperature):
+        EquationOfState.set_temperature(self, temperature)
+        x = (None,) + _MBWR_X
+        T = boltzmann * temperature / self.epsilon
+        self.a = [x[1] * T + x[2] * np.sqrt(T) + x[3] + x[4] / T + x[5] / T ** 2,
+                  x[6] * T + x[7] + x[8] / T + x[9] / T ** 2,
+                  x[10] * T + x[11] + x[12] / T,
+                  x[13],
+                  x[14] / T + x[15] / T ** 2,
+                  x[16] / T,
+                  x[17] / T + x[18] / T ** 2,
+                  x[19] / T ** 2]
+        self.b = [x[20] / T ** 2 + x[21] / T ** 3,
+                  x[22] / T ** 2 + x[23] / T ** 4,
+                  x[24] / T ** 2 + x[25] / T ** 3,
+                  x[26] / T ** 2 + x[27] / T ** 4,
+                  x[28] / T ** 2 + x[29] / T ** 3,
+                  x[30] / T ** 2 + x[31] / T ** 3 + x[32] / T ** 4]
+
+    def _G(self, rho):
+        rr = rho * self.sigma ** 3
+        F = np.exp(-self.gamma * rr ** 2)
+        ig = 1.0 / (2 * self.gamma)
+        G = [ig * (1 - F)]
+        for n in range(2, 7):
+            G.append(-ig * (F * rr ** (2 * (n - 1)) - 2 * (n - 1) * G[-1]))
+        return G
+
+    def excess_free_energy_particle(self, rho):
+        A = 0.0
+        rr = rho * self.sigma ** 3
+        for i, ai in enumerate(self.a):
+            A += ai / (i + 1) * rr ** (i + 1)
+        for bi, Gi in zip(self.b, self._G(rho)):
+            A += bi * Gi
+        return A * self.epsilon
+
+    def derivative_excess_free_energy_particle(self, rho):
+        dA = 0.0
+        rr = rho * self.sigma ** 3
+        for i, ai in enumerate(self.a):
+            dA += ai * rr ** i * self.sigma ** 3
+        F = np.exp(-self.gamma * rr ** 2)
+        for t, bi in enumerate(self.b):
+            dA += bi * self.sigma ** 3 * rr ** (2 * t + 1) * F
+        return dA * self.epsilon
+
+    def get_rough_density_grid(self, npoints):
+        return np.logspace(-10, 0, npoints) * 1.5 / self.sigma ** 3
+
+
+class CarnahanStarlingEOS(EquationOfState):
+    name = 'CS'
+
+    def __init__(self, mass, Rhs):
+        EquationOfState.__init__(self, mass)
+        self.R = float(Rhs)
+        self.eta = 4 * np.pi * self.R ** 3 / 3
+
+    def excess_free_energy_particle(self, rho):
+        kT = boltzmann * self.temperature
+        return kT * (4 * self.eta * rho - 3 * (self.eta * rho) ** 2) / (1 - self.eta * rho) ** 2
+
+    def derivative_excess_free_energy_particle(self, rho):
+        kT = boltzmann * self.temperature
+        return 2 * kT * self.eta * (2 - self.eta * rho) / (1 - self.eta * rho) ** 3
+
+
+class MFAEOS(EquationOfState):
+    name = 'MFA'
+
+    def __init__(self, mass, sigma=None, epsilon=None, a=None):
+        EquationOfState.__init__(self, mass)
+        self.a = a if a is not None else -16 / 9 * np.pi * epsilon * sigma ** 3
+
+    def excess_free_energy_particle(self, rho):
+        return self.a * rho
+
+    def derivative_excess_free_energy_particle(self, rho):
+        return self.a + 0 * rho

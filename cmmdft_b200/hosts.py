@@ -1,0 +1,136 @@
+"""Seeded synthetic hosts and the LJ parameter sets of the benchmark workloads.
+
+The reference reads hosts from yaff checkpoints plus an ``LJ:PARS`` file
+(cmmdft/system.py:54-73, cmmdft/extpot_calculator.py:705-716).  The benchmark
+workloads use synthetic hosts instead: atoms placed by random sequential
+addition (RSA) in an orthorhombic cell with a minimum nearest-image
+separation, and atom types drawn as a seeded permutation of fixed counts.
+The four atom types carry the UFF sigma/epsilon of a ZIF-8-like framework
+(C, H, N, Zn), and the guest is united-atom TraPPE methane.
+"""
+
+import numpy as np
+
+from .units import angstrom, boltzmann, amu
+
+# (sigma [angstrom], epsilon/kB [K]) per host atom type.
+HOST_LJ_TYPES = {
+    "C": (3.43, 52.8),
+    "H": (2.57, 22.1),
+    "N": (3.26, 34.7),
+    "Zn": (2.46, 62.4),
+}
+# Type counts of the 276-atom cell; larger cells keep these fractions.
+HOST_TYPE_COUNTS = {"C": 96, "H": 120, "N": 48, "Zn": 12}
+
+# United-atom methane: sigma [angstrom], epsilon/kB [K], mass [amu].
+METHANE = {"sigma": 3.73, "epsilon_K": 148.0, "mass": 16.04}
+# Helium probe for the void fraction (Hirschfelder, Curtiss and Bird).
+HELIUM = {"sigma": 2.576, "epsilon_K": 10.22}
+
+
+def lj_type_table(types=HOST_LJ_TYPES):
+    """Return ``{name: (sigma, epsilon)}`` in atomic units (bohr, Hartree)."""
+    return {k: (s * angstrom, e * boltzmann) for k, (s, e) in types.items()}
+
+
+def type_counts_for(natom, counts=HOST_TYPE_COUNTS):
+    """Split ``natom`` over the types in the ratio of ``counts`` (largest remainder)."""
+    names = list(counts)
+    w = np.array([counts[n] for n in names], dtype=float)
+    exact = natom * w / w.sum()
+    base = np.floor(exact).astype(int)
+    rem = natom - base.sum()
+    order = np.argsort(-(exact - base), kind="stable")
+    base[order[:rem]] += 1
+    return dict(zip(names, base.tolist()))
+
+
+class SyntheticHost(object):
+    """A periodic orthorhombic host cell with typed LJ atoms.
+
+    Attributes mirror what the reference's spherical external-potential path
+    reads from a yaff ``System`` (cmmdft/extpot_calculator.py:199-209):
+    ``pos`` (natom x 3, bohr), ``ffatypes`` (names), ``ffatype_ids``,
+    ``rvecs`` (3 x 3 cell vectors as rows, bohr) and ``ff`` (type name ->
+    (sigma, epsilon) in atomic units).
+    """
+
+    def __init__(self, pos, ffatypes, ffatype_ids, rvecs, ff):
+        self.pos = np.asarray(pos, dtype=np.float64)
+        self.ffatypes = list(ffatypes)
+        self.ffatype_ids = np.asarray(ffatype_ids, dtype=np.int32)
+        self.rvecs = np.asarray(rvecs, dtype=np.float64)
+        self.ff = dict(ff)
+
+    @property
+    def natom(self):
+        return len(self.pos)
+
+    @property
+    def volume(self):
+        return float(abs(np.linalg.det(self.rvecs)))
+
+    def recentred_pos(self):
+        """Positions shifted so their mean is the origin (cmmdft/system.py:70)."""
+        return self.pos - self.pos.sum(axis=0) / len(self.pos)
+
+
+def random_sequential_host(lengths_A, natom, seed, min_sep_A=1.3,
+                           counts=HOST_TYPE_COUNTS, types=HOST_LJ_TYPES,
+                           max_tries=2000000):
+    """Place ``natom`` atoms uniformly in the cell by RSA.
+
+    A trial position is rejected when its nearest-image distance to any
+    accepted atom is below ``min_sep_A``.  Types are a seeded permutation of
+    the counts returned by :func:`type_counts_for`.  Positions are returned in
+    bohr and are not recentred (the host wrapper recentres, as the reference
+    does for checkpoint hosts).
+    """
+    rng = np.random.default_rng(seed)
+    L = np.asarray(lengths_A, dtype=float).reshape(3)
+    accepted = np.zeros((natom, 3))
+    n = 0
+    tries = 0
+    min2 = min_sep_A ** 2
+    while n < natom:
+        tries += 1
+        if tries > max_tries:
+            raise RuntimeError("RSA could not place %d atoms" % natom)
+        trial = rng.uniform(0.0, 1.0, 3) * L
+        if n:
+            d = accepted[:n] - trial
+            d -= L * np.round(d / L)
+            if np.min(np.einsum("ij,ij->i", d, d)) < min2:
+                continue
+        accepted[n] = trial
+        n += 1
+    cnt = type_counts_for(natom, counts)
+    names = list(cnt)
+    ids = np.concatenate([np.full(cnt[k], i, dtype=np.int32) for i, k in enumerate(names)])
+    ids = rng.permutation(ids).astype(np.int32)
+    rvecs = np.diag(L) * angstrom
+    ff = lj_type_table({k: types[k] for k in names})
+    return SyntheticHost(accepted * angstrom, names, ids, rvecs, ff)
+
+
+def cubic_host_276(seed=0):
+    """The 276-atom cubic cell (a = 17.0 angstrom) used at 32^3 and 64^3."""
+    return random_sequential_host((17.0, 17.0, 17.0), 276, seed)
+
+
+def uneven_hosts(nhost=8, seed=2, density_A3=0.056, edge_range=(12.0, 40.0)):
+    """Orthorhombic hosts with edges drawn from U(edge_range), seeded."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(nhost):
+        L = rng.uniform(edge_range[0], edge_range[1], 3)
+        natom = int(round(density_A3 * float(np.prod(L))))
+        out.append(random_sequential_host(tuple(L), natom, seed * 1000 + i))
+    return out
+
+
+def methane_guest_params():
+    """(sigma, epsilon, mass) of the methane guest in atomic units."""
+    return (METHANE["sigma"] * angstrom, METHANE["epsilon_K"] * boltzmann,
+            METHANE["mass"] * amu)

@@ -1,0 +1,182 @@
+/* cmmdft_b200 — C ABI of the B200 (sm_100a) classical-DFT grid solve.
+ *
+ * Every entry point takes plain pointers and sizes.  Pointers named d_* are
+ * CUDA device pointers (FP64 unless stated); `stream` is a cudaStream_t
+ * passed as void*.  All work is stream-ordered; nothing synchronises unless
+ * the function says so.  Every function returns a cmm_status (0 = success).
+ *
+ * Data layout (one "shape group" of `batch` instances on an N1 x N2 x N3
+ * grid, C order, x slowest as in the reference's Grid):
+ *   real field : double [batch][N1][N2][N3]
+ *   spectrum   : double2 [batch][N1][N2][H3], H3 = N3/2 + 1, holding the
+ *                half spectrum of a real field with the y and z frequency
+ *                axes in the plan's digit-reversed order (x natural).  Use
+ *                cmm_spectrum_index() to map positions to frequencies.
+ *
+ * The reference (CmmDFT) is pure Python/numpy; it has no FFI.  Each entry
+ * point below names the reference function whose arithmetic it replaces
+ * (paths inside the reference project).
+ */
+#ifndef CMMDFT_B200_H
+#define CMMDFT_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum cmm_status {
+  CMM_OK = 0,
+  CMM_ERR_ARG = 1,          /* bad argument (null pointer, negative size) */
+  CMM_ERR_SHAPE = 2,        /* grid shape not supported by this build     */
+  CMM_ERR_CUDA = 3,         /* a CUDA runtime call failed                 */
+  CMM_ERR_SMEM = 4,         /* plane or tile does not fit in shared memory */
+  CMM_ERR_NOMEM = 5,        /* allocation of plan tables failed           */
+  CMM_ERR_WORKSPACE = 6,    /* caller workspace too small                 */
+  CMM_ERR_UNSUPPORTED = 7   /* option not implemented                     */
+} cmm_status;
+
+/* Per-instance reduction slots written by the kernels (cmm_stats_finalize). */
+enum {
+  CMM_STAT_N = 0,        /* sum rho                                   */
+  CMM_STAT_IUE = 1,      /* sum |rho - rho_ref|                       */
+  CMM_STAT_NONFIN = 2,   /* count of non-finite rho                   */
+  CMM_STAT_FID = 3,      /* sum rho_reg (ln(L^3 rho_reg) - 1)         */
+  CMM_STAT_FEXT = 4,     /* sum rho V                                 */
+  CMM_STAT_RES2 = 5,     /* sum (G - rho)^2                           */
+  CMM_STAT_PHI = 6,      /* sum Phi (hard-sphere free-energy density) */
+  CMM_STAT_MFA = 7,      /* Parseval sum for the MFA energy           */
+  CMM_STAT_N3MAX = 8,    /* max n3 (unclipped)                        */
+  CMM_STAT_GNONFIN = 9,  /* count of non-finite G                     */
+  CMM_STAT_GRAM0 = 10,   /* sum r_new r_j, j = 0..CMM_MAX_HIST-1      */
+  CMM_NSTAT = 18
+};
+#define CMM_MAX_HIST 8
+
+/* Hard-sphere functional versions (cmmdft/functionals.py:373-377). */
+enum { CMM_FMT = 0, CMM_MFMT = 1, CMM_WBII = 2, CMM_ANTISYM = 8 };
+
+/* Mix-kernel clip modes. */
+enum {
+  CMM_CLIP_NONE = 0,
+  CMM_CLIP_PICARD = 1,     /* rho < 1e-10 angstrom^-3 -> 0   (solver.py:398)      */
+  CMM_CLIP_DENSITY = 2     /* rho < 1e-12 -> 1e-30          (solver.py:146-148)   */
+};
+
+typedef struct cmm_grid cmm_grid;
+
+int cmm_version(void);
+const char* cmm_status_string(int status);
+
+/* Grid plan: twiddle tables, digit-reversal position tables and the k-space
+ * tables of a periodic N1 x N2 x N3 grid spanning the cell `rvecs` (3x3,
+ * rows are cell vectors, bohr).  Replaces the k-grid, scalprod and Lanczos
+ * tables of Grid.__init__ (cmmdft/system.py:232-295).  Allocates the plan's
+ * device tables (the only persistent device memory this library owns). */
+int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_grid** out);
+int cmm_grid_destroy(cmm_grid* grid);
+/* Number of stored frequencies per instance (N1*N2*H3) and H3. */
+int cmm_grid_spectrum_size(const cmm_grid* grid, long long* nspec, int* h3);
+/* Frequency indices (0..N-1 per axis) at each stored position:
+ * k1[N1], k2[N2], k3[H3] (host arrays). */
+int cmm_spectrum_index(const cmm_grid* grid, int* k1, int* k2, int* k3);
+/* Largest batch-independent shared-memory request of the fused plane pass
+ * with `nslot` fields (bytes), for capacity checks. */
+int cmm_plane_smem_bytes(const cmm_grid* grid, int nslot, size_t* bytes);
+
+/* Lennard-Jones external potential with Lorentz-Berthelot mixing, per-axis
+ * minimum image, R = sqrt(r^2 + 1e-16), cut-and-shifted at `cutoff`, summed
+ * over host atoms in file order; then capped: non-finite or > v_cap -> v_cap.
+ * Replaces get_external_potential / lennard_jones
+ * (cmmdft/extpot_calculator.py:156-222) and the capping in
+ * FreeEnergy.add_external_potential (cmmdft/functionals.py:247-251).
+ * d_pos: natom x 3 (recentred), d_type: natom type ids, d_type_sig/eps: per type.
+ * Output d_V: [N1][N2][N3]. */
+int cmm_extpot_lj(const cmm_grid* grid, const double* d_pos, const int* d_type, int natom,
+                  const double* d_type_sig, const double* d_type_eps, int ntype,
+                  double guest_sig, double guest_eps, double cutoff, double v_cap,
+                  double* d_V, void* stream);
+
+/* Unnormalised 3D real-to-half-complex FFT and its inverse in the plan's
+ * spectrum layout (scipy.fft.fftn / ifftn*N as used by Grid.fft/ifft,
+ * cmmdft/system.py:310-332, without the reference's phase factor, which
+ * cancels in every product the solve forms).  `batch` instances. */
+int cmm_rfft3d(const cmm_grid* grid, int batch, const double* d_in, double* d_spec, void* stream);
+int cmm_irfft3d(const cmm_grid* grid, int batch, double* d_spec, double* d_out, void* stream);
+/* (cmm_irfft3d overwrites d_spec with intermediate data.) */
+
+/* Mean-field attraction kernel spectrum: the sampled cut-and-shifted LJ
+ * potential U(r) of MFAFunctional.generate_potential_lj
+ * (cmmdft/functionals.py:878-910), transformed and folded with the Lanczos
+ * factor, the reference's phase exp(i pi scalprod), the cell volume and the
+ * FFT normalisations, then Hermitian-symmetrised, so that
+ * C1_mfa = irfft3d(rho_hat * K) reproduces MFAFunctional.derive
+ * (cmmdft/functionals.py:912-926).  rep = 1 (no tail corrections) or the
+ * supercell repetition (2 -> tailcorrections=True, functionals.py:794-796).
+ * d_work must hold (rep*N1)(rep*N2)(rep*N3) doubles plus the supercell
+ * spectrum; query with d_kst = NULL and work_bytes receiving the size.
+ * Output d_kst: double2 [N1][N2][H3] in the x-DIF/y/z position layout used
+ * by the column passes.  *vdw_a receives 0.5 * integral U (compute_vdw_a). */
+int cmm_mfa_kernel(const cmm_grid* grid, double sigma, double epsilon, double cutoff,
+                   double rmin, double limit_potential, int rep, double* d_kst,
+                   double* d_work, size_t* work_bytes, double* vdw_a, void* stream);
+
+/* Functional pipeline for `batch` densities given their spectra d_rhohat:
+ *   column pass: rho_hat -> analytic FMT weights -> n0, n3, nv2 spectra
+ *   plane pass : inverse, White-Bear/FMT dPhi/dn, forward of 5 fields
+ *   column pass: back-convolution sum w_a dPhi_a / (beta N) + rho_hat * K_mfa
+ * writing d_chat = spectrum of C1 - V (HardSphere.derive + MFA.derive,
+ * cmmdft/functionals.py:489-609, 912-926).  want: bit 0 = C1 spectrum,
+ * bit 1 = free-energy sums (PHI, MFA), bit 2 = n3 maximum.
+ * d_work: 10 spectra of batch instances.  d_part: [batch][CMM_NSTAT][nslot]. */
+int cmm_fmt_c1(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,
+               int version, const double* d_kst, const double* d_rhohat, double* d_chat,
+               double* d_work, double* d_part, int nslot, int want, void* stream);
+
+/* Fused plane pass of one static Picard step (Picard.update_rho_static,
+ * cmmdft/solver.py:392-401, with get_new_rho :128-129):
+ *   C1 = irfft(chat) + V; G = beta exp(-beta C1) f;  RES2 += (G - rho)^2
+ *   rho' = (1-a) rho + a G; rho' < thr -> 0;  writes rho', its spectrum and
+ *   the reductions N, IUE, NONFIN, FID, FEXT of rho'.
+ * d_params: [batch][4] = {fugacity f, a, unused, unused}.  d_V stride vstride. */
+int cmm_picard_static_step(const cmm_grid* grid, int batch, const int* d_active,
+                           const double* d_params, double beta, double lambda3, double thr,
+                           const double* d_chat, const double* d_rho, const double* d_V,
+                           long long vstride, double* d_rho_out, double* d_rhohat_out,
+                           double* d_part, int nslot, void* stream);
+
+/* Residual plane pass (Anderson.update_rho / _save_previous_rhos,
+ * cmmdft/solver.py:527-579): C1 = irfft(chat) + V; G = beta exp(-beta C1) f;
+ * writes r = G - rho to d_r_out; reductions RES2, GNONFIN and the Gram row
+ * sum r * r_j over `nhist` stored residuals d_hist[j] (HOST array of
+ * device pointers, instance stride hstride). */
+int cmm_residual_step(const cmm_grid* grid, int batch, const int* d_active,
+                      const double* d_params, double beta, const double* d_chat,
+                      const double* d_rho, const double* d_V, long long vstride,
+                      double* d_r_out, const double* const* d_hist, int nhist,
+                      long long hstride, double* d_part, int nslot, void* stream);
+
+/* Mix plane pass: rho' = sum_j c[b][j] field_j (up to 12 fields), clipped
+ * (CMM_CLIP_*), written with its spectrum and the reductions N, IUE (against
+ * d_ref), NONFIN, FID, FEXT.  Covers the Picard hybrid trial densities and
+ * mixing (solver.py:403-457) and the Anderson mixing (solver.py:593-598).
+ * thr is the CMM_CLIP_PICARD threshold.  d_coef: [batch][12] (device);
+ * d_fields / fstride: HOST arrays of nfield device pointers / instance strides. */
+int cmm_mix_step(const cmm_grid* grid, int batch, const int* d_active, const double* d_coef,
+                 const double* const* d_fields, const long long* fstride, int nfield,
+                 int clip, double thr, double lambda3, const double* d_ref, long long refstride,
+                 const double* d_V, long long vstride, double* d_rho_out,
+                 double* d_rhohat_out, double* d_part, int nslot, void* stream);
+
+/* Reduce d_part [batch][CMM_NSTAT][nslot] over slots into d_stats
+ * [batch][CMM_NSTAT] for the stats whose bit is set in `mask` (max for
+ * CMM_STAT_N3MAX, sums otherwise). */
+int cmm_stats_finalize(int batch, const int* d_active, const double* d_part, int nslot,
+                       unsigned mask, double* d_stats, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* CMMDFT_B200_H */

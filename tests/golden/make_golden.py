@@ -1,0 +1,215 @@
+"""Generate golden fixtures by running the UNMODIFIED reference package.
+
+Run in the build container only (the reference tree is not present on GPU
+machines):
+
+    python tests/golden/make_golden.py [--reference /root/reference] [--skip64]
+
+The reference is imported from its own source tree through the import shims
+in ``tests/golden/refshim`` (molmod units/constants backed by
+``cmmdft_b200.units``, a minimal yaff ``System``/``Cell``, a matplotlib stub)
+plus the ``np.complex_`` alias that numpy 2 removed.  Hosts are built by
+setting attributes (the shim cannot read yaff checkpoints); the external
+potential is computed by the reference's own ``get_external_potential`` and
+handed to ``FreeEnergy.add_external_potential(load_fn=...)`` so its capping
+code runs too.
+
+Outputs (small ``.npz`` files) land next to this script:
+  c0_32.npz   32^3 cubic host: V, two C1 evaluations, Omega parts,
+              static-Picard trajectory and converged density,
+              tight hybrid-Anderson solution, tail-corrected MFA.
+  c1_64.npz   64^3 cubic host: V summary and tight hybrid-Anderson solutions
+              at three pressures (scalars + one density field).
+"""
+
+import argparse
+import contextlib
+import io
+import os
+import sys
+import tempfile
+import time
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(os.path.dirname(HERE))
+
+
+def import_reference(ref_root):
+    sys.path.insert(0, REPO)
+    sys.path.insert(0, os.path.join(HERE, 'refshim'))
+    sys.path.insert(0, ref_root)
+    if not hasattr(np, 'complex_'):
+        np.complex_ = np.complex128
+    import cmmdft  # noqa: F401
+    from cmmdft import system, functionals, solver, extpot_calculator, eos
+    from cmmdft.log import log as reflog
+    reflog.set_level(0)
+    return system, functionals, solver, extpot_calculator, eos
+
+
+def build(ref, npts, host, T, P_bar, tmp, tail=False):
+    system, functionals, solver, extpot, eos = ref
+    import yaff
+    from cmmdft_b200.units import bar, angstrom
+    from cmmdft_b200.hosts import methane_guest_params
+    sig, eps, mass = methane_guest_params()
+    mol = yaff.System(pos=host.pos.copy(), ffatypes=host.ffatypes,
+                      ffatype_ids=host.ffatype_ids, rvecs=host.rvecs)
+    mol.pos -= mol.pos.sum(axis=0) / len(mol.pos)  # as system.py:70
+    h = system.NanoporousHost.__new__(system.NanoporousHost)
+    system.Host.__init__(h, 'synthetic', mol.cell)
+    h.mol, h.chk, h.par = mol, None, None
+    guest = system.SphericalLJGuest('CH4', mass, sig, eps)
+    syst = system.System(h, guest)
+    grid = system.Grid(mol.cell, npoints=npts)
+    pts = grid.points[..., :3].reshape(-1, 3)
+    t0 = time.time()
+    V = extpot.get_external_potential(pts, host.ff, sig, eps, mol, cutoff=12 * angstrom)
+    t_ext = time.time() - t0
+    fn = os.path.join(tmp, 'epot_%d.npy' % npts)
+    np.save(fn, V.reshape(grid.npoints))
+    fe = functionals.FreeEnergy(grid, syst, T, workdir=tmp, name_dict={}, overwrite=True)
+    fe.add_hard_sphere(version='WBII')
+    fe.add_mean_field(tailcorrections=tail, cutoff=12 * angstrom, rewrite=True)
+    fe.add_external_potential(load_fn=fn)
+    fe.set_temperature(T)  # user flow after adding parts (methane_ZIF8.ipynb)
+    mb = eos.ModifiedBenedictWebbRubinEOS(mass, sig, eps)
+    mu = mb.calculate_mu(T, P_bar * bar)
+    prog = types.SimpleNamespace(grid=grid, fener=fe)
+    return dict(grid=grid, fe=fe, mu=mu, prog=prog, V_raw=V, t_ext=t_ext, mbwr=mb,
+                guest=guest, mol=mol)
+
+
+def omega_parts(ref, b, rho, mu):
+    solver = ref[2]
+    s = solver.Picard(b['prog'], nsteps=1, method='static')
+    s._initiate_solving(mu)
+    krho = b['grid'].fft(rho)
+    parts = [p.value(krho) for p in b['fe'].parts]
+    om = s._get_Omega(rho, krho)
+    derivs = [p.derive(krho) for p in b['fe'].parts]
+    C1 = s._get_C1(rho, krho)
+    return parts, om, derivs, C1
+
+
+def quiet(fn, *a, **k):
+    buf = io.StringIO()
+    with contextlib.redirect_stdout(buf):
+        return fn(*a, **k)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--skip64', action='store_true')
+    args = ap.parse_args()
+    ref = import_reference(args.reference)
+    solver = ref[2]
+    from cmmdft_b200.hosts import cubic_host_276, HELIUM
+    from cmmdft_b200.units import angstrom, boltzmann, bar
+    extpot = ref[3]
+    T = 300.0
+    host = cubic_host_276(seed=0)
+    tmp = tempfile.mkdtemp(prefix='cmm_golden_')
+    out = {}
+    b = quiet(build, ref, 32, host, T, 1.0, tmp)
+    fe, grid, mu = b['fe'], b['grid'], b['mu']
+    out.update(host_pos=host.pos, host_ids=host.ffatype_ids, host_rvecs=host.rvecs,
+               T=T, mu=mu, Rhs=b['guest'].Rhs, wavelength=fe.wavelength, beta=fe.beta,
+               V=fe.part_dict['ExtPot'].potential, V_raw=b['V_raw'].reshape(grid.npoints),
+               mfa_potential=fe.part_dict['MFA'].potential)
+    # bulk density on the lowest branch at mu (calculator.py:129-131)
+    mb = b['mbwr']
+    mb.set_temperature(T)
+    out['rho_bulk'] = np.nanmin(mb.solve_densities_from_chempots([mu]), axis=1)[0]
+    # helium void fraction through the reference's own potential routine
+    Vhe = extpot.get_external_potential(grid.points[..., :3].reshape(-1, 3), host.ff,
+                                        HELIUM['sigma'] * angstrom, HELIUM['epsilon_K'] * boltzmann,
+                                        b['mol'], cutoff=12 * angstrom)
+    out['he_frac'] = grid.integrate(np.clip(np.exp(-Vhe / boltzmann / T), 0, 1)).real / grid.cell.volume
+    # two C1 evaluations: ideal-gas start and a dense liquid-like profile
+    rho_a = np.exp(fe.beta * (mu - out['V'])) / fe.wavelength ** 3
+    rho_b = 0.02 / angstrom ** 3 * np.clip(np.exp(-fe.beta * out['V']), 0, 1)
+    for tag, rho in (('a', rho_a), ('b', rho_b)):
+        parts, om, derivs, C1 = quiet(omega_parts, ref, b, rho, mu)
+        out['rho_' + tag] = rho
+        out['values_' + tag] = np.array(parts)
+        out['omega_' + tag] = om
+        out['dHS_' + tag] = derivs[0]
+        out['dMFA_' + tag] = derivs[1]
+        out['C1_' + tag] = C1
+        out['n3_' + tag] = fe.part_dict['HardSphere'].get_n3(grid.fft(rho))
+    # static Picard trajectory (solver.py:392-401), criterion RES
+    for nst, key in ((3, 'picard3'), (500, 'picard')):
+        s = solver.Picard(b['prog'], nsteps=nst, alpha_mix=0.1, method='static',
+                          criterion='res', threshold=1e-8)
+        N, rho, conv = quiet(s.solve, mu, rho_a.copy(), 3)
+        out[key + '_rho'] = rho
+        out[key + '_N'] = N
+        out[key + '_steps'] = s.curr_step
+        out[key + '_conv'] = conv
+    s = solver.Picard(b['prog'], nsteps=1, method='static')
+    s._initiate_solving(mu)
+    out['picard_omega'] = s._get_Omega(out['picard_rho'], grid.fft(out['picard_rho']))
+    # tight hybrid-Anderson (reference default method) at 1 bar
+    s = solver.Anderson(b['prog'], nsteps=300, m=5, criterion='res', threshold=1e-11)
+    t0 = time.time()
+    N, rho, conv = quiet(s.solve, mu, rho_a.copy(), 3)
+    out['and_time'] = time.time() - t0
+    out.update(and_rho=rho, and_N=N, and_steps=s.curr_step, and_conv=conv)
+    s2 = solver.Picard(b['prog'], nsteps=1, method='static')
+    s2._initiate_solving(mu)
+    out['and_omega'] = s2._get_Omega(rho, grid.fft(rho))
+    # tail-corrected MFA on the 2x2x2 supercell (functionals.py:794-796, 918-923)
+    bt = quiet(build, ref, 32, host, T, 1.0, tempfile.mkdtemp(prefix='cmm_golden_t_'), tail=True)
+    k = grid.fft(rho_b)
+    out['dMFA_tail_b'] = bt['fe'].part_dict['MFA'].derive(k)
+    out['vMFA_tail_b'] = bt['fe'].part_dict['MFA'].value(k)
+    np.savez_compressed(os.path.join(HERE, 'c0_32.npz'), **out)
+    print('wrote c0_32.npz', 'picard steps', out['picard_steps'], 'anderson steps', out['and_steps'])
+
+    if args.skip64:
+        return
+    out = {}
+    pressures = np.array([1e-3, 1.0, 10.0, 100.0])
+    b = quiet(build, ref, 64, host, T, 1.0, tempfile.mkdtemp(prefix='cmm_golden64_'))
+    fe, grid = b['fe'], b['grid']
+    mb = b['mbwr']
+    V = fe.part_dict['ExtPot'].potential
+    Vhe = extpot.get_external_potential(grid.points[..., :3].reshape(-1, 3), host.ff,
+                                        HELIUM['sigma'] * angstrom, HELIUM['epsilon_K'] * boltzmann,
+                                        b['mol'], cutoff=12 * angstrom)
+    he_frac = grid.integrate(np.clip(np.exp(-Vhe / boltzmann / T), 0, 1)).real / grid.cell.volume
+    out.update(T=T, pressures=pressures, V_sum=V.sum(), V_min=V.min(),
+               V_slice=V[:, :, 32].copy(), t_ext=b['t_ext'])
+    mus, Ns, Oms, steps, bulks = [], [], [], [], []
+    for P in pressures:
+        mu = mb.calculate_mu(T, P * bar)
+        mb.set_temperature(T)
+        bulks.append(np.nanmin(mb.solve_densities_from_chempots([mu]), axis=1)[0])
+        # Ninit = rho_bulk start of the reference's example notebook
+        # (program.py:278-287); the ideal-gas default start overflows G at
+        # 100 bar and the reference's hybrid step then fails in np.polyfit.
+        rho0 = bulks[-1] * np.exp(-np.maximum(V, 0) / boltzmann / T)
+        s = solver.Anderson(b['prog'], nsteps=300, m=5, criterion='res', threshold=1e-11)
+        N, rho, conv = quiet(s.solve, mu, rho0, 3)
+        s2 = solver.Picard(b['prog'], nsteps=1, method='static')
+        s2._initiate_solving(mu)
+        Oms.append(s2._get_Omega(rho, grid.fft(rho)))
+        mus.append(mu)
+        Ns.append(N)
+        steps.append(s.curr_step)
+        if P == 1.0:
+            out['rho_1bar'] = rho
+        print('64^3 P=%g bar: N=%.12e steps=%d conv=%s' % (P, N, s.curr_step, conv))
+    out.update(mu=np.array(mus), N=np.array(Ns), omega=np.array(Oms), steps=np.array(steps),
+               rho_bulk=np.array(bulks), he_frac=he_frac)
+    np.savez_compressed(os.path.join(HERE, 'c1_64.npz'), **out)
+    print('wrote c1_64.npz')
+
+
+if __name__ == '__main__':
+    main()

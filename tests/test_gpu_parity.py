@@ -1,0 +1,156 @@
+"""GPU parity: the CUDA path (through the C ABI) against the oracle and the
+reference's golden fixtures.
+
+Tolerances (stated per check):
+  * FFTs against scipy.fft: 1e-13 relative to max |X|.
+  * External potential: 1e-13 relative to the cap (max |V|).
+  * Functional derivatives: beta * max |dC1| below the reference's own noise
+    floor under 1-ulp input perturbations (5e-10 on the ideal-gas profile,
+    1e-7 on the sharp dense profile; see tests/test_oracle_golden.py), and
+    the MFA derivative to 1e-12 relative.
+  * Free-energy parts: 1e-11 relative.
+  * Converged densities: 1e-9 relative to max rho at RES < 1e-11; the
+    loading N and grand potential to 1e-9 relative.
+"""
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+from cmmdft_b200 import _lib as L, engine as E, batch as BT, workload as W
+from cmmdft_b200.hosts import cubic_host_276, methane_guest_params
+from cmmdft_b200.units import angstrom, kjmol, bar
+from tests._common import relerr, scalar_rel, oracle_case
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return True
+
+
+@pytest.fixture(scope="module")
+def fn32(cuda):
+    return W.build_functional(cubic_host_276(0), (32, 32, 32), 300.0, methane_guest_params())
+
+
+@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 20, 18), (30, 28, 14), (16, 12, 10), (7, 9, 22)])
+def test_rfft3d_matches_scipy(cuda, shape):
+    rng = np.random.default_rng(1)
+    x = rng.standard_normal((2,) + shape)
+    rv = np.diag([10.0, 11.0, 12.0])
+    plan = E.GridPlan(shape, rv)
+    xt = torch.as_tensor(x, device="cuda")
+    spec = plan.rfft(xt)
+    full = plan.spec_to_full(spec)
+    ref = np.fft.fftn(x, axes=(1, 2, 3))
+    assert relerr(full.real, ref.real, np.abs(ref).max()) < 1e-13
+    assert relerr(full.imag, ref.imag, np.abs(ref).max()) < 1e-13
+    back = plan.irfft(spec).cpu().numpy() / np.prod(shape)
+    assert relerr(back, x) < 1e-13
+
+
+def test_external_potential(golden32, fn32):
+    V = fn32.V.cpu().numpy()
+    assert relerr(V, golden32["V"]) < 1e-13
+
+
+def _c1(fn, rho_np):
+    plan = fn.plan
+    buf = E.Buffers(plan, 1)
+    buf.part[:, L.STAT_N3MAX, :] = -np.inf
+    rho = torch.as_tensor(rho_np[None], device="cuda")
+    spec = plan.rfft(rho)
+    chat = plan.new_spec(1)
+    fn.c1(buf, spec, chat, want=7)
+    E.finalize(buf, (1 << L.NSTAT) - 1)
+    st = buf.stats.cpu().numpy()[0]
+    C1 = plan.irfft(chat).cpu().numpy()[0]
+    dr = plan.dr
+    return C1, st, (st[L.STAT_PHI] * dr) / fn.beta, 0.5 * st[L.STAT_MFA] * dr
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_functional_derivative(golden32, fn32, tag):
+    rho = golden32["rho_" + tag]
+    C1, st, Fhs, Fmfa = _c1(fn32, rho)
+    ref = golden32["dHS_" + tag] + golden32["dMFA_" + tag]
+    floor = {"a": 5e-10, "b": 1e-7}[tag]
+    dC = fn32.beta * np.abs(C1 - ref)
+    assert dC.max() < floor
+    assert (dC * rho).max() / rho.max() < 1e-9
+    vals = golden32["values_" + tag]
+    assert scalar_rel(Fhs, vals[0]) < 1e-11
+    assert scalar_rel(Fmfa, vals[1]) < 1e-11
+    assert scalar_rel(st[L.STAT_N3MAX], golden32["n3_" + tag].max()) < 1e-12
+
+
+def test_mfa_derivative_alone(golden32, cuda):
+    host = cubic_host_276(0)
+    fn = W.build_functional(host, (32, 32, 32), 300.0, methane_guest_params())
+    rho = golden32["rho_b"]
+    # HS part from the oracle (same rho), MFA part from the GPU: isolate the MFA kernel
+    grid, fe = oracle_case(32, V=golden32["V"])
+    C1, st, Fhs, Fmfa = _c1(fn, rho)
+    dmfa = C1 - fe.part_dict["HardSphere"].derive(grid.fft(rho))
+    assert relerr(dmfa, golden32["dMFA_b"]) < 1e-9
+
+
+def test_mfa_tailcorrections(golden32, cuda):
+    fn = W.build_functional(cubic_host_276(0), (32, 32, 32), 300.0, methane_guest_params(),
+                            tailcorrections=True)
+    rho = golden32["rho_b"]
+    C1, st, Fhs, Fmfa = _c1(fn, rho)
+    assert scalar_rel(Fmfa, golden32["vMFA_tail_b"]) < 1e-11
+
+
+def _solve(fn, mu, rho0, method, thr, nsteps=500):
+    s = BT.BatchSolve(fn, np.atleast_1d(mu), method=method, nsteps=nsteps, threshold=thr, criterion='res')
+    r0 = torch.as_tensor(np.asarray(rho0)[None] if np.ndim(rho0) == 3 else rho0, device="cuda")
+    N, rho, conv = s.solve(r0)
+    return s, N, rho.cpu().numpy(), conv
+
+
+def test_static_picard_matches_reference(golden32, fn32):
+    mu = float(golden32["mu"])
+    s, N, rho, conv = _solve(fn32, mu, golden32["rho_a"], 'static', 1e-8)
+    assert conv[0]
+    assert s.steps[0] == int(golden32["picard_steps"])
+    assert relerr(rho[0], golden32["picard_rho"]) < 1e-10
+    assert scalar_rel(N[0], golden32["picard_N"]) < 1e-10
+
+
+def test_static_picard_three_steps(golden32, fn32):
+    mu = float(golden32["mu"])
+    s, N, rho, conv = _solve(fn32, mu, golden32["rho_a"], 'static', 1e-30, nsteps=3)
+    assert not conv[0]
+    assert relerr(rho[0], golden32["picard3_rho"]) < 1e-12
+
+
+def test_hybrid_anderson_matches_reference(golden32, fn32):
+    mu = float(golden32["mu"])
+    s, N, rho, conv = _solve(fn32, mu, golden32["rho_a"], 'hybridanderson', 1e-11, nsteps=300)
+    assert conv[0]
+    assert relerr(rho[0], golden32["and_rho"]) < 1e-9
+    assert scalar_rel(N[0], golden32["and_N"]) < 1e-9
+
+
+def test_isotherm_64_matches_reference(golden64, cuda):
+    host = cubic_host_276(0)
+    guest = methane_guest_params()
+    fn = W.build_functional(host, (64, 64, 64), 300.0, guest)
+    P = golden64["pressures"]
+    ok = golden64["steps"] < 300  # points the reference itself converged
+    mus, bulks = W.isotherm_inputs(P * bar, 300.0, guest)
+    assert np.allclose(mus, golden64["mu"], rtol=1e-13, atol=0)
+    r0 = W.initial_density(fn, mus, ninit=bulks)
+    s = BT.BatchSolve(fn, mus, method='hybridanderson', nsteps=300, threshold=1e-11, criterion='res')
+    N, rho, conv = s.solve(r0)
+    assert conv[ok].all()
+    for i in np.where(ok)[0]:
+        assert scalar_rel(N[i], golden64["N"][i]) < 1e-9
+    i1 = int(np.where(P == 1.0)[0][0])
+    assert relerr(rho[i1].cpu().numpy(), golden64["rho_1bar"]) < 1e-9
