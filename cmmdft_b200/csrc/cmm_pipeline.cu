@@ -238,7 +238,7 @@ __device__ inline void store_col_tile(const GridDev& g, const ColSmem& s, int sl
 }
 
 __device__ inline void col_fft(const GridDev& g, const ColSmem& s, int nslot, int tc, bool inv) {
-  PencilSet ps = {nslot * tc, nslot * tc, 0, 1, tc, true};
+  PencilSet ps = {nslot * tc, tc, g.n1 * tc, 1, tc, true};
   if (inv) fft_pencils<true>(s.slots, g.ax1, s.tw1, 1, ps);
   else fft_pencils<false>(s.slots, g.ax1, s.tw1, 1, ps);
 }
