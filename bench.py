@@ -1,0 +1,349 @@
+"""Benchmark: converged isotherm points per second at 64^3 FP64.
+
+Workload (the 64^3 configuration): the 276-atom cubic host (a = 17 A, seeded
+random sequential addition, C:H:N:Zn = 96:120:48:12), united-atom methane,
+T = 300 K, WBII + MFA + LJ external potential, 24 pressures log-spaced from
+1e-3 to 100 bar, hybrid-Anderson (m = 5) to RES < 1e-8, started from
+Ninit = rho_bulk (the reference notebook's start).  One step = one batched
+solve of the whole isotherm.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference] [--no-plain]
+
+Prints one JSON line (rank 0).  `value` is device-resident throughput (the
+functional and initial densities already on the GPU); `e2e` goes through the
+public entry point solve_isotherm from host arrays (host atoms in, loadings
+and densities out).  `--impl reference` times the numpy restatement of the
+reference path (pinned against the reference) on the host cores.
+Multi-GPU runs are replicas: every rank solves its own isotherm (weak scaling).
+"""
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+NPTS = (64, 64, 64)
+NPRESS = 24
+T = 300.0
+THRESH = 1e-8
+METRIC = "isotherm converged points/s at 64^3 FP64 (hybrid Anderson m=5, RES<1e-8)"
+
+
+def peaks():
+    try:
+        return json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))
+    except Exception:
+        return {"hbm_gbs": 6650.0, "_fallback": True}
+
+
+class ClockSampler(object):
+    """nvidia-smi samples of the SM clock and throttle reasons during the timed region."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.index), "--query-gpu=" + q,
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [x.strip() for x in line.split(",")]
+            if len(parts) >= 7:
+                self.samples.append(parts)
+
+    def __exit__(self, *a):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace('.', '').isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace('.', '').isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[3 + i].lower() == "active"})
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(self.samples)}
+
+
+def pipeline_bytes(plan, want, n_active):
+    """Algorithmic HBM bytes of one functional-pipeline launch (3 kernels).
+
+    S = one yz-spectrum of one instance (N1*N2*H3*16 B).  Column pass 1 reads
+    rho_hat and writes 5 weighted-density spectra; the plane pass reads 5 and
+    writes 5 dPhi spectra; column pass 2 reads 5 + rho_hat and writes the C1
+    spectrum.  The MFA kernel spectrum (S) is read once per launch per pass
+    that uses it.  Value-only launches (want & 1 == 0) skip the forward and the
+    second column pass.
+    """
+    S = plan.nspec * 16
+    if want & 1:
+        per = S * (1 + 5 + 5 + 5 + 5 + 1 + 1)
+        shared = S * (2 if want & 2 else 1)
+    else:
+        per = S * (1 + 5 + 5)
+        shared = S if want & 2 else 0
+    return per * n_active + shared
+
+
+def setup_case(torch):
+    from cmmdft_b200 import workload as W
+    from cmmdft_b200.hosts import cubic_host_276, methane_guest_params
+    from cmmdft_b200.units import bar
+    host = cubic_host_276(0)
+    guest = methane_guest_params()
+    pressures = np.logspace(-3, 2, NPRESS) * bar
+    fn = W.build_functional(host, NPTS, T, guest)
+    mus, bulks = W.isotherm_inputs(pressures, T, guest)
+    return host, guest, pressures, fn, mus, bulks
+
+
+def run_gpu(args):
+    import torch
+    import torch.distributed as dist
+    from cmmdft_b200 import batch as BT, workload as W, isotherm as ISO
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300))
+
+    host, guest, pressures, fn, mus, bulks = setup_case(torch)
+    rho0 = W.initial_density(fn, mus, ninit=bulks)
+
+    def one_solve(events=None):
+        s = BT.BatchSolve(fn, mus, method="hybridanderson", nsteps=500, threshold=THRESH, criterion="res")
+        s.pipeline_events = events
+        N, rho, conv = s.solve(rho0)
+        return s, conv
+
+    def barrier():
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+
+    for _ in range(args.warmup):
+        one_solve()
+    events = []
+    launches = 0
+    nconv = 0
+    iters = []
+    barrier()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record()
+        for _ in range(args.steps):
+            s, conv = one_solve(events)
+            launches += s.kernel_launches
+            nconv += int(conv.sum())
+            iters.append(int(s.steps.sum()))
+        e1.record()
+        barrier()
+    ms = e0.elapsed_time(e1)
+    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        nc = torch.tensor([nconv], dtype=torch.float64, device="cuda")
+        dist.all_reduce(nc)
+        nconv_all = float(nc.item())
+    else:
+        nconv_all = float(nconv)
+    ms_max = float(t.item())
+    value = nconv_all / (ms_max / 1e3)
+
+    # roofline of the fused functional pipeline, from its events in the timed region
+    tot_bytes = 0.0
+    tot_ms = 0.0
+    for a, b, want, nact in events:
+        tot_ms += a.elapsed_time(b)
+        tot_bytes += pipeline_bytes(fn.plan, want, nact)
+    pk = peaks()
+    achieved = tot_bytes / (tot_ms / 1e3) / 1e9 if tot_ms > 0 else None
+    roofline = {"bound": "hbm", "kernel": "functional pipeline (k_col_weights+k_plane_fmt+k_col_backconv)",
+                "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
+                "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
+                "peak_source": "fallback" if pk.get("_fallback") else "measured",
+                "traffic": None, "launches": len(events),
+                "bytes_per_launch": tot_bytes / max(len(events), 1),
+                "ms_per_launch": tot_ms / max(len(events), 1),
+                "share_of_step": tot_ms / ms_max if ms_max else None}
+
+    # end to end through the public entry point (host arrays in, loadings + densities out)
+    e2e = None
+    if not args.no_e2e:
+        barrier()
+        t0 = time.perf_counter()
+        h2d = d2h = 0
+        ne = 0
+        for _ in range(max(1, args.steps // 2)):
+            out = ISO.solve_isotherm(host, pressures, T, guest, NPTS, threshold=THRESH)
+            ne += int(out["converged"].sum())
+            h2d += host.pos.nbytes + host.ffatype_ids.nbytes + 2 * 8 * len(host.ffatypes)
+            d2h += out["rho"].nbytes + out["N"].nbytes
+        barrier()
+        dt = time.perf_counter() - t0
+        nsteps_e2e = max(1, args.steps // 2)
+        e2e = {"value": ne / dt, "unit": "points/s", "h2d_bytes_per_step": h2d // nsteps_e2e,
+               "d2h_bytes_per_step": d2h // nsteps_e2e, "includes": "extpot + MFA kernel + solve + D2H densities"}
+
+    plain = None
+    if not args.no_plain and rank == 0:
+        barrier()
+        t0 = time.perf_counter()
+        npl = 0
+        pit = 0
+        for i in range(NPRESS):
+            s = BT.BatchSolve(fn, mus[i:i + 1], method="hybridanderson", nsteps=500, threshold=THRESH,
+                              criterion="res")
+            N, rho, conv = s.solve(rho0[i:i + 1])
+            npl += int(conv.sum())
+            pit += int(s.steps.sum())
+        torch.cuda.synchronize()
+        dtp = time.perf_counter() - t0
+        plain = {"value": npl / dtp, "unit": "points/s", "iterations": pit,
+                 "batched_over_plain": value / (npl / dtp) / max(world, 1)}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        cpu = cpu_baseline_sample(one_point=True)
+
+    if world > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank != 0:
+        return
+    line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "isotherm-64cubed", "grid": list(NPTS), "host": "cubic a=17A 276 atoms seed 0",
+                       "points_per_isotherm": NPRESS, "pressures_bar": [1e-3, 100.0], "solver": "hybridanderson m=5",
+                       "tolerance": "RES<1e-8", "start": "Ninit=rho_bulk", "iterations_per_isotherm": iters,
+                       "converged_points": nconv, "parallelism": "replicas" if world > 1 else "single",
+                       "l2": "working set > L2 (24 x 2 MiB fields x ~30 live buffers)"},
+            "roofline": roofline, "cpu_baseline": cpu, "e2e": e2e, "plain": plain,
+            "gpu_launches": launches, "clocks": clk.summary()}
+    print(json.dumps(line))
+
+
+# ------------------------------------------------------------- CPU sides --
+def _oracle_point(args):
+    """One reference-path (numpy oracle) hybrid-Anderson solve at 64^3; returns (seconds, N, converged)."""
+    idx, = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    sys.path.insert(0, ROOT)
+    from oracle import cmm_oracle as O
+    from cmmdft_b200.hosts import cubic_host_276, methane_guest_params
+    from cmmdft_b200.units import bar, kjmol
+    host = cubic_host_276(0)
+    sig, eps, mass = methane_guest_params()
+    grid = O.OGrid(host.rvecs, npoints=list(NPTS))
+    V = O.external_potential(grid.points[..., :3].reshape(-1, 3), host.ff, sig, eps, host.recentred_pos(),
+                             host.ffatypes, host.ffatype_ids, host.rvecs).reshape(grid.npoints)
+    V = O.cap_potential(V, 1e4 * kjmol)
+    fe = O.build_functional(grid, sig, eps, mass, T, V)
+    P = np.logspace(-3, 2, NPRESS)[idx] * bar
+    mb = O.MBWR(mass, sig, eps)
+    mu = O.eos_calculate_mu(mb, T, P)
+    mb.set_temperature(T)
+    rb = np.nanmin(O.eos_densities_from_chempots(mb, [mu]), axis=1)[0]
+    rho0 = rb * np.exp(-np.maximum(V, 0) / (1.0 / fe.beta))
+    t0 = time.perf_counter()
+    s = O.Anderson(fe, nsteps=500, m=5, criterion="res", threshold=THRESH)
+    N, rho, conv = s.solve(mu, rho0)
+    return time.perf_counter() - t0, float(N), bool(conv), s.curr_step
+
+
+def cpu_baseline_sample(one_point=True, nproc=1, points=None):
+    """Time the numpy restatement of the reference path on host cores (spawned workers)."""
+    import multiprocessing as mp
+    if points is None:
+        points = [NPRESS // 2]
+    ctx = mp.get_context("spawn")
+    t0 = time.perf_counter()
+    with ctx.Pool(nproc) as pool:
+        res = pool.map(_oracle_point, [(i,) for i in points])
+    wall = time.perf_counter() - t0
+    solve_s = sum(r[0] for r in res)
+    nconv = sum(1 for r in res if r[2])
+    return {"value": nconv / wall if nproc > 1 else nconv / solve_s, "unit": "points/s", "cores": nproc,
+            "kind": "port",
+            "sample": "%d pressure point(s) %s of the 24-point 64^3 isotherm, numpy/scipy oracle "
+                      "(pinned to the reference), scipy.fft workers=1, %d process(es); solve time only"
+                      % (len(points), points, nproc),
+            "iterations": [r[3] for r in res]}
+
+
+def run_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    try:
+        ncores = len(os.sched_getaffinity(0))
+    except Exception:
+        ncores = os.cpu_count() or 1
+    nproc = max(1, min(ncores, 8))
+    steps = max(1, min(args.steps, 2))
+    vals = []
+    cb = None
+    t_all = time.perf_counter()
+    for k in range(steps):
+        pts = [(k * nproc + i) % NPRESS for i in range(nproc)]
+        cb = cpu_baseline_sample(nproc=nproc, points=pts)
+        vals.append(cb["value"])
+    value = float(np.mean(vals))
+    line = {"metric": METRIC, "value": value, "unit": "points/s", "n_gpus": 0, "steps": steps, "warmup": 0,
+            "ms_per_step": (time.perf_counter() - t_all) / steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "impl": "reference",
+            "config": {"workload": "isotherm-64cubed", "grid": list(NPTS), "solver": "hybridanderson m=5",
+                       "tolerance": "RES<1e-8"},
+            "cpu_baseline": dict(cb, value=value),
+            "e2e": {"value": value, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == "__main__":
+    main()

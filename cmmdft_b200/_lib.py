@@ -15,7 +15,7 @@ STAT_N, STAT_IUE, STAT_NONFIN, STAT_FID, STAT_FEXT, STAT_RES2, STAT_PHI, STAT_MF
 NSTAT = 18
 MAX_HIST = 8
 MAX_FIELDS = 12
-FMT, MFMT, WBII, ANTISYM = 0, 1, 2, 8
+FMT, MFMT, WBII, ANTISYM, NOHS = 0, 1, 2, 8, 16
 CLIP_NONE, CLIP_PICARD, CLIP_DENSITY = 0, 1, 2
 
 
@@ -40,6 +40,8 @@ _SIGS = {
                        c_double, c_double, c_void_p, c_void_p], c_int),
     "cmm_rfft3d": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
     "cmm_irfft3d": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
+    "cmm_rfft_yz": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
+    "cmm_irfft_yz": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
     "cmm_mfa_kernel": ([c_void_p, c_double, c_double, c_double, c_double, c_double, c_int, c_void_p,
                         c_void_p, P(ctypes.c_size_t), P(c_double), c_void_p], c_int),
     "cmm_fmt_c1": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p,

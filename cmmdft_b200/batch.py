@@ -129,6 +129,9 @@ class BatchSolve(object):
         self.mask_host = np.zeros(B, dtype=bool)
         self.kernel_launches = 0
         self.omega_evals = 0
+        # optional timing of the functional pipeline: list of
+        # (start_event, end_event, want, n_active) appended per launch
+        self.pipeline_events = None
 
     # ------------------------------------------------------------ helpers --
     def _set_active(self, mask):
@@ -150,7 +153,15 @@ class BatchSolve(object):
         self.kernel_launches += 1
 
     def _c1(self, spec, chat, want):
+        ev = self.pipeline_events
+        if ev is not None:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            e0.record()
         self.fn.c1(self.buf, spec, chat, want=want, active=self.active)
+        if ev is not None:
+            e1.record()
+            ev.append((e0, e1, want, int(self.mask_host.sum())))
         self.kernel_launches += 3 if (want & 1) else 2
 
     def _residual(self, chat, rho, r_out, hist):

@@ -363,10 +363,19 @@ k_col_backconv(GridDev g, const int* __restrict__ active, double R, double scale
   const int b = blockIdx.y, c0 = blockIdx.x * tc;
   if (active && !active[b]) return;
   ColSmem s = col_smem_setup(g, 6, tc);
-  for (int f = 0; f < 5; ++f) load_col_tile(g, s, f, gin + f * fsg, b, c0, tc);
+  const bool hs = (gin != nullptr);
+  if (hs)
+    for (int f = 0; f < 5; ++f) load_col_tile(g, s, f, gin + f * fsg, b, c0, tc);
   load_col_tile(g, s, 5, rhohat, b, c0, tc);
   __syncthreads();
-  col_fft(g, s, 6, tc, false);
+  if (hs) {
+    col_fft(g, s, 6, tc, false);
+  } else {
+    // only the rho_hat slot: transform it alone (slot 5 viewed as slot 0 of a shifted base)
+    ColSmem s5 = s;
+    s5.slots = s.slots + (size_t)5 * g.n1 * tc;
+    col_fft(g, s5, 1, tc, false);
+  }
   const int nc = g.n2 * g.h3;
   const size_t per = (size_t)g.n1 * tc;
   for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
@@ -374,14 +383,17 @@ k_col_backconv(GridDev g, const int* __restrict__ active, double R, double scale
     const int col = c0 + c;
     if (col >= nc) continue;
     const int p2 = col / g.h3, p3 = col - p2 * g.h3;
-    const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];
-    Weights w = fmt_weights(g.kp1[p1], g.kp2[p2], g.kp3[p3], sl, R, g.nq1[p1], g.nq2[p2], g.nq3[p3]);
-    double2 acc = cadd(cscale(s.slots[i], w.w0), cscale(s.slots[per + i], w.w3));
-    // - sum_j G_j * (-i v_j) = + i * sum_j v_j G_j
-    double2 gv = make_double2(0.0, 0.0);
-    for (int a = 0; a < 3; ++a) gv = cadd(gv, cscale(s.slots[(2 + a) * per + i], w.v[a]));
-    acc = cadd(acc, make_double2(-gv.y, gv.x));
-    acc = cscale(acc, scale);
+    double2 acc = make_double2(0.0, 0.0);
+    if (hs) {
+      const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];
+      Weights w = fmt_weights(g.kp1[p1], g.kp2[p2], g.kp3[p3], sl, R, g.nq1[p1], g.nq2[p2], g.nq3[p3]);
+      acc = cadd(cscale(s.slots[i], w.w0), cscale(s.slots[per + i], w.w3));
+      // - sum_j G_j * (-i v_j) = + i * sum_j v_j G_j
+      double2 gv = make_double2(0.0, 0.0);
+      for (int a = 0; a < 3; ++a) gv = cadd(gv, cscale(s.slots[(2 + a) * per + i], w.v[a]));
+      acc = cadd(acc, make_double2(-gv.y, gv.x));
+      acc = cscale(acc, scale);
+    }
     double2 K = __ldg(kst + (size_t)p1 * nc + col);
     acc = cadd(acc, cmul(s.slots[5 * per + i], K));
     s.slots[i] = acc;
@@ -752,6 +764,24 @@ extern "C" int cmm_irfft3d(const cmm_grid* g, int batch, double* d_spec, double*
   return last_err();
 }
 
+extern "C" int cmm_rfft_yz(const cmm_grid* g, int batch, const double* d_in, double* d_spec, void* stream) {
+  if (!g || !d_in || !d_spec || batch < 1) return CMM_ERR_ARG;
+  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  int rc = set_smem((const void*)k_plane_r2c, ps);
+  if (rc) return rc;
+  k_plane_r2c<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(g->dev, d_in, (double2*)d_spec);
+  return last_err();
+}
+
+extern "C" int cmm_irfft_yz(const cmm_grid* g, int batch, const double* d_spec, double* d_out, void* stream) {
+  if (!g || !d_spec || !d_out || batch < 1) return CMM_ERR_ARG;
+  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  int rc = set_smem((const void*)k_plane_c2r, ps);
+  if (rc) return rc;
+  k_plane_c2r<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(g->dev, (const double2*)d_spec, d_out);
+  return last_err();
+}
+
 extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, double R, double beta,
                           int version, const double* d_kst, const double* d_rhohat, double* d_chat,
                           double* d_work, double* d_part, int nslot, int want, void* stream) {
@@ -766,7 +796,17 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
   int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
   if (nslot < g->n1 || nslot < ntile) return CMM_ERR_WORKSPACE;
   size_t cs5 = col_smem_bytes(g->n1, tc, 5), cs6 = col_smem_bytes(g->n1, tc, 6);
-  int rc = set_smem((const void*)k_col_weights, cs5);
+  int rc;
+  if (version & CMM_NOHS) {  // MFA term alone: one column pass
+    if (!(want & 1)) return CMM_ERR_ARG;
+    rc = set_smem((const void*)k_col_backconv, cs6);
+    if (rc) return rc;
+    k_col_backconv<<<dim3(ntile, batch), CMM_COL_THREADS, cs6, st>>>(
+        g->dev, d_active, R, 1.0 / (beta * npts), nullptr, fs, (const double2*)d_rhohat,
+        (const double2*)d_kst, (double2*)d_chat, tc);
+    return last_err();
+  }
+  rc = set_smem((const void*)k_col_weights, cs5);
   if (rc) return rc;
   k_col_weights<<<dim3(ntile, batch), CMM_COL_THREADS, cs5, st>>>(
       g->dev, d_active, R, 1.0 / npts, (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst,

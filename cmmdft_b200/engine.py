@@ -82,6 +82,20 @@ class GridPlan(object):
         check(self.lib.cmm_irfft3d(self.handle, B, ptr(s), ptr(out), _stream()), "cmm_irfft3d")
         return out
 
+    def rfft_yz(self, x):
+        """yz-spectrum (x real, y/z half spectrum) of real fields [B, N1, N2, N3]."""
+        x = x.contiguous()
+        out = self.new_spec(x.shape[0])
+        check(self.lib.cmm_rfft_yz(self.handle, x.shape[0], ptr(x), ptr(out), _stream()), "cmm_rfft_yz")
+        return out
+
+    def irfft_yz(self, spec):
+        """Real fields from yz-spectra (unnormalised inverse of :meth:`rfft_yz`)."""
+        B = spec.shape[0]
+        out = torch.empty((B,) + self.npoints, dtype=torch.float64, device="cuda")
+        check(self.lib.cmm_irfft_yz(self.handle, B, ptr(spec), ptr(out), _stream()), "cmm_irfft_yz")
+        return out
+
     def spec_to_full(self, spec):
         """Full numpy spectrum [B, N1, N2, N3] (scipy fftn order) from a plan-layout spectrum."""
         n1, n2, n3 = self.npoints

@@ -1,0 +1,333 @@
+"""Free-energy functional parts, mirroring cmmdft/functionals.py.
+
+FreeEnergy keeps the reference's part list and add_* methods; the parts
+expose derive(krho) / value(krho) like the reference (functionals.py:365-373)
+with krho the Spectrum returned by Grid.fft.  Every evaluation runs on the
+GPU through the C ABI; the solver uses the fused pipeline of all parts at once
+(``FreeEnergy.device()``).
+
+Built: HardSphere (FMT, MFMT, WBII and their antisymmetric 'a' variants),
+MFA (with or without supercell tail corrections) and ExtPot (spherical LJ
+guests).  Not built in this package: the tensor 't' FMT variants, the WDA /
+LDA correlation parts and non-spherical guests; asking for them raises
+NotImplementedError.
+"""
+import os
+from pathlib import Path
+
+import numpy as np
+
+from . import _lib as L
+from . import engine as E
+from .system import Spectrum
+from .units import angstrom, kjmol, boltzmann
+from .workload import hs_version_code
+
+__all__ = ['FreeEnergy', 'Functional', 'HardSphereFunctional', 'MFAFunctional', 'ExternalPotential']
+
+
+def _torch():
+    import torch
+    return torch
+
+
+class Functional(object):
+    name = None
+
+    def copy(self, **kwargs):
+        raise NotImplementedError
+
+    def set_temperature(self, temperature, **kwargs):
+        pass
+
+
+class FreeEnergy(object):
+    """Container of functional parts (cmmdft/functionals.py:25-174)."""
+
+    def __init__(self, grid, system, temperature, workdir='.', name_dict={}, overwrite=False):
+        self.grid = grid
+        self.system = system
+        self.temperature = None
+        self.beta = None
+        self.wavelength = None
+        self.parts = []
+        self.part_names = []
+        self.part_dict = {}
+        self.workdir = Path(workdir)
+        self.name_dict = name_dict
+        self.overwrite = overwrite
+        self.fn_tracking = None
+        self._device = None
+        self.set_temperature(temperature)
+
+    def set_temperature(self, temperature, **kwargs):
+        self.temperature = temperature
+        self.beta = 1.0 / (boltzmann * temperature)
+        self.wavelength = self.system.guest.wavelength(temperature)
+        self.system.guest.compute_hardsphere_radius(temperature, **kwargs)
+        for p in self.parts:
+            p.set_temperature(temperature, Rhs=self.system.guest.Rhs, **kwargs)
+        self._device = None
+
+    def add_part(self, part):
+        self.parts.append(part)
+        self.part_names.append(part.name)
+        self.part_dict[part.name] = part
+        self._device = None
+
+    def remove_part(self, part_name):
+        i = self.part_names.index(part_name)
+        self.parts.pop(i)
+        self.part_names.pop(i)
+        self.part_dict.pop(part_name, None)
+        self._device = None
+
+    def add_hard_sphere(self, version='atWBII'):
+        hs = HardSphereFunctional(self.grid, self.system.guest.Rhs, version=version)
+        hs.set_temperature(self.temperature, Rhs=self.system.guest.Rhs)
+        self.add_part(hs)
+
+    def add_mean_field(self, tailcorrections=False, repetitions=[2, 2, 2], cutoff=12 * angstrom, **kwargs):
+        g = self.system.guest
+        mfa = MFAFunctional(self.grid, tailcorrections=tailcorrections, repetitions=repetitions)
+        mfa.generate_potential_lj(g.sigma, g.epsilon, cutoff=cutoff, **kwargs)
+        self.add_part(mfa)
+
+    def add_external_potential(self, temperature=None, cutoff=12 * angstrom, limit_potential=1e4 * kjmol,
+                               degree=9, interpolate=False, rewrite=False, load_fn=None, save_fn=None, **kwargs):
+        ep = ExternalPotential(self.grid, self.system, None, limit_potential=limit_potential, cutoff=cutoff)
+        if load_fn is not None:
+            ep.load_potential(load_fn)
+        else:
+            ep.generate_potential(temperature)
+            if save_fn is not None:
+                ep.dump_potential(save_fn)
+        ep.cap()
+        self.add_part(ep)
+
+    def add_correlation_wda_lj(self, **kwargs):
+        raise NotImplementedError("the WDA correlation part is not built in this package")
+
+    def add_lda(self, eos):
+        raise NotImplementedError("the LDA part is not built in this package")
+
+    def add_wdav(self, eos, **kwargs):
+        raise NotImplementedError("the WDA part is not built in this package")
+
+    # ---- device functional used by the solvers
+    def device(self):
+        """engine.Functional combining the parts (HardSphere [+ MFA] [+ ExtPot])."""
+        if self._device is not None:
+            return self._device
+        names = self.part_names
+        for n in names:
+            if n not in ('HardSphere', 'MFA', 'ExtPot'):
+                raise NotImplementedError("part %r has no GPU path" % n)
+        if 'HardSphere' not in names:
+            raise NotImplementedError("the fused solve needs a HardSphere part")
+        hs = self.part_dict['HardSphere']
+        plan = self.grid.plan
+        torch = _torch()
+        V = self.part_dict['ExtPot'].potential_device() if 'ExtPot' in names else \
+            torch.zeros(plan.npoints, dtype=torch.float64, device='cuda')
+        kst = self.part_dict['MFA'].kst if 'MFA' in names else None
+        a = self.part_dict['MFA'].vdw_a if 'MFA' in names else None
+        self._device = E.Functional(plan, hs.R, self.beta, self.wavelength, V, hs_version_code(hs.version), kst, a)
+        return self._device
+
+    def init_tracking(self, fn, rewrite=False):
+        self.fn_tracking = fn
+        if not os.path.isfile(fn) or self.overwrite or rewrite:
+            with open(fn, 'w') as f:
+                print("#phase\tstep\t     loading\t         -muN\t        IdGas\t" +
+                      "\t".join("%13s" % p.name for p in self.parts) + "\t        Total", file=f)
+
+    def track(self, chempot, rho, krho=None, iphase=0, write=True, print_out=False, fn=None, unit=1):
+        """Grand potential of rho with its parts (cmmdft/functionals.py:121-174)."""
+        g = self.grid
+        rho_np = rho if not hasattr(rho, 'detach') else rho.detach().cpu().numpy()
+        N = g.integrate(rho_np)
+        rr = np.where(rho_np <= 0 + np.isclose(rho_np, 0), 1e-30, rho_np)
+        Fid = g.integrate(rr * (np.log(self.wavelength ** 3 * rr) - 1.0)) / self.beta
+        G = Fid - chempot * N
+        if krho is None:
+            krho = g.fft(rho_np)
+        vals = [p.value(krho) for p in self.parts]
+        G += sum(vals)
+        if write and (fn or self.fn_tracking):
+            with open(fn or self.fn_tracking, 'a') as f:
+                print("%6i\t%4i\t%.6e\t%.6e\t% .6e\t" % (iphase, 0, N, -chempot * N / unit, Fid / unit) +
+                      "\t".join("% .6e" % (v / unit) for v in vals) + "\t% .6e" % (G / unit), file=f)
+        return G
+
+
+def _stats_of(plan, buf):
+    E.finalize(buf, (1 << L.NSTAT) - 1)
+    return buf.stats.cpu().numpy()[0]
+
+
+class HardSphereFunctional(Functional):
+    """Hard-sphere FMT part (cmmdft/functionals.py:375-618)."""
+    name = 'HardSphere'
+
+    def __init__(self, grid, Rhs, version='atWBII'):
+        self.grid = grid
+        self.R = Rhs
+        self.version = version
+        self.code = hs_version_code(version)
+        self.temperature = None
+        self.beta = None
+
+    def copy(self, grid=None):
+        return type(self)(grid or self.grid.copy(), self.R, self.version)
+
+    def set_temperature(self, temperature, Rhs=None, **kwargs):
+        self.temperature = temperature
+        self.beta = 1 / (boltzmann * temperature)
+        if Rhs is not None:
+            self.R = Rhs
+
+    def _functional(self):
+        torch = _torch()
+        plan = self.grid.plan
+        return E.Functional(plan, self.R, self.beta, 1.0, torch.zeros(plan.npoints, dtype=torch.float64,
+                                                                       device='cuda'), self.code)
+
+    def _run(self, krho, want):
+        krho = self.grid.as_spectrum(krho)
+        fn = self._functional()
+        buf = E.Buffers(fn.plan, 1)
+        buf.part[:, L.STAT_N3MAX, :] = -np.inf
+        chat = fn.plan.new_spec(1) if want & 1 else None
+        fn.c1(buf, krho.data, chat, want=want)
+        return fn, buf, chat
+
+    def derive(self, krho):
+        """dF_HS/drho (Hartree) as a numpy field."""
+        fn, buf, chat = self._run(krho, 1)
+        return fn.plan.irfft_yz(chat)[0].cpu().numpy()
+
+    def value(self, krho, local=False):
+        if local:
+            raise NotImplementedError("local hard-sphere free-energy density is not exposed")
+        fn, buf, chat = self._run(krho, 2)
+        st = _stats_of(fn.plan, buf)
+        return (st[L.STAT_PHI] * self.grid.dr) / self.beta
+
+    def get_n3(self, krho):
+        raise NotImplementedError("the n3 field is not exposed; max n3 is a solver reduction")
+
+
+class MFAFunctional(Functional):
+    """Mean-field attraction part (cmmdft/functionals.py:770-939)."""
+    name = 'MFA'
+
+    def __init__(self, grid, tailcorrections=False, repetitions=[2, 2, 2]):
+        self.grid = grid
+        self.tailcorrections = tailcorrections
+        self.repetitions = list(repetitions)
+        if tailcorrections and len(set(self.repetitions)) != 1:
+            raise NotImplementedError("tail corrections need equal repetitions per axis")
+        self.kst = None
+        self.vdw_a = None
+        self.params = None
+
+    def copy(self, grid=None):
+        m = type(self)(grid or self.grid.copy(), self.tailcorrections, self.repetitions)
+        m.kst, m.vdw_a, m.params = self.kst, self.vdw_a, self.params
+        return m
+
+    def generate_potential_lj(self, sigma, epsilon, rmin=None, limit_potential=0, cutoff=None, **kwargs):
+        rep = self.repetitions[0] if self.tailcorrections else 1
+        self.kst, self.vdw_a = E.mfa_kernel_spectrum(self.grid.plan, sigma, epsilon, cutoff, rmin=rmin,
+                                                     limit=limit_potential, rep=rep)
+        self.params = dict(sigma=sigma, epsilon=epsilon, rmin=rmin, limit=limit_potential, cutoff=cutoff)
+
+    def compute_vdw_a(self):
+        self.a = self.vdw_a
+        return self.a
+
+    def derive(self, krho):
+        krho = self.grid.as_spectrum(krho)
+        torch = _torch()
+        plan = self.grid.plan
+        fn = E.Functional(plan, 1.0, 1.0, 1.0, torch.zeros(plan.npoints, dtype=torch.float64, device='cuda'),
+                          L.NOHS, self.kst)
+        buf = E.Buffers(plan, 1)
+        chat = plan.new_spec(1)
+        fn.c1(buf, krho.data, chat, want=1)
+        return plan.irfft_yz(chat)[0].cpu().numpy()
+
+    def value(self, krho, local=False):
+        rho = self.grid.ifft(krho)
+        d = self.derive(krho)
+        if local:
+            return 0.5 * rho * d
+        return 0.5 * self.grid.integrate(rho * d)
+
+
+class ExternalPotential(Functional):
+    """External potential part (cmmdft/functionals.py:941-1083)."""
+    name = 'ExtPot'
+
+    def __init__(self, grid, system, epot_dr=None, limit_potential=1e4 * kjmol, degree=9, interpolate=False,
+                 cutoff=12 * angstrom):
+        self.grid = grid
+        self.system = system
+        self.host = system.host
+        self.guest = system.guest
+        self.epot_dr = epot_dr
+        self.limit_potential = limit_potential
+        self.cutoff = cutoff
+        self._V = None
+
+    def copy(self, grid=None):
+        e = type(self)(grid or self.grid.copy(), self.system, self.epot_dr, self.limit_potential, cutoff=self.cutoff)
+        e._V = self._V
+        return e
+
+    def generate_potential(self, temperature=None, rewrite=False):
+        """LJ potential of the host atoms on the grid (extpot_calculator.py:186-222) on the GPU."""
+        h = self.host
+        if not hasattr(h, 'ff') or h.ff is None:
+            raise NotImplementedError("generate_potential needs a spherical LJ host with parameters")
+        sig = np.array([h.ff[t][0] for t in h.ffatypes])
+        eps = np.array([h.ff[t][1] for t in h.ffatypes])
+        # cap at +inf here; the FreeEnergy applies limit_potential (functionals.py:247-251)
+        self._V = E.external_potential(self.grid.plan, h.recentred_pos(), h.ffatype_ids, sig, eps,
+                                       self.guest.sigma, self.guest.epsilon, self.cutoff, self.limit_potential)
+
+    def cap(self):
+        torch = _torch()
+        V = self._V
+        V = torch.where(torch.isfinite(V), V, torch.full_like(V, self.limit_potential))
+        self._V = torch.clamp(V, max=self.limit_potential)
+
+    def load_potential(self, fn):
+        torch = _torch()
+        pot = np.load(fn)
+        shape = tuple(self.grid.npoints)
+        if pot.shape == tuple(n + 1 for n in shape):
+            pot = pot[:-1, :-1, :-1]
+        elif pot.shape != shape:
+            raise ValueError('Grid shape %s does not match potential shape %s' % (shape, pot.shape))
+        self._V = torch.as_tensor(np.ascontiguousarray(pot, dtype=np.float64), device='cuda')
+
+    def dump_potential(self, fn):
+        np.save(fn, self.potential)
+
+    def potential_device(self):
+        return self._V
+
+    @property
+    def potential(self):
+        return self._V.cpu().numpy()
+
+    def derive(self, krho):
+        return self.potential
+
+    def value(self, krho, local=False):
+        rho = self.grid.ifft(krho)
+        if local:
+            return rho * self.potential
+        return self.grid.integrate(rho * self.potential)

@@ -1,0 +1,48 @@
+"""Public batched entry point: a whole isotherm (or any set of chemical
+potentials) on one host in one batched solve.
+
+The reference solves an isotherm as a Python loop of Program.solve calls, one
+per pressure (examples/methane_ZIF8.ipynb cells 7-11, cmmdft/program.py:
+331-404).  ``solve_isotherm`` takes host arrays on the CPU, builds the
+external potential and MFA kernel on the GPU, solves every point of the
+isotherm as one batch, and returns loadings (and densities) on the CPU.
+"""
+import numpy as np
+import torch
+
+from . import batch as BT
+from . import workload as W
+from .units import angstrom, kjmol
+
+__all__ = ['solve_isotherm', 'excess_loading']
+
+
+def solve_isotherm(host, pressures, temperature, guest, npoints, method='hybridanderson', threshold=1e-8,
+                   criterion='res', nsteps=500, start='bulk', version='WBII', tailcorrections=False,
+                   return_density=True, fn=None, m=5, alpha_mix=0.1):
+    """Solve the adsorption isotherm of a spherical LJ guest in ``host``.
+
+    pressures: array in atomic units (e.g. ``np.logspace(-3, 2, 24) * bar``).
+    start: 'bulk' -> rho0 = rho_bulk exp(-max(V,0)/kT) (Ninit=rho_bulk, the
+    reference notebook's choice); 'ideal' -> exp(beta (mu - V)) / Lambda^3.
+    Returns a dict with mu, rho_bulk, N (absolute loading per cell),
+    converged, steps, omega and (optionally) the densities [B, N1, N2, N3].
+    """
+    if fn is None:
+        fn = W.build_functional(host, npoints, temperature, guest, version=version,
+                                tailcorrections=tailcorrections)
+    mus, bulks = W.isotherm_inputs(pressures, temperature, guest)
+    rho0 = W.initial_density(fn, mus, ninit=bulks if start == 'bulk' else None)
+    s = BT.BatchSolve(fn, mus, method=method, nsteps=nsteps, threshold=threshold, criterion=criterion,
+                      m=m, alpha_mix=alpha_mix)
+    N, rho, conv = s.solve(rho0)
+    out = dict(mu=mus, rho_bulk=bulks, N=np.array(N), converged=np.array(conv), steps=s.steps.copy(),
+               solver=s, functional=fn)
+    if return_density:
+        out['rho'] = rho.cpu().numpy()
+    return out
+
+
+def excess_loading(N, rho_bulk, he_fraction, cell_volume):
+    """N_ex = N - rho_bulk * He_frac * V_cell (Calculator.return_loading, calculator.py:114-138)."""
+    return np.asarray(N) - np.asarray(rho_bulk) * he_fraction * cell_volume

@@ -1,0 +1,117 @@
+"""Fixed-point solvers with the reference's interface (cmmdft/solver.py:18-604).
+
+Solver / Picard / Anderson keep the reference's constructor arguments and
+``solve(chempot, rho, log_level) -> (N, rho, converged)``.  Each call runs a
+batch of one through ``batch.BatchSolve`` (all field work on the GPU); the
+batched isotherm entry point is ``isotherm.solve_isotherm`` /
+``Program.solve_isotherm``.
+"""
+import numpy as np
+
+from . import batch as BT
+from .batch import NoSolutionError
+
+__all__ = ['Solver', 'Picard', 'Anderson', 'NoSolutionError']
+
+
+class Solver(object):
+    name = 'SOLVER'
+
+    def __init__(self, program, nsteps=500, threshold=1e-6, criterion='RIUE', a_tol=1e-6, r_tol=1e-4,
+                 min_iter=1, track_history=False):
+        self.grid = program.grid
+        self.fener = program.fener
+        self.nsteps = nsteps
+        if isinstance(criterion, list):
+            for c in criterion:
+                assert c.lower() in ['riue', 'res', 'der'], \
+                    'Criterion must be either RIUE (relative integrated unsigned error), RES (Residual error) or DER (Derivative error)'
+            self.criterion = [c.lower() for c in criterion]
+            if isinstance(threshold, list):
+                assert len(criterion) == len(threshold), \
+                    'If multiple criterions are given, the same amount of thresholds should be given'
+                self.threshold = threshold
+            else:
+                self.threshold = [threshold] * len(criterion)
+        else:
+            assert criterion.lower() in ['riue', 'res', 'der'], \
+                'Criterion must be either RIUE (relative integrated unsigned error), RES (Residual error) or DER (Derivative error)'
+            if criterion.lower() == 'der':
+                threshold = 1
+            self.criterion = [criterion.lower()]
+            self.threshold = [threshold]
+        self.a_tol, self.r_tol, self.min_iter = a_tol, r_tol, min_iter
+        self.curr_step = 0
+        self.correction_factor = 1
+        self.track_history = track_history
+        self.history_header = ("Loading [au], Grand potential [Eh], Norm of residuals, RIUE, "
+                               "Norm of derivative, Time per step [s], Cumulative time [s]")
+        self.history = np.zeros((nsteps + 1, 7))
+        self.omega0 = None
+        self._last = None
+
+    def _method(self):
+        raise NotImplementedError
+
+    def _options(self):
+        return {}
+
+    def solve(self, chempot, rho, log_level=2):
+        """Converge one density (B = 1) on the GPU; returns (N, rho, converged)."""
+        import torch
+        fn = self.fener.device()
+        s = BT.BatchSolve(fn, [chempot], method=self._method(), nsteps=self.nsteps, threshold=self.threshold,
+                          criterion=self.criterion, **self._options())
+        r0 = rho if hasattr(rho, 'detach') else torch.as_tensor(np.ascontiguousarray(rho, dtype=np.float64))
+        r0 = r0.to('cuda', dtype=torch.float64).reshape((1,) + tuple(self.grid.npoints))
+        N, rr, conv = s.solve(r0)
+        self._last = s
+        self.curr_step = int(s.steps[0])
+        self.omega0 = float(s.omega0[0]) if hasattr(s, 'omega0') else None
+        if self.track_history:
+            h = np.array(s.history[0]) if s.history[0] else np.zeros((0, 3))
+            self.history = np.zeros((len(h) + 1, 7)) * np.nan
+            if len(h):
+                self.history[1:, 0] = h[:, 0]
+                self.history[1:, 2] = h[:, 1]
+                self.history[1:, 3] = h[:, 2]
+        return float(N[0]), rr[0].cpu().numpy(), bool(conv[0])
+
+
+class Picard(Solver):
+    name = 'PICARD'
+
+    def __init__(self, program, nsteps=500, alpha_mix=0.1, method='hybrid', **kwargs):
+        Solver.__init__(self, program, nsteps, **kwargs)
+        self.alpha_mix = alpha_mix
+        assert method in ('hybrid', 'static'), method
+        self.method = method
+
+    def _method(self):
+        return self.method
+
+    def _options(self):
+        return dict(alpha_mix=self.alpha_mix)
+
+
+class Anderson(Picard):
+    """Anderson and hybrid-Anderson mixing (https://doi.org/10.1063/5.0067172)."""
+    name = 'ANDERSON'
+
+    def __init__(self, program, nsteps=500, method='hybridanderson', m=5, damping=0.3, delta=0.2,
+                 damping_max=0.8, damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5), **kwargs):
+        Solver.__init__(self, program, nsteps, **{k: v for k, v in kwargs.items() if k != 'alpha_mix'})
+        self.alpha_mix = kwargs.get('alpha_mix', 0.1)
+        assert method in ('hybridanderson', 'anderson'), method
+        self.Anderson_method = method
+        self.m, self.damping, self.delta = m, damping, delta
+        self.damping_max, self.damping_min = damping_max, damping_min
+        self.adaptive_damping, self.damping_factors = adaptive_damping, damping_factors
+
+    def _method(self):
+        return self.Anderson_method
+
+    def _options(self):
+        return dict(alpha_mix=self.alpha_mix, m=self.m, damping=self.damping, delta=self.delta,
+                    damping_max=self.damping_max, damping_min=self.damping_min,
+                    adaptive_damping=self.adaptive_damping, damping_factors=self.damping_factors)

@@ -7,11 +7,15 @@
  *
  * Data layout (one "shape group" of `batch` instances on an N1 x N2 x N3
  * grid, C order, x slowest as in the reference's Grid):
- *   real field : double [batch][N1][N2][N3]
- *   spectrum   : double2 [batch][N1][N2][H3], H3 = N3/2 + 1, holding the
- *                half spectrum of a real field with the y and z frequency
- *                axes in the plan's digit-reversed order (x natural).  Use
- *                cmm_spectrum_index() to map positions to frequencies.
+ *   real field  : double [batch][N1][N2][N3]
+ *   spectrum    : double2 [batch][N1][N2][H3], H3 = N3/2 + 1, the 3D half
+ *                 spectrum of a real field, x frequencies in natural order,
+ *                 y and z frequencies in the plan's digit-reversed order.
+ *                 Use cmm_spectrum_index() to map positions to frequencies.
+ *   yz-spectrum : the same array shape with x still in real space and only
+ *                 y, z transformed (the x transform lives inside the column
+ *                 passes).  The functional pipeline and the solver plane
+ *                 passes exchange densities and C1 in this layout.
  *
  * The reference (CmmDFT) is pure Python/numpy; it has no FFI.  Each entry
  * point below names the reference function whose arithmetic it replaces
@@ -54,8 +58,9 @@ enum {
 };
 #define CMM_MAX_HIST 8
 
-/* Hard-sphere functional versions (cmmdft/functionals.py:373-377). */
-enum { CMM_FMT = 0, CMM_MFMT = 1, CMM_WBII = 2, CMM_ANTISYM = 8 };
+/* Hard-sphere functional versions (cmmdft/functionals.py:373-377).
+ * CMM_NOHS drops the hard-sphere term (the MFA convolution alone). */
+enum { CMM_FMT = 0, CMM_MFMT = 1, CMM_WBII = 2, CMM_ANTISYM = 8, CMM_NOHS = 16 };
 
 /* Mix-kernel clip modes. */
 enum {
@@ -106,6 +111,11 @@ int cmm_rfft3d(const cmm_grid* grid, int batch, const double* d_in, double* d_sp
 int cmm_irfft3d(const cmm_grid* grid, int batch, double* d_spec, double* d_out, void* stream);
 /* (cmm_irfft3d overwrites d_spec with intermediate data.) */
 
+/* Plane passes alone: y/z real-to-half-complex transform of real fields
+ * into yz-spectra, and the inverse (unnormalised). */
+int cmm_rfft_yz(const cmm_grid* grid, int batch, const double* d_in, double* d_spec, void* stream);
+int cmm_irfft_yz(const cmm_grid* grid, int batch, const double* d_spec, double* d_out, void* stream);
+
 /* Mean-field attraction kernel spectrum: the sampled cut-and-shifted LJ
  * potential U(r) of MFAFunctional.generate_potential_lj
  * (cmmdft/functionals.py:878-910), transformed and folded with the Lanczos
@@ -122,11 +132,11 @@ int cmm_mfa_kernel(const cmm_grid* grid, double sigma, double epsilon, double cu
                    double rmin, double limit_potential, int rep, double* d_kst,
                    double* d_work, size_t* work_bytes, double* vdw_a, void* stream);
 
-/* Functional pipeline for `batch` densities given their spectra d_rhohat:
+/* Functional pipeline for `batch` densities given their yz-spectra d_rhohat:
  *   column pass: rho_hat -> analytic FMT weights -> n0, n3, nv2 spectra
  *   plane pass : inverse, White-Bear/FMT dPhi/dn, forward of 5 fields
  *   column pass: back-convolution sum w_a dPhi_a / (beta N) + rho_hat * K_mfa
- * writing d_chat = spectrum of C1 - V (HardSphere.derive + MFA.derive,
+ * writing d_chat = yz-spectrum of C1 - V (HardSphere.derive + MFA.derive,
  * cmmdft/functionals.py:489-609, 912-926).  want: bit 0 = C1 spectrum,
  * bit 1 = free-energy sums (PHI, MFA), bit 2 = n3 maximum.
  * d_work: 10 spectra of batch instances.  d_part: [batch][CMM_NSTAT][nslot]. */
