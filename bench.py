@@ -139,7 +139,8 @@ def run_gpu(args):
     rho0 = W.initial_density(fn, mus, ninit=bulks)
 
     def one_solve(events=None):
-        s = BT.BatchSolve(fn, mus, method="hybridanderson", nsteps=500, threshold=THRESH, criterion="res")
+        s = BT.BatchSolve(fn, mus, method="hybridanderson", nsteps=args.max_iters, threshold=THRESH,
+                          criterion="res")
         s.pipeline_events = events
         N, rho, conv = s.solve(rho0)
         return s, conv
@@ -338,6 +339,7 @@ def main():
     ap.add_argument("--no-plain", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--max-iters", type=int, default=500, help="solver step cap (lower it only to profile)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)
