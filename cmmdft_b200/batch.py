@@ -81,7 +81,7 @@ class BatchSolve(object):
 
     def __init__(self, fn, chempots, method='hybridanderson', nsteps=500, threshold=1e-6,
                  criterion='res', alpha_mix=0.1, m=5, damping=0.3, delta=0.2, damping_max=0.8,
-                 damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5)):
+                 damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5), divergence_guard=False):
         self.fn = fn
         self.plan = fn.plan
         self.mu = np.asarray(chempots, dtype=np.float64).ravel()
@@ -104,6 +104,12 @@ class BatchSolve(object):
         self.adaptive = adaptive_damping
         self.dfac = damping_factors
         self.delta = delta
+        # Opt-in: retire an instance as not converged once RES exceeds 1e6 x its
+        # best value and has not decreased over the last 5 steps.  The
+        # reference iterates such instances to nsteps (and reports them not
+        # converged); with this guard the batch stops paying for them.
+        self.divergence_guard = bool(divergence_guard)
+        self.diverged = np.zeros(len(np.atleast_1d(chempots)), dtype=bool)
         beta = fn.beta
         # fugacity = exp(beta mu) / beta / Lambda^3 (solver.py:92)
         self.fug = np.exp(beta * self.mu) / beta / fn.wavelength ** 3
@@ -280,7 +286,8 @@ class BatchSolve(object):
                         self._finish(b, self.ring[cur[b], b], N, step - 1, True)
                         live[b] = False
                         continue
-                    if step - 1 >= self.nsteps:
+                    if step - 1 >= self.nsteps or self._diverging(b):
+                        self.diverged[b] = step - 1 < self.nsteps
                         self._finish(b, self.ring[cur[b], b], N, step - 1, False)
                         live[b] = False
                         continue
@@ -295,6 +302,15 @@ class BatchSolve(object):
             self._c1(self.rhohat, self.chat, 1)
             prev = st
         return retry
+
+    def _diverging(self, b):
+        if not self.divergence_guard:
+            return False
+        r = np.array([h[1] for h in self.history[b]])
+        if len(r) < 8 or not np.isfinite(r[-1]):
+            return len(r) >= 8
+        best = np.nanmin(r)
+        return bool(r[-1] > 1e6 * best and np.all(np.diff(r[-6:]) >= 0))
 
     def _converged(self, b, N, res, iue):
         ok = True
@@ -369,7 +385,8 @@ class BatchSolve(object):
                 if self._converged(b, N, res, iue):
                     self._finish(b, self.ring[s_new, b], N, k, True)
                     live[b] = False
-                elif k >= self.nsteps:
+                elif k >= self.nsteps or self._diverging(b):
+                    self.diverged[b] = k < self.nsteps
                     self._finish(b, self.ring[s_new, b], N, k, False)
                     live[b] = False
         return retry

@@ -19,7 +19,7 @@ __all__ = ['solve_isotherm', 'excess_loading']
 
 def solve_isotherm(host, pressures, temperature, guest, npoints, method='hybridanderson', threshold=1e-8,
                    criterion='res', nsteps=500, start='bulk', version='WBII', tailcorrections=False,
-                   return_density=True, fn=None, m=5, alpha_mix=0.1):
+                   return_density=True, fn=None, m=5, alpha_mix=0.1, divergence_guard=True):
     """Solve the adsorption isotherm of a spherical LJ guest in ``host``.
 
     pressures: array in atomic units (e.g. ``np.logspace(-3, 2, 24) * bar``).
@@ -34,9 +34,10 @@ def solve_isotherm(host, pressures, temperature, guest, npoints, method='hybrida
     mus, bulks = W.isotherm_inputs(pressures, temperature, guest)
     rho0 = W.initial_density(fn, mus, ninit=bulks if start == 'bulk' else None)
     s = BT.BatchSolve(fn, mus, method=method, nsteps=nsteps, threshold=threshold, criterion=criterion,
-                      m=m, alpha_mix=alpha_mix)
+                      m=m, alpha_mix=alpha_mix, divergence_guard=divergence_guard)
     N, rho, conv = s.solve(rho0)
     out = dict(mu=mus, rho_bulk=bulks, N=np.array(N), converged=np.array(conv), steps=s.steps.copy(),
+               diverged=s.diverged.copy(),
                solver=s, functional=fn)
     if return_density:
         out['rho'] = rho.cpu().numpy()
