@@ -45,7 +45,8 @@ _SIGS = {
     "cmm_mfa_kernel": ([c_void_p, c_double, c_double, c_double, c_double, c_double, c_int, c_void_p,
                         c_void_p, P(ctypes.c_size_t), P(c_double), c_void_p], c_int),
     "cmm_fmt_c1": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p,
-                    c_void_p, c_void_p, c_int, c_int, c_void_p], c_int),
+                    c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p], c_int),
+    "cmm_fmt_weights": ([c_void_p, c_double, c_void_p, c_void_p], c_int),
     "cmm_picard_static_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_void_p,
                                 c_void_p, c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int, c_void_p], c_int),
     "cmm_residual_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_ll,

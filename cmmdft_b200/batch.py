@@ -72,6 +72,41 @@ def simplex_qp(M, idx):
     return best
 
 
+def simplex_qp_batched(M):
+    """simplex_qp for a stack of Gram matrices M [B, n, n] (same support
+    enumeration, vectorised over the batch)."""
+    B, n, _ = M.shape
+    diag = np.abs(np.diagonal(M, axis1=1, axis2=2))
+    scale = np.maximum(diag.max(axis=1), 1e-300)
+    Ms = M / scale[:, None, None]
+    best = np.tile(np.full(n, 1.0 / n), (B, 1))
+    best_val = np.full(B, np.inf)
+    found = np.zeros(B, dtype=bool)
+    for k in range(1, n + 1):
+        for S in itertools.combinations(range(n), k):
+            S = list(S)
+            A = Ms[:, S][:, :, S]
+            one = np.ones((B, k, 1))
+            try:
+                x = np.linalg.solve(A, one)[..., 0]
+            except np.linalg.LinAlgError:
+                x = (np.linalg.pinv(A) @ one)[..., 0]
+            sx = x.sum(axis=1)
+            with np.errstate(all='ignore'):
+                a = x / sx[:, None]
+            ok = np.isfinite(sx) & (np.abs(sx) > 1e-300) & np.all(a >= -1e-14, axis=1)
+            a = np.clip(np.nan_to_num(a), 0.0, None)
+            a /= np.maximum(a.sum(axis=1, keepdims=True), 1e-300)
+            full = np.zeros((B, n))
+            full[:, S] = a
+            val = np.einsum('bi,bij,bj->b', full, Ms, full)
+            upd = ok & ((val < best_val * (1 - 1e-13)) | ~found)
+            best[upd] = full[upd]
+            best_val[upd] = val[upd]
+            found |= upd
+    return best
+
+
 class BatchSolve(object):
     """Solve B fixed points that share a Functional (grid, host, guest, T).
 
@@ -402,9 +437,6 @@ class BatchSolve(object):
         hist_slots = self._valid_hist(k, s_new)
         self._residual(self.chat2, self.ring[s_new], self.rres[s_new], [self.rres[j] for j in hist_slots])
         st = self._stats()
-        for b in np.where(mask)[0]:
-            self.rhohat[b].copy_(self.that[b])
-            self.chat[b].copy_(self.chat2[b])
         return st, hist_slots
 
     def _commit_residual(self, mask, st, k, s_new, hist_slots):
@@ -424,8 +456,10 @@ class BatchSolve(object):
         mk = min(k, self.m)
         slots = [j % m for j in range(k - mk, k)]  # oldest .. newest
         coefs = np.zeros((B, 2 * mk))
-        for b in np.where(mask)[0]:
-            al = simplex_qp(self.gram[b], slots)
+        idx = np.where(mask)[0]
+        alphas = simplex_qp_batched(self.gram[idx][:, slots][:, :, slots])
+        for ii, b in enumerate(idx):
+            al = alphas[ii]
             if self.adaptive:  # _get_damping_coefficient (solver.py:537-544)
                 r = np.sqrt(self.rnorm2[b, s_prev])
                 p = np.sqrt(self.rnorm2[b, (k - 2) % m]) if k >= 2 else 0.0
@@ -485,14 +519,15 @@ class BatchSolve(object):
             o1 = self._trial_omega(need, a1, s_prev)
             a2 = np.where(o1 <= prev, 0.9 * amax, 0.225 * amax)
             o2 = self._trial_omega(need, a2, s_prev)
-            for b in np.where(need)[0]:
-                c, bb, a = np.polyfit([0, a1[b], a2[b]], [prev[b], o1[b], o2[b]], 2)
-                hi = max(a1[b], a2[b])
-                al = np.linspace(-hi / 4, hi, 10000)
-                om = a + bb * al + c * al ** 2
-                aopt[b] = al[np.where(om == np.min(om))[0][0]]
-                mn[b] = np.min(om) / kjmol
-                mx[b] = np.max(om) / kjmol
+            idx = np.where(need)[0]
+            cf = np.array([np.polyfit([0, a1[b], a2[b]], [prev[b], o1[b], o2[b]], 2) for b in idx])
+            hi = np.maximum(a1[idx], a2[idx])
+            al = np.linspace(-hi / 4, hi, 10000, axis=1)
+            om = cf[:, 2:3] + cf[:, 1:2] * al + cf[:, 0:1] * al ** 2
+            j = np.argmin(om, axis=1)   # first minimum, as np.where(om == min)[0][0]
+            aopt[idx] = al[np.arange(len(idx)), j]
+            mn[idx] = np.min(om, axis=1) / kjmol
+            mx[idx] = np.max(om, axis=1) / kjmol
             self.omega0 = np.where(need, o2, self.omega0)
         for b in np.where(mask)[0]:
             if aopt[b] <= 0:

@@ -15,8 +15,13 @@
 #include "cmm_common.cuh"
 
 // --------------------------------------------------------- shared tables --
+// Plane layout in shared memory: nslot fields interleaved by row,
+//   slots[(r * nslot + f) * h3 + c]   (y row r, field f, stored z frequency c)
+// so y pencils (p = f*h3 + c) and z rows (p = r*nslot + f) are both uniform
+// pencil sets (base = p * pstride).  A real row of N3 doubles occupies the
+// first N3/2 double2 of its row.
 struct PlaneSmem {
-  double2* slots;   // nslot * n2 * h3
+  double2* slots;   // n2 * nslot * h3
   double2* tw2;     // n2
   double2* tw3;     // n3
   int* zpos;        // m3
@@ -29,30 +34,46 @@ __host__ __device__ inline size_t plane_smem_bytes(int n2, int n3, int nslot) {
   return (b + 15) & ~(size_t)15;
 }
 
+// Compile-time shape of a plane pass: N2C = y length, M3C = z half length
+// (0 = take them from the plan at run time).
+template <int N2C, int M3C>
+struct PlaneShape {
+  int n2, m3, h3, n3;
+  __device__ PlaneShape(const GridDev& g)
+      : n2(N2C ? N2C : g.n2), m3(M3C ? M3C : g.m3), h3((M3C ? M3C : g.m3) + 1), n3(2 * (M3C ? M3C : g.m3)) {}
+};
+
+template <int N2C, int M3C>
 __device__ inline PlaneSmem plane_smem_setup(const GridDev& g, int nslot) {
   extern __shared__ double2 smem_d2[];
+  const PlaneShape<N2C, M3C> sh(g);
   PlaneSmem s;
   s.slots = smem_d2;
-  s.tw2 = s.slots + (size_t)nslot * g.n2 * g.h3;
-  s.tw3 = s.tw2 + g.n2;
-  s.zpos = (int*)(s.tw3 + g.n3);
-  for (int i = threadIdx.x; i < g.n2; i += blockDim.x) s.tw2[i] = g.tw2[i];
-  for (int i = threadIdx.x; i < g.n3; i += blockDim.x) s.tw3[i] = g.tw3[i];
-  for (int i = threadIdx.x; i < g.m3; i += blockDim.x) s.zpos[i] = g.zpos[i];
+  s.tw2 = s.slots + (size_t)nslot * sh.n2 * sh.h3;
+  s.tw3 = s.tw2 + sh.n2;
+  s.zpos = (int*)(s.tw3 + sh.n3);
+  for (int i = threadIdx.x; i < sh.n2; i += blockDim.x) s.tw2[i] = g.tw2[i];
+  for (int i = threadIdx.x; i < sh.n3; i += blockDim.x) s.tw3[i] = g.tw3[i];
+  for (int i = threadIdx.x; i < sh.m3; i += blockDim.x) s.zpos[i] = g.zpos[i];
   return s;
 }
 
-// ------------------------------------------------ plane transforms ------
-// Forward: real rows (natural z) in each slot -> DIF z, R2C twist, DIF y.
-__device__ void plane_forward(const GridDev& g, const PlaneSmem& s, int nslot) {
-  const int n2 = g.n2, h3 = g.h3, m3 = g.m3;
-  PencilSet rows = {nslot * n2, nslot * n2, 0, h3, 1, false};
-  fft_pencils<false>(s.slots, g.ax3, s.tw3, 2, rows);
-  // R2C twist on every row: pairs (k, m3-k), k = 0..m3/2
-  const int np = m3 / 2 + 1;
-  const int total = nslot * n2 * np;
+template <bool INV, int NC>
+__device__ __forceinline__ void axis_fft(double2* base, const FftAxis& ax, const double2* tw, int twmul,
+                                         int npencil, int pstride, int estride) {
+  if constexpr (NC > 0) fft_ct<INV, NC>(base, tw, twmul, npencil, pstride, estride);
+  else fft_rt<INV>(base, ax, tw, twmul, npencil, pstride, estride);
+}
+
+// R2C twist on every row: pairs (k, m3-k), k = 0..m3/2, rows fastest.
+template <int N2C, int M3C>
+__device__ void r2c_twist(const GridDev& g, const PlaneSmem& s, int nslot) {
+  const PlaneShape<N2C, M3C> sh(g);
+  const int m3 = sh.m3, h3 = sh.h3;
+  const int nrow = nslot * sh.n2;
+  const int total = nrow * (m3 / 2 + 1);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int row = t / np, k = t - row * np;
+    const int k = t / nrow, row = t - k * nrow;
     double2* rp = s.slots + (size_t)row * h3;
     if (k == 0) {
       double2 z0 = rp[0];
@@ -61,30 +82,26 @@ __device__ void plane_forward(const GridDev& g, const PlaneSmem& s, int nslot) {
     } else {
       const int pk = s.zpos[k], pm = s.zpos[m3 - k];
       double2 zk = rp[pk], zm = rp[pm];
-      // E = (zk + conj zm)/2 ; O = -i (zk - conj zm)/2
+      // E = (zk + conj zm)/2 ; O = -i (zk - conj zm)/2 ; X[k] = E + W O ; X[m-k] = conj(E - W O)
       double2 E = make_double2(0.5 * (zk.x + zm.x), 0.5 * (zk.y - zm.y));
       double2 O = make_double2(0.5 * (zk.y + zm.y), -0.5 * (zk.x - zm.x));
       double2 WO = cmul(s.tw3[k], O);
-      double2 xk = cadd(E, WO);
-      double2 xm = cconj(csub(E, WO));
-      rp[pk] = xk;
-      if (pm != pk) rp[pm] = xm;
+      rp[pk] = cadd(E, WO);
+      if (pm != pk) rp[pm] = cconj(csub(E, WO));
     }
   }
   __syncthreads();
-  PencilSet cols = {nslot * h3, h3, n2 * h3, 1, h3, true};
-  fft_pencils<false>(s.slots, g.ax2, s.tw2, 1, cols);
 }
 
-// Inverse: spectrum slots -> DIT y, C2R twist, DIT z -> real rows (unnormalised).
-__device__ void plane_inverse(const GridDev& g, const PlaneSmem& s, int nslot) {
-  const int n2 = g.n2, h3 = g.h3, m3 = g.m3;
-  PencilSet cols = {nslot * h3, h3, n2 * h3, 1, h3, true};
-  fft_pencils<true>(s.slots, g.ax2, s.tw2, 1, cols);
-  const int np = m3 / 2 + 1;
-  const int total = nslot * n2 * np;
+// C2R twist: Zin[k] = (X[k] + conj X[m-k]) + i (X[k] - conj X[m-k]) e^{2 pi i k / N3}.
+template <int N2C, int M3C>
+__device__ void c2r_twist(const GridDev& g, const PlaneSmem& s, int nslot) {
+  const PlaneShape<N2C, M3C> sh(g);
+  const int m3 = sh.m3, h3 = sh.h3;
+  const int nrow = nslot * sh.n2;
+  const int total = nrow * (m3 / 2 + 1);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int row = t / np, k = t - row * np;
+    const int k = t / nrow, row = t - k * nrow;
     double2* rp = s.slots + (size_t)row * h3;
     if (k == 0) {
       // real parts of the DC and Nyquist bins (Grid.ifft keeps .real)
@@ -93,41 +110,66 @@ __device__ void plane_inverse(const GridDev& g, const PlaneSmem& s, int nslot) {
     } else {
       const int pk = s.zpos[k], pm = s.zpos[m3 - k];
       double2 xk = rp[pk], xm = rp[pm];
-      double2 e = make_double2(xk.x + xm.x, xk.y - xm.y);           // xk + conj(xm)
-      double2 o = cmulc(make_double2(xk.x - xm.x, xk.y + xm.y), s.tw3[k]);  // (xk - conj xm) conj(W^k)
-      // Zin[k] = e + i o ; Zin[m3-k] = conj(e) + i conj(o)
+      double2 e = make_double2(xk.x + xm.x, xk.y - xm.y);
+      double2 o = cmulc(make_double2(xk.x - xm.x, xk.y + xm.y), s.tw3[k]);
       rp[pk] = make_double2(e.x - o.y, e.y + o.x);
       if (pm != pk) rp[pm] = make_double2(e.x + o.y, -e.y + o.x);
     }
   }
   __syncthreads();
-  PencilSet rows = {nslot * n2, nslot * n2, 0, h3, 1, false};
-  fft_pencils<true>(s.slots, g.ax3, s.tw3, 2, rows);
 }
 
-// Real element (y=r, z=j) of slot f, in the row layout of a transformed plane.
-__device__ __forceinline__ double& rel(const PlaneSmem& s, const GridDev& g, int f, int r, int j) {
-  return ((double*)(s.slots + ((size_t)f * g.n2 + r) * g.h3))[j];
+// Forward: real rows (natural z) in each slot -> DIF z, R2C twist, DIF y.
+template <int N2C, int M3C>
+__device__ void plane_forward(const GridDev& g, const PlaneSmem& s, int nslot) {
+  const PlaneShape<N2C, M3C> sh(g);
+  axis_fft<false, M3C>(s.slots, g.ax3, s.tw3, 2, nslot * sh.n2, sh.h3, 1);
+  r2c_twist<N2C, M3C>(g, s, nslot);
+  axis_fft<false, N2C>(s.slots, g.ax2, s.tw2, 1, nslot * sh.h3, 1, nslot * sh.h3);
 }
 
-// Copy nslot spectrum planes from global (field stride fs, in double2) into smem.
-__device__ inline void load_spec_planes(const GridDev& g, const PlaneSmem& s, int nslot,
-                                        const double2* src, size_t plane_off, size_t fs) {
-  const int cnt = g.n2 * g.h3;
+// Inverse: spectrum slots -> DIT y, C2R twist, DIT z -> real rows (unnormalised).
+template <int N2C, int M3C>
+__device__ void plane_inverse(const GridDev& g, const PlaneSmem& s, int nslot) {
+  const PlaneShape<N2C, M3C> sh(g);
+  axis_fft<true, N2C>(s.slots, g.ax2, s.tw2, 1, nslot * sh.h3, 1, nslot * sh.h3);
+  c2r_twist<N2C, M3C>(g, s, nslot);
+  axis_fft<true, M3C>(s.slots, g.ax3, s.tw3, 2, nslot * sh.n2, sh.h3, 1);
+}
+
+// Real element (y=r, z=j) of field f.
+template <int N2C, int M3C>
+__device__ __forceinline__ double& rel(const PlaneSmem& s, const PlaneShape<N2C, M3C>& sh, int nslot, int f, int r,
+                                       int j) {
+  return ((double*)(s.slots + ((size_t)r * nslot + f) * sh.h3))[j];
+}
+
+// Copy nslot spectrum planes (global: field f at src + f*fs + plane_off, [n2][h3]) into smem.
+template <int N2C, int M3C>
+__device__ inline void load_spec_planes(const GridDev& g, const PlaneSmem& s, int nslot, const double2* src,
+                                        size_t plane_off, size_t fs) {
+  const PlaneShape<N2C, M3C> sh(g);
+  const int h3 = sh.h3, cnt = sh.n2 * h3;
   for (int f = 0; f < nslot; ++f) {
     const double2* p = src + f * fs + plane_off;
-    double2* d = s.slots + (size_t)f * cnt;
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x) d[i] = __ldg(p + i);
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const int r = i / h3, c = i - r * h3;
+      s.slots[((size_t)r * nslot + f) * h3 + c] = __ldg(p + i);
+    }
   }
 }
 
-__device__ inline void store_spec_planes(const GridDev& g, const PlaneSmem& s, int nslot,
-                                         double2* dst, size_t plane_off, size_t fs) {
-  const int cnt = g.n2 * g.h3;
+template <int N2C, int M3C>
+__device__ inline void store_spec_planes(const GridDev& g, const PlaneSmem& s, int nslot, double2* dst,
+                                         size_t plane_off, size_t fs) {
+  const PlaneShape<N2C, M3C> sh(g);
+  const int h3 = sh.h3, cnt = sh.n2 * h3;
   for (int f = 0; f < nslot; ++f) {
     double2* p = dst + f * fs + plane_off;
-    const double2* d = s.slots + (size_t)f * cnt;
-    for (int i = threadIdx.x; i < cnt; i += blockDim.x) p[i] = d[i];
+    for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
+      const int r = i / h3, c = i - r * h3;
+      p[i] = s.slots[((size_t)r * nslot + f) * h3 + c];
+    }
   }
 }
 
@@ -165,111 +207,120 @@ __device__ inline void put_part(double* part, int b, int q, int nslot, int slot,
 }
 
 // ================================================ 3D FFT (setup / tests) ==
+template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_PLANE_THREADS)
 k_plane_r2c(GridDev g, const double* __restrict__ in, double2* __restrict__ out) {
   const int i1 = blockIdx.x, b = blockIdx.y;
-  PlaneSmem s = plane_smem_setup(g, 1);
-  const size_t roff = ((size_t)b * g.n1 + i1) * g.n2 * g.n3;
-  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
-    int r = i / g.n3, j = i - r * g.n3;
-    rel(s, g, 0, r, j) = __ldg(in + roff + i);
+  PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
+  const PlaneShape<N2C, M3C> sh(g);
+  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
+  for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
+    const int r = i / sh.n3, j = i - r * sh.n3;
+    rel(s, sh, 1, 0, r, j) = __ldg(in + roff + i);
   }
   __syncthreads();
-  plane_forward(g, s, 1);
-  store_spec_planes(g, s, 1, out, ((size_t)b * g.n1 + i1) * g.n2 * g.h3, 0);
+  plane_forward<N2C, M3C>(g, s, 1);
+  store_spec_planes<N2C, M3C>(g, s, 1, out, ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3, 0);
 }
 
+template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_PLANE_THREADS)
 k_plane_c2r(GridDev g, const double2* __restrict__ in, double* __restrict__ out) {
   const int i1 = blockIdx.x, b = blockIdx.y;
-  PlaneSmem s = plane_smem_setup(g, 1);
-  load_spec_planes(g, s, 1, in, ((size_t)b * g.n1 + i1) * g.n2 * g.h3, 0);
+  PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
+  const PlaneShape<N2C, M3C> sh(g);
+  load_spec_planes<N2C, M3C>(g, s, 1, in, ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3, 0);
   __syncthreads();
-  plane_inverse(g, s, 1);
-  const size_t roff = ((size_t)b * g.n1 + i1) * g.n2 * g.n3;
-  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
-    int r = i / g.n3, j = i - r * g.n3;
-    out[roff + i] = rel(s, g, 0, r, j);
+  plane_inverse<N2C, M3C>(g, s, 1);
+  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
+  for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
+    const int r = i / sh.n3, j = i - r * sh.n3;
+    out[roff + i] = rel(s, sh, 1, 0, r, j);
   }
 }
 
-// Column tile geometry: TC consecutive (y,z) columns of one instance.
+// Column tile: TC consecutive (y,z) columns of one instance, all N1 x rows.
+// Shared layout [n1][nslot][tc]: element (f, x=p1, c) at (p1*nslot + f)*tc + c,
+// so the x pencils (p = f*tc + c) are uniform with estride nslot*tc.
 struct ColSmem {
-  double2* slots;   // nslot * n1 * tc
-  double2* tw1;     // n1
+  double2* slots;
+  double2* tw1;
 };
 
 __host__ __device__ inline size_t col_smem_bytes(int n1, int tc, int nslot) {
   return sizeof(double2) * ((size_t)nslot * n1 * tc + n1);
 }
 
-__device__ inline ColSmem col_smem_setup(const GridDev& g, int nslot, int tc) {
+template <int N1C, int TCC>
+struct ColShape {
+  int n1, tc;
+  __device__ ColShape(const GridDev& g, int tc_rt) : n1(N1C ? N1C : g.n1), tc(TCC ? TCC : tc_rt) {}
+};
+
+template <int N1C, int TCC>
+__device__ inline ColSmem col_smem_setup(const GridDev& g, const ColShape<N1C, TCC>& sh, int nslot) {
   extern __shared__ double2 smem_d2[];
   ColSmem s;
   s.slots = smem_d2;
-  s.tw1 = s.slots + (size_t)nslot * g.n1 * tc;
-  for (int i = threadIdx.x; i < g.n1; i += blockDim.x) s.tw1[i] = g.tw1[i];
+  s.tw1 = s.slots + (size_t)nslot * sh.n1 * sh.tc;
+  for (int i = threadIdx.x; i < sh.n1; i += blockDim.x) s.tw1[i] = g.tw1[i];
   return s;
 }
 
-// Load a tile [n1][tc] of field f (instance b) into slot f; zero-fill past the end.
-__device__ inline void load_col_tile(const GridDev& g, const ColSmem& s, int slot, const double2* src,
-                                     int b, int c0, int tc) {
+template <int N1C, int TCC>
+__device__ __forceinline__ double2& cel(const ColSmem& s, const ColShape<N1C, TCC>& sh, int nslot, int f, int p1,
+                                        int c) {
+  return s.slots[((size_t)p1 * nslot + f) * sh.tc + c];
+}
+
+// Load a tile [n1][tc] of one field (instance b) into slot f; zero past the last column.
+template <int N1C, int TCC>
+__device__ inline void load_col_tile(const GridDev& g, const ColSmem& s, const ColShape<N1C, TCC>& sh, int nslot,
+                                     int f, const double2* src, int b, int c0, const int* rowmap) {
   const int nc = g.n2 * g.h3;
-  const size_t base = (size_t)b * g.n1 * nc;
-  double2* d = s.slots + (size_t)slot * g.n1 * tc;
-  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
-    const int r = i / tc, c = i - r * tc;
+  const size_t base = (size_t)b * sh.n1 * nc;
+  for (int i = threadIdx.x; i < sh.n1 * sh.tc; i += blockDim.x) {
+    const int p1 = i / sh.tc, c = i - p1 * sh.tc;
     const int col = c0 + c;
-    d[i] = (col < nc) ? __ldg(src + base + (size_t)r * nc + col) : make_double2(0.0, 0.0);
+    const int r = rowmap ? rowmap[p1] : p1;
+    cel(s, sh, nslot, f, p1, c) = (col < nc) ? src[base + (size_t)r * nc + col] : make_double2(0.0, 0.0);
   }
 }
 
-__device__ inline void store_col_tile(const GridDev& g, const ColSmem& s, int slot, double2* dst,
-                                      int b, int c0, int tc) {
+template <int N1C, int TCC>
+__device__ inline void store_col_tile(const GridDev& g, const ColSmem& s, const ColShape<N1C, TCC>& sh, int nslot,
+                                      int f, double2* dst, int b, int c0, const int* rowmap) {
   const int nc = g.n2 * g.h3;
-  const size_t base = (size_t)b * g.n1 * nc;
-  const double2* d = s.slots + (size_t)slot * g.n1 * tc;
-  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
-    const int r = i / tc, c = i - r * tc;
+  const size_t base = (size_t)b * sh.n1 * nc;
+  for (int i = threadIdx.x; i < sh.n1 * sh.tc; i += blockDim.x) {
+    const int p1 = i / sh.tc, c = i - p1 * sh.tc;
     const int col = c0 + c;
-    if (col < nc) dst[base + (size_t)r * nc + col] = d[i];
+    const int r = rowmap ? rowmap[p1] : p1;
+    if (col < nc) dst[base + (size_t)r * nc + col] = cel(s, sh, nslot, f, p1, c);
   }
 }
 
-__device__ inline void col_fft(const GridDev& g, const ColSmem& s, int nslot, int tc, bool inv) {
-  PencilSet ps = {nslot * tc, tc, g.n1 * tc, 1, tc, true};
-  if (inv) fft_pencils<true>(s.slots, g.ax1, s.tw1, 1, ps);
-  else fft_pencils<false>(s.slots, g.ax1, s.tw1, 1, ps);
+// x transform of `nfield` fields starting at field f0 of an nslot tile.
+template <bool INV, int N1C, int TCC>
+__device__ inline void col_fft(const GridDev& g, const ColSmem& s, const ColShape<N1C, TCC>& sh, int nslot, int f0,
+                               int nfield) {
+  axis_fft<INV, N1C>(s.slots + (size_t)f0 * sh.tc, g.ax1, s.tw1, 1, nfield * sh.tc, 1, nslot * sh.tc);
 }
 
-// Plain x transform of a tile (setup / tests).  Forward leaves x in DIF
-// order when `keep_dif`; the HBM layout keeps x natural, so the 3D FFT
-// entry points run forward then un-permute in the same kernel.
+// Plain x transform of a tile (setup / tests).  HBM spectra keep x natural:
+// forward loads natural rows, runs DIF and stores row k1pos[p]; inverse loads
+// row k1pos[p] into position p, runs DIT and stores natural rows.
+template <int N1C, int TCC>
 __global__ void __launch_bounds__(CMM_COL_THREADS)
-k_col_fft(GridDev g, const double2* in, double2* out, int tc, int inv,
-          const int* __restrict__ k1_of_pos) {
-  const int b = blockIdx.y, c0 = blockIdx.x * tc;
-  ColSmem s = col_smem_setup(g, 1, tc);
-  // forward: load natural x, DIF, write natural (permute via k1_of_pos)
-  // inverse: load natural x, permute into DIF order, DIT, write natural
-  const int nc = g.n2 * g.h3;
-  const size_t base = (size_t)b * g.n1 * nc;
-  double2* d = s.slots;
-  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
-    const int p = i / tc, c = i - p * tc;
-    const int col = c0 + c;
-    const int r = inv ? k1_of_pos[p] : p;
-    d[i] = (col < nc) ? in[base + (size_t)r * nc + col] : make_double2(0.0, 0.0);
-  }
+k_col_fft(GridDev g, const double2* in, double2* out, int tc, int inv) {
+  const int b = blockIdx.y, c0 = blockIdx.x * (TCC ? TCC : tc);
+  const ColShape<N1C, TCC> sh(g, tc);
+  ColSmem s = col_smem_setup(g, sh, 1);
+  load_col_tile(g, s, sh, 1, 0, in, b, c0, inv ? g.k1pos : nullptr);
   __syncthreads();
-  col_fft(g, s, 1, tc, inv != 0);
-  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
-    const int p = i / tc, c = i - p * tc;
-    const int col = c0 + c;
-    const int r = inv ? p : k1_of_pos[p];
-    if (col < nc) out[base + (size_t)r * nc + col] = d[i];
-  }
+  if (inv) col_fft<true>(g, s, sh, 1, 0, 1);
+  else col_fft<false>(g, s, sh, 1, 0, 1);
+  store_col_tile(g, s, sh, 1, 0, out, b, c0, inv ? nullptr : g.k1pos);
 }
 
 // ================================================ FMT weights ===========
@@ -283,69 +334,92 @@ struct Weights {
   double v[3];    // kwv2 = -i * kw3 * k  -> stored as the real factor of -i
 };
 
-__device__ __forceinline__ Weights fmt_weights(double kx, double ky, double kz, double sl, double R,
-                                               int nqx, int nqy, int nqz) {
-  Weights w;
-  double kk = sqrt(kx * kx + ky * ky + kz * kz);
-  double om = kk * R;
-  if (fabs(om) <= 1e-8) {  // np.isclose(omega, 0)
-    w.w0 = sl;
-    w.w3 = (4.0 * M_PI * R * R * R / 3.0) * sl;
-    w.v[0] = w.v[1] = w.v[2] = 0.0;
-    return w;
-  }
+__device__ __forceinline__ double2 fmt_scalar_weights(double kx, double ky, double kz, double sl, double R) {
+  const double kk = sqrt(kx * kx + ky * ky + kz * kz);
+  const double om = kk * R;
+  if (fabs(om) <= 1e-8)  // np.isclose(omega, 0)
+    return make_double2(sl, (4.0 * M_PI * R * R * R / 3.0) * sl);
   double sn, cs;
   sincos(om, &sn, &cs);
-  double y = M_PI * (om / M_PI);
-  double j0 = sin(y) / y;  // np.sinc(omega / pi)
-  double j2 = 3.0 * (sn - om * cs) / (om * om * om);
-  w.w0 = j0 * sl;
-  w.w3 = (4.0 * M_PI * R * R * R / 3.0) * (j2 * sl);
-  w.v[0] = nqx ? 0.0 : w.w3 * kx;
-  w.v[1] = nqy ? 0.0 : w.w3 * ky;
-  w.v[2] = nqz ? 0.0 : w.w3 * kz;
+  const double y = M_PI * (om / M_PI);
+  const double j0 = sin(y) / y;  // np.sinc(omega / pi)
+  const double j2 = 3.0 * (sn - om * cs) / (om * om * om);
+  return make_double2(j0 * sl, (4.0 * M_PI * R * R * R / 3.0) * (j2 * sl));
+}
+
+// Weights at (x position p1, column col); from the table when given.
+__device__ __forceinline__ Weights fmt_weights_at(const GridDev& g, const double2* __restrict__ wtab, int p1,
+                                                  int col, double R) {
+  const int p2 = col / g.h3, p3 = col - p2 * g.h3;
+  const double kx = g.kp1[p1], ky = g.kp2[p2], kz = g.kp3[p3];
+  double2 ws;
+  if (wtab) {
+    ws = __ldg(wtab + (size_t)p1 * g.n2 * g.h3 + col);
+  } else {
+    const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];
+    ws = fmt_scalar_weights(kx, ky, kz, sl, R);
+  }
+  Weights w;
+  w.w0 = ws.x;
+  w.w3 = ws.y;
+  const bool zero = (kx == 0.0 && ky == 0.0 && kz == 0.0);
+  w.v[0] = (zero || g.nq1[p1]) ? 0.0 : w.w3 * kx;
+  w.v[1] = (zero || g.nq2[p2]) ? 0.0 : w.w3 * ky;
+  w.v[2] = (zero || g.nq3[p3]) ? 0.0 : w.w3 * kz;
   return w;
+}
+
+// Weight table (w0, w3) in the column-pass layout [x DIF position][column].
+__global__ void k_fmt_weights(GridDev g, double R, double2* __restrict__ wtab) {
+  const int nc = g.n2 * g.h3;
+  const long long tot = (long long)g.n1 * nc;
+  const long long idx = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (idx >= tot) return;
+  const int p1 = (int)(idx / nc), col = (int)(idx - (long long)p1 * nc);
+  const int p2 = col / g.h3, p3 = col - p2 * g.h3;
+  const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];
+  wtab[idx] = fmt_scalar_weights(g.kp1[p1], g.kp2[p2], g.kp3[p3], sl, R);
 }
 
 // ================================== column pass 1: rho_hat -> 5 fields ==
 // Outputs (field stride fsw): 0 = n0 (w0), 1 = n3 (w3), 2..4 = nv2 (x, y, z).
+template <int N1C, int TCC>
 __global__ void __launch_bounds__(CMM_COL_THREADS)
 k_col_weights(GridDev g, const int* __restrict__ active, double R, double inv_npts,
               const double2* __restrict__ rhohat, double2* __restrict__ wout, size_t fsw,
-              const double2* __restrict__ kst, double* __restrict__ part, int nslot_part,
-              int want_value, int tc) {
-  const int b = blockIdx.y, tile = blockIdx.x, c0 = tile * tc;
+              const double2* __restrict__ kst, const double2* __restrict__ wtab, double* __restrict__ part,
+              int nslot_part, int want_value, int tc) {
+  const int b = blockIdx.y, tile = blockIdx.x;
   if (active && !active[b]) return;
-  ColSmem s = col_smem_setup(g, 5, tc);
-  load_col_tile(g, s, 0, rhohat, b, c0, tc);
+  const ColShape<N1C, TCC> sh(g, tc);
+  const int c0 = tile * sh.tc;
+  ColSmem s = col_smem_setup(g, sh, 5);
+  load_col_tile(g, s, sh, 5, 0, rhohat, b, c0, nullptr);
   __syncthreads();
-  col_fft(g, s, 1, tc, false);
+  col_fft<false>(g, s, sh, 5, 0, 1);
   const int nc = g.n2 * g.h3;
   double mfa = 0.0;
-  const size_t per = (size_t)g.n1 * tc;
-  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
-    const int p1 = i / tc, c = i - p1 * tc;
+  for (int i = threadIdx.x; i < sh.n1 * sh.tc; i += blockDim.x) {
+    const int p1 = i / sh.tc, c = i - p1 * sh.tc;
     const int col = c0 + c;
     if (col >= nc) continue;
-    const int p2 = col / g.h3, p3 = col - p2 * g.h3;
-    double2 F = s.slots[i];
-    const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];
-    Weights w = fmt_weights(g.kp1[p1], g.kp2[p2], g.kp3[p3], sl, R, g.nq1[p1], g.nq2[p2], g.nq3[p3]);
+    double2 F = cel(s, sh, 5, 0, p1, c);
+    const Weights w = fmt_weights_at(g, wtab, p1, col, R);
     if (want_value) {
-      double2 K = __ldg(kst + (size_t)p1 * nc + col);
-      mfa += g.wt3[p3] * (F.x * F.x + F.y * F.y) * K.x;
+      const double2 K = __ldg(kst + (size_t)p1 * nc + col);
+      mfa += g.wt3[col - (col / g.h3) * g.h3] * (F.x * F.x + F.y * F.y) * K.x;
     }
     F = cscale(F, inv_npts);
-    s.slots[1 * per + i] = cscale(F, w.w3);
+    cel(s, sh, 5, 1, p1, c) = cscale(F, w.w3);
     // -i * v * F
-    s.slots[2 * per + i] = make_double2(F.y * w.v[0], -F.x * w.v[0]);
-    s.slots[3 * per + i] = make_double2(F.y * w.v[1], -F.x * w.v[1]);
-    s.slots[4 * per + i] = make_double2(F.y * w.v[2], -F.x * w.v[2]);
-    s.slots[i] = cscale(F, w.w0);
+    cel(s, sh, 5, 2, p1, c) = make_double2(F.y * w.v[0], -F.x * w.v[0]);
+    cel(s, sh, 5, 3, p1, c) = make_double2(F.y * w.v[1], -F.x * w.v[1]);
+    cel(s, sh, 5, 4, p1, c) = make_double2(F.y * w.v[2], -F.x * w.v[2]);
+    cel(s, sh, 5, 0, p1, c) = cscale(F, w.w0);
   }
   __syncthreads();
-  col_fft(g, s, 5, tc, true);
-  for (int f = 0; f < 5; ++f) store_col_tile(g, s, f, wout + f * fsw, b, c0, tc);
+  col_fft<true>(g, s, sh, 5, 0, 5);
+  for (int f = 0; f < 5; ++f) store_col_tile(g, s, sh, 5, f, wout + f * fsw, b, c0, nullptr);
   if (want_value) {
     __shared__ double red[32];
     double t = block_sum(mfa, red);
@@ -355,52 +429,47 @@ k_col_weights(GridDev g, const int* __restrict__ active, double R, double inv_np
 
 // ======================== column pass 2: dPhi spectra -> C1 spectrum ====
 // Inputs: 5 dPhi spectra (field stride fsg): g_s (pairs with w0), g3 (w3),
-// gv (x,y,z, pairs with kwv2); rho_hat for the MFA term.
+// gv (x,y,z, pairs with kwv2); rho_hat for the MFA term.  gin == NULL: MFA only.
+template <int N1C, int TCC>
 __global__ void __launch_bounds__(CMM_COL_THREADS)
 k_col_backconv(GridDev g, const int* __restrict__ active, double R, double scale,
                const double2* __restrict__ gin, size_t fsg, const double2* __restrict__ rhohat,
-               const double2* __restrict__ kst, double2* __restrict__ chat, int tc) {
-  const int b = blockIdx.y, c0 = blockIdx.x * tc;
+               const double2* __restrict__ kst, const double2* __restrict__ wtab, double2* __restrict__ chat,
+               int tc) {
+  const int b = blockIdx.y;
   if (active && !active[b]) return;
-  ColSmem s = col_smem_setup(g, 6, tc);
+  const ColShape<N1C, TCC> sh(g, tc);
+  const int c0 = blockIdx.x * sh.tc;
+  ColSmem s = col_smem_setup(g, sh, 6);
   const bool hs = (gin != nullptr);
   if (hs)
-    for (int f = 0; f < 5; ++f) load_col_tile(g, s, f, gin + f * fsg, b, c0, tc);
-  load_col_tile(g, s, 5, rhohat, b, c0, tc);
+    for (int f = 0; f < 5; ++f) load_col_tile(g, s, sh, 6, f, gin + f * fsg, b, c0, nullptr);
+  load_col_tile(g, s, sh, 6, 5, rhohat, b, c0, nullptr);
   __syncthreads();
-  if (hs) {
-    col_fft(g, s, 6, tc, false);
-  } else {
-    // only the rho_hat slot: transform it alone (slot 5 viewed as slot 0 of a shifted base)
-    ColSmem s5 = s;
-    s5.slots = s.slots + (size_t)5 * g.n1 * tc;
-    col_fft(g, s5, 1, tc, false);
-  }
+  if (hs) col_fft<false>(g, s, sh, 6, 0, 6);
+  else col_fft<false>(g, s, sh, 6, 5, 1);
   const int nc = g.n2 * g.h3;
-  const size_t per = (size_t)g.n1 * tc;
-  for (int i = threadIdx.x; i < g.n1 * tc; i += blockDim.x) {
-    const int p1 = i / tc, c = i - p1 * tc;
+  for (int i = threadIdx.x; i < sh.n1 * sh.tc; i += blockDim.x) {
+    const int p1 = i / sh.tc, c = i - p1 * sh.tc;
     const int col = c0 + c;
     if (col >= nc) continue;
-    const int p2 = col / g.h3, p3 = col - p2 * g.h3;
     double2 acc = make_double2(0.0, 0.0);
     if (hs) {
-      const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];
-      Weights w = fmt_weights(g.kp1[p1], g.kp2[p2], g.kp3[p3], sl, R, g.nq1[p1], g.nq2[p2], g.nq3[p3]);
-      acc = cadd(cscale(s.slots[i], w.w0), cscale(s.slots[per + i], w.w3));
+      const Weights w = fmt_weights_at(g, wtab, p1, col, R);
+      acc = cadd(cscale(cel(s, sh, 6, 0, p1, c), w.w0), cscale(cel(s, sh, 6, 1, p1, c), w.w3));
       // - sum_j G_j * (-i v_j) = + i * sum_j v_j G_j
       double2 gv = make_double2(0.0, 0.0);
-      for (int a = 0; a < 3; ++a) gv = cadd(gv, cscale(s.slots[(2 + a) * per + i], w.v[a]));
+      for (int a = 0; a < 3; ++a) gv = cadd(gv, cscale(cel(s, sh, 6, 2 + a, p1, c), w.v[a]));
       acc = cadd(acc, make_double2(-gv.y, gv.x));
       acc = cscale(acc, scale);
     }
-    double2 K = __ldg(kst + (size_t)p1 * nc + col);
-    acc = cadd(acc, cmul(s.slots[5 * per + i], K));
-    s.slots[i] = acc;
+    const double2 K = __ldg(kst + (size_t)p1 * nc + col);
+    acc = cadd(acc, cmul(cel(s, sh, 6, 5, p1, c), K));
+    cel(s, sh, 6, 0, p1, c) = acc;
   }
   __syncthreads();
-  col_fft(g, s, 1, tc, true);
-  store_col_tile(g, s, 0, chat, b, c0, tc);
+  col_fft<true>(g, s, sh, 6, 0, 1);
+  store_col_tile(g, s, sh, 6, 0, chat, b, c0, nullptr);
 }
 
 // ===================================== plane pass: dPhi/dn (White-Bear) ==
@@ -488,26 +557,28 @@ __device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, 
   return o;
 }
 
+template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_PLANE_THREADS)
 k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version,
             const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
             double* __restrict__ part, int nslot_part, int want) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
-  PlaneSmem s = plane_smem_setup(g, 5);
-  const size_t poff = ((size_t)b * g.n1 + i1) * g.n2 * g.h3;
-  load_spec_planes(g, s, 5, win, poff, fsw);
+  PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 5);
+  const PlaneShape<N2C, M3C> sh(g);
+  const size_t poff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3;
+  load_spec_planes<N2C, M3C>(g, s, 5, win, poff, fsw);
   __syncthreads();
-  plane_inverse(g, s, 5);
+  plane_inverse<N2C, M3C>(g, s, 5);
   double phi = 0.0, n3max = -INFINITY;
   const bool do_c1 = (want & 1) != 0;
-  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
-    const int r = i / g.n3, j = i - r * g.n3;
-    double& a0 = rel(s, g, 0, r, j);
-    double& a3 = rel(s, g, 1, r, j);
-    double& ax = rel(s, g, 2, r, j);
-    double& ay = rel(s, g, 3, r, j);
-    double& az = rel(s, g, 4, r, j);
+  for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
+    const int r = i / sh.n3, j = i - r * sh.n3;
+    double& a0 = rel(s, sh, 5, 0, r, j);
+    double& a3 = rel(s, sh, 5, 1, r, j);
+    double& ax = rel(s, sh, 5, 2, r, j);
+    double& ay = rel(s, sh, 5, 3, r, j);
+    double& az = rel(s, sh, 5, 4, r, j);
     n3max = fmax(n3max, a3);
     PhiOut o = fmt_point(a0, a3, ax, ay, az, R, version);
     phi += o.phi;
@@ -527,8 +598,8 @@ k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version,
   }
   if (!do_c1) return;
   __syncthreads();
-  plane_forward(g, s, 5);
-  store_spec_planes(g, s, 5, gout, poff, fsg);
+  plane_forward<N2C, M3C>(g, s, 5);
+  store_spec_planes<N2C, M3C>(g, s, 5, gout, poff, fsg);
 }
 
 // ========================================== plane pass: solver updates ==
@@ -557,6 +628,7 @@ __device__ inline void stats_store(const PlaneStats& st, double* part, int b, in
 }
 
 // Static Picard step fused with the C1 inverse and the forward of rho'.
+template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_PLANE_THREADS)
 k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
                double beta, double lambda3, double thr, const double2* __restrict__ chat,
@@ -565,19 +637,20 @@ k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restri
                double* __restrict__ part, int nslot_part) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
-  PlaneSmem s = plane_smem_setup(g, 1);
-  const size_t poff = ((size_t)b * g.n1 + i1) * g.n2 * g.h3;
-  load_spec_planes(g, s, 1, chat, poff, 0);
+  PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
+  const PlaneShape<N2C, M3C> sh(g);
+  const size_t poff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3;
+  load_spec_planes<N2C, M3C>(g, s, 1, chat, poff, 0);
   __syncthreads();
-  plane_inverse(g, s, 1);
+  plane_inverse<N2C, M3C>(g, s, 1);
   const double fug = params[b * 4 + 0], a = params[b * 4 + 1];
-  const size_t roff = ((size_t)b * g.n1 + i1) * g.n2 * g.n3;
-  const double* Vp = V + b * vstride + (size_t)i1 * g.n2 * g.n3;
+  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
+  const double* Vp = V + b * vstride + (size_t)i1 * sh.n2 * sh.n3;
   PlaneStats st = {0, 0, 0, 0, 0};
   double res2 = 0.0, gnf = 0.0;
-  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
-    const int r = i / g.n3, j = i - r * g.n3;
-    double& cell = rel(s, g, 0, r, j);
+  for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
+    const int r = i / sh.n3, j = i - r * sh.n3;
+    double& cell = rel(s, sh, 1, 0, r, j);
     const double v = __ldg(Vp + i);
     const double C1 = cell + v;
     const double G = beta * exp(-beta * C1) * fug;
@@ -599,13 +672,14 @@ k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restri
   }
   stats_store(st, part, b, nslot_part, i1);
   __syncthreads();
-  plane_forward(g, s, 1);
-  store_spec_planes(g, s, 1, rhohat_out, poff, 0);
+  plane_forward<N2C, M3C>(g, s, 1);
+  store_spec_planes<N2C, M3C>(g, s, 1, rhohat_out, poff, 0);
 }
 
 struct HistPtrs { const double* p[CMM_MAX_HIST]; };
 
 // Residual r = G(C1) - rho with the Gram row against stored residuals.
+template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_PLANE_THREADS)
 k_plane_residual(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
                  double beta, const double2* __restrict__ chat, const double* __restrict__ rho,
@@ -614,22 +688,23 @@ k_plane_residual(GridDev g, const int* __restrict__ active, const double* __rest
                  int nslot_part) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
-  PlaneSmem s = plane_smem_setup(g, 1);
-  const size_t poff = ((size_t)b * g.n1 + i1) * g.n2 * g.h3;
-  load_spec_planes(g, s, 1, chat, poff, 0);
+  PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
+  const PlaneShape<N2C, M3C> sh(g);
+  const size_t poff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3;
+  load_spec_planes<N2C, M3C>(g, s, 1, chat, poff, 0);
   __syncthreads();
-  plane_inverse(g, s, 1);
+  plane_inverse<N2C, M3C>(g, s, 1);
   const double fug = params[b * 4 + 0];
-  const size_t roff = ((size_t)b * g.n1 + i1) * g.n2 * g.n3;
-  const size_t hoff = (size_t)b * hstride + (size_t)i1 * g.n2 * g.n3;
-  const double* Vp = V + b * vstride + (size_t)i1 * g.n2 * g.n3;
+  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
+  const size_t hoff = (size_t)b * hstride + (size_t)i1 * sh.n2 * sh.n3;
+  const double* Vp = V + b * vstride + (size_t)i1 * sh.n2 * sh.n3;
   double res2 = 0.0, gnf = 0.0;
   double gram[CMM_MAX_HIST];
 #pragma unroll
   for (int j = 0; j < CMM_MAX_HIST; ++j) gram[j] = 0.0;
-  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
-    const int r = i / g.n3, j = i - r * g.n3;
-    const double C1 = rel(s, g, 0, r, j) + __ldg(Vp + i);
+  for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
+    const int r = i / sh.n3, j = i - r * sh.n3;
+    const double C1 = rel(s, sh, 1, 0, r, j) + __ldg(Vp + i);
     const double G = beta * exp(-beta * C1) * fug;
     const double x = __ldg(rho + roff + i);
     const double rr = G - x;
@@ -654,6 +729,7 @@ k_plane_residual(GridDev g, const int* __restrict__ active, const double* __rest
 struct FieldPtrs { const double* p[CMM_MAX_FIELDS]; long long stride[CMM_MAX_FIELDS]; };
 
 // rho' = sum_j c_j field_j, clipped, with stats and the forward transform.
+template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_PLANE_THREADS)
 k_plane_mix(GridDev g, const int* __restrict__ active, const double* __restrict__ coef,
             FieldPtrs fields, int nfield, int clip, double thr, double lambda3, const double* __restrict__ ref,
@@ -662,17 +738,18 @@ k_plane_mix(GridDev g, const int* __restrict__ active, const double* __restrict_
             double* __restrict__ part, int nslot_part) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
-  PlaneSmem s = plane_smem_setup(g, 1);
-  const size_t plane = (size_t)i1 * g.n2 * g.n3;
-  const size_t roff = (size_t)b * g.n1 * g.n2 * g.n3 + plane;
+  PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
+  const PlaneShape<N2C, M3C> sh(g);
+  const size_t plane = (size_t)i1 * sh.n2 * sh.n3;
+  const size_t roff = (size_t)b * g.n1 * sh.n2 * sh.n3 + plane;
   const double* Vp = V + b * vstride + plane;
   const double* Rp = ref + b * refstride + plane;
   double c[CMM_MAX_FIELDS];
 #pragma unroll
   for (int j = 0; j < CMM_MAX_FIELDS; ++j) c[j] = (j < nfield) ? coef[b * CMM_MAX_FIELDS + j] : 0.0;
   PlaneStats st = {0, 0, 0, 0, 0};
-  for (int i = threadIdx.x; i < g.n2 * g.n3; i += blockDim.x) {
-    const int r = i / g.n3, j = i - r * g.n3;
+  for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
+    const int r = i / sh.n3, j = i - r * sh.n3;
     double x = 0.0;
 #pragma unroll
     for (int f = 0; f < CMM_MAX_FIELDS; ++f)
@@ -681,12 +758,12 @@ k_plane_mix(GridDev g, const int* __restrict__ active, const double* __restrict_
     else if (clip == CMM_CLIP_PICARD && x < thr) x = 0.0;
     rho_out[roff + i] = x;
     stats_point(st, x, __ldg(Rp + i), __ldg(Vp + i), lambda3);
-    rel(s, g, 0, r, j) = x;
+    rel(s, sh, 1, 0, r, j) = x;
   }
   stats_store(st, part, b, nslot_part, i1);
   __syncthreads();
-  plane_forward(g, s, 1);
-  store_spec_planes(g, s, 1, rhohat_out, ((size_t)b * g.n1 + i1) * g.n2 * g.h3, 0);
+  plane_forward<N2C, M3C>(g, s, 1);
+  store_spec_planes<N2C, M3C>(g, s, 1, rhohat_out, ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3, 0);
 }
 
 // ============================================================ finalize ==
@@ -716,8 +793,51 @@ static int set_smem(const void* fn, size_t bytes) {
   return CMM_OK;
 }
 
-// Column tile width: >= 8 columns (128 B rows) when it fits, scaled down for long x.
+// Shape specialisations compiled with compile-time transform lengths.
+static int plane_kind(const cmm_grid* g) {
+  if (g->n2 == 64 && g->m3 == 32) return 1;
+  if (g->n2 == 32 && g->m3 == 16) return 2;
+  return 0;
+}
+static int col_kind(const cmm_grid* g) {
+  if (g->n1 == 64) return 1;
+  if (g->n1 == 32) return 2;
+  return 0;
+}
+
+#define LAUNCH_PLANE(kind, kern, grd, smem, st, ...)                                      \
+  do {                                                                                   \
+    int rc_;                                                                             \
+    if ((kind) == 1) {                                                                   \
+      if ((rc_ = set_smem((const void*)kern<64, 32>, smem))) return rc_;                \
+      kern<64, 32><<<grd, CMM_PLANE_THREADS, smem, st>>>(__VA_ARGS__);                   \
+    } else if ((kind) == 2) {                                                            \
+      if ((rc_ = set_smem((const void*)kern<32, 16>, smem))) return rc_;                \
+      kern<32, 16><<<grd, CMM_PLANE_THREADS, smem, st>>>(__VA_ARGS__);                   \
+    } else {                                                                             \
+      if ((rc_ = set_smem((const void*)kern<0, 0>, smem))) return rc_;                  \
+      kern<0, 0><<<grd, CMM_PLANE_THREADS, smem, st>>>(__VA_ARGS__);                     \
+    }                                                                                    \
+  } while (0)
+
+#define LAUNCH_COL(kind, kern, grd, smem, st, ...)                                        \
+  do {                                                                                   \
+    int rc_;                                                                             \
+    if ((kind) == 1) {                                                                   \
+      if ((rc_ = set_smem((const void*)kern<64, 16>, smem))) return rc_;                \
+      kern<64, 16><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                     \
+    } else if ((kind) == 2) {                                                            \
+      if ((rc_ = set_smem((const void*)kern<32, 16>, smem))) return rc_;                \
+      kern<32, 16><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                     \
+    } else {                                                                             \
+      if ((rc_ = set_smem((const void*)kern<0, 0>, smem))) return rc_;                  \
+      kern<0, 0><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                       \
+    }                                                                                    \
+  } while (0)
+
+// Column tile width: 16 columns (256 B rows) when it fits, fewer for long x.
 static int col_tile(const cmm_grid* g, int nslot) {
+  if (col_kind(g)) return 16;
   int tc = 16;
   while (tc > 1 && col_smem_bytes(g->n1, tc, nslot) > 200 * 1024) tc /= 2;
   return tc;
@@ -729,62 +849,58 @@ extern "C" int cmm_plane_smem_bytes(const cmm_grid* g, int nslot, size_t* bytes)
   return CMM_OK;
 }
 
+static int col_fft_3d(const cmm_grid* g, int batch, const double2* in, double2* out, int inv, cudaStream_t st) {
+  const int tc = col_tile(g, 1);
+  const size_t cs = col_smem_bytes(g->n1, tc, 1);
+  const int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
+  LAUNCH_COL(col_kind(g), k_col_fft, dim3(ntile, batch), cs, st, g->dev, in, out, tc, inv);
+  return last_err();
+}
+
 extern "C" int cmm_rfft3d(const cmm_grid* g, int batch, const double* d_in, double* d_spec, void* stream) {
   if (!g || !d_in || !d_spec || batch < 1) return CMM_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  int rc = set_smem((const void*)k_plane_r2c, ps);
-  if (rc) return rc;
-  k_plane_r2c<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, st>>>(g->dev, d_in, (double2*)d_spec);
-  int tc = col_tile(g, 1);
-  size_t cs = col_smem_bytes(g->n1, tc, 1);
-  rc = set_smem((const void*)k_col_fft, cs);
-  if (rc) return rc;
-  const int* k1 = g->dev.k1pos;
-  int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
-  k_col_fft<<<dim3(ntile, batch), CMM_COL_THREADS, cs, st>>>(g->dev, (const double2*)d_spec, (double2*)d_spec, tc, 0, k1);
-  return last_err();
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  LAUNCH_PLANE(plane_kind(g), k_plane_r2c, dim3(g->n1, batch), ps, st, g->dev, d_in, (double2*)d_spec);
+  return col_fft_3d(g, batch, (const double2*)d_spec, (double2*)d_spec, 0, st);
 }
 
 extern "C" int cmm_irfft3d(const cmm_grid* g, int batch, double* d_spec, double* d_out, void* stream) {
   if (!g || !d_spec || !d_out || batch < 1) return CMM_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  int tc = col_tile(g, 1);
-  size_t cs = col_smem_bytes(g->n1, tc, 1);
-  int rc = set_smem((const void*)k_col_fft, cs);
+  int rc = col_fft_3d(g, batch, (const double2*)d_spec, (double2*)d_spec, 1, st);  // in place (consumed)
   if (rc) return rc;
-  const int* k1 = g->dev.k1pos;
-  int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
-  // in place on the caller's spectrum (it is consumed)
-  k_col_fft<<<dim3(ntile, batch), CMM_COL_THREADS, cs, st>>>(g->dev, (const double2*)d_spec, (double2*)d_spec, tc, 1, k1);
-  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  rc = set_smem((const void*)k_plane_c2r, ps);
-  if (rc) return rc;
-  k_plane_c2r<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, st>>>(g->dev, (const double2*)d_spec, d_out);
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  LAUNCH_PLANE(plane_kind(g), k_plane_c2r, dim3(g->n1, batch), ps, st, g->dev, (const double2*)d_spec, d_out);
   return last_err();
 }
 
 extern "C" int cmm_rfft_yz(const cmm_grid* g, int batch, const double* d_in, double* d_spec, void* stream) {
   if (!g || !d_in || !d_spec || batch < 1) return CMM_ERR_ARG;
-  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  int rc = set_smem((const void*)k_plane_r2c, ps);
-  if (rc) return rc;
-  k_plane_r2c<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(g->dev, d_in, (double2*)d_spec);
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  LAUNCH_PLANE(plane_kind(g), k_plane_r2c, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_in,
+               (double2*)d_spec);
   return last_err();
 }
 
 extern "C" int cmm_irfft_yz(const cmm_grid* g, int batch, const double* d_spec, double* d_out, void* stream) {
   if (!g || !d_spec || !d_out || batch < 1) return CMM_ERR_ARG;
-  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  int rc = set_smem((const void*)k_plane_c2r, ps);
-  if (rc) return rc;
-  k_plane_c2r<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(g->dev, (const double2*)d_spec, d_out);
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  LAUNCH_PLANE(plane_kind(g), k_plane_c2r, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev,
+               (const double2*)d_spec, d_out);
+  return last_err();
+}
+
+extern "C" int cmm_fmt_weights(const cmm_grid* g, double R, double* d_wtab, void* stream) {
+  if (!g || !d_wtab) return CMM_ERR_ARG;
+  const long long tot = (long long)g->n1 * g->n2 * g->h3;
+  k_fmt_weights<<<(int)((tot + 255) / 256), 256, 0, (cudaStream_t)stream>>>(g->dev, R, (double2*)d_wtab);
   return last_err();
 }
 
 extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, double R, double beta,
-                          int version, const double* d_kst, const double* d_rhohat, double* d_chat,
-                          double* d_work, double* d_part, int nslot, int want, void* stream) {
+                          int version, const double* d_kst, const double* d_wtab, const double* d_rhohat,
+                          double* d_chat, double* d_work, double* d_part, int nslot, int want, void* stream) {
   if (!g || batch < 1 || !d_kst || !d_rhohat || !d_work || !d_part) return CMM_ERR_ARG;
   if ((want & 1) && !d_chat) return CMM_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
@@ -792,36 +908,28 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
   double2* wbuf = (double2*)d_work;          // 5 weighted-density spectra
   double2* gbuf = wbuf + 5 * fs;             // 5 dPhi spectra
   const double npts = (double)g->n1 * g->n2 * g->n3;
-  int tc = col_tile(g, 6);
-  int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
+  const int tc = col_tile(g, 6);
+  const int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
   if (nslot < g->n1 || nslot < ntile) return CMM_ERR_WORKSPACE;
-  size_t cs5 = col_smem_bytes(g->n1, tc, 5), cs6 = col_smem_bytes(g->n1, tc, 6);
-  int rc;
+  const size_t cs5 = col_smem_bytes(g->n1, tc, 5), cs6 = col_smem_bytes(g->n1, tc, 6);
+  const double2* wt = (const double2*)d_wtab;
+  const int ck = col_kind(g);
   if (version & CMM_NOHS) {  // MFA term alone: one column pass
     if (!(want & 1)) return CMM_ERR_ARG;
-    rc = set_smem((const void*)k_col_backconv, cs6);
-    if (rc) return rc;
-    k_col_backconv<<<dim3(ntile, batch), CMM_COL_THREADS, cs6, st>>>(
-        g->dev, d_active, R, 1.0 / (beta * npts), nullptr, fs, (const double2*)d_rhohat,
-        (const double2*)d_kst, (double2*)d_chat, tc);
+    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), cs6, st, g->dev, d_active, R, 1.0 / (beta * npts),
+               (const double2*)nullptr, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt,
+               (double2*)d_chat, tc);
     return last_err();
   }
-  rc = set_smem((const void*)k_col_weights, cs5);
-  if (rc) return rc;
-  k_col_weights<<<dim3(ntile, batch), CMM_COL_THREADS, cs5, st>>>(
-      g->dev, d_active, R, 1.0 / npts, (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst,
-      d_part, nslot, (want & 2) ? 1 : 0, tc);
-  size_t ps = plane_smem_bytes(g->n2, g->n3, 5);
-  rc = set_smem((const void*)k_plane_fmt, ps);
-  if (rc) return rc;
-  k_plane_fmt<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, st>>>(g->dev, d_active, R, version, wbuf, fs,
-                                                                gbuf, fs, d_part, nslot, want);
+  LAUNCH_COL(ck, k_col_weights, dim3(ntile, batch), cs5, st, g->dev, d_active, R, 1.0 / npts,
+             (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0, tc);
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 5);
+  LAUNCH_PLANE(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), ps, st, g->dev, d_active, R, version,
+               (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
   if (want & 1) {
-    rc = set_smem((const void*)k_col_backconv, cs6);
-    if (rc) return rc;
-    k_col_backconv<<<dim3(ntile, batch), CMM_COL_THREADS, cs6, st>>>(
-        g->dev, d_active, R, 1.0 / (beta * npts), gbuf, fs, (const double2*)d_rhohat,
-        (const double2*)d_kst, (double2*)d_chat, tc);
+    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), cs6, st, g->dev, d_active, R, 1.0 / (beta * npts),
+               (const double2*)gbuf, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt, (double2*)d_chat,
+               tc);
   }
   return last_err();
 }
@@ -834,12 +942,10 @@ extern "C" int cmm_picard_static_step(const cmm_grid* g, int batch, const int* d
   if (!g || batch < 1 || !d_params || !d_chat || !d_rho || !d_V || !d_rho_out || !d_rhohat_out || !d_part)
     return CMM_ERR_ARG;
   if (nslot < g->n1) return CMM_ERR_WORKSPACE;
-  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  int rc = set_smem((const void*)k_plane_picard, ps);
-  if (rc) return rc;
-  k_plane_picard<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(
-      g->dev, d_active, d_params, beta, lambda3, thr, (const double2*)d_chat, d_rho, d_V, vstride,
-      d_rho_out, (double2*)d_rhohat_out, d_part, nslot);
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  LAUNCH_PLANE(plane_kind(g), k_plane_picard, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_active,
+               d_params, beta, lambda3, thr, (const double2*)d_chat, d_rho, d_V, vstride, d_rho_out,
+               (double2*)d_rhohat_out, d_part, nslot);
   return last_err();
 }
 
@@ -852,12 +958,10 @@ extern "C" int cmm_residual_step(const cmm_grid* g, int batch, const int* d_acti
   if (nslot < g->n1) return CMM_ERR_WORKSPACE;
   HistPtrs hp;
   for (int j = 0; j < CMM_MAX_HIST; ++j) hp.p[j] = (j < nhist) ? d_hist[j] : nullptr;
-  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  int rc = set_smem((const void*)k_plane_residual, ps);
-  if (rc) return rc;
-  k_plane_residual<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(
-      g->dev, d_active, d_params, beta, (const double2*)d_chat, d_rho, d_V, vstride, d_r_out, hp, nhist,
-      hstride, d_part, nslot);
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  LAUNCH_PLANE(plane_kind(g), k_plane_residual, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_active,
+               d_params, beta, (const double2*)d_chat, d_rho, d_V, vstride, d_r_out, hp, nhist, hstride, d_part,
+               nslot);
   return last_err();
 }
 
@@ -875,12 +979,10 @@ extern "C" int cmm_mix_step(const cmm_grid* g, int batch, const int* d_active, c
     fp.p[j] = (j < nfield) ? d_fields[j] : nullptr;
     fp.stride[j] = (j < nfield) ? fstride[j] : 0;
   }
-  size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  int rc = set_smem((const void*)k_plane_mix, ps);
-  if (rc) return rc;
-  k_plane_mix<<<dim3(g->n1, batch), CMM_PLANE_THREADS, ps, (cudaStream_t)stream>>>(
-      g->dev, d_active, d_coef, fp, nfield, clip, thr, lambda3, d_ref, refstride, d_V, vstride, d_rho_out,
-      (double2*)d_rhohat_out, d_part, nslot);
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  LAUNCH_PLANE(plane_kind(g), k_plane_mix, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_active, d_coef,
+               fp, nfield, clip, thr, lambda3, d_ref, refstride, d_V, vstride, d_rho_out, (double2*)d_rhohat_out,
+               d_part, nslot);
   return last_err();
 }
 

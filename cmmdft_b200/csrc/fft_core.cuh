@@ -236,3 +236,83 @@ __device__ void fft_pencils(double2* s, const FftAxis& ax, const double2* tw, in
     __syncthreads();
   }
 }
+
+// ------------------------------------------------------------------------
+// Uniform pencil sets: pencil p starts at s + p * pstride, element j at
+// + j * estride.  Threads take consecutive pencils at the same butterfly
+// index (conflict-free for unit-stride pencils and for the odd row strides
+// used here; every thread of a warp reads the same twiddle).
+// ------------------------------------------------------------------------
+
+// Radix plan of a power of two N: 8-stages, then one 4 or 2 stage.
+template <int N>
+struct Pow2Plan {
+  static constexpr int log2n = (N >= 2 ? 1 : 0) + (N >= 4 ? 1 : 0) + (N >= 8 ? 1 : 0) + (N >= 16 ? 1 : 0) +
+                               (N >= 32 ? 1 : 0) + (N >= 64 ? 1 : 0) + (N >= 128 ? 1 : 0) + (N >= 256 ? 1 : 0) +
+                               (N >= 512 ? 1 : 0) + (N >= 1024 ? 1 : 0);
+  static constexpr int n8 = log2n / 3;
+  static constexpr int tail = 1 << (log2n - 3 * n8);   // 1, 2 or 4
+  static constexpr int nstage = n8 + (tail > 1 ? 1 : 0);
+  __host__ __device__ static constexpr int radix(int s) { return s < n8 ? 8 : tail; }
+  __host__ __device__ static constexpr int span(int s) {
+    int L = N;
+    for (int i = 0; i < s; ++i) L /= (i < n8 ? 8 : tail);
+    return L;
+  }
+};
+
+template <bool INV, int R, int L, int N>
+__device__ __forceinline__ void stage_ct(double2* s, const double2* tw, int twmul, int npencil, int pstride,
+                                         int estride) {
+  constexpr int sR = L / R;
+  constexpr int nb = N / R;
+  const int tstep = (N / L) * twmul;
+  const int total = npencil * nb;
+  const int es = sR * estride;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int j = t / npencil;            // one division per task (npencil runtime)
+    const int p = t - j * npencil;
+    const int blk = j / sR;               // compile-time power of two
+    const int jj = j - blk * sR;
+    double2* b = s + p * pstride + (blk * L + jj) * estride;
+    butterfly<R, INV>(b, es, tw, N * twmul, jj * tstep);
+  }
+}
+
+template <bool INV, int N, int S>
+__device__ __forceinline__ void stage_dispatch(double2* s, const double2* tw, int twmul, int npencil, int pstride,
+                                               int estride) {
+  if constexpr (S >= 0 && S < Pow2Plan<N>::nstage) {
+    constexpr int R = Pow2Plan<N>::radix(S);
+    constexpr int L = Pow2Plan<N>::span(S);
+    stage_ct<INV, R, L, N>(s, tw, twmul, npencil, pstride, estride);
+    __syncthreads();
+  }
+}
+
+// Compile-time-length transform of npencil uniform pencils (N a power of two <= 512).
+template <bool INV, int N>
+__device__ __forceinline__ void fft_ct(double2* s, const double2* tw, int twmul, int npencil, int pstride,
+                                       int estride) {
+  constexpr int ns = Pow2Plan<N>::nstage;
+  if constexpr (!INV) {
+    stage_dispatch<false, N, 0>(s, tw, twmul, npencil, pstride, estride);
+    stage_dispatch<false, N, 1>(s, tw, twmul, npencil, pstride, estride);
+    stage_dispatch<false, N, 2>(s, tw, twmul, npencil, pstride, estride);
+    stage_dispatch<false, N, 3>(s, tw, twmul, npencil, pstride, estride);
+  } else {
+    stage_dispatch<true, N, ns - 1>(s, tw, twmul, npencil, pstride, estride);
+    stage_dispatch<true, N, ns - 2>(s, tw, twmul, npencil, pstride, estride);
+    stage_dispatch<true, N, ns - 3>(s, tw, twmul, npencil, pstride, estride);
+    stage_dispatch<true, N, ns - 4>(s, tw, twmul, npencil, pstride, estride);
+  }
+  static_assert(ns <= 4, "fft_ct handles up to 4 stages (N <= 4096)");
+}
+
+// Runtime-length transform of uniform pencils (any factorisation of ax.n).
+template <bool INV>
+__device__ void fft_rt(double2* s, const FftAxis& ax, const double2* tw, int twmul, int npencil, int pstride,
+                       int estride) {
+  PencilSet ps = {npencil, npencil, 0, pstride, estride, true};
+  fft_pencils<INV>(s, ax, tw, twmul, ps);
+}

@@ -153,13 +153,18 @@ class Functional(object):
         if self.kst is None:
             self.kst = torch.zeros(plan.nspec * 2, dtype=torch.float64, device="cuda")
         self.vdw_a = vdw_a
+        # (kw0, kw3) table for this grid and radius, L2-resident during the solve
+        self.wtab = None
+        if not (self.version & L.NOHS):
+            self.wtab = torch.empty(plan.nspec * 2, dtype=torch.float64, device="cuda")
+            check(L.lib().cmm_fmt_weights(plan.handle, self.R, ptr(self.wtab), _stream()), "cmm_fmt_weights")
 
     def c1(self, buf, rhohat, chat, want=1, active=None, batch=None):
-        """Spectrum of C1 - V (HardSphere.derive + MFA.derive) for every instance."""
+        """yz-spectrum of C1 - V (HardSphere.derive + MFA.derive) for every instance."""
         B = buf.batch if batch is None else batch
         check(L.lib().cmm_fmt_c1(self.plan.handle, B, ptr(active), self.R, self.beta, self.version,
-                                 ptr(self.kst), ptr(rhohat), ptr(chat), ptr(buf.work), ptr(buf.part),
-                                 buf.nslot, int(want), _stream()), "cmm_fmt_c1")
+                                 ptr(self.kst), ptr(self.wtab), ptr(rhohat), ptr(chat), ptr(buf.work),
+                                 ptr(buf.part), buf.nslot, int(want), _stream()), "cmm_fmt_c1")
 
 
 def mfa_kernel_spectrum(plan, sigma, epsilon, cutoff, rmin=None, limit=0.0, rep=1):

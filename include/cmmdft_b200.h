@@ -137,12 +137,19 @@ int cmm_mfa_kernel(const cmm_grid* grid, double sigma, double epsilon, double cu
  *   plane pass : inverse, White-Bear/FMT dPhi/dn, forward of 5 fields
  *   column pass: back-convolution sum w_a dPhi_a / (beta N) + rho_hat * K_mfa
  * writing d_chat = yz-spectrum of C1 - V (HardSphere.derive + MFA.derive,
- * cmmdft/functionals.py:489-609, 912-926).  want: bit 0 = C1 spectrum,
+ * cmmdft/functionals.py:489-609, 912-926).  d_wtab: weight table from
+ * cmm_fmt_weights for this grid and R, or NULL.  want: bit 0 = C1 spectrum,
  * bit 1 = free-energy sums (PHI, MFA), bit 2 = n3 maximum.
  * d_work: 10 spectra of batch instances.  d_part: [batch][CMM_NSTAT][nslot]. */
 int cmm_fmt_c1(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,
-               int version, const double* d_kst, const double* d_rhohat, double* d_chat,
-               double* d_work, double* d_part, int nslot, int want, void* stream);
+               int version, const double* d_kst, const double* d_wtab, const double* d_rhohat,
+               double* d_chat, double* d_work, double* d_part, int nslot, int want, void* stream);
+
+/* Table of the scalar FMT weights (kw0, kw3 of _init_weight_functions,
+ * cmmdft/functionals.py:421-455) in the column-pass layout: double2
+ * [N1][N2][H3].  Passing it as d_wtab to cmm_fmt_c1 replaces the per-element
+ * evaluation of sin/cos (same formulas, evaluated once per grid and radius). */
+int cmm_fmt_weights(const cmm_grid* grid, double R, double* d_wtab, void* stream);
 
 /* Fused plane pass of one static Picard step (Picard.update_rho_static,
  * cmmdft/solver.py:392-401, with get_new_rho :128-129):

@@ -37,7 +37,8 @@ def fn32(cuda):
     return W.build_functional(cubic_host_276(0), (32, 32, 32), 300.0, methane_guest_params())
 
 
-@pytest.mark.parametrize("shape", [(32, 32, 32), (24, 20, 18), (30, 28, 14), (16, 12, 10), (7, 9, 22)])
+@pytest.mark.parametrize("shape", [(32, 32, 32), (64, 64, 64), (64, 32, 32), (32, 64, 64), (24, 20, 18),
+                                   (30, 28, 14), (16, 12, 10), (7, 9, 22)])
 def test_rfft3d_matches_scipy(cuda, shape):
     rng = np.random.default_rng(1)
     x = rng.standard_normal((2,) + shape)
