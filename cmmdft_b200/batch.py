@@ -72,39 +72,145 @@ def simplex_qp(M, idx):
     return best
 
 
+_SUPPORTS = {}
+
+
+def _supports(n):
+    """All non-empty supports of n variables as a boolean matrix [2^n - 1, n]."""
+    if n not in _SUPPORTS:
+        rows = [[(k >> i) & 1 for i in range(n)] for k in range(1, 1 << n)]
+        _SUPPORTS[n] = np.array(rows, dtype=bool)
+    return _SUPPORTS[n]
+
+
 def simplex_qp_batched(M):
-    """simplex_qp for a stack of Gram matrices M [B, n, n] (same support
-    enumeration, vectorised over the batch)."""
+    """simplex_qp for a stack of Gram matrices M [B, n, n].
+
+    For every support S the equality-constrained minimiser solves the
+    bordered system [M_SS 1; 1^T 0] [a; lam] = [0; 1] (well posed also for
+    rank-deficient Gram matrices); variables outside S are pinned to 0 by
+    identity rows.  All supports of all instances go through one stacked
+    solve; a singular support falls back to a least-squares solve on its own.
+    """
     B, n, _ = M.shape
+    S = _supports(n)                                     # [K, n]
+    K = len(S)
     diag = np.abs(np.diagonal(M, axis1=1, axis2=2))
     scale = np.maximum(diag.max(axis=1), 1e-300)
     Ms = M / scale[:, None, None]
-    best = np.tile(np.full(n, 1.0 / n), (B, 1))
-    best_val = np.full(B, np.inf)
-    found = np.zeros(B, dtype=bool)
-    for k in range(1, n + 1):
-        for S in itertools.combinations(range(n), k):
-            S = list(S)
-            A = Ms[:, S][:, :, S]
-            one = np.ones((B, k, 1))
+    A = np.zeros((B, K, n + 1, n + 1))
+    inS = S[:, :, None] & S[:, None, :]
+    A[:, :, :n, :n] = np.where(inS[None], Ms[:, None], 0.0)
+    idx = np.arange(n)
+    A[:, :, idx, idx] = np.where(S[None], A[:, :, idx, idx], 1.0)
+    A[:, :, :n, n] = S[None].astype(float)
+    A[:, :, n, :n] = S[None].astype(float)
+    rhs = np.zeros((B, K, n + 1, 1))
+    rhs[:, :, n, 0] = 1.0
+    try:
+        x = np.linalg.solve(A, rhs)[..., 0]
+    except np.linalg.LinAlgError:
+        x = np.empty((B, K, n + 1))
+        for k in range(K):
             try:
-                x = np.linalg.solve(A, one)[..., 0]
+                x[:, k] = np.linalg.solve(A[:, k], rhs[:, k])[..., 0]
             except np.linalg.LinAlgError:
-                x = (np.linalg.pinv(A) @ one)[..., 0]
-            sx = x.sum(axis=1)
-            with np.errstate(all='ignore'):
-                a = x / sx[:, None]
-            ok = np.isfinite(sx) & (np.abs(sx) > 1e-300) & np.all(a >= -1e-14, axis=1)
-            a = np.clip(np.nan_to_num(a), 0.0, None)
-            a /= np.maximum(a.sum(axis=1, keepdims=True), 1e-300)
-            full = np.zeros((B, n))
-            full[:, S] = a
-            val = np.einsum('bi,bij,bj->b', full, Ms, full)
-            upd = ok & ((val < best_val * (1 - 1e-13)) | ~found)
-            best[upd] = full[upd]
-            best_val[upd] = val[upd]
-            found |= upd
+                for b in range(B):
+                    x[b, k] = np.linalg.lstsq(A[b, k], rhs[b, k, :, 0], rcond=None)[0]
+    a = np.where(S[None], x[..., :n], 0.0)
+    with np.errstate(all='ignore'):
+        ok = np.all(np.isfinite(a), axis=2) & np.all(a >= -1e-12, axis=2)
+        a = np.clip(np.nan_to_num(a), 0.0, None)
+        a /= np.maximum(a.sum(axis=2, keepdims=True), 1e-300)
+        val = np.einsum('bki,bij,bkj->bk', a, Ms, a)
+    val = np.where(ok, val, np.inf)
+    # lowest objective (Ms is scaled to unit diagonal maximum, so values are
+    # O(1)); ties within 1e-14 go to the support enumerated first
+    vmin = val.min(axis=1, keepdims=True)
+    pick = np.argmax(val <= vmin + 1e-14, axis=1)
+    best = a[np.arange(B), pick]
+    best[~np.isfinite(vmin[:, 0])] = 1.0 / n
     return best
+
+
+def _grid_full(cf, hi, n):
+    al = np.linspace(-hi / 4, hi, n, axis=1)
+    om = cf[:, 2:3] + cf[:, 1:2] * al + cf[:, 0:1] * al ** 2
+    j = np.argmin(om, axis=1)                 # first minimum, as np.where(om == min)[0][0]
+    rows = np.arange(len(hi))
+    return al[rows, j], om[rows, j], np.max(om, axis=1)
+
+
+def grid_parabola(cf, hi, n=10000):
+    """First grid point minimising om = c a^2 + b a + a0 on
+    np.linspace(-hi/4, hi, n) per row, and the min/max of om on that grid
+    (cmmdft/solver.py:426-432).  Exact against evaluating all n points: for a
+    convex parabola om is evaluated with the reference's expression on the
+    ends and on every grid point within reach of the vertex, where reach
+    covers all points whose value can lie within 64 ulps of the vertex value
+    (rounding ties near a flat vertex resolve as the full search does).
+    Concave, linear or rounding-flat rows use the full grid."""
+    cf = np.asarray(cf, dtype=float)
+    hi = np.asarray(hi, dtype=float)
+    R = len(hi)
+    aopt, mn, mx = np.zeros(R), np.zeros(R), np.zeros(R)
+    c, b, a0 = cf[:, 0], cf[:, 1], cf[:, 2]
+    lo = -hi / 4
+    step = (hi - lo) / (n - 1)
+    eps = np.finfo(float).eps
+    with np.errstate(all='ignore'):
+        vert = -b / (2 * c)
+        scale = np.maximum(np.abs(a0), np.abs(a0 + b * vert + c * vert * vert))
+        W = np.ceil(np.sqrt(64 * eps * scale / c) / step) + 2
+    fast = (c > 0) & np.isfinite(W) & (W < n // 4) & (step > 0) & np.isfinite(vert)
+    slow = ~fast
+    if slow.any():
+        aopt[slow], mn[slow], mx[slow] = _grid_full(cf[slow], hi[slow], n)
+    if fast.any():
+        f = np.where(fast)[0]
+        jv = np.clip(np.floor((vert[f] - lo[f]) / step[f]), 0, n - 1)
+        Wm = int(np.max(W[f]))
+        offs = np.arange(-Wm, Wm + 1)
+        cand = np.concatenate([np.zeros((len(f), 1)), jv[:, None] + offs[None, :], np.full((len(f), 1), n - 1)],
+                              axis=1)
+        cand = np.sort(np.clip(cand, 0, n - 1).astype(np.int64), axis=1)
+        # grid values as numpy.linspace forms them: j * step + lo, last point = hi
+        al = cand * step[f, None] + lo[f, None]
+        al = np.where(cand == n - 1, hi[f, None], al)
+        om = a0[f, None] + b[f, None] * al + c[f, None] * al ** 2
+        rows = np.arange(len(f))
+        j = np.argmin(om, axis=1)             # first minimum (candidates sorted by index)
+        aopt[f], mn[f], mx[f] = al[rows, j], om[rows, j], np.max(om, axis=1)
+    return aopt, mn, mx
+
+
+def workspace(fn, B, nring):
+    """Device buffers of a batch of B instances with an nring-deep history,
+    cached on the Functional so repeated solves of the same shape reuse them."""
+    cache = fn.__dict__.setdefault('_workspaces', {})
+    key = (B, nring)
+    if key in cache:
+        return cache[key]
+    plan = fn.plan
+    n1, n2, n3 = plan.npoints
+    dev, f64 = 'cuda', torch.float64
+    ws = dict(
+        ring=torch.zeros((nring, B, n1, n2, n3), dtype=f64, device=dev),
+        rres=torch.zeros((nring, B, n1, n2, n3), dtype=f64, device=dev),
+        trial=torch.empty((B, n1, n2, n3), dtype=f64, device=dev),
+        rho0=torch.empty((B, n1, n2, n3), dtype=f64, device=dev),
+        rhohat=plan.new_spec(B), that=plan.new_spec(B), chat=plan.new_spec(B), chat2=plan.new_spec(B),
+        buf=E.Buffers(plan, B),
+        params=torch.zeros((B, 4), dtype=f64, device=dev),
+        coef=torch.zeros((B, L.MAX_FIELDS), dtype=f64, device=dev),
+        active=torch.zeros(B, dtype=torch.int32, device=dev),
+        pin=dict(active=[torch.zeros(B, dtype=torch.int32).pin_memory() for _ in range(8)],
+                 coef=[torch.zeros((B, L.MAX_FIELDS), dtype=f64).pin_memory() for _ in range(8)],
+                 params=[torch.zeros((B, 4), dtype=f64).pin_memory() for _ in range(8)]),
+    )
+    ws['buf'].part[:, L.STAT_N3MAX, :] = -np.inf
+    cache[key] = ws
+    return ws
 
 
 class BatchSolve(object):
@@ -151,22 +257,11 @@ class BatchSolve(object):
         n1, n2, n3 = self.plan.npoints
         self.npts = n1 * n2 * n3
         self.dr = self.plan.dr
-        dev = 'cuda'
-        f64 = torch.float64
         self.nring = max(self.m, 2) if 'anderson' in self.method else 2
-        self.ring = torch.zeros((self.nring, B, n1, n2, n3), dtype=f64, device=dev)
-        self.rres = torch.zeros((self.nring, B, n1, n2, n3), dtype=f64, device=dev)
-        self.trial = torch.empty((B, n1, n2, n3), dtype=f64, device=dev)
-        self.rho0 = torch.empty((B, n1, n2, n3), dtype=f64, device=dev)
-        self.rhohat = self.plan.new_spec(B)
-        self.that = self.plan.new_spec(B)
-        self.chat = self.plan.new_spec(B)
-        self.chat2 = self.plan.new_spec(B)
-        self.buf = E.Buffers(self.plan, B)
-        self.buf.part[:, L.STAT_N3MAX, :] = -np.inf
-        self.params = torch.zeros((B, 4), dtype=f64, device=dev)
-        self.coef = torch.zeros((B, L.MAX_FIELDS), dtype=f64, device=dev)
-        self.active = torch.zeros(B, dtype=torch.int32, device=dev)
+        ws = workspace(fn, B, self.nring)
+        for k, v in ws.items():
+            setattr(self, k, v)
+        self._pin_i = 0
         self.mask_host = np.zeros(B, dtype=bool)
         self.kernel_launches = 0
         self.omega_evals = 0
@@ -175,9 +270,19 @@ class BatchSolve(object):
         self.pipeline_events = None
 
     # ------------------------------------------------------------ helpers --
+    def _pinned(self, kind):
+        """Next pinned staging buffer of a small ring (host -> device uploads
+        are asynchronous; every step drains the stream at its stats read long
+        before a ring slot comes round again)."""
+        ring = self.pin[kind]
+        self._pin_i = (self._pin_i + 1) % len(ring)
+        return ring[self._pin_i]
+
     def _set_active(self, mask):
         self.mask_host = np.asarray(mask, dtype=bool).copy()
-        self.active.copy_(torch.as_tensor(self.mask_host.astype(np.int32)), non_blocking=False)
+        h = self._pinned('active')
+        h.numpy()[:] = self.mask_host
+        self.active.copy_(h, non_blocking=True)
 
     def _stats(self, mask_bits=(1 << L.NSTAT) - 1):
         E.finalize(self.buf, mask_bits, self.active)
@@ -186,9 +291,11 @@ class BatchSolve(object):
 
     def _mix(self, coefs, fields, clip, ref, out, thr=0.0):
         """out = sum_j coefs[:, j] * fields[j] (fields: [B, ...] tensors); spectrum into self.that."""
-        c = np.zeros((self.B, L.MAX_FIELDS))
+        h = self._pinned('coef')
+        c = h.numpy()
+        c[:] = 0.0
         c[:, :len(fields)] = coefs
-        self.coef.copy_(torch.as_tensor(c))
+        self.coef.copy_(h, non_blocking=True)
         E.mix_step(self.fn, self.buf, self.coef, fields, [self.npts] * len(fields), clip, ref, out, self.that,
                    thr=thr, active=self.active)
         self.kernel_launches += 1
@@ -205,8 +312,16 @@ class BatchSolve(object):
             ev.append((e0, e1, want, int(self.mask_host.sum())))
         self.kernel_launches += 3 if (want & 1) else 2
 
+    def _set_params(self, a=None):
+        h = self._pinned('params')
+        p = h.numpy()
+        p[:] = 0.0
+        p[:, 0] = self.fug
+        if a is not None:
+            p[:, 1] = a
+        self.params.copy_(h, non_blocking=True)
+
     def _residual(self, chat, rho, r_out, hist):
-        self.params[:, 0] = torch.as_tensor(self.fug)
         E.residual_step(self.fn, self.buf, self.params, chat, rho, r_out, hist=hist, hstride=self.npts,
                         active=self.active)
         self.kernel_launches += 1
@@ -245,6 +360,7 @@ class BatchSolve(object):
         self.initial_density(rho0)
         B = self.B
         self.cf = np.ones(B) if cf is None else np.asarray(cf, dtype=float).copy()
+        self._set_params()
         self.result = torch.empty_like(self.rho0)
         self.N_out = np.full(B, np.nan)
         self.conv = np.zeros(B, dtype=bool)
@@ -297,9 +413,7 @@ class BatchSolve(object):
         pending = np.zeros(B, dtype=bool)  # instances whose step `step` awaits its RES check
         while live.any():
             step += 1
-            a = self.alpha_mix * self.cf
-            self.params[:, 0] = torch.as_tensor(self.fug)
-            self.params[:, 1] = torch.as_tensor(a)
+            self._set_params(self.alpha_mix * self.cf)
             # slot choice: ring slot (cur+1)%2 per instance -> launch per parity group
             for par in (0, 1):
                 grp = live & (cur == par)
@@ -522,12 +636,9 @@ class BatchSolve(object):
             idx = np.where(need)[0]
             cf = np.array([np.polyfit([0, a1[b], a2[b]], [prev[b], o1[b], o2[b]], 2) for b in idx])
             hi = np.maximum(a1[idx], a2[idx])
-            al = np.linspace(-hi / 4, hi, 10000, axis=1)
-            om = cf[:, 2:3] + cf[:, 1:2] * al + cf[:, 0:1] * al ** 2
-            j = np.argmin(om, axis=1)   # first minimum, as np.where(om == min)[0][0]
-            aopt[idx] = al[np.arange(len(idx)), j]
-            mn[idx] = np.min(om, axis=1) / kjmol
-            mx[idx] = np.max(om, axis=1) / kjmol
+            aopt[idx], mn[idx], mx[idx] = grid_parabola(cf, hi)
+            mn[idx] /= kjmol
+            mx[idx] /= kjmol
             self.omega0 = np.where(need, o2, self.omega0)
         for b in np.where(mask)[0]:
             if aopt[b] <= 0:
