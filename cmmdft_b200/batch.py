@@ -263,6 +263,8 @@ class BatchSolve(object):
             setattr(self, k, v)
         self._pin_i = 0
         self.mask_host = np.zeros(B, dtype=bool)
+        # optional per-step record: (step, branch, omega, RES) per instance
+        self.trace = None
         self.kernel_launches = 0
         self.omega_evals = 0
         # optional timing of the functional pipeline: list of
@@ -367,6 +369,8 @@ class BatchSolve(object):
         self.steps = np.zeros(B, dtype=int)
         self.failed = np.zeros(B, dtype=bool)
         self.history = [[] for _ in range(B)]
+        if self.trace is not None:
+            self.trace = [[] for _ in range(B)]
         todo = np.ones(B, dtype=bool)
         while todo.any():
             retry = self._solve_once(todo)
@@ -495,6 +499,7 @@ class BatchSolve(object):
         self._residual(self.chat, self.ring[0], self.rres[0], [])
         st = self._stats()
         self.rnorm2[:, 0] = st[:, L.STAT_RES2]
+        self.gram[:, 0, 0] = st[:, L.STAT_RES2]
         self.gnonfin = st[:, L.STAT_GNONFIN].copy()
         k = 0
         while live.any():
@@ -517,8 +522,14 @@ class BatchSolve(object):
                 ok = self._anderson_candidate(cond, k, s_prev, s_new)
                 self.And_true |= cond
                 hyb |= cond & ~ok
+                if self.trace is not None:
+                    for b in np.where(cond)[0]:
+                        self.trace[b].append((k, 'A' if ok[b] else 'A-rejected', float(self.omega0[b])))
             if hyb.any():
                 self._hybrid_step(hyb, k, s_prev, s_new)
+                if self.trace is not None:
+                    for b in np.where(hyb)[0]:
+                        self.trace[b].append((k, 'H', float(self.omega0[b])))
             # --- after the update: non-finite check, N, convergence (solver.py:286-305)
             for b in np.where(live)[0]:
                 self.steps[b] = k
