@@ -50,13 +50,13 @@ class EquationOfState(object):
         return np.logspace(-10, 0, npoints) / angstrom ** 3
 
     def _brackets(self, values, grid_values, grid):
+        """Intervals [grid[j-1], grid[j]] with grid_values[j-1] <= v <= grid_values[j],
+        in increasing j (the scan of eos.py:101-108 / 137-144, vectorised)."""
         out = []
+        lo, hi = grid_values[:-1], grid_values[1:]
         for v in values:
-            iv = []
-            for j in range(1, len(grid)):
-                if grid_values[j - 1] <= v <= grid_values[j]:
-                    iv.append((grid[j - 1], grid[j]))
-            out.append(iv)
+            js = np.nonzero((lo <= v) & (v <= hi))[0] + 1
+            out.append([(grid[j - 1], grid[j]) for j in js])
         return out
 
     def solve_densities_from_chempots(self, chempots, n_rough_gridpoints=1000):
