@@ -11,6 +11,7 @@
 #define CMM_MAX_FIELDS 12     // fields a mix launch combines
 #define CMM_PLANE_THREADS 512
 #define CMM_COL_THREADS 256
+#define CMM_FMT_THREADS 1024   // the 5-field plane pass (one block per SM)
 
 // Per-instance reduction slots (see cmm_stat_* in the public header).
 #define NQ CMM_NSTAT

@@ -558,7 +558,7 @@ __device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, 
 }
 
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+__global__ void __launch_bounds__(CMM_FMT_THREADS)
 k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version,
             const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
             double* __restrict__ part, int nslot_part, int want) {
@@ -820,24 +820,40 @@ static int col_kind(const cmm_grid* g) {
     }                                                                                    \
   } while (0)
 
+#define LAUNCH_PLANE_T(kind, kern, grd, nthr, smem, st, ...)                              \
+  do {                                                                                   \
+    int rc_;                                                                             \
+    if ((kind) == 1) {                                                                   \
+      if ((rc_ = set_smem((const void*)kern<64, 32>, smem))) return rc_;                \
+      kern<64, 32><<<grd, nthr, smem, st>>>(__VA_ARGS__);                                \
+    } else if ((kind) == 2) {                                                            \
+      if ((rc_ = set_smem((const void*)kern<32, 16>, smem))) return rc_;                \
+      kern<32, 16><<<grd, nthr, smem, st>>>(__VA_ARGS__);                                \
+    } else {                                                                             \
+      if ((rc_ = set_smem((const void*)kern<0, 0>, smem))) return rc_;                  \
+      kern<0, 0><<<grd, nthr, smem, st>>>(__VA_ARGS__);                                  \
+    }                                                                                    \
+  } while (0)
+
 #define LAUNCH_COL(kind, kern, grd, smem, st, ...)                                        \
   do {                                                                                   \
     int rc_;                                                                             \
     if ((kind) == 1) {                                                                   \
-      if ((rc_ = set_smem((const void*)kern<64, 16>, smem))) return rc_;                \
-      kern<64, 16><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                     \
+      if ((rc_ = set_smem((const void*)kern<64, 8>, smem))) return rc_;                \
+      kern<64, 8><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                     \
     } else if ((kind) == 2) {                                                            \
-      if ((rc_ = set_smem((const void*)kern<32, 16>, smem))) return rc_;                \
-      kern<32, 16><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                     \
+      if ((rc_ = set_smem((const void*)kern<32, 8>, smem))) return rc_;                \
+      kern<32, 8><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                     \
     } else {                                                                             \
       if ((rc_ = set_smem((const void*)kern<0, 0>, smem))) return rc_;                  \
       kern<0, 0><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                       \
     }                                                                                    \
   } while (0)
 
-// Column tile width: 16 columns (256 B rows) when it fits, fewer for long x.
+// Column tile width: 8 columns (128 B rows) for the specialised kernels, up to
+// 16 when it fits otherwise.
 static int col_tile(const cmm_grid* g, int nslot) {
-  if (col_kind(g)) return 16;
+  if (col_kind(g)) return 8;
   int tc = 16;
   while (tc > 1 && col_smem_bytes(g->n1, tc, nslot) > 200 * 1024) tc /= 2;
   return tc;
@@ -924,8 +940,8 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
   LAUNCH_COL(ck, k_col_weights, dim3(ntile, batch), cs5, st, g->dev, d_active, R, 1.0 / npts,
              (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0, tc);
   const size_t ps = plane_smem_bytes(g->n2, g->n3, 5);
-  LAUNCH_PLANE(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), ps, st, g->dev, d_active, R, version,
-               (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
+  LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, d_active, R,
+                 version, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
   if (want & 1) {
     LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), cs6, st, g->dev, d_active, R, 1.0 / (beta * npts),
                (const double2*)gbuf, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt, (double2*)d_chat,
