@@ -54,6 +54,9 @@ _SIGS = {
     "cmm_mix_step": ([c_void_p, c_int, c_void_p, c_void_p, P(c_void_p), P(c_ll), c_int, c_int, c_double,
                       c_double, c_void_p, c_ll, c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int,
                       c_void_p], c_int),
+    "cmm_fmt_c1_noalloc_capacity": ([c_void_p], ctypes.c_size_t),
+    "cmm_fmt_c1_noalloc": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p,
+                            c_void_p, c_void_p, c_int, c_void_p], c_int),
     "cmm_stats_finalize": ([c_int, c_void_p, c_void_p, c_int, ctypes.c_uint, c_void_p, c_void_p], c_int),
 }
 

@@ -192,6 +192,26 @@ int cmm_mix_step(const cmm_grid* grid, int batch, const int* d_active, const dou
 int cmm_stats_finalize(int batch, const int* d_active, const double* d_part, int nslot,
                        unsigned mask, double* d_stats, void* stream);
 
+/* Allocation-free variant of cmm_fmt_c1 (no counterpart in the reference,
+ * which allocates freely in numpy).  For callers that cannot allocate device
+ * memory where they evaluate the functional -- plugin hosts that forbid
+ * allocation inside a solve callback, integrations under a fixed device
+ * memory budget, bindings whose runtime cannot own a CUDA allocation.
+ * The scratch (ten intermediate spectra and the partial sums) lives in one
+ * static device array of CMM_NOALLOC_SCRATCH_BYTES that every GPU loading
+ * the library holds until exit; batches larger than
+ * cmm_fmt_c1_noalloc_capacity(grid) are rejected with CMM_ERR_WORKSPACE.
+ * The first call on a device looks up the array's address (make it before
+ * any stream capture).  All calls share the array and it keeps the last
+ * call's contents: calls that overlap on the GPU race.  Outputs as
+ * cmm_fmt_c1; d_stats [batch][CMM_NSTAT] receives the PHI / MFA / N3MAX
+ * sums requested by `want` (may be NULL when want == 1). */
+#define CMM_NOALLOC_SCRATCH_BYTES (32u << 20)
+size_t cmm_fmt_c1_noalloc_capacity(const cmm_grid* grid);
+int cmm_fmt_c1_noalloc(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,
+                       int version, const double* d_kst, const double* d_wtab, const double* d_rhohat,
+                       double* d_chat, double* d_stats, int want, void* stream);
+
 #ifdef __cplusplus
 }
 #endif
