@@ -110,6 +110,20 @@ def pipeline_bytes(plan, want, n_active):
     return per * n_active + shared
 
 
+def reduce_over_ranks(ms, nconv, world, device):
+    """Max of the timed milliseconds and sum of converged points over ranks
+    (replicas: no data-path collective; two scalars after the timed region)."""
+    import torch
+    if world <= 1:
+        return float(ms), float(nconv)
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    nc = torch.tensor([float(nconv)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    dist.all_reduce(nc, op=dist.ReduceOp.SUM)
+    return float(t.item()), float(nc.item())
+
+
 def setup_case(torch):
     from cmmdft_b200 import workload as W
     from cmmdft_b200.hosts import cubic_host_276, methane_guest_params
@@ -171,15 +185,7 @@ def run_gpu(args):
         e1.record()
         barrier()
     ms = e0.elapsed_time(e1)
-    t = torch.tensor([ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        nc = torch.tensor([nconv], dtype=torch.float64, device="cuda")
-        dist.all_reduce(nc)
-        nconv_all = float(nc.item())
-    else:
-        nconv_all = float(nconv)
-    ms_max = float(t.item())
+    ms_max, nconv_all = reduce_over_ranks(ms, nconv, world, "cuda")
     value = nconv_all / (ms_max / 1e3)
 
     # roofline of the fused functional pipeline, from its events in the timed region
@@ -322,7 +328,7 @@ def run_reference(args):
         ncores = len(os.sched_getaffinity(0))
     except Exception:
         ncores = os.cpu_count() or 1
-    nproc = max(1, min(ncores, 8))
+    nproc = max(1, min(ncores, 21))
     steps = max(1, min(args.steps, 2))
     vals = []
     cb = None
