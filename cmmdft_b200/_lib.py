@@ -12,10 +12,19 @@ LIB_PATH = os.path.join(HERE, "libcmmdft_b200.so")
 # cmm_stat_* slots (include/cmmdft_b200.h)
 STAT_N, STAT_IUE, STAT_NONFIN, STAT_FID, STAT_FEXT, STAT_RES2, STAT_PHI, STAT_MFA, \
     STAT_N3MAX, STAT_GNONFIN, STAT_GRAM0 = range(11)
-NSTAT = 18
+STAT_WDA, STAT_DER = 18, 19
+NSTAT = 20
 MAX_HIST = 8
 MAX_FIELDS = 12
-FMT, MFMT, WBII, ANTISYM, NOHS = 0, 1, 2, 8, 16
+FMT, MFMT, WBII, ANTISYM, NOHS, WDA = 0, 1, 2, 8, 16, 32
+
+
+class WdaEos(ctypes.Structure):
+    """cmm_wda_eos of include/cmmdft_b200.h."""
+    _fields_ = [("D", ctypes.c_double), ("sigma3", ctypes.c_double), ("epsilon", ctypes.c_double),
+                ("gamma", ctypes.c_double), ("a", ctypes.c_double * 8), ("b", ctypes.c_double * 6),
+                ("eta", ctypes.c_double), ("kT", ctypes.c_double), ("a_mfa", ctypes.c_double),
+                ("factors", ctypes.c_double * 3)]
 CLIP_NONE, CLIP_PICARD, CLIP_DENSITY = 0, 1, 2
 
 
@@ -45,18 +54,19 @@ _SIGS = {
     "cmm_mfa_kernel": ([c_void_p, c_double, c_double, c_double, c_double, c_double, c_int, c_void_p,
                         c_void_p, P(ctypes.c_size_t), P(c_double), c_void_p], c_int),
     "cmm_fmt_c1": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p,
-                    c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p], c_int),
+                    c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p], c_int),
     "cmm_fmt_weights": ([c_void_p, c_double, c_void_p, c_void_p], c_int),
-    "cmm_picard_static_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_void_p,
+    "cmm_picard_static_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_double,
+                                c_double, c_void_p,
                                 c_void_p, c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int, c_void_p], c_int),
-    "cmm_residual_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p, c_ll,
-                           c_void_p, P(c_void_p), c_int, c_ll, c_void_p, c_int, c_void_p], c_int),
+    "cmm_residual_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_double, c_void_p, c_void_p, c_void_p,
+                           c_ll, c_void_p, P(c_void_p), c_int, c_ll, c_void_p, c_int, c_void_p], c_int),
     "cmm_mix_step": ([c_void_p, c_int, c_void_p, c_void_p, P(c_void_p), P(c_ll), c_int, c_int, c_double,
                       c_double, c_void_p, c_ll, c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int,
                       c_void_p], c_int),
     "cmm_fmt_c1_noalloc_capacity": ([c_void_p], ctypes.c_size_t),
     "cmm_fmt_c1_noalloc": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p,
-                            c_void_p, c_void_p, c_int, c_void_p], c_int),
+                            c_void_p, c_void_p, c_void_p, c_int, c_void_p], c_int),
     "cmm_stats_finalize": ([c_int, c_void_p, c_void_p, c_int, ctypes.c_uint, c_void_p, c_void_p], c_int),
 }
 

@@ -222,7 +222,8 @@ class BatchSolve(object):
 
     def __init__(self, fn, chempots, method='hybridanderson', nsteps=500, threshold=1e-6,
                  criterion='res', alpha_mix=0.1, m=5, damping=0.3, delta=0.2, damping_max=0.8,
-                 damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5), divergence_guard=False):
+                 damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5), divergence_guard=False,
+                 a_tol=1e-6, r_tol=1e-4):
         self.fn = fn
         self.plan = fn.plan
         self.mu = np.asarray(chempots, dtype=np.float64).ravel()
@@ -234,9 +235,10 @@ class BatchSolve(object):
         thr = threshold if isinstance(threshold, (list, tuple)) else [threshold] * len(crit)
         self.criteria = [c.lower() for c in crit]
         for c in self.criteria:
-            if c not in ('res', 'riue'):
+            if c not in ('res', 'riue', 'der'):
                 raise NotImplementedError("criterion %r" % c)
         self.thresholds = [float(t) for t in thr]
+        self.tol = (float(a_tol), float(r_tol))   # DER tolerances (solver.py:25-26)
         self.alpha_mix = float(alpha_mix)
         self.thresh = 1 * kjmol
         self.m = int(m)
@@ -321,11 +323,12 @@ class BatchSolve(object):
         p[:, 0] = self.fug
         if a is not None:
             p[:, 1] = a
+        p[:, 2] = self.mu
         self.params.copy_(h, non_blocking=True)
 
     def _residual(self, chat, rho, r_out, hist):
         E.residual_step(self.fn, self.buf, self.params, chat, rho, r_out, hist=hist, hstride=self.npts,
-                        active=self.active)
+                        active=self.active, tol=self.tol)
         self.kernel_launches += 1
 
     def _omega(self, st, b):
@@ -337,13 +340,18 @@ class BatchSolve(object):
         G += (st[L.STAT_PHI] * dr) / beta
         G += 0.5 * (st[L.STAT_MFA] * dr)
         G += st[L.STAT_FEXT] * dr
+        if self.fn.wda is not None:
+            G += st[L.STAT_WDA] * dr
         return G
 
     def _omega_parts(self, st):
         beta, dr = self.fn.beta, self.dr
-        return dict(N=st[L.STAT_N] * dr, Fid=(st[L.STAT_FID] * dr) / beta,
-                    HardSphere=(st[L.STAT_PHI] * dr) / beta, MFA=0.5 * (st[L.STAT_MFA] * dr),
-                    ExtPot=st[L.STAT_FEXT] * dr)
+        out = dict(N=st[L.STAT_N] * dr, Fid=(st[L.STAT_FID] * dr) / beta,
+                   HardSphere=(st[L.STAT_PHI] * dr) / beta, MFA=0.5 * (st[L.STAT_MFA] * dr),
+                   ExtPot=st[L.STAT_FEXT] * dr)
+        if self.fn.wda is not None:
+            out['WDA-V'] = st[L.STAT_WDA] * dr
+        return out
 
     def _eval_density(self, mask, coefs, fields, clip, out, want, ref):
         """Mix a density into `out`, forward it, run the functional pipeline
@@ -425,7 +433,7 @@ class BatchSolve(object):
                     continue
                 self._set_active(grp)
                 E.picard_static_step(self.fn, self.buf, self.params, thr, self.chat, self.ring[par],
-                                     self.ring[1 - par], self.rhohat, active=self.active)
+                                     self.ring[1 - par], self.rhohat, active=self.active, tol=self.tol)
                 self.kernel_launches += 1
             self._set_active(live)
             st = self._stats()
@@ -435,7 +443,8 @@ class BatchSolve(object):
                     N = prev[b, L.STAT_N] * self.dr
                     res = np.sqrt(st[b, L.STAT_RES2]) / np.sqrt(N) / np.sqrt(self.npts)
                     iue = prev[b, L.STAT_IUE] * self.dr
-                    if self._converged(b, N, res, iue):
+                    der = np.sqrt(st[b, L.STAT_DER]) / np.sqrt(self.npts)
+                    if self._converged(b, N, res, iue, der):
                         self._finish(b, self.ring[cur[b], b], N, step - 1, True)
                         live[b] = False
                         continue
@@ -465,11 +474,11 @@ class BatchSolve(object):
         best = np.nanmin(r)
         return bool(r[-1] > 1e6 * best and np.all(np.diff(r[-6:]) >= 0))
 
-    def _converged(self, b, N, res, iue):
+    def _converged(self, b, N, res, iue, der=np.nan):
         ok = True
         riue = iue / N if N > 0 else np.nan
         for c, t in zip(self.criteria, self.thresholds):
-            v = res if c == 'res' else riue
+            v = res if c == 'res' else (riue if c == 'riue' else der)
             ok = ok and (v < t)
         self.history[b].append((N, res, riue))
         if iue == 0 and np.isnan(riue):
@@ -541,8 +550,9 @@ class BatchSolve(object):
                 N = st_b[L.STAT_N] * self.dr
                 res = np.sqrt(self.rnorm2[b, s_new]) / np.sqrt(N) / np.sqrt(self.npts)
                 iue = st_b[L.STAT_IUE] * self.dr
+                der = np.sqrt(st_b[L.STAT_DER]) / np.sqrt(self.npts)
                 self.Ncur[b] = N
-                if self._converged(b, N, res, iue):
+                if self._converged(b, N, res, iue, der):
                     self._finish(b, self.ring[s_new, b], N, k, True)
                     live[b] = False
                 elif k >= self.nsteps or self._diverging(b):

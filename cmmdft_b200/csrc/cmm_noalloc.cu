@@ -5,7 +5,7 @@
 // callback, integrations that run under a fixed device-memory budget
 // reserved up front, and bindings from languages whose runtime cannot own
 // the lifetime of a CUDA allocation.  For them, cmm_fmt_c1_noalloc keeps its
-// scratch (the ten intermediate spectra and the per-block partial sums) in
+// scratch (the twelve intermediate spectra and the per-block partial sums) in
 // one file-scope device array of fixed size, CMM_NOALLOC_SCRATCH_BYTES, that
 // every GPU loading this library holds until the process exits.
 //
@@ -49,17 +49,19 @@ __global__ void k_noalloc_clear_part(double* part, int batch, int nslot) {
   }
 }
 
+#define NOALLOC_NSPEC 12   // intermediate spectra per instance (6 weighted densities, 6 dPhi)
+
 extern "C" size_t cmm_fmt_c1_noalloc_capacity(const cmm_grid* g) {
   if (!g) return 0;
   const size_t spec = (size_t)g->n1 * g->n2 * g->h3 * sizeof(double2);
   const size_t nslot = (size_t)((g->n1 > g->n2 * g->h3) ? g->n1 : g->n2 * g->h3);
-  const size_t per = 10 * spec + (size_t)CMM_NSTAT * nslot * sizeof(double);
+  const size_t per = NOALLOC_NSPEC * spec + (size_t)CMM_NSTAT * nslot * sizeof(double);
   return per ? (size_t)CMM_NOALLOC_SCRATCH_BYTES / per : 0;
 }
 
 extern "C" int cmm_fmt_c1_noalloc(const cmm_grid* g, int batch, const int* d_active, double R, double beta,
-                                  int version, const double* d_kst, const double* d_wtab, const double* d_rhohat,
-                                  double* d_chat, double* d_stats, int want, void* stream) {
+                                  int version, const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab,
+                                  const double* d_rhohat, double* d_chat, double* d_stats, int want, void* stream) {
   if (!g || batch < 1 || !d_kst || !d_rhohat) return CMM_ERR_ARG;
   if ((want & 1) && !d_chat) return CMM_ERR_ARG;
   if ((want & 6) && !d_stats) return CMM_ERR_ARG;
@@ -70,16 +72,16 @@ extern "C" int cmm_fmt_c1_noalloc(const cmm_grid* g, int batch, const int* d_act
   const size_t spec = (size_t)g->n1 * g->n2 * g->h3 * sizeof(double2);
   const int nslot = (g->n1 > g->n2 * g->h3) ? g->n1 : g->n2 * g->h3;
   double* work = (double*)base;
-  double* part = (double*)((unsigned char*)base + 10 * spec * (size_t)batch);
+  double* part = (double*)((unsigned char*)base + NOALLOC_NSPEC * spec * (size_t)batch);
   cudaStream_t st = (cudaStream_t)stream;
   k_noalloc_clear_part<<<148, 256, 0, st>>>(part, batch, nslot);
   if (cudaPeekAtLastError() != cudaSuccess) return CMM_ERR_CUDA;
-  rc = cmm_fmt_c1(g, batch, d_active, R, beta, version, d_kst, d_wtab, d_rhohat, d_chat, work, part, nslot, want,
-                  stream);
+  rc = cmm_fmt_c1(g, batch, d_active, R, beta, version, wda, d_kst, d_wtab, d_rhohat, d_chat, work, part, nslot,
+                  want, stream);
   if (rc) return rc;
   if (want & 6) {
     unsigned mask = 0;
-    if (want & 2) mask |= (1u << CMM_STAT_PHI) | (1u << CMM_STAT_MFA);
+    if (want & 2) mask |= (1u << CMM_STAT_PHI) | (1u << CMM_STAT_MFA) | (1u << CMM_STAT_WDA);
     if (want & 4) mask |= (1u << CMM_STAT_N3MAX);
     rc = cmm_stats_finalize(batch, d_active, part, nslot, mask, d_stats, stream);
   }

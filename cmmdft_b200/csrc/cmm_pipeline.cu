@@ -11,6 +11,7 @@
 // All transforms are in place in shared memory (fft_core.cuh).
 #include <cmath>
 #include <cstdio>
+#include <cstring>
 
 #include "cmm_common.cuh"
 
@@ -369,6 +370,65 @@ __device__ __forceinline__ Weights fmt_weights_at(const GridDev& g, const double
   return w;
 }
 
+// WDA weight (WDAVFunctional._init_weight_function, cmmdft/functionals.py:1139-1155):
+// 3 (sin x - x cos x) / x^3 sigma_L at x = |k| D, 1 sigma_L at k = 0.
+__device__ __forceinline__ double wda_weight_at(const GridDev& g, int p1, int col, double D) {
+  const int p2 = col / g.h3, p3 = col - p2 * g.h3;
+  const double kx = g.kp1[p1], ky = g.kp2[p2], kz = g.kp3[p3];
+  const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];
+  const double om = sqrt(kx * kx + ky * ky + kz * kz) * D;
+  if (fabs(om) <= 1e-8) return sl;
+  double sn, cs;
+  sincos(om, &sn, &cs);
+  return (3.0 * (sn - om * cs) / (om * om * om)) * sl;
+}
+
+// SumOfEOS(MBWR, CS, MFA) excess free energy per volume and its density
+// derivative at one weighted density (cmmdft/eos.py:226-265, 295-546).
+__device__ __forceinline__ void wda_eos(const cmm_wda_eos& e, double rho, double& fv, double& dfv) {
+  // MBWR (eos.py:368-422)
+  const double rr = rho * e.sigma3;
+  double A = 0.0, dA = 0.0, p = 1.0;  // p = rr^i
+#pragma unroll
+  for (int i = 0; i < 8; ++i) {
+    dA += e.a[i] * p * e.sigma3;
+    p *= rr;
+    A += e.a[i] / (i + 1) * p;
+  }
+  const double rr2 = rr * rr;
+  const double F = exp(-e.gamma * rr2);
+  const double ig = 1.0 / (2 * e.gamma);
+  double G = ig * (1 - F), q = 1.0, podd = rr;  // q = rr^(2(n-1)), podd = rr^(2t+1)
+  A += e.b[0] * G;
+  dA += e.b[0] * e.sigma3 * podd * F;
+#pragma unroll
+  for (int n = 2; n <= 6; ++n) {
+    q *= rr2;
+    G = -ig * (F * q - 2 * (n - 1) * G);
+    A += e.b[n - 1] * G;
+    podd *= rr2;
+    dA += e.b[n - 1] * e.sigma3 * podd * F;
+  }
+  const double fp_m = A * e.epsilon, dfp_m = dA * e.epsilon;
+  // Carnahan-Starling (eos.py:503-509)
+  const double er = e.eta * rho, om = 1 - er;
+  const double fp_c = e.kT * (4 * e.eta * rho - 3 * er * er) / (om * om);
+  const double dfp_c = 2 * e.kT * e.eta * (2 - er) / (om * om * om);
+  // mean-field EOS (eos.py:536-540)
+  const double fp_a = e.a_mfa * rho, dfp_a = e.a_mfa;
+  double d_m = rho * dfp_m; d_m += fp_m;
+  double d_c = rho * dfp_c; d_c += fp_c;
+  double d_a = rho * dfp_a; d_a += fp_a;
+  dfv = 0.0;
+  dfv += e.factors[0] * d_m;
+  dfv += e.factors[1] * d_c;
+  dfv += e.factors[2] * d_a;
+  fv = 0.0;
+  fv += e.factors[0] * (rho * fp_m);
+  fv += e.factors[1] * (rho * fp_c);
+  fv += e.factors[2] * (rho * fp_a);
+}
+
 // Weight table (w0, w3) in the column-pass layout [x DIF position][column].
 __global__ void k_fmt_weights(GridDev g, double R, double2* __restrict__ wtab) {
   const int nc = g.n2 * g.h3;
@@ -388,38 +448,40 @@ __global__ void __launch_bounds__(CMM_COL_THREADS)
 k_col_weights(GridDev g, const int* __restrict__ active, double R, double inv_npts,
               const double2* __restrict__ rhohat, double2* __restrict__ wout, size_t fsw,
               const double2* __restrict__ kst, const double2* __restrict__ wtab, double* __restrict__ part,
-              int nslot_part, int want_value, int tc) {
+              int nslot_part, int want_value, int tc, int nout, double wda_D) {
   const int b = blockIdx.y, tile = blockIdx.x;
   if (active && !active[b]) return;
   const ColShape<N1C, TCC> sh(g, tc);
   const int c0 = tile * sh.tc;
-  ColSmem s = col_smem_setup(g, sh, 5);
-  load_col_tile(g, s, sh, 5, 0, rhohat, b, c0, nullptr);
+  const int ns = nout;  // 5, or 6 with the WDA weighted density
+  ColSmem s = col_smem_setup(g, sh, ns);
+  load_col_tile(g, s, sh, ns, 0, rhohat, b, c0, nullptr);
   __syncthreads();
-  col_fft<false>(g, s, sh, 5, 0, 1);
+  col_fft<false>(g, s, sh, ns, 0, 1);
   const int nc = g.n2 * g.h3;
   double mfa = 0.0;
   for (int i = threadIdx.x; i < sh.n1 * sh.tc; i += blockDim.x) {
     const int p1 = i / sh.tc, c = i - p1 * sh.tc;
     const int col = c0 + c;
     if (col >= nc) continue;
-    double2 F = cel(s, sh, 5, 0, p1, c);
+    double2 F = cel(s, sh, ns, 0, p1, c);
     const Weights w = fmt_weights_at(g, wtab, p1, col, R);
     if (want_value) {
       const double2 K = __ldg(kst + (size_t)p1 * nc + col);
       mfa += g.wt3[col - (col / g.h3) * g.h3] * (F.x * F.x + F.y * F.y) * K.x;
     }
     F = cscale(F, inv_npts);
-    cel(s, sh, 5, 1, p1, c) = cscale(F, w.w3);
+    if (ns > 5) cel(s, sh, ns, 5, p1, c) = cscale(F, wda_weight_at(g, p1, col, wda_D));
+    cel(s, sh, ns, 1, p1, c) = cscale(F, w.w3);
     // -i * v * F
-    cel(s, sh, 5, 2, p1, c) = make_double2(F.y * w.v[0], -F.x * w.v[0]);
-    cel(s, sh, 5, 3, p1, c) = make_double2(F.y * w.v[1], -F.x * w.v[1]);
-    cel(s, sh, 5, 4, p1, c) = make_double2(F.y * w.v[2], -F.x * w.v[2]);
-    cel(s, sh, 5, 0, p1, c) = cscale(F, w.w0);
+    cel(s, sh, ns, 2, p1, c) = make_double2(F.y * w.v[0], -F.x * w.v[0]);
+    cel(s, sh, ns, 3, p1, c) = make_double2(F.y * w.v[1], -F.x * w.v[1]);
+    cel(s, sh, ns, 4, p1, c) = make_double2(F.y * w.v[2], -F.x * w.v[2]);
+    cel(s, sh, ns, 0, p1, c) = cscale(F, w.w0);
   }
   __syncthreads();
-  col_fft<true>(g, s, sh, 5, 0, 5);
-  for (int f = 0; f < 5; ++f) store_col_tile(g, s, sh, 5, f, wout + f * fsw, b, c0, nullptr);
+  col_fft<true>(g, s, sh, ns, 0, ns);
+  for (int f = 0; f < ns; ++f) store_col_tile(g, s, sh, ns, f, wout + f * fsw, b, c0, nullptr);
   if (want_value) {
     __shared__ double red[32];
     double t = block_sum(mfa, red);
@@ -435,19 +497,21 @@ __global__ void __launch_bounds__(CMM_COL_THREADS)
 k_col_backconv(GridDev g, const int* __restrict__ active, double R, double scale,
                const double2* __restrict__ gin, size_t fsg, const double2* __restrict__ rhohat,
                const double2* __restrict__ kst, const double2* __restrict__ wtab, double2* __restrict__ chat,
-               int tc) {
+               int tc, int nin, double wda_D, double inv_npts) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   const ColShape<N1C, TCC> sh(g, tc);
   const int c0 = blockIdx.x * sh.tc;
-  ColSmem s = col_smem_setup(g, sh, 6);
+  const int ns = nin + 1;    // 5 dPhi (+1 WDA) fields, then rho_hat
+  const int fr = nin;        // slot of rho_hat
+  ColSmem s = col_smem_setup(g, sh, ns);
   const bool hs = (gin != nullptr);
   if (hs)
-    for (int f = 0; f < 5; ++f) load_col_tile(g, s, sh, 6, f, gin + f * fsg, b, c0, nullptr);
-  load_col_tile(g, s, sh, 6, 5, rhohat, b, c0, nullptr);
+    for (int f = 0; f < nin; ++f) load_col_tile(g, s, sh, ns, f, gin + f * fsg, b, c0, nullptr);
+  load_col_tile(g, s, sh, ns, fr, rhohat, b, c0, nullptr);
   __syncthreads();
-  if (hs) col_fft<false>(g, s, sh, 6, 0, 6);
-  else col_fft<false>(g, s, sh, 6, 5, 1);
+  if (hs) col_fft<false>(g, s, sh, ns, 0, ns);
+  else col_fft<false>(g, s, sh, ns, fr, 1);
   const int nc = g.n2 * g.h3;
   for (int i = threadIdx.x; i < sh.n1 * sh.tc; i += blockDim.x) {
     const int p1 = i / sh.tc, c = i - p1 * sh.tc;
@@ -456,20 +520,22 @@ k_col_backconv(GridDev g, const int* __restrict__ active, double R, double scale
     double2 acc = make_double2(0.0, 0.0);
     if (hs) {
       const Weights w = fmt_weights_at(g, wtab, p1, col, R);
-      acc = cadd(cscale(cel(s, sh, 6, 0, p1, c), w.w0), cscale(cel(s, sh, 6, 1, p1, c), w.w3));
+      acc = cadd(cscale(cel(s, sh, ns, 0, p1, c), w.w0), cscale(cel(s, sh, ns, 1, p1, c), w.w3));
       // - sum_j G_j * (-i v_j) = + i * sum_j v_j G_j
       double2 gv = make_double2(0.0, 0.0);
-      for (int a = 0; a < 3; ++a) gv = cadd(gv, cscale(cel(s, sh, 6, 2 + a, p1, c), w.v[a]));
+      for (int a = 0; a < 3; ++a) gv = cadd(gv, cscale(cel(s, sh, ns, 2 + a, p1, c), w.v[a]));
       acc = cadd(acc, make_double2(-gv.y, gv.x));
       acc = cscale(acc, scale);
+      // WDA: ifft(fft(dphi) kw), no 1/beta (the EOS derivative is an energy)
+      if (nin > 5) acc = cadd(acc, cscale(cel(s, sh, ns, 5, p1, c), wda_weight_at(g, p1, col, wda_D) * inv_npts));
     }
     const double2 K = __ldg(kst + (size_t)p1 * nc + col);
-    acc = cadd(acc, cmul(cel(s, sh, 6, 5, p1, c), K));
-    cel(s, sh, 6, 0, p1, c) = acc;
+    acc = cadd(acc, cmul(cel(s, sh, ns, fr, p1, c), K));
+    cel(s, sh, ns, 0, p1, c) = acc;
   }
   __syncthreads();
-  col_fft<true>(g, s, sh, 6, 0, 1);
-  store_col_tile(g, s, sh, 6, 0, chat, b, c0, nullptr);
+  col_fft<true>(g, s, sh, ns, 0, 1);
+  store_col_tile(g, s, sh, ns, 0, chat, b, c0, nullptr);
 }
 
 // ===================================== plane pass: dPhi/dn (White-Bear) ==
@@ -559,31 +625,40 @@ __device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, 
 
 template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_FMT_THREADS)
-k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version,
+k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
             const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
             double* __restrict__ part, int nslot_part, int want) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
-  PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 5);
+  const bool has_wda = (version & CMM_WDA) != 0;
+  const int ns = has_wda ? 6 : 5;
+  PlaneSmem s = plane_smem_setup<N2C, M3C>(g, ns);
   const PlaneShape<N2C, M3C> sh(g);
   const size_t poff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3;
-  load_spec_planes<N2C, M3C>(g, s, 5, win, poff, fsw);
+  load_spec_planes<N2C, M3C>(g, s, ns, win, poff, fsw);
   __syncthreads();
-  plane_inverse<N2C, M3C>(g, s, 5);
-  double phi = 0.0, n3max = -INFINITY;
+  plane_inverse<N2C, M3C>(g, s, ns);
+  double phi = 0.0, n3max = -INFINITY, fwda = 0.0;
   const bool do_c1 = (want & 1) != 0;
   for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
     const int r = i / sh.n3, j = i - r * sh.n3;
-    double& a0 = rel(s, sh, 5, 0, r, j);
-    double& a3 = rel(s, sh, 5, 1, r, j);
-    double& ax = rel(s, sh, 5, 2, r, j);
-    double& ay = rel(s, sh, 5, 3, r, j);
-    double& az = rel(s, sh, 5, 4, r, j);
+    double& a0 = rel(s, sh, ns, 0, r, j);
+    double& a3 = rel(s, sh, ns, 1, r, j);
+    double& ax = rel(s, sh, ns, 2, r, j);
+    double& ay = rel(s, sh, ns, 3, r, j);
+    double& az = rel(s, sh, ns, 4, r, j);
     n3max = fmax(n3max, a3);
     PhiOut o = fmt_point(a0, a3, ax, ay, az, R, version);
     phi += o.phi;
     if (do_c1) {
       a0 = o.gs; a3 = o.g3; ax = o.gv[0]; ay = o.gv[1]; az = o.gv[2];
+    }
+    if (has_wda) {
+      double& aw = rel(s, sh, ns, 5, r, j);
+      double fv, dfv;
+      wda_eos(wda, aw, fv, dfv);
+      fwda += fv;
+      if (do_c1) aw = dfv;
     }
   }
   __syncthreads();
@@ -591,6 +666,10 @@ k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version,
   if (want & 2) {
     double t = block_sum(phi, red);
     put_part(part, b, CMM_STAT_PHI, nslot_part, i1, t);
+    if (has_wda) {
+      t = block_sum(fwda, red);
+      put_part(part, b, CMM_STAT_WDA, nslot_part, i1, t);
+    }
   }
   if (want & 4) {
     double t = block_max(n3max, red);
@@ -598,8 +677,8 @@ k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version,
   }
   if (!do_c1) return;
   __syncthreads();
-  plane_forward<N2C, M3C>(g, s, 5);
-  store_spec_planes<N2C, M3C>(g, s, 5, gout, poff, fsg);
+  plane_forward<N2C, M3C>(g, s, ns);
+  store_spec_planes<N2C, M3C>(g, s, ns, gout, poff, fsg);
 }
 
 // ========================================== plane pass: solver updates ==
@@ -627,11 +706,24 @@ __device__ inline void stats_store(const PlaneStats& st, double* part, int b, in
   t = block_sum(st.fext, red);   put_part(part, b, CMM_STAT_FEXT, nslot, slot, t);
 }
 
+// One term of the DER criterion (Solver._check_convergence, cmmdft/solver.py:200-205):
+// (|rho| beta dOmega / (a_tol + r_tol |rho|))^2 with dOmega = ln(L^3 rho_reg)/beta + C1 - mu,
+// skipped where np.isclose(rho, 0) (|rho| <= 1e-8).
+__device__ __forceinline__ double der_term(double rho, double C1, double mu, double beta, double lambda3,
+                                           double a_tol, double r_tol) {
+  if (fabs(rho) <= 1e-8) return 0.0;
+  const double rr = (rho < 1e-12) ? 1e-30 : rho;
+  const double dO = log(lambda3 * rr) / beta + C1 - mu;
+  const double t = fabs(rho) * beta * dO / (a_tol + r_tol * fabs(rho));
+  return t * t;
+}
+
 // Static Picard step fused with the C1 inverse and the forward of rho'.
 template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_PLANE_THREADS)
 k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
-               double beta, double lambda3, double thr, const double2* __restrict__ chat,
+               double beta, double lambda3, double thr, double a_tol, double r_tol,
+               const double2* __restrict__ chat,
                const double* __restrict__ rho, const double* __restrict__ V, long long vstride,
                double* __restrict__ rho_out, double2* __restrict__ rhohat_out,
                double* __restrict__ part, int nslot_part) {
@@ -643,11 +735,11 @@ k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restri
   load_spec_planes<N2C, M3C>(g, s, 1, chat, poff, 0);
   __syncthreads();
   plane_inverse<N2C, M3C>(g, s, 1);
-  const double fug = params[b * 4 + 0], a = params[b * 4 + 1];
+  const double fug = params[b * 4 + 0], a = params[b * 4 + 1], mu = params[b * 4 + 2];
   const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
   const double* Vp = V + b * vstride + (size_t)i1 * sh.n2 * sh.n3;
   PlaneStats st = {0, 0, 0, 0, 0};
-  double res2 = 0.0, gnf = 0.0;
+  double res2 = 0.0, gnf = 0.0, der = 0.0;
   for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
     const int r = i / sh.n3, j = i - r * sh.n3;
     double& cell = rel(s, sh, 1, 0, r, j);
@@ -657,6 +749,7 @@ k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restri
     const double x = __ldg(rho + roff + i);
     res2 += (G - x) * (G - x);
     gnf += cmm_isfinite(G) ? 0.0 : 1.0;
+    der += der_term(x, C1, mu, beta, lambda3, a_tol, r_tol);
     double xn = (1.0 - a) * x + a * G;
     if (xn < thr) xn = 0.0;
     rho_out[roff + i] = xn;
@@ -669,6 +762,8 @@ k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restri
     put_part(part, b, CMM_STAT_RES2, nslot_part, i1, t);
     t = block_sum(gnf, red2);
     put_part(part, b, CMM_STAT_GNONFIN, nslot_part, i1, t);
+    t = block_sum(der, red2);
+    put_part(part, b, CMM_STAT_DER, nslot_part, i1, t);
   }
   stats_store(st, part, b, nslot_part, i1);
   __syncthreads();
@@ -682,7 +777,8 @@ struct HistPtrs { const double* p[CMM_MAX_HIST]; };
 template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_PLANE_THREADS)
 k_plane_residual(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
-                 double beta, const double2* __restrict__ chat, const double* __restrict__ rho,
+                 double beta, double lambda3, double a_tol, double r_tol, const double2* __restrict__ chat,
+                 const double* __restrict__ rho,
                  const double* __restrict__ V, long long vstride, double* __restrict__ r_out,
                  HistPtrs hist, int nhist, long long hstride, double* __restrict__ part,
                  int nslot_part) {
@@ -694,11 +790,11 @@ k_plane_residual(GridDev g, const int* __restrict__ active, const double* __rest
   load_spec_planes<N2C, M3C>(g, s, 1, chat, poff, 0);
   __syncthreads();
   plane_inverse<N2C, M3C>(g, s, 1);
-  const double fug = params[b * 4 + 0];
+  const double fug = params[b * 4 + 0], mu = params[b * 4 + 2];
   const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
   const size_t hoff = (size_t)b * hstride + (size_t)i1 * sh.n2 * sh.n3;
   const double* Vp = V + b * vstride + (size_t)i1 * sh.n2 * sh.n3;
-  double res2 = 0.0, gnf = 0.0;
+  double res2 = 0.0, gnf = 0.0, der = 0.0;
   double gram[CMM_MAX_HIST];
 #pragma unroll
   for (int j = 0; j < CMM_MAX_HIST; ++j) gram[j] = 0.0;
@@ -710,6 +806,7 @@ k_plane_residual(GridDev g, const int* __restrict__ active, const double* __rest
     const double rr = G - x;
     res2 += rr * rr;
     gnf += cmm_isfinite(G) ? 0.0 : 1.0;
+    der += der_term(x, C1, mu, beta, lambda3, a_tol, r_tol);
     r_out[roff + i] = rr;
 #pragma unroll
     for (int h = 0; h < CMM_MAX_HIST; ++h)
@@ -720,6 +817,8 @@ k_plane_residual(GridDev g, const int* __restrict__ active, const double* __rest
   put_part(part, b, CMM_STAT_RES2, nslot_part, i1, t);
   t = block_sum(gnf, red);
   put_part(part, b, CMM_STAT_GNONFIN, nslot_part, i1, t);
+  t = block_sum(der, red);
+  put_part(part, b, CMM_STAT_DER, nslot_part, i1, t);
   for (int h = 0; h < nhist; ++h) {
     t = block_sum(gram[h], red);
     put_part(part, b, CMM_STAT_GRAM0 + h, nslot_part, i1, t);
@@ -915,69 +1014,82 @@ extern "C" int cmm_fmt_weights(const cmm_grid* g, double R, double* d_wtab, void
 }
 
 extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, double R, double beta,
-                          int version, const double* d_kst, const double* d_wtab, const double* d_rhohat,
-                          double* d_chat, double* d_work, double* d_part, int nslot, int want, void* stream) {
+                          int version, const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab,
+                          const double* d_rhohat, double* d_chat, double* d_work, double* d_part, int nslot,
+                          int want, void* stream) {
   if (!g || batch < 1 || !d_kst || !d_rhohat || !d_work || !d_part) return CMM_ERR_ARG;
   if ((want & 1) && !d_chat) return CMM_ERR_ARG;
+  const bool has_wda = (version & CMM_WDA) != 0;
+  if (has_wda && !wda) return CMM_ERR_ARG;
+  cmm_wda_eos we;
+  memset(&we, 0, sizeof(we));
+  if (has_wda) we = *wda;
+  const int nf = has_wda ? 6 : 5;            // weighted densities (and dPhi fields)
   cudaStream_t st = (cudaStream_t)stream;
   const size_t fs = (size_t)batch * g->n1 * g->n2 * g->h3;  // field stride (double2)
-  double2* wbuf = (double2*)d_work;          // 5 weighted-density spectra
-  double2* gbuf = wbuf + 5 * fs;             // 5 dPhi spectra
+  double2* wbuf = (double2*)d_work;          // weighted-density spectra (up to 6)
+  double2* gbuf = wbuf + 6 * fs;             // dPhi spectra (up to 6)
   const double npts = (double)g->n1 * g->n2 * g->n3;
-  const int tc = col_tile(g, 6);
+  const int tc = col_tile(g, 7);
   const int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
   if (nslot < g->n1 || nslot < ntile) return CMM_ERR_WORKSPACE;
-  const size_t cs5 = col_smem_bytes(g->n1, tc, 5), cs6 = col_smem_bytes(g->n1, tc, 6);
+  const size_t csw = col_smem_bytes(g->n1, tc, nf), csb = col_smem_bytes(g->n1, tc, nf + 1);
   const double2* wt = (const double2*)d_wtab;
   const int ck = col_kind(g);
   if (version & CMM_NOHS) {  // MFA term alone: one column pass
     if (!(want & 1)) return CMM_ERR_ARG;
-    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), cs6, st, g->dev, d_active, R, 1.0 / (beta * npts),
-               (const double2*)nullptr, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt,
-               (double2*)d_chat, tc);
+    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), col_smem_bytes(g->n1, tc, 6), st, g->dev, d_active, R,
+               1.0 / (beta * npts), (const double2*)nullptr, fs, (const double2*)d_rhohat, (const double2*)d_kst,
+               wt, (double2*)d_chat, tc, 5, 0.0, 1.0 / npts);
     return last_err();
   }
-  LAUNCH_COL(ck, k_col_weights, dim3(ntile, batch), cs5, st, g->dev, d_active, R, 1.0 / npts,
-             (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0, tc);
-  const size_t ps = plane_smem_bytes(g->n2, g->n3, 5);
+  LAUNCH_COL(ck, k_col_weights, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
+             (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0, tc,
+             nf, we.D);
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, nf);
   LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, d_active, R,
-                 version, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
+                 version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
   if (want & 1) {
-    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), cs6, st, g->dev, d_active, R, 1.0 / (beta * npts),
+    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),
                (const double2*)gbuf, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt, (double2*)d_chat,
-               tc);
+               tc, nf, we.D, 1.0 / npts);
   }
   return last_err();
 }
 
 extern "C" int cmm_picard_static_step(const cmm_grid* g, int batch, const int* d_active,
                                       const double* d_params, double beta, double lambda3, double thr,
-                                      const double* d_chat, const double* d_rho, const double* d_V,
+                                      double a_tol, double r_tol, const double* d_chat, const double* d_rho, const double* d_V,
                                       long long vstride, double* d_rho_out, double* d_rhohat_out,
                                       double* d_part, int nslot, void* stream) {
   if (!g || batch < 1 || !d_params || !d_chat || !d_rho || !d_V || !d_rho_out || !d_rhohat_out || !d_part)
     return CMM_ERR_ARG;
+  if (!(a_tol >= 0) || !(r_tol >= 0)) return CMM_ERR_ARG;
   if (nslot < g->n1) return CMM_ERR_WORKSPACE;
   const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
   LAUNCH_PLANE(plane_kind(g), k_plane_picard, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_active,
-               d_params, beta, lambda3, thr, (const double2*)d_chat, d_rho, d_V, vstride, d_rho_out,
+               d_params, beta, lambda3, thr, a_tol, r_tol, (const double2*)d_chat, d_rho, d_V, vstride,
+               d_rho_out,
                (double2*)d_rhohat_out, d_part, nslot);
   return last_err();
 }
 
 extern "C" int cmm_residual_step(const cmm_grid* g, int batch, const int* d_active, const double* d_params,
-                                 double beta, const double* d_chat, const double* d_rho, const double* d_V,
+                                 double beta, double lambda3, double a_tol, double r_tol, const double* d_chat,
+                                 const double* d_rho,
+                                 const double* d_V,
                                  long long vstride, double* d_r_out, const double* const* d_hist, int nhist,
                                  long long hstride, double* d_part, int nslot, void* stream) {
   if (!g || batch < 1 || !d_params || !d_chat || !d_rho || !d_V || !d_r_out || !d_part) return CMM_ERR_ARG;
   if (nhist < 0 || nhist > CMM_MAX_HIST || (nhist && !d_hist)) return CMM_ERR_ARG;
+  if (!(a_tol >= 0) || !(r_tol >= 0)) return CMM_ERR_ARG;
   if (nslot < g->n1) return CMM_ERR_WORKSPACE;
   HistPtrs hp;
   for (int j = 0; j < CMM_MAX_HIST; ++j) hp.p[j] = (j < nhist) ? d_hist[j] : nullptr;
   const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
   LAUNCH_PLANE(plane_kind(g), k_plane_residual, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_active,
-               d_params, beta, (const double2*)d_chat, d_rho, d_V, vstride, d_r_out, hp, nhist, hstride, d_part,
-               nslot);
+               d_params, beta, lambda3, a_tol, r_tol, (const double2*)d_chat, d_rho, d_V, vstride, d_r_out,
+               hp, nhist, hstride, d_part, nslot);
   return last_err();
 }
 

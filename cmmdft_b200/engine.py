@@ -126,7 +126,7 @@ class Buffers(object):
         dev = "cuda"
         f64 = torch.float64
         fs = plan.nspec * 2
-        self.work = torch.empty((10, batch, fs), dtype=f64, device=dev)
+        self.work = torch.empty((12, batch, fs), dtype=f64, device=dev)
         self.nslot = max(n1, -(-(n2 * plan.h3) // 1))  # >= ntiles for any column tile >= 1
         self.part = torch.zeros((batch, L.NSTAT, self.nslot), dtype=f64, device=dev)
         self.stats = torch.zeros((batch, L.NSTAT), dtype=f64, device=dev)
@@ -141,7 +141,7 @@ class Functional(object):
     add_mean_field and add_external_potential (cmmdft/functionals.py:176-337).
     """
 
-    def __init__(self, plan, R, beta, wavelength, V, version=L.WBII, kst=None, vdw_a=None):
+    def __init__(self, plan, R, beta, wavelength, V, version=L.WBII, kst=None, vdw_a=None, wda=None):
         self.plan = plan
         self.R = float(R)
         self.beta = float(beta)
@@ -153,6 +153,10 @@ class Functional(object):
         if self.kst is None:
             self.kst = torch.zeros(plan.nspec * 2, dtype=torch.float64, device="cuda")
         self.vdw_a = vdw_a
+        # optional WDA correlation part (an _lib.WdaEos); sets the CMM_WDA bit
+        self.wda = wda
+        if wda is not None:
+            self.version |= L.WDA
         # (kw0, kw3) table for this grid and radius, L2-resident during the solve
         self.wtab = None
         if not (self.version & L.NOHS):
@@ -162,7 +166,8 @@ class Functional(object):
     def c1(self, buf, rhohat, chat, want=1, active=None, batch=None):
         """yz-spectrum of C1 - V (HardSphere.derive + MFA.derive) for every instance."""
         B = buf.batch if batch is None else batch
-        check(L.lib().cmm_fmt_c1(self.plan.handle, B, ptr(active), self.R, self.beta, self.version,
+        wda = ctypes.byref(self.wda) if self.wda is not None else None
+        check(L.lib().cmm_fmt_c1(self.plan.handle, B, ptr(active), self.R, self.beta, self.version, wda,
                                  ptr(self.kst), ptr(self.wtab), ptr(rhohat), ptr(chat), ptr(buf.work),
                                  ptr(buf.part), buf.nslot, int(want), _stream()), "cmm_fmt_c1")
 
@@ -204,17 +209,21 @@ def finalize(buf, mask, active=None):
                                      ptr(buf.stats), _stream()), "cmm_stats_finalize")
 
 
-def picard_static_step(fn, buf, params, thr, chat, rho, rho_out, rhohat_out, active=None, vstride=0):
+def picard_static_step(fn, buf, params, thr, chat, rho, rho_out, rhohat_out, active=None, vstride=0,
+                       tol=(1e-6, 1e-4)):
+    """tol = (a_tol, r_tol) of the DER criterion (Solver, cmmdft/solver.py:25-26)."""
     check(L.lib().cmm_picard_static_step(fn.plan.handle, buf.batch, ptr(active), ptr(params), fn.beta,
-                                         fn.lambda3, float(thr), ptr(chat), ptr(rho), ptr(fn.V), int(vstride),
+                                         fn.lambda3, float(thr), float(tol[0]), float(tol[1]), ptr(chat), ptr(rho), ptr(fn.V), int(vstride),
                                          ptr(rho_out), ptr(rhohat_out), ptr(buf.part), buf.nslot, _stream()),
           "cmm_picard_static_step")
 
 
-def residual_step(fn, buf, params, chat, rho, r_out, hist=(), hstride=0, active=None, vstride=0):
+def residual_step(fn, buf, params, chat, rho, r_out, hist=(), hstride=0, active=None, vstride=0,
+                  tol=(1e-6, 1e-4)):
     n = len(hist)
     arr = (ctypes.c_void_p * max(n, 1))(*[h.data_ptr() for h in hist]) if n else None
-    check(L.lib().cmm_residual_step(fn.plan.handle, buf.batch, ptr(active), ptr(params), fn.beta, ptr(chat),
+    check(L.lib().cmm_residual_step(fn.plan.handle, buf.batch, ptr(active), ptr(params), fn.beta, fn.lambda3,
+                                    float(tol[0]), float(tol[1]), ptr(chat),
                                     ptr(rho), ptr(fn.V), int(vstride), ptr(r_out), arr, n, int(hstride),
                                     ptr(buf.part), buf.nslot, _stream()), "cmm_residual_step")
 

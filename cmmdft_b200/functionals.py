@@ -7,10 +7,10 @@ GPU through the C ABI; the solver uses the fused pipeline of all parts at once
 (``FreeEnergy.device()``).
 
 Built: HardSphere (FMT, MFMT, WBII and their antisymmetric 'a' variants),
-MFA (with or without supercell tail corrections) and ExtPot (spherical LJ
-guests).  Not built in this package: the tensor 't' FMT variants, the WDA /
-LDA correlation parts and non-spherical guests; asking for them raises
-NotImplementedError.
+MFA (with or without supercell tail corrections), ExtPot (spherical LJ
+guests) and the WDA correlation part of add_correlation_wda_lj.  Not built
+in this package: the tensor 't' FMT variants, the LDA part and non-spherical
+guests; asking for them raises NotImplementedError.
 """
 import os
 from pathlib import Path
@@ -23,7 +23,8 @@ from .system import Spectrum
 from .units import angstrom, kjmol, boltzmann
 from .workload import hs_version_code
 
-__all__ = ['FreeEnergy', 'Functional', 'HardSphereFunctional', 'MFAFunctional', 'ExternalPotential']
+__all__ = ['FreeEnergy', 'Functional', 'HardSphereFunctional', 'MFAFunctional', 'ExternalPotential',
+           'WDAVFunctional']
 
 
 def _torch():
@@ -106,7 +107,18 @@ class FreeEnergy(object):
         self.add_part(ep)
 
     def add_correlation_wda_lj(self, **kwargs):
-        raise NotImplementedError("the WDA correlation part is not built in this package")
+        """WDA correlation part with SumOfEOS([MBWR, CS, MFA], factors=[1, -1, -1])
+        (cmmdft/functionals.py:339-362); a = 0.5 integral U of the MFA part if present."""
+        from .eos import ModifiedBenedictWebbRubinEOS, CarnahanStarlingEOS, MFAEOS, SumOfEOS
+        g = self.system.guest
+        a = self.part_dict['MFA'].compute_vdw_a() if 'MFA' in self.part_names else None
+        mbwr = ModifiedBenedictWebbRubinEOS(g.mass, g.sigma, g.epsilon)
+        cs = CarnahanStarlingEOS(g.mass, g.Rhs)
+        mfa = MFAEOS(g.mass, g.sigma, g.epsilon, a=a)
+        eos = SumOfEOS(g.mass, [mbwr, cs, mfa], factors=[1, -1, -1])
+        wda = WDAVFunctional(self.grid, g.Rhs, eos)
+        wda.set_temperature(self.temperature, Rhs=g.Rhs)
+        self.add_part(wda)
 
     def add_lda(self, eos):
         raise NotImplementedError("the LDA part is not built in this package")
@@ -121,7 +133,7 @@ class FreeEnergy(object):
             return self._device
         names = self.part_names
         for n in names:
-            if n not in ('HardSphere', 'MFA', 'ExtPot'):
+            if n not in ('HardSphere', 'MFA', 'ExtPot', 'WDA-V'):
                 raise NotImplementedError("part %r has no GPU path" % n)
         if 'HardSphere' not in names:
             raise NotImplementedError("the fused solve needs a HardSphere part")
@@ -132,7 +144,9 @@ class FreeEnergy(object):
             torch.zeros(plan.npoints, dtype=torch.float64, device='cuda')
         kst = self.part_dict['MFA'].kst if 'MFA' in names else None
         a = self.part_dict['MFA'].vdw_a if 'MFA' in names else None
-        self._device = E.Functional(plan, hs.R, self.beta, self.wavelength, V, hs_version_code(hs.version), kst, a)
+        wda = self.part_dict['WDA-V'].eos_struct() if 'WDA-V' in names else None
+        self._device = E.Functional(plan, hs.R, self.beta, self.wavelength, V, hs_version_code(hs.version), kst, a,
+                                    wda=wda)
         return self._device
 
     def init_tracking(self, fn, rewrite=False):
@@ -264,6 +278,58 @@ class MFAFunctional(Functional):
         if local:
             return 0.5 * rho * d
         return 0.5 * self.grid.integrate(rho * d)
+
+
+class WDAVFunctional(Functional):
+    """Weighted-density approximation of an EOS excess free energy
+    (cmmdft/functionals.py:1116-1184).  Evaluated inside the fused functional
+    pipeline (FreeEnergy.device()); the EOS must be the SumOfEOS of
+    add_correlation_wda_lj (MBWR, Carnahan-Starling and mean-field terms)."""
+    name = 'WDA-V'
+
+    def __init__(self, grid, Rhs, eos):
+        self.grid = grid
+        self.R = Rhs
+        self.eos = eos
+        self.temperature = None
+
+    def copy(self, grid=None):
+        return type(self)(grid or self.grid.copy(), self.R, self.eos)
+
+    def set_temperature(self, temperature, Rhs=None, **kwargs):
+        self.temperature = temperature
+        if Rhs is not None:
+            self.R = Rhs
+        self.D = 2 * self.R
+        self.eos.set_temperature(temperature)
+
+    def eos_struct(self):
+        from .eos import ModifiedBenedictWebbRubinEOS, CarnahanStarlingEOS, MFAEOS
+        kinds = [type(e) for e in self.eos.list_eos]
+        if kinds != [ModifiedBenedictWebbRubinEOS, CarnahanStarlingEOS, MFAEOS]:
+            raise NotImplementedError("the GPU WDA part evaluates SumOfEOS([MBWR, CS, MFA]) only")
+        mb, cs, mf = self.eos.list_eos
+        w = L.WdaEos()
+        w.D = self.D
+        w.sigma3 = mb.sigma ** 3
+        w.epsilon = mb.epsilon
+        w.gamma = mb.gamma
+        for i in range(8):
+            w.a[i] = mb.a[i]
+        for i in range(6):
+            w.b[i] = mb.b[i]
+        w.eta = cs.eta
+        w.kT = boltzmann * cs.temperature
+        w.a_mfa = mf.a
+        for i in range(3):
+            w.factors[i] = self.eos.factors[i]
+        return w
+
+    def derive(self, krho):
+        raise NotImplementedError("the WDA part is evaluated inside FreeEnergy.device()'s fused pipeline")
+
+    def value(self, krho, local=False):
+        raise NotImplementedError("the WDA part is evaluated inside FreeEnergy.device()'s fused pipeline")
 
 
 class ExternalPotential(Functional):

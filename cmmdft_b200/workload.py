@@ -43,11 +43,39 @@ def host_type_arrays(host, guest_types=None):
     return sig, eps
 
 
+def wda_struct(sigma, epsilon, mass, temperature, R, vdw_a):
+    """cmm_wda_eos of add_correlation_wda_lj (cmmdft/functionals.py:339-362):
+    SumOfEOS([MBWR, CS(Rhs), MFA(a)], factors=[1, -1, -1]) at ``temperature``."""
+    from .eos import ModifiedBenedictWebbRubinEOS, CarnahanStarlingEOS, MFAEOS
+    mb = ModifiedBenedictWebbRubinEOS(mass, sigma, epsilon)
+    cs = CarnahanStarlingEOS(mass, R)
+    mf = MFAEOS(mass, sigma, epsilon, a=vdw_a)
+    for e in (mb, cs, mf):
+        e.set_temperature(temperature)
+    w = L.WdaEos()
+    w.D = 2 * R
+    w.sigma3 = sigma ** 3
+    w.epsilon = epsilon
+    w.gamma = mb.gamma
+    for i in range(8):
+        w.a[i] = mb.a[i]
+    for i in range(6):
+        w.b[i] = mb.b[i]
+    w.eta = cs.eta
+    w.kT = boltzmann * temperature
+    w.a_mfa = mf.a
+    for i, f in enumerate((1, -1, -1)):
+        w.factors[i] = f
+    return w
+
+
 def build_functional(host, npoints, temperature, guest, version='WBII', tailcorrections=False,
-                     cutoff=12 * angstrom, mfa_cutoff=12 * angstrom, limit_potential=1e4 * kjmol, plan=None):
+                     cutoff=12 * angstrom, mfa_cutoff=12 * angstrom, limit_potential=1e4 * kjmol, plan=None,
+                     wda=False):
     """Device Functional for ``host`` (SyntheticHost-like) at ``npoints``.
 
-    guest = (sigma, epsilon, mass) in atomic units.
+    guest = (sigma, epsilon, mass) in atomic units; wda=True adds the WDA
+    correlation part of add_correlation_wda_lj.
     """
     sigma, epsilon, mass = guest
     if plan is None:
@@ -59,7 +87,8 @@ def build_functional(host, npoints, temperature, guest, version='WBII', tailcorr
     R = hardsphere_radius(sigma, epsilon, temperature)
     beta = 1.0 / (boltzmann * temperature)
     lam = thermal_wavelength(mass, temperature)
-    return E.Functional(plan, R, beta, lam, V, hs_version_code(version), kst, a)
+    w = wda_struct(sigma, epsilon, mass, temperature, R, a) if wda else None
+    return E.Functional(plan, R, beta, lam, V, hs_version_code(version), kst, a, wda=w)
 
 
 def isotherm_inputs(pressures, temperature, guest):

@@ -54,13 +54,29 @@ enum {
   CMM_STAT_N3MAX = 8,    /* max n3 (unclipped)                        */
   CMM_STAT_GNONFIN = 9,  /* count of non-finite G                     */
   CMM_STAT_GRAM0 = 10,   /* sum r_new r_j, j = 0..CMM_MAX_HIST-1      */
-  CMM_NSTAT = 18
+  CMM_STAT_WDA = 18,     /* sum f_EOS(wd) (WDA free-energy density)   */
+  CMM_STAT_DER = 19,     /* sum (rho beta dOmega / (a_tol + r_tol rho))^2 over rho != 0 */
+  CMM_NSTAT = 20
 };
 #define CMM_MAX_HIST 8
 
 /* Hard-sphere functional versions (cmmdft/functionals.py:373-377).
- * CMM_NOHS drops the hard-sphere term (the MFA convolution alone). */
-enum { CMM_FMT = 0, CMM_MFMT = 1, CMM_WBII = 2, CMM_ANTISYM = 8, CMM_NOHS = 16 };
+ * CMM_NOHS drops the hard-sphere term (the MFA convolution alone);
+ * CMM_WDA adds the WDA correlation part described by a cmm_wda_eos. */
+enum { CMM_FMT = 0, CMM_MFMT = 1, CMM_WBII = 2, CMM_ANTISYM = 8, CMM_NOHS = 16, CMM_WDA = 32 };
+
+/* WDA correlation part (WDAVFunctional with SumOfEOS([MBWR, CS, MFA],
+ * factors), cmmdft/functionals.py:339-362, 1116-1184; cmmdft/eos.py).
+ * Weight: 3 (sin x - x cos x) / x^3 sigma_L at x = |k| D.  The MBWR
+ * coefficients a[8], b[6] are those at the solve temperature. */
+typedef struct cmm_wda_eos {
+  double D;                 /* weight diameter (2 Rhs) */
+  double sigma3, epsilon, gamma;   /* MBWR: sigma**3 (as the reference forms it), epsilon, gamma */
+  double a[8], b[6];
+  double eta, kT;           /* Carnahan-Starling: 4 pi R^3 / 3, k_B T */
+  double a_mfa;             /* mean-field EOS a */
+  double factors[3];        /* SumOfEOS factors of MBWR, CS, MFA */
+} cmm_wda_eos;
 
 /* Mix-kernel clip modes. */
 enum {
@@ -140,10 +156,13 @@ int cmm_mfa_kernel(const cmm_grid* grid, double sigma, double epsilon, double cu
  * cmmdft/functionals.py:489-609, 912-926).  d_wtab: weight table from
  * cmm_fmt_weights for this grid and R, or NULL.  want: bit 0 = C1 spectrum,
  * bit 1 = free-energy sums (PHI, MFA), bit 2 = n3 maximum.
- * d_work: 10 spectra of batch instances.  d_part: [batch][CMM_NSTAT][nslot]. */
+ * wda: WDA part (with version | CMM_WDA), else NULL; it adds one weighted
+ * density and one back-convolution field.
+ * d_work: 12 spectra of batch instances.  d_part: [batch][CMM_NSTAT][nslot]. */
 int cmm_fmt_c1(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,
-               int version, const double* d_kst, const double* d_wtab, const double* d_rhohat,
-               double* d_chat, double* d_work, double* d_part, int nslot, int want, void* stream);
+               int version, const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab,
+               const double* d_rhohat, double* d_chat, double* d_work, double* d_part, int nslot,
+               int want, void* stream);
 
 /* Table of the scalar FMT weights (kw0, kw3 of _init_weight_functions,
  * cmmdft/functionals.py:421-455) in the column-pass layout: double2
@@ -156,20 +175,25 @@ int cmm_fmt_weights(const cmm_grid* grid, double R, double* d_wtab, void* stream
  *   C1 = irfft(chat) + V; G = beta exp(-beta C1) f;  RES2 += (G - rho)^2
  *   rho' = (1-a) rho + a G; rho' < thr -> 0;  writes rho', its spectrum and
  *   the reductions N, IUE, NONFIN, FID, FEXT of rho'.
- * d_params: [batch][4] = {fugacity f, a, unused, unused}.  d_V stride vstride. */
+ * d_params: [batch][4] = {fugacity f, a, mu, unused}.  d_V stride vstride.
+ * Also the DER sum of the input density (Solver._check_convergence,
+ * solver.py:200-205) with the Solver tolerances a_tol, r_tol (solver.py:25-26,
+ * defaults 1e-6 and 1e-4; both must be >= 0). */
 int cmm_picard_static_step(const cmm_grid* grid, int batch, const int* d_active,
                            const double* d_params, double beta, double lambda3, double thr,
-                           const double* d_chat, const double* d_rho, const double* d_V,
+                           double a_tol, double r_tol, const double* d_chat, const double* d_rho, const double* d_V,
                            long long vstride, double* d_rho_out, double* d_rhohat_out,
                            double* d_part, int nslot, void* stream);
 
 /* Residual plane pass (Anderson.update_rho / _save_previous_rhos,
  * cmmdft/solver.py:527-579): C1 = irfft(chat) + V; G = beta exp(-beta C1) f;
- * writes r = G - rho to d_r_out; reductions RES2, GNONFIN and the Gram row
+ * writes r = G - rho to d_r_out; reductions RES2, GNONFIN, DER and the Gram row
  * sum r * r_j over `nhist` stored residuals d_hist[j] (HOST array of
- * device pointers, instance stride hstride). */
+ * device pointers, instance stride hstride); a_tol, r_tol as in
+ * cmm_picard_static_step. */
 int cmm_residual_step(const cmm_grid* grid, int batch, const int* d_active,
-                      const double* d_params, double beta, const double* d_chat,
+                      const double* d_params, double beta, double lambda3, double a_tol,
+                      double r_tol, const double* d_chat,
                       const double* d_rho, const double* d_V, long long vstride,
                       double* d_r_out, const double* const* d_hist, int nhist,
                       long long hstride, double* d_part, int nslot, void* stream);
@@ -197,7 +221,7 @@ int cmm_stats_finalize(int batch, const int* d_active, const double* d_part, int
  * memory where they evaluate the functional -- plugin hosts that forbid
  * allocation inside a solve callback, integrations under a fixed device
  * memory budget, bindings whose runtime cannot own a CUDA allocation.
- * The scratch (ten intermediate spectra and the partial sums) lives in one
+ * The scratch (twelve intermediate spectra and the partial sums) lives in one
  * static device array of CMM_NOALLOC_SCRATCH_BYTES that every GPU loading
  * the library holds until exit; batches larger than
  * cmm_fmt_c1_noalloc_capacity(grid) are rejected with CMM_ERR_WORKSPACE.
@@ -209,8 +233,8 @@ int cmm_stats_finalize(int batch, const int* d_active, const double* d_part, int
 #define CMM_NOALLOC_SCRATCH_BYTES (32u << 20)
 size_t cmm_fmt_c1_noalloc_capacity(const cmm_grid* grid);
 int cmm_fmt_c1_noalloc(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,
-                       int version, const double* d_kst, const double* d_wtab, const double* d_rhohat,
-                       double* d_chat, double* d_stats, int want, void* stream);
+                       int version, const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab,
+                       const double* d_rhohat, double* d_chat, double* d_stats, int want, void* stream);
 
 #ifdef __cplusplus
 }

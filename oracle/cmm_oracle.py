@@ -474,6 +474,96 @@ class CarnahanStarling(object):
         return 2 * kT * self.eta * (2 - self.eta * rho) / (1 - self.eta * rho) ** 3
 
 
+class MFAEOS(object):
+    """Mean-field EOS, cmmdft/eos.py:523-546."""
+
+    def __init__(self, mass, sigma=None, epsilon=None, a=None):
+        self.mass = mass
+        self.a = a if a is not None else -16 / 9 * np.pi * epsilon * sigma ** 3
+
+    def set_temperature(self, T):
+        self.T = T
+
+    def fex_particle(self, rho):
+        return self.a * rho
+
+    def dfex_particle(self, rho):
+        return self.a
+
+
+def eos_fex_volume(eos, rho):
+    """excess_free_energy_volume, eos.py:46-48."""
+    return rho * eos.fex_particle(rho)
+
+
+def eos_dfex_volume(eos, rho):
+    """derivative_excess_free_energy_volume, eos.py:54-58."""
+    v = rho * eos.dfex_particle(rho)
+    v += eos.fex_particle(rho)
+    return v
+
+
+class SumOfEOS(object):
+    """cmmdft/eos.py:226-265 (volume forms summed with factors)."""
+
+    def __init__(self, list_eos, factors):
+        self.list_eos, self.factors = list_eos, factors
+
+    def set_temperature(self, T):
+        for e in self.list_eos:
+            e.set_temperature(T)
+
+    def fex_volume(self, rho):
+        r = rho * 0.0
+        for e, f in zip(self.list_eos, self.factors):
+            r += f * eos_fex_volume(e, rho)
+        return r
+
+    def dfex_volume(self, rho):
+        r = rho * 0.0
+        for e, f in zip(self.list_eos, self.factors):
+            r += f * eos_dfex_volume(e, rho)
+        return r
+
+
+class WDA(object):
+    """WDAVFunctional, cmmdft/functionals.py:1116-1184."""
+    name = 'WDA-V'
+
+    def __init__(self, grid, R, eos, temperature):
+        self.grid, self.R, self.eos = grid, R, eos
+        eos.set_temperature(temperature)
+        om = grid.kpoints[..., 3] * (2 * R)
+        mask = ~np.isclose(om, 0)
+        self.kw = np.zeros_like(om, dtype=np.complex128)
+        self.kw[mask] = 3 * (np.sin(om[mask]) - om[mask] * np.cos(om[mask])) / om[mask] ** 3
+        self.kw[~mask] = 1.0
+        self.kw *= grid.sigma_lanczos
+
+    def wd(self, krho):  # functionals.py:1157-1158
+        return self.grid.ifft(krho * self.kw)
+
+    def derive(self, krho):  # functionals.py:1160-1174
+        dphi = self.eos.dfex_volume(self.wd(krho))
+        return self.grid.ifft(self.grid.fft(dphi) * self.kw)
+
+    def value(self, krho):  # functionals.py:1176-1184
+        return self.grid.integrate(self.eos.fex_volume(self.wd(krho)))
+
+
+def add_wda(fener, sigma, epsilon, mass, temperature):
+    """FreeEnergy.add_correlation_wda_lj, cmmdft/functionals.py:339-362."""
+    R = fener.part_dict['HardSphere'].R
+    a = fener.part_dict['MFA'].vdw_a() if 'MFA' in fener.part_dict else None
+    eos = SumOfEOS([MBWR(mass, sigma, epsilon), CarnahanStarling(mass, R), MFAEOS(mass, sigma, epsilon, a=a)],
+                   [1, -1, -1])
+    w = WDA(fener.grid, R, eos, temperature)
+    fener.parts.append(w)
+    fener.part_names.append(w.name)
+    fener.part_dict[w.name] = w
+    return w
+
+
 def eos_chempot(eos, rho):
     """eos.py:31-33."""
     kT = boltzmann * eos.T
@@ -540,17 +630,20 @@ class NoSolutionError(Exception):
 
 
 class Solver(object):
-    """Fixed-point driver, cmmdft/solver.py:18-345 (criteria RES/RIUE)."""
+    """Fixed-point driver, cmmdft/solver.py:18-345 (criteria RES/RIUE/DER)."""
     name = 'SOLVER'
 
-    def __init__(self, fener, nsteps=500, threshold=1e-6, criterion='RIUE', min_iter=1):
+    def __init__(self, fener, nsteps=500, threshold=1e-6, criterion='RIUE', min_iter=1, a_tol=1e-6, r_tol=1e-4):
         self.grid = fener.grid
         self.fener = fener
         self.nsteps = nsteps
         crit = criterion if isinstance(criterion, list) else [criterion]
         thr = threshold if isinstance(threshold, list) else [threshold] * len(crit)
+        if not isinstance(criterion, list) and criterion.lower() == 'der':
+            thr = [1]  # solver.py:72-73
         self.criterion = [c.lower() for c in crit]
         self.threshold = thr
+        self.a_tol, self.r_tol = a_tol, r_tol
         self.lower_density = 1e-12
         self.iphase = 0
         self.curr_step = 0
@@ -610,6 +703,14 @@ class Solver(object):
                 G = self.get_new_rho(C1_new, self.fugacity)
                 self.RES = np.linalg.norm(G - rho_new) / np.sqrt(N_new) / np.sqrt(np.prod(self.grid.npoints))
                 v = self.RES
+            elif c == 'der':  # solver.py:200-205 with _get_dOmega :131-135
+                beta = self.fener.beta
+                rr = self._clip_density(rho_new)
+                dO = np.log(self.fener.wavelength ** 3 * rr) / beta + C1_new - self.chempot
+                keep = ~np.isclose(rho_new, 0)
+                w = np.abs(rho_new) * beta * dO / (self.a_tol + self.r_tol * np.abs(rho_new))
+                self.DER = np.linalg.norm(w[keep]) / np.sqrt(np.prod(self.grid.npoints))
+                v = self.DER
             else:
                 raise NotImplementedError(c)
             ok *= (v < t)

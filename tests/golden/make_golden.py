@@ -56,7 +56,7 @@ def import_reference(ref_root):
     return system, functionals, solver, extpot_calculator, eos
 
 
-def build(ref, npts, host, T, P_bar, tmp, tail=False):
+def build(ref, npts, host, T, P_bar, tmp, tail=False, wda=False):
     system, functionals, solver, extpot, eos = ref
     import yaff
     from cmmdft_b200.units import bar, angstrom
@@ -81,6 +81,8 @@ def build(ref, npts, host, T, P_bar, tmp, tail=False):
     fe.add_hard_sphere(version='WBII')
     fe.add_mean_field(tailcorrections=tail, cutoff=12 * angstrom, rewrite=True)
     fe.add_external_potential(load_fn=fn)
+    if wda:
+        fe.add_correlation_wda_lj()
     fe.set_temperature(T)  # user flow after adding parts (methane_ZIF8.ipynb)
     mb = eos.ModifiedBenedictWebbRubinEOS(mass, sig, eps)
     mu = mb.calculate_mu(T, P_bar * bar)
@@ -157,6 +159,12 @@ def main():
         out[key + '_N'] = N
         out[key + '_steps'] = s.curr_step
         out[key + '_conv'] = conv
+    # static Picard under the DER criterion (solver.py:200-205); a list criterion
+    # keeps its threshold (a plain 'der' forces 1, solver.py:72-73)
+    s = solver.Picard(b['prog'], nsteps=500, alpha_mix=0.1, method='static', criterion=['der'],
+                      threshold=[1e-3])
+    N, rho, conv = quiet(s.solve, mu, rho_a.copy(), 3)
+    out.update(der_rho=rho, der_N=N, der_steps=s.curr_step, der_conv=conv, der_value=s.DER)
     s = solver.Picard(b['prog'], nsteps=1, method='static')
     s._initiate_solving(mu)
     out['picard_omega'] = s._get_Omega(out['picard_rho'], grid.fft(out['picard_rho']))
@@ -174,6 +182,14 @@ def main():
     k = grid.fft(rho_b)
     out['dMFA_tail_b'] = bt['fe'].part_dict['MFA'].derive(k)
     out['vMFA_tail_b'] = bt['fe'].part_dict['MFA'].value(k)
+    # WDA correlation part on top (add_correlation_wda_lj, functionals.py:339-362)
+    bw = quiet(build, ref, 32, host, T, 1.0, tempfile.mkdtemp(prefix='cmm_golden_w_'), wda=True)
+    for tag, rho in (('a', rho_a), ('b', rho_b)):
+        parts, om, derivs, C1 = quiet(omega_parts, ref, bw, rho, mu)
+        out['wda_values_' + tag] = np.array(parts)
+        out['wda_omega_' + tag] = om
+        out['wda_dWDA_' + tag] = derivs[3]
+        out['wda_C1_' + tag] = C1
     np.savez_compressed(os.path.join(HERE, 'c0_32.npz'), **out)
     print('wrote c0_32.npz', 'picard steps', out['picard_steps'], 'anderson steps', out['and_steps'])
 

@@ -91,6 +91,18 @@ def test_functional_derivative(golden32, fn32, tag):
     assert scalar_rel(st[L.STAT_N3MAX], golden32["n3_" + tag].max()) < 1e-12
 
 
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_wda_part(golden32, cuda, tag):
+    fn = W.build_functional(cubic_host_276(0), (32, 32, 32), 300.0, methane_guest_params(), wda=True)
+    rho = golden32["rho_" + tag]
+    C1, st, Fhs, Fmfa = _c1(fn, rho)
+    ref = golden32["wda_C1_" + tag] - golden32["V"]
+    floor = {"a": 2e-9, "b": 1e-7}[tag]   # the hard-sphere noise floor, as above
+    assert fn.beta * np.max(np.abs(C1 - ref)) < floor
+    Fwda = st[L.STAT_WDA] * fn.plan.dr
+    assert scalar_rel(Fwda, golden32["wda_values_" + tag][3]) < 1e-11
+
+
 def test_mfa_tailcorrections(golden32, cuda):
     fn = W.build_functional(cubic_host_276(0), (32, 32, 32), 300.0, methane_guest_params(),
                             tailcorrections=True)
@@ -117,6 +129,15 @@ def test_static_picard_matches_reference(golden32, fn32):
     assert s.steps[0] == int(golden32["picard_steps"])
     assert relerr(rho[0], golden32["picard_rho"]) < 1e-10
     assert scalar_rel(N[0], golden32["picard_N"]) < 1e-10
+
+
+def test_static_picard_der_criterion(golden32, fn32):
+    mu = float(golden32["mu"])
+    s, N, rho, conv = _solve(fn32, mu, golden32["rho_a"], 'static', [1e-3], crit=['der'])
+    assert conv[0]
+    assert s.steps[0] == int(golden32["der_steps"])
+    assert relerr(rho[0], golden32["der_rho"]) < 1e-10
+    assert scalar_rel(N[0], golden32["der_N"]) < 1e-10
 
 
 def test_static_picard_three_steps(golden32, fn32):

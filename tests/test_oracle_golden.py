@@ -96,6 +96,17 @@ def test_static_picard_trajectory(golden32, case32):
     assert scalar_rel(N, golden32["picard_N"]) < 1e-10
 
 
+def test_static_picard_der_criterion(golden32, case32):
+    grid, fe = case32
+    s = O.Picard(fe, nsteps=500, alpha_mix=0.1, method="static", criterion=["der"], threshold=[1e-3])
+    N, rho, conv = s.solve(float(golden32["mu"]), golden32["rho_a"].copy())
+    assert conv and s.curr_step == int(golden32["der_steps"])
+    # near convergence dOmega is a difference of O(10 kT) terms that cancel to
+    # ~1e-4 kT, so the C1 noise floor (~1e-9 kT) shows at ~1e-5 relative
+    assert scalar_rel(s.DER, golden32["der_value"]) < 1e-4
+    assert relerr(rho, golden32["der_rho"]) < 1e-10
+
+
 def test_hybrid_anderson_converged(golden32, case32):
     grid, fe = case32
     mu = float(golden32["mu"])
@@ -113,3 +124,14 @@ def test_mfa_tailcorrections(golden32):
     mfa = fe.part_dict["MFA"]
     assert relerr(mfa.derive(k), golden32["dMFA_tail_b"]) < 1e-13
     assert scalar_rel(mfa.value(k), golden32["vMFA_tail_b"]) < 1e-12
+
+
+@pytest.mark.parametrize("tag", ["a", "b"])
+def test_wda_part(golden32, tag):
+    grid, fe = oracle_case(32, V=golden32["V"])
+    sig, eps, mass = methane_guest_params()
+    w = O.add_wda(fe, sig, eps, mass, 300.0)
+    rho = golden32["rho_" + tag]
+    k = grid.fft(rho)
+    assert fe.beta * np.max(np.abs(w.derive(k) - golden32["wda_dWDA_" + tag])) < 1e-12
+    assert scalar_rel(w.value(k), golden32["wda_values_" + tag][3]) < 1e-12

@@ -48,7 +48,7 @@ def test_noalloc_matches_allocating_pipeline_twice(case):
     for call in range(2):
         chat = plan.new_spec(B)
         stats = torch.full((B, L.NSTAT), np.nan, dtype=torch.float64, device="cuda")
-        rc = lib.cmm_fmt_c1_noalloc(plan.handle, B, None, fn.R, fn.beta, fn.version, L.ptr(fn.kst),
+        rc = lib.cmm_fmt_c1_noalloc(plan.handle, B, None, fn.R, fn.beta, fn.version, None, L.ptr(fn.kst),
                                     L.ptr(fn.wtab), L.ptr(spec), L.ptr(chat), L.ptr(stats), 7, _stream())
         assert rc == 0, lib.cmm_status_string(rc)
         got = chat.cpu().numpy()
@@ -62,6 +62,6 @@ def test_noalloc_rejects_batches_beyond_its_scratch(case):
     fn, spec = case
     lib = L.lib()
     cap = int(lib.cmm_fmt_c1_noalloc_capacity(fn.plan.handle))
-    rc = lib.cmm_fmt_c1_noalloc(fn.plan.handle, cap + 1, None, fn.R, fn.beta, fn.version, L.ptr(fn.kst),
+    rc = lib.cmm_fmt_c1_noalloc(fn.plan.handle, cap + 1, None, fn.R, fn.beta, fn.version, None, L.ptr(fn.kst),
                                 L.ptr(fn.wtab), L.ptr(spec), L.ptr(spec), L.ptr(spec), 1, _stream())
     assert rc == 6  # CMM_ERR_WORKSPACE, before any device work
