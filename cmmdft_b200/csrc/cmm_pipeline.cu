@@ -443,17 +443,20 @@ __global__ void k_fmt_weights(GridDev g, double R, double2* __restrict__ wtab) {
 
 // ================================== column pass 1: rho_hat -> 5 fields ==
 // Outputs (field stride fsw): 0 = n0 (w0), 1 = n3 (w3), 2..4 = nv2 (x, y, z).
-template <int N1C, int TCC>
-__global__ void __launch_bounds__(CMM_COL_THREADS)
-k_col_weights(GridDev g, const int* __restrict__ active, double R, double inv_npts,
-              const double2* __restrict__ rhohat, double2* __restrict__ wout, size_t fsw,
-              const double2* __restrict__ kst, const double2* __restrict__ wtab, double* __restrict__ part,
-              int nslot_part, int want_value, int tc, int nout, double wda_D) {
+// The WDA field is a template parameter, as in the plane pass, so that the
+// plain kernels keep their register budget.
+template <int N1C, int TCC, bool WDA>
+__device__ __forceinline__ void col_weights_body(GridDev g, const int* __restrict__ active, double R,
+                                                 double inv_npts, const double2* __restrict__ rhohat,
+                                                 double2* __restrict__ wout, size_t fsw,
+                                                 const double2* __restrict__ kst, const double2* __restrict__ wtab,
+                                                 double* __restrict__ part, int nslot_part, int want_value, int tc,
+                                                 double wda_D) {
   const int b = blockIdx.y, tile = blockIdx.x;
   if (active && !active[b]) return;
   const ColShape<N1C, TCC> sh(g, tc);
   const int c0 = tile * sh.tc;
-  const int ns = nout;  // 5, or 6 with the WDA weighted density
+  const int ns = WDA ? 6 : 5;  // with the WDA weighted density last
   ColSmem s = col_smem_setup(g, sh, ns);
   load_col_tile(g, s, sh, ns, 0, rhohat, b, c0, nullptr);
   __syncthreads();
@@ -471,7 +474,7 @@ k_col_weights(GridDev g, const int* __restrict__ active, double R, double inv_np
       mfa += g.wt3[col - (col / g.h3) * g.h3] * (F.x * F.x + F.y * F.y) * K.x;
     }
     F = cscale(F, inv_npts);
-    if (ns > 5) cel(s, sh, ns, 5, p1, c) = cscale(F, wda_weight_at(g, p1, col, wda_D));
+    if (WDA) cel(s, sh, ns, 5, p1, c) = cscale(F, wda_weight_at(g, p1, col, wda_D));
     cel(s, sh, ns, 1, p1, c) = cscale(F, w.w3);
     // -i * v * F
     cel(s, sh, ns, 2, p1, c) = make_double2(F.y * w.v[0], -F.x * w.v[0]);
@@ -489,19 +492,37 @@ k_col_weights(GridDev g, const int* __restrict__ active, double R, double inv_np
   }
 }
 
+#define COL_WEIGHTS_ARGS                                                                                   \
+  GridDev g, const int *__restrict__ active, double R, double inv_npts, const double2 *__restrict__ rhohat, \
+      double2 *__restrict__ wout, size_t fsw, const double2 *__restrict__ kst,                             \
+      const double2 *__restrict__ wtab, double *__restrict__ part, int nslot_part, int want_value, int tc,  \
+      double wda_D
+template <int N1C, int TCC>
+__global__ void __launch_bounds__(CMM_COL_THREADS) k_col_weights(COL_WEIGHTS_ARGS) {
+  col_weights_body<N1C, TCC, false>(g, active, R, inv_npts, rhohat, wout, fsw, kst, wtab, part, nslot_part,
+                                    want_value, tc, wda_D);
+}
+template <int N1C, int TCC>
+__global__ void __launch_bounds__(CMM_COL_THREADS) k_col_weights_wda(COL_WEIGHTS_ARGS) {
+  col_weights_body<N1C, TCC, true>(g, active, R, inv_npts, rhohat, wout, fsw, kst, wtab, part, nslot_part,
+                                   want_value, tc, wda_D);
+}
+
 // ======================== column pass 2: dPhi spectra -> C1 spectrum ====
 // Inputs: 5 dPhi spectra (field stride fsg): g_s (pairs with w0), g3 (w3),
 // gv (x,y,z, pairs with kwv2); rho_hat for the MFA term.  gin == NULL: MFA only.
-template <int N1C, int TCC>
-__global__ void __launch_bounds__(CMM_COL_THREADS)
-k_col_backconv(GridDev g, const int* __restrict__ active, double R, double scale,
-               const double2* __restrict__ gin, size_t fsg, const double2* __restrict__ rhohat,
-               const double2* __restrict__ kst, const double2* __restrict__ wtab, double2* __restrict__ chat,
-               int tc, int nin, double wda_D, double inv_npts) {
+template <int N1C, int TCC, bool WDA>
+__device__ __forceinline__ void col_backconv_body(GridDev g, const int* __restrict__ active, double R,
+                                                  double scale, const double2* __restrict__ gin, size_t fsg,
+                                                  const double2* __restrict__ rhohat,
+                                                  const double2* __restrict__ kst, const double2* __restrict__ wtab,
+                                                  double2* __restrict__ chat, int tc, double wda_D,
+                                                  double inv_npts) {
   const int b = blockIdx.y;
   if (active && !active[b]) return;
   const ColShape<N1C, TCC> sh(g, tc);
   const int c0 = blockIdx.x * sh.tc;
+  const int nin = WDA ? 6 : 5;
   const int ns = nin + 1;    // 5 dPhi (+1 WDA) fields, then rho_hat
   const int fr = nin;        // slot of rho_hat
   ColSmem s = col_smem_setup(g, sh, ns);
@@ -527,7 +548,7 @@ k_col_backconv(GridDev g, const int* __restrict__ active, double R, double scale
       acc = cadd(acc, make_double2(-gv.y, gv.x));
       acc = cscale(acc, scale);
       // WDA: ifft(fft(dphi) kw), no 1/beta (the EOS derivative is an energy)
-      if (nin > 5) acc = cadd(acc, cscale(cel(s, sh, ns, 5, p1, c), wda_weight_at(g, p1, col, wda_D) * inv_npts));
+      if (WDA) acc = cadd(acc, cscale(cel(s, sh, ns, 5, p1, c), wda_weight_at(g, p1, col, wda_D) * inv_npts));
     }
     const double2 K = __ldg(kst + (size_t)p1 * nc + col);
     acc = cadd(acc, cmul(cel(s, sh, ns, fr, p1, c), K));
@@ -536,6 +557,19 @@ k_col_backconv(GridDev g, const int* __restrict__ active, double R, double scale
   __syncthreads();
   col_fft<true>(g, s, sh, ns, 0, 1);
   store_col_tile(g, s, sh, ns, 0, chat, b, c0, nullptr);
+}
+
+#define COL_BACKCONV_ARGS                                                                                  \
+  GridDev g, const int *__restrict__ active, double R, double scale, const double2 *__restrict__ gin,      \
+      size_t fsg, const double2 *__restrict__ rhohat, const double2 *__restrict__ kst,                     \
+      const double2 *__restrict__ wtab, double2 *__restrict__ chat, int tc, double wda_D, double inv_npts
+template <int N1C, int TCC>
+__global__ void __launch_bounds__(CMM_COL_THREADS) k_col_backconv(COL_BACKCONV_ARGS) {
+  col_backconv_body<N1C, TCC, false>(g, active, R, scale, gin, fsg, rhohat, kst, wtab, chat, tc, wda_D, inv_npts);
+}
+template <int N1C, int TCC>
+__global__ void __launch_bounds__(CMM_COL_THREADS) k_col_backconv_wda(COL_BACKCONV_ARGS) {
+  col_backconv_body<N1C, TCC, true>(g, active, R, scale, gin, fsg, rhohat, kst, wtab, chat, tc, wda_D, inv_npts);
 }
 
 // ===================================== plane pass: dPhi/dn (White-Bear) ==
@@ -623,14 +657,16 @@ __device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, 
   return o;
 }
 
-template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_FMT_THREADS)
-k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
-            const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
-            double* __restrict__ part, int nslot_part, int want) {
+// The WDA branch is a template parameter: its EOS code, compiled into the
+// plain kernel, pushes that kernel past the 64 registers a 1024-thread block
+// allows and makes it spill.
+template <int N2C, int M3C, bool has_wda>
+__device__ __forceinline__ void plane_fmt_body(GridDev g, const int* __restrict__ active, double R, int version,
+                                               const cmm_wda_eos& wda, const double2* __restrict__ win,
+                                               size_t fsw, double2* __restrict__ gout, size_t fsg,
+                                               double* __restrict__ part, int nslot_part, int want) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
-  const bool has_wda = (version & CMM_WDA) != 0;
   const int ns = has_wda ? 6 : 5;
   PlaneSmem s = plane_smem_setup<N2C, M3C>(g, ns);
   const PlaneShape<N2C, M3C> sh(g);
@@ -679,6 +715,22 @@ k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version, cm
   __syncthreads();
   plane_forward<N2C, M3C>(g, s, ns);
   store_spec_planes<N2C, M3C>(g, s, ns, gout, poff, fsg);
+}
+
+template <int N2C, int M3C>
+__global__ void __launch_bounds__(CMM_FMT_THREADS)
+k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
+            const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
+            double* __restrict__ part, int nslot_part, int want) {
+  plane_fmt_body<N2C, M3C, false>(g, active, R, version, wda, win, fsw, gout, fsg, part, nslot_part, want);
+}
+
+template <int N2C, int M3C>
+__global__ void __launch_bounds__(CMM_FMT_THREADS)
+k_plane_fmt_wda(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
+                const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
+                double* __restrict__ part, int nslot_part, int want) {
+  plane_fmt_body<N2C, M3C, true>(g, active, R, version, wda, win, fsw, gout, fsg, part, nslot_part, want);
 }
 
 // ========================================== plane pass: solver updates ==
@@ -1040,19 +1092,32 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
     if (!(want & 1)) return CMM_ERR_ARG;
     LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), col_smem_bytes(g->n1, tc, 6), st, g->dev, d_active, R,
                1.0 / (beta * npts), (const double2*)nullptr, fs, (const double2*)d_rhohat, (const double2*)d_kst,
-               wt, (double2*)d_chat, tc, 5, 0.0, 1.0 / npts);
+               wt, (double2*)d_chat, tc, 0.0, 1.0 / npts);
     return last_err();
   }
-  LAUNCH_COL(ck, k_col_weights, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
-             (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0, tc,
-             nf, we.D);
+  if (has_wda)
+    LAUNCH_COL(ck, k_col_weights_wda, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
+               (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0,
+               tc, we.D);
+  else
+    LAUNCH_COL(ck, k_col_weights, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
+               (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0,
+               tc, we.D);
   const size_t ps = plane_smem_bytes(g->n2, g->n3, nf);
-  LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, d_active, R,
-                 version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
-  if (want & 1) {
+  if (has_wda)
+    LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt_wda, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, d_active,
+                   R, version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
+  else
+    LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, d_active, R,
+                   version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
+  if ((want & 1) && has_wda) {
+    LAUNCH_COL(ck, k_col_backconv_wda, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),
+               (const double2*)gbuf, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt, (double2*)d_chat,
+               tc, we.D, 1.0 / npts);
+  } else if (want & 1) {
     LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),
                (const double2*)gbuf, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt, (double2*)d_chat,
-               tc, nf, we.D, 1.0 / npts);
+               tc, we.D, 1.0 / npts);
   }
   return last_err();
 }
