@@ -225,6 +225,7 @@ class BatchSolve(object):
                  damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5), divergence_guard=False,
                  a_tol=1e-6, r_tol=1e-4):
         self.fn = fn
+        self.host_out = None
         self.plan = fn.plan
         self.mu = np.asarray(chempots, dtype=np.float64).ravel()
         self.B = B = len(self.mu)
@@ -365,8 +366,19 @@ class BatchSolve(object):
     def initial_density(self, rho0):
         self.rho0.copy_(rho0)
 
-    def solve(self, rho0, cf=None):
-        """Run all instances from rho0 [B, N1, N2, N3]; returns (N, rho, converged)."""
+    def solve(self, rho0, cf=None, host_out=None):
+        """Run all instances from rho0 [B, N1, N2, N3]; returns (N, rho, converged).
+
+        host_out: optional pinned CPU tensor [B, N1, N2, N3].  Each instance's
+        final density is copied into it on a side stream as soon as that
+        instance is finished, overlapping the copy with the iterations of
+        the instances still running; all copies have landed when solve
+        returns."""
+        self.host_out = host_out
+        if host_out is not None:
+            if not host_out.is_pinned() or tuple(host_out.shape) != tuple(rho0.shape):
+                raise ValueError("host_out must be a pinned tensor of the shape of rho0")
+            self._copy_stream = torch.cuda.Stream()
         self.initial_density(rho0)
         B = self.B
         self.cf = np.ones(B) if cf is None else np.asarray(cf, dtype=float).copy()
@@ -389,6 +401,8 @@ class BatchSolve(object):
                     self.failed[b] = True
                     retry[b] = False
             todo = retry
+        if host_out is not None:
+            self._copy_stream.synchronize()
         if self.failed.any():
             raise NoSolutionError("instances %s hit non-finite densities on every retry"
                                   % list(np.where(self.failed)[0]))
@@ -487,6 +501,13 @@ class BatchSolve(object):
 
     def _finish(self, b, rho_b, N, steps, conv):
         self.result[b].copy_(rho_b)
+        if self.host_out is not None:
+            ev = torch.cuda.Event()
+            ev.record()
+            cs = self._copy_stream
+            cs.wait_event(ev)
+            with torch.cuda.stream(cs):
+                self.host_out[b].copy_(self.result[b], non_blocking=True)
         self.N_out[b] = N
         self.conv[b] = conv
         self.steps[b] = steps

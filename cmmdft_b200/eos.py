@@ -8,11 +8,107 @@ mean-field EOS (:523-546).  These are scalar/1-D numpy evaluations that set
 up mu(P) and bulk densities; the grid solve never calls them per point.
 """
 import numpy as np
-from scipy.optimize import brentq
 
 from .units import angstrom, boltzmann, planck
 
 __all__ = ['EquationOfState', 'SumOfEOS', 'ModifiedBenedictWebbRubinEOS', 'CarnahanStarlingEOS', 'MFAEOS']
+
+
+_scalar_powers = [False]
+
+
+def _ipow(x, k):
+    """x ** k for an integer k.  While brentq lanes are evaluated, each
+    element is raised as a Python float (C pow), which rounds differently
+    from numpy's array power in the last bit: the lanes then reproduce the
+    scalar evaluations scipy's brentq makes one root at a time."""
+    if _scalar_powers[0] and isinstance(x, np.ndarray):
+        return np.array([v ** k for v in x.tolist()])
+    return x ** k
+
+
+def brentq_lanes(f, a, b, xtol=2e-12, rtol=4 * np.finfo(float).eps, maxiter=100):
+    """Brent's root finder (R. P. Brent, Algorithms for Minimization without
+    Derivatives, 1973, ch. 4) run on many brackets at once.
+
+    Every lane takes the steps scipy.optimize.brentq (default tolerances)
+    takes on its own bracket: the same bracket bookkeeping, inverse
+    quadratic / secant trial step, acceptance test, bisection fallback and
+    minimum step of (xtol + rtol |x|) / 2.  ``f(x, idx)`` evaluates the
+    function of lanes ``idx`` at ``x`` (vectorised).  Returns the roots.
+    """
+    _scalar_powers[0] = True
+    try:
+        return _brent_loop(f, a, b, xtol, rtol, maxiter)
+    finally:
+        _scalar_powers[0] = False
+
+
+def _brent_loop(f, a, b, xtol, rtol, maxiter):
+    xpre = np.array(a, dtype=float)
+    xcur = np.array(b, dtype=float)
+    n = xpre.size
+    fpre = f(xpre, np.arange(n))
+    fcur = f(xcur, np.arange(n))
+    root = np.full(n, np.nan)
+    done = np.zeros(n, dtype=bool)
+    if np.any((fpre * fcur) > 0):
+        raise ValueError("f(a) and f(b) must have different signs")
+    z = fpre == 0
+    root[z], done[z] = xpre[z], True
+    z = (fcur == 0) & ~done
+    root[z], done[z] = xcur[z], True
+    xblk = np.zeros(n)
+    fblk = np.zeros(n)
+    spre = np.zeros(n)
+    scur = np.zeros(n)
+    for _ in range(maxiter):
+        live = np.nonzero(~done)[0]
+        if live.size == 0:
+            break
+        xp, xc, xb = xpre[live], xcur[live], xblk[live]
+        fp, fc, fb = fpre[live], fcur[live], fblk[live]
+        sp, sc = spre[live], scur[live]
+        # a sign change between pre and cur: the bracket is [pre, cur]
+        m = (fp * fc) < 0
+        xb = np.where(m, xp, xb)
+        fb = np.where(m, fp, fb)
+        sp = np.where(m, xc - xp, sp)
+        sc = np.where(m, xc - xp, sc)
+        # keep the best estimate in cur
+        sw = np.abs(fb) < np.abs(fc)
+        xp = np.where(sw, xc, xp)
+        xc, xb = np.where(sw, xb, xc), np.where(sw, xp, xb)
+        fp = np.where(sw, fc, fp)
+        fc, fb = np.where(sw, fb, fc), np.where(sw, fp, fb)
+        delta = (xtol + rtol * np.abs(xc)) / 2
+        sbis = (xb - xc) / 2
+        fin = (fc == 0) | (np.abs(sbis) < delta)
+        root[live[fin]] = xc[fin]
+        done[live[fin]] = True
+        # trial step: secant when pre and blk coincide, else inverse quadratic
+        tryit = ~fin & (np.abs(sp) > delta) & (np.abs(fc) < np.abs(fp))
+        with np.errstate(divide='ignore', invalid='ignore'):
+            stry_s = -fc * (xc - xp) / (fc - fp)
+            dpre = (fp - fc) / (xp - xc)
+            dblk = (fb - fc) / (xb - xc)
+            stry_q = -fc * (fb * dblk - fp * dpre) / (dblk * dpre * (fb - fp))
+        stry = np.where(xp == xb, stry_s, stry_q)
+        good = tryit & (2 * np.abs(stry) < np.minimum(np.abs(sp), 3 * np.abs(sbis) - delta))
+        sp_new = np.where(good, sc, sbis)
+        sc_new = np.where(good, stry, sbis)
+        step = np.where(np.abs(sc_new) > delta, sc_new, np.where(sbis > 0, delta, -delta))
+        act = ~fin
+        li = live[act]
+        xpre[li], fpre[li] = xc[act], fc[act]
+        xblk[li], fblk[li] = xb[act], fb[act]
+        spre[li], scur[li] = sp_new[act], sc_new[act]
+        xcur[li] = xc[act] + step[act]
+        if li.size:
+            fcur[li] = f(xcur[li], li)
+    live = ~done
+    root[live] = xcur[live]   # maxiter reached: the last iterate, as brentq returns it
+    return root
 
 
 class EquationOfState(object):
@@ -59,46 +155,55 @@ class EquationOfState(object):
             out.append([(grid[j - 1], grid[j]) for j in js])
         return out
 
-    def solve_densities_from_chempots(self, chempots, n_rough_gridpoints=1000):
-        """All roots rho of mu(rho) = mu per chempot (<= 2 branches kept), eos.py:85-119."""
-        grid = self.get_rough_density_grid(n_rough_gridpoints)
-        kT = boltzmann * self.temperature
-        mg = kT * np.log(self.wvl ** 3 * grid) + self.excess_free_energy_particle(grid) + \
-            grid * self.derivative_excess_free_energy_particle(grid)
-        out = np.zeros([len(chempots), 2]) * np.nan
-        for i, (mu, iv) in enumerate(zip(chempots, self._brackets(chempots, mg, grid))):
-            f = lambda r: kT * np.log(self.wvl ** 3 * r) + self.excess_free_energy_particle(r) + \
-                r * self.derivative_excess_free_energy_particle(r) - mu
-            sols = sorted(brentq(f, a, b) for a, b in iv)
+    def _solve_all(self, targets, func, grid, ncol):
+        """Every root of func(rho) = target in each bracketing interval of the
+        rough grid, sorted per target (the scan and brentq loop of
+        eos.py:85-157); the brackets of all targets are solved together by
+        brentq_lanes."""
+        targets = np.asarray(targets, dtype=float).ravel()
+        brackets = self._brackets(targets, func(grid), grid)
+        owner = np.array([i for i, iv in enumerate(brackets) for _ in iv], dtype=int)
+        out = np.zeros([len(targets), ncol]) * np.nan
+        if owner.size == 0:
+            return out
+        lo = np.array([a for iv in brackets for a, _ in iv])
+        hi = np.array([b for iv in brackets for _, b in iv])
+        tg = targets[owner]
+        roots = brentq_lanes(lambda r, idx: func(r) - tg[idx], lo, hi)
+        for i in range(len(targets)):
+            sols = sorted(roots[owner == i])
             if len(sols) > 3:
                 raise ValueError('more than 3 density branches')
             out[i, :len(sols)] = sols
         return out
+
+    def solve_densities_from_chempots(self, chempots, n_rough_gridpoints=1000):
+        """All roots rho of mu(rho) = mu per chempot (<= 2 branches kept), eos.py:85-119."""
+        kT = boltzmann * self.temperature
+        func = lambda r: kT * np.log(self.wvl ** 3 * r) + self.excess_free_energy_particle(r) + \
+            r * self.derivative_excess_free_energy_particle(r)
+        return self._solve_all(chempots, func, self.get_rough_density_grid(n_rough_gridpoints), 2)
 
     def solve_densities_from_pressures(self, pressures, n_rough_gridpoints=10000):
         """All roots rho of p(rho) = p, eos.py:121-157."""
-        grid = self.get_rough_density_grid(n_rough_gridpoints)
         kT = boltzmann * self.temperature
-        pg = kT * grid + grid ** 2 * self.derivative_excess_free_energy_particle(grid)
-        out = np.zeros([len(pressures), 3]) * np.nan
-        for i, (p, iv) in enumerate(zip(pressures, self._brackets(pressures, pg, grid))):
-            f = lambda r: kT * r + r ** 2 * self.derivative_excess_free_energy_particle(r) - p
-            sols = sorted(brentq(f, a, b) for a, b in iv)
-            if len(sols) > 3:
-                raise ValueError('more than 3 density branches')
-            out[i, :len(sols)] = sols
-        return out
+        func = lambda r: kT * r + _ipow(r, 2) * self.derivative_excess_free_energy_particle(r)
+        return self._solve_all(pressures, func, self.get_rough_density_grid(n_rough_gridpoints), 3)
 
     def calculate_mu(self, temp, pressure):
-        """Chemical potential of the lowest-density branch at (T, P), eos.py:209-215."""
+        """Chemical potential of the lowest-density branch at (T, P), eos.py:209-215.
+        ``pressure`` may be an array: one chemical potential per pressure."""
         self.set_temperature(temp)
-        rho = self.solve_densities_from_pressures([pressure])[0][0]
-        return self.compute_chempot(rho)
+        rho = self.solve_densities_from_pressures(np.atleast_1d(pressure))[:, 0]
+        mu = self.compute_chempot(rho)
+        return mu if np.ndim(pressure) else float(mu[0])
 
     def bulk_density(self, temp, chempot):
-        """Lowest density branch at (T, mu) (Calculator.return_loading, calculator.py:129-131)."""
+        """Lowest density branch at (T, mu) (Calculator.return_loading, calculator.py:129-131).
+        ``chempot`` may be an array: one density per chemical potential."""
         self.set_temperature(temp)
-        return float(np.nanmin(self.solve_densities_from_chempots([chempot]), axis=1)[0])
+        rho = np.nanmin(self.solve_densities_from_chempots(np.atleast_1d(chempot)), axis=1)
+        return rho if np.ndim(chempot) else float(rho[0])
 
 
 class SumOfEOS(EquationOfState):
@@ -171,18 +276,18 @@ class ModifiedBenedictWebbRubinEOS(EquationOfState):
 
     def _G(self, rho):
         rr = rho * self.sigma ** 3
-        F = np.exp(-self.gamma * rr ** 2)
+        F = np.exp(-self.gamma * _ipow(rr, 2))
         ig = 1.0 / (2 * self.gamma)
         G = [ig * (1 - F)]
         for n in range(2, 7):
-            G.append(-ig * (F * rr ** (2 * (n - 1)) - 2 * (n - 1) * G[-1]))
+            G.append(-ig * (F * _ipow(rr, 2 * (n - 1)) - 2 * (n - 1) * G[-1]))
         return G
 
     def excess_free_energy_particle(self, rho):
         A = 0.0
         rr = rho * self.sigma ** 3
         for i, ai in enumerate(self.a):
-            A += ai / (i + 1) * rr ** (i + 1)
+            A += ai / (i + 1) * _ipow(rr, i + 1)
         for bi, Gi in zip(self.b, self._G(rho)):
             A += bi * Gi
         return A * self.epsilon
@@ -191,10 +296,10 @@ class ModifiedBenedictWebbRubinEOS(EquationOfState):
         dA = 0.0
         rr = rho * self.sigma ** 3
         for i, ai in enumerate(self.a):
-            dA += ai * rr ** i * self.sigma ** 3
-        F = np.exp(-self.gamma * rr ** 2)
+            dA += ai * _ipow(rr, i) * self.sigma ** 3
+        F = np.exp(-self.gamma * _ipow(rr, 2))
         for t, bi in enumerate(self.b):
-            dA += bi * self.sigma ** 3 * rr ** (2 * t + 1) * F
+            dA += bi * self.sigma ** 3 * _ipow(rr, 2 * t + 1) * F
         return dA * self.epsilon
 
     def get_rough_density_grid(self, npoints):
@@ -211,11 +316,11 @@ class CarnahanStarlingEOS(EquationOfState):
 
     def excess_free_energy_particle(self, rho):
         kT = boltzmann * self.temperature
-        return kT * (4 * self.eta * rho - 3 * (self.eta * rho) ** 2) / (1 - self.eta * rho) ** 2
+        return kT * (4 * self.eta * rho - 3 * _ipow(self.eta * rho, 2)) / _ipow(1 - self.eta * rho, 2)
 
     def derivative_excess_free_energy_particle(self, rho):
         kT = boltzmann * self.temperature
-        return 2 * kT * self.eta * (2 - self.eta * rho) / (1 - self.eta * rho) ** 3
+        return 2 * kT * self.eta * (2 - self.eta * rho) / _ipow(1 - self.eta * rho, 3)
 
 
 class MFAEOS(EquationOfState):

@@ -35,12 +35,14 @@ def solve_isotherm(host, pressures, temperature, guest, npoints, method='hybrida
     rho0 = W.initial_density(fn, mus, ninit=bulks if start == 'bulk' else None)
     s = BT.BatchSolve(fn, mus, method=method, nsteps=nsteps, threshold=threshold, criterion=criterion,
                       m=m, alpha_mix=alpha_mix, divergence_guard=divergence_guard)
-    N, rho, conv = s.solve(rho0)
+    # densities land in pinned host memory while the rest of the batch iterates
+    host = torch.empty(tuple(rho0.shape), dtype=torch.float64, pin_memory=True) if return_density else None
+    N, rho, conv = s.solve(rho0, host_out=host)
     out = dict(mu=mus, rho_bulk=bulks, N=np.array(N), converged=np.array(conv), steps=s.steps.copy(),
                diverged=s.diverged.copy(),
                solver=s, functional=fn)
     if return_density:
-        out['rho'] = rho.cpu().numpy()
+        out['rho'] = host.numpy()
     return out
 
 

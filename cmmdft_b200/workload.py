@@ -95,12 +95,8 @@ def isotherm_inputs(pressures, temperature, guest):
     """(mu, rho_bulk) per pressure from the MBWR EOS (eos.py:209-215, calculator.py:129-131)."""
     sigma, epsilon, mass = guest
     mb = ModifiedBenedictWebbRubinEOS(mass, sigma, epsilon)
-    mus, bulks = [], []
-    for p in pressures:
-        mu = mb.calculate_mu(temperature, p)
-        mus.append(mu)
-        bulks.append(mb.bulk_density(temperature, mu))
-    return np.array(mus), np.array(bulks)
+    mus = mb.calculate_mu(temperature, np.asarray(pressures, dtype=float).ravel())
+    return mus, mb.bulk_density(temperature, mus)
 
 
 def initial_density(fn, chempots, ninit=None):

@@ -167,11 +167,13 @@ def test_isotherm_64_matches_reference(golden64, cuda):
     P = golden64["pressures"]
     ok = golden64["steps"] < 500  # points the reference itself converged
     mus, bulks = W.isotherm_inputs(P * bar, 300.0, guest)
-    assert np.allclose(mus, golden64["mu"], rtol=1e-13, atol=0)
+    assert np.array_equal(mus, golden64["mu"])
     r0 = W.initial_density(fn, mus, ninit=bulks)
     s = BT.BatchSolve(fn, mus, method='hybridanderson', nsteps=500, threshold=TIGHT_THR,
                       criterion=TIGHT_CRIT)
-    N, rho, conv = s.solve(r0)
+    host = torch.empty(tuple(r0.shape), dtype=torch.float64, pin_memory=True)
+    N, rho, conv = s.solve(r0, host_out=host)
+    assert torch.equal(host, rho.cpu())   # copied per instance while the batch ran
     assert conv[ok].all()
     for i in np.where(ok)[0]:
         assert scalar_rel(N[i], golden64["N"][i]) < 1e-10
