@@ -16,7 +16,7 @@ STAT_WDA, STAT_DER = 18, 19
 NSTAT = 20
 MAX_HIST = 8
 MAX_FIELDS = 12
-FMT, MFMT, WBII, ANTISYM, NOHS, WDA = 0, 1, 2, 8, 16, 32
+FMT, MFMT, WBII, ANTISYM, NOHS, WDA, TENSOR = 0, 1, 2, 8, 16, 32, 64
 
 
 class WdaEos(ctypes.Structure):
@@ -42,6 +42,7 @@ _SIGS = {
     "cmm_status_string": ([c_int], ctypes.c_char_p),
     "cmm_grid_create": ([c_int, c_int, c_int, P(c_double), P(c_void_p)], c_int),
     "cmm_grid_destroy": ([c_void_p], c_int),
+    "cmm_grid_set_staging": ([c_void_p, c_int], c_int),
     "cmm_grid_spectrum_size": ([c_void_p, P(c_ll), P(c_int)], c_int),
     "cmm_spectrum_index": ([c_void_p, P(c_int), P(c_int), P(c_int)], c_int),
     "cmm_plane_smem_bytes": ([c_void_p, c_int, P(ctypes.c_size_t)], c_int),

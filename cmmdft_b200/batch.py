@@ -200,7 +200,7 @@ def workspace(fn, B, nring):
         trial=torch.empty((B, n1, n2, n3), dtype=f64, device=dev),
         rho0=torch.empty((B, n1, n2, n3), dtype=f64, device=dev),
         rhohat=plan.new_spec(B), that=plan.new_spec(B), chat=plan.new_spec(B), chat2=plan.new_spec(B),
-        buf=E.Buffers(plan, B),
+        buf=E.Buffers(plan, B, nwork=fn.nwork),
         params=torch.zeros((B, 4), dtype=f64, device=dev),
         coef=torch.zeros((B, L.MAX_FIELDS), dtype=f64, device=dev),
         active=torch.zeros(B, dtype=torch.int32, device=dev),

@@ -12,6 +12,7 @@
 #define CMM_PLANE_THREADS 512
 #define CMM_COL_THREADS 256
 #define CMM_FMT_THREADS 1024   // the 5-field plane pass (one block per SM)
+#define CMM_ROW_THREADS 512    // staged z-row passes
 
 // Per-instance reduction slots (see cmm_stat_* in the public header).
 #define NQ CMM_NSTAT
@@ -52,6 +53,7 @@ struct cmm_grid {
   // one device allocation holding every table
   void* dmem;
   GridDev dev;
+  int staging;                 // 0: by size, 1: staged plane passes always
 };
 
 static inline int cmm_div_up(long long a, long long b) { return (int)((a + b - 1) / b); }

@@ -210,6 +210,12 @@ extern "C" int cmm_grid_destroy(cmm_grid* g) {
   return CMM_OK;
 }
 
+extern "C" int cmm_grid_set_staging(cmm_grid* g, int mode) {
+  if (!g || mode < 0 || mode > 1) return CMM_ERR_ARG;
+  g->staging = mode;
+  return CMM_OK;
+}
+
 extern "C" int cmm_grid_spectrum_size(const cmm_grid* g, long long* nspec, int* h3) {
   if (!g) return CMM_ERR_ARG;
   if (nspec) *nspec = (long long)g->n1 * g->n2 * g->h3;

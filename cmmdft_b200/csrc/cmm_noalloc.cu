@@ -63,6 +63,7 @@ extern "C" int cmm_fmt_c1_noalloc(const cmm_grid* g, int batch, const int* d_act
                                   int version, const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab,
                                   const double* d_rhohat, double* d_chat, double* d_stats, int want, void* stream) {
   if (!g || batch < 1 || !d_kst || !d_rhohat) return CMM_ERR_ARG;
+  if (version & CMM_TENSOR) return CMM_ERR_UNSUPPORTED;  // 24 spectra: beyond the sizing below
   if ((want & 1) && !d_chat) return CMM_ERR_ARG;
   if ((want & 6) && !d_stats) return CMM_ERR_ARG;
   if ((size_t)batch > cmm_fmt_c1_noalloc_capacity(g)) return CMM_ERR_WORKSPACE;  // beyond the fixed scratch

@@ -66,12 +66,10 @@ __device__ __forceinline__ void axis_fft(double2* base, const FftAxis& ax, const
   else fft_rt<INV>(base, ax, tw, twmul, npencil, pstride, estride);
 }
 
-// R2C twist on every row: pairs (k, m3-k), k = 0..m3/2, rows fastest.
-template <int N2C, int M3C>
-__device__ void r2c_twist(const GridDev& g, const PlaneSmem& s, int nslot) {
-  const PlaneShape<N2C, M3C> sh(g);
-  const int m3 = sh.m3, h3 = sh.h3;
-  const int nrow = nslot * sh.n2;
+// R2C twist on `nrow` rows: pairs (k, m3-k), k = 0..m3/2, rows fastest.
+template <int M3C>
+__device__ void r2c_twist_rows(const GridDev& g, const PlaneSmem& s, int nrow) {
+  const int m3 = M3C ? M3C : g.m3, h3 = m3 + 1;
   const int total = nrow * (m3 / 2 + 1);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     const int k = t / nrow, row = t - k * nrow;
@@ -95,11 +93,9 @@ __device__ void r2c_twist(const GridDev& g, const PlaneSmem& s, int nslot) {
 }
 
 // C2R twist: Zin[k] = (X[k] + conj X[m-k]) + i (X[k] - conj X[m-k]) e^{2 pi i k / N3}.
-template <int N2C, int M3C>
-__device__ void c2r_twist(const GridDev& g, const PlaneSmem& s, int nslot) {
-  const PlaneShape<N2C, M3C> sh(g);
-  const int m3 = sh.m3, h3 = sh.h3;
-  const int nrow = nslot * sh.n2;
+template <int M3C>
+__device__ void c2r_twist_rows(const GridDev& g, const PlaneSmem& s, int nrow) {
+  const int m3 = M3C ? M3C : g.m3, h3 = m3 + 1;
   const int total = nrow * (m3 / 2 + 1);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     const int k = t / nrow, row = t - k * nrow;
@@ -120,12 +116,26 @@ __device__ void c2r_twist(const GridDev& g, const PlaneSmem& s, int nslot) {
   __syncthreads();
 }
 
+// z rows only: real rows (natural z) -> DIF z + R2C twist, and back.
+template <int M3C>
+__device__ void row_forward(const GridDev& g, const PlaneSmem& s, int nrow) {
+  const int h3 = (M3C ? M3C : g.m3) + 1;
+  axis_fft<false, M3C>(s.slots, g.ax3, s.tw3, 2, nrow, h3, 1);
+  r2c_twist_rows<M3C>(g, s, nrow);
+}
+
+template <int M3C>
+__device__ void row_inverse(const GridDev& g, const PlaneSmem& s, int nrow) {
+  const int h3 = (M3C ? M3C : g.m3) + 1;
+  c2r_twist_rows<M3C>(g, s, nrow);
+  axis_fft<true, M3C>(s.slots, g.ax3, s.tw3, 2, nrow, h3, 1);
+}
+
 // Forward: real rows (natural z) in each slot -> DIF z, R2C twist, DIF y.
 template <int N2C, int M3C>
 __device__ void plane_forward(const GridDev& g, const PlaneSmem& s, int nslot) {
   const PlaneShape<N2C, M3C> sh(g);
-  axis_fft<false, M3C>(s.slots, g.ax3, s.tw3, 2, nslot * sh.n2, sh.h3, 1);
-  r2c_twist<N2C, M3C>(g, s, nslot);
+  row_forward<M3C>(g, s, nslot * sh.n2);
   axis_fft<false, N2C>(s.slots, g.ax2, s.tw2, 1, nslot * sh.h3, 1, nslot * sh.h3);
 }
 
@@ -134,8 +144,7 @@ template <int N2C, int M3C>
 __device__ void plane_inverse(const GridDev& g, const PlaneSmem& s, int nslot) {
   const PlaneShape<N2C, M3C> sh(g);
   axis_fft<true, N2C>(s.slots, g.ax2, s.tw2, 1, nslot * sh.h3, 1, nslot * sh.h3);
-  c2r_twist<N2C, M3C>(g, s, nslot);
-  axis_fft<true, M3C>(s.slots, g.ax3, s.tw3, 2, nslot * sh.n2, sh.h3, 1);
+  row_inverse<M3C>(g, s, nslot * sh.n2);
 }
 
 // Real element (y=r, z=j) of field f.
@@ -370,6 +379,34 @@ __device__ __forceinline__ Weights fmt_weights_at(const GridDev& g, const double
   return w;
 }
 
+// Tensor weights B (k_i k_j / k^2 - delta_ij / 3), B = -4 pi R^2 (j2 - j0) sigma_L
+// (functionals.py:457-487), in the order xx, xy, xz, yy, yz, zz, from the scalar
+// weights w0 = j0 sigma_L and w3 = (4 pi R^3 / 3) j2 sigma_L.  All vanish at k = 0.
+// Under k -> -k an off-diagonal weight k_i k_j changes sign once for every
+// one of its two components that is not on its axis' Nyquist plane (the
+// Nyquist frequency maps to itself).  Its Hermitian part (what Grid.ifft's
+// .real keeps) is therefore zero where exactly one of the two is at Nyquist,
+// and the weight itself elsewhere.
+__device__ __forceinline__ void tensor_weights_at(const GridDev& g, int p1, int col, double w0, double w3,
+                                                  double R, double* tw) {
+  const int p2 = col / g.h3, p3 = col - p2 * g.h3;
+  const double kx = g.kp1[p1], ky = g.kp2[p2], kz = g.kp3[p3];
+  const double K = sqrt(kx * kx + ky * ky + kz * kz);
+  if (!(K > 0.0)) {
+    for (int c = 0; c < 6; ++c) tw[c] = 0.0;
+    return;
+  }
+  const double K2 = K * K;
+  const double B = -4 * M_PI * (R * R) * (w3 / (4.0 * M_PI * R * R * R / 3.0) - w0);
+  const int q1 = g.nq1[p1], q2 = g.nq2[p2], q3 = g.nq3[p3];
+  tw[0] = B * ((kx * kx) / K2 - 1.0 / 3);
+  tw[1] = (q1 != q2) ? 0.0 : B * ((kx * ky) / K2);
+  tw[2] = (q1 != q3) ? 0.0 : B * ((kx * kz) / K2);
+  tw[3] = B * ((ky * ky) / K2 - 1.0 / 3);
+  tw[4] = (q2 != q3) ? 0.0 : B * ((ky * kz) / K2);
+  tw[5] = B * ((kz * kz) / K2 - 1.0 / 3);
+}
+
 // WDA weight (WDAVFunctional._init_weight_function, cmmdft/functionals.py:1139-1155):
 // 3 (sin x - x cos x) / x^3 sigma_L at x = |k| D, 1 sigma_L at k = 0.
 __device__ __forceinline__ double wda_weight_at(const GridDev& g, int p1, int col, double D) {
@@ -445,7 +482,7 @@ __global__ void k_fmt_weights(GridDev g, double R, double2* __restrict__ wtab) {
 // Outputs (field stride fsw): 0 = n0 (w0), 1 = n3 (w3), 2..4 = nv2 (x, y, z).
 // The WDA field is a template parameter, as in the plane pass, so that the
 // plain kernels keep their register budget.
-template <int N1C, int TCC, bool WDA>
+template <int N1C, int TCC, bool WDA, bool TEN>
 __device__ __forceinline__ void col_weights_body(GridDev g, const int* __restrict__ active, double R,
                                                  double inv_npts, const double2* __restrict__ rhohat,
                                                  double2* __restrict__ wout, size_t fsw,
@@ -456,7 +493,8 @@ __device__ __forceinline__ void col_weights_body(GridDev g, const int* __restric
   if (active && !active[b]) return;
   const ColShape<N1C, TCC> sh(g, tc);
   const int c0 = tile * sh.tc;
-  const int ns = WDA ? 6 : 5;  // with the WDA weighted density last
+  const int tb = WDA ? 6 : 5;           // first tensor field
+  const int ns = tb + (TEN ? 6 : 0);    // n0, n3, nv2 x/y/z, WDA, then the tensor densities
   ColSmem s = col_smem_setup(g, sh, ns);
   load_col_tile(g, s, sh, ns, 0, rhohat, b, c0, nullptr);
   __syncthreads();
@@ -480,6 +518,11 @@ __device__ __forceinline__ void col_weights_body(GridDev g, const int* __restric
     cel(s, sh, ns, 2, p1, c) = make_double2(F.y * w.v[0], -F.x * w.v[0]);
     cel(s, sh, ns, 3, p1, c) = make_double2(F.y * w.v[1], -F.x * w.v[1]);
     cel(s, sh, ns, 4, p1, c) = make_double2(F.y * w.v[2], -F.x * w.v[2]);
+    if constexpr (TEN) {
+      double tw[6];
+      tensor_weights_at(g, p1, col, w.w0, w.w3, R, tw);
+      for (int q = 0; q < 6; ++q) cel(s, sh, ns, tb + q, p1, c) = cscale(F, tw[q]);
+    }
     cel(s, sh, ns, 0, p1, c) = cscale(F, w.w0);
   }
   __syncthreads();
@@ -497,21 +540,21 @@ __device__ __forceinline__ void col_weights_body(GridDev g, const int* __restric
       double2 *__restrict__ wout, size_t fsw, const double2 *__restrict__ kst,                             \
       const double2 *__restrict__ wtab, double *__restrict__ part, int nslot_part, int want_value, int tc,  \
       double wda_D
-template <int N1C, int TCC>
-__global__ void __launch_bounds__(CMM_COL_THREADS) k_col_weights(COL_WEIGHTS_ARGS) {
-  col_weights_body<N1C, TCC, false>(g, active, R, inv_npts, rhohat, wout, fsw, kst, wtab, part, nslot_part,
-                                    want_value, tc, wda_D);
-}
-template <int N1C, int TCC>
-__global__ void __launch_bounds__(CMM_COL_THREADS) k_col_weights_wda(COL_WEIGHTS_ARGS) {
-  col_weights_body<N1C, TCC, true>(g, active, R, inv_npts, rhohat, wout, fsw, kst, wtab, part, nslot_part,
-                                   want_value, tc, wda_D);
-}
+#define COL_WEIGHTS_KERNEL(name, wda, ten)                                                              \
+  template <int N1C, int TCC>                                                                            \
+  __global__ void __launch_bounds__(CMM_COL_THREADS) name(COL_WEIGHTS_ARGS) {                           \
+    col_weights_body<N1C, TCC, wda, ten>(g, active, R, inv_npts, rhohat, wout, fsw, kst, wtab, part,     \
+                                         nslot_part, want_value, tc, wda_D);                             \
+  }
+COL_WEIGHTS_KERNEL(k_col_weights, false, false)
+COL_WEIGHTS_KERNEL(k_col_weights_wda, true, false)
+COL_WEIGHTS_KERNEL(k_col_weights_t, false, true)
+COL_WEIGHTS_KERNEL(k_col_weights_wda_t, true, true)
 
 // ======================== column pass 2: dPhi spectra -> C1 spectrum ====
 // Inputs: 5 dPhi spectra (field stride fsg): g_s (pairs with w0), g3 (w3),
 // gv (x,y,z, pairs with kwv2); rho_hat for the MFA term.  gin == NULL: MFA only.
-template <int N1C, int TCC, bool WDA>
+template <int N1C, int TCC, bool WDA, bool TEN>
 __device__ __forceinline__ void col_backconv_body(GridDev g, const int* __restrict__ active, double R,
                                                   double scale, const double2* __restrict__ gin, size_t fsg,
                                                   const double2* __restrict__ rhohat,
@@ -522,8 +565,9 @@ __device__ __forceinline__ void col_backconv_body(GridDev g, const int* __restri
   if (active && !active[b]) return;
   const ColShape<N1C, TCC> sh(g, tc);
   const int c0 = blockIdx.x * sh.tc;
-  const int nin = WDA ? 6 : 5;
-  const int ns = nin + 1;    // 5 dPhi (+1 WDA) fields, then rho_hat
+  const int tb = WDA ? 6 : 5;           // first tensor field
+  const int nin = tb + (TEN ? 6 : 0);
+  const int ns = nin + 1;    // 5 dPhi (+1 WDA, +6 tensor) fields, then rho_hat
   const int fr = nin;        // slot of rho_hat
   ColSmem s = col_smem_setup(g, sh, ns);
   const bool hs = (gin != nullptr);
@@ -546,6 +590,11 @@ __device__ __forceinline__ void col_backconv_body(GridDev g, const int* __restri
       double2 gv = make_double2(0.0, 0.0);
       for (int a = 0; a < 3; ++a) gv = cadd(gv, cscale(cel(s, sh, ns, 2 + a, p1, c), w.v[a]));
       acc = cadd(acc, make_double2(-gv.y, gv.x));
+      if constexpr (TEN) {  // + sum_ij fft(dPhi/dn_ij) w_ij (functionals.py:602-605)
+        double tw[6];
+        tensor_weights_at(g, p1, col, w.w0, w.w3, R, tw);
+        for (int q = 0; q < 6; ++q) acc = cadd(acc, cscale(cel(s, sh, ns, tb + q, p1, c), tw[q]));
+      }
       acc = cscale(acc, scale);
       // WDA: ifft(fft(dphi) kw), no 1/beta (the EOS derivative is an energy)
       if (WDA) acc = cadd(acc, cscale(cel(s, sh, ns, 5, p1, c), wda_weight_at(g, p1, col, wda_D) * inv_npts));
@@ -563,14 +612,16 @@ __device__ __forceinline__ void col_backconv_body(GridDev g, const int* __restri
   GridDev g, const int *__restrict__ active, double R, double scale, const double2 *__restrict__ gin,      \
       size_t fsg, const double2 *__restrict__ rhohat, const double2 *__restrict__ kst,                     \
       const double2 *__restrict__ wtab, double2 *__restrict__ chat, int tc, double wda_D, double inv_npts
-template <int N1C, int TCC>
-__global__ void __launch_bounds__(CMM_COL_THREADS) k_col_backconv(COL_BACKCONV_ARGS) {
-  col_backconv_body<N1C, TCC, false>(g, active, R, scale, gin, fsg, rhohat, kst, wtab, chat, tc, wda_D, inv_npts);
-}
-template <int N1C, int TCC>
-__global__ void __launch_bounds__(CMM_COL_THREADS) k_col_backconv_wda(COL_BACKCONV_ARGS) {
-  col_backconv_body<N1C, TCC, true>(g, active, R, scale, gin, fsg, rhohat, kst, wtab, chat, tc, wda_D, inv_npts);
-}
+#define COL_BACKCONV_KERNEL(name, wda, ten)                                                             \
+  template <int N1C, int TCC>                                                                            \
+  __global__ void __launch_bounds__(CMM_COL_THREADS) name(COL_BACKCONV_ARGS) {                          \
+    col_backconv_body<N1C, TCC, wda, ten>(g, active, R, scale, gin, fsg, rhohat, kst, wtab, chat, tc,    \
+                                          wda_D, inv_npts);                                              \
+  }
+COL_BACKCONV_KERNEL(k_col_backconv, false, false)
+COL_BACKCONV_KERNEL(k_col_backconv_wda, true, false)
+COL_BACKCONV_KERNEL(k_col_backconv_t, false, true)
+COL_BACKCONV_KERNEL(k_col_backconv_wda_t, true, true)
 
 // ===================================== plane pass: dPhi/dn (White-Bear) ==
 // Arithmetic of _phi*, _dphi*, get_phi and _get_dphi_* (cmmdft/functionals.py:620-767).
@@ -610,8 +661,11 @@ __device__ __forceinline__ void phi_funcs(double n3, double ln, double n32, doub
   }
 }
 
+// With TEN, T holds the tensor densities (xx, xy, xz, yy, yz, zz) and gT
+// receives dPhi/dn_T (functionals.py:634-639, 669-674, 692-717).
+template <bool TEN>
 __device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, double vy, double vz,
-                                            double R, int version) {
+                                            const double* T, double* gT, double R, int version) {
   const double n1 = R * n0;
   const double n2 = (4.0 * M_PI * R * R) * n0;
   const double i4r = 1.0 / (4 * M_PI * R);
@@ -635,6 +689,16 @@ __device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, 
   } else {
     pref3 = n2 * n2 * n2 - 3.0 * n2 * vv;
   }
+  if constexpr (TEN) {
+    const double xx = T[0], xy = T[1], xz = T[2], yy = T[3], yz = T[4], zz = T[5];
+    const double quad = xx * (vx * vx) + yy * (vy * vy) + zz * (vz * vz) + 2 * xy * vx * vy + 2 * xz * vx * vz +
+                        2 * yz * vy * vz;
+    const double tr3 = (xx * xx * xx + yy * yy * yy + zz * zz * zz) +
+                       3 * (xx * xy * xy + xx * xz * xz + yy * xy * xy + yy * yz * yz + zz * xz * xz + zz * yz * yz) +
+                       6 * xy * xz * yz;
+    pref3 += 4.5 * quad;
+    pref3 -= 4.5 * tr3;
+  }
   const double s12 = n1 * n2 - uv;
   PhiOut o;
   o.phi = n0 * p1 + s12 * p2 + pref3 * p3;
@@ -649,10 +713,26 @@ __device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, 
   o.gs = d0 + R * d1 + (4.0 * M_PI * R * R) * d2;
   o.g3 = d3;
   const double v[3] = {vx, vy, vz}, u[3] = {ux, uy, uz};
+  double tv[3] = {0.0, 0.0, 0.0};  // 2 T v, the gradient of the quadratic form
+  if constexpr (TEN) {
+    tv[0] = 2 * (T[0] * vx + T[1] * vy + T[2] * vz);
+    tv[1] = 2 * (T[1] * vx + T[3] * vy + T[4] * vz);
+    tv[2] = 2 * (T[2] * vx + T[4] * vy + T[5] * vz);
+  }
   for (int a = 0; a < 3; ++a) {
     const double dv1 = -v[a] * p2;
-    const double dv2 = -u[a] * p2 + v[a] * f3;
+    double dv2 = -u[a] * p2 + v[a] * f3;
+    if constexpr (TEN) dv2 += 4.5 * tv[a] * p3;
     o.gv[a] = dv1 * i4r + dv2;
+  }
+  if constexpr (TEN) {
+    const double xx = T[0], xy = T[1], xz = T[2], yy = T[3], yz = T[4], zz = T[5];
+    gT[0] = 4.5 * (vx * vx - 3 * (xx * xx + xy * xy + xz * xz)) * p3;
+    gT[1] = 4.5 * ((vx * vy - 3 * (xx * xy + yy * xy + xz * yz)) * 2) * p3;
+    gT[2] = 4.5 * ((vx * vz - 3 * (xx * xz + zz * xz + xy * yz)) * 2) * p3;
+    gT[3] = 4.5 * (vy * vy - 3 * (yy * yy + xy * xy + yz * yz)) * p3;
+    gT[4] = 4.5 * ((vy * vz - 3 * (yy * yz + zz * yz + xy * xz)) * 2) * p3;
+    gT[5] = 4.5 * (vz * vz - 3 * (zz * zz + xz * xz + yz * yz)) * p3;
   }
   return o;
 }
@@ -684,7 +764,7 @@ __device__ __forceinline__ void plane_fmt_body(GridDev g, const int* __restrict_
     double& ay = rel(s, sh, ns, 3, r, j);
     double& az = rel(s, sh, ns, 4, r, j);
     n3max = fmax(n3max, a3);
-    PhiOut o = fmt_point(a0, a3, ax, ay, az, R, version);
+    PhiOut o = fmt_point<false>(a0, a3, ax, ay, az, nullptr, nullptr, R, version);
     phi += o.phi;
     if (do_c1) {
       a0 = o.gs; a3 = o.g3; ax = o.gv[0]; ay = o.gv[1]; az = o.gv[2];
@@ -731,6 +811,144 @@ k_plane_fmt_wda(GridDev g, const int* __restrict__ active, double R, int version
                 const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
                 double* __restrict__ part, int nslot_part, int want) {
   plane_fmt_body<N2C, M3C, true>(g, active, R, version, wda, win, fsw, gout, fsg, part, nslot_part, want);
+}
+
+// ================================================ staged plane passes ==
+// For planes whose fields do not fit in one SM's shared memory (and for the
+// tensor variants), the plane pass runs as a y pass over HBM followed by a
+// z-row pass with the pointwise step; the y pass of the results follows.
+
+// y transform of one field of one x-plane, a tile of tc stored z frequencies
+// at a time: [n2][tc] in shared memory, pencils along y.  Fields f of the
+// launch are at src/dst + f * fs; blockIdx.z = b * nfield + f.
+template <int N2C>
+__global__ void __launch_bounds__(CMM_COL_THREADS)
+k_ypass(GridDev g, const int* __restrict__ active, const double2* src, double2* dst, size_t fs, int nfield,
+        int tc, int inv) {
+  const int i1 = blockIdx.y;
+  const int b = blockIdx.z / nfield, f = blockIdx.z - b * nfield;
+  if (active && !active[b]) return;
+  const int n2 = N2C ? N2C : g.n2, h3 = g.h3;
+  extern __shared__ double2 smem_d2[];
+  double2* t = smem_d2;       // [n2][tc]
+  double2* tw = t + (size_t)n2 * tc;
+  for (int i = threadIdx.x; i < n2; i += blockDim.x) tw[i] = g.tw2[i];
+  const int c0 = blockIdx.x * tc;
+  const size_t base = (size_t)f * fs + ((size_t)b * g.n1 + i1) * n2 * h3;
+  for (int i = threadIdx.x; i < n2 * tc; i += blockDim.x) {
+    const int r = i / tc, c = i - r * tc;
+    const int col = c0 + c;
+    t[i] = (col < h3) ? src[base + (size_t)r * h3 + col] : make_double2(0.0, 0.0);
+  }
+  __syncthreads();
+  if (inv) axis_fft<true, N2C>(t, g.ax2, tw, 1, tc, 1, tc);
+  else axis_fft<false, N2C>(t, g.ax2, tw, 1, tc, 1, tc);
+  for (int i = threadIdx.x; i < n2 * tc; i += blockDim.x) {
+    const int r = i / tc, c = i - r * tc;
+    const int col = c0 + c;
+    if (col < h3) dst[base + (size_t)r * h3 + col] = t[i];
+  }
+}
+
+__host__ __device__ inline size_t row_smem_bytes(int n3, int nrow) {
+  const int h3 = n3 / 2 + 1, m3 = n3 / 2;
+  size_t b = sizeof(double2) * ((size_t)nrow * h3 + n3) + sizeof(int) * m3;
+  return (b + 15) & ~(size_t)15;
+}
+
+template <int M3C>
+__device__ inline PlaneSmem row_smem_setup(const GridDev& g, int nrow) {
+  extern __shared__ double2 smem_d2[];
+  const int m3 = M3C ? M3C : g.m3, h3 = m3 + 1, n3 = 2 * m3;
+  PlaneSmem s;
+  s.slots = smem_d2;
+  s.tw2 = nullptr;
+  s.tw3 = s.slots + (size_t)nrow * h3;
+  s.zpos = (int*)(s.tw3 + n3);
+  for (int i = threadIdx.x; i < n3; i += blockDim.x) s.tw3[i] = g.tw3[i];
+  for (int i = threadIdx.x; i < m3; i += blockDim.x) s.zpos[i] = g.zpos[i];
+  return s;
+}
+
+// z rows of the dPhi/dn step: one block per x-plane, `chunk` y rows of all
+// fields at a time (rows interleaved by field as in the plane layout).  The
+// input fields (w, y already inverted) are read, the dPhi fields written to
+// gout (z forward; their y forward follows).  Same pointwise arithmetic and
+// reductions as k_plane_fmt.
+template <int M3C, bool WDA, bool TEN>
+__global__ void __launch_bounds__(CMM_ROW_THREADS)
+k_zrow_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
+           const double2* __restrict__ win, size_t fs, double2* __restrict__ gout, int chunk,
+           double* __restrict__ part, int nslot_part, int want) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
+  constexpr int tb = WDA ? 6 : 5;
+  constexpr int nf = tb + (TEN ? 6 : 0);
+  const int m3 = M3C ? M3C : g.m3, h3 = m3 + 1, n3 = 2 * m3, n2 = g.n2;
+  PlaneSmem s = row_smem_setup<M3C>(g, nf * chunk);
+  const size_t poff = ((size_t)b * g.n1 + i1) * n2 * h3;
+  const bool do_c1 = (want & 1) != 0;
+  double phi = 0.0, n3max = -INFINITY, fwda = 0.0;
+  for (int r0 = 0; r0 < n2; r0 += chunk) {
+    const int nr = min(chunk, n2 - r0);
+    for (int f = 0; f < nf; ++f) {
+      const double2* p = win + f * fs + poff + (size_t)r0 * h3;
+      for (int i = threadIdx.x; i < nr * h3; i += blockDim.x) {
+        const int r = i / h3, c = i - r * h3;
+        s.slots[((size_t)r * nf + f) * h3 + c] = __ldg(p + i);
+      }
+    }
+    __syncthreads();
+    row_inverse<M3C>(g, s, nf * nr);
+    for (int i = threadIdx.x; i < nr * n3; i += blockDim.x) {
+      const int r = i / n3, j = i - r * n3;
+      double* row = (double*)(s.slots + (size_t)r * nf * h3) + j;  // field f at row[2 * h3 * f]
+      const int fst = 2 * h3;
+      const double a3 = row[fst];
+      n3max = fmax(n3max, a3);
+      double T[6], gT[6];
+      if constexpr (TEN)
+        for (int q = 0; q < 6; ++q) T[q] = row[fst * (tb + q)];
+      PhiOut o = fmt_point<TEN>(row[0], a3, row[2 * fst], row[3 * fst], row[4 * fst], T, gT, R, version);
+      phi += o.phi;
+      if (do_c1) {
+        row[0] = o.gs; row[fst] = o.g3; row[2 * fst] = o.gv[0]; row[3 * fst] = o.gv[1]; row[4 * fst] = o.gv[2];
+        if constexpr (TEN)
+          for (int q = 0; q < 6; ++q) row[fst * (tb + q)] = gT[q];
+      }
+      if constexpr (WDA) {
+        double fv, dfv;
+        wda_eos(wda, row[5 * fst], fv, dfv);
+        fwda += fv;
+        if (do_c1) row[5 * fst] = dfv;
+      }
+    }
+    __syncthreads();
+    if (do_c1) {
+      row_forward<M3C>(g, s, nf * nr);
+      for (int f = 0; f < nf; ++f) {
+        double2* p = gout + f * fs + poff + (size_t)r0 * h3;
+        for (int i = threadIdx.x; i < nr * h3; i += blockDim.x) {
+          const int r = i / h3, c = i - r * h3;
+          p[i] = s.slots[((size_t)r * nf + f) * h3 + c];
+        }
+      }
+      __syncthreads();
+    }
+  }
+  __shared__ double red[32];
+  if (want & 2) {
+    double t = block_sum(phi, red);
+    put_part(part, b, CMM_STAT_PHI, nslot_part, i1, t);
+    if constexpr (WDA) {
+      t = block_sum(fwda, red);
+      put_part(part, b, CMM_STAT_WDA, nslot_part, i1, t);
+    }
+  }
+  if (want & 4) {
+    double t = block_max(n3max, red);
+    put_part(part, b, CMM_STAT_N3MAX, nslot_part, i1, t);
+  }
 }
 
 // ========================================== plane pass: solver updates ==
@@ -938,7 +1156,7 @@ __global__ void k_stats_finalize(const int* __restrict__ active, const double* _
 static int last_err() { return (cudaPeekAtLastError() == cudaSuccess) ? CMM_OK : CMM_ERR_CUDA; }
 
 static int set_smem(const void* fn, size_t bytes) {
-  if (bytes > 232448) return CMM_ERR_SMEM;
+  if (bytes > 232448) return CMM_ERR_SMEM;  // the B200 per-block opt-in limit
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
     return CMM_ERR_CUDA;
   return CMM_OK;
@@ -1010,6 +1228,78 @@ static int col_tile(const cmm_grid* g, int nslot) {
   return tc;
 }
 
+// ---------------------------------------------------- staged plane path --
+#define CMM_SMEM_MAX 232448
+
+// y pass over nfield fields (in place when src == dst): tiles of at most 16
+// stored z frequencies, spread evenly over the h3 columns.
+static int ypass(const cmm_grid* g, int batch, const int* act, const double2* src, double2* dst, size_t fs,
+                 int nfield, int inv, cudaStream_t st) {
+  const int ntile = cmm_div_up(g->h3, 16);
+  const int tc = cmm_div_up(g->h3, ntile);
+  if ((long long)batch * nfield > 65535 || g->n1 > 65535) return CMM_ERR_SHAPE;
+  const size_t sb = sizeof(double2) * ((size_t)g->n2 * tc + g->n2);
+  const dim3 grd(ntile, g->n1, batch * nfield);
+  int rc;
+  if (g->n2 == 64) {
+    if ((rc = set_smem((const void*)k_ypass<64>, sb))) return rc;
+    k_ypass<64><<<grd, CMM_COL_THREADS, sb, st>>>(g->dev, act, src, dst, fs, nfield, tc, inv);
+  } else if (g->n2 == 32) {
+    if ((rc = set_smem((const void*)k_ypass<32>, sb))) return rc;
+    k_ypass<32><<<grd, CMM_COL_THREADS, sb, st>>>(g->dev, act, src, dst, fs, nfield, tc, inv);
+  } else {
+    if ((rc = set_smem((const void*)k_ypass<0>, sb))) return rc;
+    k_ypass<0><<<grd, CMM_COL_THREADS, sb, st>>>(g->dev, act, src, dst, fs, nfield, tc, inv);
+  }
+  return last_err();
+}
+
+// y rows per z-row chunk so that nf fields fit in the shared-memory budget (0: none fit).
+static int zrow_chunk(const cmm_grid* g, int nf) {
+  const size_t fixed = row_smem_bytes(g->n3, 0) + 16;
+  const size_t per = sizeof(double2) * (size_t)nf * g->h3;
+  if (fixed + per > CMM_SMEM_MAX) return 0;
+  size_t c = (CMM_SMEM_MAX - fixed) / per;
+  return (int)(c > (size_t)g->n2 ? g->n2 : c);
+}
+
+template <int M3C, bool WDA, bool TEN>
+static int zrow_fmt_one(const cmm_grid* g, int batch, const int* act, double R, int version,
+                        const cmm_wda_eos& we, const double2* win, size_t fs, double2* gout, int chunk,
+                        double* part, int nslot, int want, cudaStream_t st) {
+  constexpr int nf = (WDA ? 6 : 5) + (TEN ? 6 : 0);
+  const size_t sb = row_smem_bytes(g->n3, nf * chunk);
+  int rc;
+  if ((rc = set_smem((const void*)k_zrow_fmt<M3C, WDA, TEN>, sb))) return rc;
+  k_zrow_fmt<M3C, WDA, TEN><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(
+      g->dev, act, R, version, we, win, fs, gout, chunk, part, nslot, want);
+  return last_err();
+}
+
+template <int M3C>
+static int zrow_fmt_m3(const cmm_grid* g, int batch, const int* act, double R, int version, const cmm_wda_eos& we,
+                       const double2* win, size_t fs, double2* gout, int chunk, double* part, int nslot, int want,
+                       cudaStream_t st) {
+  const bool wda = (version & CMM_WDA) != 0, ten = (version & CMM_TENSOR) != 0;
+  if (wda && ten)
+    return zrow_fmt_one<M3C, true, true>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+  if (wda)
+    return zrow_fmt_one<M3C, true, false>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+  if (ten)
+    return zrow_fmt_one<M3C, false, true>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+  return zrow_fmt_one<M3C, false, false>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+}
+
+static int zrow_fmt(const cmm_grid* g, int batch, const int* act, double R, int version, const cmm_wda_eos& we,
+                    const double2* win, size_t fs, double2* gout, int nf, double* part, int nslot, int want,
+                    cudaStream_t st) {
+  const int chunk = zrow_chunk(g, nf);
+  if (chunk < 1) return CMM_ERR_SMEM;
+  if (g->m3 == 32) return zrow_fmt_m3<32>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+  if (g->m3 == 16) return zrow_fmt_m3<16>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+  return zrow_fmt_m3<0>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+}
+
 extern "C" int cmm_plane_smem_bytes(const cmm_grid* g, int nslot, size_t* bytes) {
   if (!g || !bytes) return CMM_ERR_ARG;
   *bytes = plane_smem_bytes(g->n2, g->n3, nslot);
@@ -1072,17 +1362,18 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
   if (!g || batch < 1 || !d_kst || !d_rhohat || !d_work || !d_part) return CMM_ERR_ARG;
   if ((want & 1) && !d_chat) return CMM_ERR_ARG;
   const bool has_wda = (version & CMM_WDA) != 0;
+  const bool ten = (version & CMM_TENSOR) != 0;
   if (has_wda && !wda) return CMM_ERR_ARG;
   cmm_wda_eos we;
   memset(&we, 0, sizeof(we));
   if (has_wda) we = *wda;
-  const int nf = has_wda ? 6 : 5;            // weighted densities (and dPhi fields)
+  const int nf = (has_wda ? 6 : 5) + (ten ? 6 : 0);  // weighted densities (and dPhi fields)
   cudaStream_t st = (cudaStream_t)stream;
   const size_t fs = (size_t)batch * g->n1 * g->n2 * g->h3;  // field stride (double2)
-  double2* wbuf = (double2*)d_work;          // weighted-density spectra (up to 6)
-  double2* gbuf = wbuf + 6 * fs;             // dPhi spectra (up to 6)
+  double2* wbuf = (double2*)d_work;               // weighted-density spectra (up to 6, 12 with tensors)
+  double2* gbuf = wbuf + (ten ? 12 : 6) * fs;     // dPhi spectra
   const double npts = (double)g->n1 * g->n2 * g->n3;
-  const int tc = col_tile(g, 7);
+  const int tc = col_tile(g, nf + 1);
   const int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
   if (nslot < g->n1 || nslot < ntile) return CMM_ERR_WORKSPACE;
   const size_t csw = col_smem_bytes(g->n1, tc, nf), csb = col_smem_bytes(g->n1, tc, nf + 1);
@@ -1095,29 +1386,42 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
                wt, (double2*)d_chat, tc, 0.0, 1.0 / npts);
     return last_err();
   }
-  if (has_wda)
-    LAUNCH_COL(ck, k_col_weights_wda, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
-               (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0,
-               tc, we.D);
-  else
-    LAUNCH_COL(ck, k_col_weights, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
-               (const double2*)d_rhohat, wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0,
-               tc, we.D);
+#define LAUNCH_WEIGHTS(kern)                                                                             \
+  LAUNCH_COL(ck, kern, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts, (const double2*)d_rhohat, \
+             wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0, tc, we.D)
+  if (has_wda && ten) LAUNCH_WEIGHTS(k_col_weights_wda_t);
+  else if (has_wda) LAUNCH_WEIGHTS(k_col_weights_wda);
+  else if (ten) LAUNCH_WEIGHTS(k_col_weights_t);
+  else LAUNCH_WEIGHTS(k_col_weights);
+#undef LAUNCH_WEIGHTS
   const size_t ps = plane_smem_bytes(g->n2, g->n3, nf);
-  if (has_wda)
-    LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt_wda, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, d_active,
-                   R, version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
-  else
-    LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, d_active, R,
-                   version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
-  if ((want & 1) && has_wda) {
-    LAUNCH_COL(ck, k_col_backconv_wda, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),
-               (const double2*)gbuf, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt, (double2*)d_chat,
-               tc, we.D, 1.0 / npts);
-  } else if (want & 1) {
-    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),
-               (const double2*)gbuf, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt, (double2*)d_chat,
-               tc, we.D, 1.0 / npts);
+  if (!ten && !g->staging && ps <= CMM_SMEM_MAX) {  // fused plane pass
+    if (has_wda)
+      LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt_wda, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev,
+                     d_active, R, version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
+    else
+      LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, d_active,
+                     R, version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
+  } else {  // staged: y pass, z rows with the pointwise step, y pass of the results
+    int rc = ypass(g, batch, d_active, wbuf, wbuf, fs, nf, 1, st);
+    if (rc) return rc;
+    rc = zrow_fmt(g, batch, d_active, R, version, we, wbuf, fs, gbuf, nf, d_part, nslot, want, st);
+    if (rc) return rc;
+    if (want & 1) {
+      rc = ypass(g, batch, d_active, gbuf, gbuf, fs, nf, 0, st);
+      if (rc) return rc;
+    }
+  }
+  if (want & 1) {
+#define LAUNCH_BACKCONV(kern)                                                                            \
+  LAUNCH_COL(ck, kern, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),               \
+             (const double2*)gbuf, fs, (const double2*)d_rhohat, (const double2*)d_kst, wt, (double2*)d_chat, \
+             tc, we.D, 1.0 / npts)
+    if (has_wda && ten) LAUNCH_BACKCONV(k_col_backconv_wda_t);
+    else if (has_wda) LAUNCH_BACKCONV(k_col_backconv_wda);
+    else if (ten) LAUNCH_BACKCONV(k_col_backconv_t);
+    else LAUNCH_BACKCONV(k_col_backconv);
+#undef LAUNCH_BACKCONV
   }
   return last_err();
 }

@@ -54,6 +54,11 @@ class GridPlan(object):
         self.volume = float(abs(np.linalg.det(self.rvecs)))
         self.dr = self.volume / self.npts
 
+    def set_staging(self, mode):
+        """0: fused plane passes where the plane fits in shared memory (default);
+        1: always the staged y pass + z-row form (cmm_grid_set_staging)."""
+        check(self.lib.cmm_grid_set_staging(self.handle, int(mode)), "cmm_grid_set_staging")
+
     def __del__(self):
         try:
             if getattr(self, "handle", None) is not None:
@@ -119,14 +124,15 @@ class GridPlan(object):
 class Buffers(object):
     """Workspace of one shape group of ``batch`` instances."""
 
-    def __init__(self, plan, batch, nhist=0):
+    def __init__(self, plan, batch, nhist=0, nwork=12):
         self.plan = plan
         self.batch = batch
         n1, n2, n3 = plan.npoints
         dev = "cuda"
         f64 = torch.float64
         fs = plan.nspec * 2
-        self.work = torch.empty((12, batch, fs), dtype=f64, device=dev)
+        # intermediate spectra of the functional pipeline (Functional.nwork)
+        self.work = torch.empty((nwork, batch, fs), dtype=f64, device=dev)
         self.nslot = max(n1, -(-(n2 * plan.h3) // 1))  # >= ntiles for any column tile >= 1
         self.part = torch.zeros((batch, L.NSTAT, self.nslot), dtype=f64, device=dev)
         self.stats = torch.zeros((batch, L.NSTAT), dtype=f64, device=dev)
@@ -158,6 +164,8 @@ class Functional(object):
         if wda is not None:
             self.version |= L.WDA
         # (kw0, kw3) table for this grid and radius, L2-resident during the solve
+        # intermediate spectra of one pipeline launch per instance
+        self.nwork = 24 if (self.version & L.TENSOR) else 12
         self.wtab = None
         if not (self.version & L.NOHS):
             self.wtab = torch.empty(plan.nspec * 2, dtype=torch.float64, device="cuda")

@@ -6,11 +6,11 @@ with krho the Spectrum returned by Grid.fft.  Every evaluation runs on the
 GPU through the C ABI; the solver uses the fused pipeline of all parts at once
 (``FreeEnergy.device()``).
 
-Built: HardSphere (FMT, MFMT, WBII and their antisymmetric 'a' variants),
-MFA (with or without supercell tail corrections), ExtPot (spherical LJ
-guests) and the WDA correlation part of add_correlation_wda_lj.  Not built
-in this package: the tensor 't' FMT variants, the LDA part and non-spherical
-guests; asking for them raises NotImplementedError.
+Built: HardSphere (FMT, MFMT, WBII with the antisymmetric 'a' and tensor
+'t' options, 'atWBII' being the default), MFA (with or without supercell
+tail corrections), ExtPot (spherical LJ guests) and the WDA correlation part
+of add_correlation_wda_lj.  Not built in this package: the LDA part and
+non-spherical guests; asking for them raises NotImplementedError.
 """
 import os
 from pathlib import Path
@@ -210,7 +210,7 @@ class HardSphereFunctional(Functional):
     def _run(self, krho, want):
         krho = self.grid.as_spectrum(krho)
         fn = self._functional()
-        buf = E.Buffers(fn.plan, 1)
+        buf = E.Buffers(fn.plan, 1, nwork=fn.nwork)
         buf.part[:, L.STAT_N3MAX, :] = -np.inf
         chat = fn.plan.new_spec(1) if want & 1 else None
         fn.c1(buf, krho.data, chat, want=want)

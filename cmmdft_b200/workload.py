@@ -14,8 +14,12 @@ from . import engine as E
 from .eos import ModifiedBenedictWebbRubinEOS
 from .units import angstrom, kjmol, boltzmann, planck
 
-HS_VERSIONS = {'FMT': L.FMT, 'MFMT': L.MFMT, 'WBII': L.WBII,
-               'aFMT': L.FMT | L.ANTISYM, 'aMFMT': L.MFMT | L.ANTISYM, 'aWBII': L.WBII | L.ANTISYM}
+# version strings of cmmdft/functionals.py:375-377: base with 'a' and/or 't'
+HS_VERSIONS = {}
+for _base, _code in (('FMT', L.FMT), ('MFMT', L.MFMT), ('WBII', L.WBII)):
+    for _pre, _bits in (('', 0), ('a', L.ANTISYM), ('t', L.TENSOR), ('at', L.ANTISYM | L.TENSOR),
+                        ('ta', L.ANTISYM | L.TENSOR)):
+        HS_VERSIONS[_pre + _base] = _code | _bits
 
 
 def hardsphere_radius(sigma, epsilon, temperature):
@@ -33,7 +37,7 @@ def thermal_wavelength(mass, temperature):
 
 def hs_version_code(version):
     if version not in HS_VERSIONS:
-        raise NotImplementedError("hard-sphere version %r (tensor variants are not built)" % version)
+        raise ValueError("Unknown hard sphere functional version: %r" % version)
     return HS_VERSIONS[version]
 
 

@@ -60,10 +60,12 @@ enum {
 };
 #define CMM_MAX_HIST 8
 
-/* Hard-sphere functional versions (cmmdft/functionals.py:373-377).
+/* Hard-sphere functional versions (cmmdft/functionals.py:373-377): a base
+ * (FMT, MFMT, WBII) with the 'a' (CMM_ANTISYM) and 't' (CMM_TENSOR, the six
+ * tensor weighted densities of functionals.py:457-487, 534-552) options.
  * CMM_NOHS drops the hard-sphere term (the MFA convolution alone);
  * CMM_WDA adds the WDA correlation part described by a cmm_wda_eos. */
-enum { CMM_FMT = 0, CMM_MFMT = 1, CMM_WBII = 2, CMM_ANTISYM = 8, CMM_NOHS = 16, CMM_WDA = 32 };
+enum { CMM_FMT = 0, CMM_MFMT = 1, CMM_WBII = 2, CMM_ANTISYM = 8, CMM_NOHS = 16, CMM_WDA = 32, CMM_TENSOR = 64 };
 
 /* WDA correlation part (WDAVFunctional with SumOfEOS([MBWR, CS, MFA],
  * factors), cmmdft/functionals.py:339-362, 1116-1184; cmmdft/eos.py).
@@ -97,6 +99,12 @@ const char* cmm_status_string(int status);
  * device tables (the only persistent device memory this library owns). */
 int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_grid** out);
 int cmm_grid_destroy(cmm_grid* grid);
+/* Plane passes: a grid whose y-z plane of all fields fits in one SM's
+ * shared memory runs the fused plane kernels (y and z transforms and the
+ * pointwise step in one pass); larger planes, and the tensor variants, run
+ * the staged form (a y pass over HBM, then z rows with the pointwise step).
+ * mode 0 chooses by size (default), 1 always stages (tests, tuning). */
+int cmm_grid_set_staging(cmm_grid* grid, int mode);
 /* Number of stored frequencies per instance (N1*N2*H3) and H3. */
 int cmm_grid_spectrum_size(const cmm_grid* grid, long long* nspec, int* h3);
 /* Frequency indices (0..N-1 per axis) at each stored position:
@@ -157,8 +165,10 @@ int cmm_mfa_kernel(const cmm_grid* grid, double sigma, double epsilon, double cu
  * cmm_fmt_weights for this grid and R, or NULL.  want: bit 0 = C1 spectrum,
  * bit 1 = free-energy sums (PHI, MFA), bit 2 = n3 maximum.
  * wda: WDA part (with version | CMM_WDA), else NULL; it adds one weighted
- * density and one back-convolution field.
- * d_work: 12 spectra of batch instances.  d_part: [batch][CMM_NSTAT][nslot]. */
+ * density and one back-convolution field.  CMM_TENSOR adds the six tensor
+ * weighted densities and their back-convolution.
+ * d_work: 12 spectra of batch instances (24 with CMM_TENSOR).
+ * d_part: [batch][CMM_NSTAT][nslot]. */
 int cmm_fmt_c1(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,
                int version, const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab,
                const double* d_rhohat, double* d_chat, double* d_work, double* d_part, int nslot,
@@ -229,7 +239,8 @@ int cmm_stats_finalize(int batch, const int* d_active, const double* d_part, int
  * any stream capture).  All calls share the array and it keeps the last
  * call's contents: calls that overlap on the GPU race.  Outputs as
  * cmm_fmt_c1; d_stats [batch][CMM_NSTAT] receives the PHI / MFA / N3MAX
- * sums requested by `want` (may be NULL when want == 1). */
+ * sums requested by `want` (may be NULL when want == 1).  The tensor
+ * versions (CMM_TENSOR) need twice the scratch and return CMM_ERR_UNSUPPORTED. */
 #define CMM_NOALLOC_SCRATCH_BYTES (32u << 20)
 size_t cmm_fmt_c1_noalloc_capacity(const cmm_grid* grid);
 int cmm_fmt_c1_noalloc(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,

@@ -25,9 +25,9 @@ from cmmdft_b200.units import angstrom, kjmol, boltzmann, planck
 
 FFT_WORKERS = 1
 
-FMT_NAMES = ['FMT', 'aFMT']
-MFMT_NAMES = ['MFMT', 'aMFMT']
-WBII_NAMES = ['WBII', 'aWBII']
+FMT_NAMES = ['FMT', 'aFMT', 'tFMT', 'atFMT', 'taFMT']        # functionals.py:375-377
+MFMT_NAMES = ['MFMT', 'aMFMT', 'tMFMT', 'atMFMT', 'taMFMT']
+WBII_NAMES = ['WBII', 'aWBII', 'tWBII', 'atWBII', 'taWBII']
 
 
 # ---------------------------------------------------------------- grid ----
@@ -180,6 +180,17 @@ class HardSphere(object):
         kwv1 = kwv2 / (4 * np.pi * R)
         self.sw = [kw0, kw1, kw2, kw3]
         self.vw = [kwv1, kwv2]
+        self.tw = None
+        if 't' in self.version:  # tensor weights, functionals.py:457-487
+            KX, KY, KZ, K = (g.kpoints[..., i] for i in range(4))
+            K2 = K ** 2
+            with np.errstate(invalid='ignore', divide='ignore'):
+                H = [np.where(K > 0, (KX * KX) / K2, 1 / 3), np.where(K > 0, (KX * KY) / K2, 0.0),
+                     np.where(K > 0, (KX * KZ) / K2, 0.0), np.where(K > 0, (KY * KY) / K2, 1 / 3),
+                     np.where(K > 0, (KY * KZ) / K2, 0.0), np.where(K > 0, (KZ * KZ) / K2, 1 / 3)]
+            B = -4 * np.pi * R ** 2 * (j2 - kw0)
+            delta = [1 / 3, 0.0, 0.0, 1 / 3, 0.0, 1 / 3]
+            self.tw = [B * (h - d) for h, d in zip(H, delta)]
 
     def densities(self, krho):  # functionals.py:489-532
         g = self.grid
@@ -197,6 +208,13 @@ class HardSphere(object):
         n32 = n3 * n3
         return n0, n1, n2, n3, ln, n32, n32 * n3, nv1, nv2, xi
 
+    def tensor_densities(self, krho):  # functionals.py:534-548
+        xx, xy, xz, yy, yz, zz = (self.grid.ifft(krho * w) for w in self.tw)
+        tr2 = xx ** 2 + yy ** 2 + zz ** 2 + 2 * (xy ** 2 + xz ** 2 + yz ** 2)
+        tr3 = (xx ** 3 + yy ** 3 + zz ** 3 + 3 * (xx * xy * xy + xx * xz * xz + yy * xy * xy + yy * yz * yz
+                                                  + zz * xz * xz + zz * yz * yz) + 6 * xy * xz * yz)
+        return [xx, xy, xz, yy, yz, zz, tr2, tr3]
+
     def get_n3(self, krho):  # functionals.py:554-556 (unclipped)
         return self.grid.ifft(krho * self.sw[3])
 
@@ -205,21 +223,27 @@ class HardSphere(object):
             return
         self.krho = krho
         self.wd = self.densities(krho)
+        self.nt = self.tensor_densities(krho) if 't' in self.version else None
 
     def derive(self, krho):  # functionals.py:574-609
         self.set_density(krho)
         g, v, wd = self.grid, self.version, self.wd
+        nt = self.nt
         tot = 0.0
         for f, w in zip([dphi_n0, dphi_n1, dphi_n2, dphi_n3], self.sw):
-            tot += g.fft(f(*wd, version=v)) * w
+            tot += g.fft(f(*wd, nt=nt, version=v)) * w
         for f, w in zip([dphi_nv1, dphi_nv2], self.vw):
-            kd = g.fftn(f(*wd, version=v))
+            kd = g.fftn(f(*wd, nt=nt, version=v))
             tot += -(kd[..., 0] * w[..., 0] + kd[..., 1] * w[..., 1] + kd[..., 2] * w[..., 2])
+        if 't' in v:
+            kd = g.fftn(dphi_nt(*wd, nt=nt, version=v))
+            for c in range(6):
+                tot += kd[..., c] * self.tw[c]
         return g.ifft(tot) / self.beta
 
     def value(self, krho):  # functionals.py:611-618
         self.set_density(krho)
-        return self.grid.integrate(phi_total(*self.wd, version=self.version)) / self.beta
+        return self.grid.integrate(phi_total(*self.wd, nt=self.nt, version=self.version)) / self.beta
 
 
 def _phi1(n3, ln):  # functionals.py:720-721
@@ -271,28 +295,36 @@ def _dot3(a, b):
     return a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1] + a[..., 2] * b[..., 2]
 
 
-def _pref3(n2, nv2, xi, v):  # functionals.py:629-632 / 664-667
+def _pref3(n2, nv2, xi, v, nt=None):  # functionals.py:629-639 / 664-673
     if 'a' in v:
-        return (n2 ** 3) * ((1 - xi) ** 3)
-    return n2 ** 3 - 3.0 * n2 * _dot3(nv2, nv2)
+        p = (n2 ** 3) * ((1 - xi) ** 3)
+    else:
+        p = n2 ** 3 - 3.0 * n2 * _dot3(nv2, nv2)
+    if 't' in v:
+        xx, xy, xz, yy, yz, zz, tr2, tr3 = nt
+        vx, vy, vz = nv2[..., 0], nv2[..., 1], nv2[..., 2]
+        p += (9 / 2) * (xx * vx ** 2 + yy * vy ** 2 + zz * vz ** 2
+                        + 2 * xy * vx * vy + 2 * xz * vx * vz + 2 * yz * vy * vz)
+        p -= (9 / 2) * tr3
+    return p
 
 
-def phi_total(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, version):  # :620-641
+def phi_total(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, nt=None, version=None):  # :620-641
     phi = n0 * _phi1(n3, ln)
     phi += (n1 * n2 - _dot3(nv1, nv2)) * _phi2(n3, ln, n32, version)
-    phi += _pref3(n2, nv2, xi, version) * _phi3(n3, ln, n32, n33, version)
+    phi += _pref3(n2, nv2, xi, version, nt) * _phi3(n3, ln, n32, n33, version)
     return phi
 
 
-def dphi_n0(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, version):  # :643-644
+def dphi_n0(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, nt=None, version=None):  # :643-644
     return _phi1(n3, ln)
 
 
-def dphi_n1(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, version):  # :646-647
+def dphi_n1(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, nt=None, version=None):  # :646-647
     return n2 * _phi2(n3, ln, n32, version)
 
 
-def dphi_n2(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, version):  # :649-656
+def dphi_n2(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, nt=None, version=None):  # :649-656
     d = n1 * _phi2(n3, ln, n32, version)
     if 'a' in version:
         d += (3 * (n2 ** 2) * (1 + xi) * ((1 - xi) ** 2)) * _phi3(n3, ln, n32, n33, version)
@@ -301,25 +333,45 @@ def dphi_n2(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, version):  # :649-656
     return d
 
 
-def dphi_n3(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, version):  # :658-676
+def dphi_n3(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, nt=None, version=None):  # :658-676
     d = n0 * _dphi1(n3)
     d += (n1 * n2 - _dot3(nv2, nv1)) * _dphi2(n3, ln, n32, version)
-    d += _pref3(n2, nv2, xi, version) * _dphi3(n3, ln, n32, n33, version)
+    d += _pref3(n2, nv2, xi, version, nt) * _dphi3(n3, ln, n32, n33, version)
     return d
 
 
-def dphi_nv1(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, version):  # :678-680
+def dphi_nv1(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, nt=None, version=None):  # :678-680
     return -nv2 * _phi2(n3, ln, n32, version)[..., None]
 
 
-def dphi_nv2(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, version):  # :682-701
+def dphi_nv2(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, nt=None, version=None):  # :682-701
     d = -nv1 * _phi2(n3, ln, n32, version)[..., None]
     p3 = _phi3(n3, ln, n32, n33, version)
     if 'a' in version:
         d += nv2 * (-6 * n2 * ((1 - xi) ** 2) * p3)[..., None]
     else:
         d += nv2 * (-6 * n2 * p3)[..., None]
+    if 't' in version:
+        xx, xy, xz, yy, yz, zz, tr2, tr3 = nt
+        vx, vy, vz = nv2[..., 0], nv2[..., 1], nv2[..., 2]
+        gn = np.empty_like(nv2)
+        gn[..., 0] = 2 * (xx * vx + xy * vy + xz * vz)
+        gn[..., 1] = 2 * (xy * vx + yy * vy + yz * vz)
+        gn[..., 2] = 2 * (xz * vx + yz * vy + zz * vz)
+        d += (9 / 2) * gn * p3[..., None]
     return d
+
+
+def dphi_nt(n0, n1, n2, n3, ln, n32, n33, nv1, nv2, xi, nt=None, version=None):  # :703-717
+    xx, xy, xz, yy, yz, zz, tr2, tr3 = nt
+    vx, vy, vz = nv2[..., 0], nv2[..., 1], nv2[..., 2]
+    g = np.stack([vx * vx - 3 * (xx * xx + xy * xy + xz * xz),
+                  (vx * vy - 3 * (xx * xy + yy * xy + xz * yz)) * 2,
+                  (vx * vz - 3 * (xx * xz + zz * xz + xy * yz)) * 2,
+                  vy * vy - 3 * (yy * yy + xy * xy + yz * yz),
+                  (vy * vz - 3 * (yy * yz + zz * yz + xy * xz)) * 2,
+                  vz * vz - 3 * (zz * zz + xz * xz + yz * yz)], axis=-1)
+    return (9 / 2) * g * _phi3(n3, ln, n32, n33, version)[..., None]
 
 
 # ----------------------------------------------------------------- MFA ----

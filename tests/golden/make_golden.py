@@ -190,6 +190,16 @@ def main():
         out['wda_omega_' + tag] = om
         out['wda_dWDA_' + tag] = derivs[3]
         out['wda_C1_' + tag] = C1
+    # tensor FMT variants (functionals.py:457-487, 534-552, 620-717): the
+    # hard-sphere part alone, as HardSphereFunctional(grid, R, version)
+    functionals = ref[1]
+    for ver, tags in (('atWBII', 'ab'), ('tWBII', 'ab'), ('atFMT', 'b'), ('tMFMT', 'b')):
+        hs = functionals.HardSphereFunctional(grid, b['guest'].Rhs, version=ver)
+        hs.set_temperature(T, b['guest'].Rhs)
+        for tag in tags:
+            k = grid.fft(rho_a if tag == 'a' else rho_b)
+            out['hs_%s_d_%s' % (ver, tag)] = quiet(hs.derive, k)
+            out['hs_%s_v_%s' % (ver, tag)] = quiet(hs.value, k)
     np.savez_compressed(os.path.join(HERE, 'c0_32.npz'), **out)
     print('wrote c0_32.npz', 'picard steps', out['picard_steps'], 'anderson steps', out['and_steps'])
 

@@ -61,7 +61,7 @@ def test_external_potential(golden32, fn32):
 
 def _c1(fn, rho_np):
     plan = fn.plan
-    buf = E.Buffers(plan, 1)
+    buf = E.Buffers(plan, 1, nwork=fn.nwork)
     buf.part[:, L.STAT_N3MAX, :] = -np.inf
     rho = torch.as_tensor(rho_np[None], device="cuda")
     spec = plan.rfft_yz(rho)
@@ -89,6 +89,71 @@ def test_functional_derivative(golden32, fn32, tag):
     assert scalar_rel(Fhs, vals[0]) < 1e-11
     assert scalar_rel(Fmfa, vals[1]) < 1e-11
     assert scalar_rel(st[L.STAT_N3MAX], golden32["n3_" + tag].max()) < 1e-12
+
+
+def _hs_only(plan, ver, R, T=300.0):
+    """Device functional of the hard-sphere part alone (no MFA kernel, V = 0)."""
+    from cmmdft_b200.units import boltzmann
+    return E.Functional(plan, R, 1.0 / (boltzmann * T), 1.0, torch.zeros(plan.npoints, dtype=torch.float64,
+                                                                          device="cuda"), W.hs_version_code(ver))
+
+
+TENSOR_CASES = [("atWBII", "a"), ("atWBII", "b"), ("tWBII", "a"), ("tWBII", "b"), ("atFMT", "b"), ("tMFMT", "b")]
+
+
+@pytest.mark.parametrize("staged", [0, 1])
+@pytest.mark.parametrize("ver,tag", TENSOR_CASES)
+def test_tensor_hard_sphere(golden32, cuda, ver, tag, staged):
+    """Tensor FMT variants against the reference's HardSphereFunctional."""
+    plan = E.GridPlan((32, 32, 32), cubic_host_276(0).rvecs)
+    plan.set_staging(staged)
+    fn = _hs_only(plan, ver, float(golden32["Rhs"]))
+    C1, st, Fhs, _ = _c1(fn, golden32["rho_" + tag])
+    floor = {"a": 2e-9, "b": 1e-7}[tag]   # the WBII noise floor of the plain case
+    assert fn.beta * np.max(np.abs(C1 - golden32["hs_%s_d_%s" % (ver, tag)])) < floor
+    assert scalar_rel(Fhs, golden32["hs_%s_v_%s" % (ver, tag)]) < 1e-11
+
+
+@pytest.mark.parametrize("ver", ["WBII", "aWBII", "atWBII"])
+def test_tensor_64_against_oracle(cuda, ver):
+    """The 64^3 kernels (compile-time transform lengths) against the oracle."""
+    from oracle import cmm_oracle as O
+    host = cubic_host_276(0)
+    sig, eps, mass = methane_guest_params()
+    fn = W.build_functional(host, (64, 64, 64), 300.0, (sig, eps, mass))
+    R = fn.R
+    V = fn.V.cpu().numpy()
+    rho = 0.02 / angstrom ** 3 * np.clip(np.exp(-fn.beta * V), 0, 1)   # dense, sharp profile
+    hs = _hs_only(fn.plan, ver, R)
+    C1, st, Fhs, _ = _c1(hs, rho)
+    og = O.OGrid(host.rvecs, npoints=64)
+    ohs = O.HardSphere(og, R, 300.0, version=ver)
+    k = og.fft(rho)
+    ref = ohs.derive(k)
+    dC = hs.beta * np.abs(C1 - ref)
+    assert dC.max() < 1e-7
+    assert (dC * rho).max() / rho.max() < 1e-9
+    assert scalar_rel(Fhs, ohs.value(k)) < 1e-11
+
+
+@pytest.mark.parametrize("wda", [False, True])
+@pytest.mark.parametrize("n", [32, 64])
+def test_staged_plane_pass_matches_fused(golden32, cuda, n, wda):
+    """The staged form (y pass + z rows) against the fused plane kernel."""
+    host = cubic_host_276(0)
+    fn = W.build_functional(host, (n, n, n), 300.0, methane_guest_params(), wda=wda)
+    V = fn.V.cpu().numpy()
+    rho = 0.02 / angstrom ** 3 * np.clip(np.exp(-fn.beta * V), 0, 1)
+    fn.plan.set_staging(0)
+    C1a, sta, Fa, Ma = _c1(fn, rho)
+    fn.plan.set_staging(1)
+    C1b, stb, Fb, Mb = _c1(fn, rho)
+    fn.plan.set_staging(0)
+    assert np.max(np.abs(C1a - C1b)) <= 1e-12 * np.max(np.abs(C1a))
+    assert scalar_rel(Fb, Fa) < 1e-12 and scalar_rel(Mb, Ma) < 1e-12
+    assert scalar_rel(stb[L.STAT_N3MAX], sta[L.STAT_N3MAX]) < 1e-14
+    if wda:
+        assert scalar_rel(stb[L.STAT_WDA], sta[L.STAT_WDA]) < 1e-12
 
 
 @pytest.mark.parametrize("tag", ["a", "b"])

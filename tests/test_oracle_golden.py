@@ -135,3 +135,18 @@ def test_wda_part(golden32, tag):
     k = grid.fft(rho)
     assert fe.beta * np.max(np.abs(w.derive(k) - golden32["wda_dWDA_" + tag])) < 1e-12
     assert scalar_rel(w.value(k), golden32["wda_values_" + tag][3]) < 1e-12
+
+
+TENSOR_CASES = [("atWBII", "a"), ("atWBII", "b"), ("tWBII", "a"), ("tWBII", "b"), ("atFMT", "b"), ("tMFMT", "b")]
+
+
+@pytest.mark.parametrize("ver,tag", TENSOR_CASES)
+def test_tensor_hard_sphere(golden32, case32, ver, tag):
+    """Tensor FMT variants (functionals.py:457-487, 534-552, 620-717)."""
+    grid, fe = case32
+    hs = O.HardSphere(grid, float(golden32["Rhs"]), 300.0, version=ver)
+    k = grid.fft(golden32["rho_" + tag])
+    # the beta-scaled noise floor of the WBII closed forms (see the plain case)
+    floor = {"a": 2e-9, "b": 1e-7}[tag]
+    assert hs.beta * np.max(np.abs(hs.derive(k) - golden32["hs_%s_d_%s" % (ver, tag)])) < floor
+    assert scalar_rel(hs.value(k), golden32["hs_%s_v_%s" % (ver, tag)]) < 1e-12
