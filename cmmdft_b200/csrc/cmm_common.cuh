@@ -22,11 +22,12 @@
 // k-space stages never permute data.
 struct GridDev {
   int n1, n2, n3, h3, m3;      // h3 = n3/2+1 stored z frequencies, m3 = n3/2
-  FftAxis ax1, ax2, ax3;       // ax3 is the half-length complex z transform (length m3)
+  int zfull;                   // odd N3: ax3 is the full-length z transform, stored z in natural order
+  FftAxis ax1, ax2, ax3;       // ax3: the half-length complex z transform (length m3) for even N3
   const double2* tw1;          // w_{n1}^t, t < n1
   const double2* tw2;          // w_{n2}^t
   const double2* tw3;          // w_{n3}^t (the z transform and the R2C twist)
-  const int* zpos;             // z position of frequency k < m3
+  const int* zpos;             // z DIF position of frequency k (k < m3; k < n3 when zfull)
   const int* k1pos;            // x frequency at DIF position p (column passes)
   const double* kp1;           // signed k component (bohr^-1) at x position
   const double* kp2;

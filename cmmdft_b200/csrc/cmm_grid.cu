@@ -34,10 +34,11 @@ static bool factorise(int n, FftAxis* ax) {
   while (m % 8 == 0) { r.push_back(8); m /= 8; }
   while (m % 4 == 0) { r.push_back(4); m /= 4; }
   while (m % 2 == 0) { r.push_back(2); m /= 2; }
-  for (int p = 3; p <= 13 && m > 1; p += 2)
+  for (int p = 3; m > 1; p += 2)   // odd primes in increasing order; primes > 16 run as direct-DFT stages
     while (m % p == 0) { r.push_back(p); m /= p; }
-  if (m != 1) return false;  // prime factor > 13 (needs Bluestein; not in this build)
   if ((int)r.size() > CMM_MAX_STAGES) return false;
+  ax->big = 0;
+  for (int x : r) if (x > CMM_MAX_SMALL_RADIX) ax->big = 1;
   if (r.empty()) r.push_back(1);
   int L = n;
   for (size_t s = 0; s < r.size(); ++s) {
@@ -91,7 +92,9 @@ static double np_sinc(double x) {
 extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_grid** out) {
   if (!out || !rvecs || n1 < 1 || n2 < 1 || n3 < 2) return CMM_ERR_ARG;
   if (n1 > CMM_MAX_N || n2 > CMM_MAX_N || n3 > CMM_MAX_N) return CMM_ERR_SHAPE;
-  if (n3 % 2) return CMM_ERR_SHAPE;  // the z axis is transformed as a half-length complex FFT
+  // Even N3: the z axis is a half-length complex FFT plus the R2C/C2R twist.
+  // Odd N3: a full-length complex FFT of the real rows (z rows kernels only).
+  const int zfull = n3 % 2;
   cmm_grid* g = (cmm_grid*)calloc(1, sizeof(cmm_grid));
   if (!g) return CMM_ERR_NOMEM;
   g->n1 = n1; g->n2 = n2; g->n3 = n3; g->m3 = n3 / 2; g->h3 = n3 / 2 + 1;
@@ -107,7 +110,7 @@ extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_
                  r[2] * (r[3] * r[7] - r[4] * r[6]);
     g->volume = fabs(det);
   }
-  if (!factorise(n1, &g->ax1) || !factorise(n2, &g->ax2) || !factorise(g->m3, &g->ax3)) {
+  if (!factorise(n1, &g->ax1) || !factorise(n2, &g->ax2) || !factorise(zfull ? n3 : g->m3, &g->ax3)) {
     free(g);
     return CMM_ERR_SHAPE;
   }
@@ -115,12 +118,21 @@ extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_
   g->hpos_k1 = (int*)malloc(sizeof(int) * n1);
   g->hpos_k2 = (int*)malloc(sizeof(int) * n2);
   g->hpos_k3 = (int*)malloc(sizeof(int) * h3);
-  std::vector<int> zdif(m3), zpos(m3);
+  // zpos: position of frequency k in the z transform's DIF output (k < m3
+  // for even N3; k < N3 for odd N3, whose h3 stored frequencies are kept in
+  // natural order: position p holds k = p).
+  const int nz = zfull ? n3 : m3;
+  std::vector<int> zdif(nz), zpos(nz);
   dif_positions(g->ax1, g->hpos_k1);
   dif_positions(g->ax2, g->hpos_k2);
   dif_positions(g->ax3, zdif.data());
-  for (int p = 0; p < m3; ++p) { g->hpos_k3[p] = zdif[p]; zpos[zdif[p]] = p; }
-  g->hpos_k3[m3] = m3;
+  for (int p = 0; p < nz; ++p) zpos[zdif[p]] = p;
+  if (zfull) {
+    for (int p = 0; p < h3; ++p) g->hpos_k3[p] = p;
+  } else {
+    for (int p = 0; p < m3; ++p) g->hpos_k3[p] = zdif[p];
+    g->hpos_k3[m3] = m3;
+  }
 
   std::vector<double> tw1, tw2, tw3;
   twiddles(n1, tw1); twiddles(n2, tw2); twiddles(n3, tw3);
@@ -148,14 +160,14 @@ extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_
   }
   for (int p = 0; p < h3; ++p) {
     int k = g->hpos_k3[p];
-    wt3[p] = (k == 0 || k == m3) ? 1.0 : 2.0;
+    wt3[p] = (k == 0 || (!zfull && k == m3)) ? 1.0 : 2.0;  // Parseval weight of a stored frequency
   }
 
   // one device block for everything
   size_t off = 0;
   auto bump = [&](size_t bytes) { size_t o = off; off += (bytes + 255) & ~(size_t)255; return o; };
   size_t o_tw1 = bump(sizeof(double) * tw1.size()), o_tw2 = bump(sizeof(double) * tw2.size()),
-         o_tw3 = bump(sizeof(double) * tw3.size()), o_zpos = bump(sizeof(int) * m3),
+         o_tw3 = bump(sizeof(double) * tw3.size()), o_zpos = bump(sizeof(int) * nz),
          o_k1 = bump(sizeof(int) * n1);
   size_t o_kp[3], o_sl[3], o_nq[3];
   for (int a = 0; a < 3; ++a) {
@@ -168,7 +180,7 @@ extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_
   memcpy(&host[o_tw1], tw1.data(), sizeof(double) * tw1.size());
   memcpy(&host[o_tw2], tw2.data(), sizeof(double) * tw2.size());
   memcpy(&host[o_tw3], tw3.data(), sizeof(double) * tw3.size());
-  memcpy(&host[o_zpos], zpos.data(), sizeof(int) * m3);
+  memcpy(&host[o_zpos], zpos.data(), sizeof(int) * nz);
   memcpy(&host[o_k1], g->hpos_k1, sizeof(int) * n1);
   for (int a = 0; a < 3; ++a) {
     memcpy(&host[o_kp[a]], kp[a].data(), sizeof(double) * npos[a]);
@@ -188,6 +200,7 @@ extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_
   char* b = (char*)g->dmem;
   GridDev& d = g->dev;
   d.n1 = n1; d.n2 = n2; d.n3 = n3; d.h3 = h3; d.m3 = m3;
+  d.zfull = zfull;
   d.ax1 = g->ax1; d.ax2 = g->ax2; d.ax3 = g->ax3;
   d.tw1 = (const double2*)(b + o_tw1);
   d.tw2 = (const double2*)(b + o_tw2);

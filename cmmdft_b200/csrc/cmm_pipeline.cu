@@ -26,6 +26,7 @@ struct PlaneSmem {
   double2* tw2;     // n2
   double2* tw3;     // n3
   int* zpos;        // m3
+  double2* tmp;     // z rows only: direct-DFT stage scratch (z transforms with a prime factor > 16)
 };
 
 __host__ __device__ inline size_t plane_smem_bytes(int n2, int n3, int nslot) {
@@ -49,6 +50,7 @@ __device__ inline PlaneSmem plane_smem_setup(const GridDev& g, int nslot) {
   extern __shared__ double2 smem_d2[];
   const PlaneShape<N2C, M3C> sh(g);
   PlaneSmem s;
+  s.tmp = nullptr;
   s.slots = smem_d2;
   s.tw2 = s.slots + (size_t)nslot * sh.n2 * sh.h3;
   s.tw3 = s.tw2 + sh.n2;
@@ -61,9 +63,9 @@ __device__ inline PlaneSmem plane_smem_setup(const GridDev& g, int nslot) {
 
 template <bool INV, int NC>
 __device__ __forceinline__ void axis_fft(double2* base, const FftAxis& ax, const double2* tw, int twmul,
-                                         int npencil, int pstride, int estride) {
+                                         int npencil, int pstride, int estride, double2* tmp = nullptr) {
   if constexpr (NC > 0) fft_ct<INV, NC>(base, tw, twmul, npencil, pstride, estride);
-  else fft_rt<INV>(base, ax, tw, twmul, npencil, pstride, estride);
+  else fft_rt<INV>(base, ax, tw, twmul, npencil, pstride, estride, tmp);
 }
 
 // R2C twist on `nrow` rows: pairs (k, m3-k), k = 0..m3/2, rows fastest.
@@ -255,10 +257,11 @@ k_plane_c2r(GridDev g, const double2* __restrict__ in, double* __restrict__ out)
 struct ColSmem {
   double2* slots;
   double2* tw1;
+  double2* tmp;   // direct-DFT stage scratch (x axes with a prime factor > 16)
 };
 
-__host__ __device__ inline size_t col_smem_bytes(int n1, int tc, int nslot) {
-  return sizeof(double2) * ((size_t)nslot * n1 * tc + n1);
+__host__ __device__ inline size_t col_smem_bytes(int n1, int tc, int nslot, int big) {
+  return sizeof(double2) * ((size_t)nslot * n1 * tc * (big ? 2 : 1) + n1);
 }
 
 template <int N1C, int TCC>
@@ -273,6 +276,7 @@ __device__ inline ColSmem col_smem_setup(const GridDev& g, const ColShape<N1C, T
   ColSmem s;
   s.slots = smem_d2;
   s.tw1 = s.slots + (size_t)nslot * sh.n1 * sh.tc;
+  s.tmp = g.ax1.big ? s.tw1 + sh.n1 : nullptr;
   for (int i = threadIdx.x; i < sh.n1; i += blockDim.x) s.tw1[i] = g.tw1[i];
   return s;
 }
@@ -314,7 +318,7 @@ __device__ inline void store_col_tile(const GridDev& g, const ColSmem& s, const 
 template <bool INV, int N1C, int TCC>
 __device__ inline void col_fft(const GridDev& g, const ColSmem& s, const ColShape<N1C, TCC>& sh, int nslot, int f0,
                                int nfield) {
-  axis_fft<INV, N1C>(s.slots + (size_t)f0 * sh.tc, g.ax1, s.tw1, 1, nfield * sh.tc, 1, nslot * sh.tc);
+  axis_fft<INV, N1C>(s.slots + (size_t)f0 * sh.tc, g.ax1, s.tw1, 1, nfield * sh.tc, 1, nslot * sh.tc, s.tmp);
 }
 
 // Plain x transform of a tile (setup / tests).  HBM spectra keep x natural:
@@ -832,6 +836,7 @@ k_ypass(GridDev g, const int* __restrict__ active, const double2* src, double2* 
   extern __shared__ double2 smem_d2[];
   double2* t = smem_d2;       // [n2][tc]
   double2* tw = t + (size_t)n2 * tc;
+  double2* tmp = g.ax2.big ? tw + n2 : nullptr;   // direct-DFT stage scratch [n2 * tc]
   for (int i = threadIdx.x; i < n2; i += blockDim.x) tw[i] = g.tw2[i];
   const int c0 = blockIdx.x * tc;
   const size_t base = (size_t)f * fs + ((size_t)b * g.n1 + i1) * n2 * h3;
@@ -841,8 +846,8 @@ k_ypass(GridDev g, const int* __restrict__ active, const double2* src, double2* 
     t[i] = (col < h3) ? src[base + (size_t)r * h3 + col] : make_double2(0.0, 0.0);
   }
   __syncthreads();
-  if (inv) axis_fft<true, N2C>(t, g.ax2, tw, 1, tc, 1, tc);
-  else axis_fft<false, N2C>(t, g.ax2, tw, 1, tc, 1, tc);
+  if (inv) axis_fft<true, N2C>(t, g.ax2, tw, 1, tc, 1, tc, tmp);
+  else axis_fft<false, N2C>(t, g.ax2, tw, 1, tc, 1, tc, tmp);
   for (int i = threadIdx.x; i < n2 * tc; i += blockDim.x) {
     const int r = i / tc, c = i - r * tc;
     const int col = c0 + c;
@@ -850,24 +855,111 @@ k_ypass(GridDev g, const int* __restrict__ active, const double2* src, double2* 
   }
 }
 
-__host__ __device__ inline size_t row_smem_bytes(int n3, int nrow) {
-  const int h3 = n3 / 2 + 1, m3 = n3 / 2;
-  size_t b = sizeof(double2) * ((size_t)nrow * h3 + n3) + sizeof(int) * m3;
+
+// z rows in shared memory: nrow rows of rs slots (rs = h3, or n3 for odd N3)
+// | z twiddles (n3) | direct-DFT scratch (nrow * z length, when needed) | z
+// position table.
+__host__ __device__ inline size_t zrow_smem_bytes(int rs, int n3, int zlen, int nz, int big, int nrow) {
+  size_t b = sizeof(double2) * ((size_t)nrow * rs + n3 + (big ? (size_t)nrow * zlen : 0)) + sizeof(int) * nz;
   return (b + 15) & ~(size_t)15;
 }
 
+static inline size_t zrow_smem_bytes_g(const cmm_grid* g, int nrow) {
+  const int full = g->dev.zfull;
+  return zrow_smem_bytes(full ? g->n3 : g->h3, g->n3, g->ax3.n, full ? g->n3 : g->m3, g->ax3.big, nrow);
+}
+
 template <int M3C>
-__device__ inline PlaneSmem row_smem_setup(const GridDev& g, int nrow) {
+__device__ inline PlaneSmem zrow_smem_setup(const GridDev& g, int nrow) {
   extern __shared__ double2 smem_d2[];
-  const int m3 = M3C ? M3C : g.m3, h3 = m3 + 1, n3 = 2 * m3;
+  const bool full = (M3C == 0) && g.zfull;
+  const int m3 = M3C ? M3C : g.m3;
+  const int rs = full ? g.n3 : m3 + 1, n3 = full ? g.n3 : 2 * m3, nz = full ? g.n3 : m3;
   PlaneSmem s;
   s.slots = smem_d2;
   s.tw2 = nullptr;
-  s.tw3 = s.slots + (size_t)nrow * h3;
-  s.zpos = (int*)(s.tw3 + n3);
+  s.tw3 = s.slots + (size_t)nrow * rs;
+  s.tmp = g.ax3.big ? s.tw3 + n3 : nullptr;
+  s.zpos = (int*)(g.ax3.big ? s.tmp + (size_t)nrow * g.ax3.n : s.tw3 + n3);
   for (int i = threadIdx.x; i < n3; i += blockDim.x) s.tw3[i] = g.tw3[i];
-  for (int i = threadIdx.x; i < m3; i += blockDim.x) s.zpos[i] = g.zpos[i];
+  for (int i = threadIdx.x; i < nz; i += blockDim.x) s.zpos[i] = g.zpos[i];
+  __syncthreads();  // zrow_load (odd N3) reads zpos right away
   return s;
+}
+
+// Load nr stored-spectrum rows of field f (src: nr * h3 elements) into slot
+// rows r * nf + f.  Odd N3: frequency k goes to its DIF position and its
+// Hermitian partner n3 - k gets the conjugate; the k = 0 bin keeps its real
+// part (Grid.ifft's .real of a self-conjugate bin).
+template <int M3C>
+__device__ inline void zrow_load(const GridDev& g, const PlaneSmem& s, int nf, int f, int nr,
+                                 const double2* __restrict__ src) {
+  const bool full = (M3C == 0) && g.zfull;
+  const int h3 = M3C ? M3C + 1 : g.h3;
+  const int rs = full ? g.n3 : h3;
+  for (int i = threadIdx.x; i < nr * h3; i += blockDim.x) {
+    const int r = i / h3, c = i - r * h3;
+    const double2 X = __ldg(src + i);
+    double2* row = s.slots + ((size_t)r * nf + f) * rs;
+    if (!full) {
+      row[c] = X;
+    } else if (c == 0) {
+      row[s.zpos[0]] = make_double2(X.x, 0.0);
+    } else {
+      row[s.zpos[c]] = X;
+      row[s.zpos[g.n3 - c]] = cconj(X);
+    }
+  }
+}
+
+template <int M3C>
+__device__ inline void zrow_store(const GridDev& g, const PlaneSmem& s, int nf, int f, int nr,
+                                  double2* __restrict__ dst) {
+  const bool full = (M3C == 0) && g.zfull;
+  const int h3 = M3C ? M3C + 1 : g.h3;
+  const int rs = full ? g.n3 : h3;
+  for (int i = threadIdx.x; i < nr * h3; i += blockDim.x) {
+    const int r = i / h3, c = i - r * h3;
+    const double2* row = s.slots + ((size_t)r * nf + f) * rs;
+    dst[i] = full ? row[s.zpos[c]] : row[c];
+  }
+}
+
+// Real element j of slot row r * nf + f (after zrow_inverse).
+template <int M3C>
+__device__ __forceinline__ double& zrow_rel(const GridDev& g, const PlaneSmem& s, int nf, int f, int r, int j) {
+  if constexpr (M3C == 0) {
+    if (g.zfull) return s.slots[((size_t)r * nf + f) * g.n3 + j].x;
+  }
+  return ((double*)(s.slots + ((size_t)r * nf + f) * (M3C ? M3C + 1 : g.h3)))[j];
+}
+
+template <int M3C>
+__device__ void zrow_inverse(const GridDev& g, const PlaneSmem& s, int nrow) {
+  if constexpr (M3C == 0) {
+    if (g.zfull) {
+      axis_fft<true, 0>(s.slots, g.ax3, s.tw3, 1, nrow, g.n3, 1, s.tmp);
+      return;
+    }
+  }
+  const int h3 = (M3C ? M3C : g.m3) + 1;
+  c2r_twist_rows<M3C>(g, s, nrow);
+  axis_fft<true, M3C>(s.slots, g.ax3, s.tw3, 2, nrow, h3, 1, s.tmp);
+}
+
+template <int M3C>
+__device__ void zrow_forward(const GridDev& g, const PlaneSmem& s, int nrow) {
+  if constexpr (M3C == 0) {
+    if (g.zfull) {
+      for (int i = threadIdx.x; i < nrow * g.n3; i += blockDim.x) s.slots[i].y = 0.0;
+      __syncthreads();
+      axis_fft<false, 0>(s.slots, g.ax3, s.tw3, 1, nrow, g.n3, 1, s.tmp);
+      return;
+    }
+  }
+  const int h3 = (M3C ? M3C : g.m3) + 1;
+  axis_fft<false, M3C>(s.slots, g.ax3, s.tw3, 2, nrow, h3, 1, s.tmp);
+  r2c_twist_rows<M3C>(g, s, nrow);
 }
 
 // z rows of the dPhi/dn step: one block per x-plane, `chunk` y rows of all
@@ -884,57 +976,48 @@ k_zrow_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm
   if (active && !active[b]) return;
   constexpr int tb = WDA ? 6 : 5;
   constexpr int nf = tb + (TEN ? 6 : 0);
-  const int m3 = M3C ? M3C : g.m3, h3 = m3 + 1, n3 = 2 * m3, n2 = g.n2;
-  PlaneSmem s = row_smem_setup<M3C>(g, nf * chunk);
+  const int h3 = M3C ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
+  PlaneSmem s = zrow_smem_setup<M3C>(g, nf * chunk);
   const size_t poff = ((size_t)b * g.n1 + i1) * n2 * h3;
   const bool do_c1 = (want & 1) != 0;
   double phi = 0.0, n3max = -INFINITY, fwda = 0.0;
   for (int r0 = 0; r0 < n2; r0 += chunk) {
     const int nr = min(chunk, n2 - r0);
-    for (int f = 0; f < nf; ++f) {
-      const double2* p = win + f * fs + poff + (size_t)r0 * h3;
-      for (int i = threadIdx.x; i < nr * h3; i += blockDim.x) {
-        const int r = i / h3, c = i - r * h3;
-        s.slots[((size_t)r * nf + f) * h3 + c] = __ldg(p + i);
-      }
-    }
+    for (int f = 0; f < nf; ++f) zrow_load<M3C>(g, s, nf, f, nr, win + f * fs + poff + (size_t)r0 * h3);
     __syncthreads();
-    row_inverse<M3C>(g, s, nf * nr);
+    zrow_inverse<M3C>(g, s, nf * nr);
     for (int i = threadIdx.x; i < nr * n3; i += blockDim.x) {
       const int r = i / n3, j = i - r * n3;
-      double* row = (double*)(s.slots + (size_t)r * nf * h3) + j;  // field f at row[2 * h3 * f]
-      const int fst = 2 * h3;
-      const double a3 = row[fst];
+      double& a0 = zrow_rel<M3C>(g, s, nf, 0, r, j);
+      double& a3 = zrow_rel<M3C>(g, s, nf, 1, r, j);
+      double& ax = zrow_rel<M3C>(g, s, nf, 2, r, j);
+      double& ay = zrow_rel<M3C>(g, s, nf, 3, r, j);
+      double& az = zrow_rel<M3C>(g, s, nf, 4, r, j);
       n3max = fmax(n3max, a3);
       double T[6], gT[6];
       if constexpr (TEN)
-        for (int q = 0; q < 6; ++q) T[q] = row[fst * (tb + q)];
-      PhiOut o = fmt_point<TEN>(row[0], a3, row[2 * fst], row[3 * fst], row[4 * fst], T, gT, R, version);
+        for (int q = 0; q < 6; ++q) T[q] = zrow_rel<M3C>(g, s, nf, tb + q, r, j);
+      PhiOut o = fmt_point<TEN>(a0, a3, ax, ay, az, T, gT, R, version);
       phi += o.phi;
       if (do_c1) {
-        row[0] = o.gs; row[fst] = o.g3; row[2 * fst] = o.gv[0]; row[3 * fst] = o.gv[1]; row[4 * fst] = o.gv[2];
+        a0 = o.gs; a3 = o.g3; ax = o.gv[0]; ay = o.gv[1]; az = o.gv[2];
         if constexpr (TEN)
-          for (int q = 0; q < 6; ++q) row[fst * (tb + q)] = gT[q];
+          for (int q = 0; q < 6; ++q) zrow_rel<M3C>(g, s, nf, tb + q, r, j) = gT[q];
       }
       if constexpr (WDA) {
+        double& aw = zrow_rel<M3C>(g, s, nf, 5, r, j);
         double fv, dfv;
-        wda_eos(wda, row[5 * fst], fv, dfv);
+        wda_eos(wda, aw, fv, dfv);
         fwda += fv;
-        if (do_c1) row[5 * fst] = dfv;
+        if (do_c1) aw = dfv;
       }
     }
     __syncthreads();
     if (do_c1) {
-      row_forward<M3C>(g, s, nf * nr);
-      for (int f = 0; f < nf; ++f) {
-        double2* p = gout + f * fs + poff + (size_t)r0 * h3;
-        for (int i = threadIdx.x; i < nr * h3; i += blockDim.x) {
-          const int r = i / h3, c = i - r * h3;
-          p[i] = s.slots[((size_t)r * nf + f) * h3 + c];
-        }
-      }
-      __syncthreads();
+      zrow_forward<M3C>(g, s, nf * nr);
+      for (int f = 0; f < nf; ++f) zrow_store<M3C>(g, s, nf, f, nr, gout + f * fs + poff + (size_t)r0 * h3);
     }
+    __syncthreads();
   }
   __shared__ double red[32];
   if (want & 2) {
@@ -1135,6 +1218,183 @@ k_plane_mix(GridDev g, const int* __restrict__ active, const double* __restrict_
   store_spec_planes<N2C, M3C>(g, s, 1, rhohat_out, ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3, 0);
 }
 
+// ===================================== staged single-field plane passes ==
+// The solver updates and the plain transforms as z-row passes (after / before
+// a y pass over HBM): one block per x-plane, `chunk` y rows at a time.  An op
+// supplies the pointwise step (point) and the reductions (finish); kIn loads
+// and inverts a spectrum, kOut forwards and stores the rows.  The arithmetic
+// per point is that of the fused plane kernels above.
+template <int M3C, class Op>
+__global__ void __launch_bounds__(CMM_ROW_THREADS)
+k_zrow_op(GridDev g, const int* __restrict__ active, Op op, const double2* __restrict__ spec_in,
+          double2* __restrict__ spec_out, int chunk, double* __restrict__ part, int nslot_part) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
+  const int h3 = M3C ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
+  PlaneSmem s = zrow_smem_setup<M3C>(g, chunk);
+  const size_t poff = ((size_t)b * g.n1 + i1) * n2 * h3;
+  const size_t plane = (size_t)i1 * n2 * n3;
+  const size_t inst = (size_t)b * g.n1 * n2 * n3;
+  typename Op::Acc acc;
+  op.init(acc, b);
+  for (int r0 = 0; r0 < n2; r0 += chunk) {
+    const int nr = min(chunk, n2 - r0);
+    if constexpr (Op::kIn) {
+      zrow_load<M3C>(g, s, 1, 0, nr, spec_in + poff + (size_t)r0 * h3);
+      __syncthreads();
+      zrow_inverse<M3C>(g, s, nr);
+    }
+    for (int i = threadIdx.x; i < nr * n3; i += blockDim.x) {
+      const int r = i / n3, j = i - r * n3;
+      const size_t pi = plane + (size_t)(r0 + r) * n3 + j;   // index within the instance
+      op.point(acc, b, inst + pi, pi, zrow_rel<M3C>(g, s, 1, 0, r, j));
+    }
+    __syncthreads();
+    if constexpr (Op::kOut) {
+      zrow_forward<M3C>(g, s, nr);
+      zrow_store<M3C>(g, s, 1, 0, nr, spec_out + poff + (size_t)r0 * h3);
+    }
+    __syncthreads();
+  }
+  op.finish(acc, part, b, nslot_part, i1);
+}
+
+struct OpR2C {   // real rows -> spectrum (cmm_rfft_yz)
+  static constexpr bool kIn = false, kOut = true;
+  const double* in;
+  struct Acc {};
+  __device__ void init(Acc&, int) const {}
+  __device__ void point(Acc&, int, size_t gi, size_t, double& cell) const { cell = __ldg(in + gi); }
+  __device__ void finish(Acc&, double*, int, int, int) const {}
+};
+
+struct OpC2R {   // spectrum -> real rows (cmm_irfft_yz)
+  static constexpr bool kIn = true, kOut = false;
+  double* out;
+  struct Acc {};
+  __device__ void init(Acc&, int) const {}
+  __device__ void point(Acc&, int, size_t gi, size_t, double& cell) const { out[gi] = cell; }
+  __device__ void finish(Acc&, double*, int, int, int) const {}
+};
+
+struct OpPicard {   // k_plane_picard
+  static constexpr bool kIn = true, kOut = true;
+  const double* params;
+  double beta, lambda3, thr, a_tol, r_tol;
+  const double* rho;
+  const double* V;
+  long long vstride;
+  double* rho_out;
+  struct Acc { double fug, a, mu; PlaneStats st; double res2, gnf, der; };
+  __device__ void init(Acc& c, int b) const {
+    c.fug = params[b * 4 + 0]; c.a = params[b * 4 + 1]; c.mu = params[b * 4 + 2];
+    c.st = {0, 0, 0, 0, 0}; c.res2 = c.gnf = c.der = 0.0;
+  }
+  __device__ void point(Acc& c, int b, size_t gi, size_t pi, double& cell) const {
+    const double v = __ldg(V + b * vstride + pi);
+    const double C1 = cell + v;
+    const double G = beta * exp(-beta * C1) * c.fug;
+    const double x = __ldg(rho + gi);
+    c.res2 += (G - x) * (G - x);
+    c.gnf += cmm_isfinite(G) ? 0.0 : 1.0;
+    c.der += der_term(x, C1, c.mu, beta, lambda3, a_tol, r_tol);
+    double xn = (1.0 - c.a) * x + c.a * G;
+    if (xn < thr) xn = 0.0;
+    rho_out[gi] = xn;
+    stats_point(c.st, xn, x, v, lambda3);
+    cell = xn;
+  }
+  __device__ void finish(Acc& c, double* part, int b, int nslot, int slot) const {
+    __shared__ double red2[32];
+    double t = block_sum(c.res2, red2);
+    put_part(part, b, CMM_STAT_RES2, nslot, slot, t);
+    t = block_sum(c.gnf, red2);
+    put_part(part, b, CMM_STAT_GNONFIN, nslot, slot, t);
+    t = block_sum(c.der, red2);
+    put_part(part, b, CMM_STAT_DER, nslot, slot, t);
+    stats_store(c.st, part, b, nslot, slot);
+  }
+};
+
+struct OpResidual {   // k_plane_residual
+  static constexpr bool kIn = true, kOut = false;
+  const double* params;
+  double beta, lambda3, a_tol, r_tol;
+  const double* rho;
+  const double* V;
+  long long vstride;
+  double* r_out;
+  HistPtrs hist;
+  int nhist;
+  long long hstride;
+  struct Acc { double fug, mu, res2, gnf, der, gram[CMM_MAX_HIST]; };
+  __device__ void init(Acc& c, int b) const {
+    c.fug = params[b * 4 + 0]; c.mu = params[b * 4 + 2];
+    c.res2 = c.gnf = c.der = 0.0;
+#pragma unroll
+    for (int h = 0; h < CMM_MAX_HIST; ++h) c.gram[h] = 0.0;
+  }
+  __device__ void point(Acc& c, int b, size_t gi, size_t pi, double& cell) const {
+    const double C1 = cell + __ldg(V + b * vstride + pi);
+    const double G = beta * exp(-beta * C1) * c.fug;
+    const double x = __ldg(rho + gi);
+    const double rr = G - x;
+    c.res2 += rr * rr;
+    c.gnf += cmm_isfinite(G) ? 0.0 : 1.0;
+    c.der += der_term(x, C1, c.mu, beta, lambda3, a_tol, r_tol);
+    r_out[gi] = rr;
+#pragma unroll
+    for (int h = 0; h < CMM_MAX_HIST; ++h)
+      if (h < nhist) c.gram[h] += rr * __ldg(hist.p[h] + b * hstride + pi);
+  }
+  __device__ void finish(Acc& c, double* part, int b, int nslot, int slot) const {
+    __shared__ double red[32];
+    double t = block_sum(c.res2, red);
+    put_part(part, b, CMM_STAT_RES2, nslot, slot, t);
+    t = block_sum(c.gnf, red);
+    put_part(part, b, CMM_STAT_GNONFIN, nslot, slot, t);
+    t = block_sum(c.der, red);
+    put_part(part, b, CMM_STAT_DER, nslot, slot, t);
+    for (int h = 0; h < nhist; ++h) {
+      t = block_sum(c.gram[h], red);
+      put_part(part, b, CMM_STAT_GRAM0 + h, nslot, slot, t);
+    }
+  }
+};
+
+struct OpMix {   // k_plane_mix
+  static constexpr bool kIn = false, kOut = true;
+  const double* coef;
+  FieldPtrs fields;
+  int nfield, clip;
+  double thr, lambda3;
+  const double* ref;
+  long long refstride;
+  const double* V;
+  long long vstride;
+  double* rho_out;
+  struct Acc { double c[CMM_MAX_FIELDS]; PlaneStats st; };
+  __device__ void init(Acc& a, int b) const {
+#pragma unroll
+    for (int j = 0; j < CMM_MAX_FIELDS; ++j) a.c[j] = (j < nfield) ? coef[b * CMM_MAX_FIELDS + j] : 0.0;
+    a.st = {0, 0, 0, 0, 0};
+  }
+  __device__ void point(Acc& a, int b, size_t gi, size_t pi, double& cell) const {
+    double x = 0.0;
+#pragma unroll
+    for (int f = 0; f < CMM_MAX_FIELDS; ++f)
+      if (f < nfield && a.c[f] != 0.0) x += a.c[f] * __ldg(fields.p[f] + b * fields.stride[f] + pi);
+    if (clip == CMM_CLIP_DENSITY) x = (x < 1e-12) ? 1e-30 : x;
+    else if (clip == CMM_CLIP_PICARD && x < thr) x = 0.0;
+    rho_out[gi] = x;
+    stats_point(a.st, x, __ldg(ref + b * refstride + pi), __ldg(V + b * vstride + pi), lambda3);
+    cell = x;
+  }
+  __device__ void finish(Acc& a, double* part, int b, int nslot, int slot) const {
+    stats_store(a.st, part, b, nslot, slot);
+  }
+};
+
 // ============================================================ finalize ==
 __global__ void k_stats_finalize(const int* __restrict__ active, const double* __restrict__ part,
                                  int nslot, unsigned mask, double* __restrict__ stats) {
@@ -1224,7 +1484,7 @@ static int col_kind(const cmm_grid* g) {
 static int col_tile(const cmm_grid* g, int nslot) {
   if (col_kind(g)) return 8;
   int tc = 16;
-  while (tc > 1 && col_smem_bytes(g->n1, tc, nslot) > 200 * 1024) tc /= 2;
+  while (tc > 1 && col_smem_bytes(g->n1, tc, nslot, g->ax1.big) > 200 * 1024) tc /= 2;
   return tc;
 }
 
@@ -1238,7 +1498,7 @@ static int ypass(const cmm_grid* g, int batch, const int* act, const double2* sr
   const int ntile = cmm_div_up(g->h3, 16);
   const int tc = cmm_div_up(g->h3, ntile);
   if ((long long)batch * nfield > 65535 || g->n1 > 65535) return CMM_ERR_SHAPE;
-  const size_t sb = sizeof(double2) * ((size_t)g->n2 * tc + g->n2);
+  const size_t sb = sizeof(double2) * ((size_t)g->n2 * tc * (g->ax2.big ? 2 : 1) + g->n2);
   const dim3 grd(ntile, g->n1, batch * nfield);
   int rc;
   if (g->n2 == 64) {
@@ -1254,13 +1514,52 @@ static int ypass(const cmm_grid* g, int batch, const int* act, const double2* sr
   return last_err();
 }
 
+// Staged plane passes when the plane of nf fields does not fit in shared
+// memory, the y or z transform has a prime factor > 16 (direct-DFT stages
+// need scratch), N3 is odd (full-length z transform) or staging is forced.
+static bool plane_staged(const cmm_grid* g, int nf) {
+  return g->staging || g->dev.zfull || g->ax2.big || g->ax3.big ||
+         plane_smem_bytes(g->n2, g->n3, nf) > CMM_SMEM_MAX;
+}
+
+// Compile-time z half length of the z-row kernels (0: from the plan).
+static int zrow_m3(const cmm_grid* g) {
+  if (g->dev.zfull) return 0;
+  if (g->m3 == 32) return 32;
+  if (g->m3 == 16) return 16;
+  return 0;
+}
+
 // y rows per z-row chunk so that nf fields fit in the shared-memory budget (0: none fit).
 static int zrow_chunk(const cmm_grid* g, int nf) {
-  const size_t fixed = row_smem_bytes(g->n3, 0) + 16;
-  const size_t per = sizeof(double2) * (size_t)nf * g->h3;
+  const size_t fixed = zrow_smem_bytes_g(g, 0) + 16;
+  const size_t per = zrow_smem_bytes_g(g, nf) - zrow_smem_bytes_g(g, 0) + 16;
   if (fixed + per > CMM_SMEM_MAX) return 0;
   size_t c = (CMM_SMEM_MAX - fixed) / per;
   return (int)(c > (size_t)g->n2 ? g->n2 : c);
+}
+
+template <int M3C, class Op>
+static int zrow_op_m3(const cmm_grid* g, int batch, const int* act, const Op& op, const double2* in,
+                      double2* out, int chunk, double* part, int nslot, cudaStream_t st) {
+  const size_t sb = zrow_smem_bytes_g(g, chunk);
+  int rc;
+  if ((rc = set_smem((const void*)k_zrow_op<M3C, Op>, sb))) return rc;
+  k_zrow_op<M3C, Op><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(g->dev, act, op, in, out, chunk, part, nslot);
+  return last_err();
+}
+
+// One single-field z-row pass (in: y-inverted spectrum rows; out: z-forward rows).
+template <class Op>
+static int zrow_op(const cmm_grid* g, int batch, const int* act, const Op& op, const double2* in, double2* out,
+                   double* part, int nslot, cudaStream_t st) {
+  const int chunk = zrow_chunk(g, 1);
+  if (chunk < 1) return CMM_ERR_SMEM;
+  switch (zrow_m3(g)) {
+    case 32: return zrow_op_m3<32>(g, batch, act, op, in, out, chunk, part, nslot, st);
+    case 16: return zrow_op_m3<16>(g, batch, act, op, in, out, chunk, part, nslot, st);
+    default: return zrow_op_m3<0>(g, batch, act, op, in, out, chunk, part, nslot, st);
+  }
 }
 
 template <int M3C, bool WDA, bool TEN>
@@ -1268,7 +1567,7 @@ static int zrow_fmt_one(const cmm_grid* g, int batch, const int* act, double R, 
                         const cmm_wda_eos& we, const double2* win, size_t fs, double2* gout, int chunk,
                         double* part, int nslot, int want, cudaStream_t st) {
   constexpr int nf = (WDA ? 6 : 5) + (TEN ? 6 : 0);
-  const size_t sb = row_smem_bytes(g->n3, nf * chunk);
+  const size_t sb = zrow_smem_bytes_g(g, nf * chunk);
   int rc;
   if ((rc = set_smem((const void*)k_zrow_fmt<M3C, WDA, TEN>, sb))) return rc;
   k_zrow_fmt<M3C, WDA, TEN><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(
@@ -1295,9 +1594,11 @@ static int zrow_fmt(const cmm_grid* g, int batch, const int* act, double R, int 
                     cudaStream_t st) {
   const int chunk = zrow_chunk(g, nf);
   if (chunk < 1) return CMM_ERR_SMEM;
-  if (g->m3 == 32) return zrow_fmt_m3<32>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
-  if (g->m3 == 16) return zrow_fmt_m3<16>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
-  return zrow_fmt_m3<0>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+  switch (zrow_m3(g)) {
+    case 32: return zrow_fmt_m3<32>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+    case 16: return zrow_fmt_m3<16>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+    default: return zrow_fmt_m3<0>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+  }
 }
 
 extern "C" int cmm_plane_smem_bytes(const cmm_grid* g, int nslot, size_t* bytes) {
@@ -1308,17 +1609,46 @@ extern "C" int cmm_plane_smem_bytes(const cmm_grid* g, int nslot, size_t* bytes)
 
 static int col_fft_3d(const cmm_grid* g, int batch, const double2* in, double2* out, int inv, cudaStream_t st) {
   const int tc = col_tile(g, 1);
-  const size_t cs = col_smem_bytes(g->n1, tc, 1);
+  const size_t cs = col_smem_bytes(g->n1, tc, 1, g->ax1.big);
   const int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
   LAUNCH_COL(col_kind(g), k_col_fft, dim3(ntile, batch), cs, st, g->dev, in, out, tc, inv);
   return last_err();
 }
 
+// Real fields -> yz-spectra (y and z forward) of every plane.
+static int plane_r2c(const cmm_grid* g, int batch, const double* in, double2* spec, cudaStream_t st) {
+  if (plane_staged(g, 1)) {
+    int rc = zrow_op(g, batch, nullptr, OpR2C{in}, nullptr, spec, nullptr, 0, st);
+    if (rc) return rc;
+    return ypass(g, batch, nullptr, spec, spec, 0, 1, 0, st);
+  }
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  LAUNCH_PLANE(plane_kind(g), k_plane_r2c, dim3(g->n1, batch), ps, st, g->dev, in, spec);
+  return last_err();
+}
+
+// yz-spectra -> real fields; the staged form inverts y in place (spec is consumed).
+static int plane_c2r_consume(const cmm_grid* g, int batch, double2* spec, double* out, cudaStream_t st) {
+  if (plane_staged(g, 1)) {
+    int rc = ypass(g, batch, nullptr, spec, spec, 0, 1, 1, st);
+    if (rc) return rc;
+    return zrow_op(g, batch, nullptr, OpC2R{out}, spec, nullptr, nullptr, 0, st);
+  }
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
+  LAUNCH_PLANE(plane_kind(g), k_plane_c2r, dim3(g->n1, batch), ps, st, g->dev, (const double2*)spec, out);
+  return last_err();
+}
+
+// Stream-ordered scratch of `bytes` for the staged passes whose input is read-only.
+static int scratch_alloc(void** p, size_t bytes, cudaStream_t st) {
+  return (cudaMallocAsync(p, bytes, st) == cudaSuccess) ? CMM_OK : CMM_ERR_NOMEM;
+}
+
 extern "C" int cmm_rfft3d(const cmm_grid* g, int batch, const double* d_in, double* d_spec, void* stream) {
   if (!g || !d_in || !d_spec || batch < 1) return CMM_ERR_ARG;
   cudaStream_t st = (cudaStream_t)stream;
-  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  LAUNCH_PLANE(plane_kind(g), k_plane_r2c, dim3(g->n1, batch), ps, st, g->dev, d_in, (double2*)d_spec);
+  int rc = plane_r2c(g, batch, d_in, (double2*)d_spec, st);
+  if (rc) return rc;
   return col_fft_3d(g, batch, (const double2*)d_spec, (double2*)d_spec, 0, st);
 }
 
@@ -1327,24 +1657,29 @@ extern "C" int cmm_irfft3d(const cmm_grid* g, int batch, double* d_spec, double*
   cudaStream_t st = (cudaStream_t)stream;
   int rc = col_fft_3d(g, batch, (const double2*)d_spec, (double2*)d_spec, 1, st);  // in place (consumed)
   if (rc) return rc;
-  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  LAUNCH_PLANE(plane_kind(g), k_plane_c2r, dim3(g->n1, batch), ps, st, g->dev, (const double2*)d_spec, d_out);
-  return last_err();
+  return plane_c2r_consume(g, batch, (double2*)d_spec, d_out, st);
 }
 
 extern "C" int cmm_rfft_yz(const cmm_grid* g, int batch, const double* d_in, double* d_spec, void* stream) {
   if (!g || !d_in || !d_spec || batch < 1) return CMM_ERR_ARG;
-  const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  LAUNCH_PLANE(plane_kind(g), k_plane_r2c, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_in,
-               (double2*)d_spec);
-  return last_err();
+  return plane_r2c(g, batch, d_in, (double2*)d_spec, (cudaStream_t)stream);
 }
 
 extern "C" int cmm_irfft_yz(const cmm_grid* g, int batch, const double* d_spec, double* d_out, void* stream) {
   if (!g || !d_spec || !d_out || batch < 1) return CMM_ERR_ARG;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plane_staged(g, 1)) {
+    void* tmp = nullptr;
+    const size_t bytes = sizeof(double2) * (size_t)batch * g->n1 * g->n2 * g->h3;
+    int rc = scratch_alloc(&tmp, bytes, st);
+    if (rc) return rc;
+    rc = ypass(g, batch, nullptr, (const double2*)d_spec, (double2*)tmp, 0, 1, 1, st);
+    if (!rc) rc = zrow_op(g, batch, nullptr, OpC2R{d_out}, (const double2*)tmp, nullptr, nullptr, 0, st);
+    cudaFreeAsync(tmp, st);
+    return rc;
+  }
   const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  LAUNCH_PLANE(plane_kind(g), k_plane_c2r, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev,
-               (const double2*)d_spec, d_out);
+  LAUNCH_PLANE(plane_kind(g), k_plane_c2r, dim3(g->n1, batch), ps, st, g->dev, (const double2*)d_spec, d_out);
   return last_err();
 }
 
@@ -1376,12 +1711,12 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
   const int tc = col_tile(g, nf + 1);
   const int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
   if (nslot < g->n1 || nslot < ntile) return CMM_ERR_WORKSPACE;
-  const size_t csw = col_smem_bytes(g->n1, tc, nf), csb = col_smem_bytes(g->n1, tc, nf + 1);
+  const size_t csw = col_smem_bytes(g->n1, tc, nf, g->ax1.big), csb = col_smem_bytes(g->n1, tc, nf + 1, g->ax1.big);
   const double2* wt = (const double2*)d_wtab;
   const int ck = col_kind(g);
   if (version & CMM_NOHS) {  // MFA term alone: one column pass
     if (!(want & 1)) return CMM_ERR_ARG;
-    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), col_smem_bytes(g->n1, tc, 6), st, g->dev, d_active, R,
+    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), col_smem_bytes(g->n1, tc, 6, g->ax1.big), st, g->dev, d_active, R,
                1.0 / (beta * npts), (const double2*)nullptr, fs, (const double2*)d_rhohat, (const double2*)d_kst,
                wt, (double2*)d_chat, tc, 0.0, 1.0 / npts);
     return last_err();
@@ -1395,7 +1730,7 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
   else LAUNCH_WEIGHTS(k_col_weights);
 #undef LAUNCH_WEIGHTS
   const size_t ps = plane_smem_bytes(g->n2, g->n3, nf);
-  if (!ten && !g->staging && ps <= CMM_SMEM_MAX) {  // fused plane pass
+  if (!ten && !plane_staged(g, nf)) {  // fused plane pass
     if (has_wda)
       LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt_wda, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev,
                      d_active, R, version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
@@ -1435,6 +1770,16 @@ extern "C" int cmm_picard_static_step(const cmm_grid* g, int batch, const int* d
     return CMM_ERR_ARG;
   if (!(a_tol >= 0) || !(r_tol >= 0)) return CMM_ERR_ARG;
   if (nslot < g->n1) return CMM_ERR_WORKSPACE;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plane_staged(g, 1)) {  // y inverse of C1 into the output spectrum, z rows in place, y forward
+    double2* out = (double2*)d_rhohat_out;
+    int rc = ypass(g, batch, d_active, (const double2*)d_chat, out, 0, 1, 1, st);
+    if (rc) return rc;
+    OpPicard op{d_params, beta, lambda3, thr, a_tol, r_tol, d_rho, d_V, vstride, d_rho_out};
+    rc = zrow_op(g, batch, d_active, op, out, out, d_part, nslot, st);
+    if (rc) return rc;
+    return ypass(g, batch, d_active, out, out, 0, 1, 0, st);
+  }
   const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
   LAUNCH_PLANE(plane_kind(g), k_plane_picard, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_active,
                d_params, beta, lambda3, thr, a_tol, r_tol, (const double2*)d_chat, d_rho, d_V, vstride,
@@ -1455,6 +1800,17 @@ extern "C" int cmm_residual_step(const cmm_grid* g, int batch, const int* d_acti
   if (nslot < g->n1) return CMM_ERR_WORKSPACE;
   HistPtrs hp;
   for (int j = 0; j < CMM_MAX_HIST; ++j) hp.p[j] = (j < nhist) ? d_hist[j] : nullptr;
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plane_staged(g, 1)) {  // y inverse of C1 into stream-ordered scratch, then z rows
+    void* tmp = nullptr;
+    int rc = scratch_alloc(&tmp, sizeof(double2) * (size_t)batch * g->n1 * g->n2 * g->h3, st);
+    if (rc) return rc;
+    rc = ypass(g, batch, d_active, (const double2*)d_chat, (double2*)tmp, 0, 1, 1, st);
+    OpResidual op{d_params, beta, lambda3, a_tol, r_tol, d_rho, d_V, vstride, d_r_out, hp, nhist, hstride};
+    if (!rc) rc = zrow_op(g, batch, d_active, op, (const double2*)tmp, nullptr, d_part, nslot, st);
+    cudaFreeAsync(tmp, st);
+    return rc;
+  }
   const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
   LAUNCH_PLANE(plane_kind(g), k_plane_residual, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_active,
                d_params, beta, lambda3, a_tol, r_tol, (const double2*)d_chat, d_rho, d_V, vstride, d_r_out,
@@ -1475,6 +1831,13 @@ extern "C" int cmm_mix_step(const cmm_grid* g, int batch, const int* d_active, c
   for (int j = 0; j < CMM_MAX_FIELDS; ++j) {
     fp.p[j] = (j < nfield) ? d_fields[j] : nullptr;
     fp.stride[j] = (j < nfield) ? fstride[j] : 0;
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  if (plane_staged(g, 1)) {  // z rows (mix, forward) into the output spectrum, then y forward
+    OpMix op{d_coef, fp, nfield, clip, thr, lambda3, d_ref, refstride, d_V, vstride, d_rho_out};
+    int rc = zrow_op(g, batch, d_active, op, nullptr, (double2*)d_rhohat_out, d_part, nslot, st);
+    if (rc) return rc;
+    return ypass(g, batch, d_active, (double2*)d_rhohat_out, (double2*)d_rhohat_out, 0, 1, 0, st);
   }
   const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
   LAUNCH_PLANE(plane_kind(g), k_plane_mix, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_active, d_coef,

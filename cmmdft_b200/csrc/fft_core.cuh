@@ -17,9 +17,12 @@
 
 #define CMM_MAX_STAGES 16
 
+#define CMM_MAX_SMALL_RADIX 16   // larger radices run as two-phase direct DFT stages
+
 struct FftAxis {
   int n;                         // transform length
   int nstage;                    // number of radix stages
+  int big;                       // 1 when a radix exceeds CMM_MAX_SMALL_RADIX (needs scratch)
   int radix[CMM_MAX_STAGES];     // radix of stage s (forward order)
   int span[CMM_MAX_STAGES];      // block length L_s at stage s (L_0 = n)
 };
@@ -194,18 +197,63 @@ struct PencilSet {
   bool pencil_fast;  // consecutive threads take consecutive pencils (else consecutive butterflies)
 };
 
+// A stage of a large (prime) radix R: every output element is a direct
+// length-R DFT of its butterfly's inputs, written to `tmp` (ps.npencil * n
+// elements, pencil fastest) and copied back after a barrier.  Same twiddle
+// conventions as butterfly(): forward (DIF) y_q = (sum_r x_r w_R^{rq}) w_L^{jj q};
+// inverse (DIT) y_q = sum_r (x_r conj w_L^{jj r}) conj w_R^{rq}.
+template <bool INV>
+__device__ void big_stage(double2* s, int n, int R, int L, const double2* tw, int twn, const PencilSet& ps,
+                          double2* tmp) {
+  const int sR = L / R;
+  const int rstep = twn / R, lstep = twn / L;
+  const int total = ps.npencil * n;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int p = t % ps.npencil, e = t / ps.npencil;
+    const int blk = e / L, rem = e - blk * L;
+    const int q = rem / sR, jj = rem - q * sR;
+    const double2* b = s + (p / ps.ppg) * ps.gstride + (p % ps.ppg) * ps.pstride + (blk * L + jj) * ps.estride;
+    const int es = sR * ps.estride;
+    double2 acc = make_double2(0.0, 0.0);
+    for (int r = 0; r < R; ++r) {
+      double2 x = b[r * es];
+      const double2 w = tw[((r * q) % R) * rstep];
+      if (INV) {
+        if (jj) x = cmulc(x, tw[jj * r * lstep]);
+        acc = cadd(acc, cmulc(x, w));
+      } else {
+        acc = cadd(acc, cmul(x, w));
+      }
+    }
+    if (!INV && jj) acc = cmul(acc, tw[jj * q * lstep]);
+    tmp[t] = acc;
+  }
+  __syncthreads();
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    const int p = t % ps.npencil, e = t / ps.npencil;
+    s[(p / ps.ppg) * ps.gstride + (p % ps.ppg) * ps.pstride + e * ps.estride] = tmp[t];
+  }
+  __syncthreads();
+}
+
 // Transform every pencil of `ps` (length ax.n) in place.  `tw` is the twiddle
 // table w_{twn}^t in shared memory with twn = ax.n * twmul (twmul = 2 when the
 // table of the full real length is reused for a half-length complex FFT).
+// `tmp` (ps.npencil * ax.n elements) is needed when ax.big.
 // Ends with __syncthreads().
 template <bool INV>
-__device__ void fft_pencils(double2* s, const FftAxis& ax, const double2* tw, int twmul, const PencilSet& ps) {
+__device__ void fft_pencils(double2* s, const FftAxis& ax, const double2* tw, int twmul, const PencilSet& ps,
+                           double2* tmp = nullptr) {
   const int n = ax.n;
   const int twn = n * twmul;
   for (int k = 0; k < ax.nstage; ++k) {
     const int st = INV ? (ax.nstage - 1 - k) : k;
     const int R = ax.radix[st];
     const int L = ax.span[st];
+    if (R > CMM_MAX_SMALL_RADIX) {
+      big_stage<INV>(s, n, R, L, tw, twn, ps, tmp);
+      continue;
+    }
     const int sR = L / R;
     const int nb = n / R;
     const int tstep = (n / L) * twmul;
@@ -309,10 +357,11 @@ __device__ __forceinline__ void fft_ct(double2* s, const double2* tw, int twmul,
   static_assert(ns <= 4, "fft_ct handles up to 4 stages (N <= 4096)");
 }
 
-// Runtime-length transform of uniform pencils (any factorisation of ax.n).
+// Runtime-length transform of uniform pencils (any factorisation of ax.n);
+// tmp: npencil * ax.n elements of scratch when ax.big.
 template <bool INV>
 __device__ void fft_rt(double2* s, const FftAxis& ax, const double2* tw, int twmul, int npencil, int pstride,
-                       int estride) {
+                       int estride, double2* tmp = nullptr) {
   PencilSet ps = {npencil, npencil, 0, pstride, estride, true};
-  fft_pencils<INV>(s, ax, tw, twmul, ps);
+  fft_pencils<INV>(s, ax, tw, twmul, ps, tmp);
 }

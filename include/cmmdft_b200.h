@@ -93,7 +93,9 @@ int cmm_version(void);
 const char* cmm_status_string(int status);
 
 /* Grid plan: twiddle tables, digit-reversal position tables and the k-space
- * tables of a periodic N1 x N2 x N3 grid spanning the cell `rvecs` (3x3,
+ * tables of a periodic N1 x N2 x N3 grid (any sizes up to 1024; prime
+ * factors > 16 run as direct-DFT stages; odd N3 as a full-length z
+ * transform with the stored z frequencies in natural order) spanning the cell `rvecs` (3x3,
  * rows are cell vectors, bohr).  Replaces the k-grid, scalprod and Lanczos
  * tables of Grid.__init__ (cmmdft/system.py:232-295).  Allocates the plan's
  * device tables (the only persistent device memory this library owns). */
@@ -103,7 +105,11 @@ int cmm_grid_destroy(cmm_grid* grid);
  * shared memory runs the fused plane kernels (y and z transforms and the
  * pointwise step in one pass); larger planes, and the tensor variants, run
  * the staged form (a y pass over HBM, then z rows with the pointwise step).
- * mode 0 chooses by size (default), 1 always stages (tests, tuning). */
+ * mode 0 chooses by size (default), 1 always stages (tests, tuning).
+ * Grids with odd N3 or a prime factor > 16 on the y or z axis always stage.
+ * In the staged form cmm_residual_step and cmm_irfft_yz, whose spectrum
+ * input is read-only, take a stream-ordered temporary of one spectrum per
+ * instance (cudaMallocAsync / cudaFreeAsync on the call's stream). */
 int cmm_grid_set_staging(cmm_grid* grid, int mode);
 /* Number of stored frequencies per instance (N1*N2*H3) and H3. */
 int cmm_grid_spectrum_size(const cmm_grid* grid, long long* nspec, int* h3);
