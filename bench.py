@@ -98,7 +98,8 @@ def pipeline_bytes(plan, want, n_active):
     writes 5 dPhi spectra; column pass 2 reads 5 + rho_hat and writes the C1
     spectrum.  The MFA kernel spectrum (S) is read once per launch per pass
     that uses it.  Value-only launches (want & 1 == 0) skip the forward and the
-    second column pass.
+    second column pass.  With want & 8 the plane pass also writes the 5
+    weighted densities in real space (5 * N1*N2*N3*8 B).
     """
     S = plan.nspec * 16
     if want & 1:
@@ -107,6 +108,8 @@ def pipeline_bytes(plan, want, n_active):
     else:
         per = S * (1 + 5 + 5)
         shared = S if want & 2 else 0
+    if want & 8:
+        per += 5 * plan.npts * 8
     return per * n_active + shared
 
 

@@ -14,6 +14,8 @@ STAT_N, STAT_IUE, STAT_NONFIN, STAT_FID, STAT_FEXT, STAT_RES2, STAT_PHI, STAT_MF
     STAT_N3MAX, STAT_GNONFIN, STAT_GRAM0 = range(11)
 STAT_WDA, STAT_DER = 18, 19
 NSTAT = 20
+# hybrid line-search sums (cmm_ls_*)
+LS_MFA_RR, LS_MFA_XR, LS_N3MAX_G, LS_SUM_R, LS_SUM_RV, LS_FID, LS_PHI, LS_WDA, NLS = 0, 1, 2, 3, 4, 5, 8, 11, 16
 MAX_HIST = 8
 MAX_FIELDS = 12
 FMT, MFMT, WBII, ANTISYM, NOHS, WDA, TENSOR = 0, 1, 2, 8, 16, 32, 64
@@ -55,7 +57,13 @@ _SIGS = {
     "cmm_mfa_kernel": ([c_void_p, c_double, c_double, c_double, c_double, c_double, c_int, c_void_p,
                         c_void_p, P(ctypes.c_size_t), P(c_double), c_void_p], c_int),
     "cmm_fmt_c1": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p,
-                    c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p], c_int),
+                    c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p], c_int),
+    "cmm_ls_prepare": ([c_void_p, c_int, c_void_p, c_double, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                        c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p], c_int),
+    "cmm_ls_omega": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_double, c_double,
+                      c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int,
+                      c_void_p, c_void_p], c_int),
+    "cmm_ls_finalize": ([c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p], c_int),
     "cmm_fmt_weights": ([c_void_p, c_double, c_void_p, c_void_p], c_int),
     "cmm_picard_static_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_double,
                                 c_double, c_void_p,

@@ -213,6 +213,29 @@ def workspace(fn, B, nring):
     return ws
 
 
+def ls_workspace(fn, ws, B, nring):
+    """Buffers of the transform-free hybrid line search, added to ``ws`` on
+    first use: per ring slot the yz-spectrum and the weighted densities of
+    its density, the weighted densities and spectrum of a residual, and the
+    line-search partial sums."""
+    if 'wd_ring' in ws:
+        return ws
+    plan = fn.plan
+    n1, n2, n3 = plan.npoints
+    dev, f64 = 'cuda', torch.float64
+    nslot = ws['buf'].nslot
+    ws['wd_ring'] = torch.empty((nring, fn.nwd, B, n1, n2, n3), dtype=f64, device=dev)
+    ws['spec_ring'] = torch.empty((nring, B, plan.nspec * 2), dtype=f64, device=dev)
+    ws['wd_r'] = torch.empty((fn.nwd, B, n1, n2, n3), dtype=f64, device=dev)
+    ws['rhat'] = plan.new_spec(B)
+    ls_part = torch.zeros((B, L.NLS, nslot), dtype=f64, device=dev)
+    ls_part[:, L.LS_N3MAX_G, :] = -np.inf
+    ws['ls_part'] = ls_part
+    ws['ls'] = torch.zeros((B, L.NLS), dtype=f64, device=dev)
+    ws['ls_alpha'] = torch.zeros(B, dtype=f64, device=dev)
+    return ws
+
+
 class BatchSolve(object):
     """Solve B fixed points that share a Functional (grid, host, guest, T).
 
@@ -262,6 +285,8 @@ class BatchSolve(object):
         self.dr = self.plan.dr
         self.nring = max(self.m, 2) if 'anderson' in self.method else 2
         ws = workspace(fn, B, self.nring)
+        if self.method != 'static':
+            ls_workspace(fn, ws, B, self.nring)
         for k, v in ws.items():
             setattr(self, k, v)
         self._pin_i = 0
@@ -294,30 +319,32 @@ class BatchSolve(object):
         self.kernel_launches += 1
         return self.buf.stats.cpu().numpy()
 
-    def _mix(self, coefs, fields, clip, ref, out, thr=0.0):
-        """out = sum_j coefs[:, j] * fields[j] (fields: [B, ...] tensors); spectrum into self.that."""
+    def _mix(self, coefs, fields, clip, ref, out, thr=0.0, spec_out=None):
+        """out = sum_j coefs[:, j] * fields[j] (fields: [B, ...] tensors); spectrum
+        into spec_out (default self.that)."""
         h = self._pinned('coef')
         c = h.numpy()
         c[:] = 0.0
         c[:, :len(fields)] = coefs
         self.coef.copy_(h, non_blocking=True)
-        E.mix_step(self.fn, self.buf, self.coef, fields, [self.npts] * len(fields), clip, ref, out, self.that,
-                   thr=thr, active=self.active)
+        E.mix_step(self.fn, self.buf, self.coef, fields, [self.npts] * len(fields), clip, ref, out,
+                   self.that if spec_out is None else spec_out, thr=thr, active=self.active)
         self.kernel_launches += 1
 
-    def _c1(self, spec, chat, want):
+    def _c1(self, spec, chat, want, wd=None):
         ev = self.pipeline_events
         if ev is not None:
             e0 = torch.cuda.Event(enable_timing=True)
             e1 = torch.cuda.Event(enable_timing=True)
             e0.record()
-        self.fn.c1(self.buf, spec, chat, want=want, active=self.active)
+        self.fn.c1(self.buf, spec, chat, want=want, active=self.active, wd=wd)
         if ev is not None:
             e1.record()
             ev.append((e0, e1, want, int(self.mask_host.sum())))
         self.kernel_launches += 3 if (want & 1) else 2
 
-    def _set_params(self, a=None):
+    def _set_params(self, a=None, n3=None):
+        """params[b] = (fugacity, Picard mixing a, mu, max n3 of the current density)."""
         h = self._pinned('params')
         p = h.numpy()
         p[:] = 0.0
@@ -325,6 +352,8 @@ class BatchSolve(object):
         if a is not None:
             p[:, 1] = a
         p[:, 2] = self.mu
+        if n3 is not None:
+            p[:, 3] = n3
         self.params.copy_(h, non_blocking=True)
 
     def _residual(self, chat, rho, r_out, hist):
@@ -409,14 +438,24 @@ class BatchSolve(object):
         return self.N_out, self.result, self.conv
 
     def _init_state(self, todo):
-        """rho0 -> ring slot 0, its spectrum, C1, Omega and (for Anderson) r_0."""
-        st = self._eval_density(todo, np.ones((self.B, 1)), [self.rho0], L.CLIP_NONE, self.ring[0],
-                                1 | 2 | 4, self.rho0)
-        self.rhohat.copy_(self.that)
+        """rho0 -> ring slot 0, its spectrum, C1, Omega and (for Anderson) r_0.
+        The hybrid/Anderson loop also keeps the spectrum and weighted densities
+        of ring slot 0 for the line search."""
+        if self.method == 'static':
+            st = self._eval_density(todo, np.ones((self.B, 1)), [self.rho0], L.CLIP_NONE, self.ring[0],
+                                    1 | 2 | 4, self.rho0)
+            self.rhohat.copy_(self.that)
+        else:
+            self._set_active(todo)
+            self._mix(np.ones((self.B, 1)), [self.rho0], L.CLIP_NONE, self.rho0, self.ring[0],
+                      spec_out=self.spec_ring[0])
+            self._c1(self.spec_ring[0], self.chat2, 1 | 2 | 4 | 8, wd=self.wd_ring[0])
+            st = self._stats()
         self.chat.copy_(self.chat2)
         self.omega0 = np.array([self._omega(st[b], b) for b in range(self.B)])
         self.n3max = st[:, L.STAT_N3MAX].copy()
         self.Ncur = st[:, L.STAT_N] * self.dr
+        self.last_stats = st.copy()
         return st
 
     def _solve_once(self, todo):
@@ -523,7 +562,6 @@ class BatchSolve(object):
         self.And_true = np.zeros(B, dtype=bool)
         self.it_eps0 = np.full(B, np.nan)
         self.damping = np.full(B, self.damping0)
-        self.last_stats = np.zeros((B, L.NSTAT))
         # r_0 for the initial density
         self._set_active(live)
         self._residual(self.chat, self.ring[0], self.rres[0], [])
@@ -588,8 +626,9 @@ class BatchSolve(object):
         return [j % m for j in range(max(0, k_new - m + 1), k_new)]
 
     def _post_update(self, mask, k, s_new, st_mix):
-        """C1, Omega and residual of the density just written to ring slot s_new."""
-        self._c1(self.that, self.chat2, 1 | 2 | 4)
+        """C1, Omega and residual of the density just written to ring slot s_new
+        (its spectrum in spec_ring[s_new]); its weighted densities are kept."""
+        self._c1(self.spec_ring[s_new], self.chat2, 1 | 2 | 4 | 8, wd=self.wd_ring[s_new])
         hist_slots = self._valid_hist(k, s_new)
         self._residual(self.chat2, self.ring[s_new], self.rres[s_new], [self.rres[j] for j in hist_slots])
         st = self._stats()
@@ -628,7 +667,7 @@ class BatchSolve(object):
             coefs[b, mk:] = d * al
         fields = [self.ring[j] for j in slots] + [self.rres[j] for j in slots]
         self._set_active(mask)
-        self._mix(coefs, fields, L.CLIP_DENSITY, self.ring[s_prev], self.ring[s_new])
+        self._mix(coefs, fields, L.CLIP_DENSITY, self.ring[s_prev], self.ring[s_new], spec_out=self.spec_ring[s_new])
         st, hist_slots = self._post_update(mask, k, s_new, None)
         ok = np.zeros(B, dtype=bool)
         for b in np.where(mask)[0]:
@@ -654,28 +693,61 @@ class BatchSolve(object):
         self.omega_evals += int(mask.sum())
         return np.array([self._omega(st[b], b) if mask[b] else np.nan for b in range(self.B)])
 
+    def _ls_omega(self, ls_b, b, i, alpha):
+        """Omega(rho + alpha r) of instance b from the line-search sums ls_b
+        (alpha = the i-th trial alpha) and the sums of rho itself, in the
+        order of _omega (solver.py:103-119)."""
+        beta, dr = self.fn.beta, self.dr
+        st = self.last_stats[b]
+        N = (st[L.STAT_N] + alpha * ls_b[L.LS_SUM_R]) * dr
+        G = (ls_b[L.LS_FID + i] * dr) / beta - self.mu[b] * N
+        G += (ls_b[L.LS_PHI + i] * dr) / beta
+        G += 0.5 * ((st[L.STAT_MFA] + 2 * alpha * ls_b[L.LS_MFA_XR] + alpha * alpha * ls_b[L.LS_MFA_RR]) * dr)
+        G += (st[L.STAT_FEXT] + alpha * ls_b[L.LS_SUM_RV]) * dr
+        if self.fn.wda is not None:
+            G += ls_b[L.LS_WDA + i] * dr
+        return G
+
     def _hybrid_step(self, mask, k, s_prev, s_new):
-        """Picard.update_rho_hybrid for the instances in mask (solver.py:403-457)."""
+        """Picard.update_rho_hybrid for the instances in mask (solver.py:403-457).
+
+        alpha_max (from max n3 of G = rho + r) and Omega at the trial alphas
+        0.45, 0.9 and 0.225 alpha_max come from one pass over the stored
+        weighted densities of rho and r (cmm_ls_*): the trial densities are
+        never transformed, and both candidates for the second trial point are
+        evaluated before the host chooses between them."""
         B = self.B
         prev = self.omega0.copy()
-        # alpha_max from max n3 of rho and of G = rho + r (solver.py:150-165)
-        coefs = np.ones((B, 2))
-        stn = self._eval_density(mask, coefs, [self.ring[s_prev], self.rres[s_prev]], L.CLIP_NONE,
-                                 self.trial, 4, self.ring[s_prev])
-        amax = np.zeros(B)
-        for b in np.where(mask)[0]:
-            a, g = self.n3max_of_current(b), stn[b, L.STAT_N3MAX]
-            amax[b] = np.min([abs((1 - a) / ((g - a) + 1e-16)), 1])
+        self._set_active(mask)
+        self._set_params(n3=self.n3max)
+        fn = self.fn
+        fn.ls_prepare(self.buf, self.rres[s_prev], self.spec_ring[s_prev], self.wd_ring[s_prev], self.rhat,
+                      self.wd_r, self.ls_part, active=self.active)
+        fn.ls_omega(self.buf, self.params, (0.45, 0.9, 0.225), self.ring[s_prev], self.rres[s_prev],
+                    self.wd_ring[s_prev], self.wd_r, self.ls_part, self.ls_alpha, active=self.active)
+        fn.ls_finalize(self.buf, self.ls_part, self.ls, active=self.active)
+        self.kernel_launches += 6
+        ls = self.ls.cpu().numpy()
+        amax = np.where(mask, self.ls_alpha.cpu().numpy(), 0.0)
         aopt = np.zeros(B)
         mn = np.zeros(B)
         mx = np.zeros(B)
         need = mask & ~np.isclose(amax, 0)
         if need.any():
-            a1 = 0.45 * amax
-            o1 = self._trial_omega(need, a1, s_prev)
-            a2 = np.where(o1 <= prev, 0.9 * amax, 0.225 * amax)
-            o2 = self._trial_omega(need, a2, s_prev)
             idx = np.where(need)[0]
+            a1 = 0.45 * amax
+            o1 = np.full(B, np.nan)
+            o2 = np.full(B, np.nan)
+            a2 = np.zeros(B)
+            for b in idx:
+                o1[b] = self._ls_omega(ls[b], b, 0, a1[b])
+                if o1[b] <= prev[b]:
+                    a2[b] = 0.9 * amax[b]
+                    o2[b] = self._ls_omega(ls[b], b, 1, a2[b])
+                else:
+                    a2[b] = 0.225 * amax[b]
+                    o2[b] = self._ls_omega(ls[b], b, 2, a2[b])
+            self.omega_evals += 2 * len(idx)
             cf = np.array([np.polyfit([0, a1[b], a2[b]], [prev[b], o1[b], o2[b]], 2) for b in idx])
             hi = np.maximum(a1[idx], a2[idx])
             aopt[idx], mn[idx], mx[idx] = grid_parabola(cf, hi)
@@ -706,7 +778,7 @@ class BatchSolve(object):
         coefs[:, 1] = aopt * self.cf
         self._set_active(mask)
         self._mix(coefs, [self.ring[s_prev], self.rres[s_prev]], L.CLIP_DENSITY, self.ring[s_prev],
-                  self.ring[s_new])
+                  self.ring[s_new], spec_out=self.spec_ring[s_new])
         st, hist_slots = self._post_update(mask, k, s_new, None)
         for b in np.where(mask)[0]:
             self.omega0[b] = self._omega(st[b], b)

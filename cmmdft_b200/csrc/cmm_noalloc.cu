@@ -78,7 +78,7 @@ extern "C" int cmm_fmt_c1_noalloc(const cmm_grid* g, int batch, const int* d_act
   k_noalloc_clear_part<<<148, 256, 0, st>>>(part, batch, nslot);
   if (cudaPeekAtLastError() != cudaSuccess) return CMM_ERR_CUDA;
   rc = cmm_fmt_c1(g, batch, d_active, R, beta, version, wda, d_kst, d_wtab, d_rhohat, d_chat, work, part, nslot,
-                  want, stream);
+                  want & 7, nullptr, stream);
   if (rc) return rc;
   if (want & 6) {
     unsigned mask = 0;

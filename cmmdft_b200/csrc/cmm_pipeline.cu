@@ -221,8 +221,9 @@ __device__ inline void put_part(double* part, int b, int q, int nslot, int slot,
 // ================================================ 3D FFT (setup / tests) ==
 template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_PLANE_THREADS)
-k_plane_r2c(GridDev g, const double* __restrict__ in, double2* __restrict__ out) {
+k_plane_r2c(GridDev g, const int* __restrict__ active, const double* __restrict__ in, double2* __restrict__ out) {
   const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
   PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
   const PlaneShape<N2C, M3C> sh(g);
   const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
@@ -486,34 +487,47 @@ __global__ void k_fmt_weights(GridDev g, double R, double2* __restrict__ wtab) {
 // Outputs (field stride fsw): 0 = n0 (w0), 1 = n3 (w3), 2..4 = nv2 (x, y, z).
 // The WDA field is a template parameter, as in the plane pass, so that the
 // plain kernels keep their register budget.
-template <int N1C, int TCC, bool WDA, bool TEN>
+// LS (hybrid line search): the input is the spectrum of a residual r; the
+// spectrum of the current density rho (rho_ref) is forwarded alongside so
+// that the MFA energy of rho + a r can be assembled from sum |r|^2 K and the
+// cross term sum Re(conj(rho) r) K (into ls_part, CMM_LS_MFA_RR / _XR).
+template <int N1C, int TCC, bool WDA, bool TEN, bool LS>
 __device__ __forceinline__ void col_weights_body(GridDev g, const int* __restrict__ active, double R,
                                                  double inv_npts, const double2* __restrict__ rhohat,
                                                  double2* __restrict__ wout, size_t fsw,
                                                  const double2* __restrict__ kst, const double2* __restrict__ wtab,
                                                  double* __restrict__ part, int nslot_part, int want_value, int tc,
-                                                 double wda_D) {
+                                                 double wda_D, const double2* __restrict__ rho_ref,
+                                                 double* __restrict__ ls_part) {
   const int b = blockIdx.y, tile = blockIdx.x;
   if (active && !active[b]) return;
   const ColShape<N1C, TCC> sh(g, tc);
   const int c0 = tile * sh.tc;
   const int tb = WDA ? 6 : 5;           // first tensor field
-  const int ns = tb + (TEN ? 6 : 0);    // n0, n3, nv2 x/y/z, WDA, then the tensor densities
+  const int nw = tb + (TEN ? 6 : 0);    // n0, n3, nv2 x/y/z, WDA, then the tensor densities
+  const int ns = nw + (LS ? 1 : 0);     // slots: the weighted densities (+ rho_ref)
   ColSmem s = col_smem_setup(g, sh, ns);
   load_col_tile(g, s, sh, ns, 0, rhohat, b, c0, nullptr);
+  if constexpr (LS) load_col_tile(g, s, sh, ns, nw, rho_ref, b, c0, nullptr);
   __syncthreads();
   col_fft<false>(g, s, sh, ns, 0, 1);
+  if constexpr (LS) col_fft<false>(g, s, sh, ns, nw, 1);
   const int nc = g.n2 * g.h3;
-  double mfa = 0.0;
+  double mfa = 0.0, mxr = 0.0;
   for (int i = threadIdx.x; i < sh.n1 * sh.tc; i += blockDim.x) {
     const int p1 = i / sh.tc, c = i - p1 * sh.tc;
     const int col = c0 + c;
     if (col >= nc) continue;
     double2 F = cel(s, sh, ns, 0, p1, c);
     const Weights w = fmt_weights_at(g, wtab, p1, col, R);
-    if (want_value) {
+    if (want_value || LS) {
       const double2 K = __ldg(kst + (size_t)p1 * nc + col);
-      mfa += g.wt3[col - (col / g.h3) * g.h3] * (F.x * F.x + F.y * F.y) * K.x;
+      const double w3 = g.wt3[col - (col / g.h3) * g.h3];
+      mfa += w3 * (F.x * F.x + F.y * F.y) * K.x;
+      if constexpr (LS) {
+        const double2 P = cel(s, sh, ns, nw, p1, c);
+        mxr += w3 * (P.x * F.x + P.y * F.y) * K.x;
+      }
     }
     F = cscale(F, inv_npts);
     if (WDA) cel(s, sh, ns, 5, p1, c) = cscale(F, wda_weight_at(g, p1, col, wda_D));
@@ -530,12 +544,18 @@ __device__ __forceinline__ void col_weights_body(GridDev g, const int* __restric
     cel(s, sh, ns, 0, p1, c) = cscale(F, w.w0);
   }
   __syncthreads();
-  col_fft<true>(g, s, sh, ns, 0, ns);
-  for (int f = 0; f < ns; ++f) store_col_tile(g, s, sh, ns, f, wout + f * fsw, b, c0, nullptr);
-  if (want_value) {
-    __shared__ double red[32];
+  col_fft<true>(g, s, sh, ns, 0, nw);
+  for (int f = 0; f < nw; ++f) store_col_tile(g, s, sh, ns, f, wout + f * fsw, b, c0, nullptr);
+  __shared__ double red[32];
+  if (want_value && !LS) {
     double t = block_sum(mfa, red);
     put_part(part, b, CMM_STAT_MFA, nslot_part, tile, t);
+  }
+  if constexpr (LS) {
+    double t = block_sum(mfa, red);
+    if (threadIdx.x == 0) ls_part[((size_t)b * CMM_NLS + CMM_LS_MFA_RR) * nslot_part + tile] = t;
+    t = block_sum(mxr, red);
+    if (threadIdx.x == 0) ls_part[((size_t)b * CMM_NLS + CMM_LS_MFA_XR) * nslot_part + tile] = t;
   }
 }
 
@@ -543,17 +563,21 @@ __device__ __forceinline__ void col_weights_body(GridDev g, const int* __restric
   GridDev g, const int *__restrict__ active, double R, double inv_npts, const double2 *__restrict__ rhohat, \
       double2 *__restrict__ wout, size_t fsw, const double2 *__restrict__ kst,                             \
       const double2 *__restrict__ wtab, double *__restrict__ part, int nslot_part, int want_value, int tc,  \
-      double wda_D
-#define COL_WEIGHTS_KERNEL(name, wda, ten)                                                              \
+      double wda_D, const double2 *__restrict__ rho_ref, double *__restrict__ ls_part
+#define COL_WEIGHTS_KERNEL(name, wda, ten, ls)                                                          \
   template <int N1C, int TCC>                                                                            \
   __global__ void __launch_bounds__(CMM_COL_THREADS) name(COL_WEIGHTS_ARGS) {                           \
-    col_weights_body<N1C, TCC, wda, ten>(g, active, R, inv_npts, rhohat, wout, fsw, kst, wtab, part,     \
-                                         nslot_part, want_value, tc, wda_D);                             \
+    col_weights_body<N1C, TCC, wda, ten, ls>(g, active, R, inv_npts, rhohat, wout, fsw, kst, wtab, part, \
+                                             nslot_part, want_value, tc, wda_D, rho_ref, ls_part);       \
   }
-COL_WEIGHTS_KERNEL(k_col_weights, false, false)
-COL_WEIGHTS_KERNEL(k_col_weights_wda, true, false)
-COL_WEIGHTS_KERNEL(k_col_weights_t, false, true)
-COL_WEIGHTS_KERNEL(k_col_weights_wda_t, true, true)
+COL_WEIGHTS_KERNEL(k_col_weights, false, false, false)
+COL_WEIGHTS_KERNEL(k_col_weights_wda, true, false, false)
+COL_WEIGHTS_KERNEL(k_col_weights_t, false, true, false)
+COL_WEIGHTS_KERNEL(k_col_weights_wda_t, true, true, false)
+COL_WEIGHTS_KERNEL(k_col_weights_ls, false, false, true)
+COL_WEIGHTS_KERNEL(k_col_weights_ls_wda, true, false, true)
+COL_WEIGHTS_KERNEL(k_col_weights_ls_t, false, true, true)
+COL_WEIGHTS_KERNEL(k_col_weights_ls_wda_t, true, true, true)
 
 // ======================== column pass 2: dPhi spectra -> C1 spectrum ====
 // Inputs: 5 dPhi spectra (field stride fsg): g_s (pairs with w0), g3 (w3),
@@ -748,7 +772,8 @@ template <int N2C, int M3C, bool has_wda>
 __device__ __forceinline__ void plane_fmt_body(GridDev g, const int* __restrict__ active, double R, int version,
                                                const cmm_wda_eos& wda, const double2* __restrict__ win,
                                                size_t fsw, double2* __restrict__ gout, size_t fsg,
-                                               double* __restrict__ part, int nslot_part, int want) {
+                                               double* __restrict__ part, int nslot_part, int want,
+                                               double* __restrict__ wd, size_t fsr) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
   const int ns = has_wda ? 6 : 5;
@@ -759,7 +784,8 @@ __device__ __forceinline__ void plane_fmt_body(GridDev g, const int* __restrict_
   __syncthreads();
   plane_inverse<N2C, M3C>(g, s, ns);
   double phi = 0.0, n3max = -INFINITY, fwda = 0.0;
-  const bool do_c1 = (want & 1) != 0;
+  const bool do_c1 = (want & 1) != 0, do_phi = (want & 3) != 0;
+  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
   for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
     const int r = i / sh.n3, j = i - r * sh.n3;
     double& a0 = rel(s, sh, ns, 0, r, j);
@@ -768,17 +794,21 @@ __device__ __forceinline__ void plane_fmt_body(GridDev g, const int* __restrict_
     double& ay = rel(s, sh, ns, 3, r, j);
     double& az = rel(s, sh, ns, 4, r, j);
     n3max = fmax(n3max, a3);
-    PhiOut o = fmt_point<false>(a0, a3, ax, ay, az, nullptr, nullptr, R, version);
-    phi += o.phi;
-    if (do_c1) {
-      a0 = o.gs; a3 = o.g3; ax = o.gv[0]; ay = o.gv[1]; az = o.gv[2];
-    }
-    if (has_wda) {
-      double& aw = rel(s, sh, ns, 5, r, j);
-      double fv, dfv;
-      wda_eos(wda, aw, fv, dfv);
-      fwda += fv;
-      if (do_c1) aw = dfv;
+    if (want & 8)  // the weighted densities themselves (hybrid line search)
+      for (int f = 0; f < ns; ++f) wd[f * fsr + roff + i] = rel(s, sh, ns, f, r, j);
+    if (do_phi) {
+      PhiOut o = fmt_point<false>(a0, a3, ax, ay, az, nullptr, nullptr, R, version);
+      phi += o.phi;
+      if (do_c1) {
+        a0 = o.gs; a3 = o.g3; ax = o.gv[0]; ay = o.gv[1]; az = o.gv[2];
+      }
+      if (has_wda) {
+        double& aw = rel(s, sh, ns, 5, r, j);
+        double fv, dfv;
+        wda_eos(wda, aw, fv, dfv);
+        fwda += fv;
+        if (do_c1) aw = dfv;
+      }
     }
   }
   __syncthreads();
@@ -805,16 +835,18 @@ template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_FMT_THREADS)
 k_plane_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
             const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
-            double* __restrict__ part, int nslot_part, int want) {
-  plane_fmt_body<N2C, M3C, false>(g, active, R, version, wda, win, fsw, gout, fsg, part, nslot_part, want);
+            double* __restrict__ part, int nslot_part, int want, double* __restrict__ wd, size_t fsr) {
+  plane_fmt_body<N2C, M3C, false>(g, active, R, version, wda, win, fsw, gout, fsg, part, nslot_part, want, wd,
+                                  fsr);
 }
 
 template <int N2C, int M3C>
 __global__ void __launch_bounds__(CMM_FMT_THREADS)
 k_plane_fmt_wda(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
                 const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
-                double* __restrict__ part, int nslot_part, int want) {
-  plane_fmt_body<N2C, M3C, true>(g, active, R, version, wda, win, fsw, gout, fsg, part, nslot_part, want);
+                double* __restrict__ part, int nslot_part, int want, double* __restrict__ wd, size_t fsr) {
+  plane_fmt_body<N2C, M3C, true>(g, active, R, version, wda, win, fsw, gout, fsg, part, nslot_part, want, wd,
+                                 fsr);
 }
 
 // ================================================ staged plane passes ==
@@ -971,7 +1003,7 @@ template <int M3C, bool WDA, bool TEN>
 __global__ void __launch_bounds__(CMM_ROW_THREADS)
 k_zrow_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
            const double2* __restrict__ win, size_t fs, double2* __restrict__ gout, int chunk,
-           double* __restrict__ part, int nslot_part, int want) {
+           double* __restrict__ part, int nslot_part, int want, double* __restrict__ wd, size_t fsr) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
   constexpr int tb = WDA ? 6 : 5;
@@ -979,7 +1011,8 @@ k_zrow_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm
   const int h3 = M3C ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
   PlaneSmem s = zrow_smem_setup<M3C>(g, nf * chunk);
   const size_t poff = ((size_t)b * g.n1 + i1) * n2 * h3;
-  const bool do_c1 = (want & 1) != 0;
+  const bool do_c1 = (want & 1) != 0, do_phi = (want & 3) != 0;
+  const size_t roff = ((size_t)b * g.n1 + i1) * n2 * n3;
   double phi = 0.0, n3max = -INFINITY, fwda = 0.0;
   for (int r0 = 0; r0 < n2; r0 += chunk) {
     const int nr = min(chunk, n2 - r0);
@@ -994,6 +1027,9 @@ k_zrow_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm
       double& ay = zrow_rel<M3C>(g, s, nf, 3, r, j);
       double& az = zrow_rel<M3C>(g, s, nf, 4, r, j);
       n3max = fmax(n3max, a3);
+      if (want & 8)
+        for (int f = 0; f < nf; ++f) wd[f * fsr + roff + (size_t)(r0 + r) * n3 + j] = zrow_rel<M3C>(g, s, nf, f, r, j);
+      if (!do_phi) continue;
       double T[6], gT[6];
       if constexpr (TEN)
         for (int q = 0; q < 6; ++q) T[q] = zrow_rel<M3C>(g, s, nf, tb + q, r, j);
@@ -1395,6 +1431,116 @@ struct OpMix {   // k_plane_mix
   }
 };
 
+// ================================================= hybrid line search ==
+// max over each plane of n3(rho) + n3(r) (field 1 of the stored weighted densities).
+__global__ void __launch_bounds__(256)
+k_ls_n3max(GridDev g, const int* __restrict__ active, const double* __restrict__ wd_rho,
+           const double* __restrict__ wd_r, size_t fsr, double* __restrict__ ls_part, int nslot) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
+  const size_t plane = (size_t)g.n2 * g.n3;
+  const size_t off = fsr + ((size_t)b * g.n1 + i1) * plane;
+  double m = -INFINITY;
+  for (size_t i = threadIdx.x; i < plane; i += blockDim.x) m = fmax(m, __ldg(wd_rho + off + i) + __ldg(wd_r + off + i));
+  __shared__ double red[32];
+  m = block_max(m, red);
+  if (threadIdx.x == 0) ls_part[((size_t)b * CMM_NLS + CMM_LS_N3MAX_G) * nslot + i1] = m;
+}
+
+// Omega ingredients of rho + alpha_i r for three alphas, one plane per block.
+template <bool WDA, bool TEN>
+__global__ void __launch_bounds__(CMM_ROW_THREADS)
+k_ls_omega(GridDev g, const int* __restrict__ active, const double* __restrict__ params, double c0, double c1,
+           double c2, double R, double lambda3, int version, cmm_wda_eos wda, const double* __restrict__ rho,
+           const double* __restrict__ r, const double* __restrict__ V, long long vstride,
+           const double* __restrict__ wd_rho, const double* __restrict__ wd_r, size_t fsr,
+           double* __restrict__ ls_part, int nslot, double* __restrict__ alpha_out) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
+  constexpr int tb = WDA ? 6 : 5;
+  constexpr int nf = tb + (TEN ? 6 : 0);
+  __shared__ double s_alpha[3];
+  if (threadIdx.x < 32) {  // alpha_max of this instance (every block reduces the same partials)
+    const double* pm = ls_part + ((size_t)b * CMM_NLS + CMM_LS_N3MAX_G) * nslot;
+    double gmax = -INFINITY;
+    for (int k = threadIdx.x; k < nslot; k += 32) gmax = fmax(gmax, pm[k]);
+    for (int o = 16; o > 0; o >>= 1) gmax = fmax(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
+    if (threadIdx.x == 0) {
+      const double a = params[b * 4 + 3];
+      const double q = fabs((1 - a) / ((gmax - a) + 1e-16));
+      const double amax = (q != q) ? q : fmin(q, 1.0);   // np.min([q, 1]) (propagates NaN)
+      s_alpha[0] = c0 * amax; s_alpha[1] = c1 * amax; s_alpha[2] = c2 * amax;
+      if (i1 == 0) alpha_out[b] = amax;
+    }
+  }
+  __syncthreads();
+  const double al[3] = {s_alpha[0], s_alpha[1], s_alpha[2]};
+  const size_t plane = (size_t)g.n2 * g.n3;
+  const size_t pbase = (size_t)i1 * plane;
+  const size_t gbase = (size_t)b * g.n1 * plane + pbase;
+  double sr = 0.0, srv = 0.0, fid[3] = {0, 0, 0}, phi[3] = {0, 0, 0}, fw[3] = {0, 0, 0};
+  for (size_t i = threadIdx.x; i < plane; i += blockDim.x) {
+    const size_t gi = gbase + i;
+    const double x0 = __ldg(rho + gi), rr = __ldg(r + gi), v = __ldg(V + b * vstride + pbase + i);
+    sr += rr;
+    srv += rr * v;
+    double n0[nf], n1[nf];
+#pragma unroll
+    for (int f = 0; f < nf; ++f) {
+      n0[f] = __ldg(wd_rho + f * fsr + gi);
+      n1[f] = __ldg(wd_r + f * fsr + gi);
+    }
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      double x = x0 + al[k] * rr;
+      x = (x < 1e-12) ? 1e-30 : x;  // Solver._clip_density
+      fid[k] += x * (log(lambda3 * x) - 1.0);
+      double n[nf];
+#pragma unroll
+      for (int f = 0; f < nf; ++f) n[f] = n0[f] + al[k] * n1[f];
+      double gT[6];
+      phi[k] += fmt_point<TEN>(n[0], n[1], n[2], n[3], n[4], TEN ? n + tb : nullptr, gT, R, version).phi;
+      if constexpr (WDA) {
+        double fv, dfv;
+        wda_eos(wda, n[5], fv, dfv);
+        fw[k] += fv;
+      }
+    }
+  }
+  __shared__ double red[32];
+  double* out = ls_part + (size_t)b * CMM_NLS * nslot + i1;
+  double t = block_sum(sr, red);
+  if (threadIdx.x == 0) out[CMM_LS_SUM_R * nslot] = t;
+  t = block_sum(srv, red);
+  if (threadIdx.x == 0) out[CMM_LS_SUM_RV * nslot] = t;
+  for (int k = 0; k < 3; ++k) {
+    t = block_sum(fid[k], red);
+    if (threadIdx.x == 0) out[(CMM_LS_FID + k) * nslot] = t;
+    t = block_sum(phi[k], red);
+    if (threadIdx.x == 0) out[(CMM_LS_PHI + k) * nslot] = t;
+    if constexpr (WDA) {
+      t = block_sum(fw[k], red);
+      if (threadIdx.x == 0) out[(CMM_LS_WDA + k) * nslot] = t;
+    }
+  }
+}
+
+__global__ void k_ls_finalize(const int* __restrict__ active, const double* __restrict__ part, int nslot,
+                              double* __restrict__ ls) {
+  const int b = blockIdx.x, q = threadIdx.y;
+  if (q >= CMM_NLS) return;
+  if (active && !active[b]) return;
+  const double* p = part + ((size_t)b * CMM_NLS + q) * nslot;
+  const bool mx = (q == CMM_LS_N3MAX_G);
+  double acc = mx ? -INFINITY : 0.0;
+  for (int i = threadIdx.x; i < nslot; i += 32) acc = mx ? fmax(acc, p[i]) : acc + p[i];
+  for (int o = 16; o > 0; o >>= 1) {
+    double v = __shfl_xor_sync(0xffffffffu, acc, o);
+    acc = mx ? fmax(acc, v) : acc + v;
+  }
+  if (threadIdx.x == 0) ls[(size_t)b * CMM_NLS + q] = acc;
+}
+
 // ============================================================ finalize ==
 __global__ void k_stats_finalize(const int* __restrict__ active, const double* __restrict__ part,
                                  int nslot, unsigned mask, double* __restrict__ stats) {
@@ -1565,39 +1711,40 @@ static int zrow_op(const cmm_grid* g, int batch, const int* act, const Op& op, c
 template <int M3C, bool WDA, bool TEN>
 static int zrow_fmt_one(const cmm_grid* g, int batch, const int* act, double R, int version,
                         const cmm_wda_eos& we, const double2* win, size_t fs, double2* gout, int chunk,
-                        double* part, int nslot, int want, cudaStream_t st) {
+                        double* part, int nslot, int want, double* wd, cudaStream_t st) {
   constexpr int nf = (WDA ? 6 : 5) + (TEN ? 6 : 0);
   const size_t sb = zrow_smem_bytes_g(g, nf * chunk);
   int rc;
   if ((rc = set_smem((const void*)k_zrow_fmt<M3C, WDA, TEN>, sb))) return rc;
   k_zrow_fmt<M3C, WDA, TEN><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(
-      g->dev, act, R, version, we, win, fs, gout, chunk, part, nslot, want);
+      g->dev, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd,
+      (size_t)batch * g->n1 * g->n2 * g->n3);
   return last_err();
 }
 
 template <int M3C>
 static int zrow_fmt_m3(const cmm_grid* g, int batch, const int* act, double R, int version, const cmm_wda_eos& we,
                        const double2* win, size_t fs, double2* gout, int chunk, double* part, int nslot, int want,
-                       cudaStream_t st) {
+                       double* wd, cudaStream_t st) {
   const bool wda = (version & CMM_WDA) != 0, ten = (version & CMM_TENSOR) != 0;
   if (wda && ten)
-    return zrow_fmt_one<M3C, true, true>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+    return zrow_fmt_one<M3C, true, true>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
   if (wda)
-    return zrow_fmt_one<M3C, true, false>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+    return zrow_fmt_one<M3C, true, false>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
   if (ten)
-    return zrow_fmt_one<M3C, false, true>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
-  return zrow_fmt_one<M3C, false, false>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+    return zrow_fmt_one<M3C, false, true>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
+  return zrow_fmt_one<M3C, false, false>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
 }
 
 static int zrow_fmt(const cmm_grid* g, int batch, const int* act, double R, int version, const cmm_wda_eos& we,
                     const double2* win, size_t fs, double2* gout, int nf, double* part, int nslot, int want,
-                    cudaStream_t st) {
+                    double* wd, cudaStream_t st) {
   const int chunk = zrow_chunk(g, nf);
   if (chunk < 1) return CMM_ERR_SMEM;
   switch (zrow_m3(g)) {
-    case 32: return zrow_fmt_m3<32>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
-    case 16: return zrow_fmt_m3<16>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
-    default: return zrow_fmt_m3<0>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, st);
+    case 32: return zrow_fmt_m3<32>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
+    case 16: return zrow_fmt_m3<16>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
+    default: return zrow_fmt_m3<0>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
   }
 }
 
@@ -1616,14 +1763,15 @@ static int col_fft_3d(const cmm_grid* g, int batch, const double2* in, double2* 
 }
 
 // Real fields -> yz-spectra (y and z forward) of every plane.
-static int plane_r2c(const cmm_grid* g, int batch, const double* in, double2* spec, cudaStream_t st) {
+static int plane_r2c(const cmm_grid* g, int batch, const double* in, double2* spec, cudaStream_t st,
+                     const int* act = nullptr) {
   if (plane_staged(g, 1)) {
-    int rc = zrow_op(g, batch, nullptr, OpR2C{in}, nullptr, spec, nullptr, 0, st);
+    int rc = zrow_op(g, batch, act, OpR2C{in}, nullptr, spec, nullptr, 0, st);
     if (rc) return rc;
-    return ypass(g, batch, nullptr, spec, spec, 0, 1, 0, st);
+    return ypass(g, batch, act, spec, spec, 0, 1, 0, st);
   }
   const size_t ps = plane_smem_bytes(g->n2, g->n3, 1);
-  LAUNCH_PLANE(plane_kind(g), k_plane_r2c, dim3(g->n1, batch), ps, st, g->dev, in, spec);
+  LAUNCH_PLANE(plane_kind(g), k_plane_r2c, dim3(g->n1, batch), ps, st, g->dev, act, in, spec);
   return last_err();
 }
 
@@ -1690,12 +1838,40 @@ extern "C" int cmm_fmt_weights(const cmm_grid* g, double R, double* d_wtab, void
   return last_err();
 }
 
+// Plane pass of the functional pipeline over nf weighted-density spectra
+// (wbuf, field stride fs): fused where the plane fits, else staged (y pass,
+// z rows with the pointwise step, y pass of the results).  want as
+// cmm_fmt_c1; dPhi spectra into gbuf when want & 1.
+static int fmt_plane_pass(const cmm_grid* g, int batch, const int* act, double R, int version,
+                          const cmm_wda_eos& we, double2* wbuf, double2* gbuf, size_t fs, int nf, double* part,
+                          int nslot, int want, double* wd, cudaStream_t st) {
+  const bool ten = (version & CMM_TENSOR) != 0, has_wda = (version & CMM_WDA) != 0;
+  const size_t fsr = (size_t)batch * g->n1 * g->n2 * g->n3;  // real field stride of wd
+  const size_t ps = plane_smem_bytes(g->n2, g->n3, nf);
+  if (!ten && !plane_staged(g, nf)) {  // fused plane pass
+    if (has_wda)
+      LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt_wda, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, act, R,
+                     version, we, (const double2*)wbuf, fs, gbuf, fs, part, nslot, want, wd, fsr);
+    else
+      LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, act, R,
+                     version, we, (const double2*)wbuf, fs, gbuf, fs, part, nslot, want, wd, fsr);
+    return last_err();
+  }
+  int rc = ypass(g, batch, act, wbuf, wbuf, fs, nf, 1, st);
+  if (rc) return rc;
+  rc = zrow_fmt(g, batch, act, R, version, we, wbuf, fs, gbuf, nf, part, nslot, want, wd, st);
+  if (rc) return rc;
+  if (want & 1) rc = ypass(g, batch, act, gbuf, gbuf, fs, nf, 0, st);
+  return rc;
+}
+
 extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, double R, double beta,
                           int version, const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab,
                           const double* d_rhohat, double* d_chat, double* d_work, double* d_part, int nslot,
-                          int want, void* stream) {
+                          int want, double* d_wd, void* stream) {
   if (!g || batch < 1 || !d_kst || !d_rhohat || !d_work || !d_part) return CMM_ERR_ARG;
   if ((want & 1) && !d_chat) return CMM_ERR_ARG;
+  if ((want & 8) && !d_wd) return CMM_ERR_ARG;
   const bool has_wda = (version & CMM_WDA) != 0;
   const bool ten = (version & CMM_TENSOR) != 0;
   if (has_wda && !wda) return CMM_ERR_ARG;
@@ -1715,7 +1891,7 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
   const double2* wt = (const double2*)d_wtab;
   const int ck = col_kind(g);
   if (version & CMM_NOHS) {  // MFA term alone: one column pass
-    if (!(want & 1)) return CMM_ERR_ARG;
+    if (!(want & 1) || (want & 8)) return CMM_ERR_ARG;
     LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), col_smem_bytes(g->n1, tc, 6, g->ax1.big), st, g->dev, d_active, R,
                1.0 / (beta * npts), (const double2*)nullptr, fs, (const double2*)d_rhohat, (const double2*)d_kst,
                wt, (double2*)d_chat, tc, 0.0, 1.0 / npts);
@@ -1723,30 +1899,15 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
   }
 #define LAUNCH_WEIGHTS(kern)                                                                             \
   LAUNCH_COL(ck, kern, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts, (const double2*)d_rhohat, \
-             wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0, tc, we.D)
+             wbuf, fs, (const double2*)d_kst, wt, d_part, nslot, (want & 2) ? 1 : 0, tc, we.D,             \
+             (const double2*)nullptr, (double*)nullptr)
   if (has_wda && ten) LAUNCH_WEIGHTS(k_col_weights_wda_t);
   else if (has_wda) LAUNCH_WEIGHTS(k_col_weights_wda);
   else if (ten) LAUNCH_WEIGHTS(k_col_weights_t);
   else LAUNCH_WEIGHTS(k_col_weights);
 #undef LAUNCH_WEIGHTS
-  const size_t ps = plane_smem_bytes(g->n2, g->n3, nf);
-  if (!ten && !plane_staged(g, nf)) {  // fused plane pass
-    if (has_wda)
-      LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt_wda, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev,
-                     d_active, R, version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
-    else
-      LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, d_active,
-                     R, version, we, (const double2*)wbuf, fs, gbuf, fs, d_part, nslot, want);
-  } else {  // staged: y pass, z rows with the pointwise step, y pass of the results
-    int rc = ypass(g, batch, d_active, wbuf, wbuf, fs, nf, 1, st);
-    if (rc) return rc;
-    rc = zrow_fmt(g, batch, d_active, R, version, we, wbuf, fs, gbuf, nf, d_part, nslot, want, st);
-    if (rc) return rc;
-    if (want & 1) {
-      rc = ypass(g, batch, d_active, gbuf, gbuf, fs, nf, 0, st);
-      if (rc) return rc;
-    }
-  }
+  int rc = fmt_plane_pass(g, batch, d_active, R, version, we, wbuf, gbuf, fs, nf, d_part, nslot, want, d_wd, st);
+  if (rc) return rc;
   if (want & 1) {
 #define LAUNCH_BACKCONV(kern)                                                                            \
   LAUNCH_COL(ck, kern, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),               \
@@ -1843,6 +2004,92 @@ extern "C" int cmm_mix_step(const cmm_grid* g, int batch, const int* d_active, c
   LAUNCH_PLANE(plane_kind(g), k_plane_mix, dim3(g->n1, batch), ps, (cudaStream_t)stream, g->dev, d_active, d_coef,
                fp, nfield, clip, thr, lambda3, d_ref, refstride, d_V, vstride, d_rho_out, (double2*)d_rhohat_out,
                d_part, nslot);
+  return last_err();
+}
+
+extern "C" int cmm_ls_prepare(const cmm_grid* g, int batch, const int* d_active, double R, int version,
+                              const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab, const double* d_r,
+                              const double* d_rhohat, const double* d_wd_rho, double* d_rhat, double* d_work,
+                              double* d_wd_r, double* d_ls_part, int nslot, void* stream) {
+  if (!g || batch < 1 || !d_kst || !d_r || !d_rhohat || !d_wd_rho || !d_rhat || !d_work || !d_wd_r || !d_ls_part)
+    return CMM_ERR_ARG;
+  if (version & CMM_NOHS) return CMM_ERR_ARG;
+  const bool has_wda = (version & CMM_WDA) != 0, ten = (version & CMM_TENSOR) != 0;
+  if (has_wda && !wda) return CMM_ERR_ARG;
+  cmm_wda_eos we;
+  memset(&we, 0, sizeof(we));
+  if (has_wda) we = *wda;
+  const int nw = (has_wda ? 6 : 5) + (ten ? 6 : 0);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t fs = (size_t)batch * g->n1 * g->n2 * g->h3;
+  const double npts = (double)g->n1 * g->n2 * g->n3;
+  const int tc = col_tile(g, nw + 1);
+  const int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
+  if (nslot < g->n1 || nslot < ntile) return CMM_ERR_WORKSPACE;
+  double2* rhat = (double2*)d_rhat;
+  int rc = plane_r2c(g, batch, d_r, rhat, st, d_active);  // yz-spectrum of r
+  if (rc) return rc;
+  double2* wbuf = (double2*)d_work;
+  const size_t csw = col_smem_bytes(g->n1, tc, nw + 1, g->ax1.big);
+  const double2* wt = (const double2*)d_wtab;
+  const int ck = col_kind(g);
+#define LAUNCH_WEIGHTS_LS(kern)                                                                          \
+  LAUNCH_COL(ck, kern, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts, (const double2*)rhat,   \
+             wbuf, fs, (const double2*)d_kst, wt, (double*)nullptr, nslot, 0, tc, we.D,                     \
+             (const double2*)d_rhohat, d_ls_part)
+  if (has_wda && ten) LAUNCH_WEIGHTS_LS(k_col_weights_ls_wda_t);
+  else if (has_wda) LAUNCH_WEIGHTS_LS(k_col_weights_ls_wda);
+  else if (ten) LAUNCH_WEIGHTS_LS(k_col_weights_ls_t);
+  else LAUNCH_WEIGHTS_LS(k_col_weights_ls);
+#undef LAUNCH_WEIGHTS_LS
+  // inverse y/z of the weighted densities of r, stored in real space
+  rc = fmt_plane_pass(g, batch, d_active, R, version, we, wbuf, wbuf, fs, nw, d_ls_part, nslot, 8, d_wd_r, st);
+  if (rc) return rc;
+  const size_t fsr = (size_t)batch * g->n1 * g->n2 * g->n3;
+  k_ls_n3max<<<dim3(g->n1, batch), 256, 0, st>>>(g->dev, d_active, d_wd_rho, d_wd_r, fsr, d_ls_part, nslot);
+  return last_err();
+}
+
+template <bool WDA, bool TEN>
+static int ls_omega_one(const cmm_grid* g, int batch, const int* act, const double* params, double c0, double c1,
+                        double c2, double R, double lambda3, int version, const cmm_wda_eos& we, const double* rho,
+                        const double* r, const double* V, long long vstride, const double* wd_rho,
+                        const double* wd_r, double* ls_part, int nslot, double* alpha, cudaStream_t st) {
+  const size_t fsr = (size_t)batch * g->n1 * g->n2 * g->n3;
+  k_ls_omega<WDA, TEN><<<dim3(g->n1, batch), CMM_ROW_THREADS, 0, st>>>(
+      g->dev, act, params, c0, c1, c2, R, lambda3, version, we, rho, r, V, vstride, wd_rho, wd_r, fsr, ls_part,
+      nslot, alpha);
+  return last_err();
+}
+
+extern "C" int cmm_ls_omega(const cmm_grid* g, int batch, const int* d_active, const double* d_params,
+                            double c0, double c1, double c2, double R, double lambda3, int version,
+                            const cmm_wda_eos* wda, const double* d_rho, const double* d_r, const double* d_V,
+                            long long vstride, const double* d_wd_rho, const double* d_wd_r, double* d_ls_part,
+                            int nslot, double* d_alpha, void* stream) {
+  if (!g || batch < 1 || !d_params || !d_rho || !d_r || !d_V || !d_wd_rho || !d_wd_r || !d_ls_part || !d_alpha)
+    return CMM_ERR_ARG;
+  if (nslot < g->n1) return CMM_ERR_WORKSPACE;
+  const bool has_wda = (version & CMM_WDA) != 0, ten = (version & CMM_TENSOR) != 0;
+  if (has_wda && !wda) return CMM_ERR_ARG;
+  cmm_wda_eos we;
+  memset(&we, 0, sizeof(we));
+  if (has_wda) we = *wda;
+  cudaStream_t st = (cudaStream_t)stream;
+#define LS_OMEGA(w, t)                                                                                     \
+  ls_omega_one<w, t>(g, batch, d_active, d_params, c0, c1, c2, R, lambda3, version, we, d_rho, d_r, d_V, vstride, \
+                     d_wd_rho, d_wd_r, d_ls_part, nslot, d_alpha, st)
+  if (has_wda && ten) return LS_OMEGA(true, true);
+  if (has_wda) return LS_OMEGA(true, false);
+  if (ten) return LS_OMEGA(false, true);
+  return LS_OMEGA(false, false);
+#undef LS_OMEGA
+}
+
+extern "C" int cmm_ls_finalize(int batch, const int* d_active, const double* d_ls_part, int nslot, double* d_ls,
+                               void* stream) {
+  if (batch < 1 || !d_ls_part || !d_ls || nslot < 1) return CMM_ERR_ARG;
+  k_ls_finalize<<<batch, dim3(32, CMM_NLS), 0, (cudaStream_t)stream>>>(d_active, d_ls_part, nslot, d_ls);
   return last_err();
 }
 

@@ -171,13 +171,39 @@ class Functional(object):
             self.wtab = torch.empty(plan.nspec * 2, dtype=torch.float64, device="cuda")
             check(L.lib().cmm_fmt_weights(plan.handle, self.R, ptr(self.wtab), _stream()), "cmm_fmt_weights")
 
-    def c1(self, buf, rhohat, chat, want=1, active=None, batch=None):
-        """yz-spectrum of C1 - V (HardSphere.derive + MFA.derive) for every instance."""
+    @property
+    def nwd(self):
+        """Number of weighted-density fields (n0, n3, nv2 x/y/z, WDA, tensor)."""
+        return 5 + (1 if self.version & L.WDA else 0) + (6 if self.version & L.TENSOR else 0)
+
+    def c1(self, buf, rhohat, chat, want=1, active=None, batch=None, wd=None):
+        """yz-spectrum of C1 - V (HardSphere.derive + MFA.derive) for every instance;
+        want bit 3 also stores the weighted densities into ``wd`` [nwd, B, N1, N2, N3]."""
         B = buf.batch if batch is None else batch
         wda = ctypes.byref(self.wda) if self.wda is not None else None
         check(L.lib().cmm_fmt_c1(self.plan.handle, B, ptr(active), self.R, self.beta, self.version, wda,
                                  ptr(self.kst), ptr(self.wtab), ptr(rhohat), ptr(chat), ptr(buf.work),
-                                 ptr(buf.part), buf.nslot, int(want), _stream()), "cmm_fmt_c1")
+                                 ptr(buf.part), buf.nslot, int(want), ptr(wd), _stream()), "cmm_fmt_c1")
+
+    # ---- hybrid line search (Picard.update_rho_hybrid without trial transforms)
+    def ls_prepare(self, buf, r, rhohat, wd_rho, rhat, wd_r, ls_part, active=None):
+        wda = ctypes.byref(self.wda) if self.wda is not None else None
+        check(L.lib().cmm_ls_prepare(self.plan.handle, buf.batch, ptr(active), self.R, self.version, wda,
+                                     ptr(self.kst), ptr(self.wtab), ptr(r), ptr(rhohat), ptr(wd_rho), ptr(rhat),
+                                     ptr(buf.work), ptr(wd_r), ptr(ls_part), buf.nslot, _stream()),
+              "cmm_ls_prepare")
+
+    def ls_omega(self, buf, params, coefs, rho, r, wd_rho, wd_r, ls_part, alpha, active=None, vstride=0):
+        wda = ctypes.byref(self.wda) if self.wda is not None else None
+        c0, c1, c2 = [float(c) for c in coefs]
+        check(L.lib().cmm_ls_omega(self.plan.handle, buf.batch, ptr(active), ptr(params), c0, c1, c2, self.R,
+                                   self.lambda3, self.version, wda, ptr(rho), ptr(r), ptr(self.V), int(vstride),
+                                   ptr(wd_rho), ptr(wd_r), ptr(ls_part), buf.nslot, ptr(alpha), _stream()),
+              "cmm_ls_omega")
+
+    def ls_finalize(self, buf, ls_part, ls, active=None):
+        check(L.lib().cmm_ls_finalize(buf.batch, ptr(active), ptr(ls_part), buf.nslot, ptr(ls), _stream()),
+              "cmm_ls_finalize")
 
 
 def mfa_kernel_spectrum(plan, sigma, epsilon, cutoff, rmin=None, limit=0.0, rep=1):

@@ -60,6 +60,20 @@ enum {
 };
 #define CMM_MAX_HIST 8
 
+/* Sums of the hybrid line search (cmm_ls_*), per instance [CMM_NLS]; the
+ * trial densities are rho + alpha_i r, alpha_i = coef_i * alpha_max. */
+enum {
+  CMM_LS_MFA_RR = 0,    /* sum_k wt |r_k|^2 Re K (as CMM_STAT_MFA, for r)        */
+  CMM_LS_MFA_XR = 1,    /* sum_k wt Re(conj(rho_k) r_k) Re K                      */
+  CMM_LS_N3MAX_G = 2,   /* max over the grid of n3(rho) + n3(r) (= max n3 of G)   */
+  CMM_LS_SUM_R = 3,     /* sum r                                                  */
+  CMM_LS_SUM_RV = 4,    /* sum r V                                                */
+  CMM_LS_FID = 5,       /* 5..7:  sum x (ln(L^3 x) - 1), x = rho + alpha_i r clipped as _clip_density */
+  CMM_LS_PHI = 8,       /* 8..10: sum Phi(n(rho) + alpha_i n(r))                  */
+  CMM_LS_WDA = 11,      /* 11..13: sum f_EOS(wd(rho) + alpha_i wd(r))             */
+  CMM_NLS = 16
+};
+
 /* Hard-sphere functional versions (cmmdft/functionals.py:373-377): a base
  * (FMT, MFMT, WBII) with the 'a' (CMM_ANTISYM) and 't' (CMM_TENSOR, the six
  * tensor weighted densities of functionals.py:457-487, 534-552) options.
@@ -169,7 +183,10 @@ int cmm_mfa_kernel(const cmm_grid* grid, double sigma, double epsilon, double cu
  * writing d_chat = yz-spectrum of C1 - V (HardSphere.derive + MFA.derive,
  * cmmdft/functionals.py:489-609, 912-926).  d_wtab: weight table from
  * cmm_fmt_weights for this grid and R, or NULL.  want: bit 0 = C1 spectrum,
- * bit 1 = free-energy sums (PHI, MFA), bit 2 = n3 maximum.
+ * bit 1 = free-energy sums (PHI, MFA), bit 2 = n3 maximum, bit 3 = the
+ * weighted densities themselves into d_wd (real fields [nf][batch][N1][N2][N3],
+ * nf = 5, +1 with CMM_WDA, +6 with CMM_TENSOR; n0, n3, nv2 x/y/z, WDA, tensor
+ * xx, xy, xz, yy, yz, zz), the input of the cmm_ls_* line search.
  * wda: WDA part (with version | CMM_WDA), else NULL; it adds one weighted
  * density and one back-convolution field.  CMM_TENSOR adds the six tensor
  * weighted densities and their back-convolution.
@@ -178,7 +195,7 @@ int cmm_mfa_kernel(const cmm_grid* grid, double sigma, double epsilon, double cu
 int cmm_fmt_c1(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,
                int version, const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab,
                const double* d_rhohat, double* d_chat, double* d_work, double* d_part, int nslot,
-               int want, void* stream);
+               int want, double* d_wd, void* stream);
 
 /* Table of the scalar FMT weights (kw0, kw3 of _init_weight_functions,
  * cmmdft/functionals.py:421-455) in the column-pass layout: double2
@@ -231,6 +248,37 @@ int cmm_mix_step(const cmm_grid* grid, int batch, const int* d_active, const dou
  * CMM_STAT_N3MAX, sums otherwise). */
 int cmm_stats_finalize(int batch, const int* d_active, const double* d_part, int nslot,
                        unsigned mask, double* d_stats, void* stream);
+
+/* Hybrid Picard line search (Picard.update_rho_hybrid and _get_alpha_max,
+ * cmmdft/solver.py:150-165, 403-433) without transforms of the trial
+ * densities: weighted densities are linear in the density, so Omega(rho +
+ * alpha r) follows from the weighted densities of rho (cmm_fmt_c1, want bit
+ * 3) and of r pointwise; the MFA energy is quadratic and N, F_ext linear in
+ * alpha.  d_ls_part: [batch][CMM_NLS][nslot] partial sums, initialised once
+ * by the caller (0, and -inf in the CMM_LS_N3MAX_G slots); every call
+ * rewrites the same slots.
+ *
+ * cmm_ls_prepare: the weighted densities of the residuals d_r (real fields)
+ * into d_wd_r, the MFA sums of r against the yz-spectra d_rhohat of rho, and
+ * max (n3(rho) + n3(r)) with the n3 field of d_wd_rho.  d_rhat: scratch of
+ * one yz-spectrum per instance; d_work as cmm_fmt_c1. */
+int cmm_ls_prepare(const cmm_grid* grid, int batch, const int* d_active, double R, int version,
+                   const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab, const double* d_r,
+                   const double* d_rhohat, const double* d_wd_rho, double* d_rhat, double* d_work,
+                   double* d_wd_r, double* d_ls_part, int nslot, void* stream);
+/* cmm_ls_omega: alpha_max = min(|(1 - a) / ((g - a) + 1e-16)|, 1) per
+ * instance (a = d_params[b][3], the max n3 of rho; g = CMM_LS_N3MAX_G),
+ * written to d_alpha[b]; then the pointwise sums of CMM_LS_SUM_R .. WDA at
+ * alpha_i = coef[i] * alpha_max, i < 3. */
+int cmm_ls_omega(const cmm_grid* grid, int batch, const int* d_active, const double* d_params,
+                 double c0, double c1, double c2, double R, double lambda3, int version,
+                 const cmm_wda_eos* wda, const double* d_rho, const double* d_r, const double* d_V,
+                 long long vstride, const double* d_wd_rho, const double* d_wd_r, double* d_ls_part,
+                 int nslot, double* d_alpha, void* stream);
+/* Reduce d_ls_part over slots into d_ls [batch][CMM_NLS] (max for
+ * CMM_LS_N3MAX_G, sums otherwise). */
+int cmm_ls_finalize(int batch, const int* d_active, const double* d_ls_part, int nslot, double* d_ls,
+                    void* stream);
 
 /* Allocation-free variant of cmm_fmt_c1 (no counterpart in the reference,
  * which allocates freely in numpy).  For callers that cannot allocate device

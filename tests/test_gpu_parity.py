@@ -313,3 +313,50 @@ def test_isotherm_64_matches_reference(golden64, cuda):
         assert scalar_rel(s.omega0[i], golden64["omega"][i]) < 1e-10
     i1 = int(np.where(P == 1.0)[0][0])
     assert relerr(rho[i1].cpu().numpy(), golden64["rho_1bar"]) < 1e-9
+
+
+@pytest.mark.parametrize("case", ["wbii64", "atwbii_wda32"])
+def test_line_search_matches_pipeline(cuda, case):
+    """Omega(rho + alpha r) and alpha_max of the hybrid step from the stored
+    weighted densities (cmm_ls_*) against full evaluations of the trial
+    densities through the functional pipeline."""
+    host = cubic_host_276(0)
+    guest = methane_guest_params()
+    if case == "wbii64":
+        fn = W.build_functional(host, (64, 64, 64), 300.0, guest)
+    else:
+        fn = W.build_functional(host, (32, 32, 32), 300.0, guest, version='atWBII', wda=True)
+    P = np.array([1e-3, 1.0, 10.0]) * bar
+    mus, bulks = W.isotherm_inputs(P, 300.0, guest)
+    r0 = W.initial_density(fn, mus, ninit=bulks)
+    s = BT.BatchSolve(fn, mus, method='hybridanderson', nsteps=10, threshold=1e-8, criterion='res')
+    s.initial_density(r0)
+    s.cf = np.ones(3)
+    s._set_params()
+    live = np.ones(3, dtype=bool)
+    s._init_state(live)
+    s._set_active(live)
+    s._residual(s.chat, s.ring[0], s.rres[0], [])
+    s._stats()
+    # line search sums
+    s._set_active(live)
+    s._set_params(n3=s.n3max)
+    fn.ls_prepare(s.buf, s.rres[0], s.spec_ring[0], s.wd_ring[0], s.rhat, s.wd_r, s.ls_part, active=s.active)
+    coefs = (0.45, 0.9, 0.225)
+    fn.ls_omega(s.buf, s.params, coefs, s.ring[0], s.rres[0], s.wd_ring[0], s.wd_r, s.ls_part, s.ls_alpha,
+                active=s.active)
+    fn.ls_finalize(s.buf, s.ls_part, s.ls, active=s.active)
+    ls = s.ls.cpu().numpy()
+    amax = s.ls_alpha.cpu().numpy()
+    # alpha_max from a pipeline evaluation of G = rho + r (solver.py:150-165)
+    stn = s._eval_density(live, np.ones((3, 2)), [s.ring[0], s.rres[0]], L.CLIP_NONE, s.trial, 4, s.ring[0])
+    for b in range(3):
+        a, g = s.n3max[b], stn[b, L.STAT_N3MAX]
+        ref = np.min([abs((1 - a) / ((g - a) + 1e-16)), 1])
+        assert scalar_rel(amax[b], ref) < 1e-12
+        assert scalar_rel(ls[b, L.LS_N3MAX_G], g) < 1e-12
+    for i, c in enumerate(coefs):
+        om_pipe = s._trial_omega(live, c * amax, 0)
+        for b in range(3):
+            om_ls = s._ls_omega(ls[b], b, i, c * amax[b])
+            assert scalar_rel(om_ls, om_pipe[b]) < 1e-12, (case, i, b, om_ls, om_pipe[b])
