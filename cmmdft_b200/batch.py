@@ -141,6 +141,18 @@ def _grid_full(cf, hi, n):
     return al[rows, j], om[rows, j], np.max(om, axis=1)
 
 
+def parabola3(x1, x2, y0, y1, y2):
+    """Coefficients [c2, c1, c0] (np.polyfit order) of the parabola through
+    (0, y0), (x1, y1), (x2, y2), per row: the fit of np.polyfit([0, x1, x2],
+    [y0, y1, y2], 2) (solver.py:425), in closed form for all rows at once."""
+    with np.errstate(all='ignore'):
+        d1 = (y1 - y0) / x1
+        d2 = (y2 - y0) / x2
+        c2 = (d2 - d1) / (x2 - x1)
+        c1 = d1 - c2 * x1
+    return np.stack([c2, c1, np.asarray(y0, dtype=float)], axis=1)
+
+
 def grid_parabola(cf, hi, n=10000):
     """First grid point minimising om = c a^2 + b a + a0 on
     np.linspace(-hi/4, hi, n) per row, and the min/max of om on that grid
@@ -374,6 +386,19 @@ class BatchSolve(object):
             G += st[L.STAT_WDA] * dr
         return G
 
+    def _omega_rows(self, st, idx):
+        """_omega for the instances idx (rows st[idx]), elementwise in the same order."""
+        beta, dr = self.fn.beta, self.dr
+        s = st[idx]
+        N = s[:, L.STAT_N] * dr
+        G = (s[:, L.STAT_FID] * dr) / beta - self.mu[idx] * N
+        G += (s[:, L.STAT_PHI] * dr) / beta
+        G += 0.5 * (s[:, L.STAT_MFA] * dr)
+        G += s[:, L.STAT_FEXT] * dr
+        if self.fn.wda is not None:
+            G += s[:, L.STAT_WDA] * dr
+        return G
+
     def _omega_parts(self, st):
         beta, dr = self.fn.beta, self.dr
         out = dict(N=st[L.STAT_N] * dr, Fid=(st[L.STAT_FID] * dr) / beta,
@@ -527,6 +552,17 @@ class BatchSolve(object):
         best = np.nanmin(r)
         return bool(r[-1] > 1e6 * best and np.all(np.diff(r[-6:]) >= 0))
 
+    def _diverging_rows(self, idx, k):
+        """_diverging for the instances idx at step k from the RES history array."""
+        if not self.divergence_guard or k < 8:
+            return np.zeros(len(idx), dtype=bool)
+        r = self.res_hist[idx, 1:k + 1]
+        last = r[:, -1]
+        with np.errstate(invalid='ignore'):
+            best = np.nanmin(r, axis=1)
+            rising = np.all(np.diff(r[:, -6:], axis=1) >= 0, axis=1)
+        return ~np.isfinite(last) | ((last > 1e6 * best) & rising)
+
     def _converged(self, b, N, res, iue, der=np.nan):
         ok = True
         riue = iue / N if N > 0 else np.nan
@@ -562,6 +598,7 @@ class BatchSolve(object):
         self.And_true = np.zeros(B, dtype=bool)
         self.it_eps0 = np.full(B, np.nan)
         self.damping = np.full(B, self.damping0)
+        self.res_hist = np.full((B, self.nsteps + 2), np.nan)
         # r_0 for the initial density
         self._set_active(live)
         self._residual(self.chat, self.ring[0], self.rres[0], [])
@@ -599,26 +636,44 @@ class BatchSolve(object):
                     for b in np.where(hyb)[0]:
                         self.trace[b].append((k, 'H', float(self.omega0[b])))
             # --- after the update: non-finite check, N, convergence (solver.py:286-305)
-            for b in np.where(live)[0]:
-                self.steps[b] = k
-                st_b = self.last_stats[b]
-                if st_b[L.STAT_NONFIN] > 0:
-                    retry[b] = True
-                    live[b] = False
-                    continue
-                N = st_b[L.STAT_N] * self.dr
-                res = np.sqrt(self.rnorm2[b, s_new]) / np.sqrt(N) / np.sqrt(self.npts)
-                iue = st_b[L.STAT_IUE] * self.dr
-                der = np.sqrt(st_b[L.STAT_DER]) / np.sqrt(self.npts)
-                self.Ncur[b] = N
-                if self._converged(b, N, res, iue, der):
-                    self._finish(b, self.ring[s_new, b], N, k, True)
-                    live[b] = False
-                elif k >= self.nsteps or self._diverging(b):
+            idx = np.where(live)[0]
+            self.steps[idx] = k
+            st = self.last_stats[idx]
+            bad = st[:, L.STAT_NONFIN] > 0
+            retry[idx[bad]] = True
+            live[idx[bad]] = False
+            idx, st = idx[~bad], st[~bad]
+            if idx.size == 0:
+                continue
+            with np.errstate(invalid='ignore', divide='ignore'):
+                N = st[:, L.STAT_N] * self.dr
+                res = np.sqrt(self.rnorm2[idx, s_new]) / np.sqrt(N) / np.sqrt(self.npts)
+                iue = st[:, L.STAT_IUE] * self.dr
+                der = np.sqrt(st[:, L.STAT_DER]) / np.sqrt(self.npts)
+            self.Ncur[idx] = N
+            conv = self._converged_rows(idx, N, res, iue, der)
+            self.res_hist[idx, k] = res
+            done = conv | (k >= self.nsteps) | self._diverging_rows(idx, k)
+            for j in np.where(done)[0]:
+                b = idx[j]
+                if not conv[j]:
                     self.diverged[b] = k < self.nsteps
-                    self._finish(b, self.ring[s_new, b], N, k, False)
-                    live[b] = False
+                self._finish(b, self.ring[s_new, b], N[j], k, bool(conv[j]))
+                live[b] = False
         return retry
+
+    def _converged_rows(self, idx, N, res, iue, der):
+        """_converged for the instances idx (arrays), with their history entries."""
+        with np.errstate(invalid='ignore', divide='ignore'):
+            riue = np.where(N > 0, iue / N, np.nan)
+        ok = np.ones(len(idx), dtype=bool)
+        for c, t in zip(self.criteria, self.thresholds):
+            v = res if c == 'res' else (riue if c == 'riue' else der)
+            ok &= (v < t)
+        for j, b in enumerate(idx):
+            self.history[b].append((N[j], res[j], riue[j]))
+        ok |= (iue == 0) & np.isnan(riue)
+        return ok
 
     def _valid_hist(self, k_new, s_new):
         """Slots of residuals r_{k_new-m+1} .. r_{k_new-1} (excluding s_new)."""
@@ -635,15 +690,17 @@ class BatchSolve(object):
         return st, hist_slots
 
     def _commit_residual(self, mask, st, k, s_new, hist_slots):
-        for b in np.where(mask)[0]:
-            self.rnorm2[b, s_new] = st[b, L.STAT_RES2]
-            self.gram[b, s_new, s_new] = st[b, L.STAT_RES2]
-            for h, j in enumerate(hist_slots):
-                g = st[b, L.STAT_GRAM0 + h]
-                self.gram[b, s_new, j] = g
-                self.gram[b, j, s_new] = g
-            self.n3max[b] = st[b, L.STAT_N3MAX]
-            self.last_stats[b] = st[b]
+        idx = np.where(mask)[0]
+        if idx.size == 0:
+            return
+        self.rnorm2[idx, s_new] = st[idx, L.STAT_RES2]
+        self.gram[idx, s_new, s_new] = st[idx, L.STAT_RES2]
+        for h, j in enumerate(hist_slots):
+            g = st[idx, L.STAT_GRAM0 + h]
+            self.gram[idx, s_new, j] = g
+            self.gram[idx, j, s_new] = g
+        self.n3max[idx] = st[idx, L.STAT_N3MAX]
+        self.last_stats[idx] = st[idx]
 
     def _anderson_candidate(self, mask, k, s_prev, s_new):
         """Anderson.update_rho_Anderson + the acceptance tests; returns accepted mask."""
@@ -653,33 +710,27 @@ class BatchSolve(object):
         coefs = np.zeros((B, 2 * mk))
         idx = np.where(mask)[0]
         alphas = simplex_qp_batched(self.gram[idx][:, slots][:, :, slots])
-        for ii, b in enumerate(idx):
-            al = alphas[ii]
-            if self.adaptive:  # _get_damping_coefficient (solver.py:537-544)
-                r = np.sqrt(self.rnorm2[b, s_prev])
-                p = np.sqrt(self.rnorm2[b, (k - 2) % m]) if k >= 2 else 0.0
-                if r < p:
-                    self.damping[b] = min(self.damping[b] * self.dfac[0], self.damping_max)
-                else:
-                    self.damping[b] = max(self.damping[b] * self.dfac[1], self.damping_min)
-            d = self.cf[b] * self.damping[b]
-            coefs[b, :mk] = al
-            coefs[b, mk:] = d * al
+        if self.adaptive:  # _get_damping_coefficient (solver.py:537-544)
+            r = np.sqrt(self.rnorm2[idx, s_prev])
+            p = np.sqrt(self.rnorm2[idx, (k - 2) % m]) if k >= 2 else np.zeros(len(idx))
+            dm = self.damping[idx]
+            self.damping[idx] = np.where(r < p, np.minimum(dm * self.dfac[0], self.damping_max),
+                                         np.maximum(dm * self.dfac[1], self.damping_min))
+        d = self.cf[idx] * self.damping[idx]
+        coefs[idx, :mk] = alphas
+        coefs[idx, mk:] = d[:, None] * alphas
         fields = [self.ring[j] for j in slots] + [self.rres[j] for j in slots]
         self._set_active(mask)
         self._mix(coefs, fields, L.CLIP_DENSITY, self.ring[s_prev], self.ring[s_new], spec_out=self.spec_ring[s_new])
         st, hist_slots = self._post_update(mask, k, s_new, None)
         ok = np.zeros(B, dtype=bool)
-        for b in np.where(mask)[0]:
-            if st[b, L.STAT_GNONFIN] > 0:
-                continue
-            om = self._omega(st[b], b)
-            prev = self.omega0[b]
-            self.omega0[b] = om  # _get_Omega stores omega0 even when rejected
-            self.omega_evals += 1
-            if om > prev * 0.8:
-                continue
-            ok[b] = True
+        cand = idx[~(st[idx, L.STAT_GNONFIN] > 0)]
+        if cand.size:
+            om = self._omega_rows(st, cand)
+            prev = self.omega0[cand].copy()
+            self.omega0[cand] = om  # _get_Omega stores omega0 even when rejected
+            self.omega_evals += len(cand)
+            ok[cand[~(om > prev * 0.8)]] = True
         self._commit_residual(ok, st, k, s_new, hist_slots)
         return ok
 
@@ -706,6 +757,22 @@ class BatchSolve(object):
         G += (st[L.STAT_FEXT] + alpha * ls_b[L.LS_SUM_RV]) * dr
         if self.fn.wda is not None:
             G += ls_b[L.LS_WDA + i] * dr
+        return G
+
+    def _ls_omega_rows(self, ls, idx, i, alpha):
+        """_ls_omega for the instances idx; i (scalar or per-row) selects the trial alpha."""
+        beta, dr = self.fn.beta, self.dr
+        st = self.last_stats[idx]
+        lb = ls[idx]
+        rows = np.arange(len(idx))
+        i = np.broadcast_to(np.asarray(i), rows.shape)
+        N = (st[:, L.STAT_N] + alpha * lb[:, L.LS_SUM_R]) * dr
+        G = (lb[rows, L.LS_FID + i] * dr) / beta - self.mu[idx] * N
+        G += (lb[rows, L.LS_PHI + i] * dr) / beta
+        G += 0.5 * ((st[:, L.STAT_MFA] + 2 * alpha * lb[:, L.LS_MFA_XR] + alpha * alpha * lb[:, L.LS_MFA_RR]) * dr)
+        G += (st[:, L.STAT_FEXT] + alpha * lb[:, L.LS_SUM_RV]) * dr
+        if self.fn.wda is not None:
+            G += lb[rows, L.LS_WDA + i] * dr
         return G
 
     def _hybrid_step(self, mask, k, s_prev, s_new):
@@ -735,44 +802,37 @@ class BatchSolve(object):
         need = mask & ~np.isclose(amax, 0)
         if need.any():
             idx = np.where(need)[0]
-            a1 = 0.45 * amax
-            o1 = np.full(B, np.nan)
-            o2 = np.full(B, np.nan)
-            a2 = np.zeros(B)
-            for b in idx:
-                o1[b] = self._ls_omega(ls[b], b, 0, a1[b])
-                if o1[b] <= prev[b]:
-                    a2[b] = 0.9 * amax[b]
-                    o2[b] = self._ls_omega(ls[b], b, 1, a2[b])
-                else:
-                    a2[b] = 0.225 * amax[b]
-                    o2[b] = self._ls_omega(ls[b], b, 2, a2[b])
+            a1 = 0.45 * amax[idx]
+            o1 = self._ls_omega_rows(ls, idx, 0, a1)
+            first = o1 <= prev[idx]
+            a2 = np.where(first, 0.9 * amax[idx], 0.225 * amax[idx])
+            o2 = self._ls_omega_rows(ls, idx, np.where(first, 1, 2), a2)
             self.omega_evals += 2 * len(idx)
-            cf = np.array([np.polyfit([0, a1[b], a2[b]], [prev[b], o1[b], o2[b]], 2) for b in idx])
-            hi = np.maximum(a1[idx], a2[idx])
+            cf = parabola3(a1, a2, prev[idx], o1, o2)
+            hi = np.maximum(a1, a2)
             aopt[idx], mn[idx], mx[idx] = grid_parabola(cf, hi)
             mn[idx] /= kjmol
             mx[idx] /= kjmol
-            self.omega0 = np.where(need, o2, self.omega0)
-        for b in np.where(mask)[0]:
-            if aopt[b] <= 0:
-                if mx[b] - mn[b] > self.thresh:
-                    one = np.zeros(B, dtype=bool)
-                    one[b] = True
+            self.omega0[idx] = o2
+        midx = np.where(mask)[0]
+        neg = aopt[midx] <= 0
+        spread = (mx[midx] - mn[midx]) > self.thresh
+        aopt[midx[neg & ~spread]] = self.alpha_mix * amax[midx[neg & ~spread]]
+        for b in midx[neg & spread]:  # SLSQP on full evaluations of the trial density (rare)
+            one = np.zeros(B, dtype=bool)
+            one[b] = True
 
-                    def fun(alpha, b=b, one=one):
-                        al = np.zeros(B)
-                        al[b] = float(np.asarray(alpha).ravel()[0])
-                        o = self._trial_omega(one, al, s_prev)[b]
-                        self.omega0[b] = o
-                        return o
-                    bnd = opt.Bounds(0.01 * amax[b], 0.9 * amax[b])
-                    aopt[b] = float(opt.minimize(fun, [self.alpha_mix * amax[b]], bounds=bnd, method='SLSQP',
-                                                 options={'ftol': 1e-8}).x[0])
-                else:
-                    aopt[b] = self.alpha_mix * amax[b]
-            if aopt[b] <= 0 or np.isclose(aopt[b], 0):
-                aopt[b] = self.alpha_mix * amax[b]
+            def fun(alpha, b=b, one=one):
+                al = np.zeros(B)
+                al[b] = float(np.asarray(alpha).ravel()[0])
+                o = self._trial_omega(one, al, s_prev)[b]
+                self.omega0[b] = o
+                return o
+            bnd = opt.Bounds(0.01 * amax[b], 0.9 * amax[b])
+            aopt[b] = float(opt.minimize(fun, [self.alpha_mix * amax[b]], bounds=bnd, method='SLSQP',
+                                         options={'ftol': 1e-8}).x[0])
+        small = (aopt[midx] <= 0) | np.isclose(aopt[midx], 0)
+        aopt[midx[small]] = self.alpha_mix * amax[midx[small]]
         coefs = np.zeros((B, 2))
         coefs[:, 0] = 1.0
         coefs[:, 1] = aopt * self.cf
@@ -780,9 +840,8 @@ class BatchSolve(object):
         self._mix(coefs, [self.ring[s_prev], self.rres[s_prev]], L.CLIP_DENSITY, self.ring[s_prev],
                   self.ring[s_new], spec_out=self.spec_ring[s_new])
         st, hist_slots = self._post_update(mask, k, s_new, None)
-        for b in np.where(mask)[0]:
-            self.omega0[b] = self._omega(st[b], b)
-            self.omega_evals += 1
+        self.omega0[midx] = self._omega_rows(st, midx)
+        self.omega_evals += len(midx)
         self._commit_residual(mask, st, k, s_new, hist_slots)
 
     def n3max_of_current(self, b):

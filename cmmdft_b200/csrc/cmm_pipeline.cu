@@ -689,6 +689,72 @@ __device__ __forceinline__ void phi_funcs(double n3, double ln, double n32, doub
   }
 }
 
+// Prefactor of phi3 (functionals.py:629-639): n2^3 (1 - xi)^3 ('a') or
+// n2^3 - 3 n2 |nv2|^2, plus the tensor terms 9/2 (nv2 T nv2 - tr T^3) ('t').
+template <bool TEN>
+__device__ __forceinline__ double fmt_pref3(double n2, double vx, double vy, double vz, double vv, const double* T,
+                                            bool anti, double& xi) {
+  double pref3;
+  xi = 0.0;
+  if (anti) {
+    xi = vv / (n2 * n2 + 1e-16);
+    xi = fmin(fmax(xi, 0.0), 1.0);
+    const double om = 1 - xi;
+    pref3 = (n2 * n2 * n2) * (om * om * om);
+  } else {
+    pref3 = n2 * n2 * n2 - 3.0 * n2 * vv;
+  }
+  if constexpr (TEN) {
+    const double xx = T[0], xy = T[1], xz = T[2], yy = T[3], yz = T[4], zz = T[5];
+    const double quad = xx * (vx * vx) + yy * (vy * vy) + zz * (vz * vz) + 2 * xy * vx * vy + 2 * xz * vx * vz +
+                        2 * yz * vy * vz;
+    const double tr3 = (xx * xx * xx + yy * yy * yy + zz * zz * zz) +
+                       3 * (xx * xy * xy + xx * xz * xz + yy * xy * xy + yy * yz * yz + zz * xz * xz + zz * yz * yz) +
+                       6 * xy * xz * yz;
+    pref3 += 4.5 * quad;
+    pref3 -= 4.5 * tr3;
+  }
+  return pref3;
+}
+
+// phi2 and phi3 alone (the values of phi_funcs).
+__device__ __forceinline__ void phi_values(double n3, double ln, double n32, double n33, int base, double& p2,
+                                           double& p3) {
+  const double q = (1 - 2 * n3 + n32);
+  if (base == CMM_FMT) {
+    p2 = 1 / (1.0 - n3);
+    p3 = 1 / (24 * M_PI * q);
+  } else if (base == CMM_MFMT) {
+    p2 = 1 / (1.0 - n3);
+    p3 = (n3 <= 1e-8) ? (1.0 - 2 * n3 / 9 - n32 / 18) / (24 * M_PI * q) : (n3 + q * ln) / (36 * M_PI * n32 * q);
+  } else if (n3 <= 1e-8) {
+    p2 = (1 + n32 / 9) / (1 - n3);
+    p3 = (1 - 4 * n3 / 9 + n32 / 18) / (24 * M_PI * q);
+  } else {
+    p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) / (3 * (n3 - n32));
+    p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) / ((3 * n32) * 24 * M_PI * q);
+  }
+}
+
+// Phi alone at one point (get_phi, functionals.py:620-641).
+template <bool TEN>
+__device__ __forceinline__ double fmt_phi(double n0, double n3raw, double vx, double vy, double vz, const double* T,
+                                          double R, int version) {
+  const double n1 = R * n0;
+  const double n2 = (4.0 * M_PI * R * R) * n0;
+  const double i4r = 1.0 / (4 * M_PI * R);
+  const double n3 = fmin(fmax(n3raw, 1e-30), 0.99);
+  const double ln = log(1 - n3);
+  const double n32 = n3 * n3, n33 = n32 * n3;
+  double p2, p3, xi;
+  phi_values(n3, ln, n32, n33, version & 3, p2, p3);
+  const double vv = vx * vx + vy * vy + vz * vz;
+  const double uv = (vx * i4r) * vx + (vy * i4r) * vy + (vz * i4r) * vz;
+  const double pref3 = fmt_pref3<TEN>(n2, vx, vy, vz, vv, T, (version & CMM_ANTISYM) != 0, xi);
+  const double s12 = n1 * n2 - uv;
+  return n0 * (-ln) + s12 * p2 + pref3 * p3;
+}
+
 // With TEN, T holds the tensor densities (xx, xy, xz, yy, yz, zz) and gT
 // receives dPhi/dn_T (functionals.py:634-639, 669-674, 692-717).
 template <bool TEN>
@@ -708,25 +774,8 @@ __device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, 
   const double p1 = -ln, dp1 = 1.0 / (1.0 - n3);
   const double vv = vx * vx + vy * vy + vz * vz;
   const double uv = ux * vx + uy * vy + uz * vz;
-  double xi = 0.0, pref3;
-  if (anti) {
-    xi = vv / (n2 * n2 + 1e-16);
-    xi = fmin(fmax(xi, 0.0), 1.0);
-    const double om = 1 - xi;
-    pref3 = (n2 * n2 * n2) * (om * om * om);
-  } else {
-    pref3 = n2 * n2 * n2 - 3.0 * n2 * vv;
-  }
-  if constexpr (TEN) {
-    const double xx = T[0], xy = T[1], xz = T[2], yy = T[3], yz = T[4], zz = T[5];
-    const double quad = xx * (vx * vx) + yy * (vy * vy) + zz * (vz * vz) + 2 * xy * vx * vy + 2 * xz * vx * vz +
-                        2 * yz * vy * vz;
-    const double tr3 = (xx * xx * xx + yy * yy * yy + zz * zz * zz) +
-                       3 * (xx * xy * xy + xx * xz * xz + yy * xy * xy + yy * yz * yz + zz * xz * xz + zz * yz * yz) +
-                       6 * xy * xz * yz;
-    pref3 += 4.5 * quad;
-    pref3 -= 4.5 * tr3;
-  }
+  double xi;
+  const double pref3 = fmt_pref3<TEN>(n2, vx, vy, vz, vv, T, anti, xi);
   const double s12 = n1 * n2 - uv;
   PhiOut o;
   o.phi = n0 * p1 + s12 * p2 + pref3 * p3;
@@ -1498,8 +1547,7 @@ k_ls_omega(GridDev g, const int* __restrict__ active, const double* __restrict__
       double n[nf];
 #pragma unroll
       for (int f = 0; f < nf; ++f) n[f] = n0[f] + al[k] * n1[f];
-      double gT[6];
-      phi[k] += fmt_point<TEN>(n[0], n[1], n[2], n[3], n[4], TEN ? n + tb : nullptr, gT, R, version).phi;
+      phi[k] += fmt_phi<TEN>(n[0], n[1], n[2], n[3], n[4], TEN ? n + tb : nullptr, R, version);
       if constexpr (WDA) {
         double fv, dfv;
         wda_eos(wda, n[5], fv, dfv);
