@@ -60,7 +60,7 @@ _SIGS = {
                     c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_int, c_void_p, c_void_p], c_int),
     "cmm_ls_prepare": ([c_void_p, c_int, c_void_p, c_double, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
                         c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p], c_int),
-    "cmm_ls_omega": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_double, c_double,
+    "cmm_ls_omega": ([c_void_p, c_int, c_void_p, c_void_p, c_ll, c_double, c_double, c_double, c_double, c_double,
                       c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int,
                       c_void_p, c_void_p], c_int),
     "cmm_ls_finalize": ([c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p], c_int),

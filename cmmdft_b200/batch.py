@@ -196,11 +196,12 @@ def grid_parabola(cf, hi, n=10000):
     return aopt, mn, mx
 
 
-def workspace(fn, B, nring):
+def workspace(fn, B, nring, group=0):
     """Device buffers of a batch of B instances with an nring-deep history,
-    cached on the Functional so repeated solves of the same shape reuse them."""
+    cached on the Functional so repeated solves of the same shape reuse them
+    (one set per group of a grouped solve)."""
     cache = fn.__dict__.setdefault('_workspaces', {})
-    key = (B, nring)
+    key = (B, nring, group)
     if key in cache:
         return cache[key]
     plan = fn.plan
@@ -245,6 +246,9 @@ def ls_workspace(fn, ws, B, nring):
     ws['ls_part'] = ls_part
     ws['ls'] = torch.zeros((B, L.NLS), dtype=f64, device=dev)
     ws['ls_alpha'] = torch.zeros(B, dtype=f64, device=dev)
+    ws['pin_read'] = dict(stats=torch.zeros((B, L.NSTAT), dtype=f64).pin_memory(),
+                          ls=torch.zeros((B, L.NLS), dtype=f64).pin_memory(),
+                          alpha=torch.zeros(B, dtype=f64).pin_memory())
     return ws
 
 
@@ -258,7 +262,7 @@ class BatchSolve(object):
     def __init__(self, fn, chempots, method='hybridanderson', nsteps=500, threshold=1e-6,
                  criterion='res', alpha_mix=0.1, m=5, damping=0.3, delta=0.2, damping_max=0.8,
                  damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5), divergence_guard=False,
-                 a_tol=1e-6, r_tol=1e-4):
+                 a_tol=1e-6, r_tol=1e-4, group=0):
         self.fn = fn
         self.host_out = None
         self.plan = fn.plan
@@ -296,7 +300,7 @@ class BatchSolve(object):
         self.npts = n1 * n2 * n3
         self.dr = self.plan.dr
         self.nring = max(self.m, 2) if 'anderson' in self.method else 2
-        ws = workspace(fn, B, self.nring)
+        ws = workspace(fn, B, self.nring, group)
         if self.method != 'static':
             ls_workspace(fn, ws, B, self.nring)
         for k, v in ws.items():
@@ -599,10 +603,17 @@ class BatchSolve(object):
         self.it_eps0 = np.full(B, np.nan)
         self.damping = np.full(B, self.damping0)
         self.res_hist = np.full((B, self.nsteps + 2), np.nan)
-        # r_0 for the initial density
+        self.ls_host = np.zeros((B, L.NLS))
+        self.alpha_host = np.zeros(B)
+        self.ls_slot = np.full(B, -1)
+        # r_0 for the initial density, and the first line search ahead
         self._set_active(live)
         self._residual(self.chat, self.ring[0], self.rres[0], [])
-        st = self._stats()
+        E.finalize(self.buf, (1 << L.NSTAT) - 1, self.active)
+        self.kernel_launches += 1
+        self._launch_ls(live, 0, self.buf.stats[:, L.STAT_N3MAX])
+        st, ls, al = self._read(ls=True)
+        self._keep_ls(live, 0, ls, al)
         self.rnorm2[:, 0] = st[:, L.STAT_RES2]
         self.gram[:, 0, 0] = st[:, L.STAT_RES2]
         self.gnonfin = st[:, L.STAT_GNONFIN].copy()
@@ -680,13 +691,22 @@ class BatchSolve(object):
         m = self.nring
         return [j % m for j in range(max(0, k_new - m + 1), k_new)]
 
-    def _post_update(self, mask, k, s_new, st_mix):
+    def _post_update(self, mask, k, s_new, st_mix, ahead=None):
         """C1, Omega and residual of the density just written to ring slot s_new
-        (its spectrum in spec_ring[s_new]); its weighted densities are kept."""
+        (its spectrum in spec_ring[s_new]); its weighted densities are kept.
+        ahead: instances whose next step is likely a hybrid one; their line
+        search for this density is launched before the single read-back."""
         self._c1(self.spec_ring[s_new], self.chat2, 1 | 2 | 4 | 8, wd=self.wd_ring[s_new])
         hist_slots = self._valid_hist(k, s_new)
         self._residual(self.chat2, self.ring[s_new], self.rres[s_new], [self.rres[j] for j in hist_slots])
-        st = self._stats()
+        E.finalize(self.buf, (1 << L.NSTAT) - 1, self.active)
+        self.kernel_launches += 1
+        if ahead is not None and ahead.any():
+            self._launch_ls(ahead, s_new, self.buf.stats[:, L.STAT_N3MAX])
+            st, ls, al = self._read(ls=True)
+            self._keep_ls(ahead, s_new, ls, al)
+        else:
+            st = self._read()
         return st, hist_slots
 
     def _commit_residual(self, mask, st, k, s_new, hist_slots):
@@ -721,6 +741,7 @@ class BatchSolve(object):
         coefs[idx, mk:] = d[:, None] * alphas
         fields = [self.ring[j] for j in slots] + [self.rres[j] for j in slots]
         self._set_active(mask)
+        self.ls_slot[mask & (self.ls_slot == s_new)] = -1  # slot s_new gets a new density
         self._mix(coefs, fields, L.CLIP_DENSITY, self.ring[s_prev], self.ring[s_new], spec_out=self.spec_ring[s_new])
         st, hist_slots = self._post_update(mask, k, s_new, None)
         ok = np.zeros(B, dtype=bool)
@@ -775,6 +796,39 @@ class BatchSolve(object):
             G += lb[rows, L.LS_WDA + i] * dr
         return G
 
+    LS_COEFS = (0.45, 0.9, 0.225)   # trial alphas / alpha_max (solver.py:414-423)
+
+    def _launch_ls(self, mask, s, n3a):
+        """Line-search passes for the densities in ring slot s of the instances
+        in mask; n3a: device vector of their max n3."""
+        self._set_active(mask)
+        fn = self.fn
+        fn.ls_prepare(self.buf, self.rres[s], self.spec_ring[s], self.wd_ring[s], self.rhat, self.wd_r,
+                      self.ls_part, active=self.active)
+        fn.ls_omega(self.buf, n3a, self.LS_COEFS, self.ring[s], self.rres[s], self.wd_ring[s], self.wd_r,
+                    self.ls_part, self.ls_alpha, active=self.active)
+        fn.ls_finalize(self.buf, self.ls_part, self.ls, active=self.active)
+        self.kernel_launches += 6
+
+    def _read(self, stats=True, ls=False):
+        """Copy the finalized stats and/or the line-search sums to pinned host
+        memory and synchronise once."""
+        pin = self.pin_read
+        if stats:
+            pin['stats'].copy_(self.buf.stats, non_blocking=True)
+        if ls:
+            pin['ls'].copy_(self.ls, non_blocking=True)
+            pin['alpha'].copy_(self.ls_alpha, non_blocking=True)
+        torch.cuda.current_stream().synchronize()
+        if ls:
+            return pin['stats'].numpy().copy(), pin['ls'].numpy().copy(), pin['alpha'].numpy().copy()
+        return pin['stats'].numpy().copy()
+
+    def _keep_ls(self, mask, s, ls, alpha):
+        self.ls_host[mask] = ls[mask]
+        self.alpha_host[mask] = alpha[mask]
+        self.ls_slot[mask] = s
+
     def _hybrid_step(self, mask, k, s_prev, s_new):
         """Picard.update_rho_hybrid for the instances in mask (solver.py:403-457).
 
@@ -785,17 +839,14 @@ class BatchSolve(object):
         evaluated before the host chooses between them."""
         B = self.B
         prev = self.omega0.copy()
-        self._set_active(mask)
-        self._set_params(n3=self.n3max)
-        fn = self.fn
-        fn.ls_prepare(self.buf, self.rres[s_prev], self.spec_ring[s_prev], self.wd_ring[s_prev], self.rhat,
-                      self.wd_r, self.ls_part, active=self.active)
-        fn.ls_omega(self.buf, self.params, (0.45, 0.9, 0.225), self.ring[s_prev], self.rres[s_prev],
-                    self.wd_ring[s_prev], self.wd_r, self.ls_part, self.ls_alpha, active=self.active)
-        fn.ls_finalize(self.buf, self.ls_part, self.ls, active=self.active)
-        self.kernel_launches += 6
-        ls = self.ls.cpu().numpy()
-        amax = np.where(mask, self.ls_alpha.cpu().numpy(), 0.0)
+        fresh = mask & (self.ls_slot != s_prev)  # not computed ahead with the last evaluation
+        if fresh.any():
+            self._set_params(n3=self.n3max)
+            self._launch_ls(fresh, s_prev, self.params[:, 3])
+            _, ls_new, al_new = self._read(stats=False, ls=True)
+            self._keep_ls(fresh, s_prev, ls_new, al_new)
+        ls = self.ls_host
+        amax = np.where(mask, self.alpha_host, 0.0)
         aopt = np.zeros(B)
         mn = np.zeros(B)
         mx = np.zeros(B)
@@ -837,12 +888,100 @@ class BatchSolve(object):
         coefs[:, 0] = 1.0
         coefs[:, 1] = aopt * self.cf
         self._set_active(mask)
+        self.ls_slot[mask & (self.ls_slot == s_new)] = -1  # slot s_new gets a new density
         self._mix(coefs, [self.ring[s_prev], self.rres[s_prev]], L.CLIP_DENSITY, self.ring[s_prev],
                   self.ring[s_new], spec_out=self.spec_ring[s_new])
-        st, hist_slots = self._post_update(mask, k, s_new, None)
+        # the next step is a hybrid one for every instance while k + 1 <= 4
+        # (Anderson needs curr_step > 4, solver.py:561): its line search ahead
+        ahead = mask & ~self.And_true if k + 1 <= 4 else None
+        st, hist_slots = self._post_update(mask, k, s_new, None, ahead=ahead)
         self.omega0[midx] = self._omega_rows(st, midx)
         self.omega_evals += len(midx)
         self._commit_residual(mask, st, k, s_new, hist_slots)
 
     def n3max_of_current(self, b):
         return self.n3max[b]
+
+
+class GroupedSolve(object):
+    """A batch of instances solved as G independent groups, each a BatchSolve
+    on its own CUDA stream driven by its own host thread.
+
+    The batched loop alternates device work and host decisions (line-search
+    fits, Anderson coefficients, convergence tests) that read per-instance
+    sums back from the device.  With one group the device idles while the
+    host decides; with two or more, one group's kernels run while another
+    group's host logic executes (CUDA synchronisation and the ctypes launches
+    release the interpreter lock).  Instances are independent, so the
+    results equal those of a single BatchSolve over all of them.
+    Interface of BatchSolve.solve; per-instance arrays are concatenated.
+    """
+
+    def __init__(self, fn, chempots, groups=2, **kwargs):
+        self.mu = np.asarray(chempots, dtype=np.float64).ravel()
+        B = len(self.mu)
+        G = max(1, min(int(groups), B))
+        self.parts = [p for p in np.array_split(np.arange(B), G) if len(p)]
+        self.solvers = [BatchSolve(fn, self.mu[p], group=i, **kwargs) for i, p in enumerate(self.parts)]
+        self.B = B
+        self.pipeline_events = None
+
+    def solve(self, rho0, host_out=None):
+        import threading
+        if len(self.parts) == 1:  # one group: the caller's thread and stream
+            s = self.solvers[0]
+            s.pipeline_events = self.pipeline_events
+            self.N_out, self.result, self.conv = s.solve(rho0, host_out=host_out)
+            return self.N_out, self.result, self.conv
+        cur = torch.cuda.current_stream()
+        streams = [torch.cuda.Stream() for _ in self.parts]
+        out = [None] * len(self.parts)
+        errors = []
+
+        def run(i):
+            p, s, st = self.parts[i], self.solvers[i], streams[i]
+            try:
+                st.wait_stream(cur)  # rho0 and the functional are ready
+                with torch.cuda.stream(st):
+                    s.pipeline_events = self.pipeline_events
+                    ho = None if host_out is None else host_out[p[0]:p[-1] + 1]
+                    out[i] = s.solve(rho0[p[0]:p[-1] + 1], host_out=ho)
+            except BaseException as e:  # re-raised on the calling thread
+                errors.append(e)
+
+        threads = [threading.Thread(target=run, args=(i,)) for i in range(len(self.parts))]
+        for t in threads:
+            t.start()
+        for t in threads:
+            t.join()
+        for st in streams:
+            cur.wait_stream(st)
+        if errors:
+            raise errors[0]
+        self.result = torch.cat([o[1] for o in out], dim=0)
+        self.N_out = np.concatenate([o[0] for o in out])
+        self.conv = np.concatenate([o[2] for o in out])
+        return self.N_out, self.result, self.conv
+
+    def _cat(self, name):
+        return np.concatenate([getattr(s, name) for s in self.solvers])
+
+    @property
+    def steps(self):
+        return self._cat('steps')
+
+    @property
+    def diverged(self):
+        return self._cat('diverged')
+
+    @property
+    def omega0(self):
+        return self._cat('omega0')
+
+    @property
+    def kernel_launches(self):
+        return sum(s.kernel_launches for s in self.solvers)
+
+    @property
+    def omega_evals(self):
+        return sum(s.omega_evals for s in self.solvers)

@@ -1499,7 +1499,7 @@ k_ls_n3max(GridDev g, const int* __restrict__ active, const double* __restrict__
 // Omega ingredients of rho + alpha_i r for three alphas, one plane per block.
 template <bool WDA, bool TEN>
 __global__ void __launch_bounds__(CMM_ROW_THREADS)
-k_ls_omega(GridDev g, const int* __restrict__ active, const double* __restrict__ params, double c0, double c1,
+k_ls_omega(GridDev g, const int* __restrict__ active, const double* __restrict__ n3a, long long n3a_stride, double c0, double c1,
            double c2, double R, double lambda3, int version, cmm_wda_eos wda, const double* __restrict__ rho,
            const double* __restrict__ r, const double* __restrict__ V, long long vstride,
            const double* __restrict__ wd_rho, const double* __restrict__ wd_r, size_t fsr,
@@ -1515,7 +1515,7 @@ k_ls_omega(GridDev g, const int* __restrict__ active, const double* __restrict__
     for (int k = threadIdx.x; k < nslot; k += 32) gmax = fmax(gmax, pm[k]);
     for (int o = 16; o > 0; o >>= 1) gmax = fmax(gmax, __shfl_xor_sync(0xffffffffu, gmax, o));
     if (threadIdx.x == 0) {
-      const double a = params[b * 4 + 3];
+      const double a = n3a[(size_t)b * n3a_stride];
       const double q = fabs((1 - a) / ((gmax - a) + 1e-16));
       const double amax = (q != q) ? q : fmin(q, 1.0);   // np.min([q, 1]) (propagates NaN)
       s_alpha[0] = c0 * amax; s_alpha[1] = c1 * amax; s_alpha[2] = c2 * amax;
@@ -2099,23 +2099,23 @@ extern "C" int cmm_ls_prepare(const cmm_grid* g, int batch, const int* d_active,
 }
 
 template <bool WDA, bool TEN>
-static int ls_omega_one(const cmm_grid* g, int batch, const int* act, const double* params, double c0, double c1,
+static int ls_omega_one(const cmm_grid* g, int batch, const int* act, const double* n3a, long long n3s, double c0, double c1,
                         double c2, double R, double lambda3, int version, const cmm_wda_eos& we, const double* rho,
                         const double* r, const double* V, long long vstride, const double* wd_rho,
                         const double* wd_r, double* ls_part, int nslot, double* alpha, cudaStream_t st) {
   const size_t fsr = (size_t)batch * g->n1 * g->n2 * g->n3;
   k_ls_omega<WDA, TEN><<<dim3(g->n1, batch), CMM_ROW_THREADS, 0, st>>>(
-      g->dev, act, params, c0, c1, c2, R, lambda3, version, we, rho, r, V, vstride, wd_rho, wd_r, fsr, ls_part,
+      g->dev, act, n3a, n3s, c0, c1, c2, R, lambda3, version, we, rho, r, V, vstride, wd_rho, wd_r, fsr, ls_part,
       nslot, alpha);
   return last_err();
 }
 
-extern "C" int cmm_ls_omega(const cmm_grid* g, int batch, const int* d_active, const double* d_params,
-                            double c0, double c1, double c2, double R, double lambda3, int version,
+extern "C" int cmm_ls_omega(const cmm_grid* g, int batch, const int* d_active, const double* d_n3a,
+                            long long n3a_stride, double c0, double c1, double c2, double R, double lambda3, int version,
                             const cmm_wda_eos* wda, const double* d_rho, const double* d_r, const double* d_V,
                             long long vstride, const double* d_wd_rho, const double* d_wd_r, double* d_ls_part,
                             int nslot, double* d_alpha, void* stream) {
-  if (!g || batch < 1 || !d_params || !d_rho || !d_r || !d_V || !d_wd_rho || !d_wd_r || !d_ls_part || !d_alpha)
+  if (!g || batch < 1 || !d_n3a || !d_rho || !d_r || !d_V || !d_wd_rho || !d_wd_r || !d_ls_part || !d_alpha)
     return CMM_ERR_ARG;
   if (nslot < g->n1) return CMM_ERR_WORKSPACE;
   const bool has_wda = (version & CMM_WDA) != 0, ten = (version & CMM_TENSOR) != 0;
@@ -2125,7 +2125,7 @@ extern "C" int cmm_ls_omega(const cmm_grid* g, int batch, const int* d_active, c
   if (has_wda) we = *wda;
   cudaStream_t st = (cudaStream_t)stream;
 #define LS_OMEGA(w, t)                                                                                     \
-  ls_omega_one<w, t>(g, batch, d_active, d_params, c0, c1, c2, R, lambda3, version, we, d_rho, d_r, d_V, vstride, \
+  ls_omega_one<w, t>(g, batch, d_active, d_n3a, n3a_stride, c0, c1, c2, R, lambda3, version, we, d_rho, d_r, d_V, vstride, \
                      d_wd_rho, d_wd_r, d_ls_part, nslot, d_alpha, st)
   if (has_wda && ten) return LS_OMEGA(true, true);
   if (has_wda) return LS_OMEGA(true, false);

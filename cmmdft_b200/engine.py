@@ -14,7 +14,8 @@ from ._lib import check, ptr
 
 
 def _stream():
-    return ctypes.c_void_p(torch.cuda.current_stream().cuda_stream)
+    """The calling thread's current CUDA stream (torch's) as a void*."""
+    return ctypes.c_void_p(torch._C._cuda_getCurrentRawStream(torch._C._cuda_getDevice()))
 
 
 def require_cuda():
@@ -193,13 +194,15 @@ class Functional(object):
                                      ptr(buf.work), ptr(wd_r), ptr(ls_part), buf.nslot, _stream()),
               "cmm_ls_prepare")
 
-    def ls_omega(self, buf, params, coefs, rho, r, wd_rho, wd_r, ls_part, alpha, active=None, vstride=0):
+    def ls_omega(self, buf, n3a, coefs, rho, r, wd_rho, wd_r, ls_part, alpha, active=None, vstride=0):
+        """n3a: per-instance max n3 of rho, a (strided) device vector, e.g. params[:, 3]
+        or the N3MAX column of the finalized stats."""
         wda = ctypes.byref(self.wda) if self.wda is not None else None
         c0, c1, c2 = [float(c) for c in coefs]
-        check(L.lib().cmm_ls_omega(self.plan.handle, buf.batch, ptr(active), ptr(params), c0, c1, c2, self.R,
-                                   self.lambda3, self.version, wda, ptr(rho), ptr(r), ptr(self.V), int(vstride),
-                                   ptr(wd_rho), ptr(wd_r), ptr(ls_part), buf.nslot, ptr(alpha), _stream()),
-              "cmm_ls_omega")
+        check(L.lib().cmm_ls_omega(self.plan.handle, buf.batch, ptr(active), ptr(n3a), int(n3a.stride(0)), c0, c1,
+                                   c2, self.R, self.lambda3, self.version, wda, ptr(rho), ptr(r), ptr(self.V),
+                                   int(vstride), ptr(wd_rho), ptr(wd_r), ptr(ls_part), buf.nslot, ptr(alpha),
+                                   _stream()), "cmm_ls_omega")
 
     def ls_finalize(self, buf, ls_part, ls, active=None):
         check(L.lib().cmm_ls_finalize(buf.batch, ptr(active), ptr(ls_part), buf.nslot, ptr(ls), _stream()),

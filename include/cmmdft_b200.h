@@ -267,11 +267,11 @@ int cmm_ls_prepare(const cmm_grid* grid, int batch, const int* d_active, double 
                    const double* d_rhohat, const double* d_wd_rho, double* d_rhat, double* d_work,
                    double* d_wd_r, double* d_ls_part, int nslot, void* stream);
 /* cmm_ls_omega: alpha_max = min(|(1 - a) / ((g - a) + 1e-16)|, 1) per
- * instance (a = d_params[b][3], the max n3 of rho; g = CMM_LS_N3MAX_G),
- * written to d_alpha[b]; then the pointwise sums of CMM_LS_SUM_R .. WDA at
- * alpha_i = coef[i] * alpha_max, i < 3. */
-int cmm_ls_omega(const cmm_grid* grid, int batch, const int* d_active, const double* d_params,
-                 double c0, double c1, double c2, double R, double lambda3, int version,
+ * instance (a = d_n3a[b * n3a_stride], the max n3 of rho; g =
+ * CMM_LS_N3MAX_G), written to d_alpha[b]; then the pointwise sums of
+ * CMM_LS_SUM_R .. WDA at alpha_i = coef[i] * alpha_max, i < 3. */
+int cmm_ls_omega(const cmm_grid* grid, int batch, const int* d_active, const double* d_n3a,
+                 long long n3a_stride, double c0, double c1, double c2, double R, double lambda3, int version,
                  const cmm_wda_eos* wda, const double* d_rho, const double* d_r, const double* d_V,
                  long long vstride, const double* d_wd_rho, const double* d_wd_r, double* d_ls_part,
                  int nslot, double* d_alpha, void* stream);

@@ -343,7 +343,7 @@ def test_line_search_matches_pipeline(cuda, case):
     s._set_params(n3=s.n3max)
     fn.ls_prepare(s.buf, s.rres[0], s.spec_ring[0], s.wd_ring[0], s.rhat, s.wd_r, s.ls_part, active=s.active)
     coefs = (0.45, 0.9, 0.225)
-    fn.ls_omega(s.buf, s.params, coefs, s.ring[0], s.rres[0], s.wd_ring[0], s.wd_r, s.ls_part, s.ls_alpha,
+    fn.ls_omega(s.buf, s.params[:, 3], coefs, s.ring[0], s.rres[0], s.wd_ring[0], s.wd_r, s.ls_part, s.ls_alpha,
                 active=s.active)
     fn.ls_finalize(s.buf, s.ls_part, s.ls, active=s.active)
     ls = s.ls.cpu().numpy()
@@ -360,3 +360,25 @@ def test_line_search_matches_pipeline(cuda, case):
         for b in range(3):
             om_ls = s._ls_omega(ls[b], b, i, c * amax[b])
             assert scalar_rel(om_ls, om_pipe[b]) < 1e-12, (case, i, b, om_ls, om_pipe[b])
+
+
+@pytest.mark.parametrize("groups", [2, 3])
+def test_grouped_solve_equals_single_batch(cuda, groups):
+    """Instances are independent: groups on concurrent streams reproduce the
+    single batched solve exactly."""
+    host = cubic_host_276(0)
+    guest = methane_guest_params()
+    fn = W.build_functional(host, (32, 32, 32), 300.0, guest)
+    P = np.logspace(-3, 1.3, 7) * bar
+    mus, bulks = W.isotherm_inputs(P, 300.0, guest)
+    r0 = W.initial_density(fn, mus, ninit=bulks)
+    kw = dict(method='hybridanderson', nsteps=200, threshold=1e-10, criterion='res')
+    s1 = BT.BatchSolve(fn, mus, **kw)
+    N1, rho1, c1 = s1.solve(r0)
+    sg = BT.GroupedSolve(fn, mus, groups=groups, **kw)
+    host_out = torch.empty(tuple(r0.shape), dtype=torch.float64, pin_memory=True)
+    N2, rho2, c2 = sg.solve(r0, host_out=host_out)
+    assert np.array_equal(c1, c2) and np.array_equal(s1.steps, sg.steps)
+    assert np.array_equal(N1, N2)
+    assert torch.equal(rho1, rho2)
+    assert torch.equal(host_out, rho2.cpu())
