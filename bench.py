@@ -156,7 +156,8 @@ def run_gpu(args):
     rho0 = W.initial_density(fn, mus, ninit=bulks)
 
     def one_solve(events=None):
-        s = BT.GroupedSolve(fn, mus, groups=args.groups, method="hybridanderson", nsteps=args.max_iters,
+        s = BT.GroupedSolve(fn, mus, groups=args.groups, native=args.driver == "native", method="hybridanderson",
+                            nsteps=args.max_iters,
                             threshold=THRESH, criterion="res", divergence_guard=True)
         s.pipeline_events = events
         N, rho, conv = s.solve(rho0)
@@ -213,13 +214,15 @@ def run_gpu(args):
     if not args.no_e2e:
         out = None
         for _ in range(args.warmup):   # warm-up: pinned result buffers, plan tables, workspaces
-            out = ISO.solve_isotherm(host, pressures, T, guest, NPTS, threshold=THRESH, groups=args.groups)
+            out = ISO.solve_isotherm(host, pressures, T, guest, NPTS, threshold=THRESH, groups=args.groups,
+                                     native=args.driver == "native")
         barrier()
         t0 = time.perf_counter()
         h2d = d2h = 0
         ne = 0
         for _ in range(args.steps):
-            out = ISO.solve_isotherm(host, pressures, T, guest, NPTS, threshold=THRESH, groups=args.groups)
+            out = ISO.solve_isotherm(host, pressures, T, guest, NPTS, threshold=THRESH, groups=args.groups,
+                                     native=args.driver == "native")
             ne += int(out["converged"].sum())
             h2d += host.pos.nbytes + host.ffatype_ids.nbytes + 2 * 8 * len(host.ffatypes)
             d2h += out["rho"].nbytes + out["N"].nbytes
@@ -238,7 +241,8 @@ def run_gpu(args):
         npl = 0
         pit = 0
         for i in range(NPRESS):
-            s = BT.BatchSolve(fn, mus[i:i + 1], method="hybridanderson", nsteps=args.max_iters,
+            cls = BT.NativeBatchSolve if args.driver == "native" else BT.BatchSolve
+            s = cls(fn, mus[i:i + 1], method="hybridanderson", nsteps=args.max_iters,
                               threshold=THRESH, criterion="res", divergence_guard=True)
             N, rho, conv = s.solve(rho0[i:i + 1])
             npl += int(conv.sum())
@@ -262,7 +266,7 @@ def run_gpu(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "isotherm-64cubed", "grid": list(NPTS), "host": "cubic a=17A 276 atoms seed 0",
                        "points_per_isotherm": NPRESS, "pressures_bar": [1e-3, 100.0], "solver": "hybridanderson m=5",
-                       "instance_groups": args.groups,
+                       "instance_groups": args.groups, "driver": args.driver,
                        "tolerance": "RES<1e-8", "start": "Ninit=rho_bulk", "iterations_per_isotherm": iters,
                        "converged_points": nconv, "steps_per_point": per_point,
                        "diverged_points": diverged,
@@ -364,6 +368,8 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)   # ~0.5 s of timed solves: host jitter averages out
     ap.add_argument("--groups", type=int, default=1, help="instance groups on concurrent streams")
+    ap.add_argument("--driver", choices=("native", "python"), default="native",
+                    help="batched loop in the library (cmm_solve_batched) or in Python")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-plain", action="store_true")

@@ -28,6 +28,43 @@ class WdaEos(ctypes.Structure):
                 ("eta", ctypes.c_double), ("kT", ctypes.c_double), ("a_mfa", ctypes.c_double),
                 ("factors", ctypes.c_double * 3)]
 CLIP_NONE, CLIP_PICARD, CLIP_DENSITY = 0, 1, 2
+SOLVE_HYBRID, SOLVE_ANDERSON, SOLVE_HYBRIDANDERSON = 1, 2, 3
+CRIT_RES, CRIT_RIUE, CRIT_DER = 0, 1, 2
+
+_vp, _d, _i = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
+
+
+class FunctionalDesc(ctypes.Structure):
+    """cmm_functional_desc."""
+    _fields_ = [("grid", _vp), ("R", _d), ("beta", _d), ("lambda3", _d), ("version", _i), ("wda", _vp),
+                ("d_kst", _vp), ("d_wtab", _vp), ("d_V", _vp)]
+
+
+class SolveOpts(ctypes.Structure):
+    """cmm_solve_opts."""
+    _fields_ = [("method", _i), ("nsteps", _i), ("m", _i), ("ncrit", _i), ("crit", _i * 3), ("thr", _d * 3),
+                ("alpha_mix", _d), ("damping", _d), ("delta", _d), ("damping_max", _d), ("damping_min", _d),
+                ("damping_up", _d), ("damping_down", _d), ("adaptive_damping", _i), ("divergence_guard", _i),
+                ("a_tol", _d), ("r_tol", _d), ("ls_thresh", _d), ("kjmol", _d)]
+
+
+class SolveWs(ctypes.Structure):
+    """cmm_solve_ws."""
+    _fields_ = [(n, _vp) for n in ("ring", "rres", "trial", "rho0", "result", "spec_ring", "wd_ring", "wd_r", "rhat",
+                                   "chat", "chat2", "that", "work", "part", "stats", "params", "coef", "active",
+                                   "ls_part", "ls", "ls_alpha")] + \
+               [("nslot", _i), ("h_stats", _vp), ("h_ls", _vp), ("h_alpha", _vp), ("h_stage", _vp),
+                ("h_result", _vp)]
+
+
+class SolveOut(ctypes.Structure):
+    """cmm_solve_out."""
+    _fields_ = [(n, _vp) for n in ("N", "omega", "converged", "steps", "diverged", "failed", "history")] + \
+               [("launches", ctypes.c_longlong), ("omega_evals", ctypes.c_longlong)]
+
+
+FALLBACK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
+                               ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double))
 
 
 class CmmError(RuntimeError):
@@ -64,6 +101,9 @@ _SIGS = {
                       c_int, c_void_p, c_void_p, c_void_p, c_void_p, c_ll, c_void_p, c_void_p, c_void_p, c_int,
                       c_void_p, c_void_p], c_int),
     "cmm_ls_finalize": ([c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p], c_int),
+    "cmm_solve_stage_bytes": ([c_int], ctypes.c_size_t),
+    "cmm_solve_batched": ([P(FunctionalDesc), P(SolveOpts), c_int, c_void_p, c_void_p, c_void_p, P(SolveWs),
+                           P(SolveOut), FALLBACK_FN, c_void_p, c_void_p], c_int),
     "cmm_fmt_weights": ([c_void_p, c_double, c_void_p, c_void_p], c_int),
     "cmm_picard_static_step": ([c_void_p, c_int, c_void_p, c_void_p, c_double, c_double, c_double, c_double,
                                 c_double, c_void_p,

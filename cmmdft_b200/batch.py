@@ -917,12 +917,13 @@ class GroupedSolve(object):
     Interface of BatchSolve.solve; per-instance arrays are concatenated.
     """
 
-    def __init__(self, fn, chempots, groups=2, **kwargs):
+    def __init__(self, fn, chempots, groups=2, native=True, **kwargs):
         self.mu = np.asarray(chempots, dtype=np.float64).ravel()
         B = len(self.mu)
         G = max(1, min(int(groups), B))
         self.parts = [p for p in np.array_split(np.arange(B), G) if len(p)]
-        self.solvers = [BatchSolve(fn, self.mu[p], group=i, **kwargs) for i, p in enumerate(self.parts)]
+        cls = NativeBatchSolve if native else BatchSolve
+        self.solvers = [cls(fn, self.mu[p], group=i, **kwargs) for i, p in enumerate(self.parts)]
         self.B = B
         self.pipeline_events = None
 
@@ -985,3 +986,113 @@ class GroupedSolve(object):
     @property
     def omega_evals(self):
         return sum(s.omega_evals for s in self.solvers)
+
+
+class NativeBatchSolve(BatchSolve):
+    """BatchSolve whose hybrid / Anderson loop runs in the library
+    (cmm_solve_batched): the same kernels on the same buffers, with the
+    per-instance decisions evaluated in C++ between read-backs instead of in
+    the interpreter.  The rare SLSQP fallback of the line search is called
+    back into Python (scipy, on full evaluations of the trial density).
+    Static Picard runs the Python loop.  Same results as BatchSolve."""
+
+    def solve(self, rho0, cf=None, host_out=None):
+        if self.method == 'static':
+            return BatchSolve.solve(self, rho0, cf=cf, host_out=host_out)
+        if host_out is not None and (not host_out.is_pinned() or tuple(host_out.shape) != tuple(rho0.shape)):
+            raise ValueError("host_out must be a pinned tensor of the shape of rho0")
+        import ctypes
+        B, fn = self.B, self.fn
+        self.initial_density(rho0)
+        self.cf = np.ones(B) if cf is None else np.asarray(cf, dtype=float).copy()
+        self.result = torch.empty_like(self.rho0)
+        self.history = [[] for _ in range(B)]
+        self.fallbacks = 0
+        method = {'hybrid': L.SOLVE_HYBRID, 'anderson': L.SOLVE_ANDERSON,
+                  'hybridanderson': L.SOLVE_HYBRIDANDERSON}[self.method]
+        crit = {'res': L.CRIT_RES, 'riue': L.CRIT_RIUE, 'der': L.CRIT_DER}
+        nc = len(self.criteria)
+        opts = L.SolveOpts(method=method, nsteps=self.nsteps, m=self.m, ncrit=nc,
+                           alpha_mix=self.alpha_mix, damping=self.damping0, delta=self.delta,
+                           damping_max=self.damping_max, damping_min=self.damping_min,
+                           damping_up=self.dfac[0], damping_down=self.dfac[1],
+                           adaptive_damping=int(bool(self.adaptive)), divergence_guard=int(self.divergence_guard),
+                           a_tol=self.tol[0], r_tol=self.tol[1], ls_thresh=self.thresh, kjmol=kjmol)
+        for i, (c, t) in enumerate(zip(self.criteria, self.thresholds)):
+            opts.crit[i] = crit[c]
+            opts.thr[i] = t
+        wda = ctypes.addressof(fn.wda) if fn.wda is not None else None
+        desc = L.FunctionalDesc(fn.plan.handle.value, fn.R, fn.beta, fn.lambda3, fn.version, wda,
+                                fn.kst.data_ptr(), fn.wtab.data_ptr() if fn.wtab is not None else None,
+                                fn.V.data_ptr())
+        ws_d = self.__dict__
+        stage = self.pin_read.get('stage')
+        nstage = int(L.lib().cmm_solve_stage_bytes(B))
+        if stage is None or stage.numel() < nstage:
+            stage = torch.empty(nstage, dtype=torch.uint8).pin_memory()
+            self.pin_read['stage'] = stage
+        names = ("ring", "rres", "trial", "rho0", "spec_ring", "wd_ring", "wd_r", "rhat", "chat", "chat2", "that",
+                 "params", "coef", "active", "ls_part", "ls", "ls_alpha")
+        ws = L.SolveWs(**{n: ws_d[n].data_ptr() for n in names})
+        ws.result = self.result.data_ptr()
+        ws.work, ws.part, ws.stats = self.buf.work.data_ptr(), self.buf.part.data_ptr(), self.buf.stats.data_ptr()
+        ws.nslot = self.buf.nslot
+        ws.h_stats = self.pin_read['stats'].data_ptr()
+        ws.h_ls = self.pin_read['ls'].data_ptr()
+        ws.h_alpha = self.pin_read['alpha'].data_ptr()
+        ws.h_stage = stage.data_ptr()
+        ws.h_result = host_out.data_ptr() if host_out is not None else None
+        N = np.full(B, np.nan)
+        om = np.full(B, np.nan)
+        conv, steps, div, failed = (np.zeros(B, dtype=np.int32) for _ in range(4))
+        hist = np.full((B, self.nsteps + 2, 3), np.nan)
+        arr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
+        out = L.SolveOut(N=arr(N), omega=arr(om), converged=arr(conv), steps=arr(steps), diverged=arr(div),
+                         failed=arr(failed), history=arr(hist))
+        cb = L.FALLBACK_FN(self._native_fallback)
+        mu = np.ascontiguousarray(self.mu, dtype=np.float64)
+        fug = np.ascontiguousarray(self.fug, dtype=np.float64)
+        cf0 = np.ascontiguousarray(self.cf, dtype=np.float64)
+        self._fallback_error = None
+        rc = L.lib().cmm_solve_batched(ctypes.byref(desc), ctypes.byref(opts), B, arr(mu), arr(fug), arr(cf0),
+                                       ctypes.byref(ws), ctypes.byref(out), cb, None, E._stream())
+        if self._fallback_error is not None:
+            raise self._fallback_error
+        L.check(rc, "cmm_solve_batched")
+        self.N_out, self.conv = N, conv.astype(bool)
+        self.steps, self.diverged, self.failed = steps.astype(int), div.astype(bool), failed.astype(bool)
+        self.omega0 = om
+        self.kernel_launches += int(out.launches)
+        self.omega_evals += int(out.omega_evals)
+        for b in range(B):
+            for k in range(1, self.nsteps + 2):
+                if not np.isnan(hist[b, k, 0]):
+                    self.history[b].append(tuple(hist[b, k]))
+        if self.failed.any():
+            raise NoSolutionError("instances %s hit non-finite densities on every retry"
+                                  % list(np.where(self.failed)[0]))
+        return self.N_out, self.result, self.conv
+
+    def _native_fallback(self, ctx, b, s_prev, amax, alpha_p, omega_p):
+        """SLSQP over Omega((1-a) rho + a G) on full evaluations (solver.py:437-447)."""
+        try:
+            B = self.B
+            one = np.zeros(B, dtype=bool)
+            one[b] = True
+            last = [np.nan]
+
+            def fun(alpha):
+                al = np.zeros(B)
+                al[b] = float(np.asarray(alpha).ravel()[0])
+                o = self._trial_omega(one, al, s_prev)[b]
+                last[0] = o
+                return o
+            bnd = opt.Bounds(0.01 * amax, 0.9 * amax)
+            res = opt.minimize(fun, [self.alpha_mix * amax], bounds=bnd, method='SLSQP', options={'ftol': 1e-8})
+            alpha_p[0] = float(res.x[0])
+            omega_p[0] = float(last[0])
+            self.fallbacks += 1
+            return 0
+        except BaseException as e:  # reported after the native call returns
+            self._fallback_error = e
+            return 1

@@ -124,7 +124,8 @@ class Program(object):
         fn = self.fener.device()
         mus = np.asarray(chempots, dtype=float)
         rho0 = W.initial_density(fn, mus, ninit=None if Ninit is None else np.asarray(Ninit, dtype=float))
-        s = BT.BatchSolve(fn, mus, method=method, nsteps=nsteps, threshold=threshold, criterion=criterion, **options)
+        s = BT.NativeBatchSolve(fn, mus, method=method, nsteps=nsteps, threshold=threshold, criterion=criterion,
+                                **options)
         N, rho, conv = s.solve(rho0)
         rho = rho.cpu().numpy()
         if save:

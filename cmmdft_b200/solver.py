@@ -60,7 +60,7 @@ class Solver(object):
         """Converge one density (B = 1) on the GPU; returns (N, rho, converged)."""
         import torch
         fn = self.fener.device()
-        s = BT.BatchSolve(fn, [chempot], method=self._method(), nsteps=self.nsteps, threshold=self.threshold,
+        s = BT.NativeBatchSolve(fn, [chempot], method=self._method(), nsteps=self.nsteps, threshold=self.threshold,
                           criterion=self.criterion, a_tol=self.a_tol, r_tol=self.r_tol, **self._options())
         r0 = rho if hasattr(rho, 'detach') else torch.as_tensor(np.ascontiguousarray(rho, dtype=np.float64))
         r0 = r0.to('cuda', dtype=torch.float64).reshape((1,) + tuple(self.grid.npoints))

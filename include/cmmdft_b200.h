@@ -280,6 +280,91 @@ int cmm_ls_omega(const cmm_grid* grid, int batch, const int* d_active, const dou
 int cmm_ls_finalize(int batch, const int* d_active, const double* d_ls_part, int nslot, double* d_ls,
                     void* stream);
 
+/* ---------------------------------------------------------------------
+ * Native batched solve: the control flow of Solver._solve with the
+ * Picard hybrid and (hybrid-)Anderson updates (cmmdft/solver.py:236-345,
+ * 403-457, 515-604) for `batch` chemical potentials on one functional, run
+ * in C++ around the kernels above (one read-back per decision point).
+ * Equivalent to the Python driver cmmdft_b200.batch.BatchSolve, which
+ * remains its specification.
+ * ------------------------------------------------------------------- */
+typedef struct cmm_functional_desc {
+  const cmm_grid* grid;
+  double R, beta, lambda3;
+  int version;                  /* CMM_FMT / MFMT / WBII | ANTISYM | TENSOR | WDA */
+  const cmm_wda_eos* wda;       /* with CMM_WDA, else NULL */
+  const double* d_kst;          /* MFA kernel spectrum */
+  const double* d_wtab;         /* weight table or NULL */
+  const double* d_V;            /* external potential [N1][N2][N3] */
+} cmm_functional_desc;
+
+enum { CMM_SOLVE_HYBRID = 1, CMM_SOLVE_ANDERSON = 2, CMM_SOLVE_HYBRIDANDERSON = 3 };
+enum { CMM_CRIT_RES = 0, CMM_CRIT_RIUE = 1, CMM_CRIT_DER = 2 };
+
+typedef struct cmm_solve_opts {
+  int method;                   /* CMM_SOLVE_* */
+  int nsteps, m;                /* step limit, Anderson history depth */
+  int ncrit, crit[3];           /* criteria, all must hold */
+  double thr[3];
+  double alpha_mix, damping, delta, damping_max, damping_min, damping_up, damping_down;
+  int adaptive_damping;
+  int divergence_guard;         /* retire instances whose RES rises past 1e6 x best */
+  double a_tol, r_tol;          /* DER tolerances */
+  double ls_thresh;             /* 1 kJ/mol: line-search fallback threshold (Hartree) */
+  double kjmol;                 /* 1 kJ/mol in Hartree */
+} cmm_solve_opts;
+
+/* Buffers of one solve (device, except the h_* pinned host arrays).
+ * npts = N1*N2*N3, S = 2*N1*N2*H3 doubles (one yz-spectrum), nwd as
+ * cmm_fmt_c1's want bit 3, nwork = 12 (24 with CMM_TENSOR). */
+typedef struct cmm_solve_ws {
+  double* ring;                 /* [m][B][npts] densities */
+  double* rres;                 /* [m][B][npts] residuals */
+  double* trial;                /* [B][npts] */
+  double* rho0;                 /* [B][npts] initial densities (input) */
+  double* result;               /* [B][npts] final densities (output) */
+  double* spec_ring;            /* [m][B][S] */
+  double* wd_ring;              /* [m][nwd][B][npts] */
+  double* wd_r;                 /* [nwd][B][npts] */
+  double* rhat, *chat, *chat2, *that;   /* [B][S] each */
+  double* work;                 /* [nwork][B][S] */
+  double* part;                 /* [B][CMM_NSTAT][nslot], N3MAX slots -inf */
+  double* stats;                /* [B][CMM_NSTAT] */
+  double* params;               /* [B][4] */
+  double* coef;                 /* [B][12] */
+  int* active;                  /* [B] */
+  double* ls_part;              /* [B][CMM_NLS][nslot], 0 and -inf in CMM_LS_N3MAX_G */
+  double* ls;                   /* [B][CMM_NLS] */
+  double* ls_alpha;             /* [B] */
+  int nslot;
+  double* h_stats;              /* pinned [B][CMM_NSTAT] */
+  double* h_ls;                 /* pinned [B][CMM_NLS] */
+  double* h_alpha;              /* pinned [B] */
+  void* h_stage;                /* pinned staging of uploads, cmm_solve_stage_bytes(B) */
+  double* h_result;             /* optional pinned [B][npts]: each final density is copied here on a
+                                   side stream as soon as its instance finishes (NULL: none) */
+} cmm_solve_ws;
+
+typedef struct cmm_solve_out {
+  double* N;                    /* [B] loading (integral of rho) */
+  double* omega;                /* [B] grand potential of the last density */
+  int* converged, *steps, *diverged, *failed;   /* [B]; failed: non-finite on every retry */
+  double* history;              /* optional [B][nsteps + 2][3] (N, RES, RIUE per step), or NULL */
+  long long launches;           /* kernel launches issued */
+  long long omega_evals;
+} cmm_solve_out;
+
+/* The line search's SLSQP fallback (solver.py:437-447) is delegated to the
+ * caller: minimise Omega((1-a) rho + a G) over a in [0.01, 0.9] alpha_max for
+ * instance b, rho in ring slot s_prev; returns 0 and alpha (and the last
+ * Omega evaluated) on success. */
+typedef int (*cmm_fallback_fn)(void* ctx, int b, int s_prev, double alpha_max, double* alpha, double* omega);
+
+size_t cmm_solve_stage_bytes(int batch);
+int cmm_solve_batched(const cmm_functional_desc* fn, const cmm_solve_opts* opt, int batch, const double* mu,
+                      const double* fug, const double* cf0, const cmm_solve_ws* ws, cmm_solve_out* out,
+                      cmm_fallback_fn fallback, void* fallback_ctx, void* stream);
+
 /* Allocation-free variant of cmm_fmt_c1 (no counterpart in the reference,
  * which allocates freely in numpy).  For callers that cannot allocate device
  * memory where they evaluate the functional -- plugin hosts that forbid

@@ -362,8 +362,9 @@ def test_line_search_matches_pipeline(cuda, case):
             assert scalar_rel(om_ls, om_pipe[b]) < 1e-12, (case, i, b, om_ls, om_pipe[b])
 
 
+@pytest.mark.parametrize("native", [False, True])
 @pytest.mark.parametrize("groups", [2, 3])
-def test_grouped_solve_equals_single_batch(cuda, groups):
+def test_grouped_solve_equals_single_batch(cuda, groups, native):
     """Instances are independent: groups on concurrent streams reproduce the
     single batched solve exactly."""
     host = cubic_host_276(0)
@@ -373,12 +374,50 @@ def test_grouped_solve_equals_single_batch(cuda, groups):
     mus, bulks = W.isotherm_inputs(P, 300.0, guest)
     r0 = W.initial_density(fn, mus, ninit=bulks)
     kw = dict(method='hybridanderson', nsteps=200, threshold=1e-10, criterion='res')
-    s1 = BT.BatchSolve(fn, mus, **kw)
+    s1 = (BT.NativeBatchSolve if native else BT.BatchSolve)(fn, mus, **kw)
     N1, rho1, c1 = s1.solve(r0)
-    sg = BT.GroupedSolve(fn, mus, groups=groups, **kw)
+    sg = BT.GroupedSolve(fn, mus, groups=groups, native=native, **kw)
     host_out = torch.empty(tuple(r0.shape), dtype=torch.float64, pin_memory=True)
     N2, rho2, c2 = sg.solve(r0, host_out=host_out)
     assert np.array_equal(c1, c2) and np.array_equal(s1.steps, sg.steps)
     assert np.array_equal(N1, N2)
     assert torch.equal(rho1, rho2)
     assert torch.equal(host_out, rho2.cpu())
+
+
+@pytest.mark.parametrize("method,case", [("hybridanderson", "wbii"), ("hybrid", "wbii"), ("anderson", "wbii"),
+                                         ("hybridanderson", "atwbii_wda")])
+def test_native_driver_equals_python_driver(cuda, method, case):
+    """cmm_solve_batched (C++ loop) against BatchSolve (Python loop): the same
+    kernels and decisions, so the same steps and densities."""
+    host = cubic_host_276(0)
+    guest = methane_guest_params()
+    kw = {} if case == "wbii" else dict(version='atWBII', wda=True)
+    fn = W.build_functional(host, (32, 32, 32), 300.0, guest, **kw)
+    P = np.logspace(-3, 1.5, 6) * bar
+    mus, bulks = W.isotherm_inputs(P, 300.0, guest)
+    r0 = W.initial_density(fn, mus, ninit=bulks)
+    opts = dict(method=method, nsteps=120, threshold=1e-10, criterion='res', divergence_guard=True)
+    sp = BT.BatchSolve(fn, mus, **opts)
+    Np, rp, cp = sp.solve(r0)
+    sn = BT.NativeBatchSolve(fn, mus, **opts)
+    host_out = torch.empty(tuple(r0.shape), dtype=torch.float64, pin_memory=True)
+    Nn, rn, cn = sn.solve(r0, host_out=host_out)
+    assert np.array_equal(cp, cn)
+    assert np.array_equal(sp.steps, sn.steps), (sp.steps, sn.steps)
+    ok = np.isfinite(Np)
+    assert np.all(np.abs(Nn[ok] - Np[ok]) <= 1e-12 * np.abs(Np[ok]))
+    assert relerr(rn.cpu().numpy(), rp.cpu().numpy()) < 1e-10
+    assert torch.equal(host_out, rn.cpu())
+    assert np.allclose(sn.omega0[ok], sp.omega0[ok], rtol=1e-12, atol=0)
+
+
+def test_native_driver_matches_reference(golden32, fn32):
+    mu = float(golden32["mu"])
+    s = BT.NativeBatchSolve(fn32, np.atleast_1d(mu), method='hybridanderson', nsteps=500, threshold=TIGHT_THR,
+                            criterion=TIGHT_CRIT)
+    N, rho, conv = s.solve(torch.as_tensor(golden32["rho_a"][None], device="cuda"))
+    assert conv[0]
+    assert relerr(rho[0].cpu().numpy(), golden32["and_rho"]) < 1e-9
+    assert scalar_rel(N[0], golden32["and_N"]) < 1e-10
+    assert scalar_rel(s.omega0[0], golden32["and_omega"]) < 1e-10
