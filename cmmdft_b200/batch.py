@@ -1064,10 +1064,10 @@ class NativeBatchSolve(BatchSolve):
         self.omega0 = om
         self.kernel_launches += int(out.launches)
         self.omega_evals += int(out.omega_evals)
-        for b in range(B):
-            for k in range(1, self.nsteps + 2):
-                if not np.isnan(hist[b, k, 0]):
-                    self.history[b].append(tuple(hist[b, k]))
+        steps_max = int(self.steps.max()) if B else 0
+        h = hist[:, 1:steps_max + 1]
+        keep = ~np.isnan(h[:, :, 0])
+        self.history = [list(map(tuple, h[b][keep[b]])) for b in range(B)]
         if self.failed.any():
             raise NoSolutionError("instances %s hit non-finite densities on every retry"
                                   % list(np.where(self.failed)[0]))
