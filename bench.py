@@ -195,8 +195,8 @@ def run_gpu(args):
     # roofline of the fused functional pipeline, from its events in the timed region
     tot_bytes = 0.0
     tot_ms = 0.0
-    for a, b, want, nact in events:
-        tot_ms += a.elapsed_time(b)
+    for a, b, want, nact in events:  # CUDA-event pairs (Python driver) or milliseconds (native driver)
+        tot_ms += a.elapsed_time(b) if b is not None else a
         tot_bytes += pipeline_bytes(fn.plan, want, nact)
     pk = peaks()
     achieved = tot_bytes / (tot_ms / 1e3) / 1e9 if tot_ms > 0 else None

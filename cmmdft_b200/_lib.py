@@ -60,7 +60,8 @@ class SolveWs(ctypes.Structure):
 class SolveOut(ctypes.Structure):
     """cmm_solve_out."""
     _fields_ = [(n, _vp) for n in ("N", "omega", "converged", "steps", "diverged", "failed", "history")] + \
-               [("launches", ctypes.c_longlong), ("omega_evals", ctypes.c_longlong)]
+               [("launches", ctypes.c_longlong), ("omega_evals", ctypes.c_longlong), ("pipe_log", _vp),
+                ("pipe_cap", _i), ("pipe_n", _i)]
 
 
 FALLBACK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,
@@ -82,6 +83,7 @@ _SIGS = {
     "cmm_grid_create": ([c_int, c_int, c_int, P(c_double), P(c_void_p)], c_int),
     "cmm_grid_destroy": ([c_void_p], c_int),
     "cmm_grid_set_staging": ([c_void_p, c_int], c_int),
+    "cmm_part_slots": ([c_void_p], c_int),
     "cmm_grid_spectrum_size": ([c_void_p, P(c_ll), P(c_int)], c_int),
     "cmm_spectrum_index": ([c_void_p, P(c_int), P(c_int), P(c_int)], c_int),
     "cmm_plane_smem_bytes": ([c_void_p, c_int, P(ctypes.c_size_t)], c_int),

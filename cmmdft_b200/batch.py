@@ -1049,6 +1049,9 @@ class NativeBatchSolve(BatchSolve):
         arr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
         out = L.SolveOut(N=arr(N), omega=arr(om), converged=arr(conv), steps=arr(steps), diverged=arr(div),
                          failed=arr(failed), history=arr(hist))
+        if self.pipeline_events is not None:  # CUDA-event times of the full pipeline launches
+            plog = np.zeros((4096, 3))
+            out.pipe_log, out.pipe_cap = arr(plog), len(plog)
         cb = L.FALLBACK_FN(self._native_fallback)
         mu = np.ascontiguousarray(self.mu, dtype=np.float64)
         fug = np.ascontiguousarray(self.fug, dtype=np.float64)
@@ -1064,6 +1067,9 @@ class NativeBatchSolve(BatchSolve):
         self.omega0 = om
         self.kernel_launches += int(out.launches)
         self.omega_evals += int(out.omega_evals)
+        if self.pipeline_events is not None:
+            for want, nact, ms in plog[:out.pipe_n]:
+                self.pipeline_events.append((float(ms), None, int(want), int(nact)))
         steps_max = int(self.steps.max()) if B else 0
         h = hist[:, 1:steps_max + 1]
         keep = ~np.isnan(h[:, :, 0])

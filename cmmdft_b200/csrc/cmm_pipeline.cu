@@ -1497,8 +1497,11 @@ k_ls_n3max(GridDev g, const int* __restrict__ active, const double* __restrict__
 }
 
 // Omega ingredients of rho + alpha_i r for three alphas, one plane per block.
+// FP64-issue bound: three 256-thread blocks per SM (85 registers a thread)
+// keep 24 warps in flight.
+#define CMM_LS_THREADS 256
 template <bool WDA, bool TEN>
-__global__ void __launch_bounds__(CMM_ROW_THREADS)
+__global__ void __launch_bounds__(CMM_LS_THREADS, 3)
 k_ls_omega(GridDev g, const int* __restrict__ active, const double* __restrict__ n3a, long long n3a_stride, double c0, double c1,
            double c2, double R, double lambda3, int version, cmm_wda_eos wda, const double* __restrict__ rho,
            const double* __restrict__ r, const double* __restrict__ V, long long vstride,
@@ -1533,26 +1536,26 @@ k_ls_omega(GridDev g, const int* __restrict__ active, const double* __restrict__
     const double x0 = __ldg(rho + gi), rr = __ldg(r + gi), v = __ldg(V + b * vstride + pbase + i);
     sr += rr;
     srv += rr * v;
-    double n0[nf], n1[nf];
-#pragma unroll
-    for (int f = 0; f < nf; ++f) {
-      n0[f] = __ldg(wd_rho + f * fsr + gi);
-      n1[f] = __ldg(wd_r + f * fsr + gi);
-    }
-#pragma unroll
+    // one alpha at a time (the weighted densities are re-read from L1/L2):
+    // fewer live registers, two blocks per SM without spills
+#pragma unroll 1
     for (int k = 0; k < 3; ++k) {
-      double x = x0 + al[k] * rr;
+      const double a = (k == 0) ? al[0] : (k == 1 ? al[1] : al[2]);
+      double x = x0 + a * rr;
       x = (x < 1e-12) ? 1e-30 : x;  // Solver._clip_density
-      fid[k] += x * (log(lambda3 * x) - 1.0);
+      const double fk = x * (log(lambda3 * x) - 1.0);
       double n[nf];
 #pragma unroll
-      for (int f = 0; f < nf; ++f) n[f] = n0[f] + al[k] * n1[f];
-      phi[k] += fmt_phi<TEN>(n[0], n[1], n[2], n[3], n[4], TEN ? n + tb : nullptr, R, version);
+      for (int f = 0; f < nf; ++f) n[f] = __ldg(wd_rho + f * fsr + gi) + a * __ldg(wd_r + f * fsr + gi);
+      const double pk = fmt_phi<TEN>(n[0], n[1], n[2], n[3], n[4], TEN ? n + tb : nullptr, R, version);
+      double wk = 0.0;
       if constexpr (WDA) {
-        double fv, dfv;
-        wda_eos(wda, n[5], fv, dfv);
-        fw[k] += fv;
+        double dfv;
+        wda_eos(wda, n[5], wk, dfv);
       }
+      if (k == 0) { fid[0] += fk; phi[0] += pk; fw[0] += wk; }
+      else if (k == 1) { fid[1] += fk; phi[1] += pk; fw[1] += wk; }
+      else { fid[2] += fk; phi[2] += pk; fw[2] += wk; }
     }
   }
   __shared__ double red[32];
@@ -1794,6 +1797,15 @@ static int zrow_fmt(const cmm_grid* g, int batch, const int* act, double R, int 
     case 16: return zrow_fmt_m3<16>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
     default: return zrow_fmt_m3<0>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
   }
+}
+
+// Partial-sum slots any pass writes per instance: one per x-plane, or one
+// per column tile of the narrowest column pass (13 fields + rho_hat).
+extern "C" int cmm_part_slots(const cmm_grid* g) {
+  if (!g) return 0;
+  const int tc = col_tile(g, 14);
+  const int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
+  return g->n1 > ntile ? g->n1 : ntile;
 }
 
 extern "C" int cmm_plane_smem_bytes(const cmm_grid* g, int nslot, size_t* bytes) {
@@ -2104,7 +2116,7 @@ static int ls_omega_one(const cmm_grid* g, int batch, const int* act, const doub
                         const double* r, const double* V, long long vstride, const double* wd_rho,
                         const double* wd_r, double* ls_part, int nslot, double* alpha, cudaStream_t st) {
   const size_t fsr = (size_t)batch * g->n1 * g->n2 * g->n3;
-  k_ls_omega<WDA, TEN><<<dim3(g->n1, batch), CMM_ROW_THREADS, 0, st>>>(
+  k_ls_omega<WDA, TEN><<<dim3(g->n1, batch), CMM_LS_THREADS, 0, st>>>(
       g->dev, act, n3a, n3s, c0, c1, c2, R, lambda3, version, we, rho, r, V, vstride, wd_rho, wd_r, fsr, ls_part,
       nslot, alpha);
   return last_err();

@@ -251,6 +251,10 @@ struct Driver {
   int rc = CMM_OK;
   cudaStream_t copy_st = nullptr;        // side stream of the host copies of finished densities
   std::vector<cudaEvent_t> copy_ev;
+  std::vector<char> wd_ok;               // [B][m]: weighted densities of ring slot s stored
+  struct PipeRec { cudaEvent_t a, b; int want, nact; };
+  std::vector<PipeRec> pipe;             // timed full pipeline launches (out->pipe_log)
+  std::vector<char> act_now;             // the active mask last uploaded
 
   double* ring(int s) const { return w->ring + (size_t)s * B * npts; }
   double* rres(int s) const { return w->rres + (size_t)s * B * npts; }
@@ -269,6 +273,7 @@ struct Driver {
   bool cuda(cudaError_t e) { return check(e == cudaSuccess ? CMM_OK : CMM_ERR_CUDA); }
 
   void set_active(const std::vector<char>& mask) {
+    act_now = mask;
     int* h = (int*)stage();
     for (int b = 0; b < B; ++b) h[b] = mask[b] ? 1 : 0;
     cuda(cudaMemcpyAsync(w->active, h, sizeof(int) * B, cudaMemcpyHostToDevice, st));
@@ -295,8 +300,20 @@ struct Driver {
     out->launches += 1;
   }
   void c1(const double* spec, double* chat, int want, double* wd) {
+    PipeRec r{nullptr, nullptr, want, 0};
+    const bool timed = out->pipe_log && (want & 1) && (int)pipe.size() < out->pipe_cap;
+    if (timed) {
+      cuda(cudaEventCreate(&r.a));
+      cuda(cudaEventCreate(&r.b));
+      cuda(cudaEventRecord(r.a, st));
+      for (int b = 0; b < B; ++b) r.nact += act_now.size() == (size_t)B && act_now[b] ? 1 : 0;
+    }
     check(cmm_fmt_c1(g, B, w->active, fn->R, fn->beta, fn->version, fn->wda, fn->d_kst, fn->d_wtab, spec, chat,
                      w->work, w->part, w->nslot, want, wd, st));
+    if (timed) {
+      cuda(cudaEventRecord(r.b, st));
+      pipe.push_back(r);
+    }
     out->launches += (want & 1) ? 3 : 2;
   }
   void residual(const double* chat, const double* rho, double* r_out, const std::vector<int>& hist) {
@@ -373,9 +390,15 @@ struct Driver {
     return h;
   }
 
-  // C1, Omega ingredients and residual of the density in ring slot s_new
-  std::vector<int> post_update(int k, int s_new, const std::vector<char>* ahead) {
-    c1(spec_ring(s_new), w->chat2, 1 | 2 | 4 | 8, wd_ring(s_new));
+  // C1, Omega ingredients and residual of the density in ring slot s_new.
+  // The weighted densities are stored while an instance of `mask` can still
+  // take a hybrid step; later they are regenerated only if needed.
+  std::vector<int> post_update(const std::vector<char>& mask, int k, int s_new, const std::vector<char>* ahead) {
+    bool need = false;
+    for (int b = 0; b < B; ++b) need = need || (mask[b] && !And_true[b]);
+    c1(spec_ring(s_new), w->chat2, 1 | 2 | 4 | (need ? 8 : 0), need ? wd_ring(s_new) : nullptr);
+    for (int b = 0; b < B; ++b)
+      if (mask[b]) wd_ok[(size_t)b * m + s_new] = need ? 1 : 0;
     std::vector<int> hist = valid_hist(k);
     residual(w->chat2, ring(s_new), rres(s_new), hist);
     finalize();
@@ -425,6 +448,8 @@ struct Driver {
       Ncur[b] = s[CMM_STAT_N] * dr;
       std::memcpy(&last[(size_t)b * NST], s, sizeof(double) * NST);
     }
+    std::fill(wd_ok.begin(), wd_ok.end(), 0);
+    for (int b = 0; b < B; ++b) wd_ok[(size_t)b * m] = todo[b];
   }
 
   void finish(int b, int s, double N, int k, bool conv) {
@@ -478,7 +503,7 @@ struct Driver {
     for (int b = 0; b < B; ++b)
       if (mask[b] && ls_slot[b] == s_new) ls_slot[b] = -1;
     mix(coefs, fields, CLIP_DENSITY, ring(s_prev), ring(s_new), spec_ring(s_new));
-    std::vector<int> hist = post_update(k, s_new, nullptr);
+    std::vector<int> hist = post_update(mask, k, s_new, nullptr);
     for (int b = 0; b < B; ++b) {
       ok[b] = 0;
       if (!mask[b]) continue;
@@ -503,6 +528,18 @@ struct Driver {
       anyfresh |= fresh[b] != 0;
     }
     if (anyfresh) {
+      std::vector<char> regen(B, 0);
+      bool anyregen = false;
+      for (int b = 0; b < B; ++b) {
+        regen[b] = fresh[b] && !wd_ok[(size_t)b * m + s_prev];
+        anyregen = anyregen || regen[b];
+      }
+      if (anyregen) {  // weighted densities of rho from its stored spectrum
+        set_active(regen);
+        c1(spec_ring(s_prev), nullptr, 8, wd_ring(s_prev));
+        for (int b = 0; b < B; ++b)
+          if (regen[b]) wd_ok[(size_t)b * m + s_prev] = 1;
+      }
       set_params(n3max.data());
       launch_ls(fresh, s_prev, w->params + 3, 4);
       read(false, true);
@@ -561,7 +598,7 @@ struct Driver {
     std::vector<char> ahead(B, 0);
     if (k + 1 <= 4)
       for (int b = 0; b < B; ++b) ahead[b] = mask[b] && !And_true[b];
-    std::vector<int> hist = post_update(k, s_new, &ahead);
+    std::vector<int> hist = post_update(mask, k, s_new, &ahead);
     for (int b = 0; b < B; ++b)
       if (mask[b]) {
         omega0[b] = omega(&stats_h[(size_t)b * NST], b);
@@ -695,6 +732,7 @@ struct Driver {
     ls_host.assign((size_t)B * NLS, 0.0); alpha_host.assign(B, 0.0);
     res_hist.assign((size_t)B * (o->nsteps + 2), NAN);
     stats_h.assign((size_t)B * NST, 0.0); ls_h.assign((size_t)B * NLS, 0.0); alpha_h.assign(B, 0.0);
+    wd_ok.assign((size_t)B * m, 0);
     for (int b = 0; b < B; ++b) {
       out->N[b] = NAN; out->converged[b] = 0; out->steps[b] = 0; out->diverged[b] = 0; out->failed[b] = 0;
       out->omega[b] = NAN;
@@ -731,6 +769,17 @@ struct Driver {
       cudaStreamDestroy(copy_st);
     }
     for (cudaEvent_t ev : copy_ev) cudaEventDestroy(ev);
+    out->pipe_n = 0;
+    for (const PipeRec& r : pipe) {
+      float ms = 0.0f;
+      if (cudaEventElapsedTime(&ms, r.a, r.b) == cudaSuccess && out->pipe_n < out->pipe_cap) {
+        double* q = out->pipe_log + (size_t)out->pipe_n * 3;
+        q[0] = r.want; q[1] = r.nact; q[2] = ms;
+        out->pipe_n += 1;
+      }
+      cudaEventDestroy(r.a);
+      cudaEventDestroy(r.b);
+    }
     return rc;
   }
 };

@@ -134,7 +134,7 @@ class Buffers(object):
         fs = plan.nspec * 2
         # intermediate spectra of the functional pipeline (Functional.nwork)
         self.work = torch.empty((nwork, batch, fs), dtype=f64, device=dev)
-        self.nslot = max(n1, -(-(n2 * plan.h3) // 1))  # >= ntiles for any column tile >= 1
+        self.nslot = int(L.lib().cmm_part_slots(plan.handle))  # planes or column tiles written per pass
         self.part = torch.zeros((batch, L.NSTAT, self.nslot), dtype=f64, device=dev)
         self.stats = torch.zeros((batch, L.NSTAT), dtype=f64, device=dev)
         self.active = torch.ones(batch, dtype=torch.int32, device=dev)

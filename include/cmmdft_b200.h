@@ -125,6 +125,10 @@ int cmm_grid_destroy(cmm_grid* grid);
  * input is read-only, take a stream-ordered temporary of one spectrum per
  * instance (cudaMallocAsync / cudaFreeAsync on the call's stream). */
 int cmm_grid_set_staging(cmm_grid* grid, int mode);
+/* Smallest `nslot` of the partial-sum arrays d_part / d_ls_part: every pass
+ * writes at most this many slots per instance (one per x-plane or column
+ * tile); a larger nslot works and only costs the reductions. */
+int cmm_part_slots(const cmm_grid* grid);
 /* Number of stored frequencies per instance (N1*N2*H3) and H3. */
 int cmm_grid_spectrum_size(const cmm_grid* grid, long long* nspec, int* h3);
 /* Frequency indices (0..N-1 per axis) at each stored position:
@@ -352,6 +356,9 @@ typedef struct cmm_solve_out {
   double* history;              /* optional [B][nsteps + 2][3] (N, RES, RIUE per step), or NULL */
   long long launches;           /* kernel launches issued */
   long long omega_evals;
+  double* pipe_log;             /* optional [pipe_cap][3]: (want, active instances, ms) per full
+                                   functional-pipeline launch, CUDA-event timed (NULL: not timed) */
+  int pipe_cap, pipe_n;
 } cmm_solve_out;
 
 /* The line search's SLSQP fallback (solver.py:437-447) is delegated to the
