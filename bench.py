@@ -158,7 +158,7 @@ def run_gpu(args):
     def one_solve(events=None):
         s = BT.GroupedSolve(fn, mus, groups=args.groups, native=args.driver == "native", method="hybridanderson",
                             nsteps=args.max_iters,
-                            threshold=THRESH, criterion="res", divergence_guard=True)
+                            threshold=THRESH, criterion="res", divergence_guard=True, anderson_coefs=args.coefs)
         s.pipeline_events = events
         N, rho, conv = s.solve(rho0)
         return s, conv
@@ -215,14 +215,14 @@ def run_gpu(args):
         out = None
         for _ in range(args.warmup):   # warm-up: pinned result buffers, plan tables, workspaces
             out = ISO.solve_isotherm(host, pressures, T, guest, NPTS, threshold=THRESH, groups=args.groups,
-                                     native=args.driver == "native")
+                                     native=args.driver == "native", anderson_coefs=args.coefs)
         barrier()
         t0 = time.perf_counter()
         h2d = d2h = 0
         ne = 0
         for _ in range(args.steps):
             out = ISO.solve_isotherm(host, pressures, T, guest, NPTS, threshold=THRESH, groups=args.groups,
-                                     native=args.driver == "native")
+                                     native=args.driver == "native", anderson_coefs=args.coefs)
             ne += int(out["converged"].sum())
             h2d += host.pos.nbytes + host.ffatype_ids.nbytes + 2 * 8 * len(host.ffatypes)
             d2h += out["rho"].nbytes + out["N"].nbytes
@@ -243,7 +243,7 @@ def run_gpu(args):
         for i in range(NPRESS):
             cls = BT.NativeBatchSolve if args.driver == "native" else BT.BatchSolve
             s = cls(fn, mus[i:i + 1], method="hybridanderson", nsteps=args.max_iters,
-                              threshold=THRESH, criterion="res", divergence_guard=True)
+                    threshold=THRESH, criterion="res", divergence_guard=True, anderson_coefs=args.coefs)
             N, rho, conv = s.solve(rho0[i:i + 1])
             npl += int(conv.sum())
             pit += int(s.steps.sum())
@@ -266,7 +266,7 @@ def run_gpu(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": "isotherm-64cubed", "grid": list(NPTS), "host": "cubic a=17A 276 atoms seed 0",
                        "points_per_isotherm": NPRESS, "pressures_bar": [1e-3, 100.0], "solver": "hybridanderson m=5",
-                       "instance_groups": args.groups, "driver": args.driver,
+                       "instance_groups": args.groups, "driver": args.driver, "anderson_coefs": args.coefs,
                        "tolerance": "RES<1e-8", "start": "Ninit=rho_bulk", "iterations_per_isotherm": iters,
                        "converged_points": nconv, "steps_per_point": per_point,
                        "diverged_points": diverged,
@@ -370,6 +370,9 @@ def main():
     ap.add_argument("--groups", type=int, default=1, help="instance groups on concurrent streams")
     ap.add_argument("--driver", choices=("native", "python"), default="native",
                     help="batched loop in the library (cmm_solve_batched) or in Python")
+    ap.add_argument("--coefs", choices=("slsqp", "exact"), default="slsqp",
+                    help="Anderson coefficients: the reference's SLSQP (same trajectory and result as the "
+                         "reference) or the exact simplex minimiser (fewer steps, not the reference's result)")
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-plain", action="store_true")

@@ -30,6 +30,7 @@ class WdaEos(ctypes.Structure):
 CLIP_NONE, CLIP_PICARD, CLIP_DENSITY = 0, 1, 2
 SOLVE_HYBRID, SOLVE_ANDERSON, SOLVE_HYBRIDANDERSON = 1, 2, 3
 CRIT_RES, CRIT_RIUE, CRIT_DER = 0, 1, 2
+COEF_SLSQP, COEF_EXACT = 0, 1
 
 _vp, _d, _i = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
 
@@ -45,7 +46,7 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [("method", _i), ("nsteps", _i), ("m", _i), ("ncrit", _i), ("crit", _i * 3), ("thr", _d * 3),
                 ("alpha_mix", _d), ("damping", _d), ("delta", _d), ("damping_max", _d), ("damping_min", _d),
                 ("damping_up", _d), ("damping_down", _d), ("adaptive_damping", _i), ("divergence_guard", _i),
-                ("a_tol", _d), ("r_tol", _d), ("ls_thresh", _d), ("kjmol", _d)]
+                ("a_tol", _d), ("r_tol", _d), ("ls_thresh", _d), ("kjmol", _d), ("coefs", _i)]
 
 
 class SolveWs(ctypes.Structure):
@@ -104,6 +105,7 @@ _SIGS = {
                       c_void_p, c_void_p], c_int),
     "cmm_ls_finalize": ([c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p], c_int),
     "cmm_solve_stage_bytes": ([c_int], ctypes.c_size_t),
+    "cmm_anderson_slsqp": ([P(c_double), c_int, P(c_double), P(c_int), P(c_int)], c_int),
     "cmm_solve_batched": ([P(FunctionalDesc), P(SolveOpts), c_int, c_void_p, c_void_p, c_void_p, P(SolveWs),
                            P(SolveOut), FALLBACK_FN, c_void_p, c_void_p], c_int),
     "cmm_fmt_weights": ([c_void_p, c_double, c_void_p, c_void_p], c_int),

@@ -15,10 +15,14 @@ Control flow restated from cmmdft/solver.py:
   Picard.update_rho_hybrid         :403-457 (+ _get_alpha_max :150-165)
   Anderson.update_rho              :546-579
   Anderson.update_rho_Anderson     :581-604 (+ damping :537-544)
-The Anderson mixing coefficients minimise ||sum a_i r_i|| subject to
-a_i >= 0, sum a_i = 1 exactly (active-set enumeration on the Gram matrix)
-instead of through SLSQP; both target the same minimiser.
+The Anderson mixing coefficients are the reference's SLSQP iterate
+(anderson_coefs='slsqp', default: Kraft's SLSQP restated in
+cmm_anderson_slsqp on the Gram matrix of the residuals), or with
+anderson_coefs='exact' the exact minimiser of ||sum a_i r_i|| subject to
+a_i >= 0, sum a_i = 1 (support enumeration on the Gram matrix), which
+converges in fewer steps but leaves the reference's trajectory.
 """
+import ctypes
 import itertools
 
 import numpy as np
@@ -81,6 +85,23 @@ def _supports(n):
         rows = [[(k >> i) & 1 for i in range(n)] for k in range(1, 1 << n)]
         _SUPPORTS[n] = np.array(rows, dtype=bool)
     return _SUPPORTS[n]
+
+
+def anderson_slsqp(gram):
+    """SLSQP mixing coefficients of one instance (cmm_anderson_slsqp).
+
+    gram [n, n] = <r_i, r_j>, oldest residual first.  Returns (alpha, mode,
+    iterations) with SLSQP's exit mode (0 converged, 8, 9); alpha is its last
+    iterate whatever the mode, as solver.py:589-591 takes ``.x``.
+    """
+    G = np.ascontiguousarray(gram, dtype=np.float64)
+    n = G.shape[0]
+    a = np.empty(n)
+    mode, nit = ctypes.c_int(0), ctypes.c_int(0)
+    dp = ctypes.POINTER(ctypes.c_double)
+    L.check(L.lib().cmm_anderson_slsqp(G.ctypes.data_as(dp), n, a.ctypes.data_as(dp), ctypes.byref(mode),
+                                       ctypes.byref(nit)), "cmm_anderson_slsqp")
+    return a, mode.value, nit.value
 
 
 def simplex_qp_batched(M):
@@ -262,8 +283,11 @@ class BatchSolve(object):
     def __init__(self, fn, chempots, method='hybridanderson', nsteps=500, threshold=1e-6,
                  criterion='res', alpha_mix=0.1, m=5, damping=0.3, delta=0.2, damping_max=0.8,
                  damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5), divergence_guard=False,
-                 a_tol=1e-6, r_tol=1e-4, group=0):
+                 a_tol=1e-6, r_tol=1e-4, group=0, anderson_coefs='slsqp'):
         self.fn = fn
+        if anderson_coefs not in ('slsqp', 'exact'):
+            raise ValueError("anderson_coefs must be 'slsqp' or 'exact'")
+        self.anderson_coefs = anderson_coefs
         self.host_out = None
         self.plan = fn.plan
         self.mu = np.asarray(chempots, dtype=np.float64).ravel()
@@ -729,7 +753,11 @@ class BatchSolve(object):
         slots = [j % m for j in range(k - mk, k)]  # oldest .. newest
         coefs = np.zeros((B, 2 * mk))
         idx = np.where(mask)[0]
-        alphas = simplex_qp_batched(self.gram[idx][:, slots][:, :, slots])
+        grams = self.gram[idx][:, slots][:, :, slots]
+        if self.anderson_coefs == 'exact':
+            alphas = simplex_qp_batched(grams)
+        else:   # update_rho_Anderson's SLSQP (solver.py:585-591)
+            alphas = np.stack([anderson_slsqp(G)[0] for G in grams]) if len(idx) else np.zeros((0, mk))
         if self.adaptive:  # _get_damping_coefficient (solver.py:537-544)
             r = np.sqrt(self.rnorm2[idx, s_prev])
             p = np.sqrt(self.rnorm2[idx, (k - 2) % m]) if k >= 2 else np.zeros(len(idx))
@@ -1017,7 +1045,8 @@ class NativeBatchSolve(BatchSolve):
                            damping_max=self.damping_max, damping_min=self.damping_min,
                            damping_up=self.dfac[0], damping_down=self.dfac[1],
                            adaptive_damping=int(bool(self.adaptive)), divergence_guard=int(self.divergence_guard),
-                           a_tol=self.tol[0], r_tol=self.tol[1], ls_thresh=self.thresh, kjmol=kjmol)
+                           a_tol=self.tol[0], r_tol=self.tol[1], ls_thresh=self.thresh, kjmol=kjmol,
+                           coefs=L.COEF_EXACT if self.anderson_coefs == 'exact' else L.COEF_SLSQP)
         for i, (c, t) in enumerate(zip(self.criteria, self.thresholds)):
             opts.crit[i] = crit[c]
             opts.thr[i] = t

@@ -16,6 +16,9 @@
 
 #include "cmm_common.cuh"
 
+// SLSQP mixing coefficients (cmm_anderson.cu)
+int anderson_slsqp(const double* G, int n, double* x, int* nit_out);
+
 namespace {
 
 constexpr int NST = CMM_NSTAT;
@@ -482,7 +485,8 @@ struct Driver {
       const double* G = &gram[(size_t)b * m * m];
       for (int i = 0; i < mk; ++i)
         for (int j = 0; j < mk; ++j) Msub[i * mk + j] = G[slots[i] * m + slots[j]];
-      simplex_qp(Msub, mk, al);
+      if (o->coefs == CMM_COEF_EXACT) simplex_qp(Msub, mk, al);
+      else anderson_slsqp(Msub, mk, al, nullptr);   // update_rho_Anderson's SLSQP (solver.py:585-591)
       if (o->adaptive_damping) {  // _get_damping_coefficient (solver.py:537-544)
         const double r = std::sqrt(rnorm2[(size_t)b * m + s_prev]);
         const double p = (k >= 2) ? std::sqrt(rnorm2[(size_t)b * m + (k - 2) % m]) : 0.0;
@@ -798,6 +802,7 @@ extern "C" int cmm_solve_batched(const cmm_functional_desc* fn, const cmm_solve_
   if (opt->method != CMM_SOLVE_HYBRID && opt->method != CMM_SOLVE_ANDERSON && opt->method != CMM_SOLVE_HYBRIDANDERSON)
     return CMM_ERR_UNSUPPORTED;
   if (opt->ncrit < 1 || opt->ncrit > 3 || opt->nsteps < 1) return CMM_ERR_ARG;
+  if (opt->coefs != CMM_COEF_SLSQP && opt->coefs != CMM_COEF_EXACT) return CMM_ERR_ARG;
   if (!ws->h_stats || !ws->h_ls || !ws->h_alpha || !ws->h_stage) return CMM_ERR_ARG;
   Driver d;
   d.fn = fn; d.o = opt; d.B = batch; d.w = ws; d.out = out; d.fb = fallback; d.fbctx = fallback_ctx;

@@ -19,7 +19,8 @@ __all__ = ['solve_isotherm', 'excess_loading']
 
 def solve_isotherm(host, pressures, temperature, guest, npoints, method='hybridanderson', threshold=1e-8,
                    criterion='res', nsteps=500, start='bulk', version='WBII', tailcorrections=False,
-                   return_density=True, fn=None, m=5, alpha_mix=0.1, divergence_guard=True, groups=1, native=True):
+                   return_density=True, fn=None, m=5, alpha_mix=0.1, divergence_guard=True, groups=1, native=True,
+                   anderson_coefs='slsqp'):
     """Solve the adsorption isotherm of a spherical LJ guest in ``host``.
 
     pressures: array in atomic units (e.g. ``np.logspace(-3, 2, 24) * bar``).
@@ -29,6 +30,10 @@ def solve_isotherm(host, pressures, temperature, guest, npoints, method='hybrida
     decisions of one group overlap the device work of another).
     native: run the batched loop in the library (cmm_solve_batched); False
     runs the Python driver (the same kernels and decisions).
+    anderson_coefs: 'slsqp' takes the reference's SLSQP coefficients (same
+    trajectory and result as the reference at any tolerance); 'exact' the
+    exact simplex minimiser (fewer steps, a different point within the
+    tolerance).
     Returns a dict with mu, rho_bulk, N (absolute loading per cell),
     converged, steps, omega and (optionally) the densities [B, N1, N2, N3].
     """
@@ -38,7 +43,8 @@ def solve_isotherm(host, pressures, temperature, guest, npoints, method='hybrida
     mus, bulks = W.isotherm_inputs(pressures, temperature, guest)
     rho0 = W.initial_density(fn, mus, ninit=bulks if start == 'bulk' else None)
     s = BT.GroupedSolve(fn, mus, groups=groups, native=native, method=method, nsteps=nsteps, threshold=threshold,
-                        criterion=criterion, m=m, alpha_mix=alpha_mix, divergence_guard=divergence_guard)
+                        criterion=criterion, m=m, alpha_mix=alpha_mix, divergence_guard=divergence_guard,
+                        anderson_coefs=anderson_coefs)
     # densities land in pinned host memory while the rest of the batch iterates
     host = torch.empty(tuple(rho0.shape), dtype=torch.float64, pin_memory=True) if return_density else None
     N, rho, conv = s.solve(rho0, host_out=host)

@@ -304,6 +304,10 @@ typedef struct cmm_functional_desc {
 
 enum { CMM_SOLVE_HYBRID = 1, CMM_SOLVE_ANDERSON = 2, CMM_SOLVE_HYBRIDANDERSON = 3 };
 enum { CMM_CRIT_RES = 0, CMM_CRIT_RIUE = 1, CMM_CRIT_DER = 2 };
+/* Anderson coefficients: the reference's SLSQP (solver.py:585-591, restated
+ * in cmm_anderson_slsqp) or the exact minimiser of ||sum a_i r_i|| on the
+ * simplex (fewer steps; trajectories then differ from the reference's). */
+enum { CMM_COEF_SLSQP = 0, CMM_COEF_EXACT = 1 };
 
 typedef struct cmm_solve_opts {
   int method;                   /* CMM_SOLVE_* */
@@ -316,6 +320,7 @@ typedef struct cmm_solve_opts {
   double a_tol, r_tol;          /* DER tolerances */
   double ls_thresh;             /* 1 kJ/mol: line-search fallback threshold (Hartree) */
   double kjmol;                 /* 1 kJ/mol in Hartree */
+  int coefs;                    /* CMM_COEF_* */
 } cmm_solve_opts;
 
 /* Buffers of one solve (device, except the h_* pinned host arrays).
@@ -360,6 +365,16 @@ typedef struct cmm_solve_out {
                                    functional-pipeline launch, CUDA-event timed (NULL: not timed) */
   int pipe_cap, pipe_n;
 } cmm_solve_out;
+
+/* Anderson mixing coefficients of one instance as Anderson.update_rho_Anderson
+ * computes them (cmmdft/solver.py:581-591): scipy's SLSQP from a = 1/n with
+ * tol 1e-10 on sum_res(a) = ||sum_i a_i r_i||, bounds [0, 1], sum a = 1 --
+ * restated on the host from Kraft's algorithm with scipy's 2-point finite
+ * differences, the objective taken as sqrt(a^T G a) from the Gram matrix
+ * gram [n][n] = <r_i, r_j> (oldest residual first, n <= 8).  *mode receives
+ * SLSQP's exit mode (0 converged, 8 no descent direction, 9 iteration limit);
+ * alpha is SLSQP's last iterate in every case, as the reference uses it. */
+int cmm_anderson_slsqp(const double* gram, int n, double* alpha, int* mode, int* nit);
 
 /* The line search's SLSQP fallback (solver.py:437-447) is delegated to the
  * caller: minimise Omega((1-a) rho + a G) over a in [0.01, 0.9] alpha_max for

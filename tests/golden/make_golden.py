@@ -4,6 +4,7 @@ Run in the build container only (the reference tree is not present on GPU
 machines):
 
     python tests/golden/make_golden.py [--reference /root/reference] [--skip64]
+    python tests/golden/make_golden.py --iso64 [--procs 8]
 
 The reference is imported from its own source tree through the import shims
 in ``tests/golden/refshim`` (molmod units/constants backed by
@@ -20,6 +21,11 @@ Outputs (small ``.npz`` files) land next to this script:
               tight hybrid-Anderson solution, tail-corrected MFA.
   c1_64.npz   64^3 cubic host: V summary and tight hybrid-Anderson solutions
               at three pressures (scalars + one density field).
+  iso64_res8.npz  the 24-pressure 64^3 isotherm (1e-3..100 bar) solved as
+              the reference's example does it: hybrid Anderson m=5 to
+              RES < 1e-8 from Ninit = rho_bulk; N, Omega, steps and the
+              convergence flag per pressure (``--iso64`` only; one process
+              per pressure).
 """
 
 import argparse
@@ -109,11 +115,55 @@ def quiet(fn, *a, **k):
         return fn(*a, **k)
 
 
+ISO_PRESSURES = np.logspace(-3, 2, 24)
+
+
+def _iso64_point(task):
+    ref_root, i = task
+    ref = import_reference(ref_root)
+    solver = ref[2]
+    from cmmdft_b200.hosts import cubic_host_276
+    from cmmdft_b200.units import bar, boltzmann
+    T = 300.0
+    P = ISO_PRESSURES[i]
+    b = quiet(build, ref, 64, cubic_host_276(seed=0), T, P, tempfile.mkdtemp(prefix='cmm_iso64_'))
+    mb, V = b['mbwr'], b['fe'].part_dict['ExtPot'].potential
+    mb.set_temperature(T)
+    bulk = np.nanmin(mb.solve_densities_from_chempots([b['mu']]), axis=1)[0]
+    rho0 = bulk * np.exp(-np.maximum(V, 0) / boltzmann / T)
+    s = solver.Anderson(b['prog'], nsteps=500, m=5, criterion='res', threshold=1e-8)
+    t0 = time.time()
+    try:
+        N, rho, conv = quiet(s.solve, b['mu'], rho0, 3)
+    except Exception as e:  # noqa: BLE001 - recorded, not raised
+        print('P=%g bar: %s' % (P, e), flush=True)
+        return i, b['mu'], bulk, np.nan, np.nan, s.curr_step, False
+    print('iso64 P=%.4g bar: N=%.12e steps=%d conv=%s (%.0f s)' % (P, N, s.curr_step, conv, time.time() - t0),
+          flush=True)
+    return i, b['mu'], bulk, N, s.omega0, s.curr_step, bool(conv)
+
+
+def iso64(args):
+    import multiprocessing as mp
+    with mp.get_context('spawn').Pool(args.procs) as pool:
+        res = sorted(pool.map(_iso64_point, [(args.reference, i) for i in range(len(ISO_PRESSURES))]))
+    cols = list(zip(*res))
+    out = dict(pressures=ISO_PRESSURES, mu=np.array(cols[1]), rho_bulk=np.array(cols[2]), N=np.array(cols[3]),
+               omega=np.array(cols[4]), steps=np.array(cols[5]), converged=np.array(cols[6]),
+               threshold=1e-8, criterion='res', m=5)
+    np.savez_compressed(os.path.join(HERE, 'iso64_res8.npz'), **out)
+    print('wrote iso64_res8.npz')
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--reference', default='/root/reference')
     ap.add_argument('--skip64', action='store_true')
+    ap.add_argument('--iso64', action='store_true')
+    ap.add_argument('--procs', type=int, default=8)
     args = ap.parse_args()
+    if args.iso64:
+        return iso64(args)
     ref = import_reference(args.reference)
     solver = ref[2]
     from cmmdft_b200.hosts import cubic_host_276, HELIUM

@@ -11,6 +11,8 @@ Tolerances (stated per check):
   * Free-energy parts: 1e-11 relative.
   * Converged densities: 1e-9 relative to max rho at RES < 1e-11; the
     loading N and grand potential to 1e-9 relative.
+  * The 24-pressure 64^3 isotherm at the reference's tolerance (RES < 1e-8):
+    the same number of steps per pressure, N and Omega to 1e-10 relative.
 """
 import numpy as np
 import pytest
@@ -410,6 +412,39 @@ def test_native_driver_equals_python_driver(cuda, method, case):
     assert relerr(rn.cpu().numpy(), rp.cpu().numpy()) < 1e-10
     assert torch.equal(host_out, rn.cpu())
     assert np.allclose(sn.omega0[ok], sp.omega0[ok], rtol=1e-12, atol=0)
+
+
+@pytest.fixture(scope="module")
+def iso64():
+    import os
+    path = os.path.join(os.path.dirname(__file__), "golden", "iso64_res8.npz")
+    if not os.path.exists(path):
+        pytest.skip("isotherm fixture not generated")
+    return dict(np.load(path))
+
+
+@pytest.mark.parametrize("native", [True, False])
+def test_isotherm64_at_reference_tolerance(cuda, iso64, native):
+    """The 24-pressure 64^3 isotherm as the reference's example solves it
+    (hybrid Anderson m=5, RES < 1e-8, Ninit = rho_bulk).  At this tolerance
+    the result depends on the whole trajectory, SLSQP coefficients included:
+    every pressure the reference converges takes the same number of steps and
+    reaches N and Omega within 1e-10; the three it does not converge (it
+    diverges there) are retired as not converged by the divergence guard."""
+    guest = methane_guest_params()
+    fn = W.build_functional(cubic_host_276(0), (64, 64, 64), 300.0, guest)
+    mus, bulks = W.isotherm_inputs(iso64["pressures"] * bar, 300.0, guest)
+    assert np.array_equal(mus, iso64["mu"])
+    r0 = W.initial_density(fn, mus, ninit=bulks)
+    cls = BT.NativeBatchSolve if native else BT.BatchSolve
+    s = cls(fn, mus, method='hybridanderson', nsteps=500, threshold=1e-8, criterion='res', divergence_guard=True)
+    N, rho, conv = s.solve(r0)
+    ok = iso64["converged"].astype(bool)
+    assert np.array_equal(np.asarray(conv, dtype=bool), ok)
+    assert np.array_equal(s.steps[ok], iso64["steps"][ok]), (s.steps, iso64["steps"])
+    for i in np.where(ok)[0]:
+        assert scalar_rel(N[i], iso64["N"][i]) < 1e-10, i
+        assert scalar_rel(s.omega0[i], iso64["omega"][i]) < 1e-10, i
 
 
 def test_native_driver_matches_reference(golden32, fn32):
