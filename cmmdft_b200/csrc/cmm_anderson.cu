@@ -20,8 +20,8 @@
 //
 // The QP subproblem (min 1/2 s^T B s + g^T s, sum s = -c, -x <= s <= 1-x) is
 // strictly convex, so its solution does not depend on the method; it is
-// solved exactly by enumerating the supports of x + s on the simplex (the
-// upper bounds are implied by x + s >= 0 and sum (x + s) = 1).
+// solved exactly on the support of x + s that satisfies the KKT conditions
+// (the upper bounds are implied by x + s >= 0 and sum (x + s) = 1).
 #include <cmath>
 #include <cstring>
 
@@ -88,56 +88,113 @@ bool dense_solve(double* A, double* b, int N) {
   return true;
 }
 
-// min 1/2 s^T B s + g^T s  s.t.  sum s = sig, s >= -x; s and the equality
-// multiplier lam (B s + g = lam 1 on the free variables).  Lowest objective
-// over the supports whose solution is feasible.
-bool qp_subproblem(const double* B, const double* g, const double* x, double sig, int n, double* s, double* lam) {
-  bool found = false;
-  double best = 0.0;
-  const unsigned K = 1u << n;
-  for (unsigned S = 1; S < K; ++S) {
-    int idx[NMAX], k = 0;
-    double rest = 0.0;
-    double sv[NMAX];
-    for (int i = 0; i < n; ++i) {
-      if ((S >> i) & 1u) idx[k++] = i;
-      else { sv[i] = -x[i]; rest += x[i]; }
-    }
-    const int N = k + 1;
-    double A[(NMAX + 1) * (NMAX + 1)], r[NMAX + 1];
-    for (int a = 0; a < k; ++a) {
-      const int i = idx[a];
-      double t = g[i];
-      for (int j = 0; j < n; ++j)
-        if (!((S >> j) & 1u)) t += B[i * n + j] * sv[j];
-      r[a] = -t;
-      for (int b = 0; b < k; ++b) A[a * N + b] = B[i * n + idx[b]];
-      A[a * N + k] = -1.0;
-      A[k * N + a] = 1.0;
-    }
-    A[k * N + k] = 0.0;
-    r[k] = sig + rest;
-    if (!dense_solve(A, r, N)) continue;
-    bool feasible = true;
-    for (int a = 0; a < k; ++a) {
-      sv[idx[a]] = r[a];
-      if (!(r[a] >= -x[idx[a]] - 1e-14)) feasible = false;
-    }
-    if (!feasible) continue;
-    double obj = 0.0;
-    for (int i = 0; i < n; ++i) {
-      double t = 0.0;
-      for (int j = 0; j < n; ++j) t += B[i * n + j] * sv[j];
-      obj += sv[i] * (0.5 * t + g[i]);
-    }
-    if (!found || obj < best) {
-      found = true;
-      best = obj;
-      std::memcpy(s, sv, sizeof(double) * n);
-      *lam = r[k];
+// Equality-constrained minimiser of the QP on support S (variables outside S
+// at their lower bound s_i = -x_i): the bordered system
+// [B_SS -1; 1^T 0][s_S; lam] = [-(g_S + B_SN s_N); sig + sum_N x_i].
+// Returns false for a singular system; *primal: s_S >= -x_S; *dual: the
+// multipliers (B s + g)_i - lam of the bounds outside S are >= 0.
+bool support_solve(const double* B, const double* g, const double* x, double sig, int n, unsigned S,
+                   double* sv, double* lam, bool* primal, bool* dual, int* drop, int* add) {
+  int idx[NMAX], k = 0;
+  double rest = 0.0;
+  for (int i = 0; i < n; ++i) {
+    if ((S >> i) & 1u) idx[k++] = i;
+    else { sv[i] = -x[i]; rest += x[i]; }
+  }
+  const int N = k + 1;
+  double A[(NMAX + 1) * (NMAX + 1)], r[NMAX + 1];
+  for (int a = 0; a < k; ++a) {
+    const int i = idx[a];
+    double t = g[i];
+    for (int j = 0; j < n; ++j)
+      if (!((S >> j) & 1u)) t += B[i * n + j] * sv[j];
+    r[a] = -t;
+    for (int b = 0; b < k; ++b) A[a * N + b] = B[i * n + idx[b]];
+    A[a * N + k] = -1.0;
+    A[k * N + a] = 1.0;
+  }
+  A[k * N + k] = 0.0;
+  r[k] = sig + rest;
+  if (!dense_solve(A, r, N)) return false;
+  *primal = true;
+  double worst = 0.0;
+  for (int a = 0; a < k; ++a) {
+    sv[idx[a]] = r[a];
+    const double viol = -x[idx[a]] - r[a];
+    if (!(r[a] >= -x[idx[a]] - 1e-14)) {
+      if (*primal || viol > worst) { worst = viol; *drop = idx[a]; }
+      *primal = false;
     }
   }
-  if (!found) return false;
+  *lam = r[k];
+  double gmax = std::fabs(r[k]);
+  for (int i = 0; i < n; ++i) gmax = std::fmax(gmax, std::fabs(g[i]));
+  *dual = true;
+  double most = 0.0;
+  for (int i = 0; i < n; ++i) {
+    if ((S >> i) & 1u) continue;
+    double t = g[i];
+    for (int j = 0; j < n; ++j) t += B[i * n + j] * sv[j];
+    const double mult = t - r[k];
+    if (mult < -1e-12 * gmax) {
+      if (*dual || mult < most) { most = mult; *add = i; }
+      *dual = false;
+    }
+  }
+  return true;
+}
+
+double qp_objective(const double* B, const double* g, const double* sv, int n) {
+  double obj = 0.0;
+  for (int i = 0; i < n; ++i) {
+    double t = 0.0;
+    for (int j = 0; j < n; ++j) t += B[i * n + j] * sv[j];
+    obj += sv[i] * (0.5 * t + g[i]);
+  }
+  return obj;
+}
+
+// min 1/2 s^T B s + g^T s  s.t.  sum s = sig, s >= -x (the unique minimiser
+// of a strictly convex QP).  The support that satisfies the KKT conditions
+// is searched from *hint (the previous subproblem's support): a variable
+// below its bound leaves the support, else the bound with the most negative
+// multiplier is released, for at most 2n trials; when that does not settle
+// (or rounding leaves no support passing both tests) every support is tried
+// and the first passing both, else the lowest objective over the
+// primal-feasible ones, is taken.  s and the equality multiplier lam.
+bool qp_subproblem(const double* B, const double* g, const double* x, double sig, int n, double* s, double* lam,
+                   unsigned* hint) {
+  const unsigned K = 1u << n;
+  double sv[NMAX], lv;
+  bool primal, dual, done = false;
+  int drop = -1, add = -1;
+  unsigned S = (*hint > 0 && *hint < K) ? *hint : K - 1;
+  for (int trial = 0; trial < 2 * n && S > 0; ++trial) {
+    if (!support_solve(B, g, x, sig, n, S, sv, &lv, &primal, &dual, &drop, &add)) break;
+    if (primal && dual) { done = true; break; }
+    S = primal ? (S | (1u << add)) : (S & ~(1u << drop));
+  }
+  if (done) {
+    std::memcpy(s, sv, sizeof(double) * n);
+    *lam = lv;
+    *hint = S;
+  } else {
+    bool found = false, kkt = false;
+    double best = 0.0;
+    for (unsigned T = 1; T < K && !kkt; ++T) {
+      if (!support_solve(B, g, x, sig, n, T, sv, &lv, &primal, &dual, &drop, &add) || !primal) continue;
+      const double obj = qp_objective(B, g, sv, n);
+      if (dual || !found || obj < best) {
+        found = true;
+        kkt = dual;
+        best = obj;
+        std::memcpy(s, sv, sizeof(double) * n);
+        *lam = lv;
+        *hint = T;
+      }
+    }
+    if (!found) return false;
+  }
   for (int i = 0; i < n; ++i) s[i] = std::fmin(std::fmax(s[i], -x[i]), 1.0 - x[i]);
   return true;
 }
@@ -245,6 +302,7 @@ int anderson_slsqp(const double* G, int n, double* x, int* nit_out) {
   double c = sum_minus_one(x, n);
   double mu = 0.0, f0 = fx;
   int it = 0, ireset = 1, mode = 9;
+  unsigned support = (1u << n) - 1;   // x = 1/n: every variable free
   ldl_reset(L, n);
   auto relaxed = [&]() {
     return ((std::fabs(fx - f0) < TOL || norm2(s, n) < TOL) && std::fabs(c) < TOL) ? 0 : 8;
@@ -253,7 +311,7 @@ int anderson_slsqp(const double* G, int n, double* x, int* nit_out) {
     if (++it > MAXITER) { mode = 9; break; }
     ldl_dense(L, n, B);
     double r;
-    if (!qp_subproblem(B, g, x, -c, n, s, &r)) { mode = -2; break; }
+    if (!qp_subproblem(B, g, x, -c, n, s, &r, &support)) { mode = -2; break; }
     for (int i = 0; i < n; ++i) vg[i] = g[i] - r;
     f0 = fx;
     std::memcpy(x0, x, sizeof(double) * n);
@@ -286,8 +344,7 @@ int anderson_slsqp(const double* G, int n, double* x, int* nit_out) {
     if ((std::fabs(fx - f0) < ACC || norm2(s, n) < ACC) && std::fabs(c) < ACC) { mode = 0; break; }
     fd_gradient(f, x, fx, g);
     // damped BFGS on the Lagrangian gradient difference (the multiplier
-    // terms cancel: the constraint is linear)
-    ldl_dense(L, n, B);
+    // terms cancel: the constraint is linear); B still holds L D L^T
     double sv = 0.0, sBs = 0.0;
     for (int i = 0; i < n; ++i) {
       u[i] = g[i] - r - vg[i];

@@ -10,8 +10,14 @@
 // Host arithmetic follows the Python expressions operation by operation
 // (IEEE double, no contraction on the host).
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <condition_variable>
 #include <cstring>
+#include <functional>
+#include <memory>
+#include <mutex>
+#include <thread>
 #include <vector>
 
 #include "cmm_common.cuh"
@@ -229,6 +235,79 @@ void grid_parabola(double c, double b, double a0, double hi, double* aopt, doubl
 
 bool isclose0(double a) { return std::fabs(a) <= 1e-8; }   // np.isclose(a, 0)
 
+// A few host threads for per-instance work between two read-backs (the
+// Anderson coefficients of every instance are independent).  run(n, f) calls
+// f(i) for i < n on the workers and the calling thread and returns when all
+// workers have checked in; items are claimed from one atomic counter.
+class HostPool {
+ public:
+  explicit HostPool(int nthreads) {
+    try {
+      for (int i = 0; i < nthreads; ++i) th_.emplace_back([this] { worker(); });
+    } catch (...) {
+      shutdown();   // threads already started are joined before the error propagates
+      throw;
+    }
+  }
+  ~HostPool() { shutdown(); }
+  void shutdown() {
+    {
+      std::lock_guard<std::mutex> l(m_);
+      stop_ = true;
+    }
+    cv_.notify_all();
+    for (auto& t : th_)
+      if (t.joinable()) t.join();
+  }
+  void run(int n, const std::function<void(int)>& f) {
+    if (th_.empty() || n < 4) {
+      for (int i = 0; i < n; ++i) f(i);
+      return;
+    }
+    {
+      std::lock_guard<std::mutex> l(m_);
+      job_ = &f;
+      n_ = n;
+      next_.store(0);
+      pending_ = (int)th_.size();
+      ++gen_;
+    }
+    cv_.notify_all();
+    for (int i; (i = next_.fetch_add(1)) < n;) f(i);
+    std::unique_lock<std::mutex> l(m_);
+    done_.wait(l, [this] { return pending_ == 0; });
+    job_ = nullptr;
+  }
+
+ private:
+  void worker() {
+    long seen = 0;
+    for (;;) {
+      const std::function<void(int)>* job;
+      int n;
+      {
+        std::unique_lock<std::mutex> l(m_);
+        cv_.wait(l, [&] { return stop_ || gen_ != seen; });
+        if (stop_) return;
+        seen = gen_;
+        job = job_;
+        n = n_;
+      }
+      for (int i; (i = next_.fetch_add(1)) < n;) (*job)(i);
+      std::lock_guard<std::mutex> l(m_);
+      if (--pending_ == 0) done_.notify_one();
+    }
+  }
+  std::vector<std::thread> th_;
+  std::mutex m_;
+  std::condition_variable cv_, done_;
+  const std::function<void(int)>* job_ = nullptr;
+  int n_ = 0, pending_ = 0;
+  long gen_ = 0;
+  bool stop_ = false;
+  std::atomic<int> next_{0};
+};
+
 struct Driver {
   const cmm_functional_desc* fn;
   const cmm_solve_opts* o;
@@ -258,6 +337,7 @@ struct Driver {
   struct PipeRec { cudaEvent_t a, b; int want, nact; };
   std::vector<PipeRec> pipe;             // timed full pipeline launches (out->pipe_log)
   std::vector<char> act_now;             // the active mask last uploaded
+  std::unique_ptr<HostPool> pool;        // SLSQP coefficients of several instances at once
 
   double* ring(int s) const { return w->ring + (size_t)s * B * npts; }
   double* rres(int s) const { return w->rres + (size_t)s * B * npts; }
@@ -479,14 +559,24 @@ struct Driver {
     std::vector<int> slots;
     for (int j = k - mk; j < k; ++j) slots.push_back(j % m);
     std::vector<double> coefs((size_t)B * MAXF, 0.0);
-    double Msub[64], al[8];
-    for (int b = 0; b < B; ++b) {
-      if (!mask[b]) continue;
+    std::vector<int> todo;
+    for (int b = 0; b < B; ++b)
+      if (mask[b]) todo.push_back(b);
+    std::vector<double> als((size_t)B * 8);
+    auto coef_of = [&](int t) {
+      const int b = todo[t];
       const double* G = &gram[(size_t)b * m * m];
+      double Msub[64];
       for (int i = 0; i < mk; ++i)
         for (int j = 0; j < mk; ++j) Msub[i * mk + j] = G[slots[i] * m + slots[j]];
+      double* al = &als[(size_t)b * 8];
       if (o->coefs == CMM_COEF_EXACT) simplex_qp(Msub, mk, al);
       else anderson_slsqp(Msub, mk, al, nullptr);   // update_rho_Anderson's SLSQP (solver.py:585-591)
+    };
+    if (pool) pool->run((int)todo.size(), coef_of);
+    else for (int t = 0; t < (int)todo.size(); ++t) coef_of(t);
+    for (int b : todo) {
+      const double* al = &als[(size_t)b * 8];
       if (o->adaptive_damping) {  // _get_damping_coefficient (solver.py:537-544)
         const double r = std::sqrt(rnorm2[(size_t)b * m + s_prev]);
         const double p = (k >= 2) ? std::sqrt(rnorm2[(size_t)b * m + (k - 2) % m]) : 0.0;
@@ -722,6 +812,15 @@ struct Driver {
     anderson = o->method == CMM_SOLVE_ANDERSON || o->method == CMM_SOLVE_HYBRIDANDERSON;
     pure = o->method == CMM_SOLVE_ANDERSON;
     if (!anderson) m = 2;
+    if (anderson && o->coefs == CMM_COEF_SLSQP && B >= 8) {
+      const unsigned hw = std::thread::hardware_concurrency();
+      const int nt = (int)std::min(3u, hw > 1 ? hw - 1 : 0u);
+      try {
+        if (nt > 0) pool.reset(new HostPool(nt));
+      } catch (const std::exception&) {
+        pool.reset();   // no threads: the coefficients are computed inline
+      }
+    }
     dr = g->volume / (double)npts;
     beta = fn->beta;
     slot_bytes = stage_slot_bytes(B);
