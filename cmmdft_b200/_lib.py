@@ -31,6 +31,7 @@ CLIP_NONE, CLIP_PICARD, CLIP_DENSITY = 0, 1, 2
 SOLVE_HYBRID, SOLVE_ANDERSON, SOLVE_HYBRIDANDERSON = 1, 2, 3
 CRIT_RES, CRIT_RIUE, CRIT_DER = 0, 1, 2
 COEF_SLSQP, COEF_EXACT = 0, 1
+BICG_RHO, BICG_ALPHA, BICG_OMEGA, BICG_BETA, BICG_D0, BICG_D1, BICG_RR, BICG_FIRST, BICG_NS = range(9)
 
 _vp, _d, _i = ctypes.c_void_p, ctypes.c_double, ctypes.c_int
 
@@ -106,6 +107,14 @@ _SIGS = {
     "cmm_ls_finalize": ([c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p], c_int),
     "cmm_solve_stage_bytes": ([c_int], ctypes.c_size_t),
     "cmm_anderson_slsqp": ([P(c_double), c_int, P(c_double), P(c_int), P(c_int)], c_int),
+    "cmm_fmt_hvp": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_void_p, c_void_p, c_void_p,
+                     c_void_p, c_void_p, c_void_p], c_int),
+    "cmm_extpot_lj_grad": ([c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_double, c_double,
+                            c_double, c_double, c_void_p, c_void_p], c_int),
+    "cmm_contract": ([c_void_p, c_ll, c_int, c_void_p, c_ll, c_int, c_ll, c_void_p, c_int, c_void_p], c_int),
+    "cmm_bicg_vec": ([c_int, c_ll, c_int, c_void_p, c_void_p, c_void_p, c_double, c_void_p, c_void_p, c_void_p,
+                      c_void_p, c_void_p, c_void_p, c_void_p, c_int, c_void_p], c_int),
+    "cmm_bicg_scalars": ([c_int, c_void_p, c_void_p, c_int, c_void_p, c_int, c_void_p], c_int),
     "cmm_solve_batched": ([P(FunctionalDesc), P(SolveOpts), c_int, c_void_p, c_void_p, c_void_p, P(SolveWs),
                            P(SolveOut), FALLBACK_FN, c_void_p, c_void_p], c_int),
     "cmm_fmt_weights": ([c_void_p, c_double, c_void_p, c_void_p], c_int),

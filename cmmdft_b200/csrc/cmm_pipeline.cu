@@ -14,6 +14,7 @@
 #include <cstring>
 
 #include "cmm_common.cuh"
+#include "cmm_dual.cuh"
 
 // --------------------------------------------------------- shared tables --
 // Plane layout in shared memory: nslot fields interleaved by row,
@@ -653,12 +654,17 @@ COL_BACKCONV_KERNEL(k_col_backconv_wda_t, true, true)
 
 // ===================================== plane pass: dPhi/dn (White-Bear) ==
 // Arithmetic of _phi*, _dphi*, get_phi and _get_dphi_* (cmmdft/functionals.py:620-767).
-struct PhiOut { double gs, g3, gv[3], phi; };
+// The pointwise functions are templates on the scalar type: double for the
+// functional, Dual (cmm_dual.cuh) for its directional derivative in the
+// Hessian-vector product.
+template <class S>
+struct PhiOutT { S gs, g3, gv[3], phi; };
+using PhiOut = PhiOutT<double>;
 
-__device__ __forceinline__ void phi_funcs(double n3, double ln, double n32, double n33, int base,
-                                          double& p2, double& dp2, double& p3, double& dp3) {
-  const double q = (1 - 2 * n3 + n32);
-  const double c = (1 - 3 * n3 + 3 * n32 - n33);
+template <class S>
+__device__ __forceinline__ void phi_funcs(S n3, S ln, S n32, S n33, int base, S& p2, S& dp2, S& p3, S& dp3) {
+  const S q = (1 - 2 * n3 + n32);
+  const S c = (1 - 3 * n3 + 3 * n32 - n33);
   if (base == CMM_FMT) {
     p2 = 1 / (1.0 - n3);
     dp2 = 1 / q;
@@ -691,24 +697,23 @@ __device__ __forceinline__ void phi_funcs(double n3, double ln, double n32, doub
 
 // Prefactor of phi3 (functionals.py:629-639): n2^3 (1 - xi)^3 ('a') or
 // n2^3 - 3 n2 |nv2|^2, plus the tensor terms 9/2 (nv2 T nv2 - tr T^3) ('t').
-template <bool TEN>
-__device__ __forceinline__ double fmt_pref3(double n2, double vx, double vy, double vz, double vv, const double* T,
-                                            bool anti, double& xi) {
-  double pref3;
+template <bool TEN, class S>
+__device__ __forceinline__ S fmt_pref3(S n2, S vx, S vy, S vz, S vv, const S* T, bool anti, S& xi) {
+  S pref3;
   xi = 0.0;
   if (anti) {
     xi = vv / (n2 * n2 + 1e-16);
     xi = fmin(fmax(xi, 0.0), 1.0);
-    const double om = 1 - xi;
+    const S om = 1 - xi;
     pref3 = (n2 * n2 * n2) * (om * om * om);
   } else {
     pref3 = n2 * n2 * n2 - 3.0 * n2 * vv;
   }
   if constexpr (TEN) {
-    const double xx = T[0], xy = T[1], xz = T[2], yy = T[3], yz = T[4], zz = T[5];
-    const double quad = xx * (vx * vx) + yy * (vy * vy) + zz * (vz * vz) + 2 * xy * vx * vy + 2 * xz * vx * vz +
-                        2 * yz * vy * vz;
-    const double tr3 = (xx * xx * xx + yy * yy * yy + zz * zz * zz) +
+    const S xx = T[0], xy = T[1], xz = T[2], yy = T[3], yz = T[4], zz = T[5];
+    const S quad = xx * (vx * vx) + yy * (vy * vy) + zz * (vz * vz) + 2 * xy * vx * vy + 2 * xz * vx * vz +
+                   2 * yz * vy * vz;
+    const S tr3 = (xx * xx * xx + yy * yy * yy + zz * zz * zz) +
                        3 * (xx * xy * xy + xx * xz * xz + yy * xy * xy + yy * yz * yz + zz * xz * xz + zz * yz * yz) +
                        6 * xy * xz * yz;
     pref3 += 4.5 * quad;
@@ -750,60 +755,60 @@ __device__ __forceinline__ double fmt_phi(double n0, double n3raw, double vx, do
   phi_values(n3, ln, n32, n33, version & 3, p2, p3);
   const double vv = vx * vx + vy * vy + vz * vz;
   const double uv = (vx * i4r) * vx + (vy * i4r) * vy + (vz * i4r) * vz;
-  const double pref3 = fmt_pref3<TEN>(n2, vx, vy, vz, vv, T, (version & CMM_ANTISYM) != 0, xi);
+  const double pref3 = fmt_pref3<TEN, double>(n2, vx, vy, vz, vv, T, (version & CMM_ANTISYM) != 0, xi);
   const double s12 = n1 * n2 - uv;
   return n0 * (-ln) + s12 * p2 + pref3 * p3;
 }
 
 // With TEN, T holds the tensor densities (xx, xy, xz, yy, yz, zz) and gT
 // receives dPhi/dn_T (functionals.py:634-639, 669-674, 692-717).
-template <bool TEN>
-__device__ __forceinline__ PhiOut fmt_point(double n0, double n3raw, double vx, double vy, double vz,
-                                            const double* T, double* gT, double R, int version) {
-  const double n1 = R * n0;
-  const double n2 = (4.0 * M_PI * R * R) * n0;
+template <bool TEN, class S>
+__device__ __forceinline__ PhiOutT<S> fmt_point(S n0, S n3raw, S vx, S vy, S vz, const S* T, S* gT, double R,
+                                                int version) {
+  const S n1 = R * n0;
+  const S n2 = (4.0 * M_PI * R * R) * n0;
   const double i4r = 1.0 / (4 * M_PI * R);
-  const double ux = vx * i4r, uy = vy * i4r, uz = vz * i4r;  // nv1
-  const double n3 = fmin(fmax(n3raw, 1e-30), 0.99);
-  const double ln = log(1 - n3);
-  const double n32 = n3 * n3, n33 = n32 * n3;
+  const S ux = vx * i4r, uy = vy * i4r, uz = vz * i4r;  // nv1
+  const S n3 = fmin(fmax(n3raw, 1e-30), 0.99);
+  const S ln = log(1 - n3);
+  const S n32 = n3 * n3, n33 = n32 * n3;
   const int base = version & 3;
   const bool anti = (version & CMM_ANTISYM) != 0;
-  double p2, dp2, p3, dp3;
+  S p2, dp2, p3, dp3;
   phi_funcs(n3, ln, n32, n33, base, p2, dp2, p3, dp3);
-  const double p1 = -ln, dp1 = 1.0 / (1.0 - n3);
-  const double vv = vx * vx + vy * vy + vz * vz;
-  const double uv = ux * vx + uy * vy + uz * vz;
-  double xi;
-  const double pref3 = fmt_pref3<TEN>(n2, vx, vy, vz, vv, T, anti, xi);
-  const double s12 = n1 * n2 - uv;
-  PhiOut o;
+  const S p1 = -ln, dp1 = 1.0 / (1.0 - n3);
+  const S vv = vx * vx + vy * vy + vz * vz;
+  const S uv = ux * vx + uy * vy + uz * vz;
+  S xi;
+  const S pref3 = fmt_pref3<TEN, S>(n2, vx, vy, vz, vv, T, anti, xi);
+  const S s12 = n1 * n2 - uv;
+  PhiOutT<S> o;
   o.phi = n0 * p1 + s12 * p2 + pref3 * p3;
-  const double d0 = p1;
-  const double d1 = n2 * p2;
-  double d2 = n1 * p2;
+  const S d0 = p1;
+  const S d1 = n2 * p2;
+  S d2 = n1 * p2;
   if (anti) d2 += (3 * (n2 * n2) * (1 + xi) * ((1 - xi) * (1 - xi))) * p3;
   else d2 += 3 * (n2 * n2 - vv) * p3;
-  const double d3 = n0 * dp1 + s12 * dp2 + pref3 * dp3;
-  const double f3 = anti ? (-6 * n2 * ((1 - xi) * (1 - xi)) * p3) : (-6 * n2 * p3);
+  const S d3 = n0 * dp1 + s12 * dp2 + pref3 * dp3;
+  const S f3 = anti ? (-6 * n2 * ((1 - xi) * (1 - xi)) * p3) : (-6 * n2 * p3);
   // dPhi/dnv1 = -nv2 p2 ; dPhi/dnv2 = -nv1 p2 + nv2 f3
   o.gs = d0 + R * d1 + (4.0 * M_PI * R * R) * d2;
   o.g3 = d3;
-  const double v[3] = {vx, vy, vz}, u[3] = {ux, uy, uz};
-  double tv[3] = {0.0, 0.0, 0.0};  // 2 T v, the gradient of the quadratic form
+  const S v[3] = {vx, vy, vz}, u[3] = {ux, uy, uz};
+  S tv[3] = {0.0, 0.0, 0.0};  // 2 T v, the gradient of the quadratic form
   if constexpr (TEN) {
     tv[0] = 2 * (T[0] * vx + T[1] * vy + T[2] * vz);
     tv[1] = 2 * (T[1] * vx + T[3] * vy + T[4] * vz);
     tv[2] = 2 * (T[2] * vx + T[4] * vy + T[5] * vz);
   }
   for (int a = 0; a < 3; ++a) {
-    const double dv1 = -v[a] * p2;
-    double dv2 = -u[a] * p2 + v[a] * f3;
+    const S dv1 = -v[a] * p2;
+    S dv2 = -u[a] * p2 + v[a] * f3;
     if constexpr (TEN) dv2 += 4.5 * tv[a] * p3;
     o.gv[a] = dv1 * i4r + dv2;
   }
   if constexpr (TEN) {
-    const double xx = T[0], xy = T[1], xz = T[2], yy = T[3], yz = T[4], zz = T[5];
+    const S xx = T[0], xy = T[1], xz = T[2], yy = T[3], yz = T[4], zz = T[5];
     gT[0] = 4.5 * (vx * vx - 3 * (xx * xx + xy * xy + xz * xz)) * p3;
     gT[1] = 4.5 * ((vx * vy - 3 * (xx * xy + yy * xy + xz * yz)) * 2) * p3;
     gT[2] = 4.5 * ((vx * vz - 3 * (xx * xz + zz * xz + xy * yz)) * 2) * p3;
@@ -846,7 +851,7 @@ __device__ __forceinline__ void plane_fmt_body(GridDev g, const int* __restrict_
     if (want & 8)  // the weighted densities themselves (hybrid line search)
       for (int f = 0; f < ns; ++f) wd[f * fsr + roff + i] = rel(s, sh, ns, f, r, j);
     if (do_phi) {
-      PhiOut o = fmt_point<false>(a0, a3, ax, ay, az, nullptr, nullptr, R, version);
+      PhiOut o = fmt_point<false, double>(a0, a3, ax, ay, az, nullptr, nullptr, R, version);
       phi += o.phi;
       if (do_c1) {
         a0 = o.gs; a3 = o.g3; ax = o.gv[0]; ay = o.gv[1]; az = o.gv[2];
@@ -1082,7 +1087,7 @@ k_zrow_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm
       double T[6], gT[6];
       if constexpr (TEN)
         for (int q = 0; q < 6; ++q) T[q] = zrow_rel<M3C>(g, s, nf, tb + q, r, j);
-      PhiOut o = fmt_point<TEN>(a0, a3, ax, ay, az, T, gT, R, version);
+      PhiOut o = fmt_point<TEN, double>(a0, a3, ax, ay, az, T, gT, R, version);
       phi += o.phi;
       if (do_c1) {
         a0 = o.gs; a3 = o.g3; ax = o.gv[0]; ay = o.gv[1]; az = o.gv[2];
@@ -1797,6 +1802,131 @@ static int zrow_fmt(const cmm_grid* g, int batch, const int* act, double R, int 
     case 16: return zrow_fmt_m3<16>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
     default: return zrow_fmt_m3<0>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
   }
+}
+
+// ============================================ Hessian-vector product ==
+// z rows of the second-derivative step: the weighted densities of v (y
+// already inverted) arrive in the slots, those of rho are read from wdrho
+// (stored by the functional pass, want bit 3); the pointwise step is the
+// directional derivative of dPhi/dn at n(rho) along n(v), fmt_point
+// evaluated in Dual arithmetic.  Its fields go out z-forward (y forward
+// follows), in the layout of the dPhi spectra of k_zrow_fmt.
+template <int M3C, bool TEN>
+__global__ void __launch_bounds__(CMM_ROW_THREADS)
+k_zrow_hvp(GridDev g, const int* __restrict__ active, double R, int version, const double2* __restrict__ win,
+           size_t fs, double2* __restrict__ gout, int chunk, const double* __restrict__ wdrho, size_t fsr) {
+  const int i1 = blockIdx.x, b = blockIdx.y;
+  if (active && !active[b]) return;
+  constexpr int nf = 5 + (TEN ? 6 : 0);
+  const int h3 = M3C ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
+  PlaneSmem s = zrow_smem_setup<M3C>(g, nf * chunk);
+  const size_t poff = ((size_t)b * g.n1 + i1) * n2 * h3;
+  const size_t roff = ((size_t)b * g.n1 + i1) * n2 * n3;
+  for (int r0 = 0; r0 < n2; r0 += chunk) {
+    const int nr = min(chunk, n2 - r0);
+    for (int f = 0; f < nf; ++f) zrow_load<M3C>(g, s, nf, f, nr, win + f * fs + poff + (size_t)r0 * h3);
+    __syncthreads();
+    zrow_inverse<M3C>(g, s, nf * nr);
+    for (int i = threadIdx.x; i < nr * n3; i += blockDim.x) {
+      const int r = i / n3, j = i - r * n3;
+      const size_t q = roff + (size_t)(r0 + r) * n3 + j;
+      Dual n[nf], gT[6];
+      for (int f = 0; f < nf; ++f) n[f] = Dual(__ldg(wdrho + f * fsr + q), zrow_rel<M3C>(g, s, nf, f, r, j));
+      const PhiOutT<Dual> o = fmt_point<TEN, Dual>(n[0], n[1], n[2], n[3], n[4], TEN ? n + 5 : nullptr, gT, R,
+                                                   version);
+      zrow_rel<M3C>(g, s, nf, 0, r, j) = o.gs.d;
+      zrow_rel<M3C>(g, s, nf, 1, r, j) = o.g3.d;
+      zrow_rel<M3C>(g, s, nf, 2, r, j) = o.gv[0].d;
+      zrow_rel<M3C>(g, s, nf, 3, r, j) = o.gv[1].d;
+      zrow_rel<M3C>(g, s, nf, 4, r, j) = o.gv[2].d;
+      if constexpr (TEN)
+        for (int t = 0; t < 6; ++t) zrow_rel<M3C>(g, s, nf, 5 + t, r, j) = gT[t].d;
+    }
+    __syncthreads();
+    zrow_forward<M3C>(g, s, nf * nr);
+    for (int f = 0; f < nf; ++f) zrow_store<M3C>(g, s, nf, f, nr, gout + f * fs + poff + (size_t)r0 * h3);
+    __syncthreads();
+  }
+}
+
+template <int M3C, bool TEN>
+static int zrow_hvp_one(const cmm_grid* g, int batch, const int* act, double R, int version, const double2* win,
+                        size_t fs, double2* gout, int chunk, const double* wdrho, cudaStream_t st) {
+  constexpr int nf = 5 + (TEN ? 6 : 0);
+  const size_t sb = zrow_smem_bytes_g(g, nf * chunk);
+  int rc;
+  if ((rc = set_smem((const void*)k_zrow_hvp<M3C, TEN>, sb))) return rc;
+  k_zrow_hvp<M3C, TEN><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(
+      g->dev, act, R, version, win, fs, gout, chunk, wdrho, (size_t)batch * g->n1 * g->n2 * g->n3);
+  return last_err();
+}
+
+template <int M3C>
+static int zrow_hvp_m3(const cmm_grid* g, int batch, const int* act, double R, int version, const double2* win,
+                       size_t fs, double2* gout, int chunk, const double* wdrho, cudaStream_t st) {
+  if (version & CMM_TENSOR)
+    return zrow_hvp_one<M3C, true>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st);
+  return zrow_hvp_one<M3C, false>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st);
+}
+
+// Spectrum of A v = d C1 / d rho . v (Hartree per density unit), A the
+// Hessian of the excess free energy per grid volume: hard-sphere part
+// through the second derivatives of Phi at the stored weighted densities of
+// rho, plus the MFA convolution K v (the external potential does not depend
+// on rho).  The y/z steps run in the staged form for every grid shape.
+extern "C" int cmm_fmt_hvp(const cmm_grid* g, int batch, const int* d_active, double R, double beta, int version,
+                           const double* d_kst, const double* d_wtab, const double* d_wd_rho,
+                           const double* d_vhat, double* d_out_hat, double* d_work, void* stream) {
+  if (!g || batch < 1 || !d_kst || !d_vhat || !d_out_hat || !d_work) return CMM_ERR_ARG;
+  if (version & CMM_WDA) return CMM_ERR_UNSUPPORTED;
+  const bool ten = (version & CMM_TENSOR) != 0;
+  const int nf = 5 + (ten ? 6 : 0);
+  cudaStream_t st = (cudaStream_t)stream;
+  const size_t fs = (size_t)batch * g->n1 * g->n2 * g->h3;
+  double2* wbuf = (double2*)d_work;
+  double2* gbuf = wbuf + (ten ? 12 : 6) * fs;
+  const double npts = (double)g->n1 * g->n2 * g->n3;
+  const int tc = col_tile(g, nf + 1);
+  const int ntile = cmm_div_up((long long)g->n2 * g->h3, tc);
+  const double2* wt = (const double2*)d_wtab;
+  const int ck = col_kind(g);
+  if (version & CMM_NOHS) {
+    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), col_smem_bytes(g->n1, tc, 6, g->ax1.big), st, g->dev,
+               d_active, R, 1.0 / (beta * npts), (const double2*)nullptr, fs, (const double2*)d_vhat,
+               (const double2*)d_kst, wt, (double2*)d_out_hat, tc, 0.0, 1.0 / npts);
+    return last_err();
+  }
+  if (!d_wd_rho) return CMM_ERR_ARG;
+  const size_t csw = col_smem_bytes(g->n1, tc, nf, g->ax1.big), csb = col_smem_bytes(g->n1, tc, nf + 1, g->ax1.big);
+  if (ten)
+    LAUNCH_COL(ck, k_col_weights_t, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
+               (const double2*)d_vhat, wbuf, fs, (const double2*)d_kst, wt, (double*)nullptr, 0, 0, tc, 0.0,
+               (const double2*)nullptr, (double*)nullptr);
+  else
+    LAUNCH_COL(ck, k_col_weights, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
+               (const double2*)d_vhat, wbuf, fs, (const double2*)d_kst, wt, (double*)nullptr, 0, 0, tc, 0.0,
+               (const double2*)nullptr, (double*)nullptr);
+  int rc = last_err();
+  if (rc) return rc;
+  if ((rc = ypass(g, batch, d_active, wbuf, wbuf, fs, nf, 1, st))) return rc;
+  const int chunk = zrow_chunk(g, nf);
+  if (chunk < 1) return CMM_ERR_SMEM;
+  switch (zrow_m3(g)) {
+    case 32: rc = zrow_hvp_m3<32>(g, batch, d_active, R, version, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
+    case 16: rc = zrow_hvp_m3<16>(g, batch, d_active, R, version, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
+    default: rc = zrow_hvp_m3<0>(g, batch, d_active, R, version, wbuf, fs, gbuf, chunk, d_wd_rho, st);
+  }
+  if (rc) return rc;
+  if ((rc = ypass(g, batch, d_active, gbuf, gbuf, fs, nf, 0, st))) return rc;
+  if (ten)
+    LAUNCH_COL(ck, k_col_backconv_t, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),
+               (const double2*)gbuf, fs, (const double2*)d_vhat, (const double2*)d_kst, wt, (double2*)d_out_hat,
+               tc, 0.0, 1.0 / npts);
+  else
+    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),
+               (const double2*)gbuf, fs, (const double2*)d_vhat, (const double2*)d_kst, wt, (double2*)d_out_hat,
+               tc, 0.0, 1.0 / npts);
+  return last_err();
 }
 
 // Partial-sum slots any pass writes per instance: one per x-plane, or one

@@ -134,3 +134,8 @@ def methane_guest_params():
     """(sigma, epsilon, mass) of the methane guest in atomic units."""
     return (METHANE["sigma"] * angstrom, METHANE["epsilon_K"] * boltzmann,
             METHANE["mass"] * amu)
+
+
+def cubic_host_779(seed=0):
+    """The 276-atom cell's atom density at a = 24.0 angstrom (779 atoms, 96^3)."""
+    return random_sequential_host((24.0, 24.0, 24.0), 779, seed)

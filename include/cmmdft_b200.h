@@ -366,6 +366,55 @@ typedef struct cmm_solve_out {
   int pipe_cap, pipe_n;
 } cmm_solve_out;
 
+/* ---------------------------------------------------------------------
+ * Derivatives at a converged density (implicit adjoint; the reference has no
+ * derivatives -- its users difference whole solves).
+ * ------------------------------------------------------------------- */
+/* Spectrum of A v, A = d C1 / d rho the Hessian of the excess free energy
+ * (hard-sphere + MFA; C1 in Hartree, so A v is in Hartree per density unit),
+ * for `batch` yz-spectra d_vhat.  d_wd_rho: the real-space weighted
+ * densities of rho [nwd][B][npts] stored by cmm_fmt_c1 with want bit 3; the
+ * hard-sphere second derivatives are taken there.  With d_kst conjugated the
+ * MFA term becomes its transpose.  d_work: nwork spectra as for cmm_fmt_c1.
+ * CMM_WDA: CMM_ERR_UNSUPPORTED. */
+int cmm_fmt_hvp(const cmm_grid* grid, int batch, const int* d_active, double R, double beta, int version,
+                const double* d_kst, const double* d_wtab, const double* d_wd_rho, const double* d_vhat,
+                double* d_out_hat, double* d_work, void* stream);
+
+/* Parameter derivatives of the capped LJ external potential (arguments as
+ * cmm_extpot_lj): d_dV [2 + 2 ntype][npts], rows dV/d(guest eps),
+ * dV/d(guest sigma), dV/d(eps_t) for each host type, dV/d(sigma_t) for each
+ * host type; zero where the potential is capped.  ntype <= 8. */
+int cmm_extpot_lj_grad(const cmm_grid* grid, const double* d_pos, const int* d_type, int natom,
+                       const double* d_type_sig, const double* d_type_eps, int ntype, double guest_sig,
+                       double guest_eps, double cutoff, double v_cap, double* d_dV, void* stream);
+
+/* d_part[(w K + k) nchunk + c] = partial sums over chunk c of the n points of
+ * W[w] * D[k] (row strides ldw, ldd); the caller sums over c. */
+int cmm_contract(const double* d_W, long long ldw, int nw, const double* d_D, long long ldd, int K, long long n,
+                 double* d_part, int nchunk, void* stream);
+
+/* Vector steps of the batched BiCGSTAB on (I + c S A^T S) y = rhs,
+ * S = diag(sqrt(max(rho, 0))), fields [batch][npts], scalars d_sc
+ * [batch][CMM_BICG_NS] (CMM_BICG_FIRST = 1 before the first step):
+ *   op 0: out = S x
+ *   op 1: out = x + c S y, partial dots (out . a, out . out)
+ *   op 2: out (p) = x (r) + beta (out - omega y (v))
+ *   op 3: out (s) = x (r) - alpha y (v)
+ *   op 4: out (solution) += alpha x (p) + omega y (s); out2 (r) = y - omega a (t);
+ *         partial dots (rhat . r, r . r)
+ * Partial dots go to d_part [batch][2][nblk]. */
+enum { CMM_BICG_RHO = 0, CMM_BICG_ALPHA = 1, CMM_BICG_OMEGA = 2, CMM_BICG_BETA = 3, CMM_BICG_D0 = 4,
+       CMM_BICG_D1 = 5, CMM_BICG_RR = 6, CMM_BICG_FIRST = 7, CMM_BICG_NS = 8 };
+int cmm_bicg_vec(int op, long long npts, int batch, const int* d_active, const double* d_rho, const double* d_sc,
+                 double c, const double* d_x, const double* d_y, const double* d_a, double* d_out, double* d_out2,
+                 const double* d_rhat, double* d_part, int nblk, void* stream);
+/* Sum the partial dots (fixed order) and advance the scalars: stage 0 after
+ * op 4 (rho, beta, r . r), 1 after the product of p (alpha), 2 after the
+ * product of s (omega). */
+int cmm_bicg_scalars(int batch, const int* d_active, const double* d_part, int nblk, double* d_sc, int stage,
+                     void* stream);
+
 /* Anderson mixing coefficients of one instance as Anderson.update_rho_Anderson
  * computes them (cmmdft/solver.py:581-591): scipy's SLSQP from a = 1/n with
  * tol 1e-10 on sum_res(a) = ||sum_i a_i r_i||, bounds [0, 1], sum a = 1 --

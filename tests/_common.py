@@ -19,11 +19,11 @@ def scalar_rel(a, b):
     return abs(float(a) - float(b)) / max(abs(float(b)), 1e-300)
 
 
-def oracle_case(npts=32, T=300.0, host=None, V=None, hs_version='WBII', tail=False):
+def oracle_case(npts=32, T=300.0, host=None, V=None, hs_version='WBII', tail=False, guest=None):
     """Oracle functional for the 276-atom cubic host at ``npts``^3."""
     from oracle import cmm_oracle as O
     host = cubic_host_276(0) if host is None else host
-    sig, eps, mass = methane_guest_params()
+    sig, eps, mass = methane_guest_params() if guest is None else guest
     grid = O.OGrid(host.rvecs, npoints=npts)
     if V is None:
         pos = host.recentred_pos()
