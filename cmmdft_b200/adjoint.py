@@ -11,27 +11,41 @@ scalar Q(rho*, theta) has
 
 J = dE/drho = diag(1/rho) + beta A, A = dC1/drho the Hessian of the excess
 free energy.  A v is one pass of the functional pipeline with the pointwise
-step replaced by its directional derivative (cmm_fmt_hvp); A^T differs from
-A only in the MFA term, whose kernel spectrum carries the reference's
-exp(i pi scalprod) phase (a translated, non-symmetric kernel), so A^T uses
-the conjugate spectrum.  The adjoint system is solved in the scaled form
-(I + beta S A^T S) y = S rhs, S = diag(sqrt(rho)), lambda = S y, by a batched
-BiCGSTAB whose vector steps and scalars stay on the device (cmm_bicg_*).
+step replaced by its directional derivative (cmm_fmt_hvp).  A is not
+symmetric: the MFA kernel spectrum carries the reference's exp(i pi
+scalprod) phase (a translated kernel; A^T uses the conjugate spectrum), and
+where n3 is clipped the reference's dPhi/dn3 is taken at the clipped value
+(cmm_fmt_hvp's transpose mode handles those points).  The adjoint system
+is solved in the scaled form (I + beta S A^T S) y = S rhs, S = diag(sqrt(rho)),
+lambda = S y, by a batched BiCGSTAB whose vector steps and scalars stay on the
+device (cmm_bicg_*).
 
 Outputs per instance and parameter theta = (guest epsilon, guest sigma,
 epsilon and sigma of every host atom type):
   * N = integral rho: right-hand side dV 1;
   * Omega (Solver._get_Omega, :103-119): the reference's MFA derivative is
     K rho while its value is 1/2 rho^T K rho, so Omega is not stationary at
-    the fixed point; its adjoint right-hand side is dV (K^T - K) rho / 2
-    (plus the clipped ideal term, below);
+    the fixed point (dOmega/drho = dV (K^T - K) rho / 2 there, plus the
+    terms of its clipped ideal part); the right-hand side is formed term by
+    term;
   * the excess uptake N - rho_bulk He V_cell (Calculator.return_loading,
     cmmdft/calculator.py:114-138) adds the EOS bulk density and the helium
     void fraction.
 Explicit derivatives: dV/dtheta analytically on the device
-(cmm_extpot_lj_grad); the hard-sphere radius and MFA kernel (guest sigma and
-epsilon only) and the EOS mu(P) and rho_bulk(P) by central differences of
-those explicit functions (relative step ``fd_rel``).  The iterative solve
+(cmm_extpot_lj_grad).  The guest parameters also enter the hard-sphere part
+through R_hs(sigma, epsilon) and the MFA kernel: the hard-sphere C1 and F_HS
+are differentiated in R by fourth-order central differences (relative step
+``fd_rel`` = 1e-3, truncation ~1e-12; a smaller step would amplify the
+rounding noise C1 carries where the packing fraction is tiny) and chained
+with dR/dtheta; the MFA kernel is linear in epsilon (exact) and is differenced
+in sigma with a relative step of 1e-7 (its cut at r = sigma makes it jump
+when a grid point crosses; a step that small almost never meets one, and
+the convolution carries no cancellation noise).  mu(P) and rho_bulk(P)
+come from root solves of the EOS whose tolerance makes them step-like at
+the 1e-9 level, so they are differentiated implicitly: with rho* the root
+of p(rho; theta) = P, d rho*/d theta = -p_theta / p_rho and
+d mu/d theta = mu_theta + mu_rho d rho*/d theta, the partials taken by
+central differences of the closed-form p and mu.  The iterative DFT solve
 itself is never differentiated by finite differences.
 """
 import numpy as np
@@ -121,8 +135,8 @@ def hvp(fn, wd_rho, v, transpose=False, work=None):
     if work is None:
         work = torch.empty((fn.nwork, B, plan.nspec * 2), dtype=torch.float64, device="cuda")
     kst = _conj_spectrum(fn.kst) if transpose else fn.kst
-    check(L.lib().cmm_fmt_hvp(plan.handle, B, None, fn.R, fn.beta, fn.version, ptr(kst), ptr(fn.wtab), ptr(wd_rho),
-                              ptr(vhat), ptr(out), ptr(work), _stream()), "cmm_fmt_hvp")
+    check(L.lib().cmm_fmt_hvp(plan.handle, B, None, fn.R, fn.beta, fn.version, int(transpose), ptr(kst),
+                              ptr(fn.wtab), ptr(wd_rho), ptr(vhat), ptr(out), ptr(work), _stream()), "cmm_fmt_hvp")
     return plan.irfft_yz(out)
 
 
@@ -155,7 +169,7 @@ class _BiCGStab(object):
         vhat = self.plan.rfft_yz(self.u.view((self.B,) + self.plan.npoints))
         out = self.plan.new_spec(self.B)
         fn = self.fn
-        check(self.lib.cmm_fmt_hvp(self.plan.handle, self.B, None, fn.R, fn.beta, fn.version, ptr(self.kst_t),
+        check(self.lib.cmm_fmt_hvp(self.plan.handle, self.B, None, fn.R, fn.beta, fn.version, 1, ptr(self.kst_t),
                                    ptr(fn.wtab), ptr(self.wd), ptr(vhat), ptr(out), ptr(self.work), _stream()),
               "cmm_fmt_hvp")
         Au = self.plan.irfft_yz(out).view(self.B, self.npts)
@@ -195,13 +209,58 @@ class _BiCGStab(object):
         return lam
 
 
-def _functional_variant(fn, guest, temperature, mfa_cutoff, tailcorrections):
-    """The same functional with the hard-sphere radius and MFA kernel of another
-    guest (the C1 pipeline does not read the external potential)."""
-    sig, eps, _ = guest
-    kst, a = E.mfa_kernel_spectrum(fn.plan, sig, eps, mfa_cutoff, rep=2 if tailcorrections else 1)
-    R = W.hardsphere_radius(sig, eps, temperature)
-    return E.Functional(fn.plan, R, fn.beta, fn.wavelength, fn.V, fn.version, kst, a)
+def eos_inputs(pressures, temperature, guest, newton=3):
+    """(mu, rho_bulk) per pressure with the EOS root polished by Newton steps
+    on p(rho) = P.  The reference's bracketing solve (eos.py:121-157, 209-215;
+    cmmdft_b200.eos keeps it bit for bit) stops within an absolute tolerance,
+    which leaves mu(theta) step-like at ~1e-11 relative; the differentiable
+    model needs it smooth."""
+    from .eos import ModifiedBenedictWebbRubinEOS
+    sig, eps, mass = guest
+    P = np.atleast_1d(np.asarray(pressures, dtype=float))
+    mb = ModifiedBenedictWebbRubinEOS(mass, sig, eps)
+    mb.set_temperature(temperature)
+    rho = mb.solve_densities_from_pressures(P)[:, 0]
+    for _ in range(newton):
+        h = 1e-7 * rho
+        slope = (mb.compute_pressure(rho + h) - mb.compute_pressure(rho - h)) / (2 * h)
+        rho = rho - (mb.compute_pressure(rho) - P) / slope
+    return mb.compute_chempot(rho), rho
+
+
+def eos_derivatives(pressures, temperature, guest, rel=1e-6):
+    """d mu / d theta and d rho_bulk / d theta [B, 2] (theta = guest epsilon,
+    guest sigma) at fixed pressures, by implicit differentiation of the MBWR
+    root p(rho*) = P (eos.py:209-215)."""
+    from .eos import ModifiedBenedictWebbRubinEOS
+    sig, eps, mass = guest
+    rho = eos_inputs(pressures, temperature, guest)[1]
+
+    def pm(r, s_, e_):
+        m = ModifiedBenedictWebbRubinEOS(mass, s_, e_)
+        m.set_temperature(temperature)
+        return m.compute_pressure(r), m.compute_chempot(r)
+    hr = rel * rho
+    (pp, mp), (pq, mq) = pm(rho + hr, sig, eps), pm(rho - hr, sig, eps)
+    p_r, m_r = (pp - pq) / (2 * hr), (mp - mq) / (2 * hr)
+    dmu, drho = np.zeros((len(rho), 2)), np.zeros((len(rho), 2))
+    for k, (ds, de) in enumerate(((0.0, rel * eps), (rel * sig, 0.0))):
+        h = ds + de
+        (pp, mp), (pq, mq) = pm(rho, sig + ds, eps + de), pm(rho, sig - ds, eps - de)
+        p_t, m_t = (pp - pq) / (2 * h), (mp - mq) / (2 * h)
+        drho[:, k] = -p_t / p_r
+        dmu[:, k] = m_t + m_r * drho[:, k]
+    return dmu, drho
+
+
+def _mfa_values(fn, kst, rhohat, B, buf):
+    """(MFA part of C1 [B, npts], F_MFA per instance) for kernel spectrum kst."""
+    plan = fn.plan
+    ch = plan.new_spec(B)
+    check(L.lib().cmm_fmt_c1(plan.handle, B, None, fn.R, fn.beta, L.NOHS, None, ptr(kst), ptr(fn.wtab),
+                             ptr(rhohat), ptr(ch), ptr(buf.work), ptr(buf.part), buf.nslot, 1, None, _stream()),
+          "cmm_fmt_c1")
+    return plan.irfft_yz(ch).reshape(B, plan.npts)
 
 
 def _excess_values(fn, rhohat, B):
@@ -227,7 +286,7 @@ def helium_fraction(plan, host, temperature, cutoff=12 * angstrom):
 
 def adjoint_gradients(fn, host, guest, temperature, pressures, mus, rho, cutoff=12 * angstrom,
                       mfa_cutoff=12 * angstrom, limit_potential=1e4 * kjmol, tailcorrections=False,
-                      fd_rel=1e-5, tol=1e-11, maxiter=300, excess=True):
+                      fd_rel=1e-3, tol=1e-11, maxiter=300, excess=True):
     """dN/dtheta, dOmega/dtheta (and the excess uptake's) at converged densities.
 
     rho: converged densities [B, N1, N2, N3] (device) of chemical potentials
@@ -249,21 +308,20 @@ def adjoint_gradients(fn, host, guest, temperature, pressures, mus, rho, cutoff=
     buf = E.Buffers(plan, B, nwork=fn.nwork)
     wd = torch.empty((fn.nwd, B) + plan.npoints, dtype=torch.float64, device="cuda")
     fn.c1(buf, rhohat, None, want=8, wd=wd)
-    # K rho and K^T rho for Omega's adjoint right-hand side
-    lib = L.lib()
-    mfa = []
-    for k in (fn.kst, _conj_spectrum(fn.kst)):
-        ch = plan.new_spec(B)
-        check(lib.cmm_fmt_c1(plan.handle, B, None, fn.R, fn.beta, L.NOHS, None, ptr(k), ptr(fn.wtab), ptr(rhohat),
-                             ptr(ch), ptr(buf.work), ptr(buf.part), buf.nslot, 1, None, _stream()), "cmm_fmt_c1")
-        mfa.append(plan.irfft_yz(ch).reshape(B, n))
-    rhs_om = 0.5 * dV * (mfa[1] - mfa[0])
-    # where _get_Omega clips rho (< 1e-12 -> 1e-30) its ideal term is constant,
-    # so dOmega/drho there lacks ln(Lambda^3 rho)/beta, which the fixed point
-    # otherwise cancels against C1 - mu
-    small = (rho2 < 1e-12) & (rho2 > 0)
-    safe = torch.where(small, rho2, torch.ones_like(rho2))
-    rhs_om = rhs_om - torch.where(small, dV * torch.log(fn.lambda3 * safe) / beta, torch.zeros_like(rho2))
+    # dOmega/drho of Solver._get_Omega at rho, term by term (not through the
+    # fixed-point relation, which the smallest densities satisfy least):
+    # dV [ideal' - mu + V + C1 + (K^T - K) rho / 2], ideal' = ln(Lambda^3 rho)/beta
+    # where rho >= 1e-12 and 0 where _get_Omega clips it; C1 (the pipeline's,
+    # with K rho) plus (K^T - K) rho / 2 is the gradient of F_HS + rho^T K rho / 2
+    mfa = [_mfa_values(fn, k, rhohat, B, buf) for k in (fn.kst, _conj_spectrum(fn.kst))]
+    chat = plan.new_spec(B)
+    fn.c1(buf, rhohat, chat, want=1)
+    C1 = plan.irfft_yz(chat).reshape(B, n)
+    mu_t = torch.as_tensor(np.asarray(mus, dtype=np.float64), device="cuda").view(B, 1)
+    keep = rho2 >= 1e-12
+    ideal_d = torch.where(keep, torch.log(fn.lambda3 * torch.where(keep, rho2, torch.ones_like(rho2))) / beta,
+                          torch.zeros_like(rho2))
+    rhs_om = dV * (ideal_d - mu_t + fn.V.reshape(1, n) + C1 + 0.5 * (mfa[1] - mfa[0]))
     solver = _BiCGStab(fn, rho, wd)
     lam_n = solver.solve(torch.full((B, n), dV, dtype=torch.float64, device="cuda"), tol=tol, maxiter=maxiter)
     it_n, res_n = solver.iterations, solver.residual
@@ -281,22 +339,43 @@ def adjoint_gradients(fn, host, guest, temperature, pressures, mus, rho, cutoff=
     # explicit guest partials of the excess functional and of the EOS
     Gx_n, Gx_o, dF, dmu, dbulk = (np.zeros((B, K)) for _ in range(5))
     _, F0 = _excess_values(fn, rhohat, B)
+    # f' = [8 (f(h) - f(-h)) - (f(2h) - f(-2h))] / (12 h)
+    stencil = ((1.0, 8.0), (-1.0, -8.0), (2.0, -1.0), (-2.0, 1.0))
+    gsig, geps, _ = guest
+    # hard-sphere part: d/dR at fixed (zero) MFA kernel, chained with dR/dtheta
+    zero_k = torch.zeros_like(fn.kst)
+    hR = fd_rel * fn.R
+    dC_R = torch.zeros((B, n), dtype=torch.float64, device="cuda")
+    dF_R = np.zeros(B)
+    for step, wgt in stencil:
+        fr = E.Functional(plan, fn.R + step * hR, fn.beta, fn.wavelength, fn.V, fn.version, zero_k)
+        c1x, F = _excess_values(fr, rhohat, B)
+        dC_R += (wgt / (12 * hR)) * c1x
+        dF_R += (wgt / (12 * hR)) * F
+    dR = np.zeros(2)
     for k, idx in ((0, 1), (1, 0)):   # theta_0: guest epsilon (guest[1]); theta_1: guest sigma (guest[0])
-        h = fd_rel * guest[idx]
-        vals = []
-        for sgn in (1.0, -1.0):
+        h = 1e-4 * guest[idx]
+        for step, wgt in stencil:
             g = list(guest)
-            g[idx] = guest[idx] + sgn * h
-            fv = _functional_variant(fn, tuple(g), temperature, mfa_cutoff, tailcorrections)
-            c1x, F = _excess_values(fv, rhohat, B)
-            mu_v, bulk_v = W.isotherm_inputs(pressures, temperature, tuple(g))
-            vals.append((c1x, F, np.asarray(mu_v), np.asarray(bulk_v)))
-        Dk = (vals[0][0] - vals[1][0]) / (2 * h)
+            g[idx] = guest[idx] + step * h
+            dR[k] += wgt / (12 * h) * W.hardsphere_radius(g[0], g[1], temperature)
+    # MFA part: linear in epsilon; sigma by a small central difference
+    rep = 2 if tailcorrections else 1
+    c_mfa = _mfa_values(fn, fn.kst, rhohat, B, buf)
+    hs_ = 1e-7 * gsig
+    kp, _ = E.mfa_kernel_spectrum(plan, gsig + hs_, geps, mfa_cutoff, rep=rep)
+    km, _ = E.mfa_kernel_spectrum(plan, gsig - hs_, geps, mfa_cutoff, rep=rep)
+    dC_ms = (_mfa_values(fn, kp, rhohat, B, buf) - _mfa_values(fn, km, rhohat, B, buf)) / (2 * hs_)
+    half_rho = 0.5 * dV * rho2
+    D_eps = dR[0] * dC_R + c_mfa / geps
+    D_sig = dR[1] * dC_R + dC_ms
+    for k, Dk in ((0, D_eps), (1, D_sig)):
         Gx_n[:, k] = _pair_dots(lam_n, Dk)
         Gx_o[:, k] = _pair_dots(lam_o, Dk)
-        dF[:, k] = (vals[0][1] - vals[1][1]) / (2 * h)
-        dmu[:, k] = (vals[0][2] - vals[1][2]) / (2 * h)
-        dbulk[:, k] = (vals[0][3] - vals[1][3]) / (2 * h)
+    dF[:, 0] = dR[0] * dF_R + _pair_dots(half_rho, c_mfa) / geps
+    dF[:, 1] = dR[1] * dF_R + _pair_dots(half_rho, dC_ms)
+    # EOS
+    dmu[:, :2], dbulk[:, :2] = eos_derivatives(pressures, temperature, guest)
     dN = -beta * (G_n + Gx_n) + beta * dmu * sum_n[:, None]
     dOm = dV * H + dF - N[:, None] * dmu - beta * (G_o + Gx_o) + beta * dmu * sum_o[:, None]
     # Omega at rho as Solver._get_Omega forms it
@@ -305,6 +384,7 @@ def adjoint_gradients(fn, host, guest, temperature, pressures, mus, rho, cutoff=
     ext = _contract(rho2, fn.V.reshape(1, n))[:, 0] * dV
     Om = ideal + F0 + ext - np.asarray(mus) * N
     out = dict(names=param_names(host), N=N, Omega=Om, dN=dN, dOmega=dOm,
+               dOmega_explicit=dV * H + dF - N[:, None] * dmu,
                iterations=(it_n, it_o), residual=(res_n, res_o))
     if excess:
         kT = 1.0 / beta
@@ -318,7 +398,7 @@ def adjoint_gradients(fn, host, guest, temperature, pressures, mus, rho, cutoff=
         w = torch.where((Vhe > 0) & torch.isfinite(Vhe), -ehe / kT, torch.zeros_like(Vhe))
         dhe = _contract(w, _dv_fields(plan, host, he_sig, he_eps, cutoff, float('inf')))[0] * dV / vol
         dhe[:2] = 0.0   # the helium probe's own parameters are not in theta
-        bulks = np.asarray(W.isotherm_inputs(pressures, temperature, guest)[1])
+        bulks = eos_inputs(pressures, temperature, guest)[1]
         out['Nex'] = N - bulks * he_frac * vol
         out['dNex'] = dN - vol * (dbulk * he_frac + bulks[:, None] * dhe[None, :])
         out['he_frac'] = he_frac
@@ -336,7 +416,7 @@ class IsothermModel(object):
 
     def __init__(self, host, guest, temperature, npoints, pressures, quantity='excess', threshold=1e-12,
                  criterion='res', nsteps=1000, method='hybridanderson', version='WBII', tailcorrections=False,
-                 cutoff=12 * angstrom, mfa_cutoff=12 * angstrom, limit_potential=1e4 * kjmol, fd_rel=1e-5,
+                 cutoff=12 * angstrom, mfa_cutoff=12 * angstrom, limit_potential=1e4 * kjmol, fd_rel=1e-3,
                  tol=1e-11):
         assert quantity in ('excess', 'absolute', 'omega')
         self.host, self.guest = host, guest
@@ -353,16 +433,20 @@ class IsothermModel(object):
         self.last = None
 
     def solve(self, theta):
-        """Converged isotherm at parameters theta (no derivatives)."""
-        from .isotherm import solve_isotherm
+        """Converged isotherm at parameters theta (no derivatives): chemical
+        potentials from the polished EOS root (``eos_inputs``), Ninit = rho_bulk
+        start, the native batched solver."""
+        from .batch import GroupedSolve
         host, guest = unpack_params(theta, self.host, self.guest)
         fn = W.build_functional(host, self.npoints, self.T, guest, version=self.version,
                                 tailcorrections=self.tail, cutoff=self.cutoff, mfa_cutoff=self.mfa_cutoff,
                                 limit_potential=self.vcap, plan=self.plan)
-        out = solve_isotherm(host, self.pressures, self.T, guest, self.npoints, fn=fn, return_density=False,
-                             **self.solve_kw)
-        out.update(host=host, guest=guest, fn=fn, rho=out['solver'].result)
-        return out
+        mus, bulks = eos_inputs(self.pressures, self.T, guest)
+        rho0 = W.initial_density(fn, mus, ninit=bulks)
+        s = GroupedSolve(fn, mus, groups=1, divergence_guard=True, **self.solve_kw)
+        N, rho, conv = s.solve(rho0)
+        return dict(mu=mus, rho_bulk=bulks, N=np.array(N), converged=np.array(conv), solver=s, host=host,
+                    guest=guest, fn=fn, rho=rho)
 
     def quantity_values(self, sol):
         """The model's quantity at a solution, without derivatives."""

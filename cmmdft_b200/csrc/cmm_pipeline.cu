@@ -1811,7 +1811,12 @@ static int zrow_fmt(const cmm_grid* g, int batch, const int* act, double R, int 
 // directional derivative of dPhi/dn at n(rho) along n(v), fmt_point
 // evaluated in Dual arithmetic.  Its fields go out z-forward (y forward
 // follows), in the layout of the dPhi spectra of k_zrow_fmt.
-template <int M3C, bool TEN>
+// TR: the transposed pointwise Jacobian.  It equals the Jacobian except
+// where n3 is clipped (n3 < 1e-30 or > 0.99): there dPhi/dn3 is still taken
+// at the clipped value, so it depends on the other densities while nothing
+// depends on n3; the transpose passes the tangent of n3 through the clip
+// into the other outputs and returns no dPhi/dn3 tangent.
+template <int M3C, bool TEN, bool TR>
 __global__ void __launch_bounds__(CMM_ROW_THREADS)
 k_zrow_hvp(GridDev g, const int* __restrict__ active, double R, int version, const double2* __restrict__ win,
            size_t fs, double2* __restrict__ gout, int chunk, const double* __restrict__ wdrho, size_t fsr) {
@@ -1832,10 +1837,15 @@ k_zrow_hvp(GridDev g, const int* __restrict__ active, double R, int version, con
       const size_t q = roff + (size_t)(r0 + r) * n3 + j;
       Dual n[nf], gT[6];
       for (int f = 0; f < nf; ++f) n[f] = Dual(__ldg(wdrho + f * fsr + q), zrow_rel<M3C>(g, s, nf, f, r, j));
+      bool clipped = false;
+      if constexpr (TR) {
+        clipped = !(n[1].v >= 1e-30) || !(n[1].v <= 0.99);
+        if (clipped) n[1].v = fmin(fmax(n[1].v, 1e-30), 0.99);
+      }
       const PhiOutT<Dual> o = fmt_point<TEN, Dual>(n[0], n[1], n[2], n[3], n[4], TEN ? n + 5 : nullptr, gT, R,
                                                    version);
       zrow_rel<M3C>(g, s, nf, 0, r, j) = o.gs.d;
-      zrow_rel<M3C>(g, s, nf, 1, r, j) = o.g3.d;
+      zrow_rel<M3C>(g, s, nf, 1, r, j) = clipped ? 0.0 : o.g3.d;
       zrow_rel<M3C>(g, s, nf, 2, r, j) = o.gv[0].d;
       zrow_rel<M3C>(g, s, nf, 3, r, j) = o.gv[1].d;
       zrow_rel<M3C>(g, s, nf, 4, r, j) = o.gv[2].d;
@@ -1849,33 +1859,37 @@ k_zrow_hvp(GridDev g, const int* __restrict__ active, double R, int version, con
   }
 }
 
-template <int M3C, bool TEN>
+template <int M3C, bool TEN, bool TR>
 static int zrow_hvp_one(const cmm_grid* g, int batch, const int* act, double R, int version, const double2* win,
                         size_t fs, double2* gout, int chunk, const double* wdrho, cudaStream_t st) {
   constexpr int nf = 5 + (TEN ? 6 : 0);
   const size_t sb = zrow_smem_bytes_g(g, nf * chunk);
   int rc;
-  if ((rc = set_smem((const void*)k_zrow_hvp<M3C, TEN>, sb))) return rc;
-  k_zrow_hvp<M3C, TEN><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(
+  if ((rc = set_smem((const void*)k_zrow_hvp<M3C, TEN, TR>, sb))) return rc;
+  k_zrow_hvp<M3C, TEN, TR><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(
       g->dev, act, R, version, win, fs, gout, chunk, wdrho, (size_t)batch * g->n1 * g->n2 * g->n3);
   return last_err();
 }
 
 template <int M3C>
-static int zrow_hvp_m3(const cmm_grid* g, int batch, const int* act, double R, int version, const double2* win,
-                       size_t fs, double2* gout, int chunk, const double* wdrho, cudaStream_t st) {
+static int zrow_hvp_m3(const cmm_grid* g, int batch, const int* act, double R, int version, int tr,
+                       const double2* win, size_t fs, double2* gout, int chunk, const double* wdrho,
+                       cudaStream_t st) {
   if (version & CMM_TENSOR)
-    return zrow_hvp_one<M3C, true>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st);
-  return zrow_hvp_one<M3C, false>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st);
+    return tr ? zrow_hvp_one<M3C, true, true>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st)
+              : zrow_hvp_one<M3C, true, false>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st);
+  return tr ? zrow_hvp_one<M3C, false, true>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st)
+            : zrow_hvp_one<M3C, false, false>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st);
 }
 
 // Spectrum of A v = d C1 / d rho . v (Hartree per density unit), A the
 // Hessian of the excess free energy per grid volume: hard-sphere part
 // through the second derivatives of Phi at the stored weighted densities of
 // rho, plus the MFA convolution K v (the external potential does not depend
-// on rho).  The y/z steps run in the staged form for every grid shape.
+// on rho).  transpose: A^T v (the caller passes the conjugate MFA spectrum).
+// The y/z steps run in the staged form for every grid shape.
 extern "C" int cmm_fmt_hvp(const cmm_grid* g, int batch, const int* d_active, double R, double beta, int version,
-                           const double* d_kst, const double* d_wtab, const double* d_wd_rho,
+                           int transpose, const double* d_kst, const double* d_wtab, const double* d_wd_rho,
                            const double* d_vhat, double* d_out_hat, double* d_work, void* stream) {
   if (!g || batch < 1 || !d_kst || !d_vhat || !d_out_hat || !d_work) return CMM_ERR_ARG;
   if (version & CMM_WDA) return CMM_ERR_UNSUPPORTED;
@@ -1912,9 +1926,9 @@ extern "C" int cmm_fmt_hvp(const cmm_grid* g, int batch, const int* d_active, do
   const int chunk = zrow_chunk(g, nf);
   if (chunk < 1) return CMM_ERR_SMEM;
   switch (zrow_m3(g)) {
-    case 32: rc = zrow_hvp_m3<32>(g, batch, d_active, R, version, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
-    case 16: rc = zrow_hvp_m3<16>(g, batch, d_active, R, version, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
-    default: rc = zrow_hvp_m3<0>(g, batch, d_active, R, version, wbuf, fs, gbuf, chunk, d_wd_rho, st);
+    case 32: rc = zrow_hvp_m3<32>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
+    case 16: rc = zrow_hvp_m3<16>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
+    default: rc = zrow_hvp_m3<0>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st);
   }
   if (rc) return rc;
   if ((rc = ypass(g, batch, d_active, gbuf, gbuf, fs, nf, 0, st))) return rc;

@@ -374,11 +374,14 @@ typedef struct cmm_solve_out {
  * (hard-sphere + MFA; C1 in Hartree, so A v is in Hartree per density unit),
  * for `batch` yz-spectra d_vhat.  d_wd_rho: the real-space weighted
  * densities of rho [nwd][B][npts] stored by cmm_fmt_c1 with want bit 3; the
- * hard-sphere second derivatives are taken there.  With d_kst conjugated the
- * MFA term becomes its transpose.  d_work: nwork spectra as for cmm_fmt_c1.
+ * hard-sphere second derivatives are taken there.  transpose = 1: A^T v,
+ * with the caller passing the conjugate MFA spectrum as d_kst (A is not
+ * symmetric: the reference's MFA kernel is translated by its spectrum
+ * phase, and where n3 is clipped dPhi/dn3 still varies with the other
+ * densities).  d_work: nwork spectra as for cmm_fmt_c1.
  * CMM_WDA: CMM_ERR_UNSUPPORTED. */
 int cmm_fmt_hvp(const cmm_grid* grid, int batch, const int* d_active, double R, double beta, int version,
-                const double* d_kst, const double* d_wtab, const double* d_wd_rho, const double* d_vhat,
+                int transpose, const double* d_kst, const double* d_wtab, const double* d_wd_rho, const double* d_vhat,
                 double* d_out_hat, double* d_work, void* stream);
 
 /* Parameter derivatives of the capped LJ external potential (arguments as
