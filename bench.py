@@ -90,6 +90,14 @@ class ClockSampler(object):
                 "reasons": reasons, "samples": len(self.samples)}
 
 
+# DRAM bytes (read + write) of one 24-instance 64^3 pipeline launch with
+# want = 15 (column pass 1, plane pass storing the weighted densities, column
+# pass 2), summed over its three kernels from one ncu capture
+# (profiles/pipeline_traffic_isotherm64.md); reported per launch scaled by
+# the algorithmic bytes, the way roofline.achieved averages over launches.
+NCU_TRAFFIC_FULL_LAUNCH = 1339645952.0
+
+
 def pipeline_bytes(plan, want, n_active):
     """Algorithmic HBM bytes of one functional-pipeline launch (3 kernels).
 
@@ -204,7 +212,10 @@ def run_gpu(args):
                 "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
                 "peak_source": "fallback" if pk.get("_fallback") else "measured",
-                "traffic": None, "launches": len(events),
+                "traffic": (NCU_TRAFFIC_FULL_LAUNCH / pipeline_bytes(fn.plan, 15, 24) * tot_bytes / len(events))
+                if events and tuple(fn.plan.npoints) == (64, 64, 64) else None,
+                "traffic_source": "ncu DRAM bytes of one full 24-instance launch, scaled by algorithmic bytes",
+                "launches": len(events),
                 "bytes_per_launch": tot_bytes / max(len(events), 1),
                 "ms_per_launch": tot_ms / max(len(events), 1),
                 "share_of_step": tot_ms / ms_max if ms_max else None}
