@@ -13,6 +13,10 @@
 #include <cstdio>
 #include <cstring>
 
+#include <map>
+#include <mutex>
+#include <utility>
+
 #include "cmm_common.cuh"
 #include "cmm_dual.cuh"
 
@@ -1617,10 +1621,23 @@ __global__ void k_stats_finalize(const int* __restrict__ active, const double* _
 // ============================================================ host side ==
 static int last_err() { return (cudaPeekAtLastError() == cudaSuccess) ? CMM_OK : CMM_ERR_CUDA; }
 
+// The dynamic shared-memory limit is an attribute of the kernel function,
+// shared by every caller: solves of different grids on concurrent host
+// threads launch the same generic kernel with different sizes.  The limit
+// therefore only grows (under a lock, per device and kernel), so no thread
+// lowers it below a launch another thread is about to make.
 static int set_smem(const void* fn, size_t bytes) {
   if (bytes > 232448) return CMM_ERR_SMEM;  // the B200 per-block opt-in limit
+  static std::mutex mu;
+  static std::map<std::pair<int, const void*>, size_t> limits;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess) return CMM_ERR_CUDA;
+  std::lock_guard<std::mutex> lock(mu);
+  size_t& cur = limits[std::make_pair(dev, fn)];
+  if (bytes <= cur) return CMM_OK;
   if (cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes) != cudaSuccess)
     return CMM_ERR_CUDA;
+  cur = bytes;
   return CMM_OK;
 }
 

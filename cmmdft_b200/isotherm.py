@@ -14,7 +14,7 @@ from . import batch as BT
 from . import workload as W
 from .units import angstrom, kjmol
 
-__all__ = ['solve_isotherm', 'excess_loading']
+__all__ = ['solve_isotherm', 'solve_batch', 'grid_points', 'excess_loading']
 
 
 def solve_isotherm(host, pressures, temperature, guest, npoints, method='hybridanderson', threshold=1e-8,
@@ -59,3 +59,87 @@ def solve_isotherm(host, pressures, temperature, guest, npoints, method='hybrida
 def excess_loading(N, rho_bulk, he_fraction, cell_volume):
     """N_ex = N - rho_bulk * He_frac * V_cell (Calculator.return_loading, calculator.py:114-138)."""
     return np.asarray(N) - np.asarray(rho_bulk) * he_fraction * cell_volume
+
+
+def grid_points(host, spacing=0.25 * angstrom):
+    """N_a = ceil(L_a / spacing), L_a the length of cell vector a (Grid.__init__,
+    cmmdft/system.py:262-266, which measures the columns of rvecs; the hosts
+    here are orthorhombic, where rows and columns agree)."""
+    lengths = np.linalg.norm(np.asarray(host.rvecs, dtype=float), axis=0)
+    return tuple(int(np.ceil(l / spacing)) for l in lengths)
+
+
+def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25 * angstrom,
+                method='hybridanderson', threshold=1e-8, criterion='res', nsteps=500, m=5, alpha_mix=0.1,
+                divergence_guard=True, anderson_coefs='slsqp', return_density=False, max_concurrent=4,
+                version='WBII', tailcorrections=False):
+    """Isotherms of several hosts of uneven cells and grids in one call.
+
+    The reference solves every (host, pressure) point in its own Program.solve
+    loop.  Here each host is one batched solve of all its pressures (its own
+    grid plan, potential and MFA kernel, since the cell sets the k-vectors);
+    up to ``max_concurrent`` hosts run at once, each driven by the native
+    batched solver from its own host thread on its own CUDA stream, so the
+    host decisions of one host overlap the kernels of the others.  A host's
+    device buffers (~460 B per grid point and pressure with m = 5) are
+    released when its solve ends; ``max_concurrent`` bounds the total.
+
+    hosts: list of SyntheticHost-like hosts; pressures: one array for every
+    host or a list with one array per host (atomic units); npoints: None
+    (from ``spacing``), one shape for all hosts or a list of shapes.
+    Returns one dict per host as ``solve_isotherm`` does (without the solver
+    and functional objects), in the order of ``hosts``.
+    """
+    import threading
+    nh = len(hosts)
+    if npoints is None:
+        shapes = [grid_points(h, spacing) for h in hosts]
+    elif np.ndim(npoints) == 1 and len(npoints) == 3 and not isinstance(npoints[0], (tuple, list)):
+        shapes = [tuple(int(n) for n in npoints)] * nh
+    else:
+        shapes = [tuple(int(n) for n in s) for s in npoints]
+    plist = pressures if (isinstance(pressures, (list, tuple)) and len(pressures) == nh and
+                          np.ndim(pressures[0]) == 1) else [pressures] * nh
+    results = [None] * nh
+    errors = []
+    gate = threading.Semaphore(max(1, int(max_concurrent)))
+    cur = torch.cuda.current_stream()
+    device = torch.cuda.current_device()
+
+    def run(i):
+        with gate:
+            try:
+                torch.cuda.set_device(device)
+                st = torch.cuda.Stream()
+                st.wait_stream(cur)
+                with torch.cuda.stream(st):
+                    fn = W.build_functional(hosts[i], shapes[i], temperature, guest, version=version,
+                                            tailcorrections=tailcorrections)
+                    P = np.asarray(plist[i], dtype=float)
+                    mus, bulks = W.isotherm_inputs(P, temperature, guest)
+                    rho0 = W.initial_density(fn, mus, ninit=bulks)
+                    s = BT.NativeBatchSolve(fn, mus, method=method, nsteps=nsteps, threshold=threshold,
+                                            criterion=criterion, m=m, alpha_mix=alpha_mix,
+                                            divergence_guard=divergence_guard, anderson_coefs=anderson_coefs)
+                    host = (torch.empty(tuple(rho0.shape), dtype=torch.float64, pin_memory=True)
+                            if return_density else None)
+                    N, rho, conv = s.solve(rho0, host_out=host)
+                    out = dict(mu=mus, rho_bulk=bulks, N=np.array(N), converged=np.array(conv),
+                               steps=s.steps.copy(), diverged=s.diverged.copy(), omega=np.array(s.omega0),
+                               npoints=shapes[i])
+                    st.synchronize()
+                    if return_density:
+                        out['rho'] = host.numpy()
+                    results[i] = out
+                    del s, fn, rho, rho0
+            except BaseException as e:  # re-raised on the calling thread
+                errors.append(e)
+
+    threads = [threading.Thread(target=run, args=(i,)) for i in range(nh)]
+    for t in threads:
+        t.start()
+    for t in threads:
+        t.join()
+    if errors:
+        raise errors[0]
+    return results

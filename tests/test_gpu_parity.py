@@ -282,13 +282,48 @@ def test_uneven_grid_against_oracle(cuda, ver):
     assert scalar_rel(N[0], N3o) < 1e-10
 
 
+def test_solve_batch_uneven_hosts(cuda):
+    """Three hosts of uneven cells and grids (53x53x62, 50x58x60 and
+    52x49x53: prime factors and odd N3) solved concurrently by solve_batch
+    equal their one-host solves exactly; the 52x49x53 host's 1 bar point
+    against the oracle at the reference's tolerance (RES < 1e-8): the same
+    number of steps and N within 1e-10."""
+    from oracle import cmm_oracle as O
+    from cmmdft_b200 import isotherm as ISO
+    from cmmdft_b200.hosts import uneven_hosts
+    hosts = uneven_hosts(nhost=3, seed=2, edge_range=(12.0, 16.0))
+    guest = methane_guest_params()
+    P = np.array([0.1, 1.0, 10.0]) * bar
+    res = ISO.solve_batch(hosts, P, 300.0, guest, max_concurrent=3)
+    for h, r in zip(hosts, res):
+        one = ISO.solve_isotherm(h, P, 300.0, guest, ISO.grid_points(h), return_density=False)
+        assert r['npoints'] == ISO.grid_points(h)
+        assert np.array_equal(r['N'], one['N']) and np.array_equal(r['steps'], one['steps'])
+    h = hosts[2]
+    sig, eps, mass = guest
+    shape = ISO.grid_points(h)
+    og = O.OGrid(h.rvecs, npoints=list(shape))
+    V = O.external_potential(og.points[..., :3].reshape(-1, 3), h.ff, sig, eps, h.recentred_pos(), h.ffatypes,
+                             h.ffatype_ids, h.rvecs).reshape(shape)
+    V = O.cap_potential(V, 1e4 * kjmol)
+    fe = O.build_functional(og, sig, eps, mass, 300.0, V)
+    mb = O.MBWR(mass, sig, eps)
+    mu = O.eos_calculate_mu(mb, 300.0, P[1])
+    mb.set_temperature(300.0)
+    rb = np.nanmin(O.eos_densities_from_chempots(mb, [mu]), axis=1)[0]
+    s = O.Anderson(fe, nsteps=500, m=5, criterion='res', threshold=1e-8)
+    N, rho, conv = s.solve(mu, rb * np.exp(-np.maximum(V, 0) * fe.beta))
+    assert conv and res[2]['converged'][1]
+    assert res[2]['steps'][1] == s.curr_step
+    assert scalar_rel(res[2]['N'][1], N) < 1e-10
+
+
 def test_hybrid_anderson_matches_reference(golden32, fn32):
     mu = float(golden32["mu"])
     s, N, rho, conv = _solve(fn32, mu, golden32["rho_a"], 'hybridanderson', TIGHT_THR, nsteps=500,
                              crit=TIGHT_CRIT)
     assert conv[0]
-    # both sides converged to RES < 1e-13 and RIUE < 1e-12 (different
-    # trajectories: exact simplex QP here, SLSQP in the reference)
+    # both sides converged to RES < 1e-13 and RIUE < 1e-12
     assert relerr(rho[0], golden32["and_rho"]) < 1e-9
     assert scalar_rel(N[0], golden32["and_N"]) < 1e-10
     om = s.omega0[0]
