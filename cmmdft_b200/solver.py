@@ -1,8 +1,10 @@
 """Fixed-point solvers with the reference's interface (cmmdft/solver.py:18-604).
 
-Solver / Picard / Anderson keep the reference's constructor arguments and
-``solve(chempot, rho, log_level) -> (N, rho, converged)``.  Each call runs a
-batch of one through ``batch.BatchSolve`` (all field work on the GPU); the
+Solver / Picard / Anderson / QuasiNewton keep the reference's constructor
+arguments and ``solve(chempot, rho, log_level) -> (N, rho, converged)``.
+Each call runs a batch of one through the native batched driver
+(``quasinewton.QuasiNewtonSolve`` for QuasiNewton; all field work on the
+GPU); the
 batched isotherm entry point is ``isotherm.solve_isotherm`` /
 ``Program.solve_isotherm``.
 """
@@ -11,7 +13,7 @@ import numpy as np
 from . import batch as BT
 from .batch import NoSolutionError
 
-__all__ = ['Solver', 'Picard', 'Anderson', 'NoSolutionError']
+__all__ = ['Solver', 'Picard', 'Anderson', 'QuasiNewton', 'NoSolutionError']
 
 
 class Solver(object):
@@ -115,3 +117,36 @@ class Anderson(Picard):
         return dict(alpha_mix=self.alpha_mix, m=self.m, damping=self.damping, delta=self.delta,
                     damping_max=self.damping_max, damping_min=self.damping_min,
                     adaptive_damping=self.adaptive_damping, damping_factors=self.damping_factors)
+
+
+class QuasiNewton(Picard):
+    """Limited-memory quasi-Newton steps on Omega between hybrid Picard steps
+    (cmmdft/solver.py:701-1053), through ``quasinewton.QuasiNewtonSolve``."""
+    name = 'QUASI_NEWTON'
+
+    def __init__(self, program, nsteps=500, m=10, method='bfgs', hybrid=True, delta=0.5, alpha_init=0.05, c1=1e-4,
+                 c2=0.9, line_search='backtracking', n_line_search=10, trust_radius=1, verbose=True, **kwargs):
+        alpha_mix = kwargs.pop('alpha_mix', 0.1)
+        Solver.__init__(self, program, nsteps, **kwargs)
+        self.alpha_mix = alpha_mix
+        assert method.lower() in ('bfgs', 'broyden', 'cg'), \
+            "Method %s not recognized. Choose from 'bfgs', 'broyden' or 'cg'." % method
+        assert line_search in ('backtracking', 'quadratic', 'none'), \
+            "Line search method %s not recognized." % line_search
+        self.m, self.QN_method, self.hybrid, self.delta = m, method.lower(), hybrid, delta
+        self.alpha_init, self.c1, self.c2 = alpha_init, c1, c2
+        self.line_search, self.n_line_search, self.trust_radius = line_search, n_line_search, trust_radius
+        self.verbose = verbose
+
+    def solve(self, chempot, rho, log_level=2):
+        from .quasinewton import QuasiNewtonSolve
+        s = QuasiNewtonSolve(self.fener.device(), nsteps=self.nsteps, m=self.m, method=self.QN_method,
+                             hybrid=self.hybrid, delta=self.delta, alpha_init=self.alpha_init, c1=self.c1,
+                             c2=self.c2, line_search=self.line_search, n_line_search=self.n_line_search,
+                             trust_radius=self.trust_radius, threshold=self.threshold, criterion=self.criterion,
+                             a_tol=self.a_tol, r_tol=self.r_tol, alpha_mix=self.alpha_mix)
+        N, r, conv = s.solve(chempot, rho)
+        self._last = s
+        self.curr_step = int(s.steps)
+        self.omega0 = float(s.omega0)
+        return float(N), r.cpu().numpy(), bool(conv)

@@ -5,6 +5,7 @@ machines):
 
     python tests/golden/make_golden.py [--reference /root/reference] [--skip64]
     python tests/golden/make_golden.py --iso64 [--procs 8]
+    python tests/golden/make_golden.py --qn
 
 The reference is imported from its own source tree through the import shims
 in ``tests/golden/refshim`` (molmod units/constants backed by
@@ -21,6 +22,9 @@ Outputs (small ``.npz`` files) land next to this script:
               tight hybrid-Anderson solution, tail-corrected MFA.
   c1_64.npz   64^3 cubic host: V summary and tight hybrid-Anderson solutions
               at three pressures (scalars + one density field).
+  qn32.npz    the 32^3 case at 1 bar solved by the reference's QuasiNewton
+              (RES < 1e-8, Ninit = rho_bulk) for five direction / line-search
+              variants: N, Omega, steps (``--qn`` only).
   iso64_res8.npz  the 24-pressure 64^3 isotherm (1e-3..100 bar) solved as
               the reference's example does it: hybrid Anderson m=5 to
               RES < 1e-8 from Ninit = rho_bulk; N, Omega, steps and the
@@ -143,6 +147,36 @@ def _iso64_point(task):
     return i, b['mu'], bulk, N, s.omega0, s.curr_step, bool(conv)
 
 
+QN_CASES = [('bfgs', 'backtracking'), ('broyden', 'backtracking'), ('cg', 'backtracking'), ('bfgs', 'quadratic'),
+            ('bfgs', 'none')]
+
+
+def qn32(args):
+    """The reference's QuasiNewton on the 32^3 case at 1 bar, RES < 1e-8, from
+    Ninit = rho_bulk, for every direction / line-search variant in QN_CASES."""
+    ref = import_reference(args.reference)
+    solver = ref[2]
+    from cmmdft_b200.hosts import cubic_host_276
+    from cmmdft_b200.units import boltzmann
+    b = quiet(build, ref, 32, cubic_host_276(seed=0), 300.0, 1.0, tempfile.mkdtemp(prefix='cmm_qn_'))
+    V = b['fe'].part_dict['ExtPot'].potential
+    mb = b['mbwr']
+    mb.set_temperature(300.0)
+    bulk = np.nanmin(mb.solve_densities_from_chempots([b['mu']]), axis=1)[0]
+    rho0 = bulk * np.exp(-np.maximum(V, 0) / boltzmann / 300.0)
+    out = dict(mu=b['mu'], rho_bulk=bulk, threshold=1e-8)
+    for meth, ls in QN_CASES:
+        s = solver.QuasiNewton(b['prog'], nsteps=300, method=meth, line_search=ls, criterion='res',
+                               threshold=1e-8, verbose=False)
+        N, rho, conv = quiet(s.solve, b['mu'], rho0.copy(), 3)
+        tag = '%s_%s' % (meth, ls)
+        out[tag + '_N'], out[tag + '_steps'], out[tag + '_conv'] = N, s.curr_step, conv
+        out[tag + '_omega'] = s.omega0
+        print('qn %s: N=%.12e steps=%d conv=%s' % (tag, N, s.curr_step, conv), flush=True)
+    np.savez_compressed(os.path.join(HERE, 'qn32.npz'), **out)
+    print('wrote qn32.npz')
+
+
 def iso64(args):
     import multiprocessing as mp
     with mp.get_context('spawn').Pool(args.procs) as pool:
@@ -160,10 +194,13 @@ def main():
     ap.add_argument('--reference', default='/root/reference')
     ap.add_argument('--skip64', action='store_true')
     ap.add_argument('--iso64', action='store_true')
+    ap.add_argument('--qn', action='store_true')
     ap.add_argument('--procs', type=int, default=8)
     args = ap.parse_args()
     if args.iso64:
         return iso64(args)
+    if args.qn:
+        return qn32(args)
     ref = import_reference(args.reference)
     solver = ref[2]
     from cmmdft_b200.hosts import cubic_host_276, HELIUM
