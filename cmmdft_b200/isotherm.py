@@ -72,7 +72,7 @@ def grid_points(host, spacing=0.25 * angstrom):
 def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25 * angstrom,
                 method='hybridanderson', threshold=1e-8, criterion='res', nsteps=500, m=5, alpha_mix=0.1,
                 divergence_guard=True, anderson_coefs='slsqp', return_density=False, max_concurrent=4,
-                version='WBII', tailcorrections=False):
+                version='WBII', tailcorrections=False, memory_budget=None):
     """Isotherms of several hosts of uneven cells and grids in one call.
 
     The reference solves every (host, pressure) point in its own Program.solve
@@ -81,8 +81,10 @@ def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25
     up to ``max_concurrent`` hosts run at once, each driven by the native
     batched solver from its own host thread on its own CUDA stream, so the
     host decisions of one host overlap the kernels of the others.  A host's
-    device buffers (~460 B per grid point and pressure with m = 5) are
-    released when its solve ends; ``max_concurrent`` bounds the total.
+    device buffers (~520 B per grid point and pressure with m = 5) are
+    released when its solve ends.  A host starts only while the estimated
+    buffers of the running ones stay within ``memory_budget`` bytes (default
+    60% of the device's memory); a host larger than the budget runs alone.
 
     hosts: list of SyntheticHost-like hosts; pressures: one array for every
     host or a list with one array per host (atomic units); npoints: None
@@ -102,38 +104,58 @@ def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25
                           np.ndim(pressures[0]) == 1) else [pressures] * nh
     results = [None] * nh
     errors = []
-    gate = threading.Semaphore(max(1, int(max_concurrent)))
     cur = torch.cuda.current_stream()
     device = torch.cuda.current_device()
+    if memory_budget is None:
+        memory_budget = int(0.6 * torch.cuda.mem_get_info(device)[1])
+    need = [(640 * len(np.atleast_1d(plist[i])) + 512) * int(np.prod(shapes[i])) for i in range(nh)]   # bytes, generous
+    cond = threading.Condition()
+    state = dict(bytes=0, running=0)
+
+    def admit(i):
+        with cond:
+            cond.wait_for(lambda: state['running'] == 0 or (state['running'] < max(1, int(max_concurrent)) and
+                                                             state['bytes'] + need[i] <= memory_budget))
+            state['bytes'] += need[i]
+            state['running'] += 1
+
+    def leave(i):
+        with cond:
+            state['bytes'] -= need[i]
+            state['running'] -= 1
+            cond.notify_all()
 
     def run(i):
-        with gate:
-            try:
-                torch.cuda.set_device(device)
-                st = torch.cuda.Stream()
-                st.wait_stream(cur)
-                with torch.cuda.stream(st):
-                    fn = W.build_functional(hosts[i], shapes[i], temperature, guest, version=version,
-                                            tailcorrections=tailcorrections)
-                    P = np.asarray(plist[i], dtype=float)
-                    mus, bulks = W.isotherm_inputs(P, temperature, guest)
-                    rho0 = W.initial_density(fn, mus, ninit=bulks)
-                    s = BT.NativeBatchSolve(fn, mus, method=method, nsteps=nsteps, threshold=threshold,
-                                            criterion=criterion, m=m, alpha_mix=alpha_mix,
-                                            divergence_guard=divergence_guard, anderson_coefs=anderson_coefs)
-                    host = (torch.empty(tuple(rho0.shape), dtype=torch.float64, pin_memory=True)
-                            if return_density else None)
-                    N, rho, conv = s.solve(rho0, host_out=host)
-                    out = dict(mu=mus, rho_bulk=bulks, N=np.array(N), converged=np.array(conv),
-                               steps=s.steps.copy(), diverged=s.diverged.copy(), omega=np.array(s.omega0),
-                               npoints=shapes[i])
-                    st.synchronize()
-                    if return_density:
-                        out['rho'] = host.numpy()
-                    results[i] = out
-                    del s, fn, rho, rho0
-            except BaseException as e:  # re-raised on the calling thread
-                errors.append(e)
+        admit(i)
+        try:
+            torch.cuda.set_device(device)
+            st = torch.cuda.Stream()
+            st.wait_stream(cur)
+            with torch.cuda.stream(st):
+                fn = W.build_functional(hosts[i], shapes[i], temperature, guest, version=version,
+                                        tailcorrections=tailcorrections)
+                P = np.asarray(plist[i], dtype=float)
+                mus, bulks = W.isotherm_inputs(P, temperature, guest)
+                rho0 = W.initial_density(fn, mus, ninit=bulks)
+                s = BT.NativeBatchSolve(fn, mus, method=method, nsteps=nsteps, threshold=threshold,
+                                        criterion=criterion, m=m, alpha_mix=alpha_mix,
+                                        divergence_guard=divergence_guard, anderson_coefs=anderson_coefs)
+                host = (torch.empty(tuple(rho0.shape), dtype=torch.float64, pin_memory=True)
+                        if return_density else None)
+                N, rho, conv = s.solve(rho0, host_out=host)
+                out = dict(mu=mus, rho_bulk=bulks, N=np.array(N), converged=np.array(conv),
+                           steps=s.steps.copy(), diverged=s.diverged.copy(), omega=np.array(s.omega0),
+                           npoints=shapes[i])
+                st.synchronize()
+                if return_density:
+                    out['rho'] = host.numpy()
+                results[i] = out
+                del s, fn, rho, rho0
+            torch.cuda.empty_cache()
+        except BaseException as e:  # re-raised on the calling thread
+            errors.append(e)
+        finally:
+            leave(i)
 
     threads = [threading.Thread(target=run, args=(i,)) for i in range(nh)]
     for t in threads:
