@@ -205,31 +205,51 @@ struct PencilSet {
 template <bool INV>
 __device__ void big_stage(double2* s, int n, int R, int L, const double2* tw, int twn, const PencilSet& ps,
                           double2* tmp) {
+  // One thread per output pair (q, R - q) of a butterfly: both sums run over
+  // the same inputs with conjugate twiddles w^{rq} and w^{-rq}, so the four
+  // products a c, b s, a s, b c of x = a + ib and w = c + is serve both.
+  // Twiddle indices advance by addition (no division inside the sum).
   const int sR = L / R;
   const int rstep = twn / R, lstep = twn / L;
-  const int total = ps.npencil * n;
+  const int nq = R / 2 + 1;                 // q = 0 .. R/2; q pairs with R - q
+  const int nb = n / R;
+  const int total = ps.npencil * nb * nq;
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
-    const int p = t % ps.npencil, e = t / ps.npencil;
-    const int blk = e / L, rem = e - blk * L;
-    const int q = rem / sR, jj = rem - q * sR;
+    const int p = t % ps.npencil, u = t / ps.npencil;
+    const int q = u % nq, bj = u / nq;
+    const int blk = bj / sR, jj = bj - blk * sR;
     const double2* b = s + (p / ps.ppg) * ps.gstride + (p % ps.ppg) * ps.pstride + (blk * L + jj) * ps.estride;
     const int es = sR * ps.estride;
-    double2 acc = make_double2(0.0, 0.0);
+    const int wstep = q * rstep, xstep = jj * lstep;
+    double2 a1 = make_double2(0.0, 0.0), a2 = make_double2(0.0, 0.0);
+    int wi = 0, xi = 0;
     for (int r = 0; r < R; ++r) {
       double2 x = b[r * es];
-      const double2 w = tw[((r * q) % R) * rstep];
-      if (INV) {
-        if (jj) x = cmulc(x, tw[jj * r * lstep]);
-        acc = cadd(acc, cmulc(x, w));
-      } else {
-        acc = cadd(acc, cmul(x, w));
+      if (INV && jj) x = cmulc(x, tw[xi]);
+      const double2 w = tw[wi];
+      const double ac = x.x * w.x, bs = x.y * w.y, as = x.x * w.y, bc = x.y * w.x;
+      if (INV) {   // sum x conj(w) for q, sum x w for R - q
+        a1.x += ac + bs; a1.y += bc - as;
+        a2.x += ac - bs; a2.y += as + bc;
+      } else {     // sum x w for q, sum x conj(w) for R - q
+        a1.x += ac - bs; a1.y += as + bc;
+        a2.x += ac + bs; a2.y += bc - as;
       }
+      wi += wstep;
+      if (wi >= twn) wi -= twn;
+      xi += xstep;
     }
-    if (!INV && jj) acc = cmul(acc, tw[jj * q * lstep]);
-    tmp[t] = acc;
+    const int q2 = R - q;
+    if (!INV && jj) {
+      a1 = cmul(a1, tw[jj * q * lstep]);
+      a2 = cmul(a2, tw[jj * q2 * lstep]);
+    }
+    const int e1 = blk * L + q * sR + jj;
+    tmp[p + ps.npencil * e1] = a1;
+    if (q != 0 && 2 * q != R) tmp[p + ps.npencil * (blk * L + q2 * sR + jj)] = a2;
   }
   __syncthreads();
-  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+  for (int t = threadIdx.x; t < ps.npencil * n; t += blockDim.x) {
     const int p = t % ps.npencil, e = t / ps.npencil;
     s[(p / ps.ppg) * ps.gstride + (p % ps.ppg) * ps.pstride + e * ps.estride] = tmp[t];
   }
