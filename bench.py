@@ -163,8 +163,8 @@ def run_gpu(args):
     host, guest, pressures, fn, mus, bulks = setup_case(torch)
     rho0 = W.initial_density(fn, mus, ninit=bulks)
 
-    def one_solve(events=None):
-        s = BT.GroupedSolve(fn, mus, groups=args.groups, native=args.driver == "native", method="hybridanderson",
+    def one_solve(events=None, groups=None):
+        s = BT.GroupedSolve(fn, mus, groups=args.groups if groups is None else groups, native=args.driver == "native", method="hybridanderson",
                             nsteps=args.max_iters,
                             threshold=THRESH, criterion="res", divergence_guard=True, anderson_coefs=args.coefs)
         s.pipeline_events = events
@@ -200,7 +200,24 @@ def run_gpu(args):
     ms_max, nconv_all = reduce_over_ranks(ms, nconv, world, "cuda")
     value = nconv_all / (ms_max / 1e3)
 
-    # roofline of the fused functional pipeline, from its events in the timed region
+    # roofline of the fused functional pipeline, from its events in the timed
+    # region.  With concurrent groups a launch's events would also span the
+    # other group's kernels, so the pipeline is then timed in a separate
+    # pass of single-group solves (ms_ref: that pass's device time).
+    ms_ref, n_rl = ms_max / args.steps, args.steps
+    rl_pass = "timed region"
+    if args.groups > 1:
+        events = []
+        nref = max(1, min(args.steps, 5))
+        one_solve(None, groups=1)   # the single-group workspace, outside the pass
+        barrier()
+        e0.record()
+        for _ in range(nref):
+            one_solve(events, groups=1)
+        e1.record()
+        barrier()
+        ms_ref, n_rl = e0.elapsed_time(e1) / nref, nref
+        rl_pass = "%d single-group solves after the timed region" % nref
     tot_bytes = 0.0
     tot_ms = 0.0
     for a, b, want, nact in events:  # CUDA-event pairs (Python driver) or milliseconds (native driver)
@@ -218,7 +235,8 @@ def run_gpu(args):
                 "launches": len(events),
                 "bytes_per_launch": tot_bytes / max(len(events), 1),
                 "ms_per_launch": tot_ms / max(len(events), 1),
-                "share_of_step": tot_ms / ms_max if ms_max else None}
+                "share_of_step": (tot_ms / n_rl) / ms_ref if ms_ref else None,
+                "pass": rl_pass}
 
     # end to end through the public entry point (host arrays in, loadings + densities out)
     e2e = None
@@ -414,7 +432,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)   # ~0.5 s of timed solves: host jitter averages out
-    ap.add_argument("--groups", type=int, default=1, help="instance groups on concurrent streams")
+    ap.add_argument("--groups", type=int, default=2,
+                    help="instance groups on concurrent streams (one group's host decisions overlap the other's "
+                         "kernels)")
     ap.add_argument("--driver", choices=("native", "python"), default="native",
                     help="batched loop in the library (cmm_solve_batched) or in Python")
     ap.add_argument("--coefs", choices=("slsqp", "exact"), default="slsqp",
