@@ -453,7 +453,7 @@ class IsothermModel(object):
         if self.quantity == 'absolute':
             return np.asarray(sol['N'], dtype=np.float64)
         if self.quantity == 'omega':
-            return np.concatenate([s.omega0 for s in sol['solver'].solvers])
+            return np.asarray(sol['solver'].omega0)
         he = helium_fraction(self.plan, sol['host'], self.T, self.cutoff)
         return np.asarray(sol['N']) - np.asarray(sol['rho_bulk']) * he * sol['host'].volume
 
