@@ -428,6 +428,50 @@ def run_uneven(args):
     print(json.dumps(line))
 
 
+def run_gradient(args):
+    """Secondary workload (not the headline line): the differentiation case --
+    96^3 host (a = 24 A, 779 atoms), 16-point excess isotherm 0.01-10 bar,
+    squared error against a target from +-10% perturbed LJ parameters (seed
+    3), gradient with respect to the 10 parameters through the autograd
+    function (forward solve + implicit adjoint).  Wall clock with the device
+    synchronised; the central-difference cost is stated as 2 x 10 forward
+    solves, not run."""
+    import torch
+    from cmmdft_b200 import adjoint as A
+    from cmmdft_b200.hosts import cubic_host_779, methane_guest_params
+    from cmmdft_b200.units import bar
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    model = A.IsothermModel(cubic_host_779(0), methane_guest_params(), T, (96, 96, 96),
+                            np.logspace(-2, 1, 16) * bar, quantity="excess", threshold=1e-12, criterion="riue")
+    th0 = model.theta0
+    target_theta = th0 * (1 + np.random.default_rng(3).uniform(-0.1, 0.1, th0.shape))
+    with torch.no_grad():
+        target = model(torch.as_tensor(target_theta)).clone()
+    fw, bw = [], []
+    for _ in range(max(1, min(args.steps, 3))):
+        theta = torch.tensor(th0.copy(), requires_grad=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        loss = ((model(theta) - target) ** 2).sum()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        loss.backward()
+        torch.cuda.synchronize()
+        t2 = time.perf_counter()
+        fw.append(t1 - t0)
+        bw.append(t2 - t1)
+    f_ms, b_ms = 1e3 * float(np.median(fw)), 1e3 * float(np.median(bw))
+    line = {"metric": "excess-isotherm loss gradient, 10 LJ parameters, 96^3 FP64 (ms per gradient)",
+            "value": f_ms + b_ms, "unit": "ms", "n_gpus": 1, "steps": len(fw), "warmup": 1,
+            "ms_per_step": f_ms + b_ms, "higher_is_better": False, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "gradient-96cubed", "grid": [96, 96, 96], "atoms": 779, "pressures": 16,
+                       "parameters": int(len(th0)), "tolerance": "RIUE<1e-12", "forward_ms": f_ms,
+                       "adjoint_ms": b_ms, "central_difference_ms_estimate": 2 * len(th0) * f_ms,
+                       "timing": "wall clock, device synchronised, median"}}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -446,9 +490,16 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--max-iters", type=int, default=500, help="solver step cap (lower it only to profile)")
-    ap.add_argument("--workload", choices=("isotherm64", "uneven"), default="isotherm64",
-                    help="isotherm64: the headline 64^3 isotherm; uneven: 8 uneven hosts x 32 pressures")
+    ap.add_argument("--workload", choices=("isotherm64", "uneven", "gradient"), default="isotherm64",
+                    help="isotherm64: the headline 64^3 isotherm; uneven: 8 uneven hosts x 32 pressures; "
+                         "gradient: the 96^3 excess-isotherm loss gradient")
     args = ap.parse_args()
+    if args.workload == "gradient":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "the reference has no derivatives"}))
+        elif int(os.environ.get("RANK", "0")) == 0:
+            run_gradient(args)
+        return
     if args.workload == "uneven":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the uneven multi-host workload is timed on the "
