@@ -55,6 +55,7 @@ struct cmm_grid {
   void* dmem;
   GridDev dev;
   int staging;                 // 0: by size, 1: staged plane passes always
+  int exotic;                  // 1: radix 7, 11 or 13 or a Rader stage on some axis (kernels instantiated with -1)
 };
 
 static inline int cmm_div_up(long long a, long long b) { return (int)((a + b - 1) / b); }

@@ -25,13 +25,15 @@ extern "C" const char* cmm_status_string(int s) {
   return kStatusText[s];
 }
 
-// Radices for length n: 8s first, then 4, 2, then odd primes (<= 16).
-static bool factorise(int n, FftAxis* ax) {
+// Radices for length n: 8s first (4s when no8), then 4, 2, then odd primes
+// (primes > 16 run as Rader or direct-DFT stages).
+static bool factorise(int n, FftAxis* ax, bool no8 = false) {
   ax->n = n;
   ax->nstage = 0;
+  ax->rader = nullptr;
   int m = n;
   std::vector<int> r;
-  while (m % 8 == 0) { r.push_back(8); m /= 8; }
+  while (!no8 && m % 8 == 0) { r.push_back(8); m /= 8; }
   while (m % 4 == 0) { r.push_back(4); m /= 4; }
   while (m % 2 == 0) { r.push_back(2); m /= 2; }
   for (int p = 3; m > 1; p += 2)   // odd primes in increasing order; primes > 16 run as direct-DFT stages
@@ -75,6 +77,90 @@ static void twiddles(int n, std::vector<double>& out) {
     out[2 * t] = (double)cosl(a);
     out[2 * t + 1] = (double)sinl(a);
   }
+}
+
+// Host tables of one Rader stage (prime radix R, M = R - 1 smooth).
+struct RaderHost {
+  FftAxis axm;
+  std::vector<double> twm, kf, ki;   // interleaved re, im
+  std::vector<int> gin, gout;
+};
+
+static long long powmod(long long b, long long e, long long m) {
+  long long r = 1;
+  b %= m;
+  while (e) {
+    if (e & 1) r = r * b % m;
+    b = b * b % m;
+    e >>= 1;
+  }
+  return r;
+}
+
+// Smallest prime run by Rader's algorithm: below it the paired direct DFT
+// (R/2 + 1 sums of R terms per butterfly, no extra barrier) is cheaper than
+// the Rader stage's gather, two length R - 1 transforms, product and scatter
+// (measured on B200: a 41 stage slower with Rader, 97 and above faster).
+#define CMM_RADER_MIN 67
+
+// false when R < CMM_RADER_MIN or R - 1 has a prime factor above
+// CMM_MAX_SMALL_RADIX (the stage then stays a direct DFT).
+static bool rader_plan(int R, RaderHost& h) {
+  const int M = R - 1;
+  if (R < CMM_RADER_MIN) return false;
+  if (!factorise(M, &h.axm, true) || h.axm.big) return false;
+  std::vector<int> pf;
+  for (int m = M, p = 2; m > 1; ++p)
+    if (m % p == 0) {
+      pf.push_back(p);
+      while (m % p == 0) m /= p;
+    }
+  int g = 0;
+  for (int c = 2; c < R && !g; ++c) {
+    bool ok = true;
+    for (int f : pf) ok = ok && powmod(c, M / f, R) != 1;
+    if (ok) g = c;
+  }
+  if (!g) return false;
+  const int ginv = (int)powmod(g, R - 2, R);
+  h.gin.resize(M);
+  h.gout.resize(M);
+  for (int k = 0, a = 1, b = 1; k < M; ++k) {
+    h.gout[k] = a;
+    h.gin[k] = b;
+    a = (int)((long long)a * g % R);
+    b = (int)((long long)b * ginv % R);
+  }
+  twiddles(M, h.twm);
+  // B_f = sum_j b_j w_M^{jf} with b_j = w_R^{g^j} (w = e^{-2 pi i/.}); the
+  // inverse stage's kernel conj(b_j) has spectrum conj(B_{-f}).
+  const long double pi = 3.141592653589793238462643383279502884L;
+  std::vector<long double> cr(R), sr(R), cm(M), sm(M);
+  for (int t = 0; t < R; ++t) { cr[t] = cosl(-2 * pi * t / R); sr[t] = sinl(-2 * pi * t / R); }
+  for (int t = 0; t < M; ++t) { cm[t] = cosl(-2 * pi * t / M); sm[t] = sinl(-2 * pi * t / M); }
+  std::vector<long double> Br(M), Bi(M);
+  for (int f = 0; f < M; ++f) {
+    long double re = 0, im = 0;
+    for (int j = 0; j < M; ++j) {
+      const int a = h.gout[j], w = (int)((long long)j * f % M);
+      re += cr[a] * cm[w] - sr[a] * sm[w];
+      im += cr[a] * sm[w] + sr[a] * cm[w];
+    }
+    Br[f] = re / M;
+    Bi[f] = im / M;
+  }
+  std::vector<int> kpos(M);
+  dif_positions(h.axm, kpos.data());
+  h.kf.resize(2 * (size_t)M);
+  h.ki.resize(2 * (size_t)M);
+  for (int p = 0; p < M; ++p) {
+    const int f = kpos[p], fm = (M - f) % M;
+    h.kf[2 * p] = (double)Br[f];
+    h.kf[2 * p + 1] = (double)Bi[f];
+    h.ki[2 * p] = (double)Br[fm];
+    h.ki[2 * p + 1] = -(double)Bi[fm];
+  }
+  return true;
 }
 
 static int signed_freq(int k, int n) {
@@ -176,6 +262,35 @@ extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_
     o_nq[a] = bump(sizeof(int) * npos[a]);
   }
   size_t o_wt3 = bump(sizeof(double) * h3);
+  // Rader tables: per axis an array of nstage RaderTab (M = 0 for other
+  // stages) followed by the tables of each Rader stage.
+  FftAxis* axes[3] = {&g->ax1, &g->ax2, &g->ax3};
+  std::vector<RaderHost> rh[3];
+  size_t o_rt[3] = {0, 0, 0};
+  std::vector<std::vector<size_t>> o_rs(3);
+  for (int a = 0; a < 3; ++a) {
+    const FftAxis& ax = *axes[a];
+    rh[a].resize(ax.nstage);
+    bool any = false;
+    std::vector<bool> use(ax.nstage, false);
+    for (int st = 0; st < ax.nstage; ++st)
+      if (ax.radix[st] > CMM_MAX_SMALL_RADIX && rader_plan(ax.radix[st], rh[a][st])) use[st] = any = true;
+    if (!any) continue;
+    o_rt[a] = bump(sizeof(RaderTab) * ax.nstage);
+    o_rs[a].assign(ax.nstage, 0);
+    for (int st = 0; st < ax.nstage; ++st)
+      if (use[st]) {
+        const size_t M = ax.radix[st] - 1;
+        o_rs[a][st] = bump(3 * sizeof(double2) * M + 2 * sizeof(int) * M);
+      }
+  }
+  // kernels instantiated with -1 (odd radices 7, 11, 13 and Rader stages)
+  g->exotic = 0;
+  for (int a = 0; a < 3; ++a)
+    for (int st = 0; st < axes[a]->nstage; ++st) {
+      const int r = axes[a]->radix[st];
+      if (r == 7 || r == 11 || r == 13 || (!o_rs[a].empty() && o_rs[a][st])) g->exotic = 1;
+    }
   std::vector<char> host(off);
   memcpy(&host[o_tw1], tw1.data(), sizeof(double) * tw1.size());
   memcpy(&host[o_tw2], tw2.data(), sizeof(double) * tw2.size());
@@ -191,6 +306,35 @@ extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_
   if (cudaMalloc(&g->dmem, off) != cudaSuccess) {
     free(g->hpos_k1); free(g->hpos_k2); free(g->hpos_k3); free(g);
     return CMM_ERR_NOMEM;
+  }
+  for (int a = 0; a < 3; ++a) {
+    if (o_rs[a].empty()) continue;
+    FftAxis& ax = *axes[a];
+    char* dbase = (char*)g->dmem;
+    for (int st = 0; st < ax.nstage; ++st) {
+      RaderTab rt;
+      memset(&rt, 0, sizeof(rt));
+      if (o_rs[a][st]) {
+        const RaderHost& h = rh[a][st];
+        const size_t M = ax.radix[st] - 1, o = o_rs[a][st];
+        rt.axm = h.axm;
+        rt.M = (int)M;
+        const size_t o_twm = o, o_kf = o + sizeof(double2) * M, o_ki = o + 2 * sizeof(double2) * M,
+                     o_gin = o + 3 * sizeof(double2) * M, o_gout = o_gin + sizeof(int) * M;
+        memcpy(&host[o_twm], h.twm.data(), sizeof(double2) * M);
+        memcpy(&host[o_kf], h.kf.data(), sizeof(double2) * M);
+        memcpy(&host[o_ki], h.ki.data(), sizeof(double2) * M);
+        memcpy(&host[o_gin], h.gin.data(), sizeof(int) * M);
+        memcpy(&host[o_gout], h.gout.data(), sizeof(int) * M);
+        rt.twm = (const double2*)(dbase + o_twm);
+        rt.kf = (const double2*)(dbase + o_kf);
+        rt.ki = (const double2*)(dbase + o_ki);
+        rt.gin = (const int*)(dbase + o_gin);
+        rt.gout = (const int*)(dbase + o_gout);
+      }
+      memcpy(&host[o_rt[a] + sizeof(RaderTab) * st], &rt, sizeof(rt));
+    }
+    ax.rader = (const RaderTab*)(dbase + o_rt[a]);
   }
   if (cudaMemcpy(g->dmem, host.data(), off, cudaMemcpyHostToDevice) != cudaSuccess) {
     cudaFree(g->dmem);

@@ -42,12 +42,14 @@ __host__ __device__ inline size_t plane_smem_bytes(int n2, int n3, int nslot) {
 }
 
 // Compile-time shape of a plane pass: N2C = y length, M3C = z half length
-// (0 = take them from the plan at run time).
+// (0 = take them from the plan at run time, radices 2, 3, 4, 5, 8 and
+// direct-DFT stages; -1 = from the plan, also radices 7, 11, 13 and Rader
+// stages).
 template <int N2C, int M3C>
 struct PlaneShape {
   int n2, m3, h3, n3;
   __device__ PlaneShape(const GridDev& g)
-      : n2(N2C ? N2C : g.n2), m3(M3C ? M3C : g.m3), h3((M3C ? M3C : g.m3) + 1), n3(2 * (M3C ? M3C : g.m3)) {}
+      : n2(N2C > 0 ? N2C : g.n2), m3(M3C > 0 ? M3C : g.m3), h3((M3C > 0 ? M3C : g.m3) + 1), n3(2 * (M3C > 0 ? M3C : g.m3)) {}
 };
 
 template <int N2C, int M3C>
@@ -70,13 +72,13 @@ template <bool INV, int NC>
 __device__ __forceinline__ void axis_fft(double2* base, const FftAxis& ax, const double2* tw, int twmul,
                                          int npencil, int pstride, int estride, double2* tmp = nullptr) {
   if constexpr (NC > 0) fft_ct<INV, NC>(base, tw, twmul, npencil, pstride, estride);
-  else fft_rt<INV>(base, ax, tw, twmul, npencil, pstride, estride, tmp);
+  else fft_rt<INV, (NC < 0)>(base, ax, tw, twmul, npencil, pstride, estride, tmp);
 }
 
 // R2C twist on `nrow` rows: pairs (k, m3-k), k = 0..m3/2, rows fastest.
 template <int M3C>
 __device__ void r2c_twist_rows(const GridDev& g, const PlaneSmem& s, int nrow) {
-  const int m3 = M3C ? M3C : g.m3, h3 = m3 + 1;
+  const int m3 = M3C > 0 ? M3C : g.m3, h3 = m3 + 1;
   const int total = nrow * (m3 / 2 + 1);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     const int k = t / nrow, row = t - k * nrow;
@@ -102,7 +104,7 @@ __device__ void r2c_twist_rows(const GridDev& g, const PlaneSmem& s, int nrow) {
 // C2R twist: Zin[k] = (X[k] + conj X[m-k]) + i (X[k] - conj X[m-k]) e^{2 pi i k / N3}.
 template <int M3C>
 __device__ void c2r_twist_rows(const GridDev& g, const PlaneSmem& s, int nrow) {
-  const int m3 = M3C ? M3C : g.m3, h3 = m3 + 1;
+  const int m3 = M3C > 0 ? M3C : g.m3, h3 = m3 + 1;
   const int total = nrow * (m3 / 2 + 1);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     const int k = t / nrow, row = t - k * nrow;
@@ -126,14 +128,14 @@ __device__ void c2r_twist_rows(const GridDev& g, const PlaneSmem& s, int nrow) {
 // z rows only: real rows (natural z) -> DIF z + R2C twist, and back.
 template <int M3C>
 __device__ void row_forward(const GridDev& g, const PlaneSmem& s, int nrow) {
-  const int h3 = (M3C ? M3C : g.m3) + 1;
+  const int h3 = (M3C > 0 ? M3C : g.m3) + 1;
   axis_fft<false, M3C>(s.slots, g.ax3, s.tw3, 2, nrow, h3, 1);
   r2c_twist_rows<M3C>(g, s, nrow);
 }
 
 template <int M3C>
 __device__ void row_inverse(const GridDev& g, const PlaneSmem& s, int nrow) {
-  const int h3 = (M3C ? M3C : g.m3) + 1;
+  const int h3 = (M3C > 0 ? M3C : g.m3) + 1;
   c2r_twist_rows<M3C>(g, s, nrow);
   axis_fft<true, M3C>(s.slots, g.ax3, s.tw3, 2, nrow, h3, 1);
 }
@@ -273,7 +275,7 @@ __host__ __device__ inline size_t col_smem_bytes(int n1, int tc, int nslot, int 
 template <int N1C, int TCC>
 struct ColShape {
   int n1, tc;
-  __device__ ColShape(const GridDev& g, int tc_rt) : n1(N1C ? N1C : g.n1), tc(TCC ? TCC : tc_rt) {}
+  __device__ ColShape(const GridDev& g, int tc_rt) : n1(N1C > 0 ? N1C : g.n1), tc(TCC ? TCC : tc_rt) {}
 };
 
 template <int N1C, int TCC>
@@ -922,7 +924,7 @@ k_ypass(GridDev g, const int* __restrict__ active, const double2* src, double2* 
   const int i1 = blockIdx.y;
   const int b = blockIdx.z / nfield, f = blockIdx.z - b * nfield;
   if (active && !active[b]) return;
-  const int n2 = N2C ? N2C : g.n2, h3 = g.h3;
+  const int n2 = N2C > 0 ? N2C : g.n2, h3 = g.h3;
   extern __shared__ double2 smem_d2[];
   double2* t = smem_d2;       // [n2][tc]
   double2* tw = t + (size_t)n2 * tc;
@@ -962,8 +964,8 @@ static inline size_t zrow_smem_bytes_g(const cmm_grid* g, int nrow) {
 template <int M3C>
 __device__ inline PlaneSmem zrow_smem_setup(const GridDev& g, int nrow) {
   extern __shared__ double2 smem_d2[];
-  const bool full = (M3C == 0) && g.zfull;
-  const int m3 = M3C ? M3C : g.m3;
+  const bool full = (M3C <= 0) && g.zfull;
+  const int m3 = M3C > 0 ? M3C : g.m3;
   const int rs = full ? g.n3 : m3 + 1, n3 = full ? g.n3 : 2 * m3, nz = full ? g.n3 : m3;
   PlaneSmem s;
   s.slots = smem_d2;
@@ -984,8 +986,8 @@ __device__ inline PlaneSmem zrow_smem_setup(const GridDev& g, int nrow) {
 template <int M3C>
 __device__ inline void zrow_load(const GridDev& g, const PlaneSmem& s, int nf, int f, int nr,
                                  const double2* __restrict__ src) {
-  const bool full = (M3C == 0) && g.zfull;
-  const int h3 = M3C ? M3C + 1 : g.h3;
+  const bool full = (M3C <= 0) && g.zfull;
+  const int h3 = M3C > 0 ? M3C + 1 : g.h3;
   const int rs = full ? g.n3 : h3;
   for (int i = threadIdx.x; i < nr * h3; i += blockDim.x) {
     const int r = i / h3, c = i - r * h3;
@@ -1005,8 +1007,8 @@ __device__ inline void zrow_load(const GridDev& g, const PlaneSmem& s, int nf, i
 template <int M3C>
 __device__ inline void zrow_store(const GridDev& g, const PlaneSmem& s, int nf, int f, int nr,
                                   double2* __restrict__ dst) {
-  const bool full = (M3C == 0) && g.zfull;
-  const int h3 = M3C ? M3C + 1 : g.h3;
+  const bool full = (M3C <= 0) && g.zfull;
+  const int h3 = M3C > 0 ? M3C + 1 : g.h3;
   const int rs = full ? g.n3 : h3;
   for (int i = threadIdx.x; i < nr * h3; i += blockDim.x) {
     const int r = i / h3, c = i - r * h3;
@@ -1018,36 +1020,36 @@ __device__ inline void zrow_store(const GridDev& g, const PlaneSmem& s, int nf, 
 // Real element j of slot row r * nf + f (after zrow_inverse).
 template <int M3C>
 __device__ __forceinline__ double& zrow_rel(const GridDev& g, const PlaneSmem& s, int nf, int f, int r, int j) {
-  if constexpr (M3C == 0) {
+  if constexpr (M3C <= 0) {
     if (g.zfull) return s.slots[((size_t)r * nf + f) * g.n3 + j].x;
   }
-  return ((double*)(s.slots + ((size_t)r * nf + f) * (M3C ? M3C + 1 : g.h3)))[j];
+  return ((double*)(s.slots + ((size_t)r * nf + f) * (M3C > 0 ? M3C + 1 : g.h3)))[j];
 }
 
 template <int M3C>
 __device__ void zrow_inverse(const GridDev& g, const PlaneSmem& s, int nrow) {
-  if constexpr (M3C == 0) {
+  if constexpr (M3C <= 0) {
     if (g.zfull) {
-      axis_fft<true, 0>(s.slots, g.ax3, s.tw3, 1, nrow, g.n3, 1, s.tmp);
+      axis_fft<true, M3C>(s.slots, g.ax3, s.tw3, 1, nrow, g.n3, 1, s.tmp);
       return;
     }
   }
-  const int h3 = (M3C ? M3C : g.m3) + 1;
+  const int h3 = (M3C > 0 ? M3C : g.m3) + 1;
   c2r_twist_rows<M3C>(g, s, nrow);
   axis_fft<true, M3C>(s.slots, g.ax3, s.tw3, 2, nrow, h3, 1, s.tmp);
 }
 
 template <int M3C>
 __device__ void zrow_forward(const GridDev& g, const PlaneSmem& s, int nrow) {
-  if constexpr (M3C == 0) {
+  if constexpr (M3C <= 0) {
     if (g.zfull) {
       for (int i = threadIdx.x; i < nrow * g.n3; i += blockDim.x) s.slots[i].y = 0.0;
       __syncthreads();
-      axis_fft<false, 0>(s.slots, g.ax3, s.tw3, 1, nrow, g.n3, 1, s.tmp);
+      axis_fft<false, M3C>(s.slots, g.ax3, s.tw3, 1, nrow, g.n3, 1, s.tmp);
       return;
     }
   }
-  const int h3 = (M3C ? M3C : g.m3) + 1;
+  const int h3 = (M3C > 0 ? M3C : g.m3) + 1;
   axis_fft<false, M3C>(s.slots, g.ax3, s.tw3, 2, nrow, h3, 1, s.tmp);
   r2c_twist_rows<M3C>(g, s, nrow);
 }
@@ -1066,7 +1068,7 @@ k_zrow_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm
   if (active && !active[b]) return;
   constexpr int tb = WDA ? 6 : 5;
   constexpr int nf = tb + (TEN ? 6 : 0);
-  const int h3 = M3C ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
+  const int h3 = M3C > 0 ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
   PlaneSmem s = zrow_smem_setup<M3C>(g, nf * chunk);
   const size_t poff = ((size_t)b * g.n1 + i1) * n2 * h3;
   const bool do_c1 = (want & 1) != 0, do_phi = (want & 3) != 0;
@@ -1324,7 +1326,7 @@ k_zrow_op(GridDev g, const int* __restrict__ active, Op op, const double2* __res
           double2* __restrict__ spec_out, int chunk, double* __restrict__ part, int nslot_part) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
-  const int h3 = M3C ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
+  const int h3 = M3C > 0 ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
   PlaneSmem s = zrow_smem_setup<M3C>(g, chunk);
   const size_t poff = ((size_t)b * g.n1 + i1) * n2 * h3;
   const size_t plane = (size_t)i1 * n2 * n3;
@@ -1641,16 +1643,18 @@ static int set_smem(const void* fn, size_t bytes) {
   return CMM_OK;
 }
 
-// Shape specialisations compiled with compile-time transform lengths.
+// Shape specialisations compiled with compile-time transform lengths; the
+// run-time-length kernels come in two instantiations, 0 (radices 2, 3, 4, 5,
+// 8 and direct-DFT stages) and -1 (also 7, 11, 13 and Rader stages).
 static int plane_kind(const cmm_grid* g) {
   if (g->n2 == 64 && g->m3 == 32) return 1;
   if (g->n2 == 32 && g->m3 == 16) return 2;
-  return 0;
+  return g->exotic ? -1 : 0;
 }
 static int col_kind(const cmm_grid* g) {
   if (g->n1 == 64) return 1;
   if (g->n1 == 32) return 2;
-  return 0;
+  return g->exotic ? -1 : 0;
 }
 
 #define LAUNCH_PLANE(kind, kern, grd, smem, st, ...)                                      \
@@ -1662,6 +1666,9 @@ static int col_kind(const cmm_grid* g) {
     } else if ((kind) == 2) {                                                            \
       if ((rc_ = set_smem((const void*)kern<32, 16>, smem))) return rc_;                \
       kern<32, 16><<<grd, CMM_PLANE_THREADS, smem, st>>>(__VA_ARGS__);                   \
+    } else if ((kind) == -1) {                                                           \
+      if ((rc_ = set_smem((const void*)kern<-1, -1>, smem))) return rc_;                \
+      kern<-1, -1><<<grd, CMM_PLANE_THREADS, smem, st>>>(__VA_ARGS__);                 \
     } else {                                                                             \
       if ((rc_ = set_smem((const void*)kern<0, 0>, smem))) return rc_;                  \
       kern<0, 0><<<grd, CMM_PLANE_THREADS, smem, st>>>(__VA_ARGS__);                     \
@@ -1677,6 +1684,9 @@ static int col_kind(const cmm_grid* g) {
     } else if ((kind) == 2) {                                                            \
       if ((rc_ = set_smem((const void*)kern<32, 16>, smem))) return rc_;                \
       kern<32, 16><<<grd, nthr, smem, st>>>(__VA_ARGS__);                                \
+    } else if ((kind) == -1) {                                                           \
+      if ((rc_ = set_smem((const void*)kern<-1, -1>, smem))) return rc_;                \
+      kern<-1, -1><<<grd, nthr, smem, st>>>(__VA_ARGS__);                              \
     } else {                                                                             \
       if ((rc_ = set_smem((const void*)kern<0, 0>, smem))) return rc_;                  \
       kern<0, 0><<<grd, nthr, smem, st>>>(__VA_ARGS__);                                  \
@@ -1692,6 +1702,9 @@ static int col_kind(const cmm_grid* g) {
     } else if ((kind) == 2) {                                                            \
       if ((rc_ = set_smem((const void*)kern<32, 8>, smem))) return rc_;                \
       kern<32, 8><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                     \
+    } else if ((kind) == -1) {                                                           \
+      if ((rc_ = set_smem((const void*)kern<-1, 0>, smem))) return rc_;                 \
+      kern<-1, 0><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                      \
     } else {                                                                             \
       if ((rc_ = set_smem((const void*)kern<0, 0>, smem))) return rc_;                  \
       kern<0, 0><<<grd, CMM_COL_THREADS, smem, st>>>(__VA_ARGS__);                       \
@@ -1701,7 +1714,7 @@ static int col_kind(const cmm_grid* g) {
 // Column tile width: 8 columns (128 B rows) for the specialised kernels, up to
 // 16 when it fits otherwise.
 static int col_tile(const cmm_grid* g, int nslot) {
-  if (col_kind(g)) return 8;
+  if (col_kind(g) > 0) return 8;
   int tc = 16;
   while (tc > 1 && col_smem_bytes(g->n1, tc, nslot, g->ax1.big) > 200 * 1024) tc /= 2;
   return tc;
@@ -1726,6 +1739,9 @@ static int ypass(const cmm_grid* g, int batch, const int* act, const double2* sr
   } else if (g->n2 == 32) {
     if ((rc = set_smem((const void*)k_ypass<32>, sb))) return rc;
     k_ypass<32><<<grd, CMM_COL_THREADS, sb, st>>>(g->dev, act, src, dst, fs, nfield, tc, inv);
+  } else if (g->exotic) {
+    if ((rc = set_smem((const void*)k_ypass<-1>, sb))) return rc;
+    k_ypass<-1><<<grd, CMM_COL_THREADS, sb, st>>>(g->dev, act, src, dst, fs, nfield, tc, inv);
   } else {
     if ((rc = set_smem((const void*)k_ypass<0>, sb))) return rc;
     k_ypass<0><<<grd, CMM_COL_THREADS, sb, st>>>(g->dev, act, src, dst, fs, nfield, tc, inv);
@@ -1743,10 +1759,9 @@ static bool plane_staged(const cmm_grid* g, int nf) {
 
 // Compile-time z half length of the z-row kernels (0: from the plan).
 static int zrow_m3(const cmm_grid* g) {
-  if (g->dev.zfull) return 0;
-  if (g->m3 == 32) return 32;
-  if (g->m3 == 16) return 16;
-  return 0;
+  if (!g->dev.zfull && g->m3 == 32) return 32;
+  if (!g->dev.zfull && g->m3 == 16) return 16;
+  return g->exotic ? -1 : 0;
 }
 
 // y rows per z-row chunk so that nf fields fit in the shared-memory budget (0: none fit).
@@ -1777,6 +1792,7 @@ static int zrow_op(const cmm_grid* g, int batch, const int* act, const Op& op, c
   switch (zrow_m3(g)) {
     case 32: return zrow_op_m3<32>(g, batch, act, op, in, out, chunk, part, nslot, st);
     case 16: return zrow_op_m3<16>(g, batch, act, op, in, out, chunk, part, nslot, st);
+    case -1: return zrow_op_m3<-1>(g, batch, act, op, in, out, chunk, part, nslot, st);
     default: return zrow_op_m3<0>(g, batch, act, op, in, out, chunk, part, nslot, st);
   }
 }
@@ -1817,6 +1833,7 @@ static int zrow_fmt(const cmm_grid* g, int batch, const int* act, double R, int 
   switch (zrow_m3(g)) {
     case 32: return zrow_fmt_m3<32>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
     case 16: return zrow_fmt_m3<16>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
+    case -1: return zrow_fmt_m3<-1>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
     default: return zrow_fmt_m3<0>(g, batch, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd, st);
   }
 }
@@ -1840,7 +1857,7 @@ k_zrow_hvp(GridDev g, const int* __restrict__ active, double R, int version, con
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
   constexpr int nf = 5 + (TEN ? 6 : 0);
-  const int h3 = M3C ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
+  const int h3 = M3C > 0 ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
   PlaneSmem s = zrow_smem_setup<M3C>(g, nf * chunk);
   const size_t poff = ((size_t)b * g.n1 + i1) * n2 * h3;
   const size_t roff = ((size_t)b * g.n1 + i1) * n2 * n3;
@@ -1945,6 +1962,7 @@ extern "C" int cmm_fmt_hvp(const cmm_grid* g, int batch, const int* d_active, do
   switch (zrow_m3(g)) {
     case 32: rc = zrow_hvp_m3<32>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
     case 16: rc = zrow_hvp_m3<16>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
+    case -1: rc = zrow_hvp_m3<-1>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
     default: rc = zrow_hvp_m3<0>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st);
   }
   if (rc) return rc;

@@ -17,7 +17,9 @@
 
 #define CMM_MAX_STAGES 16
 
-#define CMM_MAX_SMALL_RADIX 16   // larger radices run as two-phase direct DFT stages
+#define CMM_MAX_SMALL_RADIX 16   // larger (prime) radices run as Rader or direct-DFT stages
+
+struct RaderTab;
 
 struct FftAxis {
   int n;                         // transform length
@@ -25,6 +27,24 @@ struct FftAxis {
   int big;                       // 1 when a radix exceeds CMM_MAX_SMALL_RADIX (needs scratch)
   int radix[CMM_MAX_STAGES];     // radix of stage s (forward order)
   int span[CMM_MAX_STAGES];      // block length L_s at stage s (L_0 = n)
+  const RaderTab* rader;         // device array indexed by stage (null: every big stage is a direct DFT)
+};
+
+// Rader's algorithm (C. M. Rader, Proc. IEEE 56, 1107 (1968)) for a prime
+// radix R whose M = R - 1 factors into radices <= 16.  With g a primitive
+// root mod R the outputs q = g^k, k < M, are
+//   y_{g^k} = x_0 + sum_m x_{g^-m} w_R^{g^(k-m)},
+// a length-M cyclic convolution: forward FFT of the permuted inputs, product
+// with the transformed kernel, inverse FFT.  y_0 = x_0 + sum_{r>0} x_r is the
+// DC bin of the forward transform.
+struct RaderTab {
+  FftAxis axm;          // plan of the length-M transforms (no big radix)
+  int M;                // 0: the stage keeps the direct DFT
+  const double2* twm;   // w_M^t, t < M
+  const double2* kf;    // DFT_M of b_j = w_R^{g^j}, divided by M, at the DIF output positions (forward stage)
+  const double2* ki;    // the same for b_j = conj(w_R^{g^j}) (inverse stage)
+  const int* gin;       // gin[m] = g^-m mod R
+  const int* gout;      // gout[k] = g^k mod R
 };
 
 // ------------------------------------------------------------ complex ----
@@ -123,30 +143,13 @@ __device__ __forceinline__ void dft5(double2* v) {
   v[3] = csub(a2, b2);
 }
 
-// Generic odd radix (primes > 5): direct DFT through the axis twiddle table.
-// tw holds w_n^t for the axis length n (table length twn); w_R = w_n^{n/R}.
-template <bool INV>
-__device__ __forceinline__ void dft_generic(double2* v, int R, const double2* tw, int twn) {
-  double2 out[16];
-  int step = twn / R;
-  for (int q = 0; q < R; ++q) {
-    double2 acc = v[0];
-    for (int r = 1; r < R; ++r) {
-      double2 w = tw[((r * q) % R) * step];
-      acc = cadd(acc, INV ? cmulc(v[r], w) : cmul(v[r], w));
-    }
-    out[q] = acc;
-  }
-  for (int q = 0; q < R; ++q) v[q] = out[q];
-}
-
 template <int R, bool INV>
 __device__ __forceinline__ void dftR(double2* v, const double2* tw, int twn) {
-  if (R == 2) dft2<INV>(v);
-  else if (R == 4) dft4<INV>(v);
-  else if (R == 8) dft8<INV>(v);
-  else if (R == 3) dft3<INV>(v);
-  else if (R == 5) dft5<INV>(v);
+  if constexpr (R == 2) dft2<INV>(v);
+  else if constexpr (R == 4) dft4<INV>(v);
+  else if constexpr (R == 8) dft8<INV>(v);
+  else if constexpr (R == 3) dft3<INV>(v);
+  else if constexpr (R == 5) dft5<INV>(v);
 }
 
 // One butterfly of a stage.  Forward (DIF): y = DFT_R(x); y_q *= w_L^{jj q}.
@@ -174,20 +177,67 @@ __device__ __forceinline__ void butterfly(double2* b, int es, const double2* tw,
   for (int r = 0; r < R; ++r) b[r * es] = v[r];
 }
 
-template <bool INV>
-__device__ __forceinline__ void butterfly_generic(double2* b, int R, int es, const double2* tw, int twn, int tb) {
-  double2 v[16];
-  for (int r = 0; r < R; ++r) v[r] = b[r * es];
-  if (INV) {
-    if (tb)
-      for (int q = 1; q < R; ++q) v[q] = cmulc(v[q], tw[tb * q]);
-    dft_generic<true>(v, R, tw, twn);
-  } else {
-    dft_generic<false>(v, R, tw, twn);
-    if (tb)
-      for (int q = 1; q < R; ++q) v[q] = cmul(v[q], tw[tb * q]);
+// Butterfly of an odd prime radix R (7, 11, 13).  The output pairs
+// (q, R - q) share the sums and differences of the input pairs (r, R - r):
+//   y_q, y_{R-q} = x_0 + sum_r (x_r + x_{R-r}) cos(2 pi rq/R)
+//                  -/+ i sum_r (x_r - x_{R-r}) sin(2 pi rq/R)
+// (forward signs; the inverse swaps them).  Only the pair sums and
+// differences and the R - 1 cos/sin values stay in registers; each output
+// pair is written back as soon as it is formed.  Twiddles as in butterfly().
+// Not inlined: its registers would otherwise raise the allocation of every
+// kernel that holds an FFT loop.
+template <int R, bool INV>
+__device__ __noinline__ void butterfly_odd(double2* b, int es, const double2* tw, int twn, int tb) {
+  constexpr int h = (R - 1) / 2;
+  const int step = twn / R;
+  double c[h + 1], sn[h + 1];
+#pragma unroll
+  for (int k = 1; k <= h; ++k) {
+    const double2 w = tw[k * step];
+    c[k] = w.x;
+    sn[k] = -w.y;
   }
-  for (int r = 0; r < R; ++r) b[r * es] = v[r];
+  const double2 x0 = b[0];
+  double2 sp[h + 1], dm[h + 1];
+  double2 y0 = x0;
+#pragma unroll
+  for (int r = 1; r <= h; ++r) {
+    double2 u = b[r * es], w = b[(R - r) * es];
+    if (INV && tb) {
+      u = cmulc(u, tw[tb * r]);
+      w = cmulc(w, tw[tb * (R - r)]);
+    }
+    sp[r] = cadd(u, w);
+    dm[r] = csub(u, w);
+    y0 = cadd(y0, sp[r]);
+  }
+  b[0] = y0;
+#pragma unroll
+  for (int q = 1; q <= h; ++q) {
+    double2 A = x0, B = make_double2(0.0, 0.0);
+#pragma unroll
+    for (int r = 1; r <= h; ++r) {
+      const int m = (r * q) % R;
+      const int k = m <= h ? m : R - m;
+      A.x += sp[r].x * c[k];
+      A.y += sp[r].y * c[k];
+      if (m <= h) {
+        B.x += dm[r].x * sn[k];
+        B.y += dm[r].y * sn[k];
+      } else {
+        B.x -= dm[r].x * sn[k];
+        B.y -= dm[r].y * sn[k];
+      }
+    }
+    const double2 iB = rot_mi<INV>(B);
+    double2 yq = cadd(A, iB), ym = csub(A, iB);
+    if (!INV && tb) {
+      yq = cmul(yq, tw[tb * q]);
+      ym = cmul(ym, tw[tb * (R - q)]);
+    }
+    b[q * es] = yq;
+    b[(R - q) * es] = ym;
+  }
 }
 
 // Pencil geometry inside shared memory:
@@ -256,12 +306,144 @@ __device__ void big_stage(double2* s, int n, int R, int L, const double2* tw, in
   __syncthreads();
 }
 
+// Start of butterfly u (pencil fastest) of a stage with span L and sR = L / R.
+__device__ __forceinline__ int bfly_base(const PencilSet& ps, int u, int sR, int L, int& jj) {
+  const int p = u % ps.npencil, bj = u / ps.npencil;
+  const int blk = bj / sR;
+  jj = bj - blk * sR;
+  return (p / ps.ppg) * ps.gstride + (p % ps.ppg) * ps.pstride + (blk * L + jj) * ps.estride;
+}
+
+// Calls f(t, e, base, jj) for slot e < R of every butterfly u < nbt, t = u + nbt e.
+// When the butterflies fit in the block each thread keeps one butterfly and
+// computes its base once.
+template <class F>
+__device__ __forceinline__ void for_bfly_slots(const PencilSet& ps, int nbt, int R, int sR, int L, F f) {
+  if (nbt <= (int)blockDim.x) {
+    const int per = blockDim.x / nbt;
+    const int u = threadIdx.x % nbt, e0 = threadIdx.x / nbt;
+    if (e0 >= per) return;
+    int jj;
+    const int base = bfly_base(ps, u, sR, L, jj);
+    for (int e = e0; e < R; e += per) f(u + nbt * e, e, base, jj);
+  } else {
+    for (int t = threadIdx.x; t < nbt * R; t += blockDim.x) {
+      const int u = t % nbt, e = t / nbt;
+      int jj;
+      const int base = bfly_base(ps, u, sR, L, jj);
+      f(t, e, base, jj);
+    }
+  }
+}
+
+// One stage of radix R <= 16 over every pencil of `ps`; ends with __syncthreads().
+// EX compiles the odd radices 7, 11, 13 in (kept out of the kernels of
+// other grids, whose register allocation they would raise); LEAN (the Rader
+// convolutions, whose plans have no radix 8) leaves out the radix-8
+// butterfly, the register peak of the stage loop.
+template <bool INV, bool EX, bool LEAN = false>
+__device__ __forceinline__ void small_stage(double2* s, int n, int R, int L, const double2* tw, int twmul,
+                                            const PencilSet& ps) {
+  const int twn = n * twmul;
+  const int sR = L / R;
+  const int nb = n / R;
+  const int tstep = (n / L) * twmul;
+  const int total = ps.npencil * nb;
+  for (int t = threadIdx.x; t < total; t += blockDim.x) {
+    int p, j;
+    if (ps.pencil_fast) {
+      p = t % ps.npencil;
+      j = t / ps.npencil;
+    } else {
+      j = t % nb;
+      p = t / nb;
+    }
+    const int blk = j / sR;
+    const int jj = j - blk * sR;
+    double2* b = s + (p / ps.ppg) * ps.gstride + (p % ps.ppg) * ps.pstride + (blk * L + jj) * ps.estride;
+    const int es = sR * ps.estride;
+    const int tb = jj * tstep;
+    switch (R) {
+      case 8: if constexpr (!LEAN) butterfly<8, INV>(b, es, tw, twn, tb); break;
+      case 4: butterfly<4, INV>(b, es, tw, twn, tb); break;
+      case 2: butterfly<2, INV>(b, es, tw, twn, tb); break;
+      case 3: butterfly<3, INV>(b, es, tw, twn, tb); break;
+      case 5: butterfly<5, INV>(b, es, tw, twn, tb); break;
+      case 7: if constexpr (EX) butterfly_odd<7, INV>(b, es, tw, twn, tb); break;
+      case 11: if constexpr (EX) butterfly_odd<11, INV>(b, es, tw, twn, tb); break;
+      case 13: if constexpr (EX) butterfly_odd<13, INV>(b, es, tw, twn, tb); break;
+    }
+  }
+  __syncthreads();
+}
+
+// Every stage of a Rader convolution plan (radices 4, 2 and odd primes <= 13).
+template <bool INV>
+__device__ void small_stages(double2* s, const FftAxis& ax, const double2* tw, int twmul, const PencilSet& ps) {
+  for (int k = 0; k < ax.nstage; ++k) {
+    const int st = INV ? (ax.nstage - 1 - k) : k;
+    small_stage<INV, true, true>(s, ax.n, ax.radix[st], ax.span[st], tw, twmul, ps);
+  }
+}
+
+// A stage of prime radix R by Rader's algorithm, same input/output
+// conventions as big_stage.  Scratch (ps.npencil * n elements) holds, for
+// butterfly u, slot m < M = R - 1 at tmp[u + nbt m] and x_0 at slot M:
+//   gather   a_m = x_{g^-m} (inverse stages first apply conj w_L^{jj r}),
+//   forward length-M FFT (digit-reversed output),
+//   product with the kernel spectrum (1/M included); the DC bin also takes
+//            x_0 (so the inverse adds x_0 to every output) and slot M
+//            becomes y_0 = x_0 + A_0,
+//   inverse length-M FFT (natural output: slot k holds y_{g^k}),
+//   scatter  (forward stages apply w_L^{jj q}).
+template <bool INV>
+__device__ __noinline__ void rader_stage(double2* s, int n, int R, int L, const double2* tw, int twn, const PencilSet& ps,
+                            double2* tmp, const RaderTab& rt) {
+  const int sR = L / R, lstep = twn / L, M = R - 1;
+  const int nbt = ps.npencil * (n / R);
+  const int es = sR * ps.estride;
+  const int* gin = rt.gin;
+  for_bfly_slots(ps, nbt, R, sR, L, [&](int t, int e, int base, int jj) {
+    const int r = (e < M) ? __ldg(gin + e) : 0;
+    double2 x = s[base + r * es];
+    if (INV && jj && r) x = cmulc(x, tw[jj * r * lstep]);
+    tmp[t] = x;
+  });
+  __syncthreads();
+  const PencilSet cs = {nbt, nbt, 0, 1, nbt, true};
+  small_stages<false>(tmp, rt.axm, rt.twm, 1, cs);
+  const double2* kt = INV ? rt.ki : rt.kf;
+  for (int t = threadIdx.x; t < nbt * M; t += blockDim.x) {
+    const int pos = t / nbt;
+    const double2 a = tmp[t];
+    double2 c = cmul(a, __ldg(kt + pos));
+    if (pos == 0) {
+      const double2 x0 = tmp[t + nbt * M];
+      c = cadd(c, x0);
+      tmp[t + nbt * M] = cadd(x0, a);
+    }
+    tmp[t] = c;
+  }
+  __syncthreads();
+  small_stages<true>(tmp, rt.axm, rt.twm, 1, cs);
+  const int* gout = rt.gout;
+  for_bfly_slots(ps, nbt, R, sR, L, [&](int t, int e, int base, int jj) {
+    const int q = (e < M) ? __ldg(gout + e) : 0;
+    double2 y = tmp[t];
+    if (!INV && jj && q) y = cmul(y, tw[jj * q * lstep]);
+    s[base + q * es] = y;
+  });
+  __syncthreads();
+}
+
 // Transform every pencil of `ps` (length ax.n) in place.  `tw` is the twiddle
 // table w_{twn}^t in shared memory with twn = ax.n * twmul (twmul = 2 when the
 // table of the full real length is reused for a half-length complex FFT).
-// `tmp` (ps.npencil * ax.n elements) is needed when ax.big.
-// Ends with __syncthreads().
-template <bool INV>
+// `tmp` (ps.npencil * ax.n elements) is needed when ax.big.  Without EX the
+// radices 2, 3, 4, 5, 8 and direct-DFT stages are compiled; EX adds 7, 11,
+// 13 and Rader stages (the host launches EX kernels for plans that use
+// them).  Ends with __syncthreads().
+template <bool INV, bool EX>
 __device__ void fft_pencils(double2* s, const FftAxis& ax, const double2* tw, int twmul, const PencilSet& ps,
                            double2* tmp = nullptr) {
   const int n = ax.n;
@@ -271,37 +453,16 @@ __device__ void fft_pencils(double2* s, const FftAxis& ax, const double2* tw, in
     const int R = ax.radix[st];
     const int L = ax.span[st];
     if (R > CMM_MAX_SMALL_RADIX) {
+      if constexpr (EX) {
+        if (ax.rader && ax.rader[st].M) {
+          rader_stage<INV>(s, n, R, L, tw, twn, ps, tmp, ax.rader[st]);
+          continue;
+        }
+      }
       big_stage<INV>(s, n, R, L, tw, twn, ps, tmp);
       continue;
     }
-    const int sR = L / R;
-    const int nb = n / R;
-    const int tstep = (n / L) * twmul;
-    const int total = ps.npencil * nb;
-    for (int t = threadIdx.x; t < total; t += blockDim.x) {
-      int p, j;
-      if (ps.pencil_fast) {
-        p = t % ps.npencil;
-        j = t / ps.npencil;
-      } else {
-        j = t % nb;
-        p = t / nb;
-      }
-      const int blk = j / sR;
-      const int jj = j - blk * sR;
-      double2* b = s + (p / ps.ppg) * ps.gstride + (p % ps.ppg) * ps.pstride + (blk * L + jj) * ps.estride;
-      const int es = sR * ps.estride;
-      const int tb = jj * tstep;
-      switch (R) {
-        case 8: butterfly<8, INV>(b, es, tw, twn, tb); break;
-        case 4: butterfly<4, INV>(b, es, tw, twn, tb); break;
-        case 2: butterfly<2, INV>(b, es, tw, twn, tb); break;
-        case 3: butterfly<3, INV>(b, es, tw, twn, tb); break;
-        case 5: butterfly<5, INV>(b, es, tw, twn, tb); break;
-        default: butterfly_generic<INV>(b, R, es, tw, twn, tb); break;
-      }
-    }
-    __syncthreads();
+    small_stage<INV, EX>(s, n, R, L, tw, twmul, ps);
   }
 }
 
@@ -379,9 +540,9 @@ __device__ __forceinline__ void fft_ct(double2* s, const double2* tw, int twmul,
 
 // Runtime-length transform of uniform pencils (any factorisation of ax.n);
 // tmp: npencil * ax.n elements of scratch when ax.big.
-template <bool INV>
+template <bool INV, bool EX>
 __device__ void fft_rt(double2* s, const FftAxis& ax, const double2* tw, int twmul, int npencil, int pstride,
                        int estride, double2* tmp = nullptr) {
   PencilSet ps = {npencil, npencil, 0, pstride, estride, true};
-  fft_pencils<INV>(s, ax, tw, twmul, ps, tmp);
+  fft_pencils<INV, EX>(s, ax, tw, twmul, ps, tmp);
 }

@@ -79,10 +79,11 @@ def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25
     loop.  Here each host is one batched solve of all its pressures (its own
     grid plan, potential and MFA kernel, since the cell sets the k-vectors);
     up to ``max_concurrent`` hosts run at once, each driven by the native
-    batched solver from its own host thread on its own CUDA stream, so the
-    host decisions of one host overlap the kernels of the others.  A host's
-    device buffers (~520 B per grid point and pressure with m = 5) are
-    released when its solve ends.  A host starts only while the estimated
+    batched solver from its own host thread on one of ``max_concurrent``
+    CUDA streams, so the host decisions of one host overlap the kernels of
+    the others.  A host's device buffers (~520 B per grid point and pressure
+    with m = 5) return to the caching allocator when its solve ends and serve
+    the next host on the same stream.  A host starts only while the estimated
     buffers of the running ones stay within ``memory_budget`` bytes (default
     60% of the device's memory); a host larger than the budget runs alone.
 
@@ -111,6 +112,11 @@ def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25
     need = [(640 * len(np.atleast_1d(plist[i])) + 512) * int(np.prod(shapes[i])) for i in range(nh)]   # bytes, generous
     cond = threading.Condition()
     state = dict(bytes=0, running=0)
+    # One stream per concurrency slot, reused by the hosts that take the slot:
+    # the caching allocator hands a finished host's blocks to the next host on
+    # the same stream, so hosts neither free device memory (which synchronises
+    # the device under the hosts still running) nor allocate it afresh.
+    free_streams = [torch.cuda.Stream(device=device) for _ in range(max(1, int(max_concurrent)))]
 
     def admit(i):
         with cond:
@@ -118,18 +124,19 @@ def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25
                                                              state['bytes'] + need[i] <= memory_budget))
             state['bytes'] += need[i]
             state['running'] += 1
+            return free_streams.pop()
 
-    def leave(i):
+    def leave(i, st):
         with cond:
             state['bytes'] -= need[i]
             state['running'] -= 1
+            free_streams.append(st)
             cond.notify_all()
 
     def run(i):
-        admit(i)
+        st = admit(i)
         try:
             torch.cuda.set_device(device)
-            st = torch.cuda.Stream()
             st.wait_stream(cur)
             with torch.cuda.stream(st):
                 fn = W.build_functional(hosts[i], shapes[i], temperature, guest, version=version,
@@ -151,11 +158,10 @@ def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25
                     out['rho'] = host.numpy()
                 results[i] = out
                 del s, fn, rho, rho0
-            torch.cuda.empty_cache()
         except BaseException as e:  # re-raised on the calling thread
             errors.append(e)
         finally:
-            leave(i)
+            leave(i, st)
 
     threads = [threading.Thread(target=run, args=(i,)) for i in range(nh)]
     for t in threads:

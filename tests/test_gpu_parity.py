@@ -39,12 +39,15 @@ def fn32(cuda):
     return W.build_functional(cubic_host_276(0), (32, 32, 32), 300.0, methane_guest_params())
 
 
-# shapes: specialised 32/64 kernels; small-radix mixes; prime factors > 16 on
-# each axis (direct-DFT stages) with even and odd N3 (full-length z); a
-# 160^3 fused plane and a 256^3 plane beyond shared memory (staged passes)
+# shapes: specialised 32/64 kernels; small-radix mixes; odd radices 7, 11, 13;
+# prime factors > 16 on each axis (direct-DFT stages for 17..59 and for
+# primes whose p - 1 has a factor > 16, Rader stages for 97, 127, 157) with
+# even and odd N3 (full-length z); a 160^3 fused plane and a 256^3 plane
+# beyond shared memory (staged passes)
 FFT_SHAPES = [(32, 32, 32), (64, 64, 64), (64, 32, 32), (32, 64, 64), (24, 20, 18), (30, 28, 14), (16, 12, 10),
               (7, 9, 22), (34, 51, 53), (53, 58, 62), (48, 64, 45), (37, 19, 23), (17, 29, 34), (160, 160, 160),
-              (256, 256, 256)]
+              (256, 256, 256), (91, 26, 22), (143, 14, 126), (97, 20, 18), (20, 127, 22), (18, 20, 157),
+              (59, 23, 17), (118, 59, 20)]
 
 
 @pytest.mark.parametrize("staged", [0, 1])
