@@ -108,7 +108,7 @@ const char* cmm_status_string(int status);
 
 /* Grid plan: twiddle tables, digit-reversal position tables and the k-space
  * tables of a periodic N1 x N2 x N3 grid (any sizes up to 1024; prime
- * factors > 16 run as direct-DFT stages; odd N3 as a full-length z
+ * factors > 16 run as Rader or direct-DFT stages; odd N3 as a full-length z
  * transform with the stored z frequencies in natural order) spanning the cell `rvecs` (3x3,
  * rows are cell vectors, bohr).  Replaces the k-grid, scalprod and Lanczos
  * tables of Grid.__init__ (cmmdft/system.py:232-295).  Allocates the plan's
