@@ -11,7 +11,7 @@
 #define CMM_MAX_FIELDS 12     // fields a mix launch combines
 #define CMM_PLANE_THREADS 512
 #define CMM_COL_THREADS 256
-#define CMM_FMT_THREADS 1024   // the 5-field plane pass (one block per SM)
+#define CMM_FMT_THREADS 768    // the 5-field plane pass (one block per SM; 768 balances its radix-8 rounds)
 #define CMM_ROW_THREADS 512    // staged z-row passes
 
 // Per-instance reduction slots (see cmm_stat_* in the public header).
