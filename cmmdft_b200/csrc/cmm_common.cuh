@@ -13,6 +13,7 @@
 #define CMM_COL_THREADS 256
 #define CMM_FMT_THREADS 768    // the 5-field plane pass (one block per SM; 768 balances its radix-8 rounds)
 #define CMM_ROW_THREADS 512    // staged z-row passes
+#define CMM_ZFMT_THREADS 768   // the staged z-row pass of dPhi/dn (768 measured faster than 256-512 and 1024)
 
 // Per-instance reduction slots (see cmm_stat_* in the public header).
 #define NQ CMM_NSTAT

@@ -1060,7 +1060,7 @@ __device__ void zrow_forward(const GridDev& g, const PlaneSmem& s, int nrow) {
 // gout (z forward; their y forward follows).  Same pointwise arithmetic and
 // reductions as k_plane_fmt.
 template <int M3C, bool WDA, bool TEN>
-__global__ void __launch_bounds__(CMM_ROW_THREADS)
+__global__ void __launch_bounds__(CMM_ZFMT_THREADS)
 k_zrow_fmt(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
            const double2* __restrict__ win, size_t fs, double2* __restrict__ gout, int chunk,
            double* __restrict__ part, int nslot_part, int want, double* __restrict__ wd, size_t fsr) {
@@ -1805,7 +1805,7 @@ static int zrow_fmt_one(const cmm_grid* g, int batch, const int* act, double R, 
   const size_t sb = zrow_smem_bytes_g(g, nf * chunk);
   int rc;
   if ((rc = set_smem((const void*)k_zrow_fmt<M3C, WDA, TEN>, sb))) return rc;
-  k_zrow_fmt<M3C, WDA, TEN><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(
+  k_zrow_fmt<M3C, WDA, TEN><<<dim3(g->n1, batch), CMM_ZFMT_THREADS, sb, st>>>(
       g->dev, act, R, version, we, win, fs, gout, chunk, part, nslot, want, wd,
       (size_t)batch * g->n1 * g->n2 * g->n3);
   return last_err();
