@@ -63,7 +63,7 @@ class SolveOut(ctypes.Structure):
     """cmm_solve_out."""
     _fields_ = [(n, _vp) for n in ("N", "omega", "converged", "steps", "diverged", "failed", "history")] + \
                [("launches", ctypes.c_longlong), ("omega_evals", ctypes.c_longlong), ("pipe_log", _vp),
-                ("pipe_cap", _i), ("pipe_n", _i)]
+                ("pipe_cap", _i), ("pipe_n", _i), ("cf", _vp)]
 
 
 FALLBACK_FN = ctypes.CFUNCTYPE(ctypes.c_int, ctypes.c_void_p, ctypes.c_int, ctypes.c_int, ctypes.c_double,

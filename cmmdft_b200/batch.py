@@ -283,7 +283,7 @@ class BatchSolve(object):
     def __init__(self, fn, chempots, method='hybridanderson', nsteps=500, threshold=1e-6,
                  criterion='res', alpha_mix=0.1, m=5, damping=0.3, delta=0.2, damping_max=0.8,
                  damping_min=0.01, adaptive_damping=True, damping_factors=(1.5, 0.5), divergence_guard=False,
-                 a_tol=1e-6, r_tol=1e-4, group=0, anderson_coefs='slsqp'):
+                 a_tol=1e-6, r_tol=1e-4, group=0, anderson_coefs='slsqp', track_history=False):
         self.fn = fn
         if anderson_coefs not in ('slsqp', 'exact'):
             raise ValueError("anderson_coefs must be 'slsqp' or 'exact'")
@@ -303,6 +303,13 @@ class BatchSolve(object):
                 raise NotImplementedError("criterion %r" % c)
         self.thresholds = [float(t) for t in thr]
         self.tol = (float(a_tol), float(r_tol))   # DER tolerances (solver.py:25-26)
+        # The history's derivative column (solver.py:218-220) is the DER sum
+        # without the tolerance weighting: with no 'der' criterion to serve,
+        # the kernels' DER sum is taken with a_tol = 1, r_tol = 0, which is
+        # exactly that.  With a 'der' criterion the column stays NaN.
+        self.der_history = bool(track_history) and 'der' not in self.criteria
+        if self.der_history:
+            self.tol = (1.0, 0.0)
         self.alpha_mix = float(alpha_mix)
         self.thresh = 1 * kjmol
         self.m = int(m)
@@ -597,7 +604,7 @@ class BatchSolve(object):
         for c, t in zip(self.criteria, self.thresholds):
             v = res if c == 'res' else (riue if c == 'riue' else der)
             ok = ok and (v < t)
-        self.history[b].append((N, res, riue))
+        self.history[b].append((N, res, riue, float(self.omega0[b]), der if self.der_history else np.nan))
         if iue == 0 and np.isnan(riue):
             ok = True
         return bool(ok)
@@ -706,7 +713,8 @@ class BatchSolve(object):
             v = res if c == 'res' else (riue if c == 'riue' else der)
             ok &= (v < t)
         for j, b in enumerate(idx):
-            self.history[b].append((N[j], res[j], riue[j]))
+            self.history[b].append((N[j], res[j], riue[j], float(self.omega0[b]),
+                                    der[j] if self.der_history else np.nan))
         ok |= (iue == 0) & np.isnan(riue)
         return ok
 
@@ -1074,10 +1082,11 @@ class NativeBatchSolve(BatchSolve):
         N = np.full(B, np.nan)
         om = np.full(B, np.nan)
         conv, steps, div, failed = (np.zeros(B, dtype=np.int32) for _ in range(4))
-        hist = np.full((B, self.nsteps + 2, 3), np.nan)
+        hist = np.full((B, self.nsteps + 2, 5), np.nan)
+        cf_out = np.ones(B)
         arr = lambda a: a.ctypes.data_as(ctypes.c_void_p)
         out = L.SolveOut(N=arr(N), omega=arr(om), converged=arr(conv), steps=arr(steps), diverged=arr(div),
-                         failed=arr(failed), history=arr(hist))
+                         failed=arr(failed), history=arr(hist), cf=arr(cf_out))
         if self.pipeline_events is not None:  # CUDA-event times of the full pipeline launches
             plog = np.zeros((4096, 3))
             out.pipe_log, out.pipe_cap = arr(plog), len(plog)
@@ -1094,6 +1103,9 @@ class NativeBatchSolve(BatchSolve):
         self.N_out, self.conv = N, conv.astype(bool)
         self.steps, self.diverged, self.failed = steps.astype(int), div.astype(bool), failed.astype(bool)
         self.omega0 = om
+        self.cf = cf_out
+        if not self.der_history:
+            hist[:, :, 4] = np.nan
         self.kernel_launches += int(out.launches)
         self.omega_evals += int(out.omega_evals)
         if self.pipeline_events is not None:

@@ -723,8 +723,8 @@ struct Driver {
       ok = ok && (v < o->thr[c]);
     }
     if (out->history && k <= o->nsteps + 1) {
-      double* h = out->history + ((size_t)b * (o->nsteps + 2) + k) * 3;
-      h[0] = N; h[1] = res; h[2] = riue;
+      double* h = out->history + ((size_t)b * (o->nsteps + 2) + k) * CMM_HISTORY_COLS;
+      h[0] = N; h[1] = res; h[2] = riue; h[3] = omega0[b]; h[4] = der;
     }
     if (iue == 0 && std::isnan(riue)) ok = true;
     return ok;
@@ -841,7 +841,7 @@ struct Driver {
       out->omega[b] = NAN;
     }
     if (out->history)
-      for (size_t i = 0; i < (size_t)B * (o->nsteps + 2) * 3; ++i) out->history[i] = NAN;
+      for (size_t i = 0; i < (size_t)B * (o->nsteps + 2) * CMM_HISTORY_COLS; ++i) out->history[i] = NAN;
     if (w->h_result) cuda(cudaStreamCreateWithFlags(&copy_st, cudaStreamNonBlocking));
     set_params(nullptr);
     std::vector<char> todo(B, 1);
@@ -866,6 +866,8 @@ struct Driver {
       }
     }
     for (int b = 0; b < B; ++b) out->failed[b] = failed[b];
+    if (out->cf)
+      for (int b = 0; b < B; ++b) out->cf[b] = cf[b];
     cuda(cudaStreamSynchronize(st));
     if (copy_st) {
       cuda(cudaStreamSynchronize(copy_st));

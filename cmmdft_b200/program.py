@@ -108,7 +108,8 @@ class Program(object):
         N, rho, converged = self.solver.solve(chempot, self.rho0.copy(), 2)
         if self.solver.track_history:
             fn = self.workdir / ('solving_history_%s.csv' % self.file_suffix)
-            np.savetxt(fn, self.solver.history, delimiter=',', header=self.solver.history_header)
+            np.savetxt(fn, self.solver.history[:self.solver.curr_step + 1], delimiter=',',
+                       header=self.solver.history_header)
         np.save(self.rho_fn, rho)
         return N, rho, converged
 

@@ -63,7 +63,8 @@ class Solver(object):
         import torch
         fn = self.fener.device()
         s = BT.NativeBatchSolve(fn, [chempot], method=self._method(), nsteps=self.nsteps, threshold=self.threshold,
-                          criterion=self.criterion, a_tol=self.a_tol, r_tol=self.r_tol, **self._options())
+                                criterion=self.criterion, a_tol=self.a_tol, r_tol=self.r_tol,
+                                track_history=self.track_history, **self._options())
         r0 = rho if hasattr(rho, 'detach') else torch.as_tensor(np.ascontiguousarray(rho, dtype=np.float64))
         r0 = r0.to('cuda', dtype=torch.float64).reshape((1,) + tuple(self.grid.npoints))
         N, rr, conv = s.solve(r0)
@@ -71,13 +72,33 @@ class Solver(object):
         self.curr_step = int(s.steps[0])
         self.omega0 = float(s.omega0[0]) if hasattr(s, 'omega0') else None
         if self.track_history:
-            h = np.array(s.history[0]) if s.history[0] else np.zeros((0, 3))
-            self.history = np.zeros((len(h) + 1, 7)) * np.nan
-            if len(h):
-                self.history[1:, 0] = h[:, 0]
-                self.history[1:, 2] = h[:, 1]
-                self.history[1:, 3] = h[:, 2]
+            self.history = self._history(s.history[0], float(r0.sum().item()) * self.grid.dr)
         return float(N[0]), rr[0].cpu().numpy(), bool(conv[0])
+
+
+    def _history(self, rows, N0):
+        """The reference's history array (solver.py:270-279, 208-222) from the
+        driver's per-step rows (N, RES, RIUE, Omega, DER): columns loading,
+        grand potential, residual norm (RES, or |G - rho| / N / sqrt(Npts)
+        when RES is not a criterion), RIUE, derivative norm (NaN when 'der'
+        is a criterion, whose tolerance-weighted sum the kernels then
+        compute), time per step and cumulative time (not timed: NaN).  Row 0
+        holds the loading of the initial density.  Omega is the grand
+        potential of the step's new density for the hybrid and Anderson
+        methods, the initial one for static Picard (the reference's omega0
+        without energy tracking)."""
+        h = np.array(rows, dtype=float).reshape(-1, 5)
+        out = np.full((len(h) + 1, 7), np.nan)
+        out[0, 0] = N0
+        if len(h):
+            N, res, riue, om, der = h.T
+            out[1:, 0] = N
+            out[1:, 1] = om
+            with np.errstate(invalid='ignore', divide='ignore'):
+                out[1:, 2] = res if 'res' in self.criterion else res / np.sqrt(N)
+            out[1:, 3] = riue
+            out[1:, 4] = der
+        return out
 
 
 class Picard(Solver):

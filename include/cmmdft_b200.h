@@ -358,13 +358,18 @@ typedef struct cmm_solve_out {
   double* N;                    /* [B] loading (integral of rho) */
   double* omega;                /* [B] grand potential of the last density */
   int* converged, *steps, *diverged, *failed;   /* [B]; failed: non-finite on every retry */
-  double* history;              /* optional [B][nsteps + 2][3] (N, RES, RIUE per step), or NULL */
+  double* history;              /* optional [B][nsteps + 2][CMM_HISTORY_COLS] per step: N, RES, RIUE, the
+                                   grand potential of the step's last evaluation, and sqrt(DER sum / npts)
+                                   (solver.py:208-222); or NULL */
   long long launches;           /* kernel launches issued */
   long long omega_evals;
   double* pipe_log;             /* optional [pipe_cap][3]: (want, active instances, ms) per full
                                    functional-pipeline launch, CUDA-event timed (NULL: not timed) */
   int pipe_cap, pipe_n;
+  double* cf;                   /* optional [B]: final correction factor of each instance (1, halved per
+                                   non-finite restart, solver.py:335-345), or NULL */
 } cmm_solve_out;
+#define CMM_HISTORY_COLS 5
 
 /* ---------------------------------------------------------------------
  * Derivatives at a converged density (implicit adjoint; the reference has no

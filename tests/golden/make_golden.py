@@ -3,9 +3,13 @@
 Run in the build container only (the reference tree is not present on GPU
 machines):
 
-    python tests/golden/make_golden.py [--reference /root/reference] [--skip64]
-    python tests/golden/make_golden.py --iso64 [--procs 8]
-    python tests/golden/make_golden.py --qn
+    python tests/golden/make_golden.py --reference <reference tree> [--skip64]
+    python tests/golden/make_golden.py --reference <reference tree> --iso64 [--procs 8]
+    python tests/golden/make_golden.py --reference <reference tree> --qn
+    python tests/golden/make_golden.py --reference <reference tree> --dropin
+
+``--reference`` (or the environment variable CMM_REFERENCE_ROOT) names the
+root of the reference's source tree, the directory that holds ``cmmdft/``.
 
 The reference is imported from its own source tree through the import shims
 in ``tests/golden/refshim`` (molmod units/constants backed by
@@ -28,8 +32,24 @@ Outputs (small ``.npz`` files) land next to this script:
   iso64_res8.npz  the 24-pressure 64^3 isotherm (1e-3..100 bar) solved as
               the reference's example does it: hybrid Anderson m=5 to
               RES < 1e-8 from Ninit = rho_bulk; N, Omega, steps and the
-              convergence flag per pressure (``--iso64`` only; one process
-              per pressure).
+              convergence flag per pressure, the helium void fraction and
+              the excess uptake from the reference's own
+              Calculator.return_loading(excess=True) (``--iso64`` only; one
+              process per pressure).
+  dropin32.npz    the 32^3 case driven through the reference's public API:
+              Program -> FreeEnergy.add_* -> Program.cascade_solver (static
+              Picard for 3 steps, then hybrid Anderson to RES < 1e-13 and
+              RIUE < 1e-12, continue_solving=True); Program.solve with
+              Ninit = rho_bulk (float) under hybrid Anderson to RES < 1e-8
+              with track_history=True (the history's N, Omega, RES, RIUE and
+              DER columns); and Calculator.return_loading (absolute and
+              excess), free_energy_contrib per part and grand_potential of
+              both solutions (``--dropin`` only).
+  iso64_rho.npz   the converged densities of that isotherm at the pressure
+              indices ISO_RHO_IDX, and the reference run against itself: the
+              same points re-solved from a start perturbed by one ulp, with
+              the relative differences of rho, N and Omega that this causes
+              (the trajectory's own rounding floor).
 """
 
 import argparse
@@ -98,7 +118,7 @@ def build(ref, npts, host, T, P_bar, tmp, tail=False, wda=False):
     mu = mb.calculate_mu(T, P_bar * bar)
     prog = types.SimpleNamespace(grid=grid, fener=fe)
     return dict(grid=grid, fe=fe, mu=mu, prog=prog, V_raw=V, t_ext=t_ext, mbwr=mb,
-                guest=guest, mol=mol)
+                guest=guest, mol=mol, host=h)
 
 
 def omega_parts(ref, b, rho, mu):
@@ -122,8 +142,12 @@ def quiet(fn, *a, **k):
 ISO_PRESSURES = np.logspace(-3, 2, 24)
 
 
+# pressure indices whose converged densities are kept: 1e-3, 1.1 and 8.2 bar
+ISO_RHO_IDX = (0, 14, 18)
+
+
 def _iso64_point(task):
-    ref_root, i = task
+    ref_root, i, perturb = task
     ref = import_reference(ref_root)
     solver = ref[2]
     from cmmdft_b200.hosts import cubic_host_276
@@ -135,20 +159,104 @@ def _iso64_point(task):
     mb.set_temperature(T)
     bulk = np.nanmin(mb.solve_densities_from_chempots([b['mu']]), axis=1)[0]
     rho0 = bulk * np.exp(-np.maximum(V, 0) / boltzmann / T)
+    if perturb:
+        # one ulp up at every point: the reference's sensitivity to rounding
+        rho0 = np.nextafter(rho0, np.inf)
     s = solver.Anderson(b['prog'], nsteps=500, m=5, criterion='res', threshold=1e-8)
     t0 = time.time()
     try:
         N, rho, conv = quiet(s.solve, b['mu'], rho0, 3)
     except Exception as e:  # noqa: BLE001 - recorded, not raised
         print('P=%g bar: %s' % (P, e), flush=True)
-        return i, b['mu'], bulk, np.nan, np.nan, s.curr_step, False
-    print('iso64 P=%.4g bar: N=%.12e steps=%d conv=%s (%.0f s)' % (P, N, s.curr_step, conv, time.time() - t0),
-          flush=True)
-    return i, b['mu'], bulk, N, s.omega0, s.curr_step, bool(conv)
+        return i, b['mu'], bulk, np.nan, np.nan, s.curr_step, False, None
+    print('iso64 P=%.4g bar%s: N=%.12e steps=%d conv=%s (%.0f s)'
+          % (P, ' (perturbed start)' if perturb else '', N, s.curr_step, conv, time.time() - t0), flush=True)
+    return i, b['mu'], bulk, N, s.omega0, s.curr_step, bool(conv), (rho if conv else None)
 
 
 QN_CASES = [('bfgs', 'backtracking'), ('broyden', 'backtracking'), ('cg', 'backtracking'), ('bfgs', 'quadratic'),
             ('bfgs', 'none')]
+
+
+def dropin32(args):
+    """The reference's own Program / Solver / Calculator flow on the 32^3 case."""
+    from pathlib import Path
+    ref = import_reference(args.reference)
+    system, functionals, solver, extpot, eos = ref
+    from cmmdft import program as rprogram, calculator as rcalculator
+    import yaff
+    from cmmdft_b200.hosts import cubic_host_276, methane_guest_params, HELIUM
+    from cmmdft_b200.units import angstrom, boltzmann, bar
+    T = 300.0
+    host = cubic_host_276(seed=0)
+    sig, eps, mass = methane_guest_params()
+    mol = yaff.System(pos=host.pos.copy(), ffatypes=host.ffatypes, ffatype_ids=host.ffatype_ids, rvecs=host.rvecs)
+    mol.pos -= mol.pos.sum(axis=0) / len(mol.pos)  # as system.py:70
+    h = system.NanoporousHost.__new__(system.NanoporousHost)
+    system.Host.__init__(h, 'synthetic', mol.cell)
+    h.mol, h.chk, h.par = mol, None, None
+    guest = system.SphericalLJGuest('CH4', mass, sig, eps)
+    tmp = tempfile.mkdtemp(prefix='cmm_dropin_')
+    grid0 = system.Grid(mol.cell, npoints=32)
+    V = extpot.get_external_potential(grid0.points[..., :3].reshape(-1, 3), host.ff, sig, eps, mol,
+                                      cutoff=12 * angstrom)
+    vfn = os.path.join(tmp, 'epot_32.npy')
+    np.save(vfn, V.reshape(grid0.npoints))
+    Vhe = extpot.get_external_potential(grid0.points[..., :3].reshape(-1, 3), host.ff,
+                                        HELIUM['sigma'] * angstrom, HELIUM['epsilon_K'] * boltzmann, mol,
+                                        cutoff=12 * angstrom)
+    he = grid0.integrate(np.clip(np.exp(-Vhe / boltzmann / T), 0, 1)).real / grid0.cell.volume
+
+    def program(suffix):
+        prog = rprogram.Program(prefix=tmp, hostname='synthetic', guestname='CH4', suffix=suffix)
+        prog.set_system(h, guest)
+        prog.set_grid(npoints=32)
+        prog.init_free_energy(T)
+        prog.fener.add_hard_sphere(version='WBII')
+        prog.fener.add_mean_field(cutoff=12 * angstrom, rewrite=True)
+        prog.fener.add_external_potential(load_fn=vfn)
+        prog.fener.set_temperature(T)
+        return prog
+
+    mb = eos.ModifiedBenedictWebbRubinEOS(mass, sig, eps)
+    mu = mb.calculate_mu(T, 1.0 * bar)
+    mb.set_temperature(T)
+    bulk = float(np.nanmin(mb.solve_densities_from_chempots([mu]), axis=1)[0])
+    out = dict(T=T, mu=mu, rho_bulk=bulk, he_frac=he)
+    # A: cascade, static Picard (3 steps, not converged) then tight hybrid Anderson
+    pa = program('cascade')
+    sv = [solver.Picard(pa, nsteps=3, alpha_mix=0.1, method='static', criterion='res', threshold=1e-8),
+          solver.Anderson(pa, nsteps=500, m=5, criterion=TIGHT_CRIT, threshold=TIGHT_THR)]
+    quiet(pa.cascade_solver, sv, mu, continue_solving=True)
+    rho = np.load(pa.rho_fn)
+    out.update(cascade_rho=rho, cascade_N=pa.grid.integrate(rho).real, cascade_steps=np.array([s.curr_step for s in sv]),
+               cascade_omega=sv[1].omega0)
+    # B: Program.solve from Ninit = rho_bulk (float), RES < 1e-8, history tracked
+    pb = program('ninit')
+    sb = solver.Anderson(pb, nsteps=500, m=5, criterion='res', threshold=1e-8, track_history=True)
+    pb.set_solver(sb)
+    N, rho, conv = quiet(pb.solve, mu, Ninit=bulk)
+    out.update(ninit_rho=rho, ninit_N=N, ninit_conv=conv, ninit_steps=sb.curr_step, ninit_omega=sb.omega0,
+               ninit_history=sb.history[:sb.curr_step + 1, :5].copy())
+    # Calculator observables of both solutions
+    for tag, prog in (('cascade', pa), ('ninit', pb)):
+        # Calculator.__init__ (calculator.py:27-35) copies the FreeEnergy, whose
+        # host copy re-reads a yaff checkpoint that the synthetic host does not
+        # have: set the same attributes around the program's own objects.
+        calc = rcalculator.Calculator.__new__(rcalculator.Calculator)
+        calc.program, calc.name_dict, calc.workdir = prog, prog.name_dict, prog.workdir
+        calc.grid, calc.fener = prog.grid, prog.fener
+        calc.host, calc.guest, calc.label = prog.system.host, prog.system.guest, None
+        out[tag + '_loading'] = calc.return_loading(T, [mu])[0]
+        out[tag + '_excess'] = calc.return_loading(T, [mu], excess=True, eos=mb, He_frac=he)[0]
+        out[tag + '_grand_potential'] = quiet(calc.grand_potential, T, mu)
+        for part in ('fid', 'HardSphere', 'MFA', 'ExtPot'):
+            out['%s_F_%s' % (tag, part)] = quiet(calc.free_energy_contrib, T, mu, part)
+    for k, v in out.items():
+        if np.ndim(v) == 0:
+            print('dropin %s = %r' % (k, v), flush=True)
+    np.savez_compressed(os.path.join(HERE, 'dropin32.npz'), **out)
+    print('wrote dropin32.npz')
 
 
 def qn32(args):
@@ -177,30 +285,87 @@ def qn32(args):
     print('wrote qn32.npz')
 
 
+def _excess_uptake(ref_root, mus, rhos, T=300.0):
+    """He void fraction and the excess uptake of the densities ``rhos`` (None
+    where a point did not converge) through the reference's own
+    Calculator.return_loading(excess=True) (cmmdft/calculator.py:114-138).
+    The fraction is computed as get_helium_fraction intends
+    (calculator.py:152-167; its own call of read_pars_file is broken): the
+    reference's get_external_potential for helium, clip(exp(-V/kT), 0, 1),
+    Grid.integrate, divided by the cell volume."""
+    from pathlib import Path
+    ref = import_reference(ref_root)
+    extpot = ref[3]
+    from cmmdft import calculator, tools
+    from cmmdft_b200.hosts import cubic_host_276, HELIUM
+    from cmmdft_b200.units import angstrom, boltzmann
+    host = cubic_host_276(seed=0)
+    tmp = tempfile.mkdtemp(prefix='cmm_iso64_nex_')
+    b = quiet(build, ref, 64, host, T, 1.0, tmp)
+    grid = b['grid']
+    Vhe = extpot.get_external_potential(grid.points[..., :3].reshape(-1, 3), host.ff,
+                                        HELIUM['sigma'] * angstrom, HELIUM['epsilon_K'] * boltzmann,
+                                        b['mol'], cutoff=12 * angstrom)
+    he = grid.integrate(np.clip(np.exp(-Vhe / boltzmann / T), 0, 1)).real / grid.cell.volume
+    for mu, rho in zip(mus, rhos):
+        if rho is not None:
+            np.save(os.path.join(tmp, 'rho_%s.npy' % tools.get_file_suffix(mu, T)), rho)
+    calc = calculator.Calculator.__new__(calculator.Calculator)
+    calc.workdir, calc.grid, calc.host = Path(tmp), grid, b['host']
+    Nex = calc.return_loading(T, list(mus), excess=True, eos=b['mbwr'], He_frac=he)
+    return float(he), np.asarray(Nex)
+
+
 def iso64(args):
     import multiprocessing as mp
+    n = len(ISO_PRESSURES)
+    tasks = [(args.reference, i, False) for i in range(n)] + [(args.reference, i, True) for i in ISO_RHO_IDX]
     with mp.get_context('spawn').Pool(args.procs) as pool:
-        res = sorted(pool.map(_iso64_point, [(args.reference, i) for i in range(len(ISO_PRESSURES))]))
+        allres = pool.map(_iso64_point, tasks)
+    res, pert = sorted(allres[:n], key=lambda r: r[0]), allres[n:]
     cols = list(zip(*res))
+    he, Nex = _excess_uptake(args.reference, cols[1], cols[7])
     out = dict(pressures=ISO_PRESSURES, mu=np.array(cols[1]), rho_bulk=np.array(cols[2]), N=np.array(cols[3]),
                omega=np.array(cols[4]), steps=np.array(cols[5]), converged=np.array(cols[6]),
-               threshold=1e-8, criterion='res', m=5)
+               threshold=1e-8, criterion='res', m=5, he_frac=he, N_ex=Nex)
     np.savez_compressed(os.path.join(HERE, 'iso64_res8.npz'), **out)
     print('wrote iso64_res8.npz')
+    rout = dict(idx=np.array(ISO_RHO_IDX))
+    fl = []
+    for j, i in enumerate(ISO_RHO_IDX):
+        rho = res[i][7]
+        rout['rho_%d' % i] = rho
+        p = pert[j]
+        d_rho = float(np.max(np.abs(p[7] - rho)) / np.max(np.abs(rho)))
+        d_N = abs(p[3] - res[i][3]) / abs(res[i][3])
+        d_om = abs(p[4] - res[i][4]) / abs(res[i][4])
+        fl.append((d_rho, d_N, d_om, p[5]))
+        print('floor P=%.4g bar: rho %.3e  N %.3e  Omega %.3e  steps %d vs %d'
+              % (ISO_PRESSURES[i], d_rho, d_N, d_om, p[5], res[i][5]), flush=True)
+    rout['floor'] = np.array(fl)   # per index: rel. diff of rho, N, Omega; steps of the perturbed run
+    np.savez_compressed(os.path.join(HERE, 'iso64_rho.npz'), **rout)
+    print('wrote iso64_rho.npz')
 
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument('--reference', default='/root/reference')
+    ap.add_argument('--reference', default=os.environ.get('CMM_REFERENCE_ROOT'),
+                    help="root of the reference's source tree (the directory holding cmmdft/); "
+                         "default: $CMM_REFERENCE_ROOT")
     ap.add_argument('--skip64', action='store_true')
     ap.add_argument('--iso64', action='store_true')
     ap.add_argument('--qn', action='store_true')
+    ap.add_argument('--dropin', action='store_true')
     ap.add_argument('--procs', type=int, default=8)
     args = ap.parse_args()
+    if not args.reference:
+        ap.error('--reference (or CMM_REFERENCE_ROOT) is required')
     if args.iso64:
         return iso64(args)
     if args.qn:
         return qn32(args)
+    if args.dropin:
+        return dropin32(args)
     ref = import_reference(args.reference)
     solver = ref[2]
     from cmmdft_b200.hosts import cubic_host_276, HELIUM

@@ -1,0 +1,241 @@
+"""The reference's public API end to end on the GPU path.
+
+The 32^3 case (276-atom cubic host, methane, 300 K, 1 bar) driven the way a
+user of the reference drives it: Program -> set_system / set_grid /
+init_free_energy -> FreeEnergy.add_hard_sphere / add_mean_field /
+add_external_potential -> a Solver -> Program.solve / cascade_solver ->
+Calculator.  ``tests/golden/dropin32.npz`` holds the same calls made on the
+unmodified reference (tests/golden/make_golden.py --dropin); c0_32.npz the
+part derivatives and values.
+
+Tolerances: converged loading, grand potential and Calculator observables
+1e-10 relative; densities 1e-10 relative to max rho where both sides follow
+the same trajectory to the same convergence test; part derivatives at the
+reference's 1-ulp noise floor (tests/test_gpu_parity.py); helium fraction
+1e-12.
+"""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+import cmmdft_b200 as cd
+from cmmdft_b200.hosts import cubic_host_276, methane_guest_params
+from cmmdft_b200.units import angstrom, bar
+from tests._common import relerr, scalar_rel
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+TIGHT_CRIT = ['res', 'riue']
+TIGHT_THR = [1e-13, 1e-12]
+T = 300.0
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return True
+
+
+@pytest.fixture(scope="module")
+def dropin():
+    return dict(np.load(os.path.join(ROOT, "tests", "golden", "dropin32.npz")))
+
+
+def make_program(prefix, suffix='', version='WBII'):
+    """Program of the 32^3 case through the public API only."""
+    h = cubic_host_276(0)
+    host = cd.NanoporousHost('synthetic', pos=h.pos, ffatypes=h.ffatypes, ffatype_ids=h.ffatype_ids,
+                             rvecs=h.rvecs, ff=h.ff)
+    sig, eps, mass = methane_guest_params()
+    guest = cd.SphericalLJGuest('CH4', mass, sig, eps)
+    prog = cd.Program(prefix=str(prefix), hostname='synthetic', guestname='CH4', suffix=suffix)
+    prog.set_system(host, guest)
+    prog.set_grid(npoints=32)
+    prog.init_free_energy(T)
+    prog.fener.add_hard_sphere(version=version)
+    prog.fener.add_mean_field(cutoff=12 * angstrom)
+    prog.fener.add_external_potential(cutoff=12 * angstrom)
+    prog.fener.set_temperature(T)
+    return prog
+
+
+def mbwr():
+    sig, eps, mass = methane_guest_params()
+    return cd.ModifiedBenedictWebbRubinEOS(mass, sig, eps)
+
+
+def test_parts_through_grid_fft(cuda, golden32, tmp_path):
+    """part.derive(grid.fft(rho)) and part.value(...) against the reference's
+    parts (functionals.py:574-618, 912-939, 1073-1083) on the ideal-gas
+    profile; Grid.fft's numpy view against the reference convention."""
+    prog = make_program(tmp_path)
+    fe, grid = prog.fener, prog.grid
+    assert relerr(fe.part_dict['ExtPot'].potential, golden32["V"]) < 1e-13
+    rho = golden32["rho_a"]
+    k = grid.fft(rho)
+    beta = fe.beta
+    dhs = fe.part_dict['HardSphere'].derive(k)
+    dmfa = fe.part_dict['MFA'].derive(k)
+    assert beta * np.max(np.abs(dhs - golden32["dHS_a"])) < 2e-9
+    assert relerr(dmfa, golden32["dMFA_a"]) < 1e-12
+    assert np.array_equal(fe.part_dict['ExtPot'].derive(k), fe.part_dict['ExtPot'].potential)
+    vals = [p.value(k) for p in fe.parts]
+    for v, ref in zip(vals, golden32["values_a"]):
+        assert scalar_rel(v, ref) < 1e-11
+    # Spectrum -> reference phase convention fftn(rho) exp(i pi scalprod) / Npts
+    full = np.asarray(k)
+    ref = np.fft.fftn(rho) * np.exp(1j * np.pi * grid.scalprod) / rho.size
+    assert relerr(full, ref, np.abs(ref).max()) < 1e-13
+    assert relerr(grid.ifft(k), rho) < 1e-15
+
+
+def test_program_cascade_and_calculator(cuda, dropin, tmp_path):
+    """Program.cascade_solver([static Picard x 3, tight hybrid Anderson],
+    continue_solving=True) from the ideal-gas start (program.py:315-328),
+    then Calculator.return_loading / free_energy_contrib / grand_potential
+    (calculator.py:60-138, 343-492) on the cached density."""
+    prog = make_program(tmp_path, 'cascade')
+    mu = float(dropin["mu"])
+    sv = [cd.Picard(prog, nsteps=3, alpha_mix=0.1, method='static', criterion='res', threshold=1e-8),
+          cd.Anderson(prog, nsteps=500, m=5, criterion=TIGHT_CRIT, threshold=TIGHT_THR)]
+    prog.cascade_solver(sv, mu, continue_solving=True)
+    assert [s.curr_step for s in sv][0] == dropin["cascade_steps"][0]
+    rho = np.load(prog.rho_fn)
+    N = prog.grid.integrate(rho)
+    errs = dict(rho=relerr(rho, dropin["cascade_rho"]), N=scalar_rel(N, dropin["cascade_N"]),
+                omega=scalar_rel(sv[1].omega0, dropin["cascade_omega"]))
+    calc = cd.Calculator(prog)
+    errs['loading'] = scalar_rel(calc.return_loading(T, [mu])[0], dropin["cascade_loading"])
+    errs['excess'] = scalar_rel(calc.return_loading(T, [mu], excess=True, eos=mbwr())[0], dropin["cascade_excess"])
+    errs['grand_potential'] = scalar_rel(calc.grand_potential(T, mu), dropin["cascade_grand_potential"])
+    for part in ('fid', 'HardSphere', 'MFA', 'ExtPot'):
+        errs['F_' + part] = scalar_rel(calc.free_energy_contrib(T, mu, part), dropin["cascade_F_" + part])
+    print("cascade + Calculator relative errors:", {k: "%.2e" % v for k, v in errs.items()})
+    # both sides converged to RES < 1e-13 and RIUE < 1e-12 along their own trajectories
+    assert errs['rho'] < 1e-9
+    for k, v in errs.items():
+        if k != 'rho':
+            assert v < 1e-10, (k, v)
+
+
+def test_program_solve_ninit_float_history_and_cache(cuda, dropin, tmp_path):
+    """Program.solve(mu, Ninit=rho_bulk) (the float branch of
+    program.py:278-287) under hybrid Anderson to RES < 1e-8 with
+    track_history: same steps, density, N and Omega as the reference, the
+    history's N / Omega / RES / RIUE / DER columns per step
+    (solver.py:208-222), rho_*.npy and solving_history_*.csv written, and a
+    second solve served from the cache (program.py:381-386)."""
+    prog = make_program(tmp_path, 'ninit')
+    mu = float(dropin["mu"])
+    s = cd.Anderson(prog, nsteps=500, m=5, criterion='res', threshold=1e-8, track_history=True)
+    prog.set_solver(s)
+    N, rho, conv = prog.solve(mu, Ninit=float(dropin["rho_bulk"]))
+    assert conv and s.curr_step == int(dropin["ninit_steps"])
+    errs = dict(rho=relerr(rho, dropin["ninit_rho"]), N=scalar_rel(N, dropin["ninit_N"]),
+                omega=scalar_rel(s.omega0, dropin["ninit_omega"]))
+    h, hr = s.history[:s.curr_step + 1, :5], dropin["ninit_history"]
+    assert h.shape == hr.shape
+    for c, name in enumerate(('N', 'Omega', 'RES', 'RIUE', 'DER')):
+        rows = np.isfinite(hr[1:, c])
+        assert np.array_equal(np.isfinite(h[1:, c]), rows), name
+        errs['history_' + name] = float(np.max(np.abs(h[1:, c][rows] - hr[1:, c][rows]) / np.abs(hr[1:, c][rows])))
+    print("Ninit=float relative errors:", {k: "%.2e" % v for k, v in errs.items()})
+    assert errs['rho'] < 1e-10 and errs['N'] < 1e-10 and errs['omega'] < 1e-10
+    assert errs['history_N'] < 1e-10 and errs['history_Omega'] < 1e-10
+    # RES, RIUE, DER are differences of nearly equal fields: relative 1e-6 of their own size
+    for name in ('RES', 'RIUE', 'DER'):
+        assert errs['history_' + name] < 1e-6, name
+    assert os.path.isfile(prog.rho_fn)
+    csv = prog.workdir / ('solving_history_%s.csv' % prog.file_suffix)
+    assert csv.is_file() and np.loadtxt(csv, delimiter=',').shape[0] == s.curr_step + 1
+
+    class Refuse(cd.Solver):
+        def solve(self, *a, **k):
+            raise AssertionError("the cached density must be used")
+    prog.set_solver(Refuse(prog))
+    N2, rho2, conv2 = prog.solve(mu)
+    assert conv2 and np.array_equal(rho2, rho) and N2 == prog.grid.integrate(rho)
+
+
+def test_initial_density_branches(cuda, golden32, tmp_path):
+    """_set_initial_density (program.py:219-305): ideal gas, float, array and
+    file branches, and the missing-file error."""
+    prog = make_program(tmp_path)
+    mu = float(golden32["mu"])
+    V = golden32["V"]
+    prog._set_initial_density(chempot=mu, temperature=T)
+    assert relerr(prog.rho0, golden32["rho_a"]) < 1e-14
+    n0 = 3.5e-6
+    prog._set_initial_density(Ninit=n0, chempot=mu, temperature=T)
+    assert relerr(prog.rho0, n0 * np.exp(-np.maximum(V, 0) / cd.boltzmann / T)) < 1e-14
+    arr = np.full((32, 32, 32), 1e-7)
+    prog._set_initial_density(Ninit=arr, chempot=mu, temperature=T)
+    assert prog.rho0 is arr
+    fn = tmp_path / 'guess.npy'
+    np.save(fn, arr)
+    prog._set_initial_density(Ninit=str(fn), chempot=mu, temperature=T)
+    assert np.array_equal(prog.rho0, arr)
+    with pytest.raises(FileNotFoundError):
+        prog._set_initial_density(Ninit=str(tmp_path / 'missing.npy'), chempot=mu, temperature=T)
+    with pytest.raises(AssertionError):
+        prog._set_initial_density(Ninit=np.zeros((8, 8, 8)), chempot=mu, temperature=T)
+
+
+def test_helium_fraction(cuda, golden32, golden64, tmp_path):
+    """Calculator.get_helium_fraction on the GPU against the reference's
+    helium void fraction at 32^3 and 64^3."""
+    prog = make_program(tmp_path)
+    he32 = cd.Calculator(prog).get_helium_fraction(T)
+    h = cubic_host_276(0)
+    host = cd.NanoporousHost('synthetic', pos=h.pos, ffatypes=h.ffatypes, ffatype_ids=h.ffatype_ids,
+                             rvecs=h.rvecs, ff=h.ff)
+    sig, eps, mass = methane_guest_params()
+    p64 = cd.Program(prefix=str(tmp_path), hostname='s64')
+    p64.set_system(host, cd.SphericalLJGuest('CH4', mass, sig, eps))
+    p64.set_grid(npoints=64)
+    p64.init_free_energy(T)
+    he64 = cd.Calculator(p64).get_helium_fraction(T)
+    e32 = scalar_rel(he32, golden32["he_frac"])
+    e64 = scalar_rel(he64, golden64["he_frac"])
+    print("helium fraction relative errors: 32^3 %.2e, 64^3 %.2e" % (e32, e64))
+    assert e32 < 1e-12 and e64 < 1e-12
+
+
+@pytest.mark.parametrize("method", ["static", "hybridanderson"])
+@pytest.mark.parametrize("native", [True, False])
+def test_nonfinite_member_retries_then_fails(cuda, tmp_path, native, method):
+    """The reference's failure handling (solver.py:317-345) per batch member:
+    a member seeded with NaN takes correction factors 1, 1/2 and 1/4 and then
+    raises NoSolutionError; the other members converge exactly as they do
+    without it.  (Static Picard is the reference's own path to this error: a
+    non-finite density after the update raises FloatingPointError.  Its
+    hybrid line search instead stops in np.polyfit on a NaN seed; the batch
+    treats every method the same way.)"""
+    from cmmdft_b200 import batch as BT, workload as W
+    fn = W.build_functional(cubic_host_276(0), (32, 32, 32), T, methane_guest_params())
+    mus, bulks = W.isotherm_inputs(np.array([0.1, 1.0, 10.0]) * bar, T, methane_guest_params())
+    r0 = W.initial_density(fn, mus, ninit=bulks)
+    cls = BT.NativeBatchSolve if native else BT.BatchSolve
+    kw = dict(method=method, nsteps=200 if method != 'static' else 2000, threshold=1e-8, criterion='res')
+    ref = cls(fn, mus[[0, 2]], **kw)
+    Nref, rref, cref = ref.solve(r0[[0, 2]].contiguous())
+    bad = r0.clone()
+    bad[1, 3, 4, 5] = float('nan')
+    s = cls(fn, mus, **kw)
+    with pytest.raises(cd.NoSolutionError):
+        s.solve(bad)
+    assert list(s.failed) == [False, True, False]
+    assert list(s.cf) == [1.0, 0.125, 1.0]
+    assert list(s.conv[[0, 2]]) == list(cref) == [True, True]
+    assert s.N_out[0] == Nref[0] and s.N_out[2] == Nref[1]
+    assert torch.equal(s.result[0], rref[0]) and torch.equal(s.result[2], rref[1])
+    # the drop-in Solver raises the same error for a single density
+    prog = make_program(tmp_path)
+    a = cd.Picard(prog, nsteps=50, alpha_mix=0.1, method='static', criterion='res', threshold=1e-8)
+    with pytest.raises(cd.NoSolutionError):
+        a.solve(float(mus[1]), bad[1].cpu().numpy())
