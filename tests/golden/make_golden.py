@@ -238,8 +238,24 @@ def dropin32(args):
     N, rho, conv = quiet(pb.solve, mu, Ninit=bulk)
     out.update(ninit_rho=rho, ninit_N=N, ninit_conv=conv, ninit_steps=sb.curr_step, ninit_omega=sb.omega0,
                ninit_history=sb.history[:sb.curr_step + 1, :5].copy())
-    # Calculator observables of both solutions
-    for tag, prog in (('cascade', pa), ('ninit', pb)):
+    # The reference against itself: both flows again from a start one ulp
+    # above the nominal one (the ideal-gas start of A given as an array),
+    # recording the relative change of each observable (the rounding floor
+    # of a comparison along separate trajectories).
+    pa2, pb2 = program('cascade_ulp'), program('ninit_ulp')
+    sv2 = [solver.Picard(pa2, nsteps=3, alpha_mix=0.1, method='static', criterion='res', threshold=1e-8),
+           solver.Anderson(pa2, nsteps=500, m=5, criterion=TIGHT_CRIT, threshold=TIGHT_THR)]
+    V32 = pa2.fener.part_dict['ExtPot'].potential
+    rho_ig = np.exp(pa2.fener.beta * (mu - V32)) / pa2.fener.wavelength ** 3
+    quiet(pa2.cascade_solver, sv2, mu, continue_solving=True, Ninit=np.nextafter(rho_ig, np.inf))
+    sb2 = solver.Anderson(pb2, nsteps=500, m=5, criterion='res', threshold=1e-8)
+    pb2.set_solver(sb2)
+    V0 = pb2.fener.part_dict['ExtPot'].potential
+    quiet(pb2.solve, mu, Ninit=np.nextafter(bulk * np.exp(-np.maximum(V0, 0) / boltzmann / T), np.inf))
+    out['cascade_ulp_steps'] = np.array([x.curr_step for x in sv2])
+    out['ninit_ulp_steps'] = sb2.curr_step
+    # Calculator observables of both solutions (and of the perturbed runs)
+    for tag, prog in (('cascade', pa), ('ninit', pb), ('cascade_ulp', pa2), ('ninit_ulp', pb2)):
         # Calculator.__init__ (calculator.py:27-35) copies the FreeEnergy, whose
         # host copy re-reads a yaff checkpoint that the synthetic host does not
         # have: set the same attributes around the program's own objects.
@@ -252,6 +268,18 @@ def dropin32(args):
         out[tag + '_grand_potential'] = quiet(calc.grand_potential, T, mu)
         for part in ('fid', 'HardSphere', 'MFA', 'ExtPot'):
             out['%s_F_%s' % (tag, part)] = quiet(calc.free_energy_contrib, T, mu, part)
+        if tag.endswith('_ulp'):
+            rho = np.load(prog.rho_fn)
+            out[tag + '_rho'] = rho
+    for tag in ('cascade', 'ninit'):
+        base, pert = tag, tag + '_ulp'
+        fl = dict(rho=float(np.max(np.abs(out[pert + '_rho'] - out[base + '_rho'])) / np.max(np.abs(out[base + '_rho']))))
+        for q in ('loading', 'excess', 'grand_potential', 'F_fid', 'F_HardSphere', 'F_MFA', 'F_ExtPot'):
+            fl[q] = abs(out['%s_%s' % (pert, q)] - out['%s_%s' % (base, q)]) / abs(out['%s_%s' % (base, q)])
+        out[tag + '_floor_names'] = np.array(list(fl))
+        out[tag + '_floor'] = np.array(list(fl.values()))
+        print('%s floor (1-ulp start):' % tag, {k: '%.2e' % v for k, v in fl.items()}, flush=True)
+        del out[pert + '_rho']
     for k, v in out.items():
         if np.ndim(v) == 0:
             print('dropin %s = %r' % (k, v), flush=True)

@@ -115,12 +115,21 @@ def test_program_cascade_and_calculator(cuda, dropin, tmp_path):
     errs['grand_potential'] = scalar_rel(calc.grand_potential(T, mu), dropin["cascade_grand_potential"])
     for part in ('fid', 'HardSphere', 'MFA', 'ExtPot'):
         errs['F_' + part] = scalar_rel(calc.free_energy_contrib(T, mu, part), dropin["cascade_F_" + part])
-    print("cascade + Calculator relative errors:", {k: "%.2e" % v for k, v in errs.items()})
-    # both sides converged to RES < 1e-13 and RIUE < 1e-12 along their own trajectories
-    assert errs['rho'] < 1e-9
-    for k, v in errs.items():
-        if k != 'rho':
-            assert v < 1e-10, (k, v)
+    # (the Anderson stage's step count is not compared: the reference itself
+    # takes 48 or 55 steps from starts one ulp apart at this tolerance)
+    floor = dict(zip([str(x) for x in dropin["cascade_floor_names"]], dropin["cascade_floor"]))
+    print("cascade (Anderson steps %d, reference %d) + Calculator relative errors:"
+          % (sv[1].curr_step, dropin["cascade_steps"][1]), {k: "%.2e" % v for k, v in errs.items()},
+          "| the reference against itself from a 1-ulp start:", {k: "%.2e" % v for k, v in floor.items()})
+    # Both sides stop at RES < 1e-13 and RIUE < 1e-12 along their own
+    # trajectories.  N, N_ex and the grand potentials meet 1e-10 outright; the
+    # density and the free-energy parts are held to 1e-10 or five times the
+    # reference's own spread under a 1-ulp change of its start (5e-11 for
+    # rho, 3e-11 to 4e-11 for the parts), whichever is larger.
+    for k in ('N', 'omega', 'loading', 'excess', 'grand_potential'):
+        assert errs[k] < 1e-10, (k, errs[k])
+    for k in ('rho', 'F_fid', 'F_HardSphere', 'F_MFA', 'F_ExtPot'):
+        assert errs[k] < max(1e-10, 5 * floor[k]), (k, errs[k], floor[k])
 
 
 def test_program_solve_ninit_float_history_and_cache(cuda, dropin, tmp_path):
