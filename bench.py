@@ -90,12 +90,19 @@ class ClockSampler(object):
                 "reasons": reasons, "samples": len(self.samples)}
 
 
-# DRAM bytes (read + write) of one 24-instance 64^3 pipeline launch with
-# want = 15 (column pass 1, plane pass storing the weighted densities, column
-# pass 2), summed over its three kernels from one ncu capture
-# (profiles/pipeline_traffic_isotherm64.md); reported per launch scaled by
-# the algorithmic bytes, the way roofline.achieved averages over launches.
-NCU_TRAFFIC_FULL_LAUNCH = 1339645952.0
+def ncu_traffic(plan):
+    """DRAM bytes (read + write) of one captured pipeline launch, from the
+    capture record committed beside the profile summaries: (bytes, want,
+    instances), or None when there is no record for this grid."""
+    fn = os.path.join(ROOT, "profiles", "pipeline_traffic_isotherm64.json")
+    try:
+        with open(fn) as f:
+            rec = json.load(f)
+    except (OSError, ValueError):
+        return None
+    if tuple(rec.get("grid", ())) != tuple(plan.npoints):
+        return None
+    return float(rec["dram_bytes"]), int(rec["want"]), int(rec["instances"])
 
 
 def pipeline_bytes(plan, want, n_active):
@@ -225,13 +232,21 @@ def run_gpu(args):
         tot_bytes += pipeline_bytes(fn.plan, want, nact)
     pk = peaks()
     achieved = tot_bytes / (tot_ms / 1e3) / 1e9 if tot_ms > 0 else None
+    # measured DRAM bytes per launch: the captured launch's bytes scaled by
+    # the algorithmic bytes of the average timed launch
+    cap = ncu_traffic(fn.plan)
+    traffic = (cap[0] / pipeline_bytes(fn.plan, cap[1], cap[2]) * tot_bytes / len(events)) \
+        if (cap and events) else None
+    dram_gbs = traffic / (tot_ms / len(events) / 1e3) / 1e9 if (traffic and tot_ms > 0) else None
     roofline = {"bound": "hbm", "kernel": "functional pipeline (k_col_weights+k_plane_fmt+k_col_backconv)",
                 "achieved": achieved, "peak": pk["hbm_gbs"], "unit": "GB/s",
                 "frac": (achieved / pk["hbm_gbs"]) if achieved else None,
                 "peak_source": "fallback" if pk.get("_fallback") else "measured",
-                "traffic": (NCU_TRAFFIC_FULL_LAUNCH / pipeline_bytes(fn.plan, 15, 24) * tot_bytes / len(events))
-                if events and tuple(fn.plan.npoints) == (64, 64, 64) else None,
-                "traffic_source": "ncu DRAM bytes of one full 24-instance launch, scaled by algorithmic bytes",
+                "traffic": traffic,
+                "traffic_source": ("ncu DRAM bytes of one %d-instance launch (want %d), scaled by algorithmic bytes"
+                                   % (cap[2], cap[1])) if cap else None,
+                "dram_achieved": dram_gbs,
+                "dram_frac": (dram_gbs / pk["hbm_gbs"]) if dram_gbs else None,
                 "launches": len(events),
                 "bytes_per_launch": tot_bytes / max(len(events), 1),
                 "ms_per_launch": tot_ms / max(len(events), 1),

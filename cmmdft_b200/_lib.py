@@ -28,7 +28,7 @@ class WdaEos(ctypes.Structure):
                 ("eta", ctypes.c_double), ("kT", ctypes.c_double), ("a_mfa", ctypes.c_double),
                 ("factors", ctypes.c_double * 3)]
 CLIP_NONE, CLIP_PICARD, CLIP_DENSITY = 0, 1, 2
-SOLVE_HYBRID, SOLVE_ANDERSON, SOLVE_HYBRIDANDERSON = 1, 2, 3
+SOLVE_HYBRID, SOLVE_ANDERSON, SOLVE_HYBRIDANDERSON, SOLVE_STATIC = 1, 2, 3, 4
 CRIT_RES, CRIT_RIUE, CRIT_DER = 0, 1, 2
 COEF_SLSQP, COEF_EXACT = 0, 1
 BICG_RHO, BICG_ALPHA, BICG_OMEGA, BICG_BETA, BICG_D0, BICG_D1, BICG_RR, BICG_FIRST, BICG_NS = range(9)
@@ -47,7 +47,8 @@ class SolveOpts(ctypes.Structure):
     _fields_ = [("method", _i), ("nsteps", _i), ("m", _i), ("ncrit", _i), ("crit", _i * 3), ("thr", _d * 3),
                 ("alpha_mix", _d), ("damping", _d), ("delta", _d), ("damping_max", _d), ("damping_min", _d),
                 ("damping_up", _d), ("damping_down", _d), ("adaptive_damping", _i), ("divergence_guard", _i),
-                ("a_tol", _d), ("r_tol", _d), ("ls_thresh", _d), ("kjmol", _d), ("coefs", _i)]
+                ("a_tol", _d), ("r_tol", _d), ("ls_thresh", _d), ("kjmol", _d), ("coefs", _i),
+                ("picard_thr", _d)]
 
 
 class SolveWs(ctypes.Structure):

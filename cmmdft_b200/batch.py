@@ -243,6 +243,10 @@ def workspace(fn, B, nring, group=0):
                  params=[torch.zeros((B, 4), dtype=f64).pin_memory() for _ in range(8)]),
     )
     ws['buf'].part[:, L.STAT_N3MAX, :] = -np.inf
+    # pinned read-back buffers of the native driver
+    ws['pin_read'] = dict(stats=torch.zeros((B, L.NSTAT), dtype=f64).pin_memory(),
+                          ls=torch.zeros((B, L.NLS), dtype=f64).pin_memory(),
+                          alpha=torch.zeros(B, dtype=f64).pin_memory())
     cache[key] = ws
     return ws
 
@@ -267,9 +271,6 @@ def ls_workspace(fn, ws, B, nring):
     ws['ls_part'] = ls_part
     ws['ls'] = torch.zeros((B, L.NLS), dtype=f64, device=dev)
     ws['ls_alpha'] = torch.zeros(B, dtype=f64, device=dev)
-    ws['pin_read'] = dict(stats=torch.zeros((B, L.NSTAT), dtype=f64).pin_memory(),
-                          ls=torch.zeros((B, L.NLS), dtype=f64).pin_memory(),
-                          alpha=torch.zeros(B, dtype=f64).pin_memory())
     return ws
 
 
@@ -1030,11 +1031,9 @@ class NativeBatchSolve(BatchSolve):
     per-instance decisions evaluated in C++ between read-backs instead of in
     the interpreter.  The rare SLSQP fallback of the line search is called
     back into Python (scipy, on full evaluations of the trial density).
-    Static Picard runs the Python loop.  Same results as BatchSolve."""
+    Same results as BatchSolve."""
 
     def solve(self, rho0, cf=None, host_out=None):
-        if self.method == 'static':
-            return BatchSolve.solve(self, rho0, cf=cf, host_out=host_out)
         if host_out is not None and (not host_out.is_pinned() or tuple(host_out.shape) != tuple(rho0.shape)):
             raise ValueError("host_out must be a pinned tensor of the shape of rho0")
         import ctypes
@@ -1045,7 +1044,7 @@ class NativeBatchSolve(BatchSolve):
         self.history = [[] for _ in range(B)]
         self.fallbacks = 0
         method = {'hybrid': L.SOLVE_HYBRID, 'anderson': L.SOLVE_ANDERSON,
-                  'hybridanderson': L.SOLVE_HYBRIDANDERSON}[self.method]
+                  'hybridanderson': L.SOLVE_HYBRIDANDERSON, 'static': L.SOLVE_STATIC}[self.method]
         crit = {'res': L.CRIT_RES, 'riue': L.CRIT_RIUE, 'der': L.CRIT_DER}
         nc = len(self.criteria)
         opts = L.SolveOpts(method=method, nsteps=self.nsteps, m=self.m, ncrit=nc,
@@ -1054,7 +1053,8 @@ class NativeBatchSolve(BatchSolve):
                            damping_up=self.dfac[0], damping_down=self.dfac[1],
                            adaptive_damping=int(bool(self.adaptive)), divergence_guard=int(self.divergence_guard),
                            a_tol=self.tol[0], r_tol=self.tol[1], ls_thresh=self.thresh, kjmol=kjmol,
-                           coefs=L.COEF_EXACT if self.anderson_coefs == 'exact' else L.COEF_SLSQP)
+                           coefs=L.COEF_EXACT if self.anderson_coefs == 'exact' else L.COEF_SLSQP,
+                           picard_thr=1e-10 / angstrom ** 3)
         for i, (c, t) in enumerate(zip(self.criteria, self.thresholds)):
             opts.crit[i] = crit[c]
             opts.thr[i] = t
@@ -1070,7 +1070,7 @@ class NativeBatchSolve(BatchSolve):
             self.pin_read['stage'] = stage
         names = ("ring", "rres", "trial", "rho0", "spec_ring", "wd_ring", "wd_r", "rhat", "chat", "chat2", "that",
                  "params", "coef", "active", "ls_part", "ls", "ls_alpha")
-        ws = L.SolveWs(**{n: ws_d[n].data_ptr() for n in names})
+        ws = L.SolveWs(**{n: ws_d[n].data_ptr() for n in names if n in ws_d})   # static: no line-search buffers
         ws.result = self.result.data_ptr()
         ws.work, ws.part, ws.stats = self.buf.work.data_ptr(), self.buf.part.data_ptr(), self.buf.stats.data_ptr()
         ws.nslot = self.buf.nslot

@@ -11,7 +11,10 @@
 //
 // The array's device address is looked up once per device, with that device
 // current, on the first call made on it; make that first call before any
-// stream capture.  All calls share the array and it keeps the contents of
+// stream capture.  The address is cached per device index for the life of
+// the process: after a cudaDeviceReset (or any other re-creation of the
+// device's primary context) it is stale, and the entry point must not be
+// called on that device again.  All calls share the array and it keeps the contents of
 // the last call, so calls that overlap on the GPU (other streams, other host
 // threads) race and must be serialised by the caller.
 #include <mutex>
@@ -66,6 +69,7 @@ extern "C" int cmm_fmt_c1_noalloc(const cmm_grid* g, int batch, const int* d_act
   if (version & CMM_TENSOR) return CMM_ERR_UNSUPPORTED;  // 24 spectra: beyond the sizing below
   if ((want & 1) && !d_chat) return CMM_ERR_ARG;
   if ((want & 6) && !d_stats) return CMM_ERR_ARG;
+  if ((version & CMM_NOHS) && want != 1) return CMM_ERR_ARG;  // as cmm_fmt_c1: C1 only
   if ((size_t)batch > cmm_fmt_c1_noalloc_capacity(g)) return CMM_ERR_WORKSPACE;  // beyond the fixed scratch
   void* base = nullptr;
   int rc = noalloc_scratch(&base);

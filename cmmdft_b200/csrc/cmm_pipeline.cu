@@ -2129,8 +2129,8 @@ extern "C" int cmm_fmt_c1(const cmm_grid* g, int batch, const int* d_active, dou
   const size_t csw = col_smem_bytes(g->n1, tc, nf, g->ax1.big), csb = col_smem_bytes(g->n1, tc, nf + 1, g->ax1.big);
   const double2* wt = (const double2*)d_wtab;
   const int ck = col_kind(g);
-  if (version & CMM_NOHS) {  // MFA term alone: one column pass
-    if (!(want & 1) || (want & 8)) return CMM_ERR_ARG;
+  if (version & CMM_NOHS) {  // MFA term alone: one column pass, the C1 spectrum only
+    if (want != 1) return CMM_ERR_ARG;
     LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), col_smem_bytes(g->n1, tc, 6, g->ax1.big), st, g->dev, d_active, R,
                1.0 / (beta * npts), (const double2*)nullptr, fs, (const double2*)d_rhohat, (const double2*)d_kst,
                wt, (double2*)d_chat, tc, 0.0, 1.0 / npts);

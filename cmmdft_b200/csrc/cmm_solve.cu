@@ -321,7 +321,7 @@ struct Driver {
   size_t npts, S;
   int nwd, m;
   double dr, beta;
-  bool wda, anderson, pure;
+  bool wda, anderson, pure, statik = false;
   const double *mu, *fug;
   std::vector<double> cf;
   std::vector<char> failed, And_true;
@@ -361,11 +361,12 @@ struct Driver {
     for (int b = 0; b < B; ++b) h[b] = mask[b] ? 1 : 0;
     cuda(cudaMemcpyAsync(w->active, h, sizeof(int) * B, cudaMemcpyHostToDevice, st));
   }
-  void set_params(const double* n3) {
+  // params[b] = (fugacity, Picard mixing a, mu, max n3 of the current density)
+  void set_params(const double* n3, const double* a = nullptr) {
     double* h = (double*)stage();
     for (int b = 0; b < B; ++b) {
       h[b * 4 + 0] = fug[b];
-      h[b * 4 + 1] = 0.0;
+      h[b * 4 + 1] = a ? a[b] : 0.0;
       h[b * 4 + 2] = mu[b];
       h[b * 4 + 3] = n3 ? n3[b] : 0.0;
     }
@@ -519,8 +520,13 @@ struct Driver {
     set_active(todo);
     std::vector<double> coefs((size_t)B * MAXF, 0.0);
     for (int b = 0; b < B; ++b) coefs[(size_t)b * MAXF] = 1.0;
-    mix(coefs, {w->rho0}, CLIP_NONE, w->rho0, ring(0), spec_ring(0));
-    c1(spec_ring(0), w->chat2, 1 | 2 | 4 | 8, wd_ring(0));
+    if (statik) {  // the density's spectrum lives in `that`; no line search
+      mix(coefs, {w->rho0}, CLIP_NONE, w->rho0, ring(0), w->that);
+      c1(w->that, w->chat2, 1 | 2 | 4, nullptr);
+    } else {
+      mix(coefs, {w->rho0}, CLIP_NONE, w->rho0, ring(0), spec_ring(0));
+      c1(spec_ring(0), w->chat2, 1 | 2 | 4 | 8, wd_ring(0));
+    }
     finalize();
     read(true, false);
     cuda(cudaMemcpyAsync(w->chat, w->chat2, sizeof(double) * B * S, cudaMemcpyDeviceToDevice, st));
@@ -730,6 +736,79 @@ struct Driver {
     return ok;
   }
 
+  // _loop_static (batch.py): static Picard (Picard.update_rho_static,
+  // solver.py:392-401).  One fused plane pass per step takes C1 of the
+  // current density (ring slot cur[b]) to the mixed density in the other
+  // slot and its spectrum; the residual that pass measures belongs to the
+  // current density, so the convergence test of a step's density is read
+  // one step later, as the Python driver does.
+  void loop_static(std::vector<char>& live, std::vector<char>& retry) {
+    std::vector<int> cur(B, 0);
+    std::vector<double> prev((size_t)B * NST, 0.0), a(B);
+    std::fill(res_hist.begin(), res_hist.end(), NAN);
+    int step = 0;
+    set_active(live);
+    while (rc == CMM_OK) {
+      bool any = false;
+      for (int b = 0; b < B; ++b) any |= live[b] != 0;
+      if (!any) break;
+      step += 1;
+      for (int b = 0; b < B; ++b) a[b] = o->alpha_mix * cf[b];
+      set_params(nullptr, a.data());
+      for (int par = 0; par < 2; ++par) {
+        std::vector<char> grp(B, 0);
+        bool anyg = false;
+        for (int b = 0; b < B; ++b) {
+          grp[b] = live[b] && cur[b] == par;
+          anyg |= grp[b] != 0;
+        }
+        if (!anyg) continue;
+        set_active(grp);
+        check(cmm_picard_static_step(g, B, w->active, w->params, beta, fn->lambda3, o->picard_thr, o->a_tol,
+                                     o->r_tol, w->chat, ring(par), fn->d_V, 0, ring(1 - par), w->that, w->part,
+                                     w->nslot, st));
+        out->launches += 1;
+      }
+      set_active(live);
+      finalize();
+      read(true, false);
+      if (rc != CMM_OK) return;
+      for (int b = 0; b < B; ++b) {
+        if (!live[b]) continue;
+        const double* s = &stats_h[(size_t)b * NST];
+        if (step > 1) {
+          const double* p = &prev[(size_t)b * NST];
+          const int k = step - 1;
+          const double N = p[CMM_STAT_N] * dr;
+          const double res = std::sqrt(s[CMM_STAT_RES2]) / std::sqrt(N) / std::sqrt((double)npts);
+          const double iue = p[CMM_STAT_IUE] * dr;
+          const double der = std::sqrt(s[CMM_STAT_DER]) / std::sqrt((double)npts);
+          out->steps[b] = k;
+          const bool conv = converged(b, N, res, iue, der, k);
+          if (k <= o->nsteps + 1) res_hist[(size_t)b * (o->nsteps + 2) + k] = res;
+          if (conv || k >= o->nsteps || diverging(b, k)) {
+            if (!conv) out->diverged[b] = k < o->nsteps ? 1 : 0;
+            finish(b, cur[b], N, k, conv);
+            live[b] = 0;
+            continue;
+          }
+        }
+        if (s[CMM_STAT_NONFIN] > 0) {
+          retry[b] = 1;
+          live[b] = 0;
+          continue;
+        }
+        cur[b] = 1 - cur[b];
+      }
+      any = false;
+      for (int b = 0; b < B; ++b) any |= live[b] != 0;
+      if (!any) break;
+      set_active(live);
+      c1(w->that, w->chat, 1, nullptr);
+      prev = stats_h;
+    }
+  }
+
   // _loop_general (batch.py)
   void loop_general(std::vector<char>& live, std::vector<char>& retry) {
     std::fill(gram.begin(), gram.end(), 0.0);
@@ -811,6 +890,7 @@ struct Driver {
     if (m > CMM_MAX_HIST || 2 * m > MAXF) return CMM_ERR_ARG;
     anderson = o->method == CMM_SOLVE_ANDERSON || o->method == CMM_SOLVE_HYBRIDANDERSON;
     pure = o->method == CMM_SOLVE_ANDERSON;
+    statik = o->method == CMM_SOLVE_STATIC;
     if (!anderson) m = 2;
     if (anderson && o->coefs == CMM_COEF_SLSQP && B >= 8) {
       const unsigned hw = std::thread::hardware_concurrency();
@@ -852,7 +932,8 @@ struct Driver {
       std::vector<char> live(todo), retry(B, 0);
       init_state(todo);
       if (rc) break;
-      loop_general(live, retry);
+      if (statik) loop_static(live, retry);
+      else loop_general(live, retry);
       // non-finite -> halve the correction factor and restart (solver.py:335-345)
       for (int b = 0; b < B; ++b) {
         if (retry[b]) {
@@ -900,8 +981,12 @@ extern "C" int cmm_solve_batched(const cmm_functional_desc* fn, const cmm_solve_
                                  cmm_solve_out* out, cmm_fallback_fn fallback, void* fallback_ctx, void* stream) {
   if (!fn || !fn->grid || !opt || batch < 1 || !mu || !fug || !cf0 || !ws || !out) return CMM_ERR_ARG;
   if (!out->N || !out->omega || !out->converged || !out->steps || !out->diverged || !out->failed) return CMM_ERR_ARG;
-  if (opt->method != CMM_SOLVE_HYBRID && opt->method != CMM_SOLVE_ANDERSON && opt->method != CMM_SOLVE_HYBRIDANDERSON)
+  if (opt->method != CMM_SOLVE_HYBRID && opt->method != CMM_SOLVE_ANDERSON && opt->method != CMM_SOLVE_HYBRIDANDERSON &&
+      opt->method != CMM_SOLVE_STATIC)
     return CMM_ERR_UNSUPPORTED;
+  if (opt->method == CMM_SOLVE_STATIC ? (!ws->ring || !ws->that || !ws->chat || !ws->chat2)
+                                      : (!ws->spec_ring || !ws->wd_ring || !ws->wd_r || !ws->rhat || !ws->ls_part))
+    return CMM_ERR_ARG;
   if (opt->ncrit < 1 || opt->ncrit > 3 || opt->nsteps < 1) return CMM_ERR_ARG;
   if (opt->coefs != CMM_COEF_SLSQP && opt->coefs != CMM_COEF_EXACT) return CMM_ERR_ARG;
   if (!ws->h_stats || !ws->h_ls || !ws->h_alpha || !ws->h_stage) return CMM_ERR_ARG;

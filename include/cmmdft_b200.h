@@ -195,7 +195,10 @@ int cmm_mfa_kernel(const cmm_grid* grid, double sigma, double epsilon, double cu
  * density and one back-convolution field.  CMM_TENSOR adds the six tensor
  * weighted densities and their back-convolution.
  * d_work: 12 spectra of batch instances (24 with CMM_TENSOR).
- * d_part: [batch][CMM_NSTAT][nslot]. */
+ * d_part: [batch][CMM_NSTAT][nslot].
+ * With CMM_NOHS (the MFA convolution alone) only want = 1 is accepted: the
+ * free-energy sums, the n3 maximum and the weighted densities belong to the
+ * hard-sphere passes, so any of want bits 1-3 returns CMM_ERR_ARG. */
 int cmm_fmt_c1(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,
                int version, const cmm_wda_eos* wda, const double* d_kst, const double* d_wtab,
                const double* d_rhohat, double* d_chat, double* d_work, double* d_part, int nslot,
@@ -286,8 +289,9 @@ int cmm_ls_finalize(int batch, const int* d_active, const double* d_ls_part, int
 
 /* ---------------------------------------------------------------------
  * Native batched solve: the control flow of Solver._solve with the
- * Picard hybrid and (hybrid-)Anderson updates (cmmdft/solver.py:236-345,
- * 403-457, 515-604) for `batch` chemical potentials on one functional, run
+ * Picard static and hybrid and the (hybrid-)Anderson updates
+ * (cmmdft/solver.py:236-345, 392-457, 515-604) for `batch` chemical
+ * potentials on one functional, run
  * in C++ around the kernels above (one read-back per decision point).
  * Equivalent to the Python driver cmmdft_b200.batch.BatchSolve, which
  * remains its specification.
@@ -302,7 +306,8 @@ typedef struct cmm_functional_desc {
   const double* d_V;            /* external potential [N1][N2][N3] */
 } cmm_functional_desc;
 
-enum { CMM_SOLVE_HYBRID = 1, CMM_SOLVE_ANDERSON = 2, CMM_SOLVE_HYBRIDANDERSON = 3 };
+enum { CMM_SOLVE_HYBRID = 1, CMM_SOLVE_ANDERSON = 2, CMM_SOLVE_HYBRIDANDERSON = 3,
+       CMM_SOLVE_STATIC = 4 /* Picard.update_rho_static, solver.py:392-401 */ };
 enum { CMM_CRIT_RES = 0, CMM_CRIT_RIUE = 1, CMM_CRIT_DER = 2 };
 /* Anderson coefficients: the reference's SLSQP (solver.py:585-591, restated
  * in cmm_anderson_slsqp) or the exact minimiser of ||sum a_i r_i|| on the
@@ -321,6 +326,8 @@ typedef struct cmm_solve_opts {
   double ls_thresh;             /* 1 kJ/mol: line-search fallback threshold (Hartree) */
   double kjmol;                 /* 1 kJ/mol in Hartree */
   int coefs;                    /* CMM_COEF_* */
+  double picard_thr;            /* static Picard: densities below this become 0 (1e-10 angstrom^-3 in the
+                                   caller's length unit, solver.py:398) */
 } cmm_solve_opts;
 
 /* Buffers of one solve (device, except the h_* pinned host arrays).
@@ -454,11 +461,15 @@ int cmm_solve_batched(const cmm_functional_desc* fn, const cmm_solve_opts* opt, 
  * the library holds until exit; batches larger than
  * cmm_fmt_c1_noalloc_capacity(grid) are rejected with CMM_ERR_WORKSPACE.
  * The first call on a device looks up the array's address (make it before
- * any stream capture).  All calls share the array and it keeps the last
- * call's contents: calls that overlap on the GPU race.  Outputs as
- * cmm_fmt_c1; d_stats [batch][CMM_NSTAT] receives the PHI / MFA / N3MAX
- * sums requested by `want` (may be NULL when want == 1).  The tensor
- * versions (CMM_TENSOR) need twice the scratch and return CMM_ERR_UNSUPPORTED. */
+ * any stream capture); the address is kept per device index for the life of
+ * the process, so a cudaDeviceReset (or anything else that destroys and
+ * re-creates the device's primary context) invalidates it, and this entry
+ * point must not be called on that device afterwards.  All calls share the
+ * array and it keeps the last call's contents: calls that overlap on the GPU
+ * race.  Outputs as cmm_fmt_c1; d_stats [batch][CMM_NSTAT] receives the PHI /
+ * MFA / N3MAX sums requested by `want` (may be NULL when want == 1), and
+ * CMM_NOHS accepts want = 1 only, as in cmm_fmt_c1.  The tensor versions
+ * (CMM_TENSOR) need twice the scratch and return CMM_ERR_UNSUPPORTED. */
 #define CMM_NOALLOC_SCRATCH_BYTES (32u << 20)
 size_t cmm_fmt_c1_noalloc_capacity(const cmm_grid* grid);
 int cmm_fmt_c1_noalloc(const cmm_grid* grid, int batch, const int* d_active, double R, double beta,

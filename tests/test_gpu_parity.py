@@ -203,25 +203,28 @@ TIGHT_CRIT = ['res', 'riue']
 TIGHT_THR = [1e-13, 1e-12]
 
 
-def _solve(fn, mu, rho0, method, thr, nsteps=500, crit='res'):
-    s = BT.BatchSolve(fn, np.atleast_1d(mu), method=method, nsteps=nsteps, threshold=thr, criterion=crit)
+def _solve(fn, mu, rho0, method, thr, nsteps=500, crit='res', native=False):
+    cls = BT.NativeBatchSolve if native else BT.BatchSolve
+    s = cls(fn, np.atleast_1d(mu), method=method, nsteps=nsteps, threshold=thr, criterion=crit)
     r0 = torch.as_tensor(np.asarray(rho0)[None] if np.ndim(rho0) == 3 else rho0, device="cuda")
     N, rho, conv = s.solve(r0)
     return s, N, rho.cpu().numpy(), conv
 
 
-def test_static_picard_matches_reference(golden32, fn32):
+@pytest.mark.parametrize("native", [False, True])
+def test_static_picard_matches_reference(golden32, fn32, native):
     mu = float(golden32["mu"])
-    s, N, rho, conv = _solve(fn32, mu, golden32["rho_a"], 'static', 1e-8)
+    s, N, rho, conv = _solve(fn32, mu, golden32["rho_a"], 'static', 1e-8, native=native)
     assert conv[0]
     assert s.steps[0] == int(golden32["picard_steps"])
     assert relerr(rho[0], golden32["picard_rho"]) < 1e-10
     assert scalar_rel(N[0], golden32["picard_N"]) < 1e-10
 
 
-def test_static_picard_der_criterion(golden32, fn32):
+@pytest.mark.parametrize("native", [False, True])
+def test_static_picard_der_criterion(golden32, fn32, native):
     mu = float(golden32["mu"])
-    s, N, rho, conv = _solve(fn32, mu, golden32["rho_a"], 'static', [1e-3], crit=['der'])
+    s, N, rho, conv = _solve(fn32, mu, golden32["rho_a"], 'static', [1e-3], crit=['der'], native=native)
     assert conv[0]
     assert s.steps[0] == int(golden32["der_steps"])
     assert relerr(rho[0], golden32["der_rho"]) < 1e-10
@@ -425,7 +428,7 @@ def test_grouped_solve_equals_single_batch(cuda, groups, native):
     assert torch.equal(host_out, rho2.cpu())
 
 
-@pytest.mark.parametrize("method,case", [("hybridanderson", "wbii"), ("hybrid", "wbii"), ("anderson", "wbii"),
+@pytest.mark.parametrize("method,case", [("hybridanderson", "wbii"), ("hybrid", "wbii"), ("anderson", "wbii"), ("static", "wbii"),
                                          ("hybridanderson", "atwbii_wda")])
 def test_native_driver_equals_python_driver(cuda, method, case):
     """cmm_solve_batched (C++ loop) against BatchSolve (Python loop): the same

@@ -65,3 +65,24 @@ def test_noalloc_rejects_batches_beyond_its_scratch(case):
     rc = lib.cmm_fmt_c1_noalloc(fn.plan.handle, cap + 1, None, fn.R, fn.beta, fn.version, None, L.ptr(fn.kst),
                                 L.ptr(fn.wtab), L.ptr(spec), L.ptr(spec), L.ptr(spec), 1, _stream())
     assert rc == 6  # CMM_ERR_WORKSPACE, before any device work
+
+
+def test_mfa_only_rejects_hard_sphere_outputs(case):
+    """CMM_NOHS (the MFA convolution alone) has no hard-sphere sums: both
+    entry points reject any want bit beyond the C1 spectrum with CMM_ERR_ARG
+    before any device work, and accept want = 1."""
+    fn, spec = case
+    plan, lib, B = fn.plan, L.lib(), spec.shape[0]
+    chat = plan.new_spec(B)
+    stats = torch.zeros((B, L.NSTAT), dtype=torch.float64, device="cuda")
+    buf = E.Buffers(plan, B)
+    for want in (3, 5, 7):
+        rc = lib.cmm_fmt_c1_noalloc(plan.handle, B, None, fn.R, fn.beta, L.NOHS, None, L.ptr(fn.kst), None,
+                                    L.ptr(spec), L.ptr(chat), L.ptr(stats), want, _stream())
+        assert rc == 1, (want, rc)   # CMM_ERR_ARG
+        rc = lib.cmm_fmt_c1(plan.handle, B, None, fn.R, fn.beta, L.NOHS, None, L.ptr(fn.kst), None, L.ptr(spec),
+                            L.ptr(chat), L.ptr(buf.work), L.ptr(buf.part), buf.nslot, want, None, _stream())
+        assert rc == 1, (want, rc)
+    rc = lib.cmm_fmt_c1_noalloc(plan.handle, B, None, fn.R, fn.beta, L.NOHS, None, L.ptr(fn.kst), None,
+                                L.ptr(spec), L.ptr(chat), None, 1, _stream())
+    assert rc == 0, lib.cmm_status_string(rc)
