@@ -92,6 +92,7 @@ _SIGS = {
     "cmm_plane_smem_bytes": ([c_void_p, c_int, P(ctypes.c_size_t)], c_int),
     "cmm_extpot_lj": ([c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_double, c_double,
                        c_double, c_double, c_void_p, c_void_p], c_int),
+    "cmm_extpot_set_mode": ([c_int], c_int),
     "cmm_rfft3d": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
     "cmm_irfft3d": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
     "cmm_rfft_yz": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),

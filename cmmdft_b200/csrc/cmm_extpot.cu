@@ -7,11 +7,15 @@
 // 12-6 potential for R < cutoff, accumulated in atom order.  Then the capping
 // of FreeEnergy.add_external_potential (cmmdft/functionals.py:247-251).
 //
-// One thread per grid point; atoms are staged through shared memory in tiles
-// with their mixed parameters precomputed.  Products and sums that numpy
-// rounds separately use explicit _rn intrinsics so the compiler does not
-// contract them into FMAs.
+// All-atom form: one thread per grid point; atoms are staged through shared
+// memory in tiles with their mixed parameters precomputed.  Products and sums
+// that numpy rounds separately use explicit _rn intrinsics so the compiler
+// does not contract them into FMAs.  The cell-list form below serves large
+// orthorhombic cells.
+#include <algorithm>
 #include <cmath>
+#include <cstring>
+#include <vector>
 
 #include "cmm_common.cuh"
 
@@ -97,6 +101,228 @@ k_extpot(ExtArgs a, const AtomLJ* __restrict__ atoms, double* __restrict__ V) {
   }
 }
 
+// ------------------------------------------------ cell-list form ------
+// For an orthorhombic cell much larger than the cutoff (the 64 A host at
+// 256^3: 16.8 M points x 14,700 atoms, ~3% of the pairs inside 12 A) most
+// pairs of the all-atom loop are wasted.  The cell-list form gives every
+// block one tile of XT_TX x XT_TY x XT_TZ grid points and stages in shared
+// memory only the host atoms that can reach the tile: the atoms are binned
+// on the host (bins of edge >= cutoff / 2, stably sorted so each bin keeps
+// file order), the block walks the bins that overlap the tile box grown by
+// the cutoff, keeps the atoms whose per-axis minimum-image distance from
+// the box is below the cutoff (a conservative bound: every atom that the
+// exact per-point test accepts passes), and then runs the same per-pair
+// arithmetic as k_extpot over that list.  Candidates are compacted with a
+// block-wide scan in bin order, so the summation order, and with it every
+// bit of the result, is the same from run to run; it differs from the
+// reference's file order only by the rounding of the sum.
+#define XT_TX 4
+#define XT_TY 8
+#define XT_TZ 8
+#define XT_THREADS (XT_TX * XT_TY * XT_TZ)
+#define XT_CAND 768     // staged candidates per round (48 B each)
+#define XT_MAXV 1024    // visited bins per tile (a multiple of XT_THREADS)
+
+struct CellArgs {
+  ExtArgs a;
+  int nb[3];            // bins per axis
+  double binw[3];       // bin edge L / nb
+  double cut_bound;     // cutoff with a relative margin for the box bound
+  int ntile[3];         // tiles per axis
+};
+
+// Per-axis minimum-image distance from coordinate x to the interval
+// [c - h, c + h] (0 inside), on a circle of length L.
+__device__ __forceinline__ double box_axis_dist(double x, double c, double h, double L, double invL) {
+  double d = x - c;
+  d -= L * rint(d * invL);
+  return fmax(fabs(d) - h, 0.0);
+}
+
+__global__ void __launch_bounds__(XT_THREADS)
+k_extpot_cells(CellArgs c, const AtomLJ* __restrict__ atoms, const int* __restrict__ bin_start, double* __restrict__ V) {
+  __shared__ AtomLJ cand[XT_CAND];
+  __shared__ int vb_beg[XT_MAXV], vb_off[XT_MAXV];
+  __shared__ int wsum[XT_THREADS / 32];
+  __shared__ int total_s;
+  const ExtArgs& a = c.a;
+  const int tid = threadIdx.x;
+  // tile and point of this thread
+  int t = blockIdx.x;
+  const int t3 = t % c.ntile[2]; t /= c.ntile[2];
+  const int t2 = t % c.ntile[1];
+  const int t1 = t / c.ntile[1];
+  const int tz = tid % XT_TZ, ty = (tid / XT_TZ) % XT_TY, tx = tid / (XT_TZ * XT_TY);
+  const int i = t1 * XT_TX + tx, j = t2 * XT_TY + ty, k = t3 * XT_TZ + tz;
+  const bool live = i < a.n1 && j < a.n2 && k < a.n3;
+  double p[3] = {0, 0, 0};
+  if (live) grid_point(a.rv, i, j, k, a.n1, a.n2, a.n3, p);
+  const double invL[3] = {1.0 / a.L[0], 1.0 / a.L[1], 1.0 / a.L[2]};
+  // tile box per axis (orthorhombic: coordinate a of point index q is L_a lin(q))
+  const int first[3] = {t1 * XT_TX, t2 * XT_TY, t3 * XT_TZ};
+  const int nax[3] = {a.n1, a.n2, a.n3};
+  const int ext[3] = {XT_TX, XT_TY, XT_TZ};
+  double bc[3], bh[3];
+  int blo[3], bcnt[3];
+  for (int d = 0; d < 3; ++d) {
+    const int last = min(first[d] + ext[d], nax[d]) - 1;
+    const double lo = a.rv[d * 3 + d] * lin_coord(first[d], nax[d]);
+    const double hi = a.rv[d * 3 + d] * lin_coord(last, nax[d]);
+    bc[d] = 0.5 * (lo + hi);
+    bh[d] = 0.5 * (hi - lo);
+    // bins that overlap [lo - cut, hi + cut] on the circle, one spare on each side
+    const double ulo = lo - c.cut_bound + 0.5 * a.L[d], uhi = hi + c.cut_bound + 0.5 * a.L[d];
+    int b0 = (int)floor(ulo / c.binw[d]) - 1, b1 = (int)floor(uhi / c.binw[d]) + 1;
+    if (b1 - b0 + 1 >= c.nb[d]) { b0 = 0; b1 = c.nb[d] - 1; }
+    blo[d] = b0;
+    bcnt[d] = b1 - b0 + 1;
+  }
+  // visited bins in (x, y, z) order: start and atom count, then the running
+  // offsets by a block-wide scan (XT_MAXV / XT_THREADS bins per thread)
+  const int nvis = bcnt[0] * bcnt[1] * bcnt[2];   // <= XT_MAXV (host check)
+  constexpr int PER = XT_MAXV / XT_THREADS;
+  int mycnt[PER];
+  int mysum = 0;
+  for (int q = 0; q < PER; ++q) {
+    const int v = tid * PER + q;
+    mycnt[q] = 0;
+    if (v < nvis) {
+      const int z = v % bcnt[2], y = (v / bcnt[2]) % bcnt[1], x = v / (bcnt[2] * bcnt[1]);
+      const int bx = ((blo[0] + x) % c.nb[0] + c.nb[0]) % c.nb[0];
+      const int by = ((blo[1] + y) % c.nb[1] + c.nb[1]) % c.nb[1];
+      const int bz = ((blo[2] + z) % c.nb[2] + c.nb[2]) % c.nb[2];
+      const int bin = (bx * c.nb[1] + by) * c.nb[2] + bz;
+      vb_beg[v] = bin_start[bin];
+      mycnt[q] = bin_start[bin + 1] - bin_start[bin];
+    }
+    mysum += mycnt[q];
+  }
+  {
+    const int lane = tid & 31, w = tid >> 5;
+    int incl = mysum;
+    for (int o = 1; o < 32; o <<= 1) {
+      const int y = __shfl_up_sync(0xffffffffu, incl, o);
+      if (lane >= o) incl += y;
+    }
+    if (lane == 31) wsum[w] = incl;
+    __syncthreads();
+    int before = 0, tot = 0;
+    for (int q = 0; q < XT_THREADS / 32; ++q) {
+      before += (q < w) ? wsum[q] : 0;
+      tot += wsum[q];
+    }
+    int off = before + incl - mysum;
+    for (int q = 0; q < PER; ++q) {
+      const int v = tid * PER + q;
+      if (v < nvis) vb_off[v] = off;
+      off += mycnt[q];
+    }
+    if (tid == 0) total_s = tot;
+    __syncthreads();
+  }
+  const int total = total_s;
+  const double cb2 = c.cut_bound * c.cut_bound;
+  double acc = 0.0;
+  int ncand = 0;
+  for (int base = 0; base < total; base += XT_THREADS) {
+    const int v = base + tid;
+    bool take = false;
+    AtomLJ at;
+    if (v < total) {
+      int lo = 0, hi = nvis - 1;   // last visited bin with vb_off <= v
+      while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (vb_off[mid] <= v) lo = mid; else hi = mid - 1;
+      }
+      at = atoms[vb_beg[lo] + (v - vb_off[lo])];
+      const double dx = box_axis_dist(at.x, bc[0], bh[0], a.L[0], invL[0]);
+      const double dy = box_axis_dist(at.y, bc[1], bh[1], a.L[1], invL[1]);
+      const double dz = box_axis_dist(at.z, bc[2], bh[2], a.L[2], invL[2]);
+      take = dx * dx + dy * dy + dz * dz < cb2;
+    }
+    // block-wide exclusive scan of `take`, in thread order
+    const unsigned bal = __ballot_sync(0xffffffffu, take);
+    const int lane = tid & 31, w = tid >> 5;
+    if (lane == 0) wsum[w] = __popc(bal);   // (read by every thread before the last barrier)
+    __syncthreads();
+    int before = 0, sum = 0;
+    for (int q = 0; q < XT_THREADS / 32; ++q) {
+      before += (q < w) ? wsum[q] : 0;
+      sum += wsum[q];
+    }
+    const int pos = ncand + before + __popc(bal & ((1u << lane) - 1u));
+    if (take) cand[pos] = at;
+    ncand += sum;
+    __syncthreads();
+    const bool flush = (ncand > XT_CAND - XT_THREADS) || (base + XT_THREADS >= total);
+    if (flush) {
+      if (live) {
+        for (int q = 0; q < ncand; ++q) {
+          const AtomLJ atq = cand[q];
+          const double rx = min_image(__dsub_rn(p[0], atq.x), a.L[0], invL[0]);
+          const double ry = min_image(__dsub_rn(p[1], atq.y), a.L[1], invL[1]);
+          const double rz = min_image(__dsub_rn(p[2], atq.z), a.L[2], invL[2]);
+          const double r2 =
+              __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(rx, rx), __dmul_rn(ry, ry)), __dmul_rn(rz, rz)), 1e-16);
+          const double R = sqrt(r2);
+          if (R < a.cutoff) {
+            const double qq = __ddiv_rn(atq.sm, R);
+            const double q2 = __dmul_rn(qq, qq);
+            const double r6 = __dmul_rn(__dmul_rn(q2, q2), q2);
+            const double r12 = __dmul_rn(r6, r6);
+            const double vv = __dsub_rn(__dmul_rn(atq.fe, __dsub_rn(r12, r6)), atq.shift);
+            acc = __dadd_rn(acc, vv);
+          }
+        }
+      }
+      ncand = 0;
+      __syncthreads();
+    }
+  }
+  if (live) {
+    double vv = acc;
+    if (!isfinite(vv)) vv = a.vcap;
+    if (vv > a.vcap) vv = a.vcap;
+    V[((size_t)i * a.n2 + j) * a.n3 + k] = vv;
+  }
+}
+
+// Bins of the cell-list form, or 0 when the all-atom form is the better
+// choice: the cell must be orthorhombic, every axis at least 3 bins of edge
+// >= cutoff / 2, the visited bins of one tile within XT_MAXV, and the staged
+// atoms a small share of all (mode 1 forces the cell list where legal).
+static int extpot_cell_bins(const cmm_grid* g, const ExtArgs& a, int natom, int mode, int nb[3]) {
+  const double* rv = g->rvecs;
+  if (rv[1] != 0 || rv[2] != 0 || rv[3] != 0 || rv[5] != 0 || rv[6] != 0 || rv[7] != 0) return 0;
+  if (!(a.cutoff > 0) || natom < 1) return 0;
+  const int nax[3] = {a.n1, a.n2, a.n3};
+  const int ext[3] = {XT_TX, XT_TY, XT_TZ};
+  double frac = 1.0;
+  long long vis = 1;
+  for (int d = 0; d < 3; ++d) {
+    nb[d] = (int)floor(a.L[d] / (0.5 * a.cutoff));
+    if (nb[d] < 3) return 0;
+    if (nb[d] > 256) nb[d] = 256;
+    const double binw = a.L[d] / nb[d];
+    const double box = a.L[d] * ext[d] / nax[d];
+    // the kernel visits floor(uhi/w) - floor(ulo/w) + 3 <= (uhi - ulo)/w + 4 bins
+    const int cnt = std::min(nb[d], (int)ceil((box + 2 * a.cutoff) / binw) + 4);
+    vis *= cnt;
+    frac *= std::min(1.0, ((box + 2 * a.cutoff) / binw + 3) / nb[d]);   // expected share of the atoms
+  }
+  if (vis > XT_MAXV) return 0;
+  if (mode == 1) return 1;
+  return (natom >= 1024 && frac < 0.5) ? 1 : 0;
+}
+
+static int g_extpot_mode = 0;   // 0 by size, 1 cell list where legal, 2 all atoms
+
+extern "C" int cmm_extpot_set_mode(int mode) {
+  if (mode < 0 || mode > 2) return CMM_ERR_ARG;
+  g_extpot_mode = mode;
+  return CMM_OK;
+}
+
 extern "C" int cmm_extpot_lj(const cmm_grid* g, const double* d_pos, const int* d_type, int natom,
                              const double* d_type_sig, const double* d_type_eps, int ntype,
                              double guest_sig, double guest_eps, double cutoff, double v_cap,
@@ -147,19 +373,68 @@ extern "C" int cmm_extpot_lj(const cmm_grid* g, const double* d_pos, const int* 
       h[i].shift = fe * df;
     }
     free(hpos); free(htyp); free(hs); free(he);
-    if (rc == CMM_OK && cudaMalloc(&d, sizeof(AtomLJ) * natom) != cudaSuccess) rc = CMM_ERR_NOMEM;
-    if (rc == CMM_OK && cudaMemcpyAsync(d, h, sizeof(AtomLJ) * natom, cudaMemcpyHostToDevice, st) != cudaSuccess)
-      rc = CMM_ERR_CUDA;
     if (rc != CMM_OK) {
       free(h);
-      if (d) cudaFree(d);
       return rc;
     }
   }
-  const long long npts = (long long)g->n1 * g->n2 * g->n3;
-  const int nblk = (int)((npts + EXT_THREADS - 1) / EXT_THREADS);
-  k_extpot<<<nblk, EXT_THREADS, 0, st>>>(a, d, d_V);
-  int rc = (cudaPeekAtLastError() == cudaSuccess) ? CMM_OK : CMM_ERR_CUDA;
+  int nb[3] = {0, 0, 0};
+  const bool cells = natom > 0 && g_extpot_mode != 2 && extpot_cell_bins(g, a, natom, g_extpot_mode, nb);
+  std::vector<int> bin_start;
+  if (cells) {  // stable sort of the table by bin: each bin keeps file order
+    const int nbin = nb[0] * nb[1] * nb[2];
+    std::vector<int> bin_of(natom), cnt(nbin + 1, 0);
+    for (int q = 0; q < natom; ++q) {
+      const double x[3] = {h[q].x, h[q].y, h[q].z};
+      int bi[3];
+      for (int ax = 0; ax < 3; ++ax) {
+        double w = x[ax] - a.L[ax] * rint(x[ax] / a.L[ax]);      // [-L/2, L/2]
+        int b = (int)floor((w + 0.5 * a.L[ax]) / (a.L[ax] / nb[ax]));
+        bi[ax] = b < 0 ? 0 : (b >= nb[ax] ? nb[ax] - 1 : b);
+      }
+      bin_of[q] = (bi[0] * nb[1] + bi[1]) * nb[2] + bi[2];
+      cnt[bin_of[q] + 1] += 1;
+    }
+    for (int b = 0; b < nbin; ++b) cnt[b + 1] += cnt[b];
+    bin_start = cnt;
+    std::vector<AtomLJ> sorted(natom);
+    std::vector<int> fill(cnt.begin(), cnt.end() - 1);
+    for (int q = 0; q < natom; ++q) sorted[fill[bin_of[q]]++] = h[q];
+    std::memcpy(h, sorted.data(), sizeof(AtomLJ) * natom);
+  }
+  int* d_bins = nullptr;
+  int rc = CMM_OK;
+  if (natom > 0) {
+    const size_t abytes = sizeof(AtomLJ) * natom, bbytes = sizeof(int) * bin_start.size();
+    if (cudaMalloc(&d, abytes + bbytes) != cudaSuccess) rc = CMM_ERR_NOMEM;
+    if (rc == CMM_OK && cudaMemcpyAsync(d, h, abytes, cudaMemcpyHostToDevice, st) != cudaSuccess) rc = CMM_ERR_CUDA;
+    if (rc == CMM_OK && cells) {
+      d_bins = (int*)((char*)d + abytes);
+      if (cudaMemcpyAsync(d_bins, bin_start.data(), bbytes, cudaMemcpyHostToDevice, st) != cudaSuccess)
+        rc = CMM_ERR_CUDA;
+    }
+  }
+  if (rc == CMM_OK) {
+    if (cells) {
+      CellArgs c;
+      c.a = a;
+      for (int ax = 0; ax < 3; ++ax) {
+        c.nb[ax] = nb[ax];
+        c.binw[ax] = a.L[ax] / nb[ax];
+      }
+      c.cut_bound = cutoff * (1.0 + 1e-9) + 1e-9;
+      c.ntile[0] = cmm_div_up(g->n1, XT_TX);
+      c.ntile[1] = cmm_div_up(g->n2, XT_TY);
+      c.ntile[2] = cmm_div_up(g->n3, XT_TZ);
+      const long long nt = (long long)c.ntile[0] * c.ntile[1] * c.ntile[2];
+      k_extpot_cells<<<(unsigned)nt, XT_THREADS, 0, st>>>(c, d, d_bins, d_V);
+    } else {
+      const long long npts = (long long)g->n1 * g->n2 * g->n3;
+      const int nblk = (int)((npts + EXT_THREADS - 1) / EXT_THREADS);
+      k_extpot<<<nblk, EXT_THREADS, 0, st>>>(a, d, d_V);
+    }
+    rc = (cudaPeekAtLastError() == cudaSuccess) ? CMM_OK : CMM_ERR_CUDA;
+  }
   if (d) {
     cudaStreamSynchronize(st);
     cudaFree(d);

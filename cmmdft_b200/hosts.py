@@ -93,12 +93,29 @@ def random_sequential_host(lengths_A, natom, seed, min_sep_A=1.3,
     n = 0
     tries = 0
     min2 = min_sep_A ** 2
+    # Large cells test a trial only against the accepted atoms of the 27 bins
+    # (edge >= min_sep) around it: the same accept/reject decisions as the
+    # test against every atom, since no other atom is within min_sep.
+    nb = np.floor(L / min_sep_A).astype(int)
+    binned = natom > 2000 and bool(np.all(nb >= 3))
+    if binned:
+        bins = {}
+        off = np.array([(a, b, c) for a in (-1, 0, 1) for b in (-1, 0, 1) for c in (-1, 0, 1)])
     while n < natom:
         tries += 1
         if tries > max_tries:
             raise RuntimeError("RSA could not place %d atoms" % natom)
         trial = rng.uniform(0.0, 1.0, 3) * L
-        if n:
+        if binned:
+            bt = np.minimum((trial / L * nb).astype(int), nb - 1)
+            near = [i for o in off for i in bins.get(tuple((bt + o) % nb), ())]
+            if near:
+                d = accepted[near] - trial
+                d -= L * np.round(d / L)
+                if np.min(np.einsum("ij,ij->i", d, d)) < min2:
+                    continue
+            bins.setdefault(tuple(bt), []).append(n)
+        elif n:
             d = accepted[:n] - trial
             d -= L * np.round(d / L)
             if np.min(np.einsum("ij,ij->i", d, d)) < min2:
@@ -139,3 +156,10 @@ def methane_guest_params():
 def cubic_host_779(seed=0):
     """The 276-atom cell's atom density at a = 24.0 angstrom (779 atoms, 96^3)."""
     return random_sequential_host((24.0, 24.0, 24.0), 779, seed)
+
+
+def cubic_host_64(seed=4, density_A3=0.056):
+    """The large cubic cell of the 256^3 WDA workload: a = 64 angstrom at the
+    276-atom cell's atom density (14,680 atoms, the same type mix)."""
+    natom = int(round(density_A3 * 64.0 ** 3))
+    return random_sequential_host((64.0, 64.0, 64.0), natom, seed)

@@ -150,6 +150,15 @@ int cmm_extpot_lj(const cmm_grid* grid, const double* d_pos, const int* d_type, 
                   const double* d_type_sig, const double* d_type_eps, int ntype,
                   double guest_sig, double guest_eps, double cutoff, double v_cap,
                   double* d_V, void* stream);
+/* Form of cmm_extpot_lj for the rest of the process: 0 = by size (default:
+ * the cell-list form for orthorhombic cells whose tiles reach under half of
+ * the atoms, at least 1024 atoms, and every axis at least three bins of
+ * edge cutoff / 2), 1 = the cell-list form wherever the cell allows it,
+ * 2 = the all-atom form.  The cell-list form stages, per tile of 4 x 8 x 8
+ * grid points, the atoms within the cutoff of the tile in shared memory and
+ * sums them in bin order instead of file order (the same pairs; the sum's
+ * rounding differs).  Process-wide, not per grid or thread. */
+int cmm_extpot_set_mode(int mode);
 
 /* Unnormalised 3D real-to-half-complex FFT and its inverse in the plan's
  * spectrum layout (scipy.fft.fftn / ifftn*N as used by Grid.fft/ifft,

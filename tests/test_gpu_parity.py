@@ -532,3 +532,61 @@ def test_native_driver_matches_reference(golden32, fn32):
     assert relerr(rho[0].cpu().numpy(), golden32["and_rho"]) < 1e-9
     assert scalar_rel(N[0], golden32["and_N"]) < 1e-10
     assert scalar_rel(s.omega0[0], golden32["and_omega"]) < 1e-10
+
+
+@pytest.mark.parametrize("host_name,npts", [("cubic_host_779", (96, 96, 96)), ("cubic_host_64", (64, 64, 64)),
+                                            ("uneven_host_1", None)])
+def test_extpot_cell_list_matches_all_atom(cuda, host_name, npts):
+    """The cell-list external potential (tiles of grid points with the atoms
+    within the cutoff staged in shared memory) against the all-atom form on
+    the same grid: the same pairs summed in another order, 1e-13 relative to
+    the cap."""
+    from cmmdft_b200 import hosts as H
+    if host_name == "uneven_host_1":
+        host = H.uneven_hosts(nhost=2)[1]
+        npts = tuple(int(np.ceil(np.linalg.norm(host.rvecs[a]) / (0.25 * angstrom))) for a in range(3))
+    else:
+        host = getattr(H, host_name)()
+    guest = methane_guest_params()
+    plan = E.GridPlan(npts, host.rvecs)
+    sig, eps = W.host_type_arrays(host)
+    cap = 1e4 * kjmol
+    lib = L.lib()
+    out = {}
+    try:
+        for mode in (1, 2):
+            assert lib.cmm_extpot_set_mode(mode) == 0
+            out[mode] = E.external_potential(plan, host.recentred_pos(), host.ffatype_ids, sig, eps, guest[0],
+                                             guest[1], 12 * angstrom, cap).cpu().numpy()
+    finally:
+        lib.cmm_extpot_set_mode(0)
+    err = relerr(out[1], out[2], cap)
+    print("%s %s: cell list vs all atoms %.2e of the cap" % (host_name, npts, err))
+    assert err < 1e-13
+
+
+def test_extpot_256_against_oracle(cuda):
+    """The 256^3 grid of the 64 A host (14,680 atoms, cell-list form by size)
+    against the oracle's get_external_potential restatement at 4096 seeded
+    grid points: 1e-12 relative to the cap."""
+    from cmmdft_b200.hosts import cubic_host_64
+    from oracle import cmm_oracle as O
+    host = cubic_host_64()
+    guest = methane_guest_params()
+    n = 256
+    plan = E.GridPlan((n, n, n), host.rvecs)
+    sig, eps = W.host_type_arrays(host)
+    cap = 1e4 * kjmol
+    V = E.external_potential(plan, host.recentred_pos(), host.ffatype_ids, sig, eps, guest[0], guest[1],
+                             12 * angstrom, cap).cpu().numpy()
+    rng = np.random.default_rng(11)
+    idx = rng.integers(0, n, size=(4096, 3))
+    g = np.linspace(-0.5, 0.5, n, endpoint=False)
+    frac = g[idx]
+    pts = np.einsum('ab,ia->ib', host.rvecs, frac)       # Grid.points
+    Vo = O.external_potential(pts, host.ff, guest[0], guest[1], host.recentred_pos(), host.ffatypes,
+                              host.ffatype_ids, host.rvecs)
+    Vo = O.cap_potential(Vo, cap)
+    err = relerr(V[idx[:, 0], idx[:, 1], idx[:, 2]], Vo, cap)
+    print("256^3 extpot vs oracle at 4096 points: %.2e of the cap" % err)
+    assert err < 1e-12
