@@ -164,6 +164,11 @@ __device__ __forceinline__ double& rel(const PlaneSmem& s, const PlaneShape<N2C,
 }
 
 // Copy nslot spectrum planes (global: field f at src + f*fs + plane_off, [n2][h3]) into smem.
+// Every element is an asynchronous 16-byte global-to-shared copy
+// (cp.async.cg: through L2, no register staging), so all of a thread's
+// copies are in flight at once and the plane's load latency is paid once;
+// the thread waits for its own copies, and the caller's __syncthreads()
+// makes the whole plane visible.
 template <int N2C, int M3C>
 __device__ inline void load_spec_planes(const GridDev& g, const PlaneSmem& s, int nslot, const double2* src,
                                         size_t plane_off, size_t fs) {
@@ -173,9 +178,12 @@ __device__ inline void load_spec_planes(const GridDev& g, const PlaneSmem& s, in
     const double2* p = src + f * fs + plane_off;
     for (int i = threadIdx.x; i < cnt; i += blockDim.x) {
       const int r = i / h3, c = i - r * h3;
-      s.slots[((size_t)r * nslot + f) * h3 + c] = __ldg(p + i);
+      const unsigned dst = (unsigned)__cvta_generic_to_shared(s.slots + ((size_t)r * nslot + f) * h3 + c);
+      asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(dst), "l"(p + i) : "memory");
     }
   }
+  asm volatile("cp.async.commit_group;\n" ::: "memory");
+  asm volatile("cp.async.wait_group 0;\n" ::: "memory");
 }
 
 template <int N2C, int M3C>
@@ -693,10 +701,16 @@ __device__ __forceinline__ void phi_funcs(S n3, S ln, S n32, S n33, int base, S&
       p3 = (1 - 4 * n3 / 9 + n32 / 18) / (24 * M_PI * q);
       dp3 = (7.0 / 3 - n3 / 2 + n32 / 10) / (36 * M_PI * c);
     } else {
-      p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) / (3 * (n3 - n32));
-      dp2 = -2 * (n3 - 3 * n32 + q * ln) / (3 * n32 * q);
-      p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) / ((3 * n32) * 24 * M_PI * q);
-      dp3 = (2 * n3 - 5 * n32 + 6 * n33 - n32 * n32 + 2 * c * ln) / (36 * M_PI * n33 * c);
+      // The four denominators are products of powers of n3 and (1 - n3):
+      // two reciprocals serve all of them (q = (1-n3)^2, c = (1-n3)^3).
+      // The numerators, whose cancellation at small n3 sets the accuracy of
+      // these closed forms, are formed exactly as in the reference.
+      const S d = 1 / (1.0 - n3), u = 1 / n3;
+      const S ud = u * d, ud2 = ud * ud;
+      p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) * (ud * (1.0 / 3));
+      dp2 = -2 * (n3 - 3 * n32 + q * ln) * (ud2 * (1.0 / 3));
+      p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) * (ud2 * (1.0 / (72 * M_PI)));
+      dp3 = (2 * n3 - 5 * n32 + 6 * n33 - n32 * n32 + 2 * c * ln) * (ud2 * ud * (1.0 / (36 * M_PI)));
     }
   }
 }
@@ -741,9 +755,11 @@ __device__ __forceinline__ void phi_values(double n3, double ln, double n32, dou
   } else if (n3 <= 1e-8) {
     p2 = (1 + n32 / 9) / (1 - n3);
     p3 = (1 - 4 * n3 / 9 + n32 / 18) / (24 * M_PI * q);
-  } else {
-    p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) / (3 * (n3 - n32));
-    p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) / ((3 * n32) * 24 * M_PI * q);
+  } else {  // as phi_funcs, so that Phi agrees with the derivative pass bit for bit
+    const double d = 1 / (1.0 - n3), u = 1 / n3;
+    const double ud = u * d, ud2 = ud * ud;
+    p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) * (ud * (1.0 / 3));
+    p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) * (ud2 * (1.0 / (72 * M_PI)));
   }
 }
 

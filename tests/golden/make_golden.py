@@ -7,6 +7,7 @@ machines):
     python tests/golden/make_golden.py --reference <reference tree> --iso64 [--procs 8]
     python tests/golden/make_golden.py --reference <reference tree> --qn
     python tests/golden/make_golden.py --reference <reference tree> --dropin
+    python tests/golden/make_golden.py --reference <reference tree> --uneven
 
 ``--reference`` (or the environment variable CMM_REFERENCE_ROOT) names the
 root of the reference's source tree, the directory that holds ``cmmdft/``.
@@ -45,6 +46,9 @@ Outputs (small ``.npz`` files) land next to this script:
               DER columns); and Calculator.return_loading (absolute and
               excess), free_energy_contrib per part and grand_potential of
               both solutions (``--dropin`` only).
+  uneven5.npz     host 5 of the uneven batch (uneven_hosts(8, 2)) on its
+              0.25 A grid, 119 x 157 x 125 (157 prime: Rader stages on the
+              GPU), at 0.1, 1 and 10 bar: N, Omega, steps (``--uneven``).
   iso64_rho.npz   the converged densities of that isotherm at the pressure
               indices ISO_RHO_IDX, and the reference run against itself: the
               same points re-solved from a start perturbed by one ulp, with
@@ -105,7 +109,7 @@ def build(ref, npts, host, T, P_bar, tmp, tail=False, wda=False):
     t0 = time.time()
     V = extpot.get_external_potential(pts, host.ff, sig, eps, mol, cutoff=12 * angstrom)
     t_ext = time.time() - t0
-    fn = os.path.join(tmp, 'epot_%d.npy' % npts)
+    fn = os.path.join(tmp, 'epot_%s.npy' % '_'.join(str(n) for n in np.atleast_1d(npts)))
     np.save(fn, V.reshape(grid.npoints))
     fe = functionals.FreeEnergy(grid, syst, T, workdir=tmp, name_dict={}, overwrite=True)
     fe.add_hard_sphere(version='WBII')
@@ -172,6 +176,46 @@ def _iso64_point(task):
     print('iso64 P=%.4g bar%s: N=%.12e steps=%d conv=%s (%.0f s)'
           % (P, ' (perturbed start)' if perturb else '', N, s.curr_step, conv, time.time() - t0), flush=True)
     return i, b['mu'], bulk, N, s.omega0, s.curr_step, bool(conv), (rho if conv else None)
+
+
+UNEVEN_HOST = 5                       # uneven_hosts(8, 2)[5]: 119 x 157 x 125 (prime 157), 2026 atoms
+UNEVEN_PRESSURES = (0.1, 1.0, 10.0)   # bar
+
+
+def _uneven_point(task):
+    ref_root, P_bar = task
+    ref = import_reference(ref_root)
+    solver = ref[2]
+    from cmmdft_b200.hosts import uneven_hosts
+    from cmmdft_b200.units import boltzmann, angstrom
+    T = 300.0
+    host = uneven_hosts(8, 2)[UNEVEN_HOST]
+    npts = [int(np.ceil(np.linalg.norm(host.rvecs[:, a]) / (0.25 * angstrom))) for a in range(3)]
+    b = quiet(build, ref, npts, host, T, P_bar, tempfile.mkdtemp(prefix='cmm_uneven_'))
+    mb, V = b['mbwr'], b['fe'].part_dict['ExtPot'].potential
+    mb.set_temperature(T)
+    bulk = np.nanmin(mb.solve_densities_from_chempots([b['mu']]), axis=1)[0]
+    rho0 = bulk * np.exp(-np.maximum(V, 0) / boltzmann / T)
+    s = solver.Anderson(b['prog'], nsteps=500, m=5, criterion='res', threshold=1e-8)
+    t0 = time.time()
+    N, rho, conv = quiet(s.solve, b['mu'], rho0, 3)
+    print('uneven host %d %s P=%g bar: N=%.12e steps=%d conv=%s (%.0f s)'
+          % (UNEVEN_HOST, npts, P_bar, N, s.curr_step, conv, time.time() - t0), flush=True)
+    return P_bar, b['mu'], bulk, N, s.omega0, s.curr_step, bool(conv), npts
+
+
+def uneven(args):
+    """One host of the uneven batch at its spacing-derived grid (a Rader
+    prime on y), hybrid Anderson m=5 to RES < 1e-8 from Ninit = rho_bulk."""
+    import multiprocessing as mp
+    with mp.get_context('spawn').Pool(len(UNEVEN_PRESSURES)) as pool:
+        res = pool.map(_uneven_point, [(args.reference, p) for p in UNEVEN_PRESSURES])
+    cols = list(zip(*res))
+    out = dict(host=UNEVEN_HOST, npoints=np.array(cols[7][0]), pressures=np.array(cols[0]), mu=np.array(cols[1]),
+               rho_bulk=np.array(cols[2]), N=np.array(cols[3]), omega=np.array(cols[4]), steps=np.array(cols[5]),
+               converged=np.array(cols[6]))
+    np.savez_compressed(os.path.join(HERE, 'uneven5.npz'), **out)
+    print('wrote uneven5.npz')
 
 
 QN_CASES = [('bfgs', 'backtracking'), ('broyden', 'backtracking'), ('cg', 'backtracking'), ('bfgs', 'quadratic'),
@@ -384,6 +428,7 @@ def main():
     ap.add_argument('--iso64', action='store_true')
     ap.add_argument('--qn', action='store_true')
     ap.add_argument('--dropin', action='store_true')
+    ap.add_argument('--uneven', action='store_true')
     ap.add_argument('--procs', type=int, default=8)
     args = ap.parse_args()
     if not args.reference:
@@ -394,6 +439,8 @@ def main():
         return qn32(args)
     if args.dropin:
         return dropin32(args)
+    if args.uneven:
+        return uneven(args)
     ref = import_reference(args.reference)
     solver = ref[2]
     from cmmdft_b200.hosts import cubic_host_276, HELIUM
