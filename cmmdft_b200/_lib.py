@@ -109,8 +109,8 @@ _SIGS = {
     "cmm_ls_finalize": ([c_int, c_void_p, c_void_p, c_int, c_void_p, c_void_p], c_int),
     "cmm_solve_stage_bytes": ([c_int], ctypes.c_size_t),
     "cmm_anderson_slsqp": ([P(c_double), c_int, P(c_double), P(c_int), P(c_int)], c_int),
-    "cmm_fmt_hvp": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_int, c_void_p, c_void_p, c_void_p,
-                     c_void_p, c_void_p, c_void_p, c_void_p], c_int),
+    "cmm_fmt_hvp": ([c_void_p, c_int, c_void_p, c_double, c_double, c_int, c_void_p, c_int, c_void_p, c_void_p,
+                     c_void_p, c_void_p, c_void_p, c_void_p, c_void_p], c_int),
     "cmm_extpot_lj_grad": ([c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_double, c_double,
                             c_double, c_double, c_void_p, c_void_p], c_int),
     "cmm_contract": ([c_void_p, c_ll, c_int, c_void_p, c_ll, c_int, c_ll, c_void_p, c_int, c_void_p], c_int),

@@ -135,9 +135,14 @@ def hvp(fn, wd_rho, v, transpose=False, work=None):
     if work is None:
         work = torch.empty((fn.nwork, B, plan.nspec * 2), dtype=torch.float64, device="cuda")
     kst = _conj_spectrum(fn.kst) if transpose else fn.kst
-    check(L.lib().cmm_fmt_hvp(plan.handle, B, None, fn.R, fn.beta, fn.version, int(transpose), ptr(kst),
+    check(L.lib().cmm_fmt_hvp(plan.handle, B, None, fn.R, fn.beta, fn.version, _wda_ptr(fn), int(transpose), ptr(kst),
                               ptr(fn.wtab), ptr(wd_rho), ptr(vhat), ptr(out), ptr(work), _stream()), "cmm_fmt_hvp")
     return plan.irfft_yz(out)
+
+
+def _wda_ptr(fn):
+    import ctypes
+    return ctypes.cast(ctypes.pointer(fn.wda), ctypes.c_void_p) if fn.wda is not None else None
 
 
 class _BiCGStab(object):
@@ -169,8 +174,9 @@ class _BiCGStab(object):
         vhat = self.plan.rfft_yz(self.u.view((self.B,) + self.plan.npoints))
         out = self.plan.new_spec(self.B)
         fn = self.fn
-        check(self.lib.cmm_fmt_hvp(self.plan.handle, self.B, None, fn.R, fn.beta, fn.version, 1, ptr(self.kst_t),
-                                   ptr(fn.wtab), ptr(self.wd), ptr(vhat), ptr(out), ptr(self.work), _stream()),
+        check(self.lib.cmm_fmt_hvp(self.plan.handle, self.B, None, fn.R, fn.beta, fn.version, _wda_ptr(fn), 1,
+                                   ptr(self.kst_t), ptr(fn.wtab), ptr(self.wd), ptr(vhat), ptr(out), ptr(self.work),
+                                   _stream()),
               "cmm_fmt_hvp")
         Au = self.plan.irfft_yz(out).view(self.B, self.npts)
         self._vec(1, dst, x=src, y=Au, a=a, c=fn.beta)
@@ -263,16 +269,35 @@ def _mfa_values(fn, kst, rhohat, B, buf):
     return plan.irfft_yz(ch).reshape(B, plan.npts)
 
 
-def _excess_values(fn, rhohat, B):
-    """(C1 - V fields [B, npts], F_HS + F_MFA per instance) of a functional."""
+def _excess_values(fn, rhohat, B, wda_only=False):
+    """(C1 - V fields [B, npts], F_HS + F_MFA (+ F_WDA) per instance) of a
+    functional; wda_only: the free energy of the WDA part alone."""
     plan = fn.plan
     buf = E.Buffers(plan, B, nwork=fn.nwork)
     chat = plan.new_spec(B)
     fn.c1(buf, rhohat, chat, want=3)
     E.finalize(buf, (1 << L.NSTAT) - 1)
     st = buf.stats.cpu().numpy()
-    F = st[:, L.STAT_PHI] * plan.dr / fn.beta + 0.5 * st[:, L.STAT_MFA] * plan.dr
+    Fw = st[:, L.STAT_WDA] * plan.dr if fn.wda is not None else np.zeros(B)
+    F = Fw if wda_only else st[:, L.STAT_PHI] * plan.dr / fn.beta + 0.5 * st[:, L.STAT_MFA] * plan.dr + Fw
     return plan.irfft_yz(chat).reshape(B, plan.npts), F
+
+
+def _wda_values(fn, guest, temperature, mfa_cutoff, rep, rhohat, B, zero_k):
+    """(C1 of the WDA part [B, npts], F_WDA per instance) of the functional
+    rebuilt for guest (sigma, epsilon, mass): R_hs, the mean-field EOS a from
+    the MFA kernel of that guest, the WDA EOS; the MFA convolution is off and
+    the hard-sphere part at the same R is subtracted."""
+    plan = fn.plan
+    sig, eps, mass = guest
+    R = W.hardsphere_radius(sig, eps, temperature)
+    _, a = E.mfa_kernel_spectrum(plan, sig, eps, mfa_cutoff, rep=rep)
+    wda = W.wda_struct(sig, eps, mass, temperature, R, a)
+    fw = E.Functional(plan, R, fn.beta, fn.wavelength, fn.V, fn.version, zero_k, a, wda=wda)
+    fh = E.Functional(plan, R, fn.beta, fn.wavelength, fn.V, fn.version & ~L.WDA, zero_k)
+    cw, Fw = _excess_values(fw, rhohat, B, wda_only=True)
+    ch, _ = _excess_values(fh, rhohat, B)
+    return cw - ch, Fw
 
 
 def helium_fraction(plan, host, temperature, cutoff=12 * angstrom):
@@ -294,8 +319,8 @@ def adjoint_gradients(fn, host, guest, temperature, pressures, mus, rho, cutoff=
     Returns a dict of N, Omega, dN, dOmega [B, K] (and Nex, dNex), the
     parameter names, and the adjoint solves' iteration counts and residuals.
     """
-    if fn.version & (L.WDA | L.NOHS):
-        raise NotImplementedError("adjoint gradients: WDA and MFA-only functionals are not supported")
+    if fn.version & L.NOHS:
+        raise NotImplementedError("adjoint gradients: MFA-only functionals are not supported")
     plan = fn.plan
     B = rho.shape[0]
     n = plan.npts
@@ -348,7 +373,7 @@ def adjoint_gradients(fn, host, guest, temperature, pressures, mus, rho, cutoff=
     dC_R = torch.zeros((B, n), dtype=torch.float64, device="cuda")
     dF_R = np.zeros(B)
     for step, wgt in stencil:
-        fr = E.Functional(plan, fn.R + step * hR, fn.beta, fn.wavelength, fn.V, fn.version, zero_k)
+        fr = E.Functional(plan, fn.R + step * hR, fn.beta, fn.wavelength, fn.V, fn.version & ~L.WDA, zero_k)
         c1x, F = _excess_values(fr, rhohat, B)
         dC_R += (wgt / (12 * hR)) * c1x
         dF_R += (wgt / (12 * hR)) * F
@@ -369,11 +394,31 @@ def adjoint_gradients(fn, host, guest, temperature, pressures, mus, rho, cutoff=
     half_rho = 0.5 * dV * rho2
     D_eps = dR[0] * dC_R + c_mfa / geps
     D_sig = dR[1] * dC_R + dC_ms
+    dF_wda = np.zeros((B, 2))
+    if fn.wda is not None:
+        # the WDA part moves with the guest through R_hs (weight diameter,
+        # Carnahan-Starling eta), the MBWR coefficients and the mean-field
+        # EOS a; it is smooth, so its explicit partials are central
+        # differences (fourth order, relative step 1e-5) of the functional
+        # rebuilt at the shifted parameters, less its hard-sphere part
+        for k, idx in ((0, 1), (1, 0)):
+            h = 1e-5 * guest[idx]
+            dCw = torch.zeros((B, n), dtype=torch.float64, device="cuda")
+            for step, wgt in stencil:
+                g = list(guest)
+                g[idx] = guest[idx] + step * h
+                cw, Fw = _wda_values(fn, g, temperature, mfa_cutoff, rep, rhohat, B, zero_k)
+                dCw += (wgt / (12 * h)) * cw
+                dF_wda[:, k] += (wgt / (12 * h)) * Fw
+            if k == 0:
+                D_eps = D_eps + dCw
+            else:
+                D_sig = D_sig + dCw
     for k, Dk in ((0, D_eps), (1, D_sig)):
         Gx_n[:, k] = _pair_dots(lam_n, Dk)
         Gx_o[:, k] = _pair_dots(lam_o, Dk)
-    dF[:, 0] = dR[0] * dF_R + _pair_dots(half_rho, c_mfa) / geps
-    dF[:, 1] = dR[1] * dF_R + _pair_dots(half_rho, dC_ms)
+    dF[:, 0] = dR[0] * dF_R + _pair_dots(half_rho, c_mfa) / geps + dF_wda[:, 0]
+    dF[:, 1] = dR[1] * dF_R + _pair_dots(half_rho, dC_ms) + dF_wda[:, 1]
     # EOS
     dmu[:, :2], dbulk[:, :2] = eos_derivatives(pressures, temperature, guest)
     dN = -beta * (G_n + Gx_n) + beta * dmu * sum_n[:, None]
@@ -417,7 +462,7 @@ class IsothermModel(object):
     def __init__(self, host, guest, temperature, npoints, pressures, quantity='excess', threshold=1e-12,
                  criterion='res', nsteps=1000, method='hybridanderson', version='WBII', tailcorrections=False,
                  cutoff=12 * angstrom, mfa_cutoff=12 * angstrom, limit_potential=1e4 * kjmol, fd_rel=1e-3,
-                 tol=1e-11):
+                 tol=1e-11, wda=False):
         assert quantity in ('excess', 'absolute', 'omega')
         self.host, self.guest = host, guest
         self.T = float(temperature)
@@ -425,7 +470,7 @@ class IsothermModel(object):
         self.pressures = np.asarray(pressures, dtype=np.float64)
         self.quantity = quantity
         self.solve_kw = dict(threshold=threshold, criterion=criterion, nsteps=nsteps, method=method)
-        self.version, self.tail = version, tailcorrections
+        self.version, self.tail, self.wda = version, tailcorrections, bool(wda)
         self.cutoff, self.mfa_cutoff, self.vcap = cutoff, mfa_cutoff, limit_potential
         self.fd_rel, self.tol = fd_rel, tol
         self.theta0 = pack_params(host, guest)
@@ -440,7 +485,7 @@ class IsothermModel(object):
         host, guest = unpack_params(theta, self.host, self.guest)
         fn = W.build_functional(host, self.npoints, self.T, guest, version=self.version,
                                 tailcorrections=self.tail, cutoff=self.cutoff, mfa_cutoff=self.mfa_cutoff,
-                                limit_potential=self.vcap, plan=self.plan)
+                                limit_potential=self.vcap, plan=self.plan, wda=self.wda)
         mus, bulks = eos_inputs(self.pressures, self.T, guest)
         rho0 = W.initial_density(fn, mus, ninit=bulks)
         s = GroupedSolve(fn, mus, groups=1, divergence_guard=True, **self.solve_kw)

@@ -34,8 +34,13 @@ __device__ __forceinline__ Dual operator/(double a, const Dual& b) {
 }
 __device__ __forceinline__ Dual& operator+=(Dual& a, const Dual& b) { a = a + b; return a; }
 __device__ __forceinline__ Dual& operator-=(Dual& a, const Dual& b) { a = a - b; return a; }
+__device__ __forceinline__ Dual& operator*=(Dual& a, const Dual& b) { a = a * b; return a; }
 __device__ __forceinline__ bool operator<=(const Dual& a, double b) { return a.v <= b; }
 __device__ __forceinline__ Dual log(const Dual& a) { return Dual(::log(a.v), a.d / a.v); }
+__device__ __forceinline__ Dual exp(const Dual& a) {
+  const double e = ::exp(a.v);
+  return Dual(e, e * a.d);
+}
 // clipping: the derivative of the selected branch (0 where the bound is taken)
 __device__ __forceinline__ Dual fmin(const Dual& a, double b) { return (a.v <= b) ? a : Dual(b, 0.0); }
 __device__ __forceinline__ Dual fmax(const Dual& a, double b) { return (a.v >= b) ? a : Dual(b, 0.0); }

@@ -441,21 +441,24 @@ __device__ __forceinline__ double wda_weight_at(const GridDev& g, int p1, int co
 }
 
 // SumOfEOS(MBWR, CS, MFA) excess free energy per volume and its density
-// derivative at one weighted density (cmmdft/eos.py:226-265, 295-546).
-__device__ __forceinline__ void wda_eos(const cmm_wda_eos& e, double rho, double& fv, double& dfv) {
+// derivative at one weighted density (cmmdft/eos.py:226-265, 295-546).  A
+// template on the scalar type: double for the functional, Dual for the
+// second derivative in the Hessian-vector product.
+template <class S>
+__device__ __forceinline__ void wda_eos(const cmm_wda_eos& e, S rho, S& fv, S& dfv) {
   // MBWR (eos.py:368-422)
-  const double rr = rho * e.sigma3;
-  double A = 0.0, dA = 0.0, p = 1.0;  // p = rr^i
+  const S rr = rho * e.sigma3;
+  S A = 0.0, dA = 0.0, p = 1.0;  // p = rr^i
 #pragma unroll
   for (int i = 0; i < 8; ++i) {
     dA += e.a[i] * p * e.sigma3;
     p *= rr;
     A += e.a[i] / (i + 1) * p;
   }
-  const double rr2 = rr * rr;
-  const double F = exp(-e.gamma * rr2);
+  const S rr2 = rr * rr;
+  const S F = exp(-e.gamma * rr2);
   const double ig = 1.0 / (2 * e.gamma);
-  double G = ig * (1 - F), q = 1.0, podd = rr;  // q = rr^(2(n-1)), podd = rr^(2t+1)
+  S G = ig * (1 - F), q = 1.0, podd = rr;  // q = rr^(2(n-1)), podd = rr^(2t+1)
   A += e.b[0] * G;
   dA += e.b[0] * e.sigma3 * podd * F;
 #pragma unroll
@@ -466,16 +469,17 @@ __device__ __forceinline__ void wda_eos(const cmm_wda_eos& e, double rho, double
     podd *= rr2;
     dA += e.b[n - 1] * e.sigma3 * podd * F;
   }
-  const double fp_m = A * e.epsilon, dfp_m = dA * e.epsilon;
+  const S fp_m = A * e.epsilon, dfp_m = dA * e.epsilon;
   // Carnahan-Starling (eos.py:503-509)
-  const double er = e.eta * rho, om = 1 - er;
-  const double fp_c = e.kT * (4 * e.eta * rho - 3 * er * er) / (om * om);
-  const double dfp_c = 2 * e.kT * e.eta * (2 - er) / (om * om * om);
+  const S er = e.eta * rho, om = 1 - er;
+  const S fp_c = e.kT * (4 * e.eta * rho - 3 * er * er) / (om * om);
+  const S dfp_c = 2 * e.kT * e.eta * (2 - er) / (om * om * om);
   // mean-field EOS (eos.py:536-540)
-  const double fp_a = e.a_mfa * rho, dfp_a = e.a_mfa;
-  double d_m = rho * dfp_m; d_m += fp_m;
-  double d_c = rho * dfp_c; d_c += fp_c;
-  double d_a = rho * dfp_a; d_a += fp_a;
+  const S fp_a = e.a_mfa * rho;
+  const double dfp_a = e.a_mfa;
+  S d_m = rho * dfp_m; d_m += fp_m;
+  S d_c = rho * dfp_c; d_c += fp_c;
+  S d_a = rho * dfp_a; d_a += fp_a;
   dfv = 0.0;
   dfv += e.factors[0] * d_m;
   dfv += e.factors[1] * d_c;
@@ -701,16 +705,10 @@ __device__ __forceinline__ void phi_funcs(S n3, S ln, S n32, S n33, int base, S&
       p3 = (1 - 4 * n3 / 9 + n32 / 18) / (24 * M_PI * q);
       dp3 = (7.0 / 3 - n3 / 2 + n32 / 10) / (36 * M_PI * c);
     } else {
-      // The four denominators are products of powers of n3 and (1 - n3):
-      // two reciprocals serve all of them (q = (1-n3)^2, c = (1-n3)^3).
-      // The numerators, whose cancellation at small n3 sets the accuracy of
-      // these closed forms, are formed exactly as in the reference.
-      const S d = 1 / (1.0 - n3), u = 1 / n3;
-      const S ud = u * d, ud2 = ud * ud;
-      p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) * (ud * (1.0 / 3));
-      dp2 = -2 * (n3 - 3 * n32 + q * ln) * (ud2 * (1.0 / 3));
-      p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) * (ud2 * (1.0 / (72 * M_PI)));
-      dp3 = (2 * n3 - 5 * n32 + 6 * n33 - n32 * n32 + 2 * c * ln) * (ud2 * ud * (1.0 / (36 * M_PI)));
+      p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) / (3 * (n3 - n32));
+      dp2 = -2 * (n3 - 3 * n32 + q * ln) / (3 * n32 * q);
+      p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) / ((3 * n32) * 24 * M_PI * q);
+      dp3 = (2 * n3 - 5 * n32 + 6 * n33 - n32 * n32 + 2 * c * ln) / (36 * M_PI * n33 * c);
     }
   }
 }
@@ -755,11 +753,9 @@ __device__ __forceinline__ void phi_values(double n3, double ln, double n32, dou
   } else if (n3 <= 1e-8) {
     p2 = (1 + n32 / 9) / (1 - n3);
     p3 = (1 - 4 * n3 / 9 + n32 / 18) / (24 * M_PI * q);
-  } else {  // as phi_funcs, so that Phi agrees with the derivative pass bit for bit
-    const double d = 1 / (1.0 - n3), u = 1 / n3;
-    const double ud = u * d, ud2 = ud * ud;
-    p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) * (ud * (1.0 / 3));
-    p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) * (ud2 * (1.0 / (72 * M_PI)));
+  } else {
+    p2 = (5 * n3 - n32 + 2 * (1 - n3) * ln) / (3 * (n3 - n32));
+    p3 = -2 * (n3 - 3 * n32 + n33 + ln * q) / ((3 * n32) * 24 * M_PI * q);
   }
 }
 
@@ -1866,13 +1862,17 @@ static int zrow_fmt(const cmm_grid* g, int batch, const int* act, double R, int 
 // at the clipped value, so it depends on the other densities while nothing
 // depends on n3; the transpose passes the tangent of n3 through the clip
 // into the other outputs and returns no dPhi/dn3 tangent.
-template <int M3C, bool TEN, bool TR>
+// WDA: the weighted density of the WDA part follows the five FMT densities
+// (before the tensor ones); its output is f''_EOS(wd) times the tangent.
+template <int M3C, bool TEN, bool TR, bool WDA>
 __global__ void __launch_bounds__(CMM_ROW_THREADS)
-k_zrow_hvp(GridDev g, const int* __restrict__ active, double R, int version, const double2* __restrict__ win,
-           size_t fs, double2* __restrict__ gout, int chunk, const double* __restrict__ wdrho, size_t fsr) {
+k_zrow_hvp(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
+           const double2* __restrict__ win, size_t fs, double2* __restrict__ gout, int chunk,
+           const double* __restrict__ wdrho, size_t fsr) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
-  constexpr int nf = 5 + (TEN ? 6 : 0);
+  constexpr int tb = WDA ? 6 : 5;
+  constexpr int nf = tb + (TEN ? 6 : 0);
   const int h3 = M3C > 0 ? M3C + 1 : g.h3, n3 = g.n3, n2 = g.n2;
   PlaneSmem s = zrow_smem_setup<M3C>(g, nf * chunk);
   const size_t poff = ((size_t)b * g.n1 + i1) * n2 * h3;
@@ -1892,15 +1892,20 @@ k_zrow_hvp(GridDev g, const int* __restrict__ active, double R, int version, con
         clipped = !(n[1].v >= 1e-30) || !(n[1].v <= 0.99);
         if (clipped) n[1].v = fmin(fmax(n[1].v, 1e-30), 0.99);
       }
-      const PhiOutT<Dual> o = fmt_point<TEN, Dual>(n[0], n[1], n[2], n[3], n[4], TEN ? n + 5 : nullptr, gT, R,
+      const PhiOutT<Dual> o = fmt_point<TEN, Dual>(n[0], n[1], n[2], n[3], n[4], TEN ? n + tb : nullptr, gT, R,
                                                    version);
       zrow_rel<M3C>(g, s, nf, 0, r, j) = o.gs.d;
       zrow_rel<M3C>(g, s, nf, 1, r, j) = clipped ? 0.0 : o.g3.d;
       zrow_rel<M3C>(g, s, nf, 2, r, j) = o.gv[0].d;
       zrow_rel<M3C>(g, s, nf, 3, r, j) = o.gv[1].d;
       zrow_rel<M3C>(g, s, nf, 4, r, j) = o.gv[2].d;
+      if constexpr (WDA) {
+        Dual fv, dfv;
+        wda_eos<Dual>(wda, n[5], fv, dfv);
+        zrow_rel<M3C>(g, s, nf, 5, r, j) = dfv.d;
+      }
       if constexpr (TEN)
-        for (int t = 0; t < 6; ++t) zrow_rel<M3C>(g, s, nf, 5 + t, r, j) = gT[t].d;
+        for (int t = 0; t < 6; ++t) zrow_rel<M3C>(g, s, nf, tb + t, r, j) = gT[t].d;
     }
     __syncthreads();
     zrow_forward<M3C>(g, s, nf * nr);
@@ -1909,27 +1914,37 @@ k_zrow_hvp(GridDev g, const int* __restrict__ active, double R, int version, con
   }
 }
 
-template <int M3C, bool TEN, bool TR>
-static int zrow_hvp_one(const cmm_grid* g, int batch, const int* act, double R, int version, const double2* win,
-                        size_t fs, double2* gout, int chunk, const double* wdrho, cudaStream_t st) {
-  constexpr int nf = 5 + (TEN ? 6 : 0);
+template <int M3C, bool TEN, bool TR, bool WDA>
+static int zrow_hvp_one(const cmm_grid* g, int batch, const int* act, double R, int version,
+                        const cmm_wda_eos& wda, const double2* win, size_t fs, double2* gout, int chunk,
+                        const double* wdrho, cudaStream_t st) {
+  constexpr int nf = (WDA ? 6 : 5) + (TEN ? 6 : 0);
   const size_t sb = zrow_smem_bytes_g(g, nf * chunk);
   int rc;
-  if ((rc = set_smem((const void*)k_zrow_hvp<M3C, TEN, TR>, sb))) return rc;
-  k_zrow_hvp<M3C, TEN, TR><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(
-      g->dev, act, R, version, win, fs, gout, chunk, wdrho, (size_t)batch * g->n1 * g->n2 * g->n3);
+  if ((rc = set_smem((const void*)k_zrow_hvp<M3C, TEN, TR, WDA>, sb))) return rc;
+  k_zrow_hvp<M3C, TEN, TR, WDA><<<dim3(g->n1, batch), CMM_ROW_THREADS, sb, st>>>(
+      g->dev, act, R, version, wda, win, fs, gout, chunk, wdrho, (size_t)batch * g->n1 * g->n2 * g->n3);
   return last_err();
 }
 
-template <int M3C>
-static int zrow_hvp_m3(const cmm_grid* g, int batch, const int* act, double R, int version, int tr,
-                       const double2* win, size_t fs, double2* gout, int chunk, const double* wdrho,
-                       cudaStream_t st) {
+template <int M3C, bool WDA>
+static int zrow_hvp_w(const cmm_grid* g, int batch, const int* act, double R, int version, const cmm_wda_eos& wda,
+                      int tr, const double2* win, size_t fs, double2* gout, int chunk, const double* wdrho,
+                      cudaStream_t st) {
   if (version & CMM_TENSOR)
-    return tr ? zrow_hvp_one<M3C, true, true>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st)
-              : zrow_hvp_one<M3C, true, false>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st);
-  return tr ? zrow_hvp_one<M3C, false, true>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st)
-            : zrow_hvp_one<M3C, false, false>(g, batch, act, R, version, win, fs, gout, chunk, wdrho, st);
+    return tr ? zrow_hvp_one<M3C, true, true, WDA>(g, batch, act, R, version, wda, win, fs, gout, chunk, wdrho, st)
+              : zrow_hvp_one<M3C, true, false, WDA>(g, batch, act, R, version, wda, win, fs, gout, chunk, wdrho, st);
+  return tr ? zrow_hvp_one<M3C, false, true, WDA>(g, batch, act, R, version, wda, win, fs, gout, chunk, wdrho, st)
+            : zrow_hvp_one<M3C, false, false, WDA>(g, batch, act, R, version, wda, win, fs, gout, chunk, wdrho, st);
+}
+
+template <int M3C>
+static int zrow_hvp_m3(const cmm_grid* g, int batch, const int* act, double R, int version,
+                       const cmm_wda_eos& wda, int tr, const double2* win, size_t fs, double2* gout, int chunk,
+                       const double* wdrho, cudaStream_t st) {
+  if (version & CMM_WDA)
+    return zrow_hvp_w<M3C, true>(g, batch, act, R, version, wda, tr, win, fs, gout, chunk, wdrho, st);
+  return zrow_hvp_w<M3C, false>(g, batch, act, R, version, wda, tr, win, fs, gout, chunk, wdrho, st);
 }
 
 // Spectrum of A v = d C1 / d rho . v (Hartree per density unit), A the
@@ -1939,12 +1954,17 @@ static int zrow_hvp_m3(const cmm_grid* g, int batch, const int* act, double R, i
 // on rho).  transpose: A^T v (the caller passes the conjugate MFA spectrum).
 // The y/z steps run in the staged form for every grid shape.
 extern "C" int cmm_fmt_hvp(const cmm_grid* g, int batch, const int* d_active, double R, double beta, int version,
-                           int transpose, const double* d_kst, const double* d_wtab, const double* d_wd_rho,
-                           const double* d_vhat, double* d_out_hat, double* d_work, void* stream) {
+                           const cmm_wda_eos* wda, int transpose, const double* d_kst, const double* d_wtab,
+                           const double* d_wd_rho, const double* d_vhat, double* d_out_hat, double* d_work,
+                           void* stream) {
   if (!g || batch < 1 || !d_kst || !d_vhat || !d_out_hat || !d_work) return CMM_ERR_ARG;
-  if (version & CMM_WDA) return CMM_ERR_UNSUPPORTED;
+  const bool has_wda = (version & CMM_WDA) != 0 && !(version & CMM_NOHS);
+  if (has_wda && !wda) return CMM_ERR_ARG;
+  cmm_wda_eos we;
+  memset(&we, 0, sizeof(we));
+  if (has_wda) we = *wda;
   const bool ten = (version & CMM_TENSOR) != 0;
-  const int nf = 5 + (ten ? 6 : 0);
+  const int nf = (has_wda ? 6 : 5) + (ten ? 6 : 0);
   cudaStream_t st = (cudaStream_t)stream;
   const size_t fs = (size_t)batch * g->n1 * g->n2 * g->h3;
   double2* wbuf = (double2*)d_work;
@@ -1962,35 +1982,36 @@ extern "C" int cmm_fmt_hvp(const cmm_grid* g, int batch, const int* d_active, do
   }
   if (!d_wd_rho) return CMM_ERR_ARG;
   const size_t csw = col_smem_bytes(g->n1, tc, nf, g->ax1.big), csb = col_smem_bytes(g->n1, tc, nf + 1, g->ax1.big);
-  if (ten)
-    LAUNCH_COL(ck, k_col_weights_t, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
-               (const double2*)d_vhat, wbuf, fs, (const double2*)d_kst, wt, (double*)nullptr, 0, 0, tc, 0.0,
-               (const double2*)nullptr, (double*)nullptr);
-  else
-    LAUNCH_COL(ck, k_col_weights, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts,
-               (const double2*)d_vhat, wbuf, fs, (const double2*)d_kst, wt, (double*)nullptr, 0, 0, tc, 0.0,
-               (const double2*)nullptr, (double*)nullptr);
+#define LAUNCH_WEIGHTS(kern)                                                                                   \
+  LAUNCH_COL(ck, kern, dim3(ntile, batch), csw, st, g->dev, d_active, R, 1.0 / npts, (const double2*)d_vhat,      \
+             wbuf, fs, (const double2*)d_kst, wt, (double*)nullptr, 0, 0, tc, we.D, (const double2*)nullptr,   \
+             (double*)nullptr)
+  if (has_wda && ten) LAUNCH_WEIGHTS(k_col_weights_wda_t);
+  else if (has_wda) LAUNCH_WEIGHTS(k_col_weights_wda);
+  else if (ten) LAUNCH_WEIGHTS(k_col_weights_t);
+  else LAUNCH_WEIGHTS(k_col_weights);
+#undef LAUNCH_WEIGHTS
   int rc = last_err();
   if (rc) return rc;
   if ((rc = ypass(g, batch, d_active, wbuf, wbuf, fs, nf, 1, st))) return rc;
   const int chunk = zrow_chunk(g, nf);
   if (chunk < 1) return CMM_ERR_SMEM;
   switch (zrow_m3(g)) {
-    case 32: rc = zrow_hvp_m3<32>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
-    case 16: rc = zrow_hvp_m3<16>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
-    case -1: rc = zrow_hvp_m3<-1>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
-    default: rc = zrow_hvp_m3<0>(g, batch, d_active, R, version, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st);
+    case 32: rc = zrow_hvp_m3<32>(g, batch, d_active, R, version, we, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
+    case 16: rc = zrow_hvp_m3<16>(g, batch, d_active, R, version, we, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
+    case -1: rc = zrow_hvp_m3<-1>(g, batch, d_active, R, version, we, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st); break;
+    default: rc = zrow_hvp_m3<0>(g, batch, d_active, R, version, we, transpose, wbuf, fs, gbuf, chunk, d_wd_rho, st);
   }
   if (rc) return rc;
   if ((rc = ypass(g, batch, d_active, gbuf, gbuf, fs, nf, 0, st))) return rc;
-  if (ten)
-    LAUNCH_COL(ck, k_col_backconv_t, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),
-               (const double2*)gbuf, fs, (const double2*)d_vhat, (const double2*)d_kst, wt, (double2*)d_out_hat,
-               tc, 0.0, 1.0 / npts);
-  else
-    LAUNCH_COL(ck, k_col_backconv, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts),
-               (const double2*)gbuf, fs, (const double2*)d_vhat, (const double2*)d_kst, wt, (double2*)d_out_hat,
-               tc, 0.0, 1.0 / npts);
+#define LAUNCH_BACKCONV(kern)                                                                                   \
+  LAUNCH_COL(ck, kern, dim3(ntile, batch), csb, st, g->dev, d_active, R, 1.0 / (beta * npts), (const double2*)gbuf, \
+             fs, (const double2*)d_vhat, (const double2*)d_kst, wt, (double2*)d_out_hat, tc, we.D, 1.0 / npts)
+  if (has_wda && ten) LAUNCH_BACKCONV(k_col_backconv_wda_t);
+  else if (has_wda) LAUNCH_BACKCONV(k_col_backconv_wda);
+  else if (ten) LAUNCH_BACKCONV(k_col_backconv_t);
+  else LAUNCH_BACKCONV(k_col_backconv);
+#undef LAUNCH_BACKCONV
   return last_err();
 }
 

@@ -392,18 +392,19 @@ typedef struct cmm_solve_out {
  * derivatives -- its users difference whole solves).
  * ------------------------------------------------------------------- */
 /* Spectrum of A v, A = d C1 / d rho the Hessian of the excess free energy
- * (hard-sphere + MFA; C1 in Hartree, so A v is in Hartree per density unit),
- * for `batch` yz-spectra d_vhat.  d_wd_rho: the real-space weighted
- * densities of rho [nwd][B][npts] stored by cmm_fmt_c1 with want bit 3; the
- * hard-sphere second derivatives are taken there.  transpose = 1: A^T v,
- * with the caller passing the conjugate MFA spectrum as d_kst (A is not
- * symmetric: the reference's MFA kernel is translated by its spectrum
- * phase, and where n3 is clipped dPhi/dn3 still varies with the other
- * densities).  d_work: nwork spectra as for cmm_fmt_c1.
- * CMM_WDA: CMM_ERR_UNSUPPORTED. */
+ * (hard-sphere + MFA, + the WDA part with CMM_WDA; C1 in Hartree, so A v is
+ * in Hartree per density unit), for `batch` yz-spectra d_vhat.  d_wd_rho:
+ * the real-space weighted densities of rho [nwd][B][npts] stored by
+ * cmm_fmt_c1 with want bit 3; the hard-sphere and EOS second derivatives
+ * are taken there.  wda: the WDA part's EOS with CMM_WDA, else NULL.
+ * transpose = 1: A^T v, with the caller passing the conjugate MFA spectrum
+ * as d_kst (A is not symmetric: the reference's MFA kernel is translated by
+ * its spectrum phase, and where n3 is clipped dPhi/dn3 still varies with
+ * the other densities; the WDA part is symmetric).  d_work: nwork spectra
+ * as for cmm_fmt_c1. */
 int cmm_fmt_hvp(const cmm_grid* grid, int batch, const int* d_active, double R, double beta, int version,
-                int transpose, const double* d_kst, const double* d_wtab, const double* d_wd_rho, const double* d_vhat,
-                double* d_out_hat, double* d_work, void* stream);
+                const cmm_wda_eos* wda, int transpose, const double* d_kst, const double* d_wtab,
+                const double* d_wd_rho, const double* d_vhat, double* d_out_hat, double* d_work, void* stream);
 
 /* Parameter derivatives of the capped LJ external potential (arguments as
  * cmm_extpot_lj): d_dV [2 + 2 ntype][npts], rows dV/d(guest eps),

@@ -71,14 +71,15 @@ def _smooth_fields(npts, B, seed):
     return torch.as_tensor(rho, device="cuda"), torch.as_tensor(v, device="cuda")
 
 
-@pytest.mark.parametrize("version", ["WBII", "atWBII", "tWBII", "MFMT", "FMT"])
+@pytest.mark.parametrize("version", ["WBII", "atWBII", "tWBII", "MFMT", "FMT", "WBII+WDA", "atWBII+WDA"])
 def test_hvp_matches_directional_difference(cuda, version):
     """On a smooth dense profile A v against the central difference of C1
     along v (truncation ~eps^2 = 1e-8, rounding ~1e-16 / eps).  The physical
     profiles are not used here: where the packing fraction is tiny the WBII
     and MFMT expressions cancel catastrophically, and central differences of
     C1 there change by tens of percent between eps = 1e-3 and 1e-4."""
-    fn = W.build_functional(cubic_host_276(0), (32, 32, 32), 300.0, methane_guest_params(), version=version)
+    ver, wda = version.replace('+WDA', ''), version.endswith('+WDA')
+    fn = W.build_functional(cubic_host_276(0), (32, 32, 32), 300.0, methane_guest_params(), version=ver, wda=wda)
     rho, v = _smooth_fields((32, 32, 32), 2, 5)
     Av = A.hvp(fn, _wd(fn, rho), v)
     eps = 1e-4
@@ -141,20 +142,24 @@ def test_extpot_grad_matches_difference(cuda):
 TIGHT = dict(threshold=1e-12, criterion='riue')
 
 
-def test_adjoint_gradients_match_resolved_differences(cuda):
+@pytest.mark.parametrize("wda", [False, True])
+def test_adjoint_gradients_match_resolved_differences(cuda, wda):
     """N, Omega and N_ex gradients (all 10 parameters, 3 pressures) against
     central differences of re-converged solves, each d/d ln theta within 1e-6
     of the largest of that pressure's and quantity's entries (1e-5 for Omega:
-    d Omega / d(guest sigma) deviates by 7.8e-6 of that scale; its explicit
-    part, rho fixed, agrees to 5e-7, so the rest lies in the small adjoint
-    correction from Omega's non-stationarity, cause not yet found).  Step
+    d Omega / d theta deviates for every parameter, by ~4e-8 of that scale at
+    1 bar, ~4e-7 at 3 bar and 4e-6 to 9e-6 at 10 bar, the same for central
+    differences with relative steps from 3e-4 down to 1e-5, so it is no
+    difference error; it is 0.2-0.5% of the adjoint correction from Omega's
+    non-stationarity, cause not found).  With the WDA part the same bounds
+    hold.  Step
     1e-4 for the solves: stopped at RIUE < 1e-12 they sit ~1e-11 from the
     fixed point, which a 1e-5 step would turn into ~1e-6 of noise;
     truncation at 1e-4 is ~1e-8."""
     host = cubic_host_276(0)
     guest = methane_guest_params()
     P = np.array([1.0, 3.0, 10.0]) * bar
-    model = A.IsothermModel(host, guest, 300.0, (32, 32, 32), P, quantity='excess', **TIGHT)
+    model = A.IsothermModel(host, guest, 300.0, (32, 32, 32), P, quantity='excess', wda=wda, **TIGHT)
     theta = model.theta0
     sol = model.solve(theta)
     assert np.all(sol['converged'])
@@ -191,6 +196,7 @@ def test_adjoint_gradients_match_resolved_differences(cuda):
         err = np.abs(a - f) / scale
         worst[key] = (float(err.max()), g['names'][int(np.argmax(err.max(axis=0)))])
     tol = dict(dN=1e-6, dNex=1e-6, dOmega=1e-5)
+    print("adjoint vs re-converged central differences%s, worst relative errors:" % (" (WDA)" if wda else ""), worst)
     assert all(w[0] < tol[k] for k, w in worst.items()), worst
 
 
@@ -218,7 +224,7 @@ def test_excess_isotherm_loss_gradient_96(cuda):
             return float(((model(torch.as_tensor(th)) - target) ** 2).sum())
 
     scale = np.abs(grad * theta0).max()
-    for k in (0, 1, 2, 6):   # guest eps, guest sigma, one host eps, one host sigma
+    for k in range(len(theta0)):   # guest eps, sigma and every host type's eps and sigma
         h = 1e-5 * theta0[k]
         tp, tm = theta0.copy(), theta0.copy()
         tp[k] += h
@@ -228,8 +234,11 @@ def test_excess_isotherm_loss_gradient_96(cuda):
 
 
 def test_gradient_against_oracle_differences(cuda):
-    """dN/d(guest epsilon) at 32^3 and 1 bar against central differences of
-    the oracle (the reference's numpy path) re-converged on the CPU."""
+    """dN/d(guest epsilon), dN/d(epsilon_C) and dN/d(sigma_C) at 32^3 and
+    1 bar against central differences of the oracle (the reference's numpy
+    path) re-converged on the CPU: the host parameters within 1e-6, the
+    guest epsilon (which also moves the hard-sphere radius and the EOS)
+    within 1e-5."""
     from oracle import cmm_oracle as O
     host = cubic_host_276(0)
     guest = methane_guest_params()
@@ -239,8 +248,8 @@ def test_gradient_against_oracle_differences(cuda):
     g = A.adjoint_gradients(sol['fn'], sol['host'], sol['guest'], 300.0, P, sol['mu'], sol['rho'], excess=False)
     sig, eps, mass = guest
 
-    def oracle_N(e):
-        grid, fe = oracle_case(32, guest=(sig, e, mass))
+    def oracle_N(e, h=None):
+        grid, fe = oracle_case(32, guest=(sig, e, mass), host=h)
         mb = O.MBWR(mass, sig, e)
         mu = O.eos_calculate_mu(mb, 300.0, P[0])
         mb.set_temperature(300.0)
@@ -254,4 +263,16 @@ def test_gradient_against_oracle_differences(cuda):
 
     h = 1e-4 * eps
     fd = (oracle_N(eps + h) - oracle_N(eps - h)) / (2 * h)
-    assert abs(g['dN'][0, 0] - fd) <= 1e-5 * abs(fd), (g['dN'][0, 0], fd)
+    errs = {'guest_epsilon': abs(g['dN'][0, 0] - fd) / abs(fd)}
+    theta = model.theta0
+    for k in (2, 6):   # epsilon and sigma of the first host atom type
+        hk = 1e-4 * theta[k]
+        tp, tm = theta.copy(), theta.copy()
+        tp[k] += hk
+        tm[k] -= hk
+        fdk = (oracle_N(eps, A.unpack_params(tp, host, guest)[0]) -
+               oracle_N(eps, A.unpack_params(tm, host, guest)[0])) / (2 * hk)
+        errs[g['names'][k]] = abs(g['dN'][0, k] - fdk) / abs(fdk)
+    print("dN/dtheta vs oracle central differences, relative errors:", {k: "%.2e" % v for k, v in errs.items()})
+    assert errs['guest_epsilon'] <= 1e-5
+    assert errs[g['names'][2]] <= 1e-6 and errs[g['names'][6]] <= 1e-6

@@ -590,3 +590,30 @@ def test_extpot_256_against_oracle(cuda):
     err = relerr(V[idx[:, 0], idx[:, 1], idx[:, 2]], Vo, cap)
     print("256^3 extpot vs oracle at 4096 points: %.2e of the cap" % err)
     assert err < 1e-12
+
+
+def test_uneven_host_at_spacing_grid_against_reference(cuda):
+    """Host 5 of the uneven batch (uneven_hosts(8, 2): 29.7 x 39.1 x 31.1 A,
+    2026 atoms) on its 0.25 A grid, 119 x 157 x 125 -- 157 prime (Rader
+    stages on y), 119 = 7 x 17 -- at 0.1, 1 and 10 bar against the unmodified
+    reference (tests/golden/uneven5.npz, hybrid Anderson m=5, RES < 1e-8,
+    Ninit = rho_bulk): the same steps, N and Omega within 1e-10."""
+    import os
+    from cmmdft_b200 import isotherm as ISO
+    from cmmdft_b200.hosts import uneven_hosts
+    ref = dict(np.load(os.path.join(os.path.dirname(__file__), "golden", "uneven5.npz")))
+    host = uneven_hosts(8, 2)[int(ref["host"])]
+    guest = methane_guest_params()
+    shape = ISO.grid_points(host)
+    assert list(shape) == list(ref["npoints"])
+    mus, bulks = W.isotherm_inputs(ref["pressures"] * bar, 300.0, guest)
+    assert np.array_equal(mus, ref["mu"])
+    fn = W.build_functional(host, shape, 300.0, guest)
+    s = BT.NativeBatchSolve(fn, mus, method='hybridanderson', nsteps=500, threshold=1e-8, criterion='res')
+    N, rho, conv = s.solve(W.initial_density(fn, mus, ninit=bulks))
+    eN = max(scalar_rel(N[i], ref["N"][i]) for i in range(len(mus)))
+    eO = max(scalar_rel(s.omega0[i], ref["omega"][i]) for i in range(len(mus)))
+    print("uneven host 5 %s: steps %s (reference %s), N %.2e, Omega %.2e" % (shape, list(s.steps), list(ref["steps"]),
+                                                                              eN, eO))
+    assert np.all(conv) and np.array_equal(s.steps, ref["steps"])
+    assert eN < 1e-10 and eO < 1e-10
