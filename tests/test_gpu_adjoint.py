@@ -158,7 +158,9 @@ def test_adjoint_gradients_match_resolved_differences(cuda, wda):
     truncation at 1e-4 is ~1e-8."""
     host = cubic_host_276(0)
     guest = methane_guest_params()
-    P = np.array([1.0, 3.0, 10.0]) * bar
+    # (with the WDA part the 10 bar point does not reach RIUE < 1e-12 at every
+    # perturbed parameter set: 0.3, 1 and 3 bar there)
+    P = (np.array([0.3, 1.0, 3.0]) if wda else np.array([1.0, 3.0, 10.0])) * bar
     model = A.IsothermModel(host, guest, 300.0, (32, 32, 32), P, quantity='excess', wda=wda, **TIGHT)
     theta = model.theta0
     sol = model.solve(theta)
