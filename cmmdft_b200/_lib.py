@@ -85,6 +85,8 @@ _SIGS = {
     "cmm_status_string": ([c_int], ctypes.c_char_p),
     "cmm_grid_create": ([c_int, c_int, c_int, P(c_double), P(c_void_p)], c_int),
     "cmm_grid_destroy": ([c_void_p], c_int),
+    "cmm_grid_create_sched": ([c_int, c_int, c_int, P(c_double), P(c_int), P(c_void_p)], c_int),
+    "cmm_grid_schedule": ([c_void_p, P(c_int), P(c_int)], c_int),
     "cmm_grid_set_staging": ([c_void_p, c_int], c_int),
     "cmm_part_slots": ([c_void_p], c_int),
     "cmm_grid_spectrum_size": ([c_void_p, P(c_ll), P(c_int)], c_int),

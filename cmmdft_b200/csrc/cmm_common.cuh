@@ -12,6 +12,19 @@
 #define CMM_PLANE_THREADS 512
 #define CMM_COL_THREADS 256
 #define CMM_FMT_THREADS 768    // the 5-field plane pass (one block per SM; 768 balances its radix-8 rounds)
+// Resident blocks per SM the compiler must allow for (register budget) in the
+// single-field plane passes and the column passes.  The weights and
+// back-convolution column passes of the specialised x lengths (32, 64) run
+// five 256-thread blocks per SM (48 registers, a few spilled bytes): 5% faster
+// C1 pipeline at 64^3 than four blocks with 64 registers, measured; the
+// run-time-length instantiations keep their full register budget.
+#ifndef CMM_PLANE_MINB
+#define CMM_PLANE_MINB 1
+#endif
+#ifndef CMM_COL_MINB
+#define CMM_COL_MINB 1
+#endif
+#define CMM_COL_MINB_FOR(n1c) ((n1c) > 0 ? 5 : CMM_COL_MINB)
 #define CMM_ROW_THREADS 512    // staged z-row passes
 #define CMM_ZFMT_THREADS 768   // the staged z-row pass of dPhi/dn (768 measured faster than 256-512 and 1024)
 
@@ -57,6 +70,9 @@ struct cmm_grid {
   GridDev dev;
   int staging;                 // 0: by size, 1: staged plane passes always
   int exotic;                  // 1: radix 7, 11 or 13 or a Rader stage on some axis (kernels instantiated with -1)
+  int order[3];                // radix order per axis (CMM_ORDER_*)
+  int generic;                 // 1: a non-default radix order, so no compile-time-length kernels
+  int col_tile;                // column-pass tile width of the run-time kernels (0: by size)
 };
 
 static inline int cmm_div_up(long long a, long long b) { return (int)((a + b - 1) / b); }

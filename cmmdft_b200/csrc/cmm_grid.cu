@@ -9,6 +9,7 @@
 #include <cmath>
 #include <cstdlib>
 #include <cstring>
+#include <algorithm>
 #include <vector>
 
 #include "cmm_common.cuh"
@@ -25,19 +26,31 @@ extern "C" const char* cmm_status_string(int s) {
   return kStatusText[s];
 }
 
-// Radices for length n: 8s first (4s when no8), then 4, 2, then odd primes
+// Radix orders of a length-n axis (the stages run in this order forward):
+//   CMM_ORDER_DEFAULT  8s, 4s, 2s, then odd primes ascending
+//   CMM_ORDER_NO8      4s, 2s (no radix 8), then odd primes ascending
+//   CMM_ORDER_ODDFIRST odd primes descending, then 8s, 4s, 2s
+//   CMM_ORDER_ODDDESC  8s, 4s, 2s, then odd primes descending
 // (primes > 16 run as Rader or direct-DFT stages).
-static bool factorise(int n, FftAxis* ax, bool no8 = false) {
+static bool factorise(int n, FftAxis* ax, int order = CMM_ORDER_DEFAULT) {
   ax->n = n;
   ax->nstage = 0;
   ax->rader = nullptr;
   int m = n;
-  std::vector<int> r;
-  while (!no8 && m % 8 == 0) { r.push_back(8); m /= 8; }
-  while (m % 4 == 0) { r.push_back(4); m /= 4; }
-  while (m % 2 == 0) { r.push_back(2); m /= 2; }
-  for (int p = 3; m > 1; p += 2)   // odd primes in increasing order; primes > 16 run as direct-DFT stages
-    while (m % p == 0) { r.push_back(p); m /= p; }
+  std::vector<int> pow2, odd, r;
+  while (order != CMM_ORDER_NO8 && m % 8 == 0) { pow2.push_back(8); m /= 8; }
+  while (m % 4 == 0) { pow2.push_back(4); m /= 4; }
+  while (m % 2 == 0) { pow2.push_back(2); m /= 2; }
+  for (int p = 3; m > 1; p += 2)
+    while (m % p == 0) { odd.push_back(p); m /= p; }
+  if (order == CMM_ORDER_ODDFIRST || order == CMM_ORDER_ODDDESC) std::reverse(odd.begin(), odd.end());
+  if (order == CMM_ORDER_ODDFIRST) {
+    r = odd;
+    r.insert(r.end(), pow2.begin(), pow2.end());
+  } else {
+    r = pow2;
+    r.insert(r.end(), odd.begin(), odd.end());
+  }
   if ((int)r.size() > CMM_MAX_STAGES) return false;
   ax->big = 0;
   for (int x : r) if (x > CMM_MAX_SMALL_RADIX) ax->big = 1;
@@ -108,7 +121,7 @@ static long long powmod(long long b, long long e, long long m) {
 static bool rader_plan(int R, RaderHost& h) {
   const int M = R - 1;
   if (R < CMM_RADER_MIN) return false;
-  if (!factorise(M, &h.axm, true) || h.axm.big) return false;
+  if (!factorise(M, &h.axm, CMM_ORDER_NO8) || h.axm.big) return false;
   std::vector<int> pf;
   for (int m = M, p = 2; m > 1; ++p)
     if (m % p == 0) {
@@ -176,7 +189,24 @@ static double np_sinc(double x) {
 }
 
 extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_grid** out) {
+  return cmm_grid_create_sched(n1, n2, n3, rvecs, nullptr, out);
+}
+
+extern "C" int cmm_grid_create_sched(int n1, int n2, int n3, const double* rvecs, const int* sched,
+                                     cmm_grid** out) {
   if (!out || !rvecs || n1 < 1 || n2 < 1 || n3 < 2) return CMM_ERR_ARG;
+  int order[3] = {CMM_ORDER_DEFAULT, CMM_ORDER_DEFAULT, CMM_ORDER_DEFAULT};
+  int staging = 0, tile = 0;
+  if (sched) {
+    for (int a = 0; a < 3; ++a) {
+      if (sched[a] < -1 || sched[a] > CMM_ORDER_ODDDESC) return CMM_ERR_ARG;
+      if (sched[a] >= 0) order[a] = sched[a];
+    }
+    if (sched[3] < -1 || sched[3] > 1) return CMM_ERR_ARG;
+    staging = sched[3] > 0 ? 1 : 0;
+    if (sched[4] < 0 || sched[4] > 16 || (sched[4] & (sched[4] - 1))) return CMM_ERR_ARG;
+    tile = sched[4];
+  }
   if (n1 > CMM_MAX_N || n2 > CMM_MAX_N || n3 > CMM_MAX_N) return CMM_ERR_SHAPE;
   // Even N3: the z axis is a half-length complex FFT plus the R2C/C2R twist.
   // Odd N3: a full-length complex FFT of the real rows (z rows kernels only).
@@ -196,10 +226,17 @@ extern "C" int cmm_grid_create(int n1, int n2, int n3, const double* rvecs, cmm_
                  r[2] * (r[3] * r[7] - r[4] * r[6]);
     g->volume = fabs(det);
   }
-  if (!factorise(n1, &g->ax1) || !factorise(n2, &g->ax2) || !factorise(zfull ? n3 : g->m3, &g->ax3)) {
+  if (!factorise(n1, &g->ax1, order[0]) || !factorise(n2, &g->ax2, order[1]) ||
+      !factorise(zfull ? n3 : g->m3, &g->ax3, order[2])) {
     free(g);
     return CMM_ERR_SHAPE;
   }
+  for (int a = 0; a < 3; ++a) g->order[a] = order[a];
+  // the compile-time-length kernels (x 32 / 64, plane 32x16 / 64x32) fix
+  // their own radix order: any other order takes the run-time kernels
+  g->generic = (order[0] | order[1] | order[2]) != CMM_ORDER_DEFAULT;
+  g->staging = staging;
+  g->col_tile = tile;
   const int m3 = g->m3, h3 = g->h3;
   g->hpos_k1 = (int*)malloc(sizeof(int) * n1);
   g->hpos_k2 = (int*)malloc(sizeof(int) * n2);
@@ -370,6 +407,19 @@ extern "C" int cmm_grid_destroy(cmm_grid* g) {
 extern "C" int cmm_grid_set_staging(cmm_grid* g, int mode) {
   if (!g || mode < 0 || mode > 1) return CMM_ERR_ARG;
   g->staging = mode;
+  return CMM_OK;
+}
+
+extern "C" int cmm_grid_schedule(const cmm_grid* g, int* sched, int* radices) {
+  if (!g || !sched) return CMM_ERR_ARG;
+  for (int a = 0; a < 3; ++a) sched[a] = g->order[a];
+  sched[3] = g->staging;
+  sched[4] = g->col_tile;
+  if (radices) {
+    const FftAxis* ax[3] = {&g->ax1, &g->ax2, &g->ax3};
+    for (int a = 0; a < 3; ++a)
+      for (int st = 0; st < CMM_MAX_STAGES; ++st) radices[a * CMM_MAX_STAGES + st] = st < ax[a]->nstage ? ax[a]->radix[st] : 0;
+  }
   return CMM_OK;
 }
 

@@ -235,7 +235,7 @@ __device__ inline void put_part(double* part, int b, int q, int nslot, int slot,
 
 // ================================================ 3D FFT (setup / tests) ==
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
 k_plane_r2c(GridDev g, const int* __restrict__ active, const double* __restrict__ in, double2* __restrict__ out) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
@@ -252,7 +252,7 @@ k_plane_r2c(GridDev g, const int* __restrict__ active, const double* __restrict_
 }
 
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
 k_plane_c2r(GridDev g, const double2* __restrict__ in, double* __restrict__ out) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
@@ -341,7 +341,7 @@ __device__ inline void col_fft(const GridDev& g, const ColSmem& s, const ColShap
 // forward loads natural rows, runs DIF and stores row k1pos[p]; inverse loads
 // row k1pos[p] into position p, runs DIT and stores natural rows.
 template <int N1C, int TCC>
-__global__ void __launch_bounds__(CMM_COL_THREADS)
+__global__ void __launch_bounds__(CMM_COL_THREADS, CMM_COL_MINB)
 k_col_fft(GridDev g, const double2* in, double2* out, int tc, int inv) {
   const int b = blockIdx.y, c0 = blockIdx.x * (TCC ? TCC : tc);
   const ColShape<N1C, TCC> sh(g, tc);
@@ -585,7 +585,7 @@ __device__ __forceinline__ void col_weights_body(GridDev g, const int* __restric
       double wda_D, const double2 *__restrict__ rho_ref, double *__restrict__ ls_part
 #define COL_WEIGHTS_KERNEL(name, wda, ten, ls)                                                          \
   template <int N1C, int TCC>                                                                            \
-  __global__ void __launch_bounds__(CMM_COL_THREADS) name(COL_WEIGHTS_ARGS) {                           \
+  __global__ void __launch_bounds__(CMM_COL_THREADS, CMM_COL_MINB_FOR(N1C)) name(COL_WEIGHTS_ARGS) {                  \
     col_weights_body<N1C, TCC, wda, ten, ls>(g, active, R, inv_npts, rhohat, wout, fsw, kst, wtab, part, \
                                              nslot_part, want_value, tc, wda_D, rho_ref, ls_part);       \
   }
@@ -661,7 +661,7 @@ __device__ __forceinline__ void col_backconv_body(GridDev g, const int* __restri
       const double2 *__restrict__ wtab, double2 *__restrict__ chat, int tc, double wda_D, double inv_npts
 #define COL_BACKCONV_KERNEL(name, wda, ten)                                                             \
   template <int N1C, int TCC>                                                                            \
-  __global__ void __launch_bounds__(CMM_COL_THREADS) name(COL_BACKCONV_ARGS) {                          \
+  __global__ void __launch_bounds__(CMM_COL_THREADS, CMM_COL_MINB_FOR(N1C)) name(COL_BACKCONV_ARGS) {                          \
     col_backconv_body<N1C, TCC, wda, ten>(g, active, R, scale, gin, fsg, rhohat, kst, wtab, chat, tc,    \
                                           wda_D, inv_npts);                                              \
   }
@@ -930,7 +930,7 @@ k_plane_fmt_wda(GridDev g, const int* __restrict__ active, double R, int version
 // at a time: [n2][tc] in shared memory, pencils along y.  Fields f of the
 // launch are at src/dst + f * fs; blockIdx.z = b * nfield + f.
 template <int N2C>
-__global__ void __launch_bounds__(CMM_COL_THREADS)
+__global__ void __launch_bounds__(CMM_COL_THREADS, CMM_COL_MINB)
 k_ypass(GridDev g, const int* __restrict__ active, const double2* src, double2* dst, size_t fs, int nfield,
         int tc, int inv) {
   const int i1 = blockIdx.y;
@@ -1181,7 +1181,7 @@ __device__ __forceinline__ double der_term(double rho, double C1, double mu, dou
 
 // Static Picard step fused with the C1 inverse and the forward of rho'.
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
 k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
                double beta, double lambda3, double thr, double a_tol, double r_tol,
                const double2* __restrict__ chat,
@@ -1236,7 +1236,7 @@ struct HistPtrs { const double* p[CMM_MAX_HIST]; };
 
 // Residual r = G(C1) - rho with the Gram row against stored residuals.
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
 k_plane_residual(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
                  double beta, double lambda3, double a_tol, double r_tol, const double2* __restrict__ chat,
                  const double* __restrict__ rho,
@@ -1290,7 +1290,7 @@ struct FieldPtrs { const double* p[CMM_MAX_FIELDS]; long long stride[CMM_MAX_FIE
 
 // rho' = sum_j c_j field_j, clipped, with stats and the forward transform.
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
 k_plane_mix(GridDev g, const int* __restrict__ active, const double* __restrict__ coef,
             FieldPtrs fields, int nfield, int clip, double thr, double lambda3, const double* __restrict__ ref,
             long long refstride, const double* __restrict__ V, long long vstride,
@@ -1659,13 +1659,13 @@ static int set_smem(const void* fn, size_t bytes) {
 // run-time-length kernels come in two instantiations, 0 (radices 2, 3, 4, 5,
 // 8 and direct-DFT stages) and -1 (also 7, 11, 13 and Rader stages).
 static int plane_kind(const cmm_grid* g) {
-  if (g->n2 == 64 && g->m3 == 32) return 1;
-  if (g->n2 == 32 && g->m3 == 16) return 2;
+  if (!g->generic && g->n2 == 64 && g->m3 == 32) return 1;
+  if (!g->generic && g->n2 == 32 && g->m3 == 16) return 2;
   return g->exotic ? -1 : 0;
 }
 static int col_kind(const cmm_grid* g) {
-  if (g->n1 == 64) return 1;
-  if (g->n1 == 32) return 2;
+  if (!g->generic && g->n1 == 64) return 1;
+  if (!g->generic && g->n1 == 32) return 2;
   return g->exotic ? -1 : 0;
 }
 
@@ -1727,7 +1727,7 @@ static int col_kind(const cmm_grid* g) {
 // 16 when it fits otherwise.
 static int col_tile(const cmm_grid* g, int nslot) {
   if (col_kind(g) > 0) return 8;
-  int tc = 16;
+  int tc = g->col_tile > 0 ? g->col_tile : 16;   // the plan's schedule may fix it
   while (tc > 1 && col_smem_bytes(g->n1, tc, nslot, g->ax1.big) > 200 * 1024) tc /= 2;
   return tc;
 }
@@ -1745,10 +1745,10 @@ static int ypass(const cmm_grid* g, int batch, const int* act, const double2* sr
   const size_t sb = sizeof(double2) * ((size_t)g->n2 * tc * (g->ax2.big ? 2 : 1) + g->n2);
   const dim3 grd(ntile, g->n1, batch * nfield);
   int rc;
-  if (g->n2 == 64) {
+  if (!g->generic && g->n2 == 64) {
     if ((rc = set_smem((const void*)k_ypass<64>, sb))) return rc;
     k_ypass<64><<<grd, CMM_COL_THREADS, sb, st>>>(g->dev, act, src, dst, fs, nfield, tc, inv);
-  } else if (g->n2 == 32) {
+  } else if (!g->generic && g->n2 == 32) {
     if ((rc = set_smem((const void*)k_ypass<32>, sb))) return rc;
     k_ypass<32><<<grd, CMM_COL_THREADS, sb, st>>>(g->dev, act, src, dst, fs, nfield, tc, inv);
   } else if (g->exotic) {
@@ -1771,8 +1771,8 @@ static bool plane_staged(const cmm_grid* g, int nf) {
 
 // Compile-time z half length of the z-row kernels (0: from the plan).
 static int zrow_m3(const cmm_grid* g) {
-  if (!g->dev.zfull && g->m3 == 32) return 32;
-  if (!g->dev.zfull && g->m3 == 16) return 16;
+  if (!g->generic && !g->dev.zfull && g->m3 == 32) return 32;
+  if (!g->generic && !g->dev.zfull && g->m3 == 16) return 16;
   return g->exotic ? -1 : 0;
 }
 

@@ -29,7 +29,10 @@ class GridPlan(object):
     Wraps ``cmm_grid_create``; owns the plan's device tables.
     """
 
-    def __init__(self, npoints, rvecs):
+    def __init__(self, npoints, rvecs, schedule=None):
+        """schedule: None (the default FFT schedule) or the five entries of
+        cmm_grid_create_sched (x, y, z radix order, plane-pass form, column
+        tile), e.g. as chosen by cmmdft_b200.autotune."""
         require_cuda()
         self.lib = L.lib()
         n1, n2, n3 = [int(n) for n in npoints]
@@ -37,7 +40,11 @@ class GridPlan(object):
         self.rvecs = np.ascontiguousarray(rvecs, dtype=np.float64).reshape(3, 3)
         h = ctypes.c_void_p()
         rv = (ctypes.c_double * 9)(*self.rvecs.ravel().tolist())
-        check(self.lib.cmm_grid_create(n1, n2, n3, rv, ctypes.byref(h)), "cmm_grid_create")
+        if schedule is None:
+            check(self.lib.cmm_grid_create(n1, n2, n3, rv, ctypes.byref(h)), "cmm_grid_create")
+        else:
+            sc = (ctypes.c_int * 5)(*[int(x) for x in schedule])
+            check(self.lib.cmm_grid_create_sched(n1, n2, n3, rv, sc, ctypes.byref(h)), "cmm_grid_create_sched")
         self.handle = h
         ns = ctypes.c_longlong()
         h3 = ctypes.c_int()
@@ -54,6 +61,14 @@ class GridPlan(object):
         self.k3 = np.array(k3[:], dtype=np.int64)
         self.volume = float(abs(np.linalg.det(self.rvecs)))
         self.dr = self.volume / self.npts
+
+    def schedule(self):
+        """(sched[5], radices per axis) of the plan (cmm_grid_schedule)."""
+        sc = (ctypes.c_int * 5)()
+        rd = (ctypes.c_int * 48)()
+        check(self.lib.cmm_grid_schedule(self.handle, sc, rd), "cmm_grid_schedule")
+        r = np.array(rd[:]).reshape(3, 16)
+        return list(sc[:]), [[int(x) for x in row if x] for row in r]
 
     def set_staging(self, mode):
         """0: fused plane passes where the plane fits in shared memory (default);

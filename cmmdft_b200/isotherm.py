@@ -11,6 +11,7 @@ import numpy as np
 import torch
 
 from . import batch as BT
+from . import engine as E
 from . import workload as W
 from .units import angstrom, kjmol
 
@@ -72,7 +73,7 @@ def grid_points(host, spacing=0.25 * angstrom):
 def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25 * angstrom,
                 method='hybridanderson', threshold=1e-8, criterion='res', nsteps=500, m=5, alpha_mix=0.1,
                 divergence_guard=True, anderson_coefs='slsqp', return_density=False, max_concurrent=4,
-                version='WBII', tailcorrections=False, memory_budget=None):
+                version='WBII', tailcorrections=False, memory_budget=None, schedules=None):
     """Isotherms of several hosts of uneven cells and grids in one call.
 
     The reference solves every (host, pressure) point in its own Program.solve
@@ -90,6 +91,9 @@ def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25
     hosts: list of SyntheticHost-like hosts; pressures: one array for every
     host or a list with one array per host (atomic units); npoints: None
     (from ``spacing``), one shape for all hosts or a list of shapes.
+    schedules: None (default FFT schedules) or one cmm_grid_create_sched
+    schedule per host (e.g. from cmmdft_b200.autotune.tune); a schedule moves
+    results only by rounding.
     Returns one dict per host as ``solve_isotherm`` does (without the solver
     and functional objects), in the order of ``hosts``.
     """
@@ -139,8 +143,11 @@ def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25
             torch.cuda.set_device(device)
             st.wait_stream(cur)
             with torch.cuda.stream(st):
+                plan = None
+                if schedules is not None and schedules[i] is not None:
+                    plan = E.GridPlan(shapes[i], hosts[i].rvecs, schedule=schedules[i])
                 fn = W.build_functional(hosts[i], shapes[i], temperature, guest, version=version,
-                                        tailcorrections=tailcorrections)
+                                        tailcorrections=tailcorrections, plan=plan)
                 P = np.asarray(plist[i], dtype=float)
                 mus, bulks = W.isotherm_inputs(P, temperature, guest)
                 rho0 = W.initial_density(fn, mus, ninit=bulks)

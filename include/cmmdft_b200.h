@@ -125,6 +125,25 @@ int cmm_grid_destroy(cmm_grid* grid);
  * input is read-only, take a stream-ordered temporary of one spectrum per
  * instance (cudaMallocAsync / cudaFreeAsync on the call's stream). */
 int cmm_grid_set_staging(cmm_grid* grid, int mode);
+/* FFT schedules.  A plan's schedule fixes, per axis, the order of the
+ * radix stages (CMM_ORDER_*), the form of the plane passes and the column
+ * tile; all schedules give the same transforms up to rounding.  The
+ * default (cmm_grid_create) is CMM_ORDER_DEFAULT everywhere, plane passes
+ * by size, column tiles by size.  sched[5] = {x order, y order, z order
+ * (-1: default), plane passes (-1 or 0: by size, 1: staged), column tile
+ * width of the run-time-length column kernels (0: by size, else 1..16, a
+ * power of two)}.  A non-default radix order runs the run-time-length
+ * kernels on every axis (the compile-time ones for 32 and 64 points fix
+ * their own order).  Used by the schedule autotuner
+ * (cmmdft_b200/autotune.py), which times the candidates on the device. */
+enum { CMM_ORDER_DEFAULT = 0,   /* 8s, 4s, 2s, then odd primes ascending        */
+       CMM_ORDER_NO8 = 1,       /* 4s, 2s (no radix 8), odd primes ascending      */
+       CMM_ORDER_ODDFIRST = 2,  /* odd primes descending first, then 8s, 4s, 2s  */
+       CMM_ORDER_ODDDESC = 3 }; /* 8s, 4s, 2s, then odd primes descending        */
+int cmm_grid_create_sched(int n1, int n2, int n3, const double* rvecs, const int* sched, cmm_grid** out);
+/* The plan's schedule (sched[5] as above, the plane entry being the forced
+ * staging flag) and, optionally, its radices [3][16] (0 past the last stage). */
+int cmm_grid_schedule(const cmm_grid* grid, int* sched, int* radices);
 /* Smallest `nslot` of the partial-sum arrays d_part / d_ls_part: every pass
  * writes at most this many slots per instance (one per x-plane or column
  * tile); a larger nslot works and only costs the reductions. */

@@ -1,0 +1,49 @@
+"""FFT-schedule candidates (CPU) and schedule-independent results (GPU)."""
+import numpy as np
+import pytest
+
+from cmmdft_b200 import autotune as AT
+
+
+def test_candidates_distinct_orders():
+    c = AT.candidates((60, 63, 66))
+    assert c[0] == [0, 0, 0, -1, 0]
+    assert len({tuple(x) for x in c}) == len(c)
+    # 60 = 4 3 5 (orders 0, 2, 3 distinct; NO8 equals the default), 63 = 3 3 7,
+    # z half length 33 = 3 11
+    assert {x[0] for x in c} == {0, 2, 3} and {x[1] for x in c} == {0, 2} and {x[2] for x in c} == {0, 2}
+    assert AT._stage_orders(64) == {(8, 8): 0, (4, 4, 4): 1}
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("shape", [(60, 63, 66), (64, 64, 64), (97, 41, 34)])
+def test_every_schedule_gives_the_same_transforms(shape):
+    """Every candidate schedule of a grid: the 3D transform against numpy to
+    1e-13 and one C1 evaluation against the default schedule's to 1e-12
+    (relative to the largest value); tune() returns one of them."""
+    torch = pytest.importorskip("torch")
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    from cmmdft_b200 import engine as E, workload as W
+    from cmmdft_b200.hosts import cubic_host_276, methane_guest_params
+    host = cubic_host_276(0)
+    guest = methane_guest_params()
+    rng = np.random.default_rng(0)
+    x = torch.as_tensor(rng.standard_normal((1,) + shape), device="cuda")
+    ref_fft = np.fft.rfftn(x[0].cpu().numpy())
+    base = None
+    for sched in AT.candidates(shape, max_candidates=16):
+        plan = E.GridPlan(shape, host.rvecs, schedule=sched)
+        full = plan.spec_to_full(plan.rfft(x))[0][:, :, :shape[2] // 2 + 1]
+        assert np.max(np.abs(full - ref_fft)) < 1e-13 * np.max(np.abs(ref_fft)), sched
+        fn = W.build_functional(host, shape, 300.0, guest, plan=plan)
+        rho = W.initial_density(fn, [-0.0140], ninit=[3.5e-6])
+        chat = plan.new_spec(1)
+        fn.c1(E.Buffers(plan, 1), plan.rfft_yz(rho), chat, want=1)
+        c1 = plan.irfft_yz(chat)[0].cpu().numpy()
+        if base is None:
+            base = c1
+        else:
+            assert np.max(np.abs(c1 - base)) < 1e-12 * np.max(np.abs(base)), sched
+    best, table = AT.tune(shape, host.rvecs, batch=2, max_candidates=16)
+    assert best in [t[0] for t in table] and table[0][0] == best
