@@ -596,9 +596,9 @@ def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=20)   # ~0.5 s of timed solves: host jitter averages out
-    ap.add_argument("--groups", type=int, default=2,
-                    help="instance groups on concurrent streams (one group's host decisions overlap the other's "
-                         "kernels)")
+    ap.add_argument("--groups", type=int, default=4,
+                    help="instance groups on concurrent streams, each driven from its own host thread (one "
+                         "group's host decisions overlap the others' kernels; 4 groups of 6 measured best)")
     ap.add_argument("--driver", choices=("native", "python"), default="native",
                     help="batched loop in the library (cmm_solve_batched) or in Python")
     ap.add_argument("--coefs", choices=("slsqp", "exact"), default="slsqp",
