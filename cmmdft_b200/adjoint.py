@@ -321,6 +321,8 @@ def adjoint_gradients(fn, host, guest, temperature, pressures, mus, rho, cutoff=
     """
     if fn.version & L.NOHS:
         raise NotImplementedError("adjoint gradients: MFA-only functionals are not supported")
+    if fn.wda is not None and fn.wda.D < 0:
+        raise NotImplementedError("adjoint gradients: the LDA part's explicit parameter derivatives are not built")
     plan = fn.plan
     B = rho.shape[0]
     n = plan.npts

@@ -429,7 +429,11 @@ __device__ __forceinline__ void tensor_weights_at(const GridDev& g, int p1, int 
 
 // WDA weight (WDAVFunctional._init_weight_function, cmmdft/functionals.py:1139-1155):
 // 3 (sin x - x cos x) / x^3 sigma_L at x = |k| D, 1 sigma_L at k = 0.
+// D < 0 selects the LDA part (LDAFunctional, cmmdft/functionals.py:1085-1114):
+// weight 1 at every frequency, without the Lanczos factor, so that the
+// "weighted density" is the density itself up to the transforms' rounding.
 __device__ __forceinline__ double wda_weight_at(const GridDev& g, int p1, int col, double D) {
+  if (D < 0) return 1.0;
   const int p2 = col / g.h3, p3 = col - p2 * g.h3;
   const double kx = g.kp1[p1], ky = g.kp2[p2], kz = g.kp3[p3];
   const double sl = (g.sl1[p1] * g.sl2[p2]) * g.sl3[p3];

@@ -9,8 +9,9 @@ GPU through the C ABI; the solver uses the fused pipeline of all parts at once
 Built: HardSphere (FMT, MFMT, WBII with the antisymmetric 'a' and tensor
 't' options, 'atWBII' being the default), MFA (with or without supercell
 tail corrections), ExtPot (spherical LJ guests) and the WDA correlation part
-of add_correlation_wda_lj.  Not built in this package: the LDA part and
-non-spherical guests; asking for them raises NotImplementedError.
+of add_correlation_wda_lj, the LDA part (LDAFunctional, add_lda).  Not built in
+this package: non-spherical guests; asking for them raises
+NotImplementedError.
 """
 import os
 from pathlib import Path
@@ -24,7 +25,7 @@ from .units import angstrom, kjmol, boltzmann
 from .workload import hs_version_code
 
 __all__ = ['FreeEnergy', 'Functional', 'HardSphereFunctional', 'MFAFunctional', 'ExternalPotential',
-           'WDAVFunctional']
+           'WDAVFunctional', 'LDAFunctional', 'eos_struct']
 
 
 def _torch():
@@ -121,7 +122,14 @@ class FreeEnergy(object):
         self.add_part(wda)
 
     def add_lda(self, eos):
-        raise NotImplementedError("the LDA part is not built in this package")
+        """LDA part of an EOS (cmmdft/functionals.py:256-268; the reference
+        passes its temperature as an extra constructor argument there, which
+        its LDAFunctional does not take -- the part itself follows
+        functionals.py:1085-1114)."""
+        eos.set_temperature(self.temperature)
+        lda = LDAFunctional(self.grid, eos)
+        lda.set_temperature(self.temperature)
+        self.add_part(lda)
 
     def add_wdav(self, eos, **kwargs):
         raise NotImplementedError("the WDA part is not built in this package")
@@ -133,8 +141,10 @@ class FreeEnergy(object):
             return self._device
         names = self.part_names
         for n in names:
-            if n not in ('HardSphere', 'MFA', 'ExtPot', 'WDA-V'):
+            if n not in ('HardSphere', 'MFA', 'ExtPot', 'WDA-V', 'LDA'):
                 raise NotImplementedError("part %r has no GPU path" % n)
+        if 'WDA-V' in names and 'LDA' in names:
+            raise NotImplementedError("the fused pipeline holds one EOS part: WDA-V or LDA")
         if 'HardSphere' not in names:
             raise NotImplementedError("the fused solve needs a HardSphere part")
         hs = self.part_dict['HardSphere']
@@ -144,7 +154,8 @@ class FreeEnergy(object):
             torch.zeros(plan.npoints, dtype=torch.float64, device='cuda')
         kst = self.part_dict['MFA'].kst if 'MFA' in names else None
         a = self.part_dict['MFA'].vdw_a if 'MFA' in names else None
-        wda = self.part_dict['WDA-V'].eos_struct() if 'WDA-V' in names else None
+        wda = self.part_dict['WDA-V'].eos_struct() if 'WDA-V' in names else \
+            (self.part_dict['LDA'].eos_struct() if 'LDA' in names else None)
         self._device = E.Functional(plan, hs.R, self.beta, self.wavelength, V, hs_version_code(hs.version), kst, a,
                                     wda=wda)
         return self._device
@@ -304,32 +315,78 @@ class WDAVFunctional(Functional):
         self.eos.set_temperature(temperature)
 
     def eos_struct(self):
-        from .eos import ModifiedBenedictWebbRubinEOS, CarnahanStarlingEOS, MFAEOS
-        kinds = [type(e) for e in self.eos.list_eos]
-        if kinds != [ModifiedBenedictWebbRubinEOS, CarnahanStarlingEOS, MFAEOS]:
-            raise NotImplementedError("the GPU WDA part evaluates SumOfEOS([MBWR, CS, MFA]) only")
-        mb, cs, mf = self.eos.list_eos
-        w = L.WdaEos()
-        w.D = self.D
-        w.sigma3 = mb.sigma ** 3
-        w.epsilon = mb.epsilon
-        w.gamma = mb.gamma
-        for i in range(8):
-            w.a[i] = mb.a[i]
-        for i in range(6):
-            w.b[i] = mb.b[i]
-        w.eta = cs.eta
-        w.kT = boltzmann * cs.temperature
-        w.a_mfa = mf.a
-        for i in range(3):
-            w.factors[i] = self.eos.factors[i]
-        return w
+        return eos_struct(self.eos, self.D)
 
     def derive(self, krho):
         raise NotImplementedError("the WDA part is evaluated inside FreeEnergy.device()'s fused pipeline")
 
     def value(self, krho, local=False):
         raise NotImplementedError("the WDA part is evaluated inside FreeEnergy.device()'s fused pipeline")
+
+
+def eos_struct(eos, D):
+    """cmm_wda_eos of an EOS the GPU evaluates: MBWR, Carnahan-Starling, the
+    mean-field EOS, or a SumOfEOS with at most one of each (cmmdft/eos.py);
+    D is the weight diameter of a WDA part, or -1 for the LDA part."""
+    from .eos import ModifiedBenedictWebbRubinEOS, CarnahanStarlingEOS, MFAEOS, SumOfEOS
+    if isinstance(eos, SumOfEOS):
+        comps = list(zip(eos.list_eos, eos.factors))
+    else:
+        comps = [(eos, 1.0)]
+    w = L.WdaEos()
+    w.D = D
+    w.gamma = 3.0
+    seen = set()
+    for e, f in comps:
+        kind = type(e)
+        if kind in seen or kind not in (ModifiedBenedictWebbRubinEOS, CarnahanStarlingEOS, MFAEOS):
+            raise NotImplementedError("the GPU EOS parts evaluate MBWR, CS and MFA terms, one of each")
+        seen.add(kind)
+        if kind is ModifiedBenedictWebbRubinEOS:
+            w.sigma3, w.epsilon, w.gamma = e.sigma ** 3, e.epsilon, e.gamma
+            for i in range(8):
+                w.a[i] = e.a[i]
+            for i in range(6):
+                w.b[i] = e.b[i]
+            w.factors[0] = f
+        elif kind is CarnahanStarlingEOS:
+            w.eta, w.kT = e.eta, boltzmann * e.temperature
+            w.factors[1] = f
+        else:
+            w.a_mfa = e.a
+            w.factors[2] = f
+    return w
+
+
+class LDAFunctional(Functional):
+    """Local density approximation of an EOS excess free energy
+    (cmmdft/functionals.py:1085-1114): dF/drho = f'_EOS(rho), F = integral
+    f_EOS(rho).  Evaluated inside the fused functional pipeline
+    (FreeEnergy.device()) as the WDA machinery with weight 1; the EOS must be
+    one the GPU evaluates (see ``eos_struct``).  A FreeEnergy holds at most
+    one of the LDA and WDA parts."""
+    name = 'LDA'
+
+    def __init__(self, grid, eos):
+        self.grid = grid
+        self.eos = eos
+        self.temperature = None
+
+    def copy(self, grid=None):
+        return type(self)(grid or self.grid.copy(), self.eos)
+
+    def set_temperature(self, temperature, **kwargs):
+        self.temperature = temperature
+        self.eos.set_temperature(temperature)
+
+    def eos_struct(self):
+        return eos_struct(self.eos, -1.0)
+
+    def derive(self, krho):
+        raise NotImplementedError("the LDA part is evaluated inside FreeEnergy.device()'s fused pipeline")
+
+    def value(self, krho, local=False):
+        raise NotImplementedError("the LDA part is evaluated inside FreeEnergy.device()'s fused pipeline")
 
 
 class ExternalPotential(Functional):

@@ -86,7 +86,8 @@ enum { CMM_FMT = 0, CMM_MFMT = 1, CMM_WBII = 2, CMM_ANTISYM = 8, CMM_NOHS = 16, 
  * Weight: 3 (sin x - x cos x) / x^3 sigma_L at x = |k| D.  The MBWR
  * coefficients a[8], b[6] are those at the solve temperature. */
 typedef struct cmm_wda_eos {
-  double D;                 /* weight diameter (2 Rhs) */
+  double D;                 /* weight diameter (2 Rhs); D < 0: the LDA part (LDAFunctional,
+                               cmmdft/functionals.py:1085-1114), weight 1: the EOS at the density itself */
   double sigma3, epsilon, gamma;   /* MBWR: sigma**3 (as the reference forms it), epsilon, gamma */
   double a[8], b[6];
   double eta, kT;           /* Carnahan-Starling: 4 pi R^3 / 3, k_B T */

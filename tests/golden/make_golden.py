@@ -8,6 +8,7 @@ machines):
     python tests/golden/make_golden.py --reference <reference tree> --qn
     python tests/golden/make_golden.py --reference <reference tree> --dropin
     python tests/golden/make_golden.py --reference <reference tree> --uneven
+    python tests/golden/make_golden.py --reference <reference tree> --lda
 
 ``--reference`` (or the environment variable CMM_REFERENCE_ROOT) names the
 root of the reference's source tree, the directory that holds ``cmmdft/``.
@@ -49,6 +50,9 @@ Outputs (small ``.npz`` files) land next to this script:
   uneven5.npz     host 5 of the uneven batch (uneven_hosts(8, 2)) on its
               0.25 A grid, 119 x 157 x 125 (157 prime: Rader stages on the
               GPU), at 0.1, 1 and 10 bar: N, Omega, steps (``--uneven``).
+  lda32.npz       the 32^3 case with an LDA part (SumOfEOS of MBWR, CS and
+              the mean-field EOS): part values, the LDA derivative, C1 and
+              Omega of the two profiles, three static Picard steps (``--lda``).
   iso64_rho.npz   the converged densities of that isotherm at the pressure
               indices ISO_RHO_IDX, and the reference run against itself: the
               same points re-solved from a start perturbed by one ulp, with
@@ -176,6 +180,46 @@ def _iso64_point(task):
     print('iso64 P=%.4g bar%s: N=%.12e steps=%d conv=%s (%.0f s)'
           % (P, ' (perturbed start)' if perturb else '', N, s.curr_step, conv, time.time() - t0), flush=True)
     return i, b['mu'], bulk, N, s.omega0, s.curr_step, bool(conv), (rho if conv else None)
+
+
+def lda32(args):
+    """The LDA part (LDAFunctional, cmmdft/functionals.py:1085-1114) on the
+    32^3 case: WBII + MFA + ExtPot + LDA of SumOfEOS([MBWR, CS, MFA],
+    [1, -1, -1]).  The reference's own FreeEnergy.add_lda passes an extra
+    argument to LDAFunctional (functionals.py:267) and its set_temperature
+    forwards Rhs to an EOS that does not take it, so the part is built
+    directly, added with add_part and given its temperature alone."""
+    ref = import_reference(args.reference)
+    system, functionals, solver, extpot, eos = ref
+    from cmmdft_b200.hosts import cubic_host_276, methane_guest_params
+    from cmmdft_b200.units import angstrom
+    sig, eps, mass = methane_guest_params()
+    T = 300.0
+    b = quiet(build, ref, 32, cubic_host_276(seed=0), T, 1.0, tempfile.mkdtemp(prefix='cmm_lda_'))
+    fe, grid, mu = b['fe'], b['grid'], b['mu']
+    Rhs = b['guest'].Rhs
+    a = fe.part_dict['MFA'].compute_vdw_a()
+    S = eos.SumOfEOS(mass, [eos.ModifiedBenedictWebbRubinEOS(mass, sig, eps), eos.CarnahanStarlingEOS(mass, Rhs),
+                            eos.MFAEOS(mass, sig, eps, a=a)], factors=[1, -1, -1])
+    lda = functionals.LDAFunctional(grid, S)
+    lda.set_temperature(T)
+    fe.add_part(lda)
+    out = dict(mu=mu, T=T)
+    V = fe.part_dict['ExtPot'].potential
+    rho_a = np.exp(fe.beta * (mu - V)) / fe.wavelength ** 3
+    from cmmdft_b200.units import angstrom as A
+    rho_b = 0.02 / A ** 3 * np.clip(np.exp(-fe.beta * V), 0, 1)
+    for tag, rho in (('a', rho_a), ('b', rho_b)):
+        parts, om, derivs, C1 = quiet(omega_parts, ref, b, rho, mu)
+        out['values_' + tag] = np.array(parts)
+        out['omega_' + tag] = om
+        out['dLDA_' + tag] = derivs[3]
+        out['C1_' + tag] = C1
+    s = solver.Picard(b['prog'], nsteps=3, alpha_mix=0.1, method='static', criterion='res', threshold=1e-8)
+    N, rho, conv = quiet(s.solve, mu, rho_a.copy(), 3)
+    out.update(picard3_rho=rho, picard3_N=N)
+    np.savez_compressed(os.path.join(HERE, 'lda32.npz'), **out)
+    print('wrote lda32.npz', {k: v for k, v in out.items() if np.ndim(v) == 0})
 
 
 UNEVEN_HOST = 5                       # uneven_hosts(8, 2)[5]: 119 x 157 x 125 (prime 157), 2026 atoms
@@ -429,6 +473,7 @@ def main():
     ap.add_argument('--qn', action='store_true')
     ap.add_argument('--dropin', action='store_true')
     ap.add_argument('--uneven', action='store_true')
+    ap.add_argument('--lda', action='store_true')
     ap.add_argument('--procs', type=int, default=8)
     args = ap.parse_args()
     if not args.reference:
@@ -441,6 +486,8 @@ def main():
         return dropin32(args)
     if args.uneven:
         return uneven(args)
+    if args.lda:
+        return lda32(args)
     ref = import_reference(args.reference)
     solver = ref[2]
     from cmmdft_b200.hosts import cubic_host_276, HELIUM
