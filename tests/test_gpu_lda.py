@@ -78,7 +78,6 @@ def test_lda_part_against_reference(golden32, tmp_path):
                                                                       e_d, e_F))
         assert e_d < 1e-12 and e_F < 1e-11
     s = BT.NativeBatchSolve(fn, [mu], method='static', nsteps=3, threshold=1e-30, criterion='res')
-    N, rho, conv = s.solve(torch.as_tensor(np.exp(fn.beta * (mu - fn.V.cpu().numpy()))[None] / fn.lambda3,
-                                           device="cuda"))
+    N, rho, conv = s.solve(torch.as_tensor(golden32["rho_a"][None], device="cuda"))
     assert relerr(rho[0].cpu().numpy(), ref["picard3_rho"]) < 1e-10
     assert scalar_rel(N[0], ref["picard3_N"]) < 1e-10
