@@ -190,6 +190,12 @@ class EquationOfState(object):
         func = lambda r: kT * r + _ipow(r, 2) * self.derivative_excess_free_energy_particle(r)
         return self._solve_all(pressures, func, self.get_rough_density_grid(n_rough_gridpoints), 3)
 
+    def calculate_pressure(self, temp, chempot):
+        """Pressure of the lowest-density branch at a chemical potential (eos.py:201-207)."""
+        self.set_temperature(temp)
+        rho = self.solve_densities_from_chempots([chempot])[0][0]
+        return self.compute_pressure(rho)
+
     def calculate_mu(self, temp, pressure):
         """Chemical potential of the lowest-density branch at (T, P), eos.py:209-215.
         ``pressure`` may be an array: one chemical potential per pressure."""

@@ -160,30 +160,61 @@ class FreeEnergy(object):
                                     wda=wda)
         return self._device
 
+    def _part_values(self, rho_np, krho=None):
+        """Values of the parts at rho: the fused pipeline when it holds every
+        part (the WDA and LDA parts have no standalone value), else part by
+        part."""
+        if 'HardSphere' in self.part_names:
+            return _fused_part_values(self, rho_np)
+        if krho is None:
+            krho = self.grid.fft(rho_np)
+        return [p.value(krho) for p in self.parts]
+
     def init_tracking(self, fn, rewrite=False):
         self.fn_tracking = fn
         if not os.path.isfile(fn) or self.overwrite or rewrite:
             with open(fn, 'w') as f:
-                print("#phase\tstep\t     loading\t         -muN\t        IdGas\t" +
+                print("#phase\tstep\t     loading\t         -\u00b5N\t        IdGas\t" +
                       "\t".join("%13s" % p.name for p in self.parts) + "\t        Total", file=f)
 
-    def track(self, chempot, rho, krho=None, iphase=0, write=True, print_out=False, fn=None, unit=1):
-        """Grand potential of rho with its parts (cmmdft/functionals.py:121-174)."""
+    def track(self, chempot, rho, krho=None, iphase=0, write=True, print_out=False, fn=None, unit=1, step=0):
+        """Grand potential of rho with its parts (cmmdft/functionals.py:121-174),
+        appended as one line (phase, step, loading, -mu N, ideal part, each
+        part, total) to the tracking file when one is set."""
         g = self.grid
         rho_np = rho if not hasattr(rho, 'detach') else rho.detach().cpu().numpy()
         N = g.integrate(rho_np)
         rr = np.where(rho_np <= 0 + np.isclose(rho_np, 0), 1e-30, rho_np)
         Fid = g.integrate(rr * (np.log(self.wavelength ** 3 * rr) - 1.0)) / self.beta
         G = Fid - chempot * N
-        if krho is None:
-            krho = g.fft(rho_np)
-        vals = [p.value(krho) for p in self.parts]
+        vals = self._part_values(rho_np, krho)
         G += sum(vals)
         if write and (fn or self.fn_tracking):
             with open(fn or self.fn_tracking, 'a') as f:
-                print("%6i\t%4i\t%.6e\t%.6e\t% .6e\t" % (iphase, 0, N, -chempot * N / unit, Fid / unit) +
+                print("%6i\t%4i\t%.6e\t%.6e\t% .6e\t" % (iphase, step, N, -chempot * N / unit, Fid / unit) +
                       "\t".join("% .6e" % (v / unit) for v in vals) + "\t% .6e" % (G / unit), file=f)
         return G
+
+
+def _fused_part_values(fe, rho_np):
+    """Free-energy value of every part of ``fe`` at the density rho (numpy),
+    in part order, from one evaluation of the fused pipeline: PHI, the MFA
+    Parseval sum and the EOS part's sum from its reductions, the external
+    part as integral rho V."""
+    torch = _torch()
+    fn = fe.device()
+    plan = fn.plan
+    rho_t = torch.as_tensor(np.ascontiguousarray(rho_np, dtype=np.float64), device='cuda').reshape(
+        (1,) + tuple(plan.npoints))
+    buf = E.Buffers(plan, 1, nwork=fn.nwork)
+    buf.part[:, L.STAT_N3MAX, :] = -np.inf
+    fn.c1(buf, plan.rfft_yz(rho_t), None, want=2)
+    st = _stats_of(plan, buf)
+    dr = plan.dr
+    by = {'HardSphere': st[L.STAT_PHI] * dr / fn.beta, 'MFA': 0.5 * st[L.STAT_MFA] * dr,
+          'WDA-V': st[L.STAT_WDA] * dr, 'LDA': st[L.STAT_WDA] * dr,
+          'ExtPot': float((rho_t[0] * fn.V).sum().item()) * dr}
+    return [float(by[p.name]) for p in fe.parts]
 
 
 def _stats_of(plan, buf):

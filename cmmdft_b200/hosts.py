@@ -23,6 +23,10 @@ HOST_LJ_TYPES = {
 # Type counts of the 276-atom cell; larger cells keep these fractions.
 HOST_TYPE_COUNTS = {"C": 96, "H": 120, "N": 48, "Zn": 12}
 
+# Standard atomic weights [amu] of the host atom types (for unit conversions
+# of loadings only; the grid solve does not use host masses).
+ATOM_MASSES = {"C": 12.011, "H": 1.008, "N": 14.007, "Zn": 65.38}
+
 # United-atom methane: sigma [angstrom], epsilon/kB [K], mass [amu].
 METHANE = {"sigma": 3.73, "epsilon_K": 148.0, "mass": 16.04}
 # Helium probe for the void fraction (Hirschfelder, Curtiss and Bird).
@@ -70,6 +74,12 @@ class SyntheticHost(object):
     @property
     def volume(self):
         return float(abs(np.linalg.det(self.rvecs)))
+
+    @property
+    def masses(self):
+        """Atomic masses (atomic units) from the type names' standard weights."""
+        w = np.array([ATOM_MASSES.get(t, np.nan) for t in self.ffatypes])
+        return w[self.ffatype_ids] * amu
 
     def recentred_pos(self):
         """Positions shifted so their mean is the origin (cmmdft/system.py:70)."""

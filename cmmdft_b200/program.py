@@ -99,13 +99,19 @@ class Program(object):
               continue_solving=False):
         """Equilibrium density at one chemical potential (cmmdft/program.py:331-404)."""
         self.file_suffix = get_file_suffix(chempot, self.fener.temperature)
+        if energy_tracking:   # convergence_*.txt (program.py:372-374, functionals.py:121-174)
+            self.fener.init_tracking(os.path.join(self.workdir, 'convergence_%s.txt' % self.file_suffix))
         self.rho_fn = os.path.join(self.workdir, 'rho_%s.npy' % self.file_suffix)
         if os.path.isfile(self.rho_fn) and not self.overwrite and not rewrite and not continue_solving:
             rho = np.load(self.rho_fn)
             return self.grid.integrate(rho), rho, True
         self._set_initial_density(Ninit=Ninit, chempot=chempot, rewrite=rewrite,
                                   temperature=self.fener.temperature, silent=silent)
+        if energy_tracking:   # the start density's line (the reference writes one per step)
+            self.fener.track(chempot, self.rho0, step=0)
         N, rho, converged = self.solver.solve(chempot, self.rho0.copy(), 2)
+        if energy_tracking:   # the final density's line
+            self.fener.track(chempot, rho, step=self.solver.curr_step)
         if self.solver.track_history:
             fn = self.workdir / ('solving_history_%s.csv' % self.file_suffix)
             np.savetxt(fn, self.solver.history[:self.solver.curr_step + 1], delimiter=',',

@@ -130,7 +130,8 @@ class NanoporousHost(Host):
     ``ff`` ({type: (sigma, epsilon)}) must be given.
     """
 
-    def __init__(self, name, chk=None, par=None, pos=None, ffatypes=None, ffatype_ids=None, rvecs=None, ff=None):
+    def __init__(self, name, chk=None, par=None, pos=None, ffatypes=None, ffatype_ids=None, rvecs=None, ff=None,
+                 masses=None):
         self.chk, self.par = chk, par
         if chk is not None:
             d = read_chk(chk)
@@ -138,6 +139,9 @@ class NanoporousHost(Host):
             ffatypes = list(d['ffatypes'])
             ffatype_ids = d['ffatype_ids']
             rvecs = d['rvecs']
+            masses = d.get('masses', masses)
+        # atomic masses (atomic units), used for loading-unit conversions only
+        self.masses = None if masses is None else np.asarray(masses, dtype=np.float64)
         if ff is None and par is not None:
             ff = read_pars_file(par)
         self.pos = np.asarray(pos, dtype=np.float64).copy()
@@ -152,7 +156,7 @@ class NanoporousHost(Host):
     def from_synthetic(cls, name, synth):
         """Wrap a hosts.SyntheticHost."""
         return cls(name, pos=synth.pos, ffatypes=synth.ffatypes, ffatype_ids=synth.ffatype_ids,
-                   rvecs=synth.rvecs, ff=synth.ff)
+                   rvecs=synth.rvecs, ff=synth.ff, masses=getattr(synth, 'masses', None))
 
     @property
     def natom(self):

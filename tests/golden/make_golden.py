@@ -278,7 +278,8 @@ def dropin32(args):
     T = 300.0
     host = cubic_host_276(seed=0)
     sig, eps, mass = methane_guest_params()
-    mol = yaff.System(pos=host.pos.copy(), ffatypes=host.ffatypes, ffatype_ids=host.ffatype_ids, rvecs=host.rvecs)
+    mol = yaff.System(pos=host.pos.copy(), ffatypes=host.ffatypes, ffatype_ids=host.ffatype_ids, rvecs=host.rvecs,
+                      masses=host.masses)
     mol.pos -= mol.pos.sum(axis=0) / len(mol.pos)  # as system.py:70
     h = system.NanoporousHost.__new__(system.NanoporousHost)
     system.Host.__init__(h, 'synthetic', mol.cell)
@@ -296,7 +297,8 @@ def dropin32(args):
     he = grid0.integrate(np.clip(np.exp(-Vhe / boltzmann / T), 0, 1)).real / grid0.cell.volume
 
     def program(suffix):
-        prog = rprogram.Program(prefix=tmp, hostname='synthetic', guestname='CH4', suffix=suffix)
+        prog = rprogram.Program(prefix=tmp, hostname='synthetic', guestname='CH4', ff_suffix='trappe_uff',
+                                suffix=suffix)
         prog.set_system(h, guest)
         prog.set_grid(npoints=32)
         prog.init_free_energy(T)
@@ -326,6 +328,12 @@ def dropin32(args):
     N, rho, conv = quiet(pb.solve, mu, Ninit=bulk)
     out.update(ninit_rho=rho, ninit_N=N, ninit_conv=conv, ninit_steps=sb.curr_step, ninit_omega=sb.omega0,
                ninit_history=sb.history[:sb.curr_step + 1, :5].copy())
+    # energy tracking (Program.solve's default): the start and final lines
+    conv_fn = os.path.join(pb.workdir, 'convergence_%s.txt' % pb.file_suffix)
+    with open(conv_fn) as f:
+        lines = [l.split() for l in f if l.strip() and not l.startswith('#')]
+    out['ninit_track_first'] = np.array([float(x) for x in lines[0]])
+    out['ninit_track_last'] = np.array([float(x) for x in lines[-1]])
     # The reference against itself: both flows again from a start one ulp
     # above the nominal one (the ideal-gas start of A given as an array),
     # recording the relative change of each observable (the rounding floor
@@ -359,6 +367,15 @@ def dropin32(args):
         if tag.endswith('_ulp'):
             rho = np.load(prog.rho_fn)
             out[tag + '_rho'] = rho
+        if tag == 'ninit':   # the loading exports (calculator.py:186-340)
+            f1 = calc.save_loadings(T, [mu], fn=os.path.join(tmp, 'loads.csv'))
+            calc.save_loadings(T, [mu], pressure=True, eos=mb, fn=os.path.join(tmp, 'loads_P.csv'))
+            calc.save_loadings_AIF(T, chempots=np.array([mu]), eos=mb, user='tester', loading_unit='mol/kg',
+                                   fn=os.path.join(tmp, 'ads.aif'))
+            for key, name in (('csv', 'loads.csv'), ('csv_P', 'loads_P.csv'), ('aif', 'ads.aif')):
+                with open(os.path.join(tmp, name)) as f:
+                    out['ninit_' + key] = np.array(f.read())
+            del f1
     for tag in ('cascade', 'ninit'):
         base, pert = tag, tag + '_ulp'
         fl = dict(rho=float(np.max(np.abs(out[pert + '_rho'] - out[base + '_rho'])) / np.max(np.abs(out[base + '_rho']))))

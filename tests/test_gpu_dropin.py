@@ -50,10 +50,11 @@ def make_program(prefix, suffix='', version='WBII'):
     """Program of the 32^3 case through the public API only."""
     h = cubic_host_276(0)
     host = cd.NanoporousHost('synthetic', pos=h.pos, ffatypes=h.ffatypes, ffatype_ids=h.ffatype_ids,
-                             rvecs=h.rvecs, ff=h.ff)
+                             rvecs=h.rvecs, ff=h.ff, masses=h.masses)
     sig, eps, mass = methane_guest_params()
     guest = cd.SphericalLJGuest('CH4', mass, sig, eps)
-    prog = cd.Program(prefix=str(prefix), hostname='synthetic', guestname='CH4', suffix=suffix)
+    prog = cd.Program(prefix=str(prefix), hostname='synthetic', guestname='CH4', ff_suffix='trappe_uff',
+                      suffix=suffix)
     prog.set_system(host, guest)
     prog.set_grid(npoints=32)
     prog.init_free_energy(T)
@@ -162,6 +163,33 @@ def test_program_solve_ninit_float_history_and_cache(cuda, dropin, tmp_path):
     assert os.path.isfile(prog.rho_fn)
     csv = prog.workdir / ('solving_history_%s.csv' % prog.file_suffix)
     assert csv.is_file() and np.loadtxt(csv, delimiter=',').shape[0] == s.curr_step + 1
+
+    # energy tracking (convergence_*.txt): the start and final lines against
+    # the reference's first and last (its columns: phase, step, N, -mu N,
+    # ideal part, each part, total; written with 7 significant digits)
+    conv_fn = prog.workdir / ('convergence_%s.txt' % prog.file_suffix)
+    rows = [l.split() for l in open(conv_fn) if l.strip() and not l.startswith('#')]
+    for got, ref in ((rows[0], dropin["ninit_track_first"]), (rows[-1], dropin["ninit_track_last"])):
+        got = np.array([float(x) for x in got])
+        assert got.shape == ref.shape and np.allclose(got, ref, rtol=2e-6, atol=0), (got, ref)
+    # the loading exports (calculator.py:186-340) against the reference's files
+    calc = cd.Calculator(prog)
+    eos = mbwr()
+    tmp = tmp_path / 'exports'
+    tmp.mkdir()
+    calc.save_loadings(T, [mu], fn=tmp / 'loads.csv')
+    calc.save_loadings(T, [mu], pressure=True, eos=eos, fn=tmp / 'loads_P.csv')
+    calc.save_loadings_AIF(T, chempots=np.array([mu]), eos=eos, user='tester', loading_unit='mol/kg',
+                           fn=tmp / 'ads.aif')
+    for name, key in (('loads.csv', 'ninit_csv'), ('loads_P.csv', 'ninit_csv_P')):
+        got = np.loadtxt(tmp / name, delimiter=',', skiprows=1)
+        ref = np.loadtxt(str(dropin[key]).splitlines()[1:], delimiter=',')
+        assert open(tmp / name).readline().strip() == str(dropin[key]).splitlines()[0]
+        assert np.allclose(got, ref, rtol=1e-10, atol=0), (name, got, ref)
+    skip = ('_simltn_date', '_simltn_code')
+    got = [l for l in open(tmp / 'ads.aif').read().splitlines() if not l.startswith(skip)]
+    ref = [l for l in str(dropin["ninit_aif"]).splitlines() if not l.startswith(skip)]
+    assert got == ref, (got, ref)
 
     class Refuse(cd.Solver):
         def solve(self, *a, **k):
