@@ -95,6 +95,14 @@ _SIGS = {
     "cmm_extpot_lj": ([c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, c_double, c_double,
                        c_double, c_double, c_void_p, c_void_p], c_int),
     "cmm_extpot_set_mode": ([c_int], c_int),
+    "cmm_extpot_rot": ([c_void_p, c_void_p, c_void_p, c_int, c_void_p, c_void_p, c_int, P(c_double), P(c_double),
+                        P(c_double), P(c_double), c_int, c_void_p, c_void_p, c_int, c_double, c_double, c_double,
+                        c_void_p, c_void_p], c_int),
+    "cmm_extpot_lj_deriv": ([P(c_double), c_int, c_int, c_int, P(c_double), c_void_p, c_void_p, c_int, c_void_p,
+                             c_void_p, c_int, c_double, c_double, c_double, c_double, c_void_p, c_void_p], c_int),
+    "cmm_extpot_rot_interp": ([c_void_p, c_void_p, c_int, P(c_int), P(c_double), P(c_double), P(c_double),
+                               P(c_double), P(c_int), c_int, c_void_p, c_void_p, c_int, c_double, c_double, c_void_p,
+                               c_void_p], c_int),
     "cmm_rfft3d": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
     "cmm_irfft3d": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),
     "cmm_rfft_yz": ([c_void_p, c_int, c_void_p, c_void_p, c_void_p], c_int),

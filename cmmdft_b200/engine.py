@@ -256,6 +256,78 @@ def external_potential(plan, pos, type_ids, type_sigma, type_epsilon, guest_sigm
     return V
 
 
+def effective_potential(plan, pos, type_ids, type_sigma, type_epsilon, guest_pos, guest_masses, site_sigma,
+                        site_epsilon, rotations, weights, cutoff, beta, v_limit):
+    """Orientation-averaged LJ potential of a rigid multi-site guest on the
+    plan's grid (device tensor [N1,N2,N3], uncapped; cmm_extpot_rot)."""
+    dev = "cuda"
+    f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+    pos_t, sig_t, eps_t = f64(pos), f64(type_sigma), f64(type_epsilon)
+    typ_t = torch.as_tensor(np.ascontiguousarray(type_ids, dtype=np.int32), device=dev)
+    rot_t, w_t = f64(np.asarray(rotations).reshape(-1, 9)), f64(weights)
+    gp = np.ascontiguousarray(guest_pos, dtype=np.float64).reshape(-1)
+    gm, gs, ge = (np.ascontiguousarray(a, dtype=np.float64) for a in (guest_masses, site_sigma, site_epsilon))
+    ns = len(gm)
+    if not (len(gp) == 3 * ns and len(gs) == ns and len(ge) == ns and len(w_t) == len(rot_t)):
+        raise ValueError("guest arrays or rotations/weights have inconsistent lengths")
+    cd = lambda a: a.ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    V = torch.empty(plan.npoints, dtype=torch.float64, device=dev)
+    check(L.lib().cmm_extpot_rot(plan.handle, ptr(pos_t), ptr(typ_t), int(len(pos_t)), ptr(sig_t), ptr(eps_t),
+                                 int(len(sig_t)), cd(gp), cd(gm), cd(gs), cd(ge), ns, ptr(rot_t), ptr(w_t),
+                                 int(len(w_t)), float(cutoff), float(beta), float(v_limit), ptr(V), _stream()),
+          "cmm_extpot_rot")
+    return V
+
+
+def external_potential_derivatives(rvecs, npoints, spacings, pos, type_ids, type_sigma, type_epsilon, guest_sigma,
+                                   guest_epsilon, cutoff, v_max, out=None):
+    """The eight LJ channels (V and its derivatives in unit-cube scaling) of
+    one guest atom type on an npoints grid over the cell: device tensor
+    [8, n1, n2, n3] (cmm_extpot_lj_deriv)."""
+    dev = "cuda"
+    f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+    pos_t, sig_t, eps_t = f64(pos), f64(type_sigma), f64(type_epsilon)
+    typ_t = torch.as_tensor(np.ascontiguousarray(type_ids, dtype=np.int32), device=dev)
+    n1, n2, n3 = (int(n) for n in npoints)
+    if out is None:
+        out = torch.empty((8, n1, n2, n3), dtype=torch.float64, device=dev)
+    rv = (ctypes.c_double * 9)(*np.asarray(rvecs, dtype=np.float64).ravel().tolist())
+    sp = (ctypes.c_double * 3)(*[float(s) for s in spacings])
+    check(L.lib().cmm_extpot_lj_deriv(rv, n1, n2, n3, sp, ptr(pos_t), ptr(typ_t), int(len(pos_t)), ptr(sig_t),
+                                      ptr(eps_t), int(len(sig_t)), float(guest_sigma), float(guest_epsilon),
+                                      float(cutoff), float(v_max), ptr(out), _stream()), "cmm_extpot_lj_deriv")
+    return out
+
+
+def effective_potential_interpolated(plan, tables, site_tab, origin, spacing, guest_pos, guest_masses, rotations,
+                                     weights, beta, v_limit):
+    """Orientation-averaged potential with tricubically interpolated site
+    potentials (cmm_extpot_rot_interp).  ``tables``: device tensor
+    [ntab, 8, f1, f2, f3] of channel grids; ``site_tab[s]``: the table of
+    site s; ``origin``/``spacing``: the interpolator's."""
+    dev = "cuda"
+    f64 = lambda a: torch.as_tensor(np.ascontiguousarray(a, dtype=np.float64), device=dev)
+    tables = tables.contiguous()
+    if tables.dim() != 5 or tables.shape[1] != 8:
+        raise ValueError("tables must be [ntab, 8, f1, f2, f3]")
+    rot_t, w_t = f64(np.asarray(rotations).reshape(-1, 9)), f64(weights)
+    gp = np.ascontiguousarray(guest_pos, dtype=np.float64).reshape(-1)
+    gm = np.ascontiguousarray(guest_masses, dtype=np.float64)
+    st = np.ascontiguousarray(site_tab, dtype=np.int32)
+    ns = len(gm)
+    if not (len(gp) == 3 * ns and len(st) == ns and len(w_t) == len(rot_t)):
+        raise ValueError("guest arrays or rotations/weights have inconsistent lengths")
+    cd = lambda a: np.ascontiguousarray(a, dtype=np.float64).ctypes.data_as(ctypes.POINTER(ctypes.c_double))
+    fn = (ctypes.c_int * 3)(*[int(n) for n in tables.shape[2:]])
+    org, spc = np.asarray(origin, dtype=np.float64), np.asarray(spacing, dtype=np.float64)
+    V = torch.empty(plan.npoints, dtype=torch.float64, device=dev)
+    check(L.lib().cmm_extpot_rot_interp(plan.handle, ptr(tables), int(tables.shape[0]), fn, cd(org), cd(spc),
+                                        cd(gp), cd(gm), st.ctypes.data_as(ctypes.POINTER(ctypes.c_int)), ns,
+                                        ptr(rot_t), ptr(w_t), int(len(w_t)), float(beta), float(v_limit), ptr(V),
+                                        _stream()), "cmm_extpot_rot_interp")
+    return V
+
+
 def finalize(buf, mask, active=None):
     check(L.lib().cmm_stats_finalize(buf.batch, ptr(active), ptr(buf.part), buf.nslot, ctypes.c_uint(mask),
                                      ptr(buf.stats), _stream()), "cmm_stats_finalize")

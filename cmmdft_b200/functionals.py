@@ -8,10 +8,10 @@ GPU through the C ABI; the solver uses the fused pipeline of all parts at once
 
 Built: HardSphere (FMT, MFMT, WBII with the antisymmetric 'a' and tensor
 't' options, 'atWBII' being the default), MFA (with or without supercell
-tail corrections), ExtPot (spherical LJ guests) and the WDA correlation part
-of add_correlation_wda_lj, the LDA part (LDAFunctional, add_lda).  Not built in
-this package: non-spherical guests; asking for them raises
-NotImplementedError.
+tail corrections), ExtPot (spherical LJ guests, and multi-site guests by the
+orientational average, directly or tricubically interpolated), the WDA
+correlation part of add_correlation_wda_lj and the LDA part (LDAFunctional,
+add_lda).
 """
 import os
 from pathlib import Path
@@ -31,6 +31,11 @@ __all__ = ['FreeEnergy', 'Functional', 'HardSphereFunctional', 'MFAFunctional', 
 def _torch():
     import torch
     return torch
+
+
+def format_temperature(temperature):
+    """'<T>K' as the reference names temperature-dependent files (f'{T:#3.2f}K')."""
+    return '%#3.2fK' % temperature
 
 
 class Functional(object):
@@ -97,13 +102,50 @@ class FreeEnergy(object):
 
     def add_external_potential(self, temperature=None, cutoff=12 * angstrom, limit_potential=1e4 * kjmol,
                                degree=9, interpolate=False, rewrite=False, load_fn=None, save_fn=None, **kwargs):
-        ep = ExternalPotential(self.grid, self.system, None, limit_potential=limit_potential, cutoff=cutoff)
+        """External potential part (cmmdft/functionals.py:176-254).
+
+        With the Program's names set, the potential is kept where the
+        reference keeps it, prefix/host/guest/ff_suffix/grid_suffix/suffix/
+        (epot.npy, or eff_epot_<T>K.npy for a multi-site guest, with a
+        workdir/ExtPots link to it) and loaded from there unless
+        ``rewrite`` or the FreeEnergy's ``overwrite`` is set.  Capping:
+        non-finite or above ``limit_potential`` -> ``limit_potential``.
+        """
+        from .system import NonSphericalGuest
+        fn = None
         if load_fn is not None:
+            assert str(load_fn).endswith('.npy'), 'fn must be a filename of an external potential'
+            assert os.path.isfile(load_fn), 'fn must be a filename of an external potential, %s' % load_fn
+            ep = ExternalPotential(self.grid, self.system, Path(load_fn).parent, limit_potential=limit_potential,
+                                   **kwargs)
             ep.load_potential(load_fn)
         else:
-            ep.generate_potential(temperature)
+            epot_dr = None
             if save_fn is not None:
-                ep.dump_potential(save_fn)
+                fn = Path(save_fn)
+                epot_dr = fn.parent
+            elif self.name_dict:
+                nd = self.name_dict
+                epot_dr = Path(nd.get('prefix', '')) / nd.get('hostname', '') / nd.get('guestname', '') / \
+                    nd.get('ff_suffix', '') / nd.get('grid_suffix', '') / nd.get('suffix', '')
+                epot_dr.mkdir(parents=True, exist_ok=True)
+                g = self.system.guest
+                if isinstance(g, NonSphericalGuest) and g.mol.natom != 1:
+                    assert temperature is not None, 'Temperature must be provided for non-spherical particles'
+                    fn = epot_dr / ('eff_epot_%s.npy' % format_temperature(temperature))
+                else:
+                    fn = epot_dr / 'epot.npy'
+                link = self.workdir / 'ExtPots'
+                if not link.is_symlink() and not link.exists():
+                    link.symlink_to(epot_dr.absolute())
+            ep = ExternalPotential(self.grid, self.system, epot_dr, limit_potential=limit_potential, degree=degree,
+                                   interpolate=interpolate, cutoff=cutoff)
+            if fn is None or not os.path.isfile(fn) or self.overwrite or rewrite:
+                ep.generate_potential(temperature, rewrite=rewrite)
+                if fn is not None:
+                    ep.dump_potential(fn)
+            else:
+                ep.load_potential(fn)
         ep.cap()
         self.add_part(ep)
 
@@ -177,14 +219,24 @@ class FreeEnergy(object):
                 print("#phase\tstep\t     loading\t         -\u00b5N\t        IdGas\t" +
                       "\t".join("%13s" % p.name for p in self.parts) + "\t        Total", file=f)
 
-    def track(self, chempot, rho, krho=None, iphase=0, write=True, print_out=False, fn=None, unit=1, step=0):
+    def track(self, chempot, rho, krho=None, iphase=0, write=True, print_out=False, fn=None, unit=1, step=0,
+              lower_density=None):
         """Grand potential of rho with its parts (cmmdft/functionals.py:121-174),
         appended as one line (phase, step, loading, -mu N, ideal part, each
-        part, total) to the tracking file when one is set."""
+        part, total) to the tracking file when one is set.
+
+        The ideal part regularises rho as FreeEnergy.track does (values <= 0,
+        or within 1e-8 of 0, -> 1e-30); with ``lower_density`` it clips as
+        the solvers' own tracking lines do instead (Solver._get_Omega and
+        _clip_density, cmmdft/solver.py:103-148: rho < lower_density ->
+        1e-30)."""
         g = self.grid
         rho_np = rho if not hasattr(rho, 'detach') else rho.detach().cpu().numpy()
         N = g.integrate(rho_np)
-        rr = np.where(rho_np <= 0 + np.isclose(rho_np, 0), 1e-30, rho_np)
+        if lower_density is None:
+            rr = np.where(rho_np <= 0 + np.isclose(rho_np, 0), 1e-30, rho_np)
+        else:
+            rr = np.where(rho_np < lower_density, 1e-30, rho_np)
         Fid = g.integrate(rr * (np.log(self.wavelength ** 3 * rr) - 1.0)) / self.beta
         G = Fid - chempot * N
         vals = self._part_values(rho_np, krho)
@@ -421,7 +473,14 @@ class LDAFunctional(Functional):
 
 
 class ExternalPotential(Functional):
-    """External potential part (cmmdft/functionals.py:941-1083)."""
+    """External potential part (cmmdft/functionals.py:941-1083).
+
+    Spherical LJ guests: the LJ potential of the host atoms
+    (extpot_calculator.py:186-222).  Multi-site guests (NonSphericalGuest,
+    DualModelGuest): the orientation average of their sites' LJ potentials at
+    the temperature (extpot_calculator.py:569-655), regenerated by
+    set_temperature.  Both on the GPU.
+    """
     name = 'ExtPot'
 
     def __init__(self, grid, system, epot_dr=None, limit_potential=1e4 * kjmol, degree=9, interpolate=False,
@@ -432,24 +491,98 @@ class ExternalPotential(Functional):
         self.guest = system.guest
         self.epot_dr = epot_dr
         self.limit_potential = limit_potential
+        self.degree = degree
+        self.interpolate = interpolate
         self.cutoff = cutoff
         self._V = None
 
     def copy(self, grid=None):
-        e = type(self)(grid or self.grid.copy(), self.system, self.epot_dr, self.limit_potential, cutoff=self.cutoff)
+        e = type(self)(grid or self.grid.copy(), self.system, self.epot_dr, self.limit_potential, self.degree,
+                       self.interpolate, self.cutoff)
         e._V = self._V
         return e
 
-    def generate_potential(self, temperature=None, rewrite=False):
-        """LJ potential of the host atoms on the grid (extpot_calculator.py:186-222) on the GPU."""
+    def set_temperature(self, temperature, **kwargs):
+        """A multi-site guest's potential depends on the temperature: it is
+        generated for a new one unless its file exists (functionals.py:
+        1019-1025; the reference then keeps the potential it has, and leaves
+        a regenerated one uncapped -- here it is capped like every other)."""
+        from .system import NonSphericalGuest
+        if not isinstance(self.guest, NonSphericalGuest):
+            return
+        fn = None
+        if self.epot_dr is not None:
+            fn = Path(self.epot_dr) / ('eff_epot_%s.npy' % format_temperature(temperature))
+            if fn.exists():
+                return
+        self.generate_potential(temperature)
+        if fn is not None:
+            self.dump_potential(fn)
+        self.cap()
+
+    def _host_arrays(self):
         h = self.host
         if not hasattr(h, 'ff') or h.ff is None:
-            raise NotImplementedError("generate_potential needs a spherical LJ host with parameters")
+            raise NotImplementedError("generate_potential needs a host with LJ parameters")
         sig = np.array([h.ff[t][0] for t in h.ffatypes])
         eps = np.array([h.ff[t][1] for t in h.ffatypes])
-        # cap at +inf here; the FreeEnergy applies limit_potential (functionals.py:247-251)
-        self._V = E.external_potential(self.grid.plan, h.recentred_pos(), h.ffatype_ids, sig, eps,
-                                       self.guest.sigma, self.guest.epsilon, self.cutoff, self.limit_potential)
+        return h.recentred_pos(), h.ffatype_ids, sig, eps
+
+    # fine grid of the interpolated path and the interpolator's spacing
+    # (cmmdft/functionals.py:1039, 1047: both 0.15 angstrom)
+    INTERP_SPACING = 0.15 * angstrom
+    DERIV_VMAX = 1e+6 * kjmol            # clip of get_external_potential_derivatives
+
+    def _interpolated(self, pos, ids, sig, eps, rot, w, beta):
+        """interpolate=True (functionals.py:1032-1055): for every guest atom
+        type the eight LJ channels on a grid of spacing 0.15 A over the cell,
+        then the orientational average with tricubic interpolation, the
+        interpolator at the solve grid's first point with spacing 0.15 A on
+        every axis (as the reference sets it, not the fine grid's own
+        spacing)."""
+        torch = _torch()
+        g = self.guest
+        h = self.host
+        rv = h.cell.rvecs
+        lengths = np.linalg.norm(rv, axis=1)
+        fine_n = [int(np.ceil(l / self.INTERP_SPACING)) for l in lengths]
+        fine_sp = [np.linalg.norm(rv[:, a]) / fine_n[a] for a in range(3)]
+        if g.ff is None:
+            raise ValueError("guest %s has no LJ parameters (par file or ff)" % g.name)
+        types = list(g.mol.ffatypes)
+        tables = torch.empty((len(types), 8) + tuple(fine_n), dtype=torch.float64, device='cuda')
+        for k, t in enumerate(types):
+            sg, eg = g.ff[t]
+            E.external_potential_derivatives(rv, fine_n, fine_sp, pos, ids, sig, eps, sg, eg, self.cutoff,
+                                             self.DERIV_VMAX, out=tables[k])
+        origin = self.grid.points[0, 0, 0, :3]
+        spacing = np.array([1.0, 1.0, 1.0]) * self.INTERP_SPACING
+        V = E.effective_potential_interpolated(self.grid.plan, tables, g.mol.ffatype_ids, origin, spacing,
+                                               g.mol.pos, g.mol.masses, rot, w, beta, self.limit_potential)
+        del tables
+        return V
+
+    def generate_potential(self, temperature=None, rewrite=False):
+        """The potential on the grid, uncapped above limit_potential for
+        multi-site guests and capped for spherical ones (cap() caps both)."""
+        from .system import NonSphericalGuest
+        from .rotations import combined_rotations
+        pos, ids, sig, eps = self._host_arrays()
+        g = self.guest
+        if isinstance(g, NonSphericalGuest):
+            if temperature is None:
+                raise ValueError('Temperature must be provided for non-spherical particles')
+            beta = 1 / temperature / boltzmann
+            rot, w = combined_rotations(self.degree)
+            if self.interpolate:
+                self._V = self._interpolated(pos, ids, sig, eps, rot, w, beta)
+            else:
+                ssig, seps = g.site_parameters()
+                self._V = E.effective_potential(self.grid.plan, pos, ids, sig, eps, g.mol.pos, g.mol.masses, ssig,
+                                                seps, rot, w, self.cutoff, beta, self.limit_potential)
+        else:
+            self._V = E.external_potential(self.grid.plan, pos, ids, sig, eps, g.sigma, g.epsilon, self.cutoff,
+                                           self.limit_potential)
 
     def cap(self):
         torch = _torch()

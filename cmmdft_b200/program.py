@@ -17,6 +17,9 @@ from .units import angstrom, boltzmann
 
 __all__ = ['Program']
 
+# Solver.lower_density (cmmdft/solver.py:83): the clip of the solvers' tracking lines
+LOWER_DENSITY = 1e-12
+
 
 class Program(object):
     def __init__(self, prefix='', hostname='', guestname='', ff_suffix='', funct_suffix='', grid_suffix='',
@@ -107,11 +110,13 @@ class Program(object):
             return self.grid.integrate(rho), rho, True
         self._set_initial_density(Ninit=Ninit, chempot=chempot, rewrite=rewrite,
                                   temperature=self.fener.temperature, silent=silent)
-        if energy_tracking:   # the start density's line (the reference writes one per step)
-            self.fener.track(chempot, self.rho0, step=0)
+        # the start density's line, as the solver writes it (solver.py:103-127;
+        # the reference's solvers add one line per step)
+        if energy_tracking:
+            self.fener.track(chempot, self.rho0, step=0, lower_density=LOWER_DENSITY)
         N, rho, converged = self.solver.solve(chempot, self.rho0.copy(), 2)
         if energy_tracking:   # the final density's line
-            self.fener.track(chempot, rho, step=self.solver.curr_step)
+            self.fener.track(chempot, rho, step=self.solver.curr_step, lower_density=LOWER_DENSITY)
         if self.solver.track_history:
             fn = self.workdir / ('solving_history_%s.csv' % self.file_suffix)
             np.savetxt(fn, self.solver.history[:self.solver.curr_step + 1], delimiter=',',

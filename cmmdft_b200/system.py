@@ -19,7 +19,7 @@ from .units import angstrom, boltzmann, planck, parse_unit
 from .workload import hardsphere_radius
 
 __all__ = ['Cell', 'System', 'Host', 'NanoporousHost', 'EmptyHost', 'Guest', 'SphericalLJGuest',
-           'Grid', 'Spectrum', 'read_chk', 'read_pars_file']
+           'NonSphericalGuest', 'DualModelGuest', 'Grid', 'Spectrum', 'read_chk', 'read_pars_file']
 
 
 class Cell(object):
@@ -232,6 +232,86 @@ class SphericalLJGuest(Guest):
 
     def _calculate_hardsphere_radius(self, temperature, **kwargs):
         return hardsphere_radius(self.sigma, self.epsilon, temperature), self.sigma
+
+
+class _Molecule(object):
+    """The guest's atoms as the reference reads them from a yaff checkpoint
+    (positions in bohr, masses in atomic units, atom types)."""
+
+    def __init__(self, pos, masses, ffatypes, ffatype_ids):
+        self.pos = np.asarray(pos, dtype=np.float64).reshape(-1, 3).copy()
+        self.masses = None if masses is None else np.asarray(masses, dtype=np.float64).reshape(-1)
+        self.ffatypes = list(ffatypes)
+        self.ffatype_ids = np.asarray(ffatype_ids, dtype=np.int32).reshape(-1)
+
+    @property
+    def natom(self):
+        return len(self.pos)
+
+
+class NonSphericalGuest(Guest):
+    """Rigid multi-site guest (cmmdft/system.py:162-212).
+
+    Either ``chk`` (yaff text checkpoint with masses) and ``par`` (LJ:PARS
+    file of the guest's atom types) or the arrays ``pos`` (bohr),
+    ``masses``, ``ffatypes``, ``ffatype_ids`` and ``ff``
+    ({type: (sigma, epsilon)}) must be given.  The external potential of
+    such a guest is the orientation average of the LJ potentials of its
+    sites (ExternalPotential.generate_potential with a temperature).
+    """
+
+    def __init__(self, name, chk=None, par=None, pos=None, masses=None, ffatypes=None, ffatype_ids=None, ff=None):
+        self.chk, self.par = chk, par
+        if chk is not None:
+            d = read_chk(chk)
+            pos, ffatypes, ffatype_ids = d['pos'], list(d['ffatypes']), d['ffatype_ids']
+            m = d.get('masses')
+            masses = m if isinstance(m, np.ndarray) and m.size else None
+        if ff is None and par is not None:
+            ff = read_pars_file(par)
+        self.mol = _Molecule(pos, masses, ffatypes, ffatype_ids)
+        self.natom = self.mol.natom
+        self.ff = dict(ff) if ff is not None else None
+        if self.mol.masses is None:
+            raise ValueError('Masses not defined in guest chk file, cannot compute total mass for NonSphericalGuest')
+        Guest.__init__(self, name, self.mol.masses.sum())
+
+    def _arrays(self):
+        return dict(chk=self.chk, par=self.par, pos=self.mol.pos, masses=self.mol.masses,
+                    ffatypes=self.mol.ffatypes, ffatype_ids=self.mol.ffatype_ids, ff=self.ff)
+
+    def copy(self):
+        return type(self)(self.name, **self._arrays())
+
+    def site_parameters(self):
+        """(sigma, epsilon) per guest atom from the guest's LJ table."""
+        if self.ff is None:
+            raise ValueError("guest %s has no LJ parameters (par file or ff)" % self.name)
+        ids = self.mol.ffatype_ids
+        sig = np.array([self.ff[self.mol.ffatypes[t]][0] for t in ids])
+        eps = np.array([self.ff[self.mol.ffatypes[t]][1] for t in ids])
+        return sig, eps
+
+    def _calculate_hardsphere_radius(self, temperature, **kwargs):
+        raise NotImplementedError('Using generic NonSphericalGuest class, cannot compute hardsphere radius, '
+                                  'use DualModelGuest class')
+
+
+class DualModelGuest(SphericalLJGuest, NonSphericalGuest):
+    """Guest with a spherical LJ model (hard-sphere radius, attraction) and a
+    multi-site model (external potential), cmmdft/system.py:214-228."""
+
+    def __init__(self, name, mass, sigma, epsilon, chk=None, par=None, **arrays):
+        SphericalLJGuest.__init__(self, name, mass, sigma, epsilon)
+        NonSphericalGuest.__init__(self, name, chk, par, **arrays)
+
+    def copy(self):
+        a = self._arrays()
+        chk, par = a.pop('chk'), a.pop('par')
+        return type(self)(self.name, self.mass, self.sigma, self.epsilon, chk, par, **a)
+
+    def _calculate_hardsphere_radius(self, temperature, **kwargs):
+        return SphericalLJGuest._calculate_hardsphere_radius(self, temperature, **kwargs)
 
 
 class Spectrum(object):

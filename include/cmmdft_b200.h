@@ -179,6 +179,47 @@ int cmm_extpot_lj(const cmm_grid* grid, const double* d_pos, const int* d_type, 
  * sums them in bin order instead of file order (the same pairs; the sum's
  * rounding differs).  Process-wide, not per grid or thread. */
 int cmm_extpot_set_mode(int mode);
+/* Orientation-averaged external potential of a rigid multi-site guest.
+ * Replaces effective_potential_vectorized as generate_effective_potential
+ * calls it (cmmdft/extpot_calculator.py:569-655): at every grid point p the
+ * guest (guest_pos: nsite x 3 in its own frame, guest_mass: nsite) is moved
+ * to p, centred on its centre of mass, turned by each of the nrot matrices
+ * d_rot [nrot][3][3] (row-major, applied as R x) and put back; each site's LJ
+ * sum over the host atoms uses the site's own sigma/epsilon (guest_sig,
+ * guest_eps: nsite, mixed as in cmm_extpot_lj).  Site potentials are
+ * rounded to float32 and summed there, scaled by float32(-beta), and the
+ * weighted log-sum-exp over rotations (weights d_w [nrot]) is taken in
+ * float64 as scipy.special.logsumexp does; d_V = -lse / beta, NaN ->
+ * v_limit.  No cap is applied (the caller caps as cmm_extpot_lj does).
+ * nsite <= 8, nsite * ntype <= 128, nrot <= 6144.  Synchronous. */
+int cmm_extpot_rot(const cmm_grid* grid, const double* d_pos, const int* d_type, int natom,
+                   const double* d_type_sig, const double* d_type_eps, int ntype,
+                   const double* guest_pos, const double* guest_mass, const double* guest_sig,
+                   const double* guest_eps, int nsite, const double* d_rot, const double* d_w, int nrot,
+                   double cutoff, double beta, double v_limit, double* d_V, void* stream);
+/* LJ potential and derivatives of one guest atom type on an n1 x n2 x n3
+ * grid over the cell (rvecs row-major, points as Grid.points), the eight
+ * channels of get_external_potential_derivatives
+ * (cmmdft/extpot_calculator.py:264-338): V, dV/dx, dV/dy, dV/dz, d2V/dxdy,
+ * d2V/dxdz, d2V/dydz, d3V/dxdydz, with V and the first derivatives clipped
+ * to +-v_max (the reference uses 1e6 kJ/mol), the cross derivatives zeroed
+ * where V > v_max, and the derivatives scaled by the axes' `spacings`.
+ * d_out: [8][n1][n2][n3].  Synchronous. */
+int cmm_extpot_lj_deriv(const double* rvecs, int n1, int n2, int n3, const double* spacings,
+                        const double* d_pos, const int* d_type, int natom, const double* d_type_sig,
+                        const double* d_type_eps, int ntype, double guest_sig, double guest_eps,
+                        double cutoff, double v_max, double* d_out, void* stream);
+/* cmm_extpot_rot with each site potential interpolated tricubically
+ * (Interpolator.tricubic_interpolation, cmmdft/extpot_calculator.py:391-549)
+ * from channel tables d_tab [ntab][8][fine_n0][fine_n1][fine_n2] (as
+ * cmm_extpot_lj_deriv writes them); site s reads table site_tab[s]; the cell
+ * of a site position q is floor((q - origin) / spacing) with periodic
+ * corner indices.  Replaces ExternalPotential.generate_potential with
+ * interpolate=True (cmmdft/functionals.py:1032-1055).  Synchronous. */
+int cmm_extpot_rot_interp(const cmm_grid* grid, const double* d_tab, int ntab, const int* fine_n,
+                          const double* origin, const double* spacing, const double* guest_pos,
+                          const double* guest_mass, const int* site_tab, int nsite, const double* d_rot,
+                          const double* d_w, int nrot, double beta, double v_limit, double* d_V, void* stream);
 
 /* Unnormalised 3D real-to-half-complex FFT and its inverse in the plan's
  * spectrum layout (scipy.fft.fftn / ifftn*N as used by Grid.fft/ifft,

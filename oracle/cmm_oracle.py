@@ -142,6 +142,160 @@ def external_potential(points, ff, sig_g, eps_g, pos, ffatypes, ffatype_ids, rve
     return Vext
 
 
+def effective_potential(points, guest_pos, guest_masses, site_sigma, site_epsilon, rotations, weights, beta,
+                        ff, pos, ffatypes, ffatype_ids, rvecs, cutoff=12 * angstrom,
+                        limit_potential=1e4 * kjmol):
+    """Orientation-averaged potential of a rigid multi-site guest at
+    ``points`` [m, 3] (effective_potential_vectorized as
+    generate_effective_potential calls it, cmmdft/extpot_calculator.py:
+    569-655): the guest moved to each point and centred on its centre of
+    mass, each rotation applied about it, the site potentials (the host-atom
+    LJ sum of external_potential with the site's own sigma/epsilon) stored in
+    float32 and summed there, then -logsumexp(-beta pot, b=weights) / beta,
+    NaN -> limit_potential.  ``pos`` must already be recentred."""
+    from scipy.special import logsumexp
+    m, nsite, nrot = len(points), len(guest_pos), len(rotations)
+    masses = np.asarray(guest_masses, dtype=np.float64).reshape(nsite, 1)
+    neutral = guest_pos[None, :, :] + points[:, None, :]
+    com = np.sum(neutral * masses[None, :, :], axis=1) / np.sum(masses)
+    rel = neutral - com[:, None, :]
+    rotated = np.einsum('rij,mnj->mnri', rotations, rel) + com[:, None, None, :]
+    pot = np.zeros((m, nsite, nrot), dtype=np.float32)
+    for a in range(nsite):
+        coords = rotated[:, a, :, :].reshape(m * nrot, 3)
+        pot[:, a, :] = external_potential(coords, ff, site_sigma[a], site_epsilon[a], pos, ffatypes, ffatype_ids,
+                                          rvecs, cutoff).reshape(m, nrot)
+    pot = np.sum(pot, axis=1)
+    res = -logsumexp(-float(beta) * pot, b=weights, axis=1) / beta
+    return np.where(np.isnan(res), limit_potential, res)
+
+
+def lennard_jones_derivatives(r, sigma, epsilon, cutoff):
+    """V and the radial factors dV, ddV, dddV of lennard_jones(derivative=True)
+    (cmmdft/extpot_calculator.py:156-183)."""
+    inside = r < cutoff
+    V, dV, ddV, dddV = (np.zeros_like(r) for _ in range(4))
+    ri = r[inside]
+    r6 = (sigma / ri) ** 6
+    r12 = r6 * r6
+    rc6 = (sigma / cutoff) ** 6
+    V[inside] = 4 * epsilon * (r12 - r6) - 4 * epsilon * (rc6 ** 2 - rc6)
+    dV[inside] = 24 * epsilon * (r6 - 2 * r12) / ri ** 2
+    ddV[inside] = 96 * epsilon * (7 * r12 - 2 * r6) / ri ** 4
+    dddV[inside] = 384 * epsilon * (5 * r6 - 28 * r12) / ri ** 6
+    return V, dV, ddV, dddV
+
+
+def external_potential_derivatives(points, ff, sig_g, eps_g, pos, ffatypes, ffatype_ids, rvecs, spacings,
+                                   cutoff=12 * angstrom):
+    """[8, m]: V, dV/dx, dV/dy, dV/dz, d2V/dxdy, d2V/dxdz, d2V/dydz, d3V/dxdydz
+    at ``points`` in the unit-cube scaling of a grid with ``spacings``, with
+    the clipping of get_external_potential_derivatives
+    (cmmdft/extpot_calculator.py:264-338).  ``pos`` must already be recentred."""
+    n = len(points)
+    out = np.zeros((8, n))
+    X, Y, Z = points.T
+    L = np.linalg.norm(rvecs, axis=1)
+    for i, tid in enumerate(ffatype_ids):
+        s, e = ff[ffatypes[tid]]
+        sm = 0.5 * (s + sig_g)
+        em = np.sqrt(e * eps_g)
+        rx = X - pos[i, 0]
+        ry = Y - pos[i, 1]
+        rz = Z - pos[i, 2]
+        rx -= L[0] * (rx / L[0]).round()
+        ry -= L[1] * (ry / L[1]).round()
+        rz -= L[2] * (rz / L[2]).round()
+        R = np.sqrt(rx ** 2 + ry ** 2 + rz ** 2 + 1e-16)
+        V, dV, ddV, dddV = lennard_jones_derivatives(R, sm, em, cutoff)
+        out[0] += V
+        out[1] += dV * rx
+        out[2] += dV * ry
+        out[3] += dV * rz
+        out[4] += ddV * rx * ry
+        out[5] += ddV * rx * rz
+        out[6] += ddV * ry * rz
+        out[7] += dddV * rx * ry * rz
+    vmax = 1e+6 * kjmol
+    mask = out[0] > vmax
+    for c in range(4):
+        out[c] = np.clip(out[c], -vmax, vmax)
+    out[4:, mask] = 0.0
+    dx, dy, dz = spacings
+    for c, f in ((1, dx), (2, dy), (3, dz), (4, dx * dy), (5, dx * dz), (6, dy * dz), (7, dx * dy * dz)):
+        out[c] *= f
+    return out
+
+
+# corner offsets and derivative orders of the tricubic scheme
+# (cmmdft/extpot_calculator.py:408-413 and the channel order above)
+TRICUBIC_CORNERS = ((0, 0, 0), (1, 0, 0), (0, 1, 0), (1, 1, 0), (0, 0, 1), (1, 0, 1), (0, 1, 1), (1, 1, 1))
+TRICUBIC_ORDERS = ((0, 0, 0), (1, 0, 0), (0, 1, 0), (0, 0, 1), (1, 1, 0), (1, 0, 1), (0, 1, 1), (1, 1, 1))
+
+
+def _hermite(c, o, t):
+    """Cubic Hermite basis on [0, 1]: value (o = 0) or slope (o = 1) at end c."""
+    if o == 0:
+        return (1 - t) ** 2 * (1 + 2 * t) if c == 0 else t * t * (3 - 2 * t)
+    return t * (1 - t) ** 2 if c == 0 else t * t * (t - 1)
+
+
+def tricubic(deriv_at, positions, origin, spacing, npoints):
+    """Interpolator.tricubic_interpolation (cmmdft/extpot_calculator.py:
+    391-549) of the channel values that ``deriv_at(idx [m, 3]) -> [8, m]``
+    gives at fine-grid indices: cell of each position by floor((p - origin)
+    / spacing), periodic corner indices, and the tricubic polynomial fixed by
+    the 64 corner values -- the tensor product of cubic Hermite interpolants,
+    which is what the reference's 64 x 64 matrix encodes."""
+    s = (positions - origin) / spacing
+    ix = np.floor(s).astype(int)
+    r = s - ix
+    npoints = np.asarray(npoints)
+    res = np.zeros(len(positions))
+    for (cx, cy, cz) in TRICUBIC_CORNERS:
+        idx = (ix + np.array([cx, cy, cz])) % npoints
+        vals = deriv_at(idx)
+        for d, (ox, oy, oz) in enumerate(TRICUBIC_ORDERS):
+            res += vals[d] * _hermite(cx, ox, r[:, 0]) * _hermite(cy, oy, r[:, 1]) * _hermite(cz, oz, r[:, 2])
+    return res
+
+
+def interpolated_effective_potential(points, guest_pos, guest_masses, site_types, type_params, rotations, weights,
+                                     beta, ff, pos, ffatypes, ffatype_ids, rvecs, fine_npoints, origin, spacing,
+                                     cutoff=12 * angstrom, limit_potential=1e4 * kjmol):
+    """The orientational average of ``effective_potential`` with the site
+    potentials interpolated tricubically from per-type derivative grids
+    (ExternalPotential.generate_potential(interpolate=True),
+    cmmdft/functionals.py:1032-1055): the fine grid has ``fine_npoints`` points
+    per axis over the cell (Grid points, spacing |a_i| / n_i), the
+    interpolator takes ``origin`` and ``spacing``.  Channel values are
+    computed at the corners that are needed only."""
+    from scipy.special import logsumexp
+    fine_npoints = np.asarray(fine_npoints)
+    fine_sp = np.linalg.norm(rvecs, axis=0) / fine_npoints          # Grid.spacings (columns)
+    m, nsite, nrot = len(points), len(guest_pos), len(rotations)
+    masses = np.asarray(guest_masses, dtype=np.float64).reshape(nsite, 1)
+    neutral = guest_pos[None, :, :] + points[:, None, :]
+    com = np.sum(neutral * masses[None, :, :], axis=1) / np.sum(masses)
+    rel = neutral - com[:, None, :]
+    rotated = np.einsum('rij,mnj->mnri', rotations, rel) + com[:, None, None, :]
+    pot = np.zeros((m, nsite, nrot), dtype=np.float32)
+
+    def grid_points(idx):
+        g = idx * (1.0 / fine_npoints) + (-0.5)     # linspace(-0.5, 0.5, n, endpoint=False)[i]
+        return np.einsum('ab,ia->ib', rvecs, g)
+
+    for a in range(nsite):
+        sg, eg = type_params[site_types[a]]
+        at = lambda idx: external_potential_derivatives(grid_points(idx), ff, sg, eg, pos, ffatypes, ffatype_ids,
+                                                        rvecs, fine_sp, cutoff)
+        coords = rotated[:, a, :, :].reshape(m * nrot, 3)
+        pot[:, a, :] = tricubic(at, coords, origin, spacing, fine_npoints).reshape(m, nrot)
+    pot = np.sum(pot, axis=1)
+    res = -logsumexp(-float(beta) * pot, b=weights, axis=1) / beta
+    return np.where(np.isnan(res), limit_potential, res)
+
+
 def cap_potential(V, limit):
     """cmmdft/functionals.py:247-251 (non-finite and > limit -> limit)."""
     V = V.copy()

@@ -26,3 +26,15 @@ def golden64():
     if not os.path.exists(path):
         pytest.skip("64^3 golden fixture not generated")
     return dict(np.load(path))
+
+
+@pytest.fixture(scope="session")
+def golden_rot():
+    import numpy as np
+    return dict(np.load(os.path.join(ROOT, "tests", "golden", "rot20.npz")))
+
+
+@pytest.fixture(scope="session")
+def golden_rotinterp():
+    import numpy as np
+    return dict(np.load(os.path.join(ROOT, "tests", "golden", "rotinterp12.npz")))

@@ -9,6 +9,8 @@ machines):
     python tests/golden/make_golden.py --reference <reference tree> --dropin
     python tests/golden/make_golden.py --reference <reference tree> --uneven
     python tests/golden/make_golden.py --reference <reference tree> --lda
+    python tests/golden/make_golden.py --reference <reference tree> --rot
+    python tests/golden/make_golden.py --reference <reference tree> --rotinterp
 
 ``--reference`` (or the environment variable CMM_REFERENCE_ROOT) names the
 root of the reference's source tree, the directory that holds ``cmmdft/``.
@@ -52,7 +54,23 @@ Outputs (small ``.npz`` files) land next to this script:
               GPU), at 0.1, 1 and 10 bar: N, Omega, steps (``--uneven``).
   lda32.npz       the 32^3 case with an LDA part (SumOfEOS of MBWR, CS and
               the mean-field EOS): part values, the LDA derivative, C1 and
-              Omega of the two profiles, three static Picard steps (``--lda``).
+              Omega of the two profiles, three static Picard steps and their
+              rounding floor (the same steps from a start one ulp above)
+              (``--lda``).
+  rot20.npz       the orientation-averaged external potential of rigid CO2
+              (the reference's InputFiles/Guest/CO2 struct_AA.chk and
+              pars_vdw_AA_trappe.txt) in the 32^3 case's host on a 20^3
+              grid at 300 K, from the reference's own
+              generate_effective_potential and get_external_potential_dict
+              (their file readers answered from memory), at Lebedev degrees 9
+              and 11; with the reference's rotation matrices and weights and
+              the guest's arrays (``--rot``).
+  rotinterp12.npz the same guest and host through the reference's
+              ExternalPotential.generate_potential(interpolate=True) on a
+              12^3 grid at Lebedev degree 9 (derivative grids at 0.15 A,
+              tricubic interpolation), with the channel values of
+              get_external_potential_derivatives at 3000 seeded points of
+              each type's derivative grid (``--rotinterp``).
   iso64_rho.npz   the converged densities of that isotherm at the pressure
               indices ISO_RHO_IDX, and the reference run against itself: the
               same points re-solved from a start perturbed by one ulp, with
@@ -218,6 +236,12 @@ def lda32(args):
     s = solver.Picard(b['prog'], nsteps=3, alpha_mix=0.1, method='static', criterion='res', threshold=1e-8)
     N, rho, conv = quiet(s.solve, mu, rho_a.copy(), 3)
     out.update(picard3_rho=rho, picard3_N=N)
+    # the reference against itself from a start one ulp above: the rounding
+    # floor of the three-step trajectory
+    s2 = solver.Picard(b['prog'], nsteps=3, alpha_mix=0.1, method='static', criterion='res', threshold=1e-8)
+    N2, rho2, _ = quiet(s2.solve, mu, np.nextafter(rho_a, np.inf), 3)
+    out['picard3_floor'] = np.max(np.abs(rho2 - rho)) / np.max(np.abs(rho))
+    out['picard3_N_floor'] = abs(N2 - N) / abs(N)
     np.savez_compressed(os.path.join(HERE, 'lda32.npz'), **out)
     print('wrote lda32.npz', {k: v for k, v in out.items() if np.ndim(v) == 0})
 
@@ -480,6 +504,121 @@ def iso64(args):
     print('wrote iso64_rho.npz')
 
 
+def rot20(args):
+    """Effective potential of rigid CO2 from the reference's own code."""
+    ref = import_reference(args.reference)
+    system, extpot = ref[0], ref[3]
+    import yaff
+    from cmmdft_b200.system import read_chk, read_pars_file
+    from cmmdft_b200.hosts import cubic_host_276
+    from cmmdft_b200.units import angstrom, boltzmann
+    gdir = os.path.join(args.reference, 'InputFiles', 'Guest', 'CO2')
+    g = read_chk(os.path.join(gdir, 'struct_AA.chk'))
+    gff = read_pars_file(os.path.join(gdir, 'pars_vdw_AA_trappe.txt'))
+    host = cubic_host_276(0)
+    files = {
+        'host.chk': lambda: yaff.System(pos=host.pos.copy(), ffatypes=host.ffatypes,
+                                        ffatype_ids=host.ffatype_ids, rvecs=host.rvecs),
+        'guest.chk': lambda: yaff.System(pos=g['pos'].copy(), ffatypes=list(g['ffatypes']),
+                                         ffatype_ids=g['ffatype_ids'], masses=g['masses'].copy()),
+    }
+    pars = {'host.par': dict(host.ff), 'guest.par': dict(gff)}
+
+    class _System(object):          # System.from_file of the shim cannot read checkpoints
+        from_file = staticmethod(lambda fn: files[fn]())
+    extpot.System = _System
+    extpot.read_pars_file = lambda fn: pars[fn]
+    epot_dict = extpot.get_external_potential_dict('host.par', 'guest.par', 'host.chk', cutoff=12 * angstrom)
+    n, T = 20, 300.0
+    grid = system.Grid(files['host.chk']().cell, npoints=n)
+    out = dict(T=T, n=n, guest_pos=g['pos'], guest_masses=g['masses'], guest_ffatypes=np.array(g['ffatypes']),
+               guest_ffatype_ids=g['ffatype_ids'],
+               guest_sigma=np.array([gff[t][0] for t in g['ffatypes']]),
+               guest_epsilon=np.array([gff[t][1] for t in g['ffatypes']]))
+    # the reference reads its Lebedev tables relative to the working directory
+    cwd = os.getcwd()
+    tmp = tempfile.mkdtemp(prefix='cmm_rot_')
+    os.symlink(os.path.abspath(args.reference), os.path.join(tmp, 'CmmDFT'))
+    os.chdir(tmp)
+    try:
+        for deg in (9, 11):
+            t0 = time.time()
+            V = extpot.generate_effective_potential('guest.chk', grid.points[..., :3], 1 / T / boltzmann, epot_dict,
+                                                    degree=deg)
+            print('degree %d: %.1f s, V in [%.4g, %.4g]' % (deg, time.time() - t0, np.nanmin(V), np.nanmax(V)))
+            R1, w1 = extpot.generate_rotation_matrix(deg, 3)
+            R2, w2 = extpot.generate_rotation_matrix(deg, 2)
+            out['V%d' % deg] = V
+            out['rot%d' % deg] = np.einsum('aij,bjk->abij', R1, R2).reshape(-1, 3, 3)
+            out['w%d' % deg] = np.repeat(w1 * w2, len(R2))
+    finally:
+        os.chdir(cwd)
+    np.savez_compressed(os.path.join(HERE, 'rot20.npz'), **out)
+
+
+def rotinterp12(args):
+    """Tricubic-interpolated effective potential of rigid CO2 from the
+    reference's own ExternalPotential.generate_potential(interpolate=True)."""
+    ref = import_reference(args.reference)
+    system, functionals, extpot = ref[0], ref[1], ref[3]
+    import yaff
+    from cmmdft_b200.system import read_chk, read_pars_file
+    from cmmdft_b200.hosts import cubic_host_276
+    from cmmdft_b200.units import angstrom, kjmol
+    gdir = os.path.join(args.reference, 'InputFiles', 'Guest', 'CO2')
+    g = read_chk(os.path.join(gdir, 'struct_AA.chk'))
+    gff = read_pars_file(os.path.join(gdir, 'pars_vdw_AA_trappe.txt'))
+    host = cubic_host_276(0)
+    guest_mol = lambda: yaff.System(pos=g['pos'].copy(), ffatypes=list(g['ffatypes']),
+                                    ffatype_ids=g['ffatype_ids'], masses=g['masses'].copy())
+    pars = {'host.par': dict(host.ff), 'guest.par': dict(gff)}
+
+    class _System(object):          # System.from_file of the shim cannot read checkpoints
+        from_file = staticmethod(lambda fn: guest_mol())
+    extpot.System = _System
+    extpot.read_pars_file = functionals.read_pars_file = lambda fn: pars[fn]
+    mol = yaff.System(pos=host.pos.copy(), ffatypes=host.ffatypes, ffatype_ids=host.ffatype_ids, rvecs=host.rvecs)
+    mol.pos -= mol.pos.sum(axis=0) / len(mol.pos)  # as system.py:70
+    h = system.NanoporousHost.__new__(system.NanoporousHost)
+    system.Host.__init__(h, 'synthetic', mol.cell)
+    h.mol, h.chk, h.par = mol, 'host.chk', 'host.par'
+    gu = system.NonSphericalGuest.__new__(system.NonSphericalGuest)
+    system.Guest.__init__(gu, 'CO2', g['masses'].sum())
+    gu.mol, gu.natom, gu.chk, gu.par = guest_mol(), 3, 'guest.chk', 'guest.par'
+    syst = system.System(h, gu)
+    n, T, deg = 12, 300.0, 9
+    grid = system.Grid(mol.cell, npoints=n)
+    tmp = tempfile.mkdtemp(prefix='cmm_rotinterp_')
+    ep = functionals.ExternalPotential(grid, syst, tmp, limit_potential=1e4 * kjmol, degree=deg, interpolate=True,
+                                       cutoff=12 * angstrom)
+    cwd = os.getcwd()
+    os.symlink(os.path.abspath(args.reference), os.path.join(tmp, 'CmmDFT'))
+    os.chdir(tmp)
+    try:
+        t0 = time.time()
+        quiet(ep.generate_potential, T)
+        print('interpolated potential: %.1f s' % (time.time() - t0))
+    finally:
+        os.chdir(cwd)
+    fine = system.Grid(mol.cell, spacing=0.15 * angstrom)
+    out = dict(T=T, n=n, degree=deg, V=ep.potential, fine_npoints=np.array(fine.npoints),
+               fine_spacings=np.array(fine.spacings), origin=grid.points[0, 0, 0, :3],
+               interp_spacing=np.array([0.15, 0.15, 0.15]) * angstrom,
+               guest_pos=g['pos'], guest_masses=g['masses'], guest_ffatypes=np.array(g['ffatypes']),
+               guest_ffatype_ids=g['ffatype_ids'],
+               guest_sigma=np.array([gff[t][0] for t in g['ffatypes']]),
+               guest_epsilon=np.array([gff[t][1] for t in g['ffatypes']]))
+    rng = np.random.default_rng(17)
+    idx = np.stack([rng.integers(0, m, 3000) for m in fine.npoints], axis=1)
+    out['deriv_idx'] = idx
+    pts = fine.points[idx[:, 0], idx[:, 1], idx[:, 2], :3]
+    for t in g['ffatypes']:
+        sg, eg = gff[t]
+        out['deriv_' + t] = extpot.get_external_potential_derivatives(pts, host.ff, sg, eg, mol, fine.spacings,
+                                                                      cutoff=12 * angstrom)
+    np.savez_compressed(os.path.join(HERE, 'rotinterp12.npz'), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--reference', default=os.environ.get('CMM_REFERENCE_ROOT'),
@@ -491,6 +630,8 @@ def main():
     ap.add_argument('--dropin', action='store_true')
     ap.add_argument('--uneven', action='store_true')
     ap.add_argument('--lda', action='store_true')
+    ap.add_argument('--rot', action='store_true')
+    ap.add_argument('--rotinterp', action='store_true')
     ap.add_argument('--procs', type=int, default=8)
     args = ap.parse_args()
     if not args.reference:
@@ -505,6 +646,10 @@ def main():
         return uneven(args)
     if args.lda:
         return lda32(args)
+    if args.rot:
+        return rot20(args)
+    if args.rotinterp:
+        return rotinterp12(args)
     ref = import_reference(args.reference)
     solver = ref[2]
     from cmmdft_b200.hosts import cubic_host_276, HELIUM

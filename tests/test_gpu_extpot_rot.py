@@ -1,0 +1,166 @@
+"""Orientation-averaged external potential of a rigid multi-site guest
+(cmm_extpot_rot) against the unmodified reference: rigid CO2 (TraPPE) in the
+276-atom host on a 20^3 grid at 300 K, Lebedev degrees 9 and 11
+(tests/golden/rot20.npz, from the reference's own
+generate_effective_potential).
+
+The reference stores site potentials in float32, so a rounding difference in
+a float64 site sum can move a float32 value by one unit in the last place;
+tolerance: per point 1e-6 relative (float32 has 6e-8) with an absolute floor
+of 1e-12 Hartree, non-finite values (sites inside host atoms) where the
+reference has them, and after the capping of add_external_potential 1e-9 of
+the cap."""
+import os
+
+import numpy as np
+import pytest
+
+torch = pytest.importorskip("torch")
+
+pytestmark = pytest.mark.gpu
+
+import cmmdft_b200 as cd
+from cmmdft_b200 import engine as E
+from cmmdft_b200 import workload as W
+from cmmdft_b200.hosts import cubic_host_276
+from cmmdft_b200.rotations import combined_rotations
+from cmmdft_b200.units import angstrom, boltzmann, kjmol
+
+CAP = 1e4 * kjmol
+
+
+@pytest.fixture(scope="module")
+def cuda():
+    if not torch.cuda.is_available():
+        pytest.skip("no CUDA device")
+    return True
+
+
+def site_params(ref):
+    ids = ref["guest_ffatype_ids"]
+    return ref["guest_sigma"][ids], ref["guest_epsilon"][ids]
+
+
+def compare(V, Vr):
+    fin = np.isfinite(Vr)
+    assert np.array_equal(np.isfinite(V), fin)
+    mod = fin & (np.abs(Vr) < CAP)
+    d = np.abs(V[mod] - Vr[mod])
+    rel = float(np.max(d / (np.abs(Vr[mod]) + 1e-12 / 1e-6)))
+    exact = int(np.sum(V == Vr))
+    cap = lambda a: np.minimum(np.where(np.isfinite(a), a, CAP), CAP)
+    capped = float(np.max(np.abs(cap(V) - cap(Vr)))) / CAP
+    return rel, capped, exact
+
+
+@pytest.mark.parametrize("deg", [9, 11])
+@pytest.mark.parametrize("rotations", ["reference", "package"])
+def test_effective_potential_against_reference(cuda, golden_rot, deg, rotations):
+    ref = golden_rot
+    h = cubic_host_276(0)
+    n = int(ref["n"])
+    plan = E.GridPlan((n, n, n), h.rvecs)
+    sig, eps = W.host_type_arrays(h)
+    ss, se = site_params(ref)
+    rot, w = (ref["rot%d" % deg], ref["w%d" % deg]) if rotations == "reference" else combined_rotations(deg)
+    V = E.effective_potential(plan, h.recentred_pos(), h.ffatype_ids, sig, eps, ref["guest_pos"],
+                              ref["guest_masses"], ss, se, rot, w, 12 * angstrom, 1 / float(ref["T"]) / boltzmann,
+                              CAP).cpu().numpy()
+    rel, capped, exact = compare(V, ref["V%d" % deg])
+    print("CO2 degree %d, %s rotations: max rel %.2e, capped %.2e of the cap, %d of %d bit-identical"
+          % (deg, rotations, rel, capped, exact, V.size))
+    assert rel < 1e-6 and capped < 1e-9
+
+
+def test_dual_model_guest_through_program(cuda, golden_rot, tmp_path):
+    """Program -> FreeEnergy.add_external_potential(temperature=T, degree=11)
+    with a DualModelGuest: the capped potential against the reference's, the
+    eff_epot_<T>K.npy file in the reference's directory layout, a second
+    Program served from it, and set_temperature generating the potential of
+    a new temperature (functionals.py:213-251, 1019-1025)."""
+    ref = golden_rot
+    h = cubic_host_276(0)
+    types = [str(t) for t in ref["guest_ffatypes"]]
+    ff = {t: (s, e) for t, s, e in zip(types, ref["guest_sigma"], ref["guest_epsilon"])}
+    T = float(ref["T"])
+
+    def program():
+        host = cd.NanoporousHost('synthetic', pos=h.pos, ffatypes=h.ffatypes, ffatype_ids=h.ffatype_ids,
+                                 rvecs=h.rvecs, ff=h.ff, masses=h.masses)
+        guest = cd.DualModelGuest('CO2', 44.0 * cd.amu, 3.9 * angstrom, 200 * boltzmann, pos=ref["guest_pos"],
+                                  masses=ref["guest_masses"], ffatypes=types, ffatype_ids=ref["guest_ffatype_ids"],
+                                  ff=ff)
+        prog = cd.Program(prefix=str(tmp_path), hostname='synthetic', guestname='CO2', ff_suffix='trappe')
+        prog.set_system(host, guest)
+        prog.set_grid(npoints=int(ref["n"]))
+        prog.init_free_energy(T)
+        prog.fener.add_hard_sphere(version='WBII')
+        prog.fener.add_external_potential(temperature=T, cutoff=12 * angstrom, degree=11)
+        return prog
+
+    prog = program()
+    ext = prog.fener.part_dict['ExtPot']
+    V300 = ext.potential.copy()
+    Vr = ref["V11"]
+    Vr_c = np.minimum(np.where(np.isfinite(Vr), Vr, CAP), CAP)
+    err = float(np.max(np.abs(ext.potential - Vr_c))) / CAP
+    print("DualModelGuest through Program: %.2e of the cap" % err)
+    assert err < 1e-9
+    fn = tmp_path / 'synthetic' / 'CO2' / 'trappe' / '' / '' / 'eff_epot_300.00K.npy'
+    assert fn.is_file() and (prog.workdir / 'ExtPots').is_symlink()
+    again = program()                                    # loaded from the file
+    assert np.array_equal(again.fener.part_dict['ExtPot'].potential, ext.potential)
+    prog.fener.set_temperature(350.0)                    # a new temperature: generated and written
+    assert (tmp_path / 'synthetic' / 'CO2' / 'trappe' / 'eff_epot_350.00K.npy').is_file()
+    V350 = prog.fener.part_dict['ExtPot'].potential
+    assert np.all(V350 <= CAP) and not np.array_equal(V350, V300)
+
+
+def test_derivative_channels_against_reference(cuda, golden_rotinterp):
+    """cmm_extpot_lj_deriv on the 0.15 A grid (114^3) against the reference's
+    get_external_potential_derivatives at 3000 seeded points per guest atom
+    type: 1e-12 of each channel's largest magnitude there."""
+    ref = golden_rotinterp
+    h = cubic_host_276(0)
+    sig, eps = W.host_type_arrays(h)
+    fn = [int(x) for x in ref["fine_npoints"]]
+    idx = ref["deriv_idx"]
+    for t, s, e in zip(ref["guest_ffatypes"], ref["guest_sigma"], ref["guest_epsilon"]):
+        d = E.external_potential_derivatives(h.rvecs, fn, ref["fine_spacings"], h.recentred_pos(), h.ffatype_ids,
+                                             sig, eps, s, e, 12 * angstrom, 1e6 * kjmol)
+        got = d[:, idx[:, 0], idx[:, 1], idx[:, 2]].cpu().numpy()
+        r = ref["deriv_" + str(t)]
+        errs = [float(np.max(np.abs(got[c] - r[c])) / max(np.max(np.abs(r[c])), 1e-300)) for c in range(8)]
+        print("channels of %s: %s" % (t, " ".join("%.1e" % x for x in errs)))
+        assert max(errs) < 1e-12
+
+
+def test_interpolated_potential_through_program(cuda, golden_rotinterp, tmp_path):
+    """add_external_potential(temperature=T, degree=9, interpolate=True) with a
+    NonSphericalGuest on the 12^3 grid against the reference's
+    ExternalPotential.generate_potential(interpolate=True), capped as
+    add_external_potential caps: 1e-9 of the cap, and per point 1e-6
+    relative below the cap."""
+    ref = golden_rotinterp
+    h = cubic_host_276(0)
+    types = [str(t) for t in ref["guest_ffatypes"]]
+    ff = {t: (s, e) for t, s, e in zip(types, ref["guest_sigma"], ref["guest_epsilon"])}
+    host = cd.NanoporousHost('synthetic', pos=h.pos, ffatypes=h.ffatypes, ffatype_ids=h.ffatype_ids, rvecs=h.rvecs,
+                             ff=h.ff)
+    guest = cd.DualModelGuest('CO2', 44.0 * cd.amu, 3.9 * angstrom, 200 * boltzmann, pos=ref["guest_pos"],
+                              masses=ref["guest_masses"], ffatypes=types, ffatype_ids=ref["guest_ffatype_ids"], ff=ff)
+    prog = cd.Program(prefix=str(tmp_path), hostname='synthetic', guestname='CO2')
+    prog.set_system(host, guest)
+    prog.set_grid(npoints=int(ref["n"]))
+    prog.init_free_energy(float(ref["T"]))
+    prog.fener.add_external_potential(temperature=float(ref["T"]), cutoff=12 * angstrom, degree=int(ref["degree"]),
+                                      interpolate=True)
+    V = prog.fener.part_dict['ExtPot'].potential
+    Vr = ref["V"]
+    Vr_c = np.minimum(np.where(np.isfinite(Vr), Vr, CAP), CAP)
+    err = float(np.max(np.abs(V - Vr_c))) / CAP
+    mod = np.abs(Vr_c) < CAP
+    rel = float(np.max(np.abs(V[mod] - Vr_c[mod]) / (np.abs(Vr_c[mod]) + 1e-6)))
+    print("interpolated CO2 potential: %.2e of the cap, %.2e relative, %d of %d bit-identical"
+          % (err, rel, int(np.sum(V == Vr_c)), V.size))
+    assert err < 1e-9 and rel < 1e-6

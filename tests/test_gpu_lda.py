@@ -5,7 +5,8 @@ drop-in API against the unmodified reference (tests/golden/lda32.npz): the
 machinery with weight 1.  Tolerances as the other C1 checks: beta |dC1| at
 the reference's WBII noise floor (2e-9 ideal gas, 1e-7 dense), the LDA
 derivative alone 1e-12 relative, free-energy parts and Omega 1e-11, three
-static Picard steps 1e-10."""
+static Picard steps 1e-10 (N) and max(1e-10, 3 x the reference's own floor on
+that trajectory) for rho."""
 import os
 
 import numpy as np
@@ -65,7 +66,13 @@ def test_lda_part_against_reference(golden32, tmp_path):
         st = buf.stats.cpu().numpy()[0]
         C1 = plan.irfft_yz(chat)[0].cpu().numpy() + fn.V.cpu().numpy()
         beta = fn.beta
-        assert beta * np.max(np.abs(C1 - ref["C1_" + tag])) < floor
+        err = np.abs(C1 - ref["C1_" + tag])
+        at = np.unravel_index(int(np.argmax(err)), err.shape)
+        assert beta * err[at] < floor, ("C1 error at", at, "rho", golden32["rho_" + tag][at], "V",
+                                        float(fn.V[at].item()), "dLDA", ref["dLDA_" + tag][at], "a", fn.vdw_a,
+                                        "eos", (fn.wda.eta, fn.wda.kT, fn.wda.a_mfa, fn.wda.sigma3, fn.wda.epsilon,
+                                                list(fn.wda.factors)), "points above floor",
+                                        int(np.sum(beta * err >= floor)))
         # the LDA part alone: the pipeline with and without it (same HS and MFA arithmetic)
         fh = E.Functional(plan, fn.R, fn.beta, fn.wavelength, fn.V, fn.version & ~L.WDA, fn.kst, fn.vdw_a)
         chat_h = plan.new_spec(1)
@@ -79,5 +86,10 @@ def test_lda_part_against_reference(golden32, tmp_path):
         assert e_d < 1e-12 and e_F < 1e-11
     s = BT.NativeBatchSolve(fn, [mu], method='static', nsteps=3, threshold=1e-30, criterion='res')
     N, rho, conv = s.solve(torch.as_tensor(golden32["rho_a"][None], device="cuda"))
-    assert relerr(rho[0].cpu().numpy(), ref["picard3_rho"]) < 1e-10
-    assert scalar_rel(N[0], ref["picard3_N"]) < 1e-10
+    # the north star's 1e-10, or three times the reference's own floor on this
+    # trajectory (the same steps from a start one ulp above) where larger
+    e_rho = relerr(rho[0].cpu().numpy(), ref["picard3_rho"])
+    e_N = scalar_rel(N[0], ref["picard3_N"])
+    print("LDA three static Picard steps: rho %.2e (floor %.2e), N %.2e" % (e_rho, ref["picard3_floor"], e_N))
+    assert e_rho < max(1e-10, 3 * float(ref["picard3_floor"]))
+    assert e_N < 1e-10
