@@ -75,7 +75,7 @@ def candidates(npoints, max_candidates=48):
     # radix orders first, then the plane-pass form, then column tiles: a
     # truncated list keeps the widest spread of orders
     for tile in (0, 8, 4):
-        for st in (-1, 1):
+        for st in (-1, 1, 2):
             for o in itertools.product(*orders):
                 c = [o[0], o[1], o[2], st, tile]
                 if c != default and c not in out:

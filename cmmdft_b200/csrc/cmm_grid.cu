@@ -202,8 +202,8 @@ extern "C" int cmm_grid_create_sched(int n1, int n2, int n3, const double* rvecs
       if (sched[a] < -1 || sched[a] > CMM_ORDER_ODDDESC) return CMM_ERR_ARG;
       if (sched[a] >= 0) order[a] = sched[a];
     }
-    if (sched[3] < -1 || sched[3] > 1) return CMM_ERR_ARG;
-    staging = sched[3] > 0 ? 1 : 0;
+    if (sched[3] < -1 || sched[3] > 2) return CMM_ERR_ARG;
+    staging = sched[3] > 0 ? sched[3] : 0;
     if (sched[4] < 0 || sched[4] > 16 || (sched[4] & (sched[4] - 1))) return CMM_ERR_ARG;
     tile = sched[4];
   }
@@ -405,7 +405,7 @@ extern "C" int cmm_grid_destroy(cmm_grid* g) {
 }
 
 extern "C" int cmm_grid_set_staging(cmm_grid* g, int mode) {
-  if (!g || mode < 0 || mode > 1) return CMM_ERR_ARG;
+  if (!g || mode < 0 || mode > 2) return CMM_ERR_ARG;
   g->staging = mode;
   return CMM_OK;
 }

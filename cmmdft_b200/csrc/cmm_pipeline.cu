@@ -17,6 +17,8 @@
 #include <mutex>
 #include <utility>
 
+#include <cooperative_groups.h>
+
 #include "cmm_common.cuh"
 #include "cmm_dual.cuh"
 
@@ -925,6 +927,128 @@ k_plane_fmt_wda(GridDev g, const int* __restrict__ active, double R, int version
                                  fsr);
 }
 
+// ---------------------------------------- plane pass split over 2 CTAs ---
+// The same plane pass with the plane's fields split between the two CTAs of
+// a cluster (fields [0, nA) on rank 0, [nA, ns) on rank 1; nA = ceil(ns/2)),
+// so that a CTA holds ~100 KB instead of ~170 KB of shared memory and two
+// CTAs (of different planes) share an SM: one block's memory phases overlap
+// the other's FP64 phases.  Each CTA transforms its own fields; the
+// pointwise step reads and writes every field through distributed shared
+// memory.  The results are bit for bit those of plane_fmt_body: CTA rank r,
+// thread t plays thread v = r * T + t of the one-CTA pass (T = half its
+// block) and visits the same points in the same order, and the block
+// reductions combine the same 32-lane warp partials in the same tree.
+#define CMM_FMT2_THREADS (CMM_FMT_THREADS / 2)
+
+template <int N2C, int M3C, bool has_wda>
+__device__ __forceinline__ void plane_fmt_body_c2(GridDev g, const int* __restrict__ active, double R, int version,
+                                                  const cmm_wda_eos& wda, const double2* __restrict__ win,
+                                                  size_t fsw, double2* __restrict__ gout, size_t fsg,
+                                                  double* __restrict__ part, int nslot_part, int want,
+                                                  double* __restrict__ wd, size_t fsr) {
+  namespace cg = cooperative_groups;
+  cg::cluster_group cl = cg::this_cluster();
+  const unsigned rank = cl.block_rank();
+  const int i1 = blockIdx.x >> 1, b = blockIdx.y;
+  if (active && !active[b]) return;  // the same for both CTAs of the cluster
+  constexpr int ns = has_wda ? 6 : 5, nA = (ns + 1) / 2, nB = ns - nA;
+  const int f0 = rank ? nA : 0, nloc = rank ? nB : nA;
+  PlaneSmem s = plane_smem_setup<N2C, M3C>(g, nloc);
+  const PlaneShape<N2C, M3C> sh(g);
+  const size_t poff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3;
+  load_spec_planes<N2C, M3C>(g, s, nloc, win + (size_t)f0 * fsw, poff, fsw);
+  __syncthreads();
+  plane_inverse<N2C, M3C>(g, s, nloc);
+  cl.sync();  // both halves of the plane in real space
+  double2* peer = cl.map_shared_rank(s.slots, rank ^ 1u);
+  double* bA = (double*)(rank == 0 ? s.slots : peer);
+  double* bB = (double*)(rank == 1 ? s.slots : peer);
+  const size_t rowA = (size_t)nA * sh.h3 * 2, rowB = (size_t)nB * sh.h3 * 2;  // doubles per y row
+  auto fld = [&](int f, int r, int j) -> double& {
+    return f < nA ? bA[r * rowA + (size_t)f * sh.h3 * 2 + j] : bB[r * rowB + (size_t)(f - nA) * sh.h3 * 2 + j];
+  };
+  double phi = 0.0, n3max = -INFINITY, fwda = 0.0;
+  const bool do_c1 = (want & 1) != 0, do_phi = (want & 3) != 0;
+  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
+  const int vstride = 2 * blockDim.x;
+  for (int i = (int)(rank * blockDim.x + threadIdx.x); i < sh.n2 * sh.n3; i += vstride) {
+    const int r = i / sh.n3, j = i - r * sh.n3;
+    double& a0 = fld(0, r, j);
+    double& a3 = fld(1, r, j);
+    double& ax = fld(2, r, j);
+    double& ay = fld(3, r, j);
+    double& az = fld(4, r, j);
+    n3max = fmax(n3max, a3);
+    if (want & 8)
+      for (int f = 0; f < ns; ++f) wd[f * fsr + roff + i] = fld(f, r, j);
+    if (do_phi) {
+      PhiOut o = fmt_point<false, double>(a0, a3, ax, ay, az, nullptr, nullptr, R, version);
+      phi += o.phi;
+      if (do_c1) {
+        a0 = o.gs; a3 = o.g3; ax = o.gv[0]; ay = o.gv[1]; az = o.gv[2];
+      }
+      if (has_wda) {
+        double& aw = fld(5, r, j);
+        double fv, dfv;
+        wda_eos(wda, aw, fv, dfv);
+        fwda += fv;
+        if (do_c1) aw = dfv;
+      }
+    }
+  }
+  // warp partials of the one-CTA pass's virtual warps, gathered on rank 0
+  __shared__ double red[3][32];
+  for (int o = 16; o > 0; o >>= 1) {
+    phi += __shfl_xor_sync(0xffffffffu, phi, o);
+    fwda += __shfl_xor_sync(0xffffffffu, fwda, o);
+    n3max = fmax(n3max, __shfl_xor_sync(0xffffffffu, n3max, o));
+  }
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31, nw = blockDim.x >> 5;
+  if (l == 0) {
+    double* dst = cl.map_shared_rank(&red[0][0], 0u);
+    const int vw = (int)rank * nw + w;
+    dst[vw] = phi;
+    dst[32 + vw] = fwda;
+    dst[64 + vw] = n3max;
+  }
+  cl.sync();  // dPhi of every point and the warp partials in place; no remote access after this
+  if (rank == 0 && threadIdx.x < 32) {
+    double t0 = (l < 2 * nw) ? red[0][l] : 0.0, t1 = (l < 2 * nw) ? red[1][l] : 0.0;
+    double t2 = (l < 2 * nw) ? red[2][l] : -INFINITY;
+    for (int o = 16; o > 0; o >>= 1) {
+      t0 += __shfl_xor_sync(0xffffffffu, t0, o);
+      t1 += __shfl_xor_sync(0xffffffffu, t1, o);
+      t2 = fmax(t2, __shfl_xor_sync(0xffffffffu, t2, o));
+    }
+    if (want & 2) {
+      put_part(part, b, CMM_STAT_PHI, nslot_part, i1, t0);
+      if (has_wda) put_part(part, b, CMM_STAT_WDA, nslot_part, i1, t1);
+    }
+    if (want & 4) put_part(part, b, CMM_STAT_N3MAX, nslot_part, i1, t2);
+  }
+  if (!do_c1) return;
+  plane_forward<N2C, M3C>(g, s, nloc);
+  store_spec_planes<N2C, M3C>(g, s, nloc, gout + (size_t)f0 * fsg, poff, fsg);
+}
+
+template <int N2C, int M3C>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CMM_FMT2_THREADS, 2)
+k_plane_fmt_c2(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
+               const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
+               double* __restrict__ part, int nslot_part, int want, double* __restrict__ wd, size_t fsr) {
+  plane_fmt_body_c2<N2C, M3C, false>(g, active, R, version, wda, win, fsw, gout, fsg, part, nslot_part, want, wd,
+                                     fsr);
+}
+
+template <int N2C, int M3C>
+__global__ void __cluster_dims__(2, 1, 1) __launch_bounds__(CMM_FMT2_THREADS, 2)
+k_plane_fmt_wda_c2(GridDev g, const int* __restrict__ active, double R, int version, cmm_wda_eos wda,
+                   const double2* __restrict__ win, size_t fsw, double2* __restrict__ gout, size_t fsg,
+                   double* __restrict__ part, int nslot_part, int want, double* __restrict__ wd, size_t fsr) {
+  plane_fmt_body_c2<N2C, M3C, true>(g, active, R, version, wda, win, fsw, gout, fsg, part, nslot_part, want, wd,
+                                    fsr);
+}
+
 // ================================================ staged plane passes ==
 // For planes whose fields do not fit in one SM's shared memory (and for the
 // tensor variants), the plane pass runs as a y pass over HBM followed by a
@@ -1769,7 +1893,7 @@ static int ypass(const cmm_grid* g, int batch, const int* act, const double2* sr
 // memory, the y or z transform has a prime factor > 16 (direct-DFT stages
 // need scratch), N3 is odd (full-length z transform) or staging is forced.
 static bool plane_staged(const cmm_grid* g, int nf) {
-  return g->staging || g->dev.zfull || g->ax2.big || g->ax3.big ||
+  return g->staging == 1 || g->dev.zfull || g->ax2.big || g->ax3.big ||
          plane_smem_bytes(g->n2, g->n3, nf) > CMM_SMEM_MAX;
 }
 
@@ -2128,6 +2252,16 @@ static int fmt_plane_pass(const cmm_grid* g, int batch, const int* act, double R
   const bool ten = (version & CMM_TENSOR) != 0, has_wda = (version & CMM_WDA) != 0;
   const size_t fsr = (size_t)batch * g->n1 * g->n2 * g->n3;  // real field stride of wd
   const size_t ps = plane_smem_bytes(g->n2, g->n3, nf);
+  if (!ten && !plane_staged(g, nf) && g->staging == 0) {  // fused, the plane split over a CTA pair
+    const size_t ps2 = plane_smem_bytes(g->n2, g->n3, (nf + 1) / 2);
+    if (has_wda)
+      LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt_wda_c2, dim3(2 * g->n1, batch), CMM_FMT2_THREADS, ps2, st, g->dev,
+                     act, R, version, we, (const double2*)wbuf, fs, gbuf, fs, part, nslot, want, wd, fsr);
+    else
+      LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt_c2, dim3(2 * g->n1, batch), CMM_FMT2_THREADS, ps2, st, g->dev, act,
+                     R, version, we, (const double2*)wbuf, fs, gbuf, fs, part, nslot, want, wd, fsr);
+    return last_err();
+  }
   if (!ten && !plane_staged(g, nf)) {  // fused plane pass
     if (has_wda)
       LAUNCH_PLANE_T(plane_kind(g), k_plane_fmt_wda, dim3(g->n1, batch), CMM_FMT_THREADS, ps, st, g->dev, act, R,

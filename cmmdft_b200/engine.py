@@ -71,8 +71,10 @@ class GridPlan(object):
         return list(sc[:]), [[int(x) for x in row if x] for row in r]
 
     def set_staging(self, mode):
-        """0: fused plane passes where the plane fits in shared memory (default);
-        1: always the staged y pass + z-row form (cmm_grid_set_staging)."""
+        """0: fused plane passes where the plane fits in shared memory, the
+        functional's plane split over a CTA pair (default); 1: always the
+        staged y pass + z-row form; 2: fused, the functional's plane in one
+        CTA (cmm_grid_set_staging)."""
         check(self.lib.cmm_grid_set_staging(self.handle, int(mode)), "cmm_grid_set_staging")
 
     def __del__(self):

@@ -120,7 +120,10 @@ int cmm_grid_destroy(cmm_grid* grid);
  * shared memory runs the fused plane kernels (y and z transforms and the
  * pointwise step in one pass); larger planes, and the tensor variants, run
  * the staged form (a y pass over HBM, then z rows with the pointwise step).
- * mode 0 chooses by size (default), 1 always stages (tests, tuning).
+ * mode 0 chooses by size (default), 1 always stages (tests, tuning), 2
+ * chooses by size but runs the fused functional plane pass in one CTA per
+ * plane instead of the default CTA pair (a 2-CTA cluster holding half of
+ * the plane's fields each, two pairs per SM pair; bit-identical results).
  * Grids with odd N3 or a prime factor > 16 on the y or z axis always stage.
  * In the staged form cmm_residual_step and cmm_irfft_yz, whose spectrum
  * input is read-only, take a stream-ordered temporary of one spectrum per
@@ -131,7 +134,8 @@ int cmm_grid_set_staging(cmm_grid* grid, int mode);
  * tile; all schedules give the same transforms up to rounding.  The
  * default (cmm_grid_create) is CMM_ORDER_DEFAULT everywhere, plane passes
  * by size, column tiles by size.  sched[5] = {x order, y order, z order
- * (-1: default), plane passes (-1 or 0: by size, 1: staged), column tile
+ * (-1: default), plane passes (-1 or 0: by size, 1: staged, 2: by size with
+ * the one-CTA functional plane pass), column tile
  * width of the run-time-length column kernels (0: by size, else 1..16, a
  * power of two)}.  A non-default radix order runs the run-time-length
  * kernels on every axis (the compile-time ones for 32 and 64 points fix

@@ -617,3 +617,39 @@ def test_uneven_host_at_spacing_grid_against_reference(cuda):
                                                                               eN, eO))
     assert np.all(conv) and np.array_equal(s.steps, ref["steps"])
     assert eN < 1e-10 and eO < 1e-10
+
+
+@pytest.mark.parametrize("shape,wda,host_kind", [((32, 32, 32), False, "c"), ((64, 64, 64), False, "c"),
+                                                 ((64, 64, 64), True, "c"), ((40, 36, 30), False, "o"),
+                                                 ((28, 42, 26), True, "o")])
+def test_split_plane_pass_is_bit_identical(cuda, shape, wda, host_kind):
+    """The fused plane pass with the plane split over a 2-CTA cluster
+    (staging mode 0, the default) gives bit for bit the one-CTA pass's
+    (mode 2) C1 spectrum,
+    reductions and stored weighted densities: compile-time 32/64 lengths,
+    run-time lengths and a radix-7 axis, with and without the WDA field."""
+    from cmmdft_b200.hosts import random_sequential_host
+    host = cubic_host_276(0) if host_kind == "c" else random_sequential_host((14.0, 15.0, 13.0), 150, 3)
+    sig, eps, mass = methane_guest_params()
+    fn = W.build_functional(host, shape, 300.0, (sig, eps, mass), wda=wda)
+    plan = fn.plan
+    V = fn.V.cpu().numpy()
+    B = 3
+    rho = np.stack([s * 0.02 / angstrom ** 3 * np.clip(np.exp(-fn.beta * V), 0, 1) for s in (0.2, 0.6, 1.0)])
+    rt = torch.as_tensor(rho, device="cuda")
+    nwd = fn.nwd() if callable(fn.nwd) else fn.nwd
+    outs = []
+    for mode in (0, 2):
+        plan.set_staging(mode)
+        buf = E.Buffers(plan, B, nwork=fn.nwork)
+        buf.part[:, L.STAT_N3MAX, :] = -np.inf
+        chat = plan.new_spec(B)
+        wd = torch.zeros((nwd, B) + tuple(plan.npoints), dtype=torch.float64, device="cuda")
+        fn.c1(buf, plan.rfft_yz(rt), chat, want=15, wd=wd)
+        torch.cuda.synchronize()
+        outs.append((chat.cpu().numpy(), buf.part.cpu().numpy(), wd.cpu().numpy()))
+    plan.set_staging(0)
+    (c0, p0, w0), (c2, p2, w2) = outs
+    assert np.array_equal(c0, c2)
+    assert np.array_equal(p0, p2)
+    assert np.array_equal(w0, w2)
