@@ -11,6 +11,7 @@ machines):
     python tests/golden/make_golden.py --reference <reference tree> --lda
     python tests/golden/make_golden.py --reference <reference tree> --rot
     python tests/golden/make_golden.py --reference <reference tree> --rotinterp
+    python tests/golden/make_golden.py --reference <reference tree> --proj
 
 ``--reference`` (or the environment variable CMM_REFERENCE_ROOT) names the
 root of the reference's source tree, the directory that holds ``cmmdft/``.
@@ -71,6 +72,13 @@ Outputs (small ``.npz`` files) land next to this script:
               tricubic interpolation), with the channel values of
               get_external_potential_derivatives at 3000 seeded points of
               each type's derivative grid (``--rotinterp``).
+  proj32.npz      the reference's Calculator post-processing of three
+              converged 32^3 densities (0.1, 1 and 10 bar, Program.solve,
+              hybrid Anderson to RES < 1e-8): collective_variable along a
+              tilted axis (3 x 3 x 3 supercell, 3 A from the axis) and from
+              ring atoms, project_density, save_loading_and_grand_potential,
+              free_energy_path and project_contributions('fid',
+              'pure_extpot'); with the densities themselves (``--proj``).
   iso64_rho.npz   the converged densities of that isotherm at the pressure
               indices ISO_RHO_IDX, and the reference run against itself: the
               same points re-solved from a start perturbed by one ulp, with
@@ -619,6 +627,85 @@ def rotinterp12(args):
     np.savez_compressed(os.path.join(HERE, 'rotinterp12.npz'), **out)
 
 
+PROJ_PRESSURES = (0.1, 1.0, 10.0)   # bar
+
+
+def proj32(args):
+    """The reference's projections and free-energy path on three 32^3 densities."""
+    ref = import_reference(args.reference)
+    system, functionals, solver, extpot, eos = ref
+    from cmmdft import program as rprogram, calculator as rcalculator
+    import yaff
+    from cmmdft_b200.hosts import cubic_host_276, methane_guest_params
+    from cmmdft_b200.units import angstrom, bar
+    T = 300.0
+    host = cubic_host_276(seed=0)
+    sig, eps, mass = methane_guest_params()
+    mol = yaff.System(pos=host.pos.copy(), ffatypes=host.ffatypes, ffatype_ids=host.ffatype_ids, rvecs=host.rvecs,
+                      masses=host.masses)
+    mol.pos -= mol.pos.sum(axis=0) / len(mol.pos)  # as system.py:70
+    h = system.NanoporousHost.__new__(system.NanoporousHost)
+    system.Host.__init__(h, 'synthetic', mol.cell)
+    h.mol, h.chk, h.par = mol, None, None
+    guest = system.SphericalLJGuest('CH4', mass, sig, eps)
+    tmp = tempfile.mkdtemp(prefix='cmm_proj_')
+    grid0 = system.Grid(mol.cell, npoints=32)
+    V = extpot.get_external_potential(grid0.points[..., :3].reshape(-1, 3), host.ff, sig, eps, mol,
+                                      cutoff=12 * angstrom)
+    vfn = os.path.join(tmp, 'epot_32.npy')
+    np.save(vfn, V.reshape(grid0.npoints))
+    prog = rprogram.Program(prefix=tmp, hostname='synthetic', guestname='CH4', ff_suffix='trappe_uff', suffix='proj')
+    prog.set_system(h, guest)
+    prog.set_grid(npoints=32)
+    prog.init_free_energy(T)
+    prog.fener.add_hard_sphere(version='WBII')
+    prog.fener.add_mean_field(cutoff=12 * angstrom, rewrite=True)
+    prog.fener.add_external_potential(load_fn=vfn)
+    prog.fener.set_temperature(T)
+    mb = eos.ModifiedBenedictWebbRubinEOS(mass, sig, eps)
+    mb.set_temperature(T)
+    mus = [mb.calculate_mu(T, p * bar) for p in PROJ_PRESSURES]
+    out = dict(T=T, mus=np.array(mus))
+    for i, mu in enumerate(mus):
+        bulk = float(np.nanmin(mb.solve_densities_from_chempots([mu]), axis=1)[0])
+        prog.set_solver(solver.Anderson(prog, nsteps=500, m=5, criterion='res', threshold=1e-8))
+        N, rho, conv = quiet(prog.solve, mu, Ninit=bulk, energy_tracking=False)
+        assert conv
+        out['rho%d' % i] = rho
+    calc = rcalculator.Calculator.__new__(rcalculator.Calculator)
+    calc.program, calc.name_dict, calc.workdir = prog, prog.name_dict, prog.workdir
+    calc.grid, calc.fener = prog.grid, prog.fener
+    calc.host, calc.guest, calc.label = prog.system.host, prog.system.guest, None
+    path = np.array([[1.0, -0.5, 0.0], [1.6, -0.1, 1.0]])
+    cvs, cvs_mat, dist_mask = quiet(calc.collective_variable, diffusion_path=path, dist_from_axis=3 * angstrom,
+                                    supercell=True, step_dist=0.5 * angstrom)
+    out.update(path=path, cvs=cvs, cvs_mat_sum=np.sum(cvs_mat), cvs_mat_sample=cvs_mat.reshape(-1)[::997],
+               dist_mask_count=int(np.sum(dist_mask)), cvs_mat_shape=np.array(cvs_mat.shape))
+    for i, mu in enumerate(mus):
+        q, n = quiet(calc.project_density, T, mu, cvs, cvs_mat, dist_mask, rewrite=True)
+        out['proj_q'], out['proj_n%d' % i] = q, n
+        quiet(calc.save_loading_and_grand_potential, T, mu)
+    with open(os.path.join(prog.workdir, 'loading_grand_potential_%7.5fK.csv' % T)) as f:
+        out['lgp_csv'] = np.array(f.read())
+    quiet(calc.free_energy_path, T, mus[-1], chempots=mus)
+    fe_fn = prog.workdir / ('free_energy_profile_%#0.8fkjmol_%#0.3fK.csv' % (mus[-1] / kjmol_unit(), T))
+    out['fe_path'] = np.loadtxt(fe_fn, delimiter=',', skiprows=1)
+    quiet(calc.project_contributions, T, mus[1], ['fid', 'pure_extpot'], cvs, cvs_mat, dist_mask)
+    from cmmdft_b200.tools import get_file_suffix
+    pc_fn = prog.workdir / ('projected_contributions_%s.csv' % get_file_suffix(mus[1], T))
+    out['proj_contrib'] = np.loadtxt(pc_fn, delimiter=',', skiprows=1)
+    ring = list(range(6))
+    cvs_r, cvs_mat_r, mask_r = quiet(calc.collective_variable, ring_indices=ring, step_dist=0.5 * angstrom)
+    out.update(ring=np.array(ring), ring_cvs=cvs_r, ring_cvs_mat=cvs_mat_r)
+    np.savez_compressed(os.path.join(HERE, 'proj32.npz'), **out)
+    print('wrote proj32.npz', {k: v for k, v in out.items() if np.ndim(v) == 0})
+
+
+def kjmol_unit():
+    from cmmdft_b200.units import kjmol
+    return kjmol
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--reference', default=os.environ.get('CMM_REFERENCE_ROOT'),
@@ -632,6 +719,7 @@ def main():
     ap.add_argument('--lda', action='store_true')
     ap.add_argument('--rot', action='store_true')
     ap.add_argument('--rotinterp', action='store_true')
+    ap.add_argument('--proj', action='store_true')
     ap.add_argument('--procs', type=int, default=8)
     args = ap.parse_args()
     if not args.reference:
@@ -650,6 +738,8 @@ def main():
         return rot20(args)
     if args.rotinterp:
         return rotinterp12(args)
+    if args.proj:
+        return proj32(args)
     ref = import_reference(args.reference)
     solver = ref[2]
     from cmmdft_b200.hosts import cubic_host_276, HELIUM

@@ -276,3 +276,58 @@ def test_nonfinite_member_retries_then_fails(cuda, tmp_path, native, method):
     a = cd.Picard(prog, nsteps=50, alpha_mix=0.1, method='static', criterion='res', threshold=1e-8)
     with pytest.raises(cd.NoSolutionError):
         a.solve(float(mus[1]), bad[1].cpu().numpy())
+
+
+def test_projections_and_free_energy_path(cuda, tmp_path):
+    """Calculator post-processing (calculator.py:494-899) on the reference's
+    own three converged 32^3 densities (tests/golden/proj32.npz, placed as
+    the rho_*.npy files of the Program): collective variables along a tilted
+    axis on the 3 x 3 x 3 supercell and from ring atoms (exact), projected
+    densities and contributions (1e-12 of their largest value), the loading
+    and grand-potential table (1e-12 / 1e-10) and the free-energy path
+    (1e-10 relative to the largest Omega)."""
+    from cmmdft_b200.tools import get_file_suffix
+    ref = dict(np.load(os.path.join(ROOT, "tests", "golden", "proj32.npz")))
+    prog = make_program(tmp_path, 'proj')
+    mus = ref["mus"]
+    for i, mu in enumerate(mus):
+        np.save(prog.workdir / ('rho_%s.npy' % get_file_suffix(mu, T)), ref["rho%d" % i])
+    calc = cd.Calculator(prog)
+    cvs, cvs_mat, mask = calc.collective_variable(diffusion_path=ref["path"], dist_from_axis=3 * angstrom,
+                                                  supercell=True, step_dist=0.5 * angstrom)
+    assert np.array_equal(cvs, ref["cvs"]) and tuple(cvs_mat.shape) == tuple(ref["cvs_mat_shape"])
+    assert np.array_equal(cvs_mat.reshape(-1)[::997], ref["cvs_mat_sample"])
+    assert int(np.sum(mask)) == int(ref["dist_mask_count"])
+    errs = {}
+    for i, mu in enumerate(mus):
+        q, n = calc.project_density(T, mu, cvs, cvs_mat, mask, rewrite=True)
+        assert np.array_equal(q, ref["proj_q"])
+        errs['n%d' % i] = float(np.max(np.abs(n - ref["proj_n%d" % i])) / np.max(np.abs(ref["proj_n%d" % i])))
+        calc.save_loading_and_grand_potential(T, mu)
+    got = np.loadtxt(prog.workdir / ('loading_grand_potential_%7.5fK.csv' % T), delimiter=',', skiprows=1)
+    exp = np.array([[float(x) for x in l.split(',')] for l in str(ref["lgp_csv"]).strip().splitlines()[1:]])
+    assert got.shape == exp.shape and np.array_equal(got[:, 0], exp[:, 0])
+    errs['loading'] = float(np.max(np.abs(got[:, 1] - exp[:, 1]) / np.abs(exp[:, 1])))
+    errs['omega'] = float(np.max(np.abs(got[:, 2] - exp[:, 2]) / np.abs(exp[:, 2])))
+    fe = calc.free_energy_path(T, mus[-1], chempots=list(mus))
+    rf = ref["fe_path"].T
+    assert np.array_equal(fe[0], rf[0])
+    for c, name in ((1, 'fe_density'), (2, 'fe_omega'), (3, 'fe_free')):
+        fin = np.isfinite(rf[c])
+        assert np.array_equal(np.isfinite(fe[c]), fin), name
+        errs[name] = float(np.max(np.abs(fe[c][fin] - rf[c][fin])) / np.max(np.abs(rf[c][fin])))
+    pc = calc.project_contributions(T, mus[1], ['fid', 'pure_extpot'], cvs, cvs_mat, mask)
+    rc = ref["proj_contrib"].T
+    for c, name in ((2, 'fid'), (3, 'pure_extpot')):
+        fin = np.isfinite(rc[c])
+        assert np.array_equal(np.isfinite(pc[c]), fin), name
+        errs[name] = float(np.max(np.abs(pc[c][fin] - rc[c][fin])) / np.max(np.abs(rc[c][fin])))
+    cr, cmr, _ = calc.collective_variable(ring_indices=list(ref["ring"]), step_dist=0.5 * angstrom)
+    errs['ring_cvs'] = float(np.max(np.abs(cr - ref["ring_cvs"])))
+    errs['ring_cvs_mat'] = float(np.max(np.abs(cmr - ref["ring_cvs_mat"])))
+    print("projections:", {k: "%.1e" % v for k, v in errs.items()})
+    assert max(errs[k] for k in errs if k.startswith('n')) < 1e-12
+    assert errs['loading'] < 1e-12 and errs['omega'] < 1e-10
+    assert errs['fe_density'] < 1e-12 and errs['fe_omega'] < 1e-10 and errs['fe_free'] < 1e-10
+    assert errs['fid'] < 1e-12 and errs['pure_extpot'] < 1e-12
+    assert errs['ring_cvs'] < 1e-12 and errs['ring_cvs_mat'] < 1e-12
