@@ -25,6 +25,12 @@
 #define CMM_COL_MINB 1
 #endif
 #define CMM_COL_MINB_FOR(n1c) ((n1c) > 0 ? 5 : CMM_COL_MINB)
+// The single-field plane passes (transforms, Picard, residual, mix) run two
+// 512-thread blocks per SM (64 registers, no spills) except in the
+// instantiation with radix 7/11/13 and Rader stages (-1), whose stage code
+// needs more registers: residual 0.235 -> 0.156 ms, mix 0.225 -> 0.179 ms,
+// Picard 0.185 -> 0.125 ms for 24 instances at 64^3 against one block per SM.
+#define CMM_PLANE_MINB_FOR(n2c) ((n2c) >= 0 ? 2 : CMM_PLANE_MINB)
 #define CMM_ROW_THREADS 512    // staged z-row passes
 #define CMM_ZFMT_THREADS 768   // the staged z-row pass of dPhi/dn (768 measured faster than 256-512 and 1024)
 

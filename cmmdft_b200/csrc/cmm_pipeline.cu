@@ -237,7 +237,7 @@ __device__ inline void put_part(double* part, int b, int q, int nslot, int slot,
 
 // ================================================ 3D FFT (setup / tests) ==
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB_FOR(N2C))
 k_plane_r2c(GridDev g, const int* __restrict__ active, const double* __restrict__ in, double2* __restrict__ out) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   if (active && !active[b]) return;
@@ -254,7 +254,7 @@ k_plane_r2c(GridDev g, const int* __restrict__ active, const double* __restrict_
 }
 
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB_FOR(N2C))
 k_plane_c2r(GridDev g, const double2* __restrict__ in, double* __restrict__ out) {
   const int i1 = blockIdx.x, b = blockIdx.y;
   PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
@@ -1309,7 +1309,7 @@ __device__ __forceinline__ double der_term(double rho, double C1, double mu, dou
 
 // Static Picard step fused with the C1 inverse and the forward of rho'.
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB_FOR(N2C))
 k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
                double beta, double lambda3, double thr, double a_tol, double r_tol,
                const double2* __restrict__ chat,
@@ -1364,7 +1364,7 @@ struct HistPtrs { const double* p[CMM_MAX_HIST]; };
 
 // Residual r = G(C1) - rho with the Gram row against stored residuals.
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB_FOR(N2C))
 k_plane_residual(GridDev g, const int* __restrict__ active, const double* __restrict__ params,
                  double beta, double lambda3, double a_tol, double r_tol, const double2* __restrict__ chat,
                  const double* __restrict__ rho,
@@ -1418,7 +1418,7 @@ struct FieldPtrs { const double* p[CMM_MAX_FIELDS]; long long stride[CMM_MAX_FIE
 
 // rho' = sum_j c_j field_j, clipped, with stats and the forward transform.
 template <int N2C, int M3C>
-__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB)
+__global__ void __launch_bounds__(CMM_PLANE_THREADS, CMM_PLANE_MINB_FOR(N2C))
 k_plane_mix(GridDev g, const int* __restrict__ active, const double* __restrict__ coef,
             FieldPtrs fields, int nfield, int clip, double thr, double lambda3, const double* __restrict__ ref,
             long long refstride, const double* __restrict__ V, long long vstride,
