@@ -48,7 +48,7 @@ class SolveOpts(ctypes.Structure):
                 ("alpha_mix", _d), ("damping", _d), ("delta", _d), ("damping_max", _d), ("damping_min", _d),
                 ("damping_up", _d), ("damping_down", _d), ("adaptive_damping", _i), ("divergence_guard", _i),
                 ("a_tol", _d), ("r_tol", _d), ("ls_thresh", _d), ("kjmol", _d), ("coefs", _i),
-                ("picard_thr", _d)]
+                ("picard_thr", _d), ("device_loop", _i)]
 
 
 class SolveWs(ctypes.Structure):

@@ -1031,7 +1031,11 @@ class NativeBatchSolve(BatchSolve):
     per-instance decisions evaluated in C++ between read-backs instead of in
     the interpreter.  The rare SLSQP fallback of the line search is called
     back into Python (scipy, on full evaluations of the trial density).
-    Same results as BatchSolve."""
+    Static Picard runs with its decisions on the device and the step
+    replayed as a CUDA graph (``device_loop``; False: host decisions after
+    every step).  Same results as BatchSolve."""
+
+    device_loop = True
 
     def solve(self, rho0, cf=None, host_out=None):
         if host_out is not None and (not host_out.is_pinned() or tuple(host_out.shape) != tuple(rho0.shape)):
@@ -1054,7 +1058,7 @@ class NativeBatchSolve(BatchSolve):
                            adaptive_damping=int(bool(self.adaptive)), divergence_guard=int(self.divergence_guard),
                            a_tol=self.tol[0], r_tol=self.tol[1], ls_thresh=self.thresh, kjmol=kjmol,
                            coefs=L.COEF_EXACT if self.anderson_coefs == 'exact' else L.COEF_SLSQP,
-                           picard_thr=1e-10 / angstrom ** 3)
+                           picard_thr=1e-10 / angstrom ** 3, device_loop=int(bool(self.device_loop)))
         for i, (c, t) in enumerate(zip(self.criteria, self.thresholds)):
             opts.crit[i] = crit[c]
             opts.thr[i] = t

@@ -20,6 +20,8 @@
 #include <thread>
 #include <vector>
 
+#include <math_constants.h>
+
 #include "cmm_common.cuh"
 
 // SLSQP mixing coefficients (cmm_anderson.cu)
@@ -239,6 +241,111 @@ bool isclose0(double a) { return std::fabs(a) <= 1e-8; }   // np.isclose(a, 0)
 // Anderson coefficients of every instance are independent).  run(n, f) calls
 // f(i) for i < n on the workers and the calling thread and returns when all
 // workers have checked in; items are claimed from one atomic counter.
+// ------------------------------------------------ device-side static loop --
+// Static Picard with the per-instance decisions on the device: one step is a
+// fixed launch sequence (the Picard pass of each ring parity, the stats
+// reduction, k_static_decide, the C1 pipeline) that a CUDA graph replays; the
+// host reads one counter every few steps.  k_static_decide is the
+// convergence / divergence / retry logic of Driver::loop_static evaluated per
+// instance with the same operations in the same order (explicitly rounded,
+// no contraction), so the trajectory and every reported number are those of
+// the host loop.
+struct StaticDev {
+  int* live;       // [B] stepping
+  int* act;        // [2][B] instances whose current density is in ring slot 0 / 1
+  int* cur;        // [B] ring slot of the current density
+  int* retry;      // [B] non-finite density: restart with a halved correction factor
+  int* fin;        // [B] finished (converged, step limit or diverging)
+  int* steps;      // [B]
+  int* conv;       // [B]
+  int* divg;       // [B]
+  int* ctr;        // [0] step, [1] instances still stepping
+  double* prev;    // [B][NST] the previous step's stats
+  double* N;       // [B] loading at finish
+  double* omega0;  // [B]
+  double* res_hist;   // [B][nsteps + 2]
+  double* history;    // [B][nsteps + 2][CMM_HISTORY_COLS] or null
+};
+
+struct StaticParams {
+  int B, nsteps, ncrit, guard;
+  int crit[3];
+  double thr[3];
+  double dr, npts;
+};
+
+__device__ bool dev_diverging(const double* r, int k, int guard) {
+  if (!guard || k < 8) return false;
+  const double last_r = r[k];
+  if (!isfinite(last_r)) return true;
+  double best = CUDART_NAN;
+  for (int j = 1; j <= k; ++j)
+    if (!isnan(r[j])) best = isnan(best) ? r[j] : fmin(best, r[j]);
+  bool rising = true;
+  for (int j = k - 4; j <= k; ++j) rising = rising && (__dsub_rn(r[j], r[j - 1]) >= 0);
+  return last_r > __dmul_rn(1e6, best) && rising;
+}
+
+__global__ void k_static_decide(StaticParams P, const double* __restrict__ stats, StaticDev D) {
+  const int step = D.ctr[0] + 1;
+  __shared__ int nlive;
+  if (threadIdx.x == 0) nlive = 0;
+  __syncthreads();
+  for (int b = threadIdx.x; b < P.B; b += blockDim.x) {
+    const double* s = stats + (size_t)b * NST;
+    double* pv = D.prev + (size_t)b * NST;
+    if (D.live[b]) {
+      bool done = false;
+      if (step > 1) {
+        const int k = step - 1;
+        const double N = __dmul_rn(pv[CMM_STAT_N], P.dr);
+        const double res = __ddiv_rn(__ddiv_rn(__dsqrt_rn(s[CMM_STAT_RES2]), __dsqrt_rn(N)), __dsqrt_rn(P.npts));
+        const double iue = __dmul_rn(pv[CMM_STAT_IUE], P.dr);
+        const double der = __ddiv_rn(__dsqrt_rn(s[CMM_STAT_DER]), __dsqrt_rn(P.npts));
+        D.steps[b] = k;
+        const double riue = (N > 0) ? __ddiv_rn(iue, N) : CUDART_NAN;
+        bool ok = true;
+        for (int c = 0; c < P.ncrit; ++c) {
+          const double v = P.crit[c] == CMM_CRIT_RES ? res : (P.crit[c] == CMM_CRIT_RIUE ? riue : der);
+          ok = ok && (v < P.thr[c]);
+        }
+        if (D.history && k <= P.nsteps + 1) {
+          double* h = D.history + ((size_t)b * (P.nsteps + 2) + k) * CMM_HISTORY_COLS;
+          h[0] = N; h[1] = res; h[2] = riue; h[3] = D.omega0[b]; h[4] = der;
+        }
+        if (iue == 0 && isnan(riue)) ok = true;
+        double* rh = D.res_hist + (size_t)b * (P.nsteps + 2);
+        if (k <= P.nsteps + 1) rh[k] = res;
+        if (ok || k >= P.nsteps || dev_diverging(rh, k, P.guard)) {
+          if (!ok) D.divg[b] = k < P.nsteps ? 1 : 0;
+          D.conv[b] = ok ? 1 : 0;
+          D.N[b] = N;
+          D.fin[b] = 1;
+          D.live[b] = 0;
+          done = true;
+        }
+      }
+      if (!done && s[CMM_STAT_NONFIN] > 0) {
+        D.retry[b] = 1;
+        D.live[b] = 0;
+        done = true;
+      }
+      if (!done) {
+        D.cur[b] = 1 - D.cur[b];
+        atomicAdd(&nlive, 1);
+      }
+    }
+    D.act[b] = D.live[b] && D.cur[b] == 0;
+    D.act[P.B + b] = D.live[b] && D.cur[b] == 1;
+    for (int q = 0; q < NST; ++q) pv[q] = s[q];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    D.ctr[0] = step;
+    D.ctr[1] = nlive;
+  }
+}
+
 class HostPool {
  public:
   explicit HostPool(int nthreads) {
@@ -809,6 +916,127 @@ struct Driver {
     }
   }
 
+  // loop_static with the decisions on the device (k_static_decide) and the
+  // step replayed as a CUDA graph; the host reads the count of instances
+  // still stepping every STATIC_CHECK steps.  Same trajectory and outputs as
+  // loop_static.
+  static constexpr int STATIC_CHECK = 4;
+  void static_step(const StaticParams& P, const StaticDev& D, cudaStream_t s) {
+    for (int par = 0; par < 2; ++par)
+      check(cmm_picard_static_step(g, B, D.act + par * B, w->params, beta, fn->lambda3, o->picard_thr, o->a_tol,
+                                   o->r_tol, w->chat, ring(par), fn->d_V, 0, ring(1 - par), w->that, w->part,
+                                   w->nslot, s));
+    check(cmm_stats_finalize(B, D.live, w->part, w->nslot, (1u << NST) - 1u, w->stats, s));
+    k_static_decide<<<1, 256, 0, s>>>(P, w->stats, D);
+    cuda(cudaPeekAtLastError());
+    check(cmm_fmt_c1(g, B, D.live, fn->R, fn->beta, fn->version, fn->wda, fn->d_kst, fn->d_wtab, w->that,
+                     w->chat, w->work, w->part, w->nslot, 1, nullptr, s));
+    out->launches += 7;
+  }
+
+  void loop_static_device(std::vector<char>& live, std::vector<char>& retry) {
+    const int H = o->nsteps + 2;
+    const size_t ni = (size_t)B, nd_hist = out->history ? (size_t)B * H * CMM_HISTORY_COLS : 0;
+    const size_t ibytes = sizeof(int) * (ni * 9 + 2);
+    const size_t dbytes = sizeof(double) * (ni * NST + 2 * ni + ni * H + nd_hist);
+    void* mem = nullptr;
+    const size_t ioff = (ibytes + 15) & ~(size_t)15;
+    if (!cuda(cudaMalloc(&mem, ioff + dbytes))) return;
+    StaticDev D;
+    int* ip = (int*)mem;
+    D.live = ip; D.act = ip + ni; D.cur = ip + 3 * ni; D.retry = ip + 4 * ni; D.fin = ip + 5 * ni;
+    D.steps = ip + 6 * ni; D.conv = ip + 7 * ni; D.divg = ip + 8 * ni; D.ctr = ip + 9 * ni;
+    double* dp = (double*)((char*)mem + ioff);
+    D.prev = dp; D.N = dp + ni * NST; D.omega0 = D.N + ni; D.res_hist = D.omega0 + ni;
+    D.history = out->history ? D.res_hist + ni * H : nullptr;
+    // initial state, as loop_static starts
+    std::vector<int> hi(ni * 9 + 2, 0);
+    int nl = 0;
+    for (int b = 0; b < B; ++b) {
+      hi[b] = live[b] ? 1 : 0;          // live
+      hi[ni + b] = live[b] ? 1 : 0;     // act[0]: every current density in slot 0
+      nl += live[b] ? 1 : 0;
+    }
+    hi[ni * 9 + 1] = nl;
+    std::vector<double> hd(ni * NST + 2 * ni + ni * H + nd_hist, 0.0);
+    for (int b = 0; b < B; ++b) hd[ni * NST + ni + b] = omega0[b];
+    for (size_t q = 0; q < ni * H; ++q) hd[ni * NST + 2 * ni + q] = NAN;
+    if (nd_hist) std::memcpy(&hd[ni * NST + 2 * ni + ni * H], out->history, sizeof(double) * nd_hist);
+    cuda(cudaMemcpyAsync(D.live, hi.data(), sizeof(int) * hi.size(), cudaMemcpyHostToDevice, st));
+    cuda(cudaMemcpyAsync(D.prev, hd.data(), sizeof(double) * hd.size(), cudaMemcpyHostToDevice, st));
+    std::vector<double> a(B);
+    for (int b = 0; b < B; ++b) a[b] = o->alpha_mix * cf[b];
+    set_params(nullptr, a.data());
+    StaticParams P;
+    P.B = B; P.nsteps = o->nsteps; P.ncrit = o->ncrit; P.guard = o->divergence_guard;
+    for (int c = 0; c < 3; ++c) { P.crit[c] = o->crit[c]; P.thr[c] = o->thr[c]; }
+    P.dr = dr; P.npts = (double)npts;
+    // the first step eagerly (it also raises the kernels' shared-memory
+    // limits outside any capture), then the step captured on a private
+    // stream (the caller's may be the legacy default stream, which cannot
+    // be captured) and replayed on the caller's stream
+    static_step(P, D, st);
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    cudaStream_t cs = nullptr;
+    if (rc == CMM_OK && cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking) == cudaSuccess) {
+      if (cudaStreamBeginCapture(cs, cudaStreamCaptureModeThreadLocal) == cudaSuccess) {
+        const long long l0 = out->launches;
+        static_step(P, D, cs);
+        out->launches = l0;
+        const bool ok = cudaStreamEndCapture(cs, &graph) == cudaSuccess && rc == CMM_OK &&
+                        cudaGraphInstantiate(&exec, graph, 0) == cudaSuccess;
+        if (!ok) {
+          if (exec) cudaGraphExecDestroy(exec);
+          exec = nullptr;
+          rc = CMM_OK;          // no graph: the same step sequence is launched eagerly
+        }
+      }
+    }
+    cudaGetLastError();         // a refused capture leaves only a non-sticky error behind
+    int* hc = (int*)stage();
+    int steps_run = 1;
+    while (rc == CMM_OK) {
+      cuda(cudaMemcpyAsync(hc, D.ctr, sizeof(int) * 2, cudaMemcpyDeviceToHost, st));
+      cuda(cudaStreamSynchronize(st));
+      if (hc[1] == 0 || steps_run > o->nsteps + 2) break;
+      for (int i = 0; i < STATIC_CHECK && rc == CMM_OK; ++i, ++steps_run) {
+        if (exec) {
+          cuda(cudaGraphLaunch(exec, st));
+          out->launches += 7;
+        } else {
+          static_step(P, D, st);
+        }
+      }
+    }
+    if (exec) cudaGraphExecDestroy(exec);
+    if (graph) cudaGraphDestroy(graph);
+    if (cs) cudaStreamDestroy(cs);
+    if (rc == CMM_OK) {
+      cuda(cudaMemcpyAsync(hi.data(), D.live, sizeof(int) * hi.size(), cudaMemcpyDeviceToHost, st));
+      cuda(cudaMemcpyAsync(hd.data(), D.prev, sizeof(double) * hd.size(), cudaMemcpyDeviceToHost, st));
+      cuda(cudaStreamSynchronize(st));
+    }
+    if (rc == CMM_OK) {
+      if (nd_hist) std::memcpy(out->history, &hd[ni * NST + 2 * ni + ni * H], sizeof(double) * nd_hist);
+      for (int b = 0; b < B; ++b) {
+        if (!live[b]) continue;
+        const int k = hi[6 * ni + b];
+        if (k > 0) out->steps[b] = k;
+        if (hi[5 * ni + b]) {           // finished
+          if (!hi[7 * ni + b]) out->diverged[b] = hi[8 * ni + b];
+          finish(b, hi[3 * ni + b], hd[ni * NST + b], k, hi[7 * ni + b] != 0);
+          live[b] = 0;
+        } else if (hi[4 * ni + b]) {    // non-finite: retried by the caller
+          retry[b] = 1;
+          live[b] = 0;
+        }
+      }
+    }
+    cudaStreamSynchronize(st);
+    cudaFree(mem);
+  }
+
   // _loop_general (batch.py)
   void loop_general(std::vector<char>& live, std::vector<char>& retry) {
     std::fill(gram.begin(), gram.end(), 0.0);
@@ -932,7 +1160,8 @@ struct Driver {
       std::vector<char> live(todo), retry(B, 0);
       init_state(todo);
       if (rc) break;
-      if (statik) loop_static(live, retry);
+      if (statik && o->device_loop) loop_static_device(live, retry);
+      else if (statik) loop_static(live, retry);
       else loop_general(live, retry);
       // non-finite -> halve the correction factor and restart (solver.py:335-345)
       for (int b = 0; b < B; ++b) {

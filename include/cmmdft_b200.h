@@ -402,6 +402,9 @@ typedef struct cmm_solve_opts {
   int coefs;                    /* CMM_COEF_* */
   double picard_thr;            /* static Picard: densities below this become 0 (1e-10 angstrom^-3 in the
                                    caller's length unit, solver.py:398) */
+  int device_loop;              /* static Picard: 1 = the per-instance decisions in a device kernel and the
+                                   step replayed as a CUDA graph (the host reads one counter every 4 steps),
+                                   0 = decisions on the host after every step; same results */
 } cmm_solve_opts;
 
 /* Buffers of one solve (device, except the h_* pinned host arrays).

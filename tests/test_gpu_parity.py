@@ -653,3 +653,36 @@ def test_split_plane_pass_is_bit_identical(cuda, shape, wda, host_kind):
     assert np.array_equal(c0, c2)
     assert np.array_equal(p0, p2)
     assert np.array_equal(w0, w2)
+
+
+@pytest.mark.parametrize("guard", [False, True])
+def test_static_device_loop_matches_host_loop(cuda, guard):
+    """Static Picard with the decisions in k_static_decide and the step
+    replayed as a CUDA graph (the native driver's default) against the host
+    decisions after every step: the same densities, loadings, step counts,
+    divergence flags and per-step history, bit for bit, for four pressures
+    (0.01 to 10 bar) with and without the divergence guard."""
+    import time
+    guest = methane_guest_params()
+    fn = W.build_functional(cubic_host_276(0), (32, 32, 32), 300.0, guest)
+    mus, bulks = W.isotherm_inputs(np.array([0.01, 0.3, 1.0, 10.0]) * bar, 300.0, guest)
+    r0 = W.initial_density(fn, mus, ninit=bulks)
+    outs, times = [], []
+    for dl in (False, True):
+        s = BT.NativeBatchSolve(fn, mus, method='static', nsteps=700, threshold=1e-8, criterion='res',
+                                divergence_guard=guard, track_history=True)
+        s.device_loop = dl
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        N, rho, conv = s.solve(r0.clone())
+        torch.cuda.synchronize()
+        times.append(time.perf_counter() - t0)
+        outs.append((np.asarray(N), rho.cpu().numpy(), np.asarray(conv), np.asarray(s.steps),
+                     np.asarray(s.diverged), [np.asarray(h) for h in s.history]))
+    (Nh, rh, ch, sh, dh, hh), (Nd, rd, cd_, sd, dd, hd) = outs
+    print("static Picard, 4 pressures at 32^3: steps %s, host loop %.3f s, device loop %.3f s"
+          % (list(sd), times[0], times[1]))
+    assert np.array_equal(Nh, Nd) and np.array_equal(rh, rd)
+    assert np.array_equal(ch, cd_) and np.array_equal(sh, sd) and np.array_equal(dh, dd)
+    for a, b in zip(hh, hd):
+        assert a.shape == b.shape and np.array_equal(np.isnan(a), np.isnan(b)) and np.array_equal(a[~np.isnan(a)], b[~np.isnan(b)])
