@@ -940,6 +940,20 @@ class BatchSolve(object):
         return self.n3max[b]
 
 
+_STREAMS = {}
+
+
+def _group_streams(n):
+    """n CUDA streams of the current device, the same ones on every call: the
+    caching allocator keeps freed blocks per stream, so the workspaces of one
+    solve serve the next instead of new device allocations."""
+    dev = torch.cuda.current_device()
+    pool = _STREAMS.setdefault(dev, [])
+    while len(pool) < n:
+        pool.append(torch.cuda.Stream(device=dev))
+    return pool[:n]
+
+
 class GroupedSolve(object):
     """A batch of instances solved as G independent groups, each a BatchSolve
     on its own CUDA stream driven by its own host thread.
@@ -972,7 +986,7 @@ class GroupedSolve(object):
             self.N_out, self.result, self.conv = s.solve(rho0, host_out=host_out)
             return self.N_out, self.result, self.conv
         cur = torch.cuda.current_stream()
-        streams = [torch.cuda.Stream() for _ in self.parts]
+        streams = _group_streams(len(self.parts))
         out = [None] * len(self.parts)
         errors = []
 
