@@ -17,14 +17,17 @@
 // back-convolution column passes of the specialised x lengths (32, 64) run
 // five 256-thread blocks per SM (48 registers, a few spilled bytes): 5% faster
 // C1 pipeline at 64^3 than four blocks with 64 registers, measured; the
-// run-time-length instantiations keep their full register budget.
+// run-time-length instantiation without radix 7/11/13 and Rader stages (0)
+// runs four blocks (64 registers; C1 5-7 % faster on 80x96x72 and
+// 160x144x160, with the y pass of the staged plane passes likewise); the one
+// with them (-1) keeps its full register budget.
 #ifndef CMM_PLANE_MINB
 #define CMM_PLANE_MINB 1
 #endif
 #ifndef CMM_COL_MINB
 #define CMM_COL_MINB 1
 #endif
-#define CMM_COL_MINB_FOR(n1c) ((n1c) > 0 ? 5 : CMM_COL_MINB)
+#define CMM_COL_MINB_FOR(n1c) ((n1c) > 0 ? 5 : ((n1c) == 0 ? 4 : CMM_COL_MINB))
 // The single-field plane passes (transforms, Picard, residual, mix) run two
 // 512-thread blocks per SM (64 registers, no spills) except in the
 // instantiation with radix 7/11/13 and Rader stages (-1), whose stage code

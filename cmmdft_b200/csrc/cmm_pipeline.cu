@@ -1058,7 +1058,7 @@ k_plane_fmt_wda_c2(GridDev g, const int* __restrict__ active, double R, int vers
 // at a time: [n2][tc] in shared memory, pencils along y.  Fields f of the
 // launch are at src/dst + f * fs; blockIdx.z = b * nfield + f.
 template <int N2C>
-__global__ void __launch_bounds__(CMM_COL_THREADS, CMM_COL_MINB)
+__global__ void __launch_bounds__(CMM_COL_THREADS, (N2C >= 0 ? 4 : CMM_COL_MINB))
 k_ypass(GridDev g, const int* __restrict__ active, const double2* src, double2* dst, size_t fs, int nfield,
         int tc, int inv) {
   const int i1 = blockIdx.y;
