@@ -12,7 +12,7 @@ from .eos import (EquationOfState, SumOfEOS, ModifiedBenedictWebbRubinEOS, Carna
                   MFAEOS)
 from .functionals import (FreeEnergy, HardSphereFunctional, MFAFunctional, ExternalPotential,  # noqa: F401
                           WDAVFunctional, LDAFunctional)
-from .solver import Solver, Picard, Anderson, NoSolutionError  # noqa: F401
+from .solver import Solver, Picard, Anderson, QuasiNewton, Fire, NoSolutionError  # noqa: F401
 from .program import Program  # noqa: F401
 from .calculator import Calculator  # noqa: F401
 from .tools import get_file_suffix  # noqa: F401

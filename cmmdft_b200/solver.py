@@ -1,10 +1,10 @@
 """Fixed-point solvers with the reference's interface (cmmdft/solver.py:18-604).
 
-Solver / Picard / Anderson / QuasiNewton keep the reference's constructor
-arguments and ``solve(chempot, rho, log_level) -> (N, rho, converged)``.
-Each call runs a batch of one through the native batched driver
-(``quasinewton.QuasiNewtonSolve`` for QuasiNewton; all field work on the
-GPU); the
+Solver / Picard / Anderson / QuasiNewton / Fire keep the reference's
+constructor arguments and ``solve(chempot, rho, log_level) -> (N, rho,
+converged)``.  Each call runs a batch of one through the native batched
+driver (``quasinewton.QuasiNewtonSolve`` for QuasiNewton, ``fire.FireSolve``
+for Fire; all field work on the GPU); the
 batched isotherm entry point is ``isotherm.solve_isotherm`` /
 ``Program.solve_isotherm``.
 """
@@ -13,7 +13,7 @@ import numpy as np
 from . import batch as BT
 from .batch import NoSolutionError
 
-__all__ = ['Solver', 'Picard', 'Anderson', 'QuasiNewton', 'NoSolutionError']
+__all__ = ['Solver', 'Picard', 'Anderson', 'QuasiNewton', 'Fire', 'NoSolutionError']
 
 
 class Solver(object):
@@ -170,4 +170,36 @@ class QuasiNewton(Picard):
         self._last = s
         self.curr_step = int(s.steps)
         self.omega0 = float(s.omega0)
+        return float(N), r.cpu().numpy(), bool(conv)
+
+
+class Fire(Solver):
+    """FIRE / ABC-FIRE relaxation of the log-density (cmmdft/solver.py:606-698),
+    through ``fire.FireSolve``.  As in the reference the update acts on the
+    points of ``self.mask``, which the caller sets (a boolean field of the
+    grid's shape selecting points with rho > 0) before solving; without it
+    solve raises AttributeError, as the reference's update does."""
+    name = 'FIRE'
+
+    def __init__(self, program, nsteps=500, method='abc-fire', alpha=0.2, dt=0.02, **kwargs):
+        Solver.__init__(self, program, nsteps, **kwargs)
+        self.method = method
+        self.alpha0 = self.alpha = alpha
+        self.dt0 = self.dt = dt
+        self._solver = None
+
+    def solve(self, chempot, rho, log_level=2):
+        from .fire import FireSolve
+        mask = self.mask   # AttributeError when unset, as Fire.update_rho raises
+        if self._solver is None or self._solver.fn is not self.fener.device():
+            self._solver = FireSolve(self.fener.device(), mask, nsteps=self.nsteps, method=self.method,
+                                     alpha=self.alpha0, dt=self.dt0, threshold=self.threshold,
+                                     criterion=self.criterion, a_tol=self.a_tol, r_tol=self.r_tol)
+        else:
+            self._solver.set_mask(mask)
+        s = self._solver
+        N, r, conv = s.solve(chempot, rho)
+        self.curr_step = int(s.steps)
+        self.omega0 = float(s.omega0)
+        self.dt, self.alpha, self.Npos, self.Nneg = s.dt, s.alpha, s.Npos, s.Nneg
         return float(N), r.cpu().numpy(), bool(conv)

@@ -12,6 +12,7 @@ machines):
     python tests/golden/make_golden.py --reference <reference tree> --rot
     python tests/golden/make_golden.py --reference <reference tree> --rotinterp
     python tests/golden/make_golden.py --reference <reference tree> --proj
+    python tests/golden/make_golden.py --reference <reference tree> --fire
 
 ``--reference`` (or the environment variable CMM_REFERENCE_ROOT) names the
 root of the reference's source tree, the directory that holds ``cmmdft/``.
@@ -79,6 +80,14 @@ Outputs (small ``.npz`` files) land next to this script:
               ring atoms, project_density, save_loading_and_grand_potential,
               free_energy_path and project_contributions('fid',
               'pure_extpot'); with the densities themselves (``--proj``).
+  fire32.npz      the reference's Fire solver ('abc-fire' and 'fire') on
+              the 32^3 case at 1 bar from Ninit = rho_bulk, RES < 1e-6, the
+              mask (which the reference reads but never sets) = rho0 > 0:
+              steps, N, density and the final dt, alpha, N_pos, N_neg; a
+              second 'abc-fire' solve with the same solver object (its
+              counters carry over); and the first solves' rounding floors
+              (the same solves with the density moved one ulp up before
+              every update) (``--fire``).
   iso64_rho.npz   the converged densities of that isotherm at the pressure
               indices ISO_RHO_IDX, and the reference run against itself: the
               same points re-solved from a start perturbed by one ulp, with
@@ -706,6 +715,47 @@ def kjmol_unit():
     return kjmol
 
 
+def fire32(args):
+    """The reference's Fire solver on the 32^3 case."""
+    ref = import_reference(args.reference)
+    solver = ref[2]
+    from cmmdft_b200.hosts import cubic_host_276
+    from cmmdft_b200.units import boltzmann
+    T = 300.0
+    b = quiet(build, ref, 32, cubic_host_276(0), T, 1.0, tempfile.mkdtemp(prefix='cmm_fire_'))
+    fe, mu = b['fe'], b['mu']
+    V = fe.part_dict['ExtPot'].potential
+    mb = b['mbwr']
+    mb.set_temperature(T)
+    bulk = float(np.nanmin(mb.solve_densities_from_chempots([mu]), axis=1)[0])
+    rho0 = bulk * np.exp(-np.maximum(V, 0) / boltzmann / T)
+    out = dict(T=T, mu=mu, rho_bulk=bulk)
+    for meth, tag in (('abc-fire', 'abc'), ('fire', 'plain')):
+        f = solver.Fire(b['prog'], nsteps=400, method=meth, criterion='res', threshold=1e-6)
+        f.mask = rho0 > 0
+        runs = 2 if tag == 'abc' else 1
+        for r in range(runs):
+            N, rho, conv = quiet(f.solve, mu, rho0.copy(), 3)
+            key = '%s%d' % (tag, r)
+            out.update({key + '_steps': f.curr_step, key + '_N': N, key + '_conv': conv, key + '_rho': rho,
+                        key + '_dt': f.dt, key + '_alpha': f.alpha, key + '_Npos': f.Npos, key + '_Nneg': f.Nneg})
+            print(key, f.curr_step, N, conv, f.dt, f.alpha, f.Npos, f.Nneg, flush=True)
+        # the reference against itself with its density moved one ulp up
+        # before every update: the rounding floor of the first solve's
+        # trajectory under a per-step perturbation of rounding size
+        class _FireUlp(solver.Fire):
+            def update_rho(self, rho, krho, C1):
+                return solver.Fire.update_rho(self, np.nextafter(rho, np.inf), krho, C1)
+        f2 = _FireUlp(b['prog'], nsteps=400, method=meth, criterion='res', threshold=1e-6)
+        f2.mask = rho0 > 0
+        N2, rho2, _ = quiet(f2.solve, mu, rho0.copy(), 3)
+        key = tag + '0'
+        out[key + '_rho_floor'] = np.max(np.abs(rho2 - out[key + '_rho'])) / np.max(np.abs(out[key + '_rho']))
+        out[key + '_N_floor'] = abs(N2 - out[key + '_N']) / abs(out[key + '_N'])
+        print(key, 'floor rho %.2e N %.2e' % (out[key + '_rho_floor'], out[key + '_N_floor']), flush=True)
+    np.savez_compressed(os.path.join(HERE, 'fire32.npz'), **out)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument('--reference', default=os.environ.get('CMM_REFERENCE_ROOT'),
@@ -720,6 +770,7 @@ def main():
     ap.add_argument('--rot', action='store_true')
     ap.add_argument('--rotinterp', action='store_true')
     ap.add_argument('--proj', action='store_true')
+    ap.add_argument('--fire', action='store_true')
     ap.add_argument('--procs', type=int, default=8)
     args = ap.parse_args()
     if not args.reference:
@@ -740,6 +791,8 @@ def main():
         return rotinterp12(args)
     if args.proj:
         return proj32(args)
+    if args.fire:
+        return fire32(args)
     ref = import_reference(args.reference)
     solver = ref[2]
     from cmmdft_b200.hosts import cubic_host_276, HELIUM

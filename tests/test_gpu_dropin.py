@@ -331,3 +331,43 @@ def test_projections_and_free_energy_path(cuda, tmp_path):
     assert errs['fe_density'] < 1e-12 and errs['fe_omega'] < 1e-10 and errs['fe_free'] < 1e-10
     assert errs['fid'] < 1e-12 and errs['pure_extpot'] < 1e-12
     assert errs['ring_cvs'] < 1e-12 and errs['ring_cvs_mat'] < 1e-12
+
+
+def test_fire_against_reference(cuda, tmp_path):
+    """Fire (solver.py:606-698) through the drop-in API against the
+    reference's own runs (tests/golden/fire32.npz): 'abc-fire' twice with
+    one solver object (its N_pos / N_neg counters carry over) and 'fire',
+    from Ninit = rho_bulk to RES < 1e-6 with mask = rho0 > 0: the same step
+    counts and FIRE state, N and rho within max(1e-10, 3 x the reference's
+    own floor under a one-ulp perturbation per step) of the reference's; an
+    unset mask raises AttributeError as in the reference."""
+    from cmmdft_b200.units import boltzmann
+    ref = dict(np.load(os.path.join(ROOT, "tests", "golden", "fire32.npz")))
+    prog = make_program(tmp_path)
+    V = prog.fener.part_dict['ExtPot'].potential
+    mu, bulk = float(ref["mu"]), float(ref["rho_bulk"])
+    rho0 = bulk * np.exp(-np.maximum(V, 0) / boltzmann / T)
+    errs = {}
+    for meth, tag, runs in (('abc-fire', 'abc', 2), ('fire', 'plain', 1)):
+        f = cd.Fire(prog, nsteps=400, method=meth, criterion='res', threshold=1e-6)
+        if tag == 'abc':
+            with pytest.raises(AttributeError):
+                f.solve(mu, rho0.copy())
+        f.mask = rho0 > 0
+        for r in range(runs):
+            key = '%s%d' % (tag, r)
+            N, rho, conv = f.solve(mu, rho0.copy())
+            assert conv == bool(ref[key + "_conv"]) and f.curr_step == int(ref[key + "_steps"]), key
+            assert (f.Npos, f.Nneg) == (int(ref[key + "_Npos"]), int(ref[key + "_Nneg"])), key
+            errs[key] = dict(N=scalar_rel(N, ref[key + "_N"]), rho=relerr(rho, ref[key + "_rho"]),
+                             dt=scalar_rel(f.dt, ref[key + "_dt"]), alpha=scalar_rel(f.alpha, ref[key + "_alpha"]))
+    print("Fire vs reference:", {k: {q: "%.1e" % v for q, v in d.items()} for k, d in errs.items()})
+    for key, d in errs.items():
+        # the north star's 1e-10, or 3x the reference's own floor on the first
+        # solve's trajectory (the same solve with its density moved one ulp
+        # before every update); the second solve continues from the first's
+        # counters and is held to the first's floor
+        k0 = key[:-1] + '0'
+        fl = ref.get(k0 + "_rho_floor", 0.0), ref.get(k0 + "_N_floor", 0.0)
+        assert d['rho'] < max(1e-10, 3 * float(fl[0])) and d['N'] < max(1e-10, 3 * float(fl[1])), key
+        assert d['dt'] < 1e-14 and d['alpha'] < 1e-12, key
