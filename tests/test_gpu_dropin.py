@@ -363,7 +363,7 @@ def test_fire_against_reference(cuda, tmp_path):
                              dt=scalar_rel(f.dt, ref[key + "_dt"]), alpha=scalar_rel(f.alpha, ref[key + "_alpha"]))
     print("Fire vs reference:", {k: {q: "%.1e" % v for q, v in d.items()} for k, d in errs.items()})
     for key, d in errs.items():
-        # the north star's 1e-10, or 3x the reference's own floor on the first
+        # the target 1e-10, or 3x the reference's own floor on the first
         # solve's trajectory (the same solve with its density moved one ulp
         # before every update); the second solve continues from the first's
         # counters and is held to the first's floor

@@ -86,7 +86,7 @@ def test_lda_part_against_reference(golden32, tmp_path):
         assert e_d < 1e-12 and e_F < 1e-11
     s = BT.NativeBatchSolve(fn, [mu], method='static', nsteps=3, threshold=1e-30, criterion='res')
     N, rho, conv = s.solve(torch.as_tensor(golden32["rho_a"][None], device="cuda"))
-    # the north star's 1e-10, or three times the reference's own floor on this
+    # the target 1e-10, or three times the reference's own floor on this
     # trajectory (the same steps from a start one ulp above) where larger
     e_rho = relerr(rho[0].cpu().numpy(), ref["picard3_rho"])
     e_N = scalar_rel(N[0], ref["picard3_N"])
