@@ -238,15 +238,20 @@ def workspace(fn, B, nring, group=0):
         params=torch.zeros((B, 4), dtype=f64, device=dev),
         coef=torch.zeros((B, L.MAX_FIELDS), dtype=f64, device=dev),
         active=torch.zeros(B, dtype=torch.int32, device=dev),
-        pin=dict(active=[torch.zeros(B, dtype=torch.int32).pin_memory() for _ in range(8)],
-                 coef=[torch.zeros((B, L.MAX_FIELDS), dtype=f64).pin_memory() for _ in range(8)],
-                 params=[torch.zeros((B, 4), dtype=f64).pin_memory() for _ in range(8)]),
     )
     ws['buf'].part[:, L.STAT_N3MAX, :] = -np.inf
-    # pinned read-back buffers of the native driver
-    ws['pin_read'] = dict(stats=torch.zeros((B, L.NSTAT), dtype=f64).pin_memory(),
-                          ls=torch.zeros((B, L.NLS), dtype=f64).pin_memory(),
-                          alpha=torch.zeros(B, dtype=f64).pin_memory())
+    # pinned staging of uploads (8-deep rings) and the native driver's
+    # read-backs, carved from two page-locked blocks
+    nf = 8 * B * (L.MAX_FIELDS + 4) + B * (L.NSTAT + L.NLS + 1)
+    pf = torch.zeros(nf, dtype=f64, pin_memory=True)
+    pi = torch.zeros(8 * B, dtype=torch.int32, pin_memory=True)
+    cuts = itertools.accumulate([0] + [B * L.MAX_FIELDS] * 8 + [B * 4] * 8 + [B * L.NSTAT, B * L.NLS, B])
+    o = list(cuts)
+    ws['pin'] = dict(active=[pi[i * B:(i + 1) * B] for i in range(8)],
+                     coef=[pf[o[i]:o[i + 1]].view(B, L.MAX_FIELDS) for i in range(8)],
+                     params=[pf[o[8 + i]:o[9 + i]].view(B, 4) for i in range(8)])
+    ws['pin_read'] = dict(stats=pf[o[16]:o[17]].view(B, L.NSTAT), ls=pf[o[17]:o[18]].view(B, L.NLS),
+                          alpha=pf[o[18]:o[19]])
     cache[key] = ws
     return ws
 
@@ -1084,7 +1089,7 @@ class NativeBatchSolve(BatchSolve):
         stage = self.pin_read.get('stage')
         nstage = int(L.lib().cmm_solve_stage_bytes(B))
         if stage is None or stage.numel() < nstage:
-            stage = torch.empty(nstage, dtype=torch.uint8).pin_memory()
+            stage = torch.empty(nstage, dtype=torch.uint8, pin_memory=True)
             self.pin_read['stage'] = stage
         names = ("ring", "rres", "trial", "rho0", "spec_ring", "wd_ring", "wd_r", "rhat", "chat", "chat2", "that",
                  "params", "coef", "active", "ls_part", "ls", "ls_alpha")
