@@ -380,7 +380,8 @@ class Calculator(object):
             if 'pure_extpot' in name:
                 m = np.asarray(dist_mask, dtype=np.float64) * (~rho_mask)
                 tot, cnt = _binned_sums(cvs, cvs_mat, data, m, counts=True)
-                out[ee + 2] = tot / cnt
+                with np.errstate(invalid='ignore', divide='ignore'):
+                    out[ee + 2] = tot / cnt        # NaN in an empty bin, as the reference's 0/0
             else:
                 out[ee + 2] = _binned_sums(cvs, cvs_mat, data, dist_mask) * self.grid.dr
         if fn is None:

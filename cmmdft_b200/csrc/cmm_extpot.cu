@@ -558,14 +558,17 @@ __device__ void rot_finish(const RotArgs& c, const double* s_a, const double* __
 
 __global__ void __launch_bounds__(ROT_THREADS)
 k_extpot_rot(RotArgs c, const HostAtom* __restrict__ atoms, const MixLJ* __restrict__ mix,
-             const double* __restrict__ rot, const double* __restrict__ w, double* __restrict__ V) {
+             const double* __restrict__ rot, const double* __restrict__ w, double* __restrict__ V,
+             long long idx0, double* __restrict__ scratch) {
   __shared__ HostAtom tile[ROT_THREADS];
   __shared__ MixLJ smix[ROT_MAX_PAIRTYPES];
   __shared__ double frame[ROT_MAX_SITES + 1][3];   // rel_k, then COM
   __shared__ double red[32];
-  extern __shared__ double s_a[];                  // a_r, r < nrot
+  extern __shared__ double s_dyn[];
+  // a_r, r < nrot: in shared memory, or this block's row of a global scratch
+  double* s_a = scratch ? scratch + (size_t)blockIdx.x * c.nrot : s_dyn;
   const ExtArgs& a = c.a;
-  const long long idx = blockIdx.x;
+  const long long idx = idx0 + blockIdx.x;
   const int k = (int)(idx % a.n3), j = (int)((idx / a.n3) % a.n2), i = (int)(idx / ((long long)a.n3 * a.n2));
   for (int t = threadIdx.x; t < c.nsite * c.nhtype; t += blockDim.x) smix[t] = mix[t];
   rot_frame(c, i, j, k, frame);
@@ -609,6 +612,30 @@ k_extpot_rot(RotArgs c, const HostAtom* __restrict__ atoms, const MixLJ* __restr
   rot_finish(c, s_a, w, red, V + idx);
 }
 
+// Launch a rotation-average kernel over npts grid points: a_r in dynamic
+// shared memory when nrot fits (ROT_MAX_ROT), else in a global scratch of
+// one row per block, the points taken in chunks that keep it under 1 GiB
+// but never below 8 blocks per SM (7.3 GB at the largest Lebedev set).
+template <class Launch>
+static int rot_launch(long long npts, int nrot, const void* kern, cudaStream_t st, Launch launch) {
+  if (npts <= 0) return CMM_OK;
+  if (nrot <= ROT_MAX_ROT) {
+    const size_t dyn = sizeof(double) * (size_t)nrot;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess)
+      return CMM_ERR_CUDA;
+    for (long long p0 = 0; p0 < npts; p0 += 0x7fffffffLL)
+      launch((unsigned)std::min(npts - p0, 0x7fffffffLL), dyn, p0, (double*)nullptr);
+    return (cudaPeekAtLastError() == cudaSuccess) ? CMM_OK : CMM_ERR_CUDA;
+  }
+  const long long chunk = std::min(npts, std::max(148LL * 8, (1LL << 30) / (8LL * nrot)));
+  double* scr = nullptr;
+  if (cudaMallocAsync((void**)&scr, sizeof(double) * (size_t)chunk * nrot, st) != cudaSuccess) return CMM_ERR_NOMEM;
+  for (long long p0 = 0; p0 < npts; p0 += chunk) launch((unsigned)std::min(chunk, npts - p0), 0, p0, scr);
+  const int rc = (cudaPeekAtLastError() == cudaSuccess) ? CMM_OK : CMM_ERR_CUDA;
+  cudaFreeAsync(scr, st);
+  return rc;
+}
+
 extern "C" int cmm_extpot_rot(const cmm_grid* g, const double* d_pos, const int* d_type, int natom,
                               const double* d_type_sig, const double* d_type_eps, int ntype, const double* guest_pos,
                               const double* guest_mass, const double* guest_sig, const double* guest_eps, int nsite,
@@ -618,7 +645,7 @@ extern "C" int cmm_extpot_rot(const cmm_grid* g, const double* d_pos, const int*
   if (natom < 0 || ntype < 1 || nsite < 1 || nrot < 1 || !(beta > 0) ||
       (natom > 0 && (!d_pos || !d_type || !d_type_sig || !d_type_eps)))
     return CMM_ERR_ARG;
-  if (nsite > ROT_MAX_SITES || nsite * ntype > ROT_MAX_PAIRTYPES || nrot > ROT_MAX_ROT) return CMM_ERR_UNSUPPORTED;
+  if (nsite > ROT_MAX_SITES || nsite * ntype > ROT_MAX_PAIRTYPES) return CMM_ERR_UNSUPPORTED;
   cudaStream_t st = (cudaStream_t)stream;
   RotArgs c;
   memset(&c, 0, sizeof(c));
@@ -671,10 +698,6 @@ extern "C" int cmm_extpot_rot(const cmm_grid* g, const double* d_pos, const int*
       }
   }
   const long long npts = (long long)g->n1 * g->n2 * g->n3;
-  if (npts > 0x7fffffffLL) return CMM_ERR_SHAPE;
-  const size_t dyn = sizeof(double) * (size_t)nrot;
-  if (cudaFuncSetAttribute(k_extpot_rot, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) != cudaSuccess)
-    return CMM_ERR_CUDA;
   void* d = nullptr;
   const size_t ab = sizeof(HostAtom) * h.size(), mb = sizeof(MixLJ) * mx.size();
   if (cudaMalloc(&d, ab + mb) != cudaSuccess) return CMM_ERR_NOMEM;
@@ -684,10 +707,10 @@ extern "C" int cmm_extpot_rot(const cmm_grid* g, const double* d_pos, const int*
   if (cudaMemcpyAsync(da, h.data(), ab, cudaMemcpyHostToDevice, st) != cudaSuccess ||
       cudaMemcpyAsync(dm, mx.data(), mb, cudaMemcpyHostToDevice, st) != cudaSuccess)
     rc = CMM_ERR_CUDA;
-  if (rc == CMM_OK) {
-    k_extpot_rot<<<(unsigned)npts, ROT_THREADS, dyn, st>>>(c, da, dm, d_rot, d_w, d_V);
-    rc = (cudaPeekAtLastError() == cudaSuccess) ? CMM_OK : CMM_ERR_CUDA;
-  }
+  if (rc == CMM_OK)
+    rc = rot_launch(npts, nrot, (const void*)k_extpot_rot, st, [&](unsigned nb, size_t dyn, long long p0, double* scr) {
+      k_extpot_rot<<<nb, ROT_THREADS, dyn, st>>>(c, da, dm, d_rot, d_w, d_V, p0, scr);
+    });
   if (cudaStreamSynchronize(st) != cudaSuccess) rc = CMM_ERR_CUDA;
   cudaFree(d);
   return rc;
@@ -895,12 +918,14 @@ __device__ double tricubic_at(const double* __restrict__ tab, long long npts, co
 
 __global__ void __launch_bounds__(ROT_THREADS)
 k_extpot_rot_interp(RotArgs c, InterpArgs ia, const double* __restrict__ tab, const double* __restrict__ rot,
-                    const double* __restrict__ w, double* __restrict__ V) {
+                    const double* __restrict__ w, double* __restrict__ V, long long idx0,
+                    double* __restrict__ scratch) {
   __shared__ double frame[ROT_MAX_SITES + 1][3];
   __shared__ double red[32];
-  extern __shared__ double s_a[];
+  extern __shared__ double s_dyn[];
+  double* s_a = scratch ? scratch + (size_t)blockIdx.x * c.nrot : s_dyn;
   const ExtArgs& a = c.a;
-  const long long idx = blockIdx.x;
+  const long long idx = idx0 + blockIdx.x;
   const int k = (int)(idx % a.n3), j = (int)((idx / a.n3) % a.n2), i = (int)(idx / ((long long)a.n3 * a.n2));
   rot_frame(c, i, j, k, frame);
   __syncthreads();
@@ -929,7 +954,7 @@ extern "C" int cmm_extpot_rot_interp(const cmm_grid* g, const double* d_tab, int
   if (!g || !d_tab || !fine_n || !origin || !spacing || !guest_pos || !guest_mass || !site_tab || !d_rot || !d_w ||
       !d_V || ntab < 1 || nsite < 1 || nrot < 1 || !(beta > 0))
     return CMM_ERR_ARG;
-  if (nsite > ROT_MAX_SITES || nrot > ROT_MAX_ROT) return CMM_ERR_UNSUPPORTED;
+  if (nsite > ROT_MAX_SITES) return CMM_ERR_UNSUPPORTED;
   RotArgs c;
   memset(&c, 0, sizeof(c));
   InterpArgs ia;
@@ -954,14 +979,11 @@ extern "C" int cmm_extpot_rot_interp(const cmm_grid* g, const double* d_tab, int
   if (!(mt > 0)) return CMM_ERR_ARG;
   c.mtot = mt;
   const long long npts = (long long)g->n1 * g->n2 * g->n3;
-  if (npts > 0x7fffffffLL) return CMM_ERR_SHAPE;
   cudaStream_t st = (cudaStream_t)stream;
-  const size_t dyn = sizeof(double) * (size_t)nrot;
-  if (cudaFuncSetAttribute(k_extpot_rot_interp, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dyn) !=
-      cudaSuccess)
-    return CMM_ERR_CUDA;
-  k_extpot_rot_interp<<<(unsigned)npts, ROT_THREADS, dyn, st>>>(c, ia, d_tab, d_rot, d_w, d_V);
-  int rc = (cudaPeekAtLastError() == cudaSuccess) ? CMM_OK : CMM_ERR_CUDA;
+  int rc = rot_launch(npts, nrot, (const void*)k_extpot_rot_interp, st,
+                      [&](unsigned nb, size_t dyn, long long p0, double* scr) {
+                        k_extpot_rot_interp<<<nb, ROT_THREADS, dyn, st>>>(c, ia, d_tab, d_rot, d_w, d_V, p0, scr);
+                      });
   if (cudaStreamSynchronize(st) != cudaSuccess) rc = CMM_ERR_CUDA;
   return rc;
 }

@@ -195,7 +195,11 @@ int cmm_extpot_set_mode(int mode);
  * weighted log-sum-exp over rotations (weights d_w [nrot]) is taken in
  * float64 as scipy.special.logsumexp does; d_V = -lse / beta, NaN ->
  * v_limit.  No cap is applied (the caller caps as cmm_extpot_lj does).
- * nsite <= 8, nsite * ntype <= 128, nrot <= 6144.  Synchronous. */
+ * nsite <= 8, nsite * ntype <= 128.  Up to 6144 rotations the per-point
+ * rotation energies stay in shared memory; above that (Lebedev degree >= 27)
+ * they go to a stream-ordered global scratch (1 GiB, or 1184 points' rows
+ * where that is more), the points taken in chunks that fit it, with the same arithmetic and reduction order.
+ * Synchronous. */
 int cmm_extpot_rot(const cmm_grid* grid, const double* d_pos, const int* d_type, int natom,
                    const double* d_type_sig, const double* d_type_eps, int ntype,
                    const double* guest_pos, const double* guest_mass, const double* guest_sig,
@@ -219,7 +223,8 @@ int cmm_extpot_lj_deriv(const double* rvecs, int n1, int n2, int n3, const doubl
  * cmm_extpot_lj_deriv writes them); site s reads table site_tab[s]; the cell
  * of a site position q is floor((q - origin) / spacing) with periodic
  * corner indices.  Replaces ExternalPotential.generate_potential with
- * interpolate=True (cmmdft/functionals.py:1032-1055).  Synchronous. */
+ * interpolate=True (cmmdft/functionals.py:1032-1055).  Any nrot, as
+ * cmm_extpot_rot.  Synchronous. */
 int cmm_extpot_rot_interp(const cmm_grid* grid, const double* d_tab, int ntab, const int* fine_n,
                           const double* origin, const double* spacing, const double* guest_pos,
                           const double* guest_mass, const int* site_tab, int nsite, const double* d_rot,

@@ -164,3 +164,54 @@ def test_interpolated_potential_through_program(cuda, golden_rotinterp, tmp_path
     print("interpolated CO2 potential: %.2e of the cap, %.2e relative, %d of %d bit-identical"
           % (err, rel, int(np.sum(V == Vr_c)), V.size))
     assert err < 1e-9 and rel < 1e-6
+
+
+@pytest.mark.parametrize("interpolate", [False, True])
+def test_large_rotation_set_against_oracle(cuda, golden_rotinterp, interpolate, tmp_path):
+    """Lebedev degree 29 (8758 rotations): more rotations than one block's
+    shared memory holds, so the rotation energies go through the global
+    scratch of one row per grid point.  The 4^3 grid through
+    ExternalPotential.generate_potential against the oracle at 4 seeded
+    points: per point 1e-6 relative (the float32 storage of the site
+    potentials), non-finite values where the oracle has them."""
+    from oracle import cmm_oracle as O
+    ref = golden_rotinterp
+    h = cubic_host_276(0)
+    types = [str(t) for t in ref["guest_ffatypes"]]
+    tp = {t: (s, e) for t, s, e in zip(types, ref["guest_sigma"], ref["guest_epsilon"])}
+    guest = cd.NonSphericalGuest('CO2', pos=ref["guest_pos"], masses=ref["guest_masses"], ffatypes=types,
+                                 ffatype_ids=ref["guest_ffatype_ids"], ff=tp)
+    host = cd.NanoporousHost('synthetic', pos=h.pos, ffatypes=h.ffatypes, ffatype_ids=h.ffatype_ids, rvecs=h.rvecs,
+                             ff=h.ff)
+    n, deg, T = 4, 29, float(ref["T"])
+    prog = cd.Program(prefix=str(tmp_path), hostname='synthetic', guestname='CO2')
+    prog.set_system(host, guest)
+    prog.set_grid(npoints=n)
+    ext = cd.ExternalPotential(prog.grid, prog.system, cutoff=12 * angstrom, degree=deg,
+                                           interpolate=interpolate)
+    ext.generate_potential(temperature=T)
+    V = ext._V.cpu().numpy()
+    rot, w = combined_rotations(deg)
+    assert len(w) == 8758
+    g = np.linspace(-0.5, 0.5, n, endpoint=False)
+    idx = np.random.default_rng(11).integers(0, n, size=(4, 3))
+    pts = np.einsum('ab,ia->ib', h.rvecs, g[idx])
+    beta = 1 / T / boltzmann
+    if interpolate:
+        st = [types[i] for i in ref["guest_ffatype_ids"]]
+        fine_n = [int(np.ceil(l / ext.INTERP_SPACING)) for l in np.linalg.norm(h.rvecs, axis=1)]
+        Vo = O.interpolated_effective_potential(pts, ref["guest_pos"], ref["guest_masses"], st, tp, rot, w, beta,
+                                                h.ff, h.recentred_pos(), h.ffatypes, h.ffatype_ids, h.rvecs, fine_n,
+                                                prog.grid.points[0, 0, 0, :3], np.full(3, ext.INTERP_SPACING),
+                                                limit_potential=ext.limit_potential)
+    else:
+        ids = ref["guest_ffatype_ids"]
+        Vo = O.effective_potential(pts, ref["guest_pos"], ref["guest_masses"], ref["guest_sigma"][ids],
+                                   ref["guest_epsilon"][ids], rot, w, beta, h.ff, h.recentred_pos(), h.ffatypes,
+                                   h.ffatype_ids, h.rvecs, limit_potential=ext.limit_potential)
+    Vg = V[idx[:, 0], idx[:, 1], idx[:, 2]]
+    fin = np.isfinite(Vo) & (np.abs(Vo) < ext.limit_potential)
+    assert np.array_equal(np.isfinite(Vg) & (np.abs(Vg) < ext.limit_potential), fin)
+    rel = float(np.max(np.abs(Vg[fin] - Vo[fin]) / (np.abs(Vo[fin]) + 1e-6))) if fin.any() else 0.0
+    print("degree 29, interpolate=%s: %d finite points, max rel %.2e" % (interpolate, int(fin.sum()), rel))
+    assert fin.any() and rel < 1e-6
