@@ -30,6 +30,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 NPTS = (64, 64, 64)
+ROT_NPTS = (32, 32, 32)
 NPRESS = 24
 T = 300.0
 THRESH = 1e-8
@@ -592,6 +593,129 @@ def run_large(args):
     print(json.dumps(line))
 
 
+def _oracle_rot_sample(args):
+    """Oracle (numpy restatement of the reference's generate_effective_potential
+    and of its interpolated path) on ``m`` grid points; returns seconds."""
+    kind, degree, m = args
+    os.environ.setdefault("OMP_NUM_THREADS", "1")
+    sys.path.insert(0, ROOT)
+    from oracle import cmm_oracle as O
+    from cmmdft_b200.hosts import cubic_host_276, co2_trappe_guest
+    from cmmdft_b200.rotations import combined_rotations
+    from cmmdft_b200.units import angstrom, boltzmann
+    host = cubic_host_276(0)
+    g = co2_trappe_guest()
+    rot, w = combined_rotations(degree)
+    grid = O.OGrid(host.rvecs, npoints=list(ROT_NPTS))
+    pts = grid.points[..., :3].reshape(-1, 3)[:: max(1, int(np.prod(ROT_NPTS)) // m)][:m]
+    beta = 1 / T / boltzmann
+    t0 = time.perf_counter()
+    if kind == "direct":
+        O.effective_potential(pts, g["pos"], g["masses"], g["site_sigma"], g["site_epsilon"], rot, w, beta, host.ff,
+                              host.recentred_pos(), host.ffatypes, host.ffatype_ids, host.rvecs)
+    else:
+        st = [g["ffatypes"][i] for i in g["ffatype_ids"]]
+        fine_n = [int(np.ceil(l / (0.15 * angstrom))) for l in np.linalg.norm(host.rvecs, axis=1)]
+        O.interpolated_effective_potential(pts, g["pos"], g["masses"], st, g["ff"], rot, w, beta, host.ff,
+                                           host.recentred_pos(), host.ffatypes, host.ffatype_ids, host.rvecs, fine_n,
+                                           grid.points[0, 0, 0, :3], np.full(3, 0.15 * angstrom))
+    return time.perf_counter() - t0
+
+
+def run_rotavg(args):
+    """Secondary workload (not the headline line): the orientation-averaged
+    external potential of rigid TraPPE CO2 in the 276-atom cubic host at
+    300 K on a 32^3 grid, Lebedev degree 9 x planar rotations (342),
+    direct (k_extpot_rot) and tricubic-interpolated from 0.15 A derivative
+    grids (k_extpot_deriv + k_extpot_rot_interp).  ``value``: grid points/s
+    of the direct path on the device (inputs resident, CUDA events);
+    ``e2e``: ExternalPotential.generate_potential through the public API
+    (host arrays in, the potential back on the host); ``cpu_baseline``: the
+    oracle's restatement of the reference path on a sample of points, one
+    core."""
+    import torch
+    import multiprocessing as mp
+    import cmmdft_b200 as cd
+    from cmmdft_b200 import engine as E, workload as W
+    from cmmdft_b200.hosts import cubic_host_276, co2_trappe_guest
+    from cmmdft_b200.rotations import combined_rotations
+    from cmmdft_b200.system import Grid, System
+    from cmmdft_b200.units import angstrom, boltzmann, kjmol
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    degree = 9
+    host = cubic_host_276(0)
+    g = co2_trappe_guest()
+    rot, w = combined_rotations(degree)
+    beta = 1 / T / boltzmann
+    plan = E.GridPlan(ROT_NPTS, host.rvecs)
+    sig, eps = W.host_type_arrays(host)
+    pos = host.recentred_pos()
+    npt = int(np.prod(ROT_NPTS))
+
+    def direct():
+        return E.effective_potential(plan, pos, host.ffatype_ids, sig, eps, g["pos"], g["masses"], g["site_sigma"],
+                                     g["site_epsilon"], rot, w, 12 * angstrom, beta, 1e4 * kjmol)
+    nh = cd.NanoporousHost("synthetic", pos=host.pos, ffatypes=host.ffatypes, ffatype_ids=host.ffatype_ids,
+                           rvecs=host.rvecs, ff=host.ff)
+    guest = cd.NonSphericalGuest("CO2", pos=g["pos"], masses=g["masses"], ffatypes=g["ffatypes"],
+                                 ffatype_ids=g["ffatype_ids"], ff=g["ff"])
+    system = System(nh, guest)
+    grid = Grid(nh.cell, npoints=ROT_NPTS)
+
+    def api(interpolate):
+        ext = cd.ExternalPotential(grid, system, degree=degree, interpolate=interpolate, cutoff=12 * angstrom)
+        ext.generate_potential(temperature=T)
+        return ext.potential          # on the host
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    for _ in range(max(1, args.warmup)):
+        direct()
+        api(False)
+        api(True)
+    torch.cuda.synchronize()
+    nrep = max(1, min(args.steps, 5))
+    dev_ms, e2e_s = [], {}
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for _ in range(nrep):
+            ev[0].record()
+            direct()
+            ev[1].record()
+            torch.cuda.synchronize()
+            dev_ms.append(ev[0].elapsed_time(ev[1]))
+        for interp in (False, True):
+            t0 = time.perf_counter()
+            for _ in range(nrep):
+                api(interp)
+            e2e_s[interp] = (time.perf_counter() - t0) / nrep
+    ms = float(np.median(dev_ms))
+    pairs = float(npt) * len(w) * len(g["masses"]) * host.natom
+    cpu = {}
+    if not args.no_cpu:
+        ctx = mp.get_context("spawn")
+        with ctx.Pool(1) as pool:
+            for kind, m in (("direct", 1024), ("interpolated", 64)):
+                sec = pool.map(_oracle_rot_sample, [(kind, degree, m)])[0]
+                cpu[kind] = {"value": m / sec, "unit": "points/s", "cores": 1, "kind": "port",
+                             "sample": "%d of the %d grid points, numpy oracle of the reference's %s path "
+                                       "(pinned to it bit for bit)" % (m, npt, kind)}
+    line = {"metric": "orientation-averaged external potential, grid points/s (32^3, CO2, 342 rotations)",
+            "value": npt / (ms / 1e3), "unit": "points/s", "n_gpus": 1, "steps": nrep, "warmup": args.warmup,
+            "ms_per_step": ms, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+            "data": "synthetic",
+            "config": {"workload": "rotavg-co2-32cubed", "grid": list(ROT_NPTS),
+                       "host": "cubic a=17A 276 atoms seed 0", "guest": "rigid TraPPE CO2 (3 sites)",
+                       "degree": degree, "rotations": len(w), "temperature_K": T, "cutoff_A": 12.0},
+            "roofline": {"bound": "fp64", "kernel": "k_extpot_rot", "site_atom_pairs": pairs,
+                         "pairs_per_s": pairs / (ms / 1e3), "flop_per_pair": 25,
+                         "achieved": 25 * pairs / (ms / 1e3) / 1e12, "unit": "TFLOP/s", "peak": None,
+                         "note": "no measured FP64 peak on this pool; minimum-image LJ over all host atoms"},
+            "e2e": {"direct": {"value": npt / e2e_s[False], "unit": "points/s"},
+                    "interpolated": {"value": npt / e2e_s[True], "unit": "points/s"},
+                    "includes": "ExternalPotential.generate_potential: host arrays to the device, rotation "
+                                "set, kernels, potential back to the host"},
+            "cpu_baseline": cpu or None, "clocks": clk.summary()}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -612,11 +736,26 @@ def main():
     ap.add_argument("--max-iters", type=int, default=500, help="solver step cap (lower it only to profile)")
     ap.add_argument("--autotune", action="store_true",
                     help="uneven workload: tune each host grid's FFT schedule first and solve with it")
-    ap.add_argument("--workload", choices=("isotherm64", "uneven", "gradient", "large"), default="isotherm64",
+    ap.add_argument("--workload", choices=("isotherm64", "uneven", "gradient", "large", "rotavg"),
+                    default="isotherm64",
                     help="isotherm64: the headline 64^3 isotherm; uneven: 8 uneven hosts x 32 pressures; "
                          "gradient: the 96^3 excess-isotherm loss gradient; large: the 256^3 WDA isotherm of "
-                         "the 64 A host")
+                         "the 64 A host; rotavg: the orientation-averaged CO2 potential at 32^3")
     args = ap.parse_args()
+    if args.workload == "rotavg":
+        if args.impl == "reference":
+            if int(os.environ.get("RANK", "0")) == 0:
+                sec = _oracle_rot_sample(("direct", 9, 1024))
+                print(json.dumps({"impl": "reference", "metric": "orientation-averaged external potential, grid "
+                                  "points/s (32^3, CO2, 342 rotations)", "value": 1024 / sec, "unit": "points/s",
+                                  "higher_is_better": True,
+                                  "cpu_baseline": {"value": 1024 / sec, "kind": "port", "cores": 1,
+                                                   "sample": "1024 of the 32768 grid points"},
+                                  "e2e": {"value": 1024 / sec, "unit": "points/s", "h2d_bytes_per_step": 0,
+                                          "d2h_bytes_per_step": 0}}))
+        elif int(os.environ.get("RANK", "0")) == 0:
+            run_rotavg(args)
+        return
     if args.workload == "large":
         if args.impl == "reference":
             print(json.dumps({"impl": "reference", "unavailable": "the 256^3 large-cell workload takes hours per "

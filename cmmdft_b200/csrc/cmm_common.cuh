@@ -87,3 +87,17 @@ struct cmm_grid {
 static inline int cmm_div_up(long long a, long long b) { return (int)((a + b - 1) / b); }
 
 __device__ __forceinline__ bool cmm_isfinite(double x) { return isfinite(x); }
+
+// A hint: bring [p, p + bytes) into L2 by bulk prefetches of at most 16 KB
+// (cp.async.bulk.prefetch.L2).  Issued by one thread; skipped unless p and
+// bytes are multiples of 16 bytes.  Plane passes call it for the real-space
+// planes their pointwise step reads, so that those reads hit L2 instead of
+// waiting on HBM one loop iteration at a time.
+__device__ __forceinline__ void cmm_prefetch_l2(const void* p, size_t bytes) {
+  if ((((uintptr_t)p) & 15) || (bytes & 15)) return;
+  const char* c = (const char*)p;
+  for (size_t o = 0; o < bytes; o += 16384) {
+    const unsigned n = (unsigned)((bytes - o) < 16384 ? (bytes - o) : 16384);
+    asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(c + o), "r"(n) : "memory");
+  }
+}

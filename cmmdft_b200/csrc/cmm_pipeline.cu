@@ -1321,12 +1321,15 @@ k_plane_picard(GridDev g, const int* __restrict__ active, const double* __restri
   PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
   const PlaneShape<N2C, M3C> sh(g);
   const size_t poff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3;
+  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
+  const double* Vp = V + b * vstride + (size_t)i1 * sh.n2 * sh.n3;
+  const size_t pbytes = sizeof(double) * sh.n2 * sh.n3;
+  if (threadIdx.x == 0) cmm_prefetch_l2(Vp, pbytes);
+  if (threadIdx.x == 32) cmm_prefetch_l2(rho + roff, pbytes);
   load_spec_planes<N2C, M3C>(g, s, 1, chat, poff, 0);
   __syncthreads();
   plane_inverse<N2C, M3C>(g, s, 1);
   const double fug = params[b * 4 + 0], a = params[b * 4 + 1], mu = params[b * 4 + 2];
-  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
-  const double* Vp = V + b * vstride + (size_t)i1 * sh.n2 * sh.n3;
   PlaneStats st = {0, 0, 0, 0, 0};
   double res2 = 0.0, gnf = 0.0, der = 0.0;
   for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
@@ -1376,13 +1379,24 @@ k_plane_residual(GridDev g, const int* __restrict__ active, const double* __rest
   PlaneSmem s = plane_smem_setup<N2C, M3C>(g, 1);
   const PlaneShape<N2C, M3C> sh(g);
   const size_t poff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.h3;
+  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
+  const size_t hoff = (size_t)b * hstride + (size_t)i1 * sh.n2 * sh.n3;
+  const double* Vp = V + b * vstride + (size_t)i1 * sh.n2 * sh.n3;
+  {
+    const size_t pbytes = sizeof(double) * sh.n2 * sh.n3;
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      if (w == 0) cmm_prefetch_l2(Vp, pbytes);
+      else if (w == 1) cmm_prefetch_l2(rho + roff, pbytes);
+#pragma unroll
+      for (int h = 0; h < CMM_MAX_HIST; ++h)   // static indices: the pointer table stays in parameter space
+        if (w == h + 2 && h < nhist) cmm_prefetch_l2(hist.p[h] + hoff, pbytes);
+    }
+  }
   load_spec_planes<N2C, M3C>(g, s, 1, chat, poff, 0);
   __syncthreads();
   plane_inverse<N2C, M3C>(g, s, 1);
   const double fug = params[b * 4 + 0], mu = params[b * 4 + 2];
-  const size_t roff = ((size_t)b * g.n1 + i1) * sh.n2 * sh.n3;
-  const size_t hoff = (size_t)b * hstride + (size_t)i1 * sh.n2 * sh.n3;
-  const double* Vp = V + b * vstride + (size_t)i1 * sh.n2 * sh.n3;
   double res2 = 0.0, gnf = 0.0, der = 0.0;
   double gram[CMM_MAX_HIST];
 #pragma unroll
@@ -1435,6 +1449,18 @@ k_plane_mix(GridDev g, const int* __restrict__ active, const double* __restrict_
   double c[CMM_MAX_FIELDS];
 #pragma unroll
   for (int j = 0; j < CMM_MAX_FIELDS; ++j) c[j] = (j < nfield) ? coef[b * CMM_MAX_FIELDS + j] : 0.0;
+  {
+    const size_t pbytes = sizeof(double) * sh.n2 * sh.n3;
+    const int w = threadIdx.x >> 5;
+    if ((threadIdx.x & 31) == 0) {
+      if (w == 0) cmm_prefetch_l2(Vp, pbytes);
+      else if (w == 1) cmm_prefetch_l2(Rp, pbytes);
+#pragma unroll
+      for (int f = 0; f < CMM_MAX_FIELDS; ++f)
+        if (w == f + 2 && f < nfield && c[f] != 0.0)
+          cmm_prefetch_l2(fields.p[f] + b * fields.stride[f] + plane, pbytes);
+    }
+  }
   PlaneStats st = {0, 0, 0, 0, 0};
   for (int i = threadIdx.x; i < sh.n2 * sh.n3; i += blockDim.x) {
     const int r = i / sh.n3, j = i - r * sh.n3;

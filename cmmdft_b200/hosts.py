@@ -173,3 +173,24 @@ def cubic_host_64(seed=4, density_A3=0.056):
     276-atom cell's atom density (14,680 atoms, the same type mix)."""
     natom = int(round(density_A3 * 64.0 ** 3))
     return random_sequential_host((64.0, 64.0, 64.0), natom, seed)
+
+
+# Rigid TraPPE CO2 (Potoff and Siepmann, AIChE J. 47, 1676 (2001)): C-O bond
+# 1.16 angstrom, site (sigma [angstrom], epsilon/kB [K]) and mass [amu].
+CO2_TRAPPE = {"bond": 1.16, "types": {"O_CD": (3.05, 79.0), "C_CD": (2.80, 27.0)},
+              "masses": {"O_CD": 15.9994, "C_CD": 12.0107}}
+
+
+def co2_trappe_guest():
+    """Sites of rigid linear CO2 along z (O, C, O): dict with pos [3, 3],
+    masses [3], ffatypes, ffatype_ids, ff {type: (sigma, epsilon)} and the
+    per-site sigma/epsilon arrays, all in atomic units."""
+    b = CO2_TRAPPE["bond"] * angstrom
+    types = ["O_CD", "C_CD"]
+    ids = np.array([0, 1, 0], dtype=np.int32)
+    ff = {t: (CO2_TRAPPE["types"][t][0] * angstrom, CO2_TRAPPE["types"][t][1] * boltzmann) for t in types}
+    pos = np.array([[0.0, 0.0, b], [0.0, 0.0, 0.0], [0.0, 0.0, -b]])
+    masses = np.array([CO2_TRAPPE["masses"][types[i]] * amu for i in ids])
+    return dict(pos=pos, masses=masses, ffatypes=types, ffatype_ids=ids, ff=ff,
+                site_sigma=np.array([ff[types[i]][0] for i in ids]),
+                site_epsilon=np.array([ff[types[i]][1] for i in ids]))

@@ -215,3 +215,34 @@ def test_large_rotation_set_against_oracle(cuda, golden_rotinterp, interpolate, 
     rel = float(np.max(np.abs(Vg[fin] - Vo[fin]) / (np.abs(Vo[fin]) + 1e-6))) if fin.any() else 0.0
     print("degree 29, interpolate=%s: %d finite points, max rel %.2e" % (interpolate, int(fin.sum()), rel))
     assert fin.any() and rel < 1e-6
+
+
+def test_five_site_guest_against_oracle(cuda):
+    """A five-site guest (tetrahedral CH4-like: a centre and four sites at
+    1.09 A) takes the kernel's any-guest form (more than three sites in
+    registers): the 4^3 grid at Lebedev degree 5 against the oracle at every
+    point, per point 1e-6 relative (float32 site sums), non-finite values
+    where the oracle has them."""
+    from oracle import cmm_oracle as O
+    h = cubic_host_276(0)
+    sig, eps = W.host_type_arrays(h)
+    d = 1.09 * angstrom / np.sqrt(3.0)
+    gpos = np.array([[0, 0, 0], [d, d, d], [-d, -d, d], [-d, d, -d], [d, -d, -d]], dtype=float)
+    gm = np.array([12.011, 1.008, 1.008, 1.008, 1.008])
+    ss = np.array([3.40, 2.65, 2.65, 2.65, 2.65]) * angstrom
+    se = np.array([55.0, 7.9, 7.9, 7.9, 7.9]) * boltzmann
+    n = 4
+    plan = E.GridPlan((n, n, n), h.rvecs)
+    rot, w = combined_rotations(5)
+    beta = 1 / 300.0 / boltzmann
+    V = E.effective_potential(plan, h.recentred_pos(), h.ffatype_ids, sig, eps, gpos, gm, ss, se, rot, w,
+                              12 * angstrom, beta, CAP).cpu().numpy().ravel()
+    g = np.linspace(-0.5, 0.5, n, endpoint=False)
+    idx = np.stack(np.meshgrid(np.arange(n), np.arange(n), np.arange(n), indexing='ij'), -1).reshape(-1, 3)
+    pts = np.einsum('ab,ia->ib', h.rvecs, g[idx])
+    Vo = O.effective_potential(pts, gpos, gm, ss, se, rot, w, beta, h.ff, h.recentred_pos(), h.ffatypes,
+                               h.ffatype_ids, h.rvecs, limit_potential=CAP)
+    rel, capped, exact = compare(V, Vo)
+    print("five-site guest, degree 5: max rel %.2e, capped %.2e of the cap, %d of %d bit-identical"
+          % (rel, capped, exact, V.size))
+    assert rel < 1e-6 and capped < 1e-9
