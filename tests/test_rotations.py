@@ -126,3 +126,19 @@ def test_oracle_interpolated_potential_is_bit_exact(golden_rotinterp):
                                             h.ffatype_ids, h.rvecs, ref["fine_npoints"], ref["origin"],
                                             ref["interp_spacing"])
     assert np.array_equal(Vo, ref["V"][idx[:, 0], idx[:, 1], idx[:, 2]])
+
+
+def test_co2_trappe_guest_matches_reference_files(golden_rot):
+    """The rigid TraPPE CO2 of the rotation-average benchmark line has the
+    geometry and site LJ parameters of the reference's own guest files
+    (positions to 1e-15 bohr; masses from standard atomic weights, within
+    2e-7 relative of the reference's)."""
+    from cmmdft_b200.hosts import co2_trappe_guest
+    ref = golden_rot
+    g = co2_trappe_guest()
+    ids = ref["guest_ffatype_ids"]
+    assert np.abs(g["pos"] - ref["guest_pos"]).max() < 1e-15
+    assert np.array_equal(g["site_sigma"], ref["guest_sigma"][ids])
+    assert np.array_equal(g["site_epsilon"], ref["guest_epsilon"][ids])
+    assert [g["ffatypes"][i] for i in g["ffatype_ids"]] == [str(ref["guest_ffatypes"][i]) for i in ids]
+    assert np.abs(g["masses"] / ref["guest_masses"] - 1).max() < 2e-7
