@@ -120,7 +120,9 @@ def solve_batch(hosts, pressures, temperature, guest, npoints=None, spacing=0.25
     # the caching allocator hands a finished host's blocks to the next host on
     # the same stream, so hosts neither free device memory (which synchronises
     # the device under the hosts still running) nor allocate it afresh.
-    free_streams = [torch.cuda.Stream(device=device) for _ in range(max(1, int(max_concurrent)))]
+    # The slots' streams are the same ones on every call (BT._group_streams),
+    # so a call's workspaces come from the blocks the previous call freed.
+    free_streams = list(BT._group_streams(max(1, int(max_concurrent))))
 
     def admit(i):
         with cond:

@@ -46,4 +46,7 @@ def test_every_schedule_gives_the_same_transforms(shape):
         else:
             assert np.max(np.abs(c1 - base)) < 1e-12 * np.max(np.abs(base)), sched
     best, table = AT.tune(shape, host.rvecs, batch=2, max_candidates=16)
-    assert best in [t[0] for t in table] and table[0][0] == best
+    assert best in [t[0] for t in table]
+    ms = {tuple(t[0]): t[2] for t in table}
+    # the fastest, or the default one when nothing beats it by more than 5 %
+    assert best == table[0][0] or (best == [0, 0, 0, -1, 0] and table[0][2] > 0.95 * ms[tuple(best)])
