@@ -789,6 +789,74 @@ def run_rotavg(args):
     print(json.dumps(line))
 
 
+def run_solvers(args):
+    """Secondary workload (not the headline line): one pressure point (1 bar)
+    of the 64^3 isotherm host from Ninit = rho_bulk through each solver the
+    package carries: static Picard (device-resident loop), hybrid Anderson
+    (the headline's solver, one instance), QuasiNewton (L-BFGS with the
+    backtracking search) and FIRE ('abc-fire', mask rho0 > 0), each to its
+    criterion; device time of one solve (CUDA events, after one untimed
+    solve), solver steps and ms per step."""
+    import torch
+    from cmmdft_b200 import batch as BT, workload as W
+    from cmmdft_b200.fire import FireSolve
+    from cmmdft_b200.quasinewton import QuasiNewtonSolve
+    from cmmdft_b200.hosts import cubic_host_276, methane_guest_params
+    from cmmdft_b200.units import bar
+    torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+    host, guest = cubic_host_276(0), methane_guest_params()
+    fn = W.build_functional(host, NPTS, T, guest)
+    mus, bulks = W.isotherm_inputs(np.array([1.0]) * bar, T, guest)
+    mu = float(mus[0])
+    rho0 = W.initial_density(fn, mus, ninit=bulks)
+
+    def picard():
+        s = BT.NativeBatchSolve(fn, mus, method="static", nsteps=2000, threshold=1e-6, criterion="res")
+        s.solve(rho0)
+        return int(s.steps[0]), bool(s.conv[0])
+
+    def hybrid_anderson():
+        s = BT.NativeBatchSolve(fn, mus, method="hybridanderson", nsteps=500, threshold=THRESH, criterion="res")
+        s.solve(rho0)
+        return int(s.steps[0]), bool(s.conv[0])
+
+    def quasi_newton():
+        s = QuasiNewtonSolve(fn, nsteps=500, method="bfgs", line_search="backtracking", threshold=THRESH,
+                             criterion="res")
+        _, _, conv = s.solve(mu, rho0[0])
+        return int(s.steps), bool(conv)
+
+    def fire():
+        s = FireSolve(fn, (rho0[0] > 0).cpu().numpy(), nsteps=2000, method="abc-fire", threshold=1e-6,
+                      criterion="res")
+        _, _, conv = s.solve(mu, rho0[0])
+        return int(s.steps), bool(conv)
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2)]
+    out = {}
+    with ClockSampler(int(os.environ.get("LOCAL_RANK", "0"))) as clk:
+        for name, f, crit in (("static Picard", picard, "RES<1e-6"), ("hybrid Anderson m=5", hybrid_anderson,
+                                                                        "RES<1e-8"),
+                              ("QuasiNewton bfgs backtracking", quasi_newton, "RES<1e-8"),
+                              ("FIRE abc-fire", fire, "RES<1e-6")):
+            f()
+            torch.cuda.synchronize()
+            ev[0].record()
+            steps, conv = f()
+            ev[1].record()
+            torch.cuda.synchronize()
+            ms = ev[0].elapsed_time(ev[1])
+            out[name] = {"ms": ms, "steps": steps, "converged": conv, "ms_per_step": ms / max(steps, 1),
+                         "criterion": crit}
+    ha = out["hybrid Anderson m=5"]
+    line = {"metric": "single-point solve time per solver, 64^3 FP64 at 1 bar (ms)", "value": ha["ms"],
+            "unit": "ms", "n_gpus": 1, "steps": 1, "warmup": 1, "ms_per_step": ha["ms"], "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "solvers-64cubed-1bar", "grid": list(NPTS), "host": "cubic a=17A 276 atoms seed 0",
+                       "pressure_bar": 1.0, "start": "Ninit=rho_bulk"},
+            "solvers": out, "clocks": clk.summary()}
+    print(json.dumps(line))
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -809,12 +877,20 @@ def main():
     ap.add_argument("--max-iters", type=int, default=500, help="solver step cap (lower it only to profile)")
     ap.add_argument("--autotune", action="store_true",
                     help="uneven workload: tune each host grid's FFT schedule first and solve with it")
-    ap.add_argument("--workload", choices=("isotherm64", "uneven", "gradient", "large", "rotavg"),
+    ap.add_argument("--workload", choices=("isotherm64", "uneven", "gradient", "large", "rotavg", "solvers"),
                     default="isotherm64",
                     help="isotherm64: the headline 64^3 isotherm; uneven: 8 uneven hosts x 32 pressures; "
                          "gradient: the 96^3 excess-isotherm loss gradient; large: the 256^3 WDA isotherm of "
-                         "the 64 A host; rotavg: the orientation-averaged CO2 potential at 32^3")
+                         "the 64 A host; rotavg: the orientation-averaged CO2 potential at 32^3; solvers: one "
+                         "64^3 point through each solver")
     args = ap.parse_args()
+    if args.workload == "solvers":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "unavailable": "a per-solver timing line of the package only; "
+                                                                "the reference arm times the isotherm workload"}))
+        elif int(os.environ.get("RANK", "0")) == 0:
+            run_solvers(args)
+        return
     if args.workload == "rotavg":
         if args.impl == "reference":
             if int(os.environ.get("RANK", "0")) == 0:
