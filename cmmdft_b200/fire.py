@@ -44,6 +44,9 @@ class FireSolve(QuasiNewtonSolve):
         if m.numel() != self.npts:
             raise ValueError("mask must have one entry per grid point")
         self.mask = m
+        # the masked points as indices (ascending, as boolean indexing takes
+        # them): gathers and scatters by index need no device read-back
+        self.midx = torch.nonzero(m).squeeze(1)
 
     def _solve(self, rho):
         self.vel = torch.zeros(self.npts, dtype=torch.float64, device="cuda")   # _initiate_solving (V there)
@@ -51,7 +54,7 @@ class FireSolve(QuasiNewtonSolve):
         return super()._solve(rho)
 
     def update(self, rho, C1):   # Fire.update_rho (solver.py:660-698)
-        m = self.mask
+        m = self.midx   # the mask's points, in the order boolean indexing gives them
         beta = self.fn.beta
         lnrho = torch.where(rho > 0, torch.log(torch.where(rho > 0, rho, torch.ones_like(rho))), torch.zeros_like(rho))
         F = -beta * self.domega(rho, C1)
