@@ -53,20 +53,24 @@ def _lbfgs(g, dX, dG, h0, eps=1e-12):
     q = g.clone()
     kept = []
     mk = len(dX)
+    # s.y, |s| and |y| of every pair do not depend on q: one read-back for
+    # all of them (the same reductions, so the same values)
+    sc = torch.stack([v for s, y in zip(dX, dG) for v in (torch.dot(s, y), torch.linalg.vector_norm(s),
+                                                          torch.linalg.vector_norm(y))]).cpu().tolist() if mk else []
     for i in range(mk - 1, -1, -1):
         s, y = dX[i], dG[i]
-        sy = _dot(s, y)
-        if sy <= eps * _norm(s) * _norm(y):
+        sy, ns, ny = sc[3 * i:3 * i + 3]
+        if sy <= eps * ns * ny:
             continue
         r = 1.0 / sy
-        a = r * _dot(s, q)
+        a = r * torch.dot(s, q)   # a device scalar: the same double products, no read-back
         q -= a * y
         kept.append((i, a, r))
     if (mk - len(kept)) / mk > 0.5:
         raise SwitchToPicard('Too many skipped pairs')
     z = h0 * q
     for i, a, r in reversed(kept):
-        b = r * _dot(dG[i], z)
+        b = r * torch.dot(dG[i], z)
         z += dX[i] * (a - b)
     return -z
 
