@@ -156,8 +156,10 @@ class QuasiNewtonSolve(object):
         spec = self.plan.rfft_yz(rho.reshape((1,) + self.plan.npoints))
         chat = self.plan.new_spec(1) if want & 1 else None
         self.fn.c1(buf, spec, chat, want=want)
-        E.finalize(buf, (1 << L.NSTAT) - 1)
-        st = buf.stats[0].cpu().numpy()
+        st = None
+        if want & 6:   # the sums stay on the device; the caller reads them back with its own
+            E.finalize(buf, (1 << L.NSTAT) - 1)
+            st = buf.stats[0]
         C1 = self.plan.irfft_yz(chat).reshape(-1) + self.V if want & 1 else None
         return C1, st
 
@@ -170,13 +172,17 @@ class QuasiNewtonSolve(object):
     def omega(self, rho):   # _get_Omega (solver.py:103-119); stores omega0
         _, st = self._pipeline(rho, 2)
         fn, dV = self.fn, self.dV
-        N = float(rho.sum()) * dV
         rr = self._clip(rho)
-        fid = float((rr * (torch.log(fn.lambda3 * rr) - 1.0)).sum()) * dV / fn.beta
+        # one read-back of the pipeline's sums and the three reductions here
+        sums = torch.stack([rho.sum(), (rr * (torch.log(fn.lambda3 * rr) - 1.0)).sum(), (rho * self.V).sum()])
+        vals = torch.cat([st, sums]).cpu().numpy()
+        st, (s_n, s_id, s_ext) = vals[:L.NSTAT], vals[L.NSTAT:]
+        N = float(s_n) * dV
+        fid = float(s_id) * dV / fn.beta
         G = fid - self.mu * N
         G += st[L.STAT_PHI] * dV / fn.beta
         G += 0.5 * st[L.STAT_MFA] * dV
-        G += float((rho * self.V).sum()) * dV
+        G += float(s_ext) * dV
         self.omega0 = G
         return G
 
